@@ -1,0 +1,245 @@
+/*
+ * mdff_engine.h -- C ABI of the B200 force engine for the MDFF force and
+ * integration hot path.
+ *
+ * The reference (MDFF, Fortran 90 + MPI) has no argument-passing interface on
+ * this path: engforce_driver (src/field.f90:1111) and the integrators
+ * (src/integration.f90:131,476) read and write module globals.  Every entry
+ * point below replaces one of those routines; the comment on each names the
+ * reference routine and file:line it stands in for.  A Fortran caller binds
+ * these with iso_c_binding (fortran/mdff_engine.f90); Python binds them with
+ * ctypes (mdff_b200/abi.py).
+ *
+ * Conventions
+ *   - Arrays are structure-of-arrays FP64, one array per Cartesian component,
+ *     exactly like rx(natm), ry(natm), rz(natm) in src/config.f90:44-89.
+ *   - Atom types and neighbour-list indices are 1-based, as in the reference.
+ *   - The cell matrix A[9] is column-major (Fortran order): A[3*j+i] is
+ *     component i of basis vector j, i.e. simu_cell%A(i+1,j+1).
+ *   - Per-type tables in mdff_params are indexed [i][j] for the reference's
+ *     (i+1,j+1); the 3-index damping tables [p][i][j] for (p+1,i+1,j+1).
+ *   - Input units are the control-file units of the reference: lengths in
+ *     Angstrom, energies in eV, masses in amu, charges in e, dt and
+ *     timesca_thermo in ps, temp in K (src/md.f90:314-324 conversions are done
+ *     inside the engine).  With lreduced != 0 every unit factor is 1
+ *     (src/constants.f90:135-146).
+ *   - Every call returns 0 on success or a negative MDFF_E_* code; the message
+ *     is available from mdff_last_error().  The library never exits or traps.
+ *   - One context per host thread; a context owns one CUDA stream and all its
+ *     device buffers.  No caller pointer is retained past a call.
+ */
+#ifndef MDFF_ENGINE_H
+#define MDFF_ENGINE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDFF_NTYPE_MAX 16          /* ntypemax, src/config.f90:40 */
+#define MDFF_TT_MAX_ORDER 8        /* maximum_of_TT_expansion, src/tt_damp.f90:8 */
+
+/* status codes */
+#define MDFF_OK            0
+#define MDFF_E_ARG        -1       /* invalid argument / parameter */
+#define MDFF_E_CUDA       -2       /* CUDA runtime error */
+#define MDFF_E_NOCONV     -3       /* induced-dipole solve did not converge */
+#define MDFF_E_LISTOVF    -4       /* neighbour list capacity exceeded (host regrows and retries) */
+#define MDFF_E_NONFINITE  -5       /* NaN/Inf in energies or forces */
+#define MDFF_E_STATE      -6       /* call out of order (e.g. step before set_system) */
+#define MDFF_E_UNSUPPORTED -7      /* feature outside the engine's scope */
+#define MDFF_E_NOMEM      -8       /* device allocation failed */
+
+/* ctrunc (src/field.f90:54-58) */
+#define MDFF_TRUNC_NONE      0
+#define MDFF_TRUNC_LINEAR    1
+#define MDFF_TRUNC_QUADRATIC 2
+
+/* algo_moment_from_pola (src/field.f90:150-152) */
+#define MDFF_POLA_SCF 0            /* reference fixed-point iteration */
+#define MDFF_POLA_PCG 1            /* preconditioned conjugate gradient (new) */
+
+/* algo_ext_dipole (src/field.f90:146-148) */
+#define MDFF_EXT_POLY 0
+#define MDFF_EXT_ASPC 1
+
+/* integrator (src/md.f90:71-76); only the two on the hot path */
+#define MDFF_NVE_VV   0
+#define MDFF_NVT_NHCN 1
+
+/* arithmetic of the bulk pair and k-space work */
+#define MDFF_PREC_FP64  0          /* plain FP64 everywhere */
+#define MDFF_PREC_MIXED 1          /* FP32 bulk + FP64 accumulation/scalars */
+
+/*
+ * Parameters: the union of &controltag (src/control.f90:128-160), &fieldtag
+ * (src/field.f90:450-500) and &mdtag (src/md.f90:109-132) tags on the path,
+ * plus engine choices.  mdff_params_default() fills the reference defaults
+ * (control_default_tag, field_default_tag, md_default_tag).
+ */
+typedef struct mdff_params {
+    int ntype;
+    /* &controltag */
+    int lnmlj, lbmhft, lbmhftd, lmorse, lcoulomb, lvnlist, lreduced, lsurf;
+    double cutshortrange, cutlongrange, skindiff;
+    /* &fieldtag: per-type properties */
+    double mass[MDFF_NTYPE_MAX];
+    double qch[MDFF_NTYPE_MAX];
+    double dip[MDFF_NTYPE_MAX][3];             /* static dipoles */
+    double poldip_iso[MDFF_NTYPE_MAX];         /* isotropic dipole polarisability, A^3 */
+    int    ldip_polar[MDFF_NTYPE_MAX];
+    int    symmetric_pot;
+    int    trunc;                              /* MDFF_TRUNC_* */
+    double epslj[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double sigmalj[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double plj[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double qlj[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double epsmor[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double sigmamor[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double rhomor[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double Abmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double Bbmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double Cbmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double Dbmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double BDbmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    int    ldip_damping[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double dip_pol_damp_b[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double dip_pol_damp_c[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    int    dip_pol_damp_k[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    /* Ewald (src/field.f90:163-168, ewald_param :860-908) */
+    double alphaES;
+    int    kES[3];
+    int    lautoES;
+    double epsw;
+    int    doefield, doefg;
+    /* induced dipoles (src/field.f90:128-140) */
+    double conv_tol_ind;
+    int    min_scf_pol_iter, max_scf_pol_iter;
+    int    algo_moment_from_pola;              /* MDFF_POLA_* */
+    int    extrapolate_order;
+    int    algo_ext_dipole;                    /* MDFF_EXT_* */
+    /* &mdtag */
+    int    integrator;                         /* MDFF_NVE_VV / MDFF_NVT_NHCN */
+    double dt;                                 /* ps */
+    double temp;                               /* K */
+    int    nhc_n, nhc_yosh_order, nhc_mults;
+    double timesca_thermo;                     /* ps */
+    /* engine choices (no reference counterpart) */
+    int    precision;                          /* MDFF_PREC_* */
+    int    efg_period;                         /* EFG every n MD steps when doefg (0 = every step) */
+    int    nlist_capacity;                     /* neighbours per atom reserved (0 = automatic) */
+    int    device;                             /* CUDA device ordinal */
+} mdff_params;
+
+/* Energies and scalar outputs of one force evaluation (thermodynamic module
+ * variables written by engforce_driver, src/thermo.f90 and field.f90). */
+typedef struct mdff_energies {
+    double u_lj, u_bmhft, u_morse;             /* eV */
+    double u_coul;                             /* eV, includes u_pol (field.f90:1974-1990) */
+    double u_dir, u_rec, u_self, u_surf, u_pol;/* eV (coul_unit applied) */
+    double vir_lj, vir_bmhft, vir_morse;       /* eV (sum r.f / 3) */
+    double pvirial_coul;                       /* eV/A^3 */
+    double utail, ptail;                       /* long-range LJ corrections (not in u_lj) */
+    int    scf_iter;                           /* induced-dipole iterations used */
+    double scf_rmsd;                           /* final RMS residual of mu/alpha - E */
+} mdff_energies;
+
+/* Per-step thermodynamics (calc_thermo, src/thermo.f90:116-207). */
+typedef struct mdff_thermo {
+    int    step;
+    double e_kin, temp_r;                      /* eV, K */
+    double u_tot, e_tot, h_tot;                /* eV; h_tot is the conserved quantity */
+    double u_lj, u_bmhft, u_morse, u_coul, u_pol;
+    double e_nvt;                              /* NHC thermostat energy (0 for NVE) */
+    double pressure_tot;                       /* GPa */
+    double pvirial_tot;                        /* GPa */
+    int    nlist_rebuilt;                      /* 1 if the Verlet list was rebuilt after this step */
+    int    scf_iter;
+    double scf_rmsd;
+} mdff_thermo;
+
+/* Fill p with the reference defaults (control_default_tag, src/control.f90:199-243;
+ * field_default_tag, src/field.f90:192-273; md_default_tag, src/md.f90:178-205). */
+void mdff_params_default(mdff_params* p);
+
+typedef struct mdff_ctx mdff_ctx;
+
+/* Create a context on p->device (replaces the set-up done by field_init and
+ * md_init, src/field.f90:439-560, src/md.f90:99-357).  Parameters are
+ * validated as field_check_tag / md_check_tag do (src/field.f90:282-432). */
+int  mdff_create(const mdff_params* p, mdff_ctx** out);
+
+/* Release the context and every device buffer it owns. */
+void mdff_destroy(mdff_ctx* ctx);
+
+/* Message of the last failing call on ctx (never NULL). */
+const char* mdff_last_error(const mdff_ctx* ctx);
+
+/* Define the system: natm atoms, 1-based types, Cartesian positions and the
+ * cell.  Replaces read_pos + typeinfo_init (src/read_pos.f90:35-219): the cell
+ * goes through lattice() (src/lattice.f90:60-175), positions are wrapped with
+ * kardir/periodicbc/dirkar (src/read_pos.f90:148-150), ewald_param clamps
+ * cutlongrange (src/field.f90:860-908), initialize_param_non_bonded and
+ * initialize_coulomb run (src/field.f90:914-1101, 1596-1662), and the Verlet
+ * lists are built (src/mdff.f90:192-193).  Resets the MD state. */
+int  mdff_set_system(mdff_ctx* ctx, int natm, const int* itype,
+                     const double* rx, const double* ry, const double* rz,
+                     const double A[9]);
+
+/* Replace the positions (no wrap, no list rebuild): the state engforce_driver
+ * sees when a caller moved the atoms itself. */
+int  mdff_set_positions(mdff_ctx* ctx, const double* rx, const double* ry, const double* rz);
+
+/* Wrapped positions as the engine holds them. */
+int  mdff_get_positions(mdff_ctx* ctx, double* rx, double* ry, double* rz);
+
+/* One force evaluation at the current positions with the current lists:
+ * replaces engforce_driver (src/field.f90:1111-1166), i.e. the LJ / BMH(FTD) /
+ * Morse pair loops, the induced-dipole solve and the multipole Ewald sum.
+ * fx,fy,fz (natm each) receive the total force in eV/A; tau_nonb and tau_coul
+ * (3x3, column-major) the stresses in GPa; ef (3*natm, component-major:
+ * ef[c*natm+i]) the electric field in e/A^2 without coul_unit, as the
+ * reference returns it (field.f90:1977); efg (6*natm, components xx,yy,zz,xy,
+ * xz,yz, each natm long) the field gradient times coul_unit; mu (3*natm) the
+ * total dipoles.  Any output pointer may be NULL. */
+int  mdff_engforce(mdff_ctx* ctx, double* fx, double* fy, double* fz,
+                   mdff_energies* e, double tau_nonb[9], double tau_coul[9],
+                   double* ef, double* efg, double* mu);
+
+/* Rebuild the Verlet lists at the current positions: vnlist_pbc
+ * (src/tools.f90:274-370). */
+int  mdff_nlist_build(mdff_ctx* ctx);
+
+/* Copy a Verlet list out in the reference's own layout (verlet_vdw /
+ * verlet_coul, src/config.f90:64-72): point[natm+1] and list[...], both
+ * 1-based, the half list with the reference's parity ownership rule
+ * (src/tools.f90:320-321) and ascending j per atom.  which = 0 for the vdW
+ * list (cutshortrange + skindiff), 1 for the Coulomb list (cutlongrange +
+ * skindiff).  *nlist receives the number of entries; returns MDFF_E_LISTOVF
+ * if cap is too small. */
+int  mdff_nlist_get(mdff_ctx* ctx, int which, int* point, int* list, int cap, int* nlist);
+
+/* Start MD from the current positions with the given velocities (A/ps
+ * scaled like the reference's internal velocities: A per internal time unit):
+ * computes step-0 forces and thermodynamics as md_run does before its loop
+ * (src/runmd.f90:150-165).  t0 may be NULL. */
+int  mdff_md_start(mdff_ctx* ctx, const double* vx, const double* vy, const double* vz,
+                   mdff_thermo* t0);
+
+/* Advance nsteps MD steps: the body of md_run's loop (src/runmd.f90:231-454):
+ * prop_velocity_verlet (src/integration.f90:131-194) or nhcn
+ * (src/integration.f90:476-713), then vnlistcheck (src/tools.f90:446-535) and
+ * calc_thermo (src/thermo.f90:116-207).  Non-NULL position / velocity arrays
+ * are uploaded before the first step and all non-NULL arrays (positions,
+ * velocities, forces) are written back after the last.  thermo, if not NULL,
+ * receives nsteps records. */
+int  mdff_step(mdff_ctx* ctx, int nsteps,
+               double* rx, double* ry, double* rz,
+               double* vx, double* vy, double* vz,
+               double* fx, double* fy, double* fz,
+               mdff_thermo* thermo);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MDFF_ENGINE_H */

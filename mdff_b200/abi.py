@@ -1,0 +1,125 @@
+"""ctypes mirror of include/mdff_engine.h.
+
+The structures below must match the C declarations field for field; a CPU
+test compares ``ctypes.sizeof`` and the defaults against the compiled
+library.  Field meanings follow the reference's namelist tags
+(src/control.f90:128-160, src/field.f90:450-500, src/md.f90:109-132).
+"""
+import ctypes as C
+
+NTYPE_MAX = 16
+TT_MAX_ORDER = 8
+
+OK = 0
+E_ARG = -1
+E_CUDA = -2
+E_NOCONV = -3
+E_LISTOVF = -4
+E_NONFINITE = -5
+E_STATE = -6
+E_UNSUPPORTED = -7
+E_NOMEM = -8
+
+TRUNC_NONE, TRUNC_LINEAR, TRUNC_QUADRATIC = 0, 1, 2
+POLA_SCF, POLA_PCG = 0, 1
+EXT_POLY, EXT_ASPC = 0, 1
+NVE_VV, NVT_NHCN = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+_T = NTYPE_MAX
+_D1 = C.c_double * _T
+_D2 = (C.c_double * _T) * _T
+_I1 = C.c_int * _T
+_D3 = ((C.c_double * _T) * _T) * _T
+_I3 = ((C.c_int * _T) * _T) * _T
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("ntype", C.c_int),
+        ("lnmlj", C.c_int), ("lbmhft", C.c_int), ("lbmhftd", C.c_int), ("lmorse", C.c_int),
+        ("lcoulomb", C.c_int), ("lvnlist", C.c_int), ("lreduced", C.c_int), ("lsurf", C.c_int),
+        ("cutshortrange", C.c_double), ("cutlongrange", C.c_double), ("skindiff", C.c_double),
+        ("mass", _D1), ("qch", _D1), ("dip", (C.c_double * 3) * _T), ("poldip_iso", _D1),
+        ("ldip_polar", _I1), ("symmetric_pot", C.c_int), ("trunc", C.c_int),
+        ("epslj", _D2), ("sigmalj", _D2), ("plj", _D2), ("qlj", _D2),
+        ("epsmor", _D2), ("sigmamor", _D2), ("rhomor", _D2),
+        ("Abmhftd", _D2), ("Bbmhftd", _D2), ("Cbmhftd", _D2), ("Dbmhftd", _D2), ("BDbmhftd", _D2),
+        ("ldip_damping", _I3), ("dip_pol_damp_b", _D3), ("dip_pol_damp_c", _D3), ("dip_pol_damp_k", _I3),
+        ("alphaES", C.c_double), ("kES", C.c_int * 3), ("lautoES", C.c_int), ("epsw", C.c_double),
+        ("doefield", C.c_int), ("doefg", C.c_int),
+        ("conv_tol_ind", C.c_double), ("min_scf_pol_iter", C.c_int), ("max_scf_pol_iter", C.c_int),
+        ("algo_moment_from_pola", C.c_int), ("extrapolate_order", C.c_int), ("algo_ext_dipole", C.c_int),
+        ("integrator", C.c_int), ("dt", C.c_double), ("temp", C.c_double),
+        ("nhc_n", C.c_int), ("nhc_yosh_order", C.c_int), ("nhc_mults", C.c_int),
+        ("timesca_thermo", C.c_double),
+        ("precision", C.c_int), ("efg_period", C.c_int), ("nlist_capacity", C.c_int), ("device", C.c_int),
+    ]
+
+
+class Energies(C.Structure):
+    _fields_ = [
+        ("u_lj", C.c_double), ("u_bmhft", C.c_double), ("u_morse", C.c_double),
+        ("u_coul", C.c_double),
+        ("u_dir", C.c_double), ("u_rec", C.c_double), ("u_self", C.c_double), ("u_surf", C.c_double),
+        ("u_pol", C.c_double),
+        ("vir_lj", C.c_double), ("vir_bmhft", C.c_double), ("vir_morse", C.c_double),
+        ("pvirial_coul", C.c_double),
+        ("utail", C.c_double), ("ptail", C.c_double),
+        ("scf_iter", C.c_int), ("scf_rmsd", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Thermo(C.Structure):
+    _fields_ = [
+        ("step", C.c_int),
+        ("e_kin", C.c_double), ("temp_r", C.c_double),
+        ("u_tot", C.c_double), ("e_tot", C.c_double), ("h_tot", C.c_double),
+        ("u_lj", C.c_double), ("u_bmhft", C.c_double), ("u_morse", C.c_double),
+        ("u_coul", C.c_double), ("u_pol", C.c_double),
+        ("e_nvt", C.c_double), ("pressure_tot", C.c_double), ("pvirial_tot", C.c_double),
+        ("nlist_rebuilt", C.c_int), ("scf_iter", C.c_int), ("scf_rmsd", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def default_params():
+    """Reference defaults: control_default_tag (src/control.f90:199-243),
+    field_default_tag (src/field.f90:192-273), md_default_tag
+    (src/md.f90:178-205).  Mirrors mdff_params_default() in the library."""
+    p = Params()
+    p.ntype = 1
+    p.lvnlist = 1
+    p.skindiff = 0.15
+    p.symmetric_pot = 1
+    p.trunc = TRUNC_NONE
+    for i in range(_T):
+        p.mass[i] = 1.0
+        for j in range(_T):
+            p.qlj[i][j] = 12.0
+            p.plj[i][j] = 6.0
+    p.alphaES = 1.0
+    p.kES[0] = p.kES[1] = p.kES[2] = 10
+    p.epsw = 1e-6
+    p.conv_tol_ind = 1e-6
+    p.min_scf_pol_iter = 3
+    p.max_scf_pol_iter = 100
+    p.extrapolate_order = 0
+    p.algo_ext_dipole = EXT_POLY
+    p.algo_moment_from_pola = POLA_SCF
+    p.integrator = NVE_VV
+    p.temp = 1.0
+    p.nhc_n = 4
+    p.nhc_yosh_order = 3
+    p.nhc_mults = 2
+    p.timesca_thermo = 1.0
+    p.precision = PREC_FP64
+    p.efg_period = 0
+    p.nlist_capacity = 0
+    p.device = 0
+    return p

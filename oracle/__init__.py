@@ -1,0 +1,186 @@
+"""CPU FP64 oracle of MDFF's force-and-integration path -- TEST INFRASTRUCTURE.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
+this module; the engine (mdff_b200) never imports it.  The C++ restatement in
+mdff_oracle.cpp follows the reference routine by routine (file:line cited
+there); this wrapper only marshals arrays through ctypes.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from mdff_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.POINTER(abi.Params), C.c_int, ip, dp, dp, dp, dp]
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_set_erfc_mode.argtypes = [C.c_void_p, C.c_int]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_errfc.restype = C.c_double
+        L.orc_errfc.argtypes = [C.c_double]
+        L.orc_tt_damp.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, dp, dp]
+        L.orc_lattice.argtypes = [dp, dp, dp, dp, dp]
+        L.orc_ewald_info.argtypes = [C.c_void_p, dp, ip, ip, dp]
+        L.orc_set_positions.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_get_positions.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_nlist_build.argtypes = [C.c_void_p]
+        L.orc_nlist_get.argtypes = [C.c_void_p, C.c_int, ip, ip, C.c_int, ip]
+        L.orc_engforce.argtypes = [C.c_void_p, dp, dp, dp, C.POINTER(abi.Energies), dp, dp, dp, dp, dp]
+        L.orc_coulomb_field.argtypes = [C.c_void_p, dp, dp, C.c_int, dp, dp, dp]
+        L.orc_md_start.argtypes = [C.c_void_p, dp, dp, dp, C.POINTER(abi.Thermo)]
+        L.orc_step.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def errfc(x):
+    return lib().orc_errfc(float(x))
+
+
+def tt_damp(b, c, r, order):
+    f = C.c_double()
+    fd = C.c_double()
+    lib().orc_tt_damp(b, c, r, order, C.byref(f), C.byref(fd))
+    return f.value, fd.value
+
+
+class Oracle:
+    """Same call shape as mdff_b200.Engine, computed on the CPU in FP64."""
+
+    def __init__(self, params, itype, pos, cell, erfc_mode=1):
+        self.n = len(itype)
+        self.itype = np.ascontiguousarray(itype, dtype=np.int32)
+        pos = np.asarray(pos, dtype=np.float64)
+        rx, ry, rz = (np.ascontiguousarray(pos[:, k]) for k in range(3))
+        A = np.ascontiguousarray(np.asarray(cell, dtype=np.float64).T.reshape(9))  # column-major
+        self._p = params
+        self._h = lib().orc_create(C.byref(params), self.n, _ip(self.itype), _dp(rx), _dp(ry), _dp(rz), _dp(A))
+        lib().orc_set_erfc_mode(self._h, erfc_mode)
+
+    def close(self):
+        if self._h:
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def ewald_info(self):
+        a = C.c_double()
+        km = (C.c_int * 3)()
+        nk = C.c_int()
+        cl = C.c_double()
+        lib().orc_ewald_info(self._h, C.byref(a), km, C.byref(nk), C.byref(cl))
+        return {"alpha": a.value, "kmax": tuple(km), "nk": nk.value, "cutlongrange": cl.value}
+
+    def positions(self):
+        r = [np.empty(self.n) for _ in range(3)]
+        lib().orc_get_positions(self._h, *(_dp(a) for a in r))
+        return np.stack(r, axis=1)
+
+    def set_positions(self, pos):
+        pos = np.asarray(pos, dtype=np.float64)
+        r = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+        lib().orc_set_positions(self._h, *(_dp(a) for a in r))
+
+    def nlist_build(self):
+        lib().orc_nlist_build(self._h)
+
+    def nlist(self, which):
+        point = np.empty(self.n + 1, dtype=np.int32)
+        cnt = C.c_int()
+        cap = 0
+        rc = lib().orc_nlist_get(self._h, which, _ip(point), None, 0, C.byref(cnt))
+        cap = cnt.value
+        lst = np.empty(max(cap, 1), dtype=np.int32)
+        rc = lib().orc_nlist_get(self._h, which, _ip(point), _ip(lst), cap, C.byref(cnt))
+        assert rc == 0, rc
+        return point, lst[:cnt.value]
+
+    def engforce(self):
+        n = self.n
+        f = [np.empty(n) for _ in range(3)]
+        e = abi.Energies()
+        tn = np.empty(9)
+        tc = np.empty(9)
+        ef = np.empty(3 * n)
+        efg = np.empty(6 * n)
+        mu = np.empty(3 * n)
+        lib().orc_engforce(self._h, *(_dp(a) for a in f), C.byref(e), _dp(tn), _dp(tc), _dp(ef), _dp(efg), _dp(mu))
+        return {
+            "f": np.stack(f, axis=1),
+            "e": e.as_dict(),
+            "tau_nonb": tn.reshape(3, 3).T.copy(),
+            "tau_coul": tc.reshape(3, 3).T.copy(),
+            "ef": ef.reshape(3, n).T.copy(),
+            "efg": efg.reshape(6, n).T.copy(),
+            "mu": mu.reshape(3, n).T.copy(),
+        }
+
+    def coulomb_field(self, q, mu, damp=False):
+        n = self.n
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        m = np.ascontiguousarray(np.asarray(mu, dtype=np.float64).T.reshape(3 * n))
+        ef = np.empty(3 * n)
+        efg = np.empty(6 * n)
+        u = C.c_double()
+        lib().orc_coulomb_field(self._h, _dp(q), _dp(m), int(damp), _dp(ef), _dp(efg), C.byref(u))
+        return ef.reshape(3, n).T.copy(), efg.reshape(6, n).T.copy(), u.value
+
+    def md_start(self, vel):
+        vel = np.asarray(vel, dtype=np.float64)
+        v = [np.ascontiguousarray(vel[:, k]) for k in range(3)]
+        t0 = abi.Thermo()
+        lib().orc_md_start(self._h, *(_dp(a) for a in v), C.byref(t0))
+        return t0.as_dict()
+
+    def step(self, nsteps):
+        n = self.n
+        r = [np.empty(n) for _ in range(3)]
+        v = [np.empty(n) for _ in range(3)]
+        f = [np.empty(n) for _ in range(3)]
+        th = (abi.Thermo * max(nsteps, 1))()
+        # positions/velocities are read back only: pass buffers filled from the current state
+        pos = self.positions()
+        for k in range(3):
+            r[k][:] = pos[:, k]
+        lib().orc_step(self._h, nsteps, *(_dp(a) for a in r), None, None, None, *(_dp(a) for a in f), th)
+        return {
+            "pos": np.stack(r, axis=1),
+            "f": np.stack(f, axis=1),
+            "thermo": [th[i].as_dict() for i in range(nsteps)],
+        }

@@ -128,6 +128,8 @@ typedef struct mdff_params {
     int    efg_period;                         /* EFG every n MD steps when doefg (0 = every step) */
     int    nlist_capacity;                     /* neighbours per atom reserved (0 = automatic) */
     int    device;                             /* CUDA device ordinal */
+    int    erfc_ref;                           /* 1: the reference's fitted erfc (src/functions.f90:28-39) */
+    int    nhc_literal;                        /* 1: chain_nhcn's literal force order (stale G(2..M-1)) */
 } mdff_params;
 
 /* Energies and scalar outputs of one force evaluation (thermodynamic module
@@ -156,6 +158,11 @@ typedef struct mdff_thermo {
     int    scf_iter;
     double scf_rmsd;
 } mdff_thermo;
+
+/* sizeof(mdff_params), sizeof(mdff_energies), sizeof(mdff_thermo) for
+ * which = 0, 1, 2 (lets a binding check its mirror of these structs); no
+ * reference counterpart. */
+int  mdff_struct_size(int which);
 
 /* Fill p with the reference defaults (control_default_tag, src/control.f90:199-243;
  * field_default_tag, src/field.f90:192-273; md_default_tag, src/md.f90:178-205). */

@@ -1,0 +1,188 @@
+"""B200 force engine for MDFF's force-and-integration hot path.
+
+Python binding of the C ABI in include/mdff_engine.h.  The compute runs in the
+CUDA library mdff_b200/lib/libmdff_engine.so (sm_100a); there is no CPU
+fallback: importing works without a GPU, but creating an Engine without the
+library or without a CUDA device raises.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libmdff_engine.so")
+_lib = None
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mdff engine error {code}: {msg}")
+        self.code = code
+
+
+def build(force=False):
+    """Compile the CUDA engine library in place (nvcc, sm_100a)."""
+    args = ["make", "-s", "-C", os.path.join(_HERE, "csrc")]
+    if force:
+        subprocess.run(args + ["clean"], check=True)
+    subprocess.run(args, check=True)
+
+
+def lib():
+    """Load the engine library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EngineError(abi.E_STATE, f"engine library missing: {LIB_PATH} (run mdff_b200.build())")
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        vp = C.c_void_p
+        L.mdff_params_default.argtypes = [C.POINTER(abi.Params)]
+        L.mdff_params_default.restype = None
+        L.mdff_create.argtypes = [C.POINTER(abi.Params), C.POINTER(vp)]
+        L.mdff_destroy.argtypes = [vp]
+        L.mdff_destroy.restype = None
+        L.mdff_last_error.argtypes = [vp]
+        L.mdff_last_error.restype = C.c_char_p
+        L.mdff_set_system.argtypes = [vp, C.c_int, ip, dp, dp, dp, dp]
+        L.mdff_set_positions.argtypes = [vp, dp, dp, dp]
+        L.mdff_get_positions.argtypes = [vp, dp, dp, dp]
+        L.mdff_engforce.argtypes = [vp, dp, dp, dp, C.POINTER(abi.Energies), dp, dp, dp, dp, dp]
+        L.mdff_nlist_build.argtypes = [vp]
+        L.mdff_nlist_get.argtypes = [vp, C.c_int, ip, ip, C.c_int, ip]
+        L.mdff_md_start.argtypes = [vp, dp, dp, dp, C.POINTER(abi.Thermo)]
+        L.mdff_step.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+
+
+def params_default():
+    p = abi.Params()
+    lib().mdff_params_default(C.byref(p))
+    return p
+
+
+class Engine:
+    """One engine context on one GPU: the state engforce_driver and md_run
+    share through module globals in the reference."""
+
+    def __init__(self, params, itype, pos, cell):
+        L = lib()
+        self._h = C.c_void_p()
+        self.params = params
+        rc = L.mdff_create(C.byref(params), C.byref(self._h))
+        self._check(rc)
+        self.n = len(itype)
+        self.itype = np.ascontiguousarray(itype, dtype=np.int32)
+        pos = np.asarray(pos, dtype=np.float64)
+        r = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+        A = np.ascontiguousarray(np.asarray(cell, dtype=np.float64).T.reshape(9))   # rows = vectors -> column-major
+        self._check(L.mdff_set_system(self._h, self.n, _ip(self.itype), *(_dp(a) for a in r), _dp(A)))
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = lib().mdff_last_error(self._h).decode() if self._h else "no context"
+            raise EngineError(rc, msg)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().mdff_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def positions(self):
+        r = [np.empty(self.n) for _ in range(3)]
+        self._check(lib().mdff_get_positions(self._h, *(_dp(a) for a in r)))
+        return np.stack(r, axis=1)
+
+    def set_positions(self, pos):
+        pos = np.asarray(pos, dtype=np.float64)
+        r = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+        self._check(lib().mdff_set_positions(self._h, *(_dp(a) for a in r)))
+
+    def nlist_build(self):
+        self._check(lib().mdff_nlist_build(self._h))
+
+    def nlist(self, which):
+        point = np.empty(self.n + 1, dtype=np.int32)
+        cnt = C.c_int()
+        rc = lib().mdff_nlist_get(self._h, which, _ip(point), None, 0, C.byref(cnt))
+        if rc not in (0, abi.E_LISTOVF):
+            self._check(rc)
+        lst = np.empty(max(cnt.value, 1), dtype=np.int32)
+        self._check(lib().mdff_nlist_get(self._h, which, _ip(point), _ip(lst), cnt.value, C.byref(cnt)))
+        return point, lst[:cnt.value]
+
+    def engforce(self):
+        n = self.n
+        f = [np.empty(n) for _ in range(3)]
+        e = abi.Energies()
+        tn = np.empty(9)
+        tc = np.empty(9)
+        ef = np.empty(3 * n)
+        efg = np.empty(6 * n)
+        mu = np.empty(3 * n)
+        self._check(lib().mdff_engforce(self._h, *(_dp(a) for a in f), C.byref(e), _dp(tn), _dp(tc), _dp(ef),
+                                        _dp(efg), _dp(mu)))
+        return {
+            "f": np.stack(f, axis=1),
+            "e": e.as_dict(),
+            "tau_nonb": tn.reshape(3, 3).T.copy(),
+            "tau_coul": tc.reshape(3, 3).T.copy(),
+            "ef": ef.reshape(3, n).T.copy(),
+            "efg": efg.reshape(6, n).T.copy(),
+            "mu": mu.reshape(3, n).T.copy(),
+        }
+
+    def md_start(self, vel):
+        vel = np.asarray(vel, dtype=np.float64)
+        v = [np.ascontiguousarray(vel[:, k]) for k in range(3)]
+        t0 = abi.Thermo()
+        self._check(lib().mdff_md_start(self._h, *(_dp(a) for a in v), C.byref(t0)))
+        return t0.as_dict()
+
+    def step(self, nsteps, thermo=True):
+        """Advance nsteps; return final positions, velocities, forces and the
+        per-step thermodynamics."""
+        n = self.n
+        r = [np.empty(n) for _ in range(3)]
+        v = [np.empty(n) for _ in range(3)]
+        f = [np.empty(n) for _ in range(3)]
+        th = (abi.Thermo * max(nsteps, 1))() if thermo else None
+        # no upload (NULL position/velocity inputs would skip the download too),
+        # so advance first, then read the state back
+        self._check(lib().mdff_step(self._h, nsteps, None, None, None, None, None, None, *(_dp(a) for a in f),
+                                    th if thermo else None))
+        pos = self.positions()
+        return {
+            "pos": pos,
+            "f": np.stack(f, axis=1),
+            "thermo": [th[i].as_dict() for i in range(nsteps)] if thermo else [],
+        }
+
+    def step_host(self, nsteps, pos, vel, thermo=None):
+        """The host-buffer form of mdff_step: positions and velocities are
+        uploaded from, and written back to, the given (N,3)-shaped SoA arrays."""
+        n = self.n
+        f = [np.empty(n) for _ in range(3)]
+        self._check(lib().mdff_step(self._h, nsteps, *(_dp(pos[k]) for k in range(3)), *(_dp(vel[k]) for k in range(3)),
+                                    *(_dp(a) for a in f), thermo))
+        return f

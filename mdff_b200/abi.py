@@ -54,6 +54,7 @@ class Params(C.Structure):
         ("nhc_n", C.c_int), ("nhc_yosh_order", C.c_int), ("nhc_mults", C.c_int),
         ("timesca_thermo", C.c_double),
         ("precision", C.c_int), ("efg_period", C.c_int), ("nlist_capacity", C.c_int), ("device", C.c_int),
+        ("erfc_ref", C.c_int), ("nhc_literal", C.c_int),
     ]
 
 

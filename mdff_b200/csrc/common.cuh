@@ -1,0 +1,65 @@
+// common.cuh -- device helpers shared by the engine's kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "engine_internal.h"
+
+namespace mdff {
+
+// Minimum-image pair vector from direct (fractional) coordinates in exactly the
+// operation order of vnlist_pbc (src/tools.f90:323-332): d = si - sj,
+// d - NINT(d) (half away from zero: round()), then r = A d row by row, and
+// |r|^2 summed x, y, z.  Every multiply and add is a separate IEEE operation
+// (no FMA), so the inclusion test matches the reference bit for bit.
+__device__ __forceinline__ double pairvec_exact(const CellP& c, double si1, double si2, double si3,
+                                                double sj1, double sj2, double sj3,
+                                                double& rx, double& ry, double& rz) {
+    double dx = __dsub_rn(si1, sj1), dy = __dsub_rn(si2, sj2), dz = __dsub_rn(si3, sj3);
+    dx = __dsub_rn(dx, round(dx));
+    dy = __dsub_rn(dy, round(dy));
+    dz = __dsub_rn(dz, round(dz));
+    rx = __dadd_rn(__dadd_rn(__dmul_rn(dx, c.A[0]), __dmul_rn(dy, c.A[1])), __dmul_rn(dz, c.A[2]));
+    ry = __dadd_rn(__dadd_rn(__dmul_rn(dx, c.A[3]), __dmul_rn(dy, c.A[4])), __dmul_rn(dz, c.A[5]));
+    rz = __dadd_rn(__dadd_rn(__dmul_rn(dx, c.A[6]), __dmul_rn(dy, c.A[7])), __dmul_rn(dz, c.A[8]));
+    return __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum over a group of G consecutive lanes (G a power of two <= 32); every lane
+// of the group receives the group sum.
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of K values per thread, written as per-block partials
+// out[blockLinear*K + k].  Fixed reduction tree: deterministic.
+template <int K>
+__device__ __forceinline__ void block_partials(double (&v)[K], double* out) {
+    __shared__ double red[32][K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarp = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = warp_sum(v[k]);
+        if (lane == 0) red[warp][k] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int bl = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = lane < nwarp ? red[lane][k] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) out[(size_t)bl * K + k] = s;
+        }
+    }
+}
+
+}  // namespace mdff

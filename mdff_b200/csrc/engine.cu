@@ -1,0 +1,1154 @@
+// engine.cu -- host side of the B200 force engine and its C ABI.
+//
+// One translation unit: the kernels live in the *.cuh files included below.
+// The host code owns one CUDA stream and every device buffer of a context;
+// all device work for a call is queued on that stream and the call returns
+// after the results it reports are on the host.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine_internal.h"
+#include "common.cuh"
+#include "nlist.cuh"
+#include "pair.cuh"
+#include "ewald_real.cuh"
+#include "ewald_recip.cuh"
+#include "solve.cuh"
+#include "integrate.cuh"
+
+using namespace mdff;
+
+namespace {
+
+struct Units { double press, boltz, time, coul; };
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+};
+
+}  // namespace
+
+struct mdff_ctx {
+    mdff_params p;
+    std::string err;
+    cudaStream_t st = nullptr;
+    Units u;
+    // system
+    int n = 0;
+    int ntype = 0;
+    int npol = 0;
+    bool any_q = false, any_dip0 = false;
+    CellP cell;
+    double W[3], anorm[3];
+    double cut_vdw = 0.0, cut_coul = 0.0;
+    double alphaES = 0.0;
+    int kES[3] = {0, 0, 0};
+    double utail = 0.0, ptail = 0.0;
+    std::vector<int> natmi;
+    std::vector<void*> allocs;
+    // device state
+    double *x = nullptr, *y = nullptr, *z = nullptr;
+    double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    double *fx = nullptr, *fy = nullptr, *fz = nullptr;
+    double *fox = nullptr, *foy = nullptr, *foz = nullptr;
+    double *sx = nullptr, *sy = nullptr, *sz = nullptr;
+    double *xs = nullptr, *ys = nullptr, *zs = nullptr;
+    int* type = nullptr;
+    double *q = nullptr, *mass = nullptr, *alpha = nullptr, *inv_alpha = nullptr, *dip0 = nullptr;
+    double *mu = nullptr, *mu_ind = nullptr, *Estat = nullptr, *Eind = nullptr, *E = nullptr;
+    double *cg_r = nullptr, *cg_z = nullptr, *cg_d = nullptr, *cg_Ad = nullptr, *mu_save = nullptr;
+    double* hist = nullptr;
+    double* coef = nullptr;
+    double *ef = nullptr, *efg = nullptr, *fcoul = nullptr;
+    PairConst* pc = nullptr;
+    NList lv, lc;
+    bool shared_list = false;
+    CellGrid grid;
+    KGrid kg;
+    RecScratch rs;
+    Partials part;
+    DevScalars* dsc = nullptr;
+    DevScalars* hsc = nullptr;   // pinned mirror
+    int* d_overflow = nullptr;
+    // state
+    bool have_system = false, have_list = false, forces_valid = false, md_started = false;
+    int itime = 0;
+    int nhist = 1;
+    double e_kin = 0.0, temp_r = 0.0;
+    mdff_energies en;
+    double tau_nonb[9], tau_coul[9];
+    int last_rebuilt = 0;
+    int nrebuild = 0;
+};
+
+namespace {
+
+int fail(mdff_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(ctx, MDFF_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+#define TRY(expr)                  \
+    do {                           \
+        int r_ = (expr);           \
+        if (r_ != MDFF_OK) return r_; \
+    } while (0)
+
+template <class T>
+int dalloc(mdff_ctx* ctx, T** ptr, size_t count) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
+    if (e != cudaSuccess) return fail(ctx, MDFF_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    ctx->allocs.push_back(p);
+    *ptr = (T*)p;
+    return MDFF_OK;
+}
+
+void free_all(mdff_ctx* ctx) {
+    for (void* p : ctx->allocs) cudaFree(p);
+    ctx->allocs.clear();
+}
+
+int check_launch(mdff_ctx* ctx, const char* where) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ctx, MDFF_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+    return MDFF_OK;
+}
+
+int sync_scalars(mdff_ctx* ctx) {
+    CK(cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+// lattice (src/lattice.f90:60-175) on the host, for A given column-major.
+void lattice(const double A9[9], CellP& c, double W[3], double anorm[3]) {
+    double A[3][3], B[3][3];
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) A[i][j] = A9[3 * j + i];
+    auto expro = [&](int out, int a, int b) {
+        B[0][out] = A[1][a] * A[2][b] - A[2][a] * A[1][b];
+        B[1][out] = A[2][a] * A[0][b] - A[0][a] * A[2][b];
+        B[2][out] = A[0][a] * A[1][b] - A[1][a] * A[0][b];
+    };
+    expro(0, 1, 2);
+    expro(1, 2, 0);
+    expro(2, 0, 1);
+    double omega = B[0][0] * A[0][0] + B[1][0] * A[1][0] + B[2][0] * A[2][0];
+    for (int j = 0; j < 3; ++j) W[j] = omega / std::sqrt(B[0][j] * B[0][j] + B[1][j] * B[1][j] + B[2][j] * B[2][j]);
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) B[i][j] = B[i][j] / omega;
+    for (int i = 0; i < 3; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k) s += A[k][i] * A[k][i];
+        anorm[i] = std::sqrt(s);
+    }
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) { c.A[3 * i + j] = A[i][j]; c.B[3 * i + j] = B[i][j]; }
+    c.omega = omega;
+}
+
+void symmetrise(mdff_params& p) {   // field_check_tag (src/field.f90:316-339)
+    if (!p.symmetric_pot) return;
+    int n = p.ntype;
+    for (int it = 0; it < n; ++it)
+        for (int jt = 0; jt < n; ++jt) {
+            p.epslj[jt][it] = p.epslj[it][jt];
+            p.sigmalj[jt][it] = p.sigmalj[it][jt];
+            p.plj[jt][it] = p.plj[it][jt];
+            p.qlj[jt][it] = p.qlj[it][jt];
+            p.Abmhftd[jt][it] = p.Abmhftd[it][jt];
+            p.Bbmhftd[jt][it] = p.Bbmhftd[it][jt];
+            p.Cbmhftd[jt][it] = p.Cbmhftd[it][jt];
+            p.Dbmhftd[jt][it] = p.Dbmhftd[it][jt];
+            p.BDbmhftd[jt][it] = p.BDbmhftd[it][jt];
+            for (int it2 = 0; it2 < n; ++it2) {
+                p.ldip_damping[it2][jt][it] = p.ldip_damping[it2][it][jt];
+                p.dip_pol_damp_b[it2][jt][it] = p.dip_pol_damp_b[it2][it][jt];
+                p.dip_pol_damp_c[it2][jt][it] = p.dip_pol_damp_c[it2][it][jt];
+                p.dip_pol_damp_k[it2][jt][it] = p.dip_pol_damp_k[it2][it][jt];
+            }
+        }
+}
+
+// Validation of the tags on the path (field_check_tag, md_check_tag).
+int check_params(mdff_ctx* ctx, const mdff_params& p) {
+    if (p.ntype < 1 || p.ntype > MDFF_NTYPE_MAX) return fail(ctx, MDFF_E_ARG, "ntype out of range");
+    if (p.trunc < 0 || p.trunc > 2) return fail(ctx, MDFF_E_ARG, "ctrunc should be notrunc, linear or quadratic");
+    bool nonb = p.lnmlj || p.lbmhft || p.lbmhftd || p.lmorse;
+    if (nonb && p.cutshortrange <= 0.0) return fail(ctx, MDFF_E_ARG, "controltag: cutshortrange is null");
+    if (p.lcoulomb && p.cutlongrange <= 0.0) return fail(ctx, MDFF_E_ARG, "controltag: cutlongrange is null");
+    for (int a = 0; a < p.ntype; ++a)
+        for (int b = 0; b < p.ntype; ++b)
+            for (int c = 0; c < p.ntype; ++c)
+                if (p.dip_pol_damp_k[a][b][c] > MDFF_TT_MAX_ORDER || p.dip_pol_damp_k[a][b][c] < 0)
+                    return fail(ctx, MDFF_E_ARG, "Tang-Toennies expansion order too large (dip_pol_damp_k)");
+    if (p.integrator != MDFF_NVE_VV && p.integrator != MDFF_NVT_NHCN)
+        return fail(ctx, MDFF_E_UNSUPPORTED, "integrator: only nve-vv and nvt-nhcn are on the engine's path");
+    if (p.integrator == MDFF_NVT_NHCN && (p.nhc_n < 2 || p.nhc_n > 16))
+        return fail(ctx, MDFF_E_ARG, "nhc_n = 1 is not allowed with Nose Hoover chains thermostats");
+    int yo = p.nhc_yosh_order;
+    if (p.integrator == MDFF_NVT_NHCN && !(yo == 1 || yo == 3 || yo == 5 || yo == 7 || yo == 9))
+        return fail(ctx, MDFF_E_ARG, "value of yoshida order not available");
+    if (p.integrator == MDFF_NVT_NHCN && p.nhc_mults < 1) return fail(ctx, MDFF_E_ARG, "nhc_mults < 1");
+    if (p.extrapolate_order < 0 || p.extrapolate_order > 5)
+        return fail(ctx, MDFF_E_ARG, "extrapolate_order should be 0 <= order <= 5");
+    if (p.algo_moment_from_pola != MDFF_POLA_SCF && p.algo_moment_from_pola != MDFF_POLA_PCG)
+        return fail(ctx, MDFF_E_ARG, "algo_moment_from_pola should be scf or pcg");
+    if (p.algo_ext_dipole != MDFF_EXT_POLY && p.algo_ext_dipole != MDFF_EXT_ASPC)
+        return fail(ctx, MDFF_E_ARG, "algo_ext_dipole should be poly or aspc");
+    if (p.precision != MDFF_PREC_FP64 && p.precision != MDFF_PREC_MIXED)
+        return fail(ctx, MDFF_E_ARG, "precision should be MDFF_PREC_FP64 or MDFF_PREC_MIXED");
+    bool pol = false;
+    for (int t = 0; t < p.ntype; ++t) if (p.ldip_polar[t]) pol = true;
+    if (pol && p.lsurf) return fail(ctx, MDFF_E_UNSUPPORTED, "lsurf with polarisable ions is outside the engine's path");
+    return MDFF_OK;
+}
+
+// ewald_param (src/field.f90:860-908)
+void ewald_param(mdff_ctx* ctx) {
+    const mdff_params& p = ctx->p;
+    double rcut = 0.5 * std::min(ctx->W[0], std::min(ctx->W[1], ctx->W[2]));
+    double cl = std::min(p.cutlongrange, rcut);
+    double eps = std::min(std::fabs(p.epsw), 0.5);
+    double tol = std::sqrt(std::fabs(std::log(eps * cl)));
+    double alpha = std::sqrt(std::fabs(std::log(eps * cl * tol))) / rcut;
+    double tol1 = std::sqrt(-std::log(eps * cl * (2.0 * tol * alpha) * (2.0 * tol * alpha)));
+    ctx->cut_coul = cl;
+    ctx->alphaES = p.alphaES;
+    for (int i = 0; i < 3; ++i) ctx->kES[i] = p.kES[i];
+    if (p.lautoES) {
+        ctx->alphaES = alpha;
+        for (int i = 0; i < 3; ++i) ctx->kES[i] = (int)std::round(0.25 + ctx->anorm[i] * alpha * tol1 / PI);
+    }
+}
+
+// initialize_param_non_bonded (src/field.f90:914-1101) and the damping
+// tables, packed per ordered type pair.
+void build_pair_consts(mdff_ctx* ctx, std::vector<PairConst>& tab) {
+    const mdff_params& p = ctx->p;
+    tab.assign(NT * NT, PairConst());
+    std::memset(tab.data(), 0, sizeof(PairConst) * NT * NT);
+    double two16 = std::pow(2.0, 1.0 / 6.0);
+    ctx->utail = ctx->ptail = 0.0;
+    for (int it = 0; it < ctx->ntype; ++it)
+        for (int jt = 0; jt < ctx->ntype; ++jt) {
+            PairConst& P = tab[it * NT + jt];
+            double pp = p.plj[it][jt], qq = p.qlj[it][jt];
+            double rcut = p.cutshortrange;
+            P.rcutsq = rcut * rcut;
+            double rcut3 = rcut * P.rcutsq;
+            double ppqq = pp * qq;
+            P.epsp = p.epslj[it][jt] / (qq - pp);
+            P.sigsq = two16 * two16 * p.sigmalj[it][jt] * p.sigmalj[it][jt];
+            P.plj = pp;
+            P.qlj = qq;
+            double sr2 = P.sigsq / P.rcutsq;
+            double sr = std::sqrt(sr2);
+            double srp = std::pow(sr, pp), srq = std::pow(sr, qq);
+            P.uc = P.epsp * (pp * srq - qq * srp);
+            P.uc1 = P.epsp * ppqq / (2.0 * P.rcutsq) * (srq - srp);
+            P.uc2 = 0.5 * P.epsp * ((2.0 * pp + ppqq) * srq - (2.0 * qq + ppqq) * srp);
+            P.fc = ppqq * P.epsp / P.sigsq;
+            double ut = P.epsp * (pp * srq / (qq - 3.0) - qq * srp / (pp - 3.0)) * rcut3 * 2.0 * PI;
+            double pt = ppqq * P.epsp * (srq / (qq - 3.0) - srp / (pp - 3.0)) * rcut3 * 2.0 * PI;
+            if (ctx->natmi[it] != 0 && ctx->natmi[jt] != 0) {
+                ctx->utail += ut * ctx->natmi[it] * ctx->natmi[jt] / ctx->cell.omega;
+                ctx->ptail += pt * ctx->natmi[it] * ctx->natmi[jt] / ctx->cell.omega;
+            }
+            P.A = p.Abmhftd[it][jt];
+            P.B = p.Bbmhftd[it][jt];
+            P.C = p.Cbmhftd[it][jt];
+            P.D = p.Dbmhftd[it][jt];
+            P.BD = p.BDbmhftd[it][jt];
+            P.epsmor = p.epsmor[it][jt];
+            P.rhomor = p.rhomor[it][jt];
+            P.rs = std::exp(p.rhomor[it][jt] * p.sigmamor[it][jt]);
+            P.db_i = p.dip_pol_damp_b[it][it][jt];
+            P.dc_i = p.dip_pol_damp_c[it][it][jt];
+            P.dk_i = p.dip_pol_damp_k[it][it][jt];
+            P.db_j = p.dip_pol_damp_b[jt][it][jt];
+            P.dc_j = p.dip_pol_damp_c[jt][it][jt];
+            P.dk_j = p.dip_pol_damp_k[jt][it][jt];
+            P.ldamp = (p.ldip_damping[it][it][jt] || p.ldip_damping[jt][it][jt]) ? 1 : 0;
+        }
+    ctx->ptail = ctx->ptail / ctx->u.press / ctx->cell.omega / 3.0;
+}
+
+double rlist_max(const mdff_ctx* ctx, double skin) {
+    double r = 0.0;
+    bool nonb = ctx->p.lnmlj || ctx->p.lbmhft || ctx->p.lbmhftd || ctx->p.lmorse;
+    if (nonb) r = std::max(r, ctx->cut_vdw + skin);
+    if (ctx->p.lcoulomb) r = std::max(r, ctx->cut_coul + skin);
+    return r;
+}
+
+int ensure_lists(mdff_ctx* ctx, int cap) {
+    bool nonb = ctx->p.lnmlj || ctx->p.lbmhft || ctx->p.lbmhftd || ctx->p.lmorse;
+    ctx->shared_list = !(nonb && ctx->p.lcoulomb) || (ctx->cut_vdw == ctx->cut_coul);
+    auto alloc_list = [&](NList& L) -> int {
+        if (L.cap >= cap && L.nbr) return MDFF_OK;
+        if (L.nbr) { cudaFree(L.nbr); ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void*)L.nbr)); L.nbr = nullptr; }
+        TRY(dalloc(ctx, &L.nbr, (size_t)ctx->n * cap));
+        if (!L.cnt) TRY(dalloc(ctx, &L.cnt, (size_t)ctx->n));
+        L.cap = cap;
+        return MDFF_OK;
+    };
+    TRY(alloc_list(ctx->lv));
+    if (!ctx->shared_list) TRY(alloc_list(ctx->lc));
+    return MDFF_OK;
+}
+
+// vnlist_pbc (src/tools.f90:274-370): both lists at the current positions.
+int build_lists(mdff_ctx* ctx, double skin) {
+    const int n = ctx->n;
+    double rl = rlist_max(ctx, skin);
+    if (rl <= 0.0) return MDFF_OK;
+    CellGrid& g = ctx->grid;
+    for (int d = 0; d < 3; ++d) {
+        int nc = (int)std::floor(ctx->W[d] / (rl * (1.0 + 1e-12)));
+        g.nc[d] = std::max(1, std::min(nc, 256));
+    }
+    g.ncell = g.nc[0] * g.nc[1] * g.nc[2];
+    if (g.ncell > g.ncell_alloc) {
+        TRY(dalloc(ctx, &g.cell_count, g.ncell));
+        TRY(dalloc(ctx, &g.cell_start, g.ncell + 1));
+        TRY(dalloc(ctx, &g.cell_cursor, g.ncell));
+        g.ncell_alloc = g.ncell;
+    }
+    launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
+    launch_bin(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, g);
+    bool nonb = ctx->p.lnmlj || ctx->p.lbmhft || ctx->p.lbmhftd || ctx->p.lmorse;
+    double cut_a = nonb ? ctx->cut_vdw : ctx->cut_coul;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        double ra = cut_a + skin, rb = ctx->cut_coul + skin;
+        CK(cudaMemsetAsync(ctx->d_overflow, 0, sizeof(int), ctx->st));
+        launch_nlist(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->cell, g, ra * ra, ctx->lv, rb * rb,
+                     ctx->shared_list ? nullptr : &ctx->lc, ctx->d_overflow);
+        TRY(check_launch(ctx, "nlist"));
+        int ovf = 0;
+        CK(cudaMemcpyAsync(&ovf, ctx->d_overflow, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (ovf == 0) break;
+        if (attempt == 3) return fail(ctx, MDFF_E_LISTOVF, "neighbour list capacity exceeded");
+        int cap = (int)(ovf * 1.25) + 32;
+        TRY(ensure_lists(ctx, cap));
+    }
+    ctx->lv.cut = cut_a;
+    ctx->lc.cut = ctx->cut_coul;
+    CK(cudaMemcpyAsync(ctx->xs, ctx->sx, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->ys, ctx->sy, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->zs, ctx->sz, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    ctx->have_list = true;
+    ctx->nrebuild++;
+    return MDFF_OK;
+}
+
+const NList& coul_list(const mdff_ctx* ctx) { return ctx->shared_list ? ctx->lv : ctx->lc; }
+
+__global__ void k_axpy(int n, double a, const double* x, double* y) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) y[t] = fma(a, x[t], y[t]);
+}
+
+__global__ void k_add3(int n, const double* a, const double* b, double* out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = a[t] + b[t];
+}
+
+// Final assembly of multipole_ES (src/field.f90:1930-1990): self (and surface)
+// terms, coul_unit, forces added to the total.
+__global__ void k_coul_finish(int n, const double* q, const double* mu, double* ef, double* efg, const double* fc,
+                              double* fx, double* fy, double* fz, double selfa2, double cu, int do_efg, int lsurf,
+                              double s0, double s1, double s2, double fpi_3V) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double qi = q[i];
+    double sv[3] = {s0, s1, s2};
+    for (int c = 0; c < 3; ++c) {
+        double e = ef[(size_t)c * n + i] + 2.0 * selfa2 * mu[(size_t)c * n + i];
+        if (lsurf) e += sv[c];
+        ef[(size_t)c * n + i] = e;
+    }
+    if (do_efg) {
+        for (int k = 0; k < 6; ++k) {
+            double v = efg[(size_t)k * n + i];
+            if (k < 3) v += -2.0 * selfa2 * qi;
+            efg[(size_t)k * n + i] = v * cu;
+        }
+    }
+    double f0 = fc[i], f1 = fc[n + i], f2 = fc[2 * n + i];
+    if (lsurf) { f0 += -qi * s0 * fpi_3V; f1 += -qi * s1 * fpi_3V; f2 += -qi * s2 * fpi_3V; }
+    fx[i] += f0 * cu;
+    fy[i] += f1 * cu;
+    fz[i] += f2 * cu;
+}
+
+inline int nb(int n, int t = 256) { return (n + t - 1) / t; }
+
+double selfa(const mdff_ctx* ctx) { return ctx->alphaES / std::sqrt(PI); }
+double selfa2(const mdff_ctx* ctx) { return 2.0 * selfa(ctx) * ctx->alphaES * ctx->alphaES / 3.0; }
+
+DirFlags dir_flags(const mdff_ctx* ctx) {
+    DirFlags f;
+    std::memset(&f, 0, sizeof f);
+    f.ntype = ctx->ntype;
+    f.alpha = ctx->alphaES;
+    f.cutsq = ctx->cut_coul * ctx->cut_coul;
+    f.erfc_ref = ctx->p.erfc_ref ? 1 : 0;
+    return f;
+}
+
+// Field of the induced dipoles: real space (dipole-dipole, undamped) +
+// reciprocal space + self term; src/field.f90:3354-3357.
+int induced_field(mdff_ctx* ctx, const double* m, double* out) {
+    const int n = ctx->n;
+    DirFlags f = dir_flags(ctx);
+    f.dd = 1;
+    f.field = 1;
+    launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, nullptr, m, ctx->cell, coul_list(ctx), ctx->pc,
+                     f, out, nullptr, nullptr, ctx->part, ctx->dsc);
+    RecFlags rf{0, 1, 1, 0, 0, ctx->p.precision};
+    launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, nullptr, m, ctx->cell, ctx->kg, rf, ctx->rs, out, nullptr,
+                     nullptr, ctx->part, ctx->dsc);
+    k_axpy<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, 2.0 * selfa2(ctx), m, out);
+    return check_launch(ctx, "induced_field");
+}
+
+// Static field of the charges (and static dipoles), damped
+// (src/field.f90:3270-3272).
+int static_field(mdff_ctx* ctx) {
+    const int n = ctx->n;
+    DirFlags f = dir_flags(ctx);
+    f.qq = 1;
+    f.qd = ctx->any_dip0 ? 1 : 0;
+    f.dd = ctx->any_dip0 ? 1 : 0;
+    f.damp = 1;
+    f.field = 1;
+    launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->dip0, ctx->cell, coul_list(ctx),
+                     ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc);
+    RecFlags rf{1, ctx->any_dip0 ? 1 : 0, 1, 0, 0, ctx->p.precision};
+    launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->dip0, ctx->cell, ctx->kg, rf, ctx->rs,
+                     ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc);
+    k_axpy<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, 2.0 * selfa2(ctx), ctx->dip0, ctx->Estat);
+    return check_launch(ctx, "static_field");
+}
+
+// Extrapolated initial guess from the stored history (extrapolate_dipole_poly,
+// src/field.f90:3807-3920; ASPC predictor, src/field.f90:3924-3984).
+int predict(mdff_ctx* ctx, double* x) {
+    const int n3 = 3 * ctx->n;
+    const int ord = ctx->p.extrapolate_order;
+    const int itime = ctx->itime;
+    double coef[16] = {0};
+    int mode = 0, npt = 1, shift_from = 0;   // shift history slots [shift_from..1] down by one
+    if (ctx->p.algo_ext_dipole == MDFF_EXT_ASPC) {
+        int eo = (itime >= ord + 1) ? ord : ((itime == 1 || itime == 0) ? 0 : itime - 1);
+        static const double B[6][6] = {{1.0},
+                                       {2.0, -1.0},
+                                       {2.5, -2.0, 0.5},
+                                       {2.8, -2.8, 1.2, -0.2},
+                                       {3.0, -24.0 / 7.0, 27.0 / 14.0, -4.0 / 7.0, 1.0 / 14.0},
+                                       {22.0 / 7.0, -55.0 / 14.0, 55.0 / 21.0, -22.0 / 21.0, 5.0 / 21.0, -1.0 / 42.0}};
+        for (int k = 0; k <= eo; ++k) coef[k] = B[eo][k];
+        npt = eo + 1;
+        shift_from = eo;
+    } else if (ord == 0) {
+        coef[0] = 1.0;
+    } else if (ord == 1) {
+        if (itime > 1) { coef[0] = 2.0; coef[1] = -1.0; npt = 2; }
+        shift_from = 1;
+    } else {
+        if (itime > ord) { mode = 1; npt = ord + 1; }
+        else if (itime <= 1) { coef[0] = 1.0; }
+        else if (itime == 2) { coef[0] = 2.0; coef[1] = -1.0; npt = 2; }
+        else { mode = 1; npt = itime + 1; }
+        shift_from = ord;
+    }
+    CK(cudaMemcpyAsync(ctx->coef, coef, sizeof(coef), cudaMemcpyHostToDevice, ctx->st));
+    k_extrapolate<<<nb(n3), 256, 0, ctx->st>>>(n3, mode, npt, ctx->hist, ctx->coef, x);
+    for (int k = shift_from; k >= 1; --k)
+        CK(cudaMemcpyAsync(ctx->hist + (size_t)k * n3, ctx->hist + (size_t)(k - 1) * n3, sizeof(double) * n3,
+                           cudaMemcpyDeviceToDevice, ctx->st));
+    return check_launch(ctx, "predict");
+}
+
+// Induced dipoles: moment_from_pola_scf (src/field.f90:3200-3458) or PCG.
+int solve_dipoles(mdff_ctx* ctx) {
+    const int n = ctx->n, n3 = 3 * n;
+    const mdff_params& p = ctx->p;
+    DevScalars* d = ctx->dsc;
+    TRY(static_field(ctx));
+    const double inv_npol = 1.0 / (double)ctx->npol;
+    int iscf = 0;
+    double rmsd = 1e300;
+    int vb = std::min(592, nb(n3));
+    if (p.algo_moment_from_pola == MDFF_POLA_SCF) {
+        bool aspc = p.algo_ext_dipole == MDFF_EXT_ASPC;
+        while (((iscf < p.max_scf_pol_iter) && (rmsd > p.conv_tol_ind)) || (iscf < p.min_scf_pol_iter)) {
+            iscf++;
+            if (iscf != 1) k_induced_moment<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->E, ctx->alpha, ctx->mu_ind);
+            else TRY(predict(ctx, ctx->mu_ind));
+            TRY(induced_field(ctx, ctx->mu_ind, ctx->Eind));
+            if (iscf == 1 && aspc) {
+                // ASPC corrector: mu = w alpha E + (1-w) mu_p (src/field.f90:3986-3991)
+                int ord = p.extrapolate_order, itime = ctx->itime;
+                int eo = (itime >= ord + 1) ? ord : ((itime == 1 || itime == 0) ? 0 : itime - 1);
+                static const double W[6] = {0.0, 2.0 / 3.0, 0.6, 4.0 / 7.0, 5.0 / 9.0, 6.0 / 11.0};
+                k_aspc_correct<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->Estat, ctx->Eind, ctx->alpha, W[eo], ctx->mu_ind);
+            }
+            k_scf_residual<<<vb, 256, 0, ctx->st>>>(n, ctx->Estat, ctx->Eind, ctx->mu_ind, ctx->inv_alpha, ctx->E,
+                                                    ctx->part.buf);
+            launch_reduce_partials(ctx->st, ctx->part.buf, vb, 1, &d->rr, 0);
+            TRY(sync_scalars(ctx));
+            rmsd = std::sqrt(ctx->hsc->rr * inv_npol);
+        }
+    } else {
+        TRY(predict(ctx, ctx->mu_ind));
+        // zero the guess on non-polarisable atoms: Ad = A x uses the mask
+        TRY(induced_field(ctx, ctx->mu_ind, ctx->Eind));
+        k_apply_A<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->mu_ind, ctx->Eind, ctx->inv_alpha, ctx->cg_Ad);
+        k_cg_init<<<vb, 256, 0, ctx->st>>>(n, ctx->Estat, ctx->cg_Ad, ctx->alpha, ctx->inv_alpha, ctx->cg_r, ctx->cg_z,
+                                           ctx->cg_d, ctx->part.buf);
+        launch_reduce_partials(ctx->st, ctx->part.buf, vb, 2, &d->rr, 0);
+        k_cg_first<<<1, 32, 0, ctx->st>>>(d, inv_npol);
+        TRY(sync_scalars(ctx));
+        rmsd = ctx->hsc->rmsd;
+        while ((iscf < p.max_scf_pol_iter && rmsd > p.conv_tol_ind) || iscf < 1) {
+            iscf++;
+            TRY(induced_field(ctx, ctx->cg_d, ctx->Eind));
+            k_apply_A<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->Eind, ctx->inv_alpha, ctx->cg_Ad);
+            launch_dot(ctx->st, n3, ctx->cg_d, ctx->cg_Ad, ctx->part, &d->dAd);
+            k_cg_update<<<vb, 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->cg_Ad, ctx->alpha, ctx->mu_ind, ctx->cg_r, ctx->cg_z,
+                                                 d, ctx->part.buf);
+            launch_reduce_partials(ctx->st, ctx->part.buf, vb, 2, &d->rr, 0);
+            k_cg_scalars<<<1, 32, 0, ctx->st>>>(d, inv_npol, p.conv_tol_ind);
+            k_cg_direction<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->cg_z, ctx->cg_d, d);
+            TRY(sync_scalars(ctx));
+            rmsd = ctx->hsc->rmsd;
+            if (!std::isfinite(rmsd)) return fail(ctx, MDFF_E_NONFINITE, "non-finite residual in the dipole solve");
+        }
+    }
+    TRY(check_launch(ctx, "solve_dipoles"));
+    // u_pol = 1/2 mu.alpha^-1.mu (induced_moment, src/field.f90:1780-1790)
+    k_upol<<<vb, 256, 0, ctx->st>>>(n, ctx->mu_ind, ctx->inv_alpha, ctx->part.buf);
+    launch_reduce_partials(ctx->st, ctx->part.buf, vb, 1, d->upol, 0);
+    // store the induced dipoles at t (src/field.f90:3440)
+    CK(cudaMemcpyAsync(ctx->hist, ctx->mu_ind, sizeof(double) * n3, cudaMemcpyDeviceToDevice, ctx->st));
+    ctx->en.scf_iter = iscf;
+    ctx->en.scf_rmsd = rmsd;
+    if (iscf >= p.max_scf_pol_iter && rmsd > p.conv_tol_ind && p.algo_moment_from_pola == MDFF_POLA_PCG)
+        return fail(ctx, MDFF_E_NOCONV, "induced-dipole solve did not converge within max_scf_pol_iter");
+    return MDFF_OK;
+}
+
+// engforce_driver (src/field.f90:1111-1166) on the device; results stay in
+// device memory and ctx->hsc/en after the trailing sync.
+int engforce_device(mdff_ctx* ctx) {
+    const int n = ctx->n;
+    const mdff_params& p = ctx->p;
+    if (!p.lvnlist) TRY(build_lists(ctx, 0.0));
+    launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
+    std::memset(&ctx->en, 0, sizeof ctx->en);
+    bool nonb = p.lnmlj || p.lbmhft || p.lbmhftd || p.lmorse;
+    if (nonb) {
+        PairFlags fl{p.lnmlj, p.lbmhft, p.lbmhftd, p.lmorse, p.trunc, ctx->ntype};
+        launch_pair(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->cell, ctx->lv, ctx->pc, fl, ctx->fx, ctx->fy,
+                    ctx->fz, ctx->part, ctx->dsc);
+    } else {
+        CK(cudaMemsetAsync(ctx->fx, 0, sizeof(double) * n, ctx->st));
+        CK(cudaMemsetAsync(ctx->fy, 0, sizeof(double) * n, ctx->st));
+        CK(cudaMemsetAsync(ctx->fz, 0, sizeof(double) * n, ctx->st));
+        CK(cudaMemsetAsync(ctx->dsc->nonb, 0, sizeof(double) * 12, ctx->st));
+    }
+    TRY(check_launch(ctx, "pair"));
+    CK(cudaMemsetAsync(ctx->dsc->upol, 0, sizeof(double) * 2, ctx->st));
+    if (p.lcoulomb) {
+        const int n3 = 3 * n;
+        if (ctx->npol > 0) {
+            TRY(solve_dipoles(ctx));
+            k_add3<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->dip0, ctx->mu_ind, ctx->mu);
+        } else {
+            CK(cudaMemcpyAsync(ctx->mu, ctx->dip0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, ctx->st));
+        }
+        bool dip = ctx->any_dip0 || ctx->npol > 0;
+        DirFlags f = dir_flags(ctx);
+        f.qq = ctx->any_q ? 1 : 0;
+        f.qd = (dip && ctx->any_q) ? 1 : 0;
+        f.dd = dip ? 1 : 0;
+        f.damp = 1;
+        f.field = p.doefield ? 1 : 0;
+        f.efg = p.doefg ? 1 : 0;
+        f.forces = 1;
+        CK(cudaMemsetAsync(ctx->ef, 0, sizeof(double) * n3, ctx->st));
+        if (p.doefg) CK(cudaMemsetAsync(ctx->efg, 0, sizeof(double) * 6 * n, ctx->st));
+        launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->mu, ctx->cell, coul_list(ctx),
+                         ctx->pc, f, ctx->ef, ctx->efg, ctx->fcoul, ctx->part, ctx->dsc);
+        RecFlags rf{ctx->any_q ? 1 : 0, dip ? 1 : 0, p.doefield ? 1 : 0, (p.doefg || dip) ? 1 : 0, 1, p.precision};
+        launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->mu, ctx->cell, ctx->kg, rf, ctx->rs, ctx->ef,
+                         p.doefg ? ctx->efg : nullptr, ctx->fcoul, ctx->part, ctx->dsc);
+        int vb = std::min(592, nb(n));
+        k_coul_sums<<<vb, 256, 0, ctx->st>>>(n, ctx->q, ctx->mu, ctx->x, ctx->y, ctx->z, ctx->part.buf);
+        launch_reduce_partials(ctx->st, ctx->part.buf, vb, 8, ctx->dsc->sums, 0);
+        TRY(check_launch(ctx, "coulomb"));
+    }
+    TRY(sync_scalars(ctx));
+    const DevScalars& h = *ctx->hsc;
+    if (p.lcoulomb) {
+        double cu = ctx->u.coul;
+        double tpi_V = 2.0 * PI / ctx->cell.omega;
+        double s[3] = {h.sums[2] + h.sums[5], h.sums[3] + h.sums[6], h.sums[4] + h.sums[7]};
+        k_coul_finish<<<nb(n), 256, 0, ctx->st>>>(n, ctx->q, ctx->mu, ctx->ef, ctx->efg, ctx->fcoul, ctx->fx, ctx->fy,
+                                                  ctx->fz, selfa2(ctx), cu, p.doefg, p.lsurf, s[0], s[1], s[2],
+                                                  2.0 * tpi_V / 3.0);
+        TRY(check_launch(ctx, "coul_finish"));
+        double u_dir = h.dir[0], u_rec = h.rec[0] * 2.0 * tpi_V;
+        double u_self = -selfa(ctx) * h.sums[0] - selfa2(ctx) * h.sums[1];
+        double u_pol = 0.5 * h.upol[0];
+        double qt[3] = {h.sums[2], h.sums[3], h.sums[4]}, mt[3] = {h.sums[5], h.sums[6], h.sums[7]};
+        double u_surf = (qt[0] * qt[0] + qt[1] * qt[1] + qt[2] * qt[2]) + 2.0 * (qt[0] * mt[0] + qt[1] * mt[1] + qt[2] * mt[2]) +
+                        (mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2]);
+        u_surf *= tpi_V / 3.0;
+        double u = u_dir + u_rec + u_self + u_pol + (p.lsurf ? u_surf : 0.0);
+        ctx->en.u_dir = u_dir * cu;
+        ctx->en.u_rec = u_rec * cu;
+        ctx->en.u_self = u_self * cu;
+        ctx->en.u_surf = p.lsurf ? u_surf * cu : 0.0;
+        ctx->en.u_pol = u_pol * cu;
+        ctx->en.u_coul = u * cu;
+        static const int map[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+        double sd = 0.25 / ctx->cell.omega, sr = 2.0 * tpi_V / ctx->cell.omega;
+        std::memset(ctx->tau_coul, 0, sizeof ctx->tau_coul);
+        for (int k = 0; k < 6; ++k) {
+            double v = (h.dir[1 + k] * sd + h.rec[1 + k] * sr) * cu / ctx->u.press;
+            int a = map[k][0], b = map[k][1];
+            ctx->tau_coul[b * 3 + a] = v;
+            ctx->tau_coul[a * 3 + b] = v;
+        }
+        ctx->en.pvirial_coul = (ctx->tau_coul[0] + ctx->tau_coul[4] + ctx->tau_coul[8]) / 3.0 * ctx->u.press;
+    } else {
+        std::memset(ctx->tau_coul, 0, sizeof ctx->tau_coul);
+    }
+    ctx->en.u_lj = h.nonb[0];
+    ctx->en.vir_lj = h.nonb[1] / 3.0;
+    ctx->en.u_bmhft = h.nonb[2];
+    ctx->en.vir_bmhft = h.nonb[3] / 3.0;
+    ctx->en.u_morse = h.nonb[4];
+    ctx->en.vir_morse = h.nonb[5] / 3.0;
+    ctx->en.utail = ctx->utail;
+    ctx->en.ptail = ctx->ptail;
+    {
+        static const int map[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+        std::memset(ctx->tau_nonb, 0, sizeof ctx->tau_nonb);
+        for (int k = 0; k < 6; ++k) {
+            double v = h.nonb[6 + k] / ctx->cell.omega / ctx->u.press;
+            int a = map[k][0], b = map[k][1];
+            ctx->tau_nonb[b * 3 + a] = v;
+            ctx->tau_nonb[a * 3 + b] = v;
+        }
+    }
+    double usum = ctx->en.u_lj + ctx->en.u_bmhft + ctx->en.u_morse + ctx->en.u_coul;
+    if (!std::isfinite(usum)) return fail(ctx, MDFF_E_NONFINITE, "non-finite energy");
+    ctx->forces_valid = true;
+    return MDFF_OK;
+}
+
+int set_units(mdff_ctx* ctx) {
+    if (ctx->p.lreduced) ctx->u = {1.0, 1.0, 1.0, 1.0};
+    else ctx->u = {0.00624150964712042, 8.61734229648141e-05, 98.2269514139276, 14.3996441494161};
+    return MDFF_OK;
+}
+
+int upload(mdff_ctx* ctx, double* dst, const double* src, int n) {
+    CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+    return MDFF_OK;
+}
+int download(mdff_ctx* ctx, double* dst, const double* src, int n) {
+    CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+    return MDFF_OK;
+}
+
+void nhc_const(const mdff_ctx* ctx, NhcConst& c) {
+    const mdff_params& p = ctx->p;
+    std::memset(&c, 0, sizeof c);
+    c.nhc_n = p.nhc_n;
+    c.yosh = p.nhc_yosh_order;
+    c.mults = p.nhc_mults;
+    c.literal = p.nhc_literal ? 1 : 0;
+    c.dt = p.dt * ctx->u.time;
+    c.temp = p.temp * ctx->u.boltz;
+    c.L = 3.0 * (double)ctx->n;
+    double ts = p.timesca_thermo * ctx->u.time;
+    for (int k = 0; k < p.nhc_n; ++k) c.Q[k] = ts * ts * c.temp;   // timesca_thermo**2 * temp
+    c.Q[0] = c.Q[0] * c.L;
+    double* w = c.w;
+    switch (p.nhc_yosh_order) {
+        case 1: w[0] = 1.0; break;
+        case 3: w[0] = 1.0 / (2.0 - std::pow(2.0, 1.0 / 3.0)); w[1] = 1.0 - 2.0 * w[0]; w[2] = w[0]; break;
+        case 5: w[0] = 1.0 / (4.0 - std::pow(4.0, 1.0 / 3.0)); w[1] = w[0]; w[2] = w[0]; w[3] = w[0]; w[4] = 1.0 - 4.0 * w[0]; break;
+        case 7:
+            w[0] = .78451361047756; w[1] = .235573213359357; w[2] = -1.17767998417887;
+            w[3] = 1.0 - 2.0 * (w[0] + w[1] + w[2]); w[4] = w[2]; w[5] = w[1]; w[6] = w[0]; break;
+        default:
+            w[0] = 0.192; w[1] = 0.554910818409783619692725006662999; w[2] = 0.124659619941888644216504240951585;
+            w[3] = -0.843182063596933505315033808282941; w[4] = 1.0 - 2.0 * (w[0] + w[1] + w[2] + w[3]);
+            w[5] = w[3]; w[6] = w[2]; w[7] = w[1]; w[8] = w[0]; break;
+    }
+}
+
+int ke_reduce(mdff_ctx* ctx, int apply_scale) {
+    const int n = ctx->n;
+    k_scale_ke<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->mass, ctx->dsc, apply_scale,
+                                           ctx->part.buf);
+    launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
+    return check_launch(ctx, "ke");
+}
+
+// calc_thermo (src/thermo.f90:116-207) from the host copies.
+void fill_thermo(mdff_ctx* ctx, mdff_thermo* t, int step) {
+    const double nr = ctx->p.lreduced ? (double)ctx->n : 1.0;
+    double omega = ctx->cell.omega;
+    t->step = step;
+    t->e_kin = ctx->e_kin / nr;
+    t->temp_r = ctx->temp_r;
+    t->u_lj = ctx->en.u_lj / nr;
+    t->u_bmhft = ctx->en.u_bmhft / nr;
+    t->u_morse = ctx->en.u_morse / nr;
+    t->u_coul = ctx->en.u_coul / nr;
+    t->u_pol = ctx->en.u_pol / nr;
+    t->u_tot = t->u_lj + t->u_coul + t->u_morse + t->u_bmhft;
+    t->e_tot = t->u_tot + t->e_kin;
+    t->e_nvt = (ctx->p.integrator == MDFF_NVT_NHCN ? ctx->hsc->e_nvt : 0.0) / nr;
+    t->h_tot = ctx->p.integrator == MDFF_NVT_NHCN ? t->e_tot + t->e_nvt : t->e_tot;
+    double pv = (ctx->en.vir_lj + ctx->en.vir_morse + ctx->en.vir_bmhft) / omega / nr + ctx->en.pvirial_coul / nr;
+    t->pvirial_tot = pv / ctx->u.press;
+    t->pressure_tot = (pv + ctx->temp_r * ctx->u.boltz / omega) / ctx->u.press;
+    t->nlist_rebuilt = ctx->last_rebuilt;
+    t->scf_iter = ctx->en.scf_iter;
+    t->scf_rmsd = ctx->en.scf_rmsd;
+}
+
+void set_kin(mdff_ctx* ctx) {
+    ctx->e_kin = 0.5 * ctx->hsc->ke2[0];
+    ctx->temp_r = 2.0 * ctx->e_kin / ctx->u.boltz / (3.0 * (double)ctx->n);
+}
+
+// One MD step (body of md_run's loop, src/runmd.f90:266-277).
+int md_step(mdff_ctx* ctx) {
+    const int n = ctx->n;
+    const mdff_params& p = ctx->p;
+    const double dt = p.dt * ctx->u.time;
+    ctx->itime++;
+    if (p.integrator == MDFF_NVE_VV) {
+        k_vv_positions<<<nb(n), 256, 0, ctx->st>>>(n, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy,
+                                                   ctx->fz, ctx->fox, ctx->foy, ctx->foz, ctx->mass, dt);
+        TRY(check_launch(ctx, "vv_positions"));
+        TRY(engforce_device(ctx));
+        k_vv_velocities<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->fox,
+                                                    ctx->foy, ctx->foz, ctx->mass, dt, ctx->part.buf);
+        launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
+    } else {
+        NhcConst c;
+        nhc_const(ctx, c);
+        TRY(ke_reduce(ctx, 0));
+        k_nhc_chain<<<1, 1, 0, ctx->st>>>(ctx->dsc, c, ctx->dsc->ke2);
+        TRY(ke_reduce(ctx, 1));
+        k_kick_drift<<<nb(n), 256, 0, ctx->st>>>(n, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy,
+                                                 ctx->fz, ctx->mass, dt);
+        TRY(check_launch(ctx, "kick_drift"));
+        TRY(engforce_device(ctx));
+        k_kick<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mass, dt,
+                                           ctx->part.buf);
+        launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
+        k_nhc_chain<<<1, 1, 0, ctx->st>>>(ctx->dsc, c, ctx->dsc->ke2);
+        TRY(ke_reduce(ctx, 1));
+        k_nhc_energy<<<1, 1, 0, ctx->st>>>(ctx->dsc, c);
+    }
+    TRY(check_launch(ctx, "step"));
+    ctx->last_rebuilt = 0;
+    if (p.lvnlist) {
+        // positions unchanged since the force call: sx is current
+        launch_skin_check(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->xs, ctx->ys, ctx->zs, ctx->cell, p.skindiff,
+                          ctx->part, ctx->dsc);
+        TRY(check_launch(ctx, "skin"));
+    }
+    TRY(sync_scalars(ctx));
+    set_kin(ctx);
+    if (p.lvnlist && ctx->hsc->rebuild) {
+        TRY(build_lists(ctx, p.skindiff));
+        ctx->last_rebuilt = 1;
+    }
+    return MDFF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdff_struct_size(int which) {
+    switch (which) {
+        case 0: return (int)sizeof(mdff_params);
+        case 1: return (int)sizeof(mdff_energies);
+        case 2: return (int)sizeof(mdff_thermo);
+        default: return -1;
+    }
+}
+
+void mdff_params_default(mdff_params* p) {
+    std::memset(p, 0, sizeof *p);
+    p->ntype = 1;
+    p->lvnlist = 1;
+    p->skindiff = 0.15;
+    p->symmetric_pot = 1;
+    p->trunc = MDFF_TRUNC_NONE;
+    for (int i = 0; i < MDFF_NTYPE_MAX; ++i) {
+        p->mass[i] = 1.0;
+        for (int j = 0; j < MDFF_NTYPE_MAX; ++j) { p->qlj[i][j] = 12.0; p->plj[i][j] = 6.0; }
+    }
+    p->alphaES = 1.0;
+    p->kES[0] = p->kES[1] = p->kES[2] = 10;
+    p->epsw = 1e-6;
+    p->conv_tol_ind = 1e-6;
+    p->min_scf_pol_iter = 3;
+    p->max_scf_pol_iter = 100;
+    p->extrapolate_order = 0;
+    p->algo_ext_dipole = MDFF_EXT_POLY;
+    p->algo_moment_from_pola = MDFF_POLA_SCF;
+    p->integrator = MDFF_NVE_VV;
+    p->temp = 1.0;
+    p->nhc_n = 4;
+    p->nhc_yosh_order = 3;
+    p->nhc_mults = 2;
+    p->timesca_thermo = 1.0;
+    p->precision = MDFF_PREC_FP64;
+}
+
+int mdff_create(const mdff_params* p, mdff_ctx** out) {
+    if (!p || !out) return MDFF_E_ARG;
+    *out = nullptr;
+    mdff_ctx* ctx = new mdff_ctx();
+    ctx->p = *p;
+    int rc = check_params(ctx, ctx->p);
+    if (rc != MDFF_OK) { *out = ctx; return rc; }
+    symmetrise(ctx->p);
+    set_units(ctx);
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        ctx->err = std::string("no CUDA device: ") + cudaGetErrorString(e);
+        *out = ctx;
+        return MDFF_E_CUDA;
+    }
+    if (p->device < 0 || p->device >= ndev) { ctx->err = "device ordinal out of range"; *out = ctx; return MDFF_E_ARG; }
+    cudaSetDevice(p->device);
+    e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->hsc, sizeof(DevScalars));
+    if (e != cudaSuccess) { ctx->err = std::string("stream/pinned alloc: ") + cudaGetErrorString(e); *out = ctx; return MDFF_E_CUDA; }
+    *out = ctx;
+    return MDFF_OK;
+}
+
+void mdff_destroy(mdff_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->st) {
+        cudaSetDevice(ctx->p.device);
+        cudaStreamSynchronize(ctx->st);
+        free_all(ctx);
+        cudaStreamDestroy(ctx->st);
+    }
+    if (ctx->hsc) cudaFreeHost(ctx->hsc);
+    delete ctx;
+}
+
+const char* mdff_last_error(const mdff_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx, const double* ry, const double* rz,
+                    const double A[9]) {
+    if (!ctx || !ctx->st) return MDFF_E_STATE;
+    if (natm < 1 || !itype || !rx || !ry || !rz || !A) return fail(ctx, MDFF_E_ARG, "invalid system arguments");
+    cudaSetDevice(ctx->p.device);
+    cudaStreamSynchronize(ctx->st);
+    free_all(ctx);
+    ctx->lv = NList();
+    ctx->lc = NList();
+    ctx->grid = CellGrid();
+    ctx->have_system = ctx->have_list = ctx->forces_valid = ctx->md_started = false;
+    const mdff_params& p = ctx->p;
+    const int n = natm;
+    ctx->n = n;
+    ctx->ntype = p.ntype;
+    lattice(A, ctx->cell, ctx->W, ctx->anorm);
+    if (!(ctx->cell.omega > 0.0)) return fail(ctx, MDFF_E_ARG, "cell volume must be positive");
+    ctx->natmi.assign(NT, 0);
+    std::vector<int> t0(n);
+    std::vector<double> hq(n), hm(n), ha(n), hia(n), hd(3 * (size_t)n);
+    ctx->npol = 0;
+    ctx->any_q = ctx->any_dip0 = false;
+    for (int t = 0; t < p.ntype; ++t) {
+        if (p.qch[t] != 0.0) ctx->any_q = true;
+        for (int c = 0; c < 3; ++c) if (p.dip[t][c] != 0.0) ctx->any_dip0 = true;
+    }
+    for (int i = 0; i < n; ++i) {
+        int t = itype[i] - 1;
+        if (t < 0 || t >= p.ntype) return fail(ctx, MDFF_E_ARG, "itype out of range (1-based)");
+        t0[i] = t;
+        ctx->natmi[t]++;
+        hq[i] = p.qch[t];
+        hm[i] = p.mass[t];
+        if (!(hm[i] > 0.0)) return fail(ctx, MDFF_E_ARG, "mass must be positive");
+        ha[i] = p.ldip_polar[t] ? p.poldip_iso[t] : 0.0;
+        hia[i] = ha[i] != 0.0 ? 1.0 / ha[i] : 0.0;
+        if (ha[i] != 0.0) ctx->npol++;
+        for (int c = 0; c < 3; ++c) hd[(size_t)c * n + i] = p.dip[t][c];
+    }
+    ctx->cut_vdw = p.cutshortrange;
+    if (p.lcoulomb) ewald_param(ctx);
+    else ctx->cut_coul = p.cutlongrange;
+    std::vector<PairConst> tab;
+    build_pair_consts(ctx, tab);
+    // device buffers
+    double** d1[] = {&ctx->x, &ctx->y, &ctx->z, &ctx->vx, &ctx->vy, &ctx->vz, &ctx->fx, &ctx->fy, &ctx->fz,
+                     &ctx->fox, &ctx->foy, &ctx->foz, &ctx->sx, &ctx->sy, &ctx->sz, &ctx->xs, &ctx->ys, &ctx->zs,
+                     &ctx->q, &ctx->mass, &ctx->alpha, &ctx->inv_alpha};
+    for (double** b : d1) TRY(dalloc(ctx, b, n));
+    double** d3[] = {&ctx->dip0, &ctx->mu, &ctx->mu_ind, &ctx->Estat, &ctx->Eind, &ctx->E, &ctx->cg_r, &ctx->cg_z,
+                     &ctx->cg_d, &ctx->cg_Ad, &ctx->mu_save, &ctx->ef, &ctx->fcoul};
+    for (double** b : d3) TRY(dalloc(ctx, b, 3 * (size_t)n));
+    TRY(dalloc(ctx, &ctx->efg, 6 * (size_t)n));
+    ctx->nhist = p.extrapolate_order + 1;
+    TRY(dalloc(ctx, &ctx->hist, (size_t)ctx->nhist * 3 * n));
+    TRY(dalloc(ctx, &ctx->coef, 16));
+    TRY(dalloc(ctx, &ctx->type, n));
+    TRY(dalloc(ctx, &ctx->pc, NT * NT));
+    TRY(dalloc(ctx, &ctx->dsc, 1));
+    TRY(dalloc(ctx, &ctx->d_overflow, 1));
+    TRY(dalloc(ctx, &ctx->grid.cell_of, n));
+    TRY(dalloc(ctx, &ctx->grid.cell_atoms, n));
+    CK(cudaMemsetAsync(ctx->dsc, 0, sizeof(DevScalars), ctx->st));
+    CK(cudaMemsetAsync(ctx->hist, 0, sizeof(double) * ctx->nhist * 3 * (size_t)n, ctx->st));
+    CK(cudaMemsetAsync(ctx->mu_ind, 0, sizeof(double) * 3 * (size_t)n, ctx->st));
+    CK(cudaMemsetAsync(ctx->vx, 0, sizeof(double) * n, ctx->st));
+    CK(cudaMemsetAsync(ctx->vy, 0, sizeof(double) * n, ctx->st));
+    CK(cudaMemsetAsync(ctx->vz, 0, sizeof(double) * n, ctx->st));
+    CK(cudaMemsetAsync(ctx->fcoul, 0, sizeof(double) * 3 * (size_t)n, ctx->st));
+    CK(cudaMemsetAsync(ctx->efg, 0, sizeof(double) * 6 * (size_t)n, ctx->st));
+    CK(cudaMemcpyAsync(ctx->type, t0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->pc, tab.data(), sizeof(PairConst) * NT * NT, cudaMemcpyHostToDevice, ctx->st));
+    TRY(upload(ctx, ctx->q, hq.data(), n));
+    TRY(upload(ctx, ctx->mass, hm.data(), n));
+    TRY(upload(ctx, ctx->alpha, ha.data(), n));
+    TRY(upload(ctx, ctx->inv_alpha, hia.data(), n));
+    TRY(upload(ctx, ctx->dip0, hd.data(), 3 * n));
+    TRY(upload(ctx, ctx->x, rx, n));
+    TRY(upload(ctx, ctx->y, ry, n));
+    TRY(upload(ctx, ctx->z, rz, n));
+    launch_wrap_positions(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell);
+    // Ewald k grid (kpoint_sum_init, src/kspace.f90:142-207) as a full rectangle
+    if (p.lcoulomb) {
+        KGrid& kg = ctx->kg;
+        for (int d = 0; d < 3; ++d) kg.kmax[d] = ctx->kES[d];
+        kg.ncol = (kg.kmax[0] + 1) * (2 * kg.kmax[1] + 1);
+        kg.nzl = 2 * kg.kmax[2] + 1;
+        kg.nrect = kg.ncol * kg.nzl;
+        std::vector<double> ak(kg.nrect, 0.0), kc(kg.nrect, 0.0);
+        double a2 = ctx->alphaES * ctx->alphaES;
+        const CellP& c = ctx->cell;
+        for (int col = 0; col < kg.ncol; ++col) {
+            int nx = col / (2 * kg.kmax[1] + 1), ny = col % (2 * kg.kmax[1] + 1) - kg.kmax[1];
+            for (int m = 0; m < kg.nzl; ++m) {
+                int nz = m - kg.kmax[2];
+                bool keep = nx > 0 || (nx == 0 && ny > 0) || (nx == 0 && ny == 0 && nz > 0);
+                if (!keep) continue;
+                double kx = 2.0 * PI * (double(nx) * c.B[0] + double(ny) * c.B[1] + double(nz) * c.B[2]);
+                double ky = 2.0 * PI * (double(nx) * c.B[3] + double(ny) * c.B[4] + double(nz) * c.B[5]);
+                double kz = 2.0 * PI * (double(nx) * c.B[6] + double(ny) * c.B[7] + double(nz) * c.B[8]);
+                double kk = kx * kx + ky * ky + kz * kz;
+                if (kk == 0.0) continue;
+                ak[(size_t)col * kg.nzl + m] = std::exp(-kk * 0.25 / a2) / kk;
+                kc[(size_t)col * kg.nzl + m] = 2.0 * (1.0 / kk + 1.0 / a2 / 4.0);
+            }
+        }
+        TRY(dalloc(ctx, &kg.Ak, kg.nrect));
+        TRY(dalloc(ctx, &kg.kcoe, kg.nrect));
+        TRY(upload(ctx, kg.Ak, ak.data(), kg.nrect));
+        TRY(upload(ctx, kg.kcoe, kc.data(), kg.nrect));
+        size_t fp = 0;
+        size_t pc = rec_scratch_doubles(n, kg, &fp);
+        TRY(dalloc(ctx, &ctx->rs.part, pc));
+        TRY(dalloc(ctx, &ctx->rs.fpart, fp));
+        TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));
+        ctx->rs.part_cap = pc;
+        ctx->rs.fpart_cap = fp;
+    }
+    int parts = std::max(16 * 1024, 12 * (int)(((size_t)n * 32 + 255) / 256));
+    TRY(dalloc(ctx, &ctx->part.buf, parts));
+    ctx->part.capacity = parts;
+    // neighbour lists
+    int cap = p.nlist_capacity;
+    if (cap <= 0) {
+        double rl = rlist_max(ctx, p.skindiff);
+        double dens = (double)n / ctx->cell.omega;
+        double est = 4.0 / 3.0 * PI * rl * rl * rl * dens;
+        cap = (int)std::min<double>((double)n, est * 1.4 + 32.0);
+        cap = std::max(cap, 32);
+    }
+    TRY(ensure_lists(ctx, cap));
+    ctx->itime = 0;
+    ctx->have_system = true;
+    if (p.lvnlist) TRY(build_lists(ctx, p.skindiff));
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+int mdff_set_positions(mdff_ctx* ctx, const double* rx, const double* ry, const double* rz) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    cudaSetDevice(ctx->p.device);
+    TRY(upload(ctx, ctx->x, rx, ctx->n));
+    TRY(upload(ctx, ctx->y, ry, ctx->n));
+    TRY(upload(ctx, ctx->z, rz, ctx->n));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->forces_valid = false;
+    return MDFF_OK;
+}
+
+int mdff_get_positions(mdff_ctx* ctx, double* rx, double* ry, double* rz) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    cudaSetDevice(ctx->p.device);
+    TRY(download(ctx, rx, ctx->x, ctx->n));
+    TRY(download(ctx, ry, ctx->y, ctx->n));
+    TRY(download(ctx, rz, ctx->z, ctx->n));
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+int mdff_nlist_build(mdff_ctx* ctx) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    cudaSetDevice(ctx->p.device);
+    TRY(build_lists(ctx, ctx->p.skindiff));
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+int mdff_nlist_get(mdff_ctx* ctx, int which, int* point, int* list, int cap, int* nlist) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!ctx->have_list) return fail(ctx, MDFF_E_STATE, "no Verlet list has been built");
+    if (!point || !nlist || (which != 0 && which != 1)) return fail(ctx, MDFF_E_ARG, "invalid nlist_get arguments");
+    cudaSetDevice(ctx->p.device);
+    const int n = ctx->n;
+    bool nonb = ctx->p.lnmlj || ctx->p.lbmhft || ctx->p.lbmhftd || ctx->p.lmorse;
+    if (which == 0 && !nonb) return fail(ctx, MDFF_E_STATE, "no vdW list without a short-range potential");
+    if (which == 1 && !ctx->p.lcoulomb) return fail(ctx, MDFF_E_STATE, "no Coulomb list without lcoulomb");
+    const NList* L = which == 0 ? &ctx->lv : &coul_list(ctx);
+    const double want = which == 0 ? ctx->cut_vdw : ctx->cut_coul;
+    if (L->cut != want) return fail(ctx, MDFF_E_STATE, "list radius mismatch");
+    std::vector<int> cnt(n), nbr((size_t)n * L->cap);
+    CK(cudaMemcpyAsync(cnt.data(), L->cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(nbr.data(), L->nbr, sizeof(int) * (size_t)n * L->cap, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    int total = 0;
+    std::vector<int> row;
+    for (int i = 0; i < n; ++i) {
+        point[i] = total + 1;
+        row.clear();
+        const int I = i + 1;
+        for (int k = 0; k < cnt[i]; ++k) {
+            int j = nbr[(size_t)i * L->cap + k];
+            int J = j + 1;
+            if ((I > J && ((I + J) % 2 == 0)) || (I < J && ((I + J) % 2 != 0))) row.push_back(J);
+        }
+        std::sort(row.begin(), row.end());
+        if (list && total + (int)row.size() <= cap) std::memcpy(list + total, row.data(), sizeof(int) * row.size());
+        total += (int)row.size();
+    }
+    point[n] = total + 1;
+    *nlist = total;
+    if (total > cap) return fail(ctx, MDFF_E_LISTOVF, "list buffer too small");
+    return MDFF_OK;
+}
+
+int mdff_engforce(mdff_ctx* ctx, double* fx, double* fy, double* fz, mdff_energies* e, double tau_nonb[9],
+                  double tau_coul[9], double* ef, double* efg, double* mu) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    cudaSetDevice(ctx->p.device);
+    TRY(engforce_device(ctx));
+    const int n = ctx->n;
+    if (fx) TRY(download(ctx, fx, ctx->fx, n));
+    if (fy) TRY(download(ctx, fy, ctx->fy, n));
+    if (fz) TRY(download(ctx, fz, ctx->fz, n));
+    if (ef) TRY(download(ctx, ef, ctx->ef, 3 * n));
+    if (efg) TRY(download(ctx, efg, ctx->efg, 6 * n));
+    if (mu) TRY(download(ctx, mu, ctx->mu, 3 * n));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (ef && !ctx->p.lcoulomb) std::memset(ef, 0, sizeof(double) * 3 * n);
+    if (efg && !(ctx->p.lcoulomb && ctx->p.doefg)) std::memset(efg, 0, sizeof(double) * 6 * n);
+    if (mu && !ctx->p.lcoulomb) std::memset(mu, 0, sizeof(double) * 3 * n);
+    if (e) *e = ctx->en;
+    if (tau_nonb) std::memcpy(tau_nonb, ctx->tau_nonb, sizeof ctx->tau_nonb);
+    if (tau_coul) std::memcpy(tau_coul, ctx->tau_coul, sizeof ctx->tau_coul);
+    return MDFF_OK;
+}
+
+int mdff_md_start(mdff_ctx* ctx, const double* vx, const double* vy, const double* vz, mdff_thermo* t0) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    cudaSetDevice(ctx->p.device);
+    const int n = ctx->n;
+    if (vx) TRY(upload(ctx, ctx->vx, vx, n));
+    if (vy) TRY(upload(ctx, ctx->vy, vy, n));
+    if (vz) TRY(upload(ctx, ctx->vz, vz, n));
+    CK(cudaMemsetAsync(ctx->dsc->xi, 0, sizeof(double) * 16, ctx->st));
+    CK(cudaMemsetAsync(ctx->dsc->vxi, 0, sizeof(double) * 16, ctx->st));
+    CK(cudaMemsetAsync(&ctx->dsc->e_nvt, 0, sizeof(double), ctx->st));
+    ctx->itime = 0;
+    TRY(ke_reduce(ctx, 0));
+    TRY(engforce_device(ctx));   // syncs the scalars
+    set_kin(ctx);
+    ctx->last_rebuilt = 0;
+    ctx->md_started = true;
+    if (t0) fill_thermo(ctx, t0, 0);
+    return MDFF_OK;
+}
+
+int mdff_step(mdff_ctx* ctx, int nsteps, double* rx, double* ry, double* rz, double* vx, double* vy, double* vz,
+              double* fx, double* fy, double* fz, mdff_thermo* thermo) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!ctx->md_started) return fail(ctx, MDFF_E_STATE, "mdff_md_start first");
+    if (nsteps < 0) return fail(ctx, MDFF_E_ARG, "nsteps < 0");
+    cudaSetDevice(ctx->p.device);
+    const int n = ctx->n;
+    bool new_pos = rx || ry || rz;
+    if (rx) TRY(upload(ctx, ctx->x, rx, n));
+    if (ry) TRY(upload(ctx, ctx->y, ry, n));
+    if (rz) TRY(upload(ctx, ctx->z, rz, n));
+    if (vx) TRY(upload(ctx, ctx->vx, vx, n));
+    if (vy) TRY(upload(ctx, ctx->vy, vy, n));
+    if (vz) TRY(upload(ctx, ctx->vz, vz, n));
+    if (new_pos && !ctx->forces_valid) TRY(engforce_device(ctx));
+    for (int k = 0; k < nsteps; ++k) {
+        TRY(md_step(ctx));
+        if (thermo) fill_thermo(ctx, &thermo[k], ctx->itime);
+    }
+    if (rx) TRY(download(ctx, rx, ctx->x, n));
+    if (ry) TRY(download(ctx, ry, ctx->y, n));
+    if (rz) TRY(download(ctx, rz, ctx->z, n));
+    if (vx) TRY(download(ctx, vx, ctx->vx, n));
+    if (vy) TRY(download(ctx, vy, ctx->vy, n));
+    if (vz) TRY(download(ctx, vz, ctx->vz, n));
+    if (fx) TRY(download(ctx, fx, ctx->fx, n));
+    if (fy) TRY(download(ctx, fy, ctx->fy, n));
+    if (fz) TRY(download(ctx, fz, ctx->fz, n));
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+}  // extern "C"

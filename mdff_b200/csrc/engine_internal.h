@@ -1,0 +1,163 @@
+// engine_internal.h -- declarations shared by the engine's host code and its
+// CUDA kernels.  Nothing here is part of the public C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mdff_engine.h"
+
+namespace mdff {
+
+constexpr int NT = MDFF_NTYPE_MAX;
+constexpr double PI = 3.14159265358979323846264338327950;
+
+// Simulation cell as the kernels see it (passed by value).
+// A[3*i+j] = simu_cell%A(i+1,j+1); B likewise, already divided by omega
+// (src/lattice.f90:60-175).
+struct CellP {
+    double A[9];
+    double B[9];
+    double omega;
+};
+
+// Constants of one ordered type pair (ti,tj), index ti*NT+tj.  Built on the
+// host from mdff_params exactly as initialize_param_non_bonded
+// (src/field.f90:914-1101) and the damping tables of field_check_tag
+// (src/field.f90:316-339).
+struct PairConst {
+    // Lennard-Jones n-m
+    double rcutsq, sigsq, epsp, plj, qlj, fc, uc, uc1, uc2;
+    // BMH / BMHFTD
+    double A, B, C, D, BD;
+    // Morse
+    double epsmor, rhomor, rs;
+    // Tang-Toennies dipole damping: "_i" = (ti,ti,tj) damps the field of j's
+    // charge at i; "_j" = (tj,ti,tj) damps the field of i's charge at j
+    // (src/field.f90:2205-2217).
+    double db_i, dc_i, db_j, dc_j;
+    int dk_i, dk_j;
+    int ldamp;   // ldip_damping(ti,ti,tj) .or. ldip_damping(tj,ti,tj)
+    int pad;
+};
+
+// Neighbour lists in ELL layout: row i holds cnt[i] entries at nbr[i*cap ...].
+// The row is the FULL list (every j != i within cut+skin); the reference's
+// half list is the subset satisfying its parity ownership rule.
+struct NList {
+    int* nbr = nullptr;
+    int* cnt = nullptr;
+    int cap = 0;
+    double cut = 0.0;     // verlet_*%cut
+};
+
+// Deterministic reduction scratch: each kernel writes per-block partials of K
+// values; reduce_partials sums them in block order.
+struct Partials {
+    double* buf = nullptr;
+    int capacity = 0;   // doubles
+};
+
+// Scalars kept on the device between kernels.  Reductions write straight
+// into these slots, so each group is contiguous.
+struct DevScalars {
+    double nonb[12];    // u_lj vir_lj u_bmh vir_bmh u_mor vir_mor, stress xx yy zz xy xz yz (half-pair sums)
+    double dir[8];      // real-space energy, stress sums xx yy zz xy xz yz, pad
+    double rec[8];      // sum_k A_k|S|^2, stress sums xx yy zz xy xz yz, pad
+    double sums[8];     // qsq musq qtot(3) mutot(3)
+    double upol[2];     // sum mu.alpha^-1.mu, pad
+    double ke2[2];      // sum m v^2, pad
+    // solver
+    double rr, rz_new;  // written together by one reduction
+    double rz, dAd, beta_cg, rmsd;
+    int iter, converged;
+    // MD
+    double s_scale, e_nvt;
+    double xi[16], vxi[16];
+    // neighbour-list check
+    double dmax1, dmax2;
+    int rebuild;
+    int overflow;
+};
+
+// Launchers (kernels live in the *.cuh files, compiled as one unit by engine.cu).
+void launch_frac(cudaStream_t st, int n, const double* x, const double* y, const double* z, CellP c,
+                 double* sx, double* sy, double* sz);
+void launch_wrap_positions(cudaStream_t st, int n, double* x, double* y, double* z, CellP c);
+
+struct CellGrid {
+    int nc[3] = {1, 1, 1};
+    int ncell = 1;
+    int* cell_of = nullptr;     // [n]
+    int* cell_count = nullptr;  // [ncell]
+    int* cell_start = nullptr;  // [ncell+1]
+    int* cell_cursor = nullptr; // [ncell]
+    int* cell_atoms = nullptr;  // [n]
+    int ncell_alloc = 0;
+};
+void launch_bin(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, CellGrid& g);
+void launch_nlist(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, CellP c,
+                  const CellGrid& g, double rskinsq_a, NList& la, double rskinsq_b, NList* lb, int* overflow);
+void launch_skin_check(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
+                       const double* xs, const double* ys, const double* zs, CellP c, double skindiff,
+                       Partials& part, DevScalars* d);
+
+// Short-range pair loop: LJ / BMH(FTD) / Morse, forces written (not added).
+struct PairFlags { int lj, bmh, bmhftd, morse, trunc, ntype; };
+void launch_pair(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, const int* type,
+                 CellP c, const NList& l, const PairConst* pc, PairFlags fl,
+                 double* fx, double* fy, double* fz, Partials& part, DevScalars* d);
+
+// Real-space multipole Ewald (charges + dipoles).
+struct DirFlags {
+    int qq, qd, dd;        // tasks
+    int damp;              // damp_ind
+    int field, efg, forces;// outputs (forces implies energy + stress)
+    int ntype;
+    double alpha;          // Ewald alpha
+    double cutsq;          // verlet_coul%cut^2
+    int erfc_ref;          // use the reference's fitted erfc
+};
+void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
+                      const int* type, const double* q, const double* mu, CellP c, const NList& l,
+                      const PairConst* pc, DirFlags fl,
+                      double* ef, double* efg, double* f, Partials& part, DevScalars* d);
+
+// Reciprocal-space multipole Ewald.
+struct KGrid {
+    int kmax[3];
+    int ncol;            // (kmax0+1)*(2*kmax1+1)
+    int nzl;             // 2*kmax2+1
+    int nrect;           // ncol*nzl
+    double* Ak = nullptr;      // [nrect], 0 for excluded k
+    double* kcoe = nullptr;    // [nrect]
+};
+struct RecScratch {
+    double* part = nullptr;    // structure-factor partials
+    size_t part_cap = 0;       // doubles
+    double* aks = nullptr;     // [2][nrect] Ak*S (re, im)
+    double* fpart = nullptr;   // per-atom field partials [split][9][n]
+    size_t fpart_cap = 0;
+    float* part32 = nullptr;
+    float* aks32 = nullptr;
+};
+struct RecFlags {
+    int with_q, with_mu;
+    int field;     // E
+    int grad;      // full field gradient (for EFG and dipole forces)
+    int energy;    // energy + stress
+    int prec;      // MDFF_PREC_*
+};
+void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
+                      const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl,
+                      RecScratch& rs, double* ef, double* efg6, double* fo, Partials& part, DevScalars* d);
+size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart);
+
+// Solver vector kernels.
+void launch_dot(cudaStream_t st, int n3, const double* a, const double* b, Partials& part, double* out);
+
+// Reduce per-block partials: out[k] = sum_b buf[b*K + k].
+void launch_reduce_partials(cudaStream_t st, const double* buf, int nblocks, int K, double* out, int accumulate);
+
+}  // namespace mdff

@@ -1,0 +1,213 @@
+// ewald_real.cu -- real-space part of the multipole Ewald sum for point
+// charges and dipoles: energy, electric field, field gradient, forces, stress.
+//
+// Replaces multipole_ES_dir (src/field.f90:2057-2643) for the charge-charge,
+// charge-dipole and dipole-dipole tasks with the Tang-Toennies damping of the
+// charge-dipole interaction.  The reference builds the full rank-0..5
+// interaction tensors for every pair; here each contraction is written in
+// closed form from the screened radial functions F0..F3
+// (F1 = F0 + 2 a r e, F2 = F1 + 4/3 a^3 r^3 e, F3 = F2 + 8/15 a^5 r^5 e with
+// e = exp(-a^2 r^2)/sqrt(pi), src/field.f90:2220-2225):
+//   T1 v   = -(r.v) F1/r^3
+//   T2 v   =  r (r.v) 3F2/r^5 - v F1/r^3
+//   T3 uv  = -r (r.u)(r.v) 15F3/r^7 + [u (r.v) + v (r.u) + r (u.v)] 3F2/r^5
+// G lanes share one atom's full neighbour row and accumulate onto that atom
+// only; energies and stresses are halved per ordered pair.
+#include "common.cuh"
+
+namespace mdff {
+
+// errfc (src/functions.f90:28-39): the reference's fitted erfc (Numerical
+// Recipes' Chebyshev approximation), selectable for bit-level parity studies.
+__device__ __forceinline__ double erfc_fit(double x) {
+    double z = fabs(x);
+    double t = 1.0 / (1.0 + 0.5 * z);
+    double r = t * exp(-z * z - 1.26551223 + t * (1.00002368 + t * (.37409196 + t * (.09678418 +
+               t * (-.18628806 + t * (.27886807 + t * (-1.13520398 + t * (1.48851587 +
+               t * (-.82215223 + t * .17087277)))))))));
+    return x < 0.0 ? 2.0 - r : r;
+}
+
+__device__ __forceinline__ void tt_damp_d(double b, double c, double r, int k, double& f, double& fd) {
+    const double br = b * r;
+    const double e = exp(-br) * c;
+    double term = 1.0, sum = 1.0, inv = 1.0;
+    for (int m = 1; m <= k; ++m) {
+        inv = inv / (double)m;
+        term = term * br;
+        sum = fma(term, inv, sum);
+    }
+    f = 1.0 - sum * e;
+    fd = term * inv * e * b;
+}
+
+// MODE 0: full evaluation (tasks from flags; field / efg / forces from flags)
+// MODE 1: induced-dipole field operator E_i = sum_j T2(r_ij) mu_j (no damping),
+//         the dipole-dipole field of src/field.f90:3354.
+template <int G, int MODE>
+__global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restrict__ sx, const double* __restrict__ sy,
+                                                   const double* __restrict__ sz, const int* __restrict__ type,
+                                                   const double* __restrict__ q, const double* __restrict__ mu,
+                                                   CellP c, const int* __restrict__ nbr, const int* __restrict__ cnt,
+                                                   int cap, const PairConst* __restrict__ pc, DirFlags fl,
+                                                   double* __restrict__ ef, double* __restrict__ efg,
+                                                   double* __restrict__ fo, double* part) {
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int sub = threadIdx.x & (G - 1);
+    const bool active = gid < n;
+    const int i = active ? gid : 0;
+    const double a = fl.alpha, a2 = a * a, a3 = a2 * a, a5 = a3 * a2;
+    const double rsqpi = 0.56418958354775628695;   // 1/sqrt(pi)
+    double E[3] = {0, 0, 0}, Gd[6] = {0, 0, 0, 0, 0, 0}, F[3] = {0, 0, 0};
+    double u = 0.0, S[6] = {0, 0, 0, 0, 0, 0};
+    if (active) {
+        const double si1 = sx[i], si2 = sy[i], si3 = sz[i];
+        const int ti = type[i];
+        const double qi = MODE == 0 ? q[i] : 0.0;
+        const double mi0 = mu[i], mi1 = mu[n + i], mi2 = mu[2 * n + i];
+        const int m = cnt[i];
+        const int* row = nbr + (size_t)i * cap;
+        for (int k = sub; k < m; k += G) {
+            const int j = row[k];
+            double rx, ry, rz;
+            const double d2 = pairvec_exact(c, si1, si2, si3, sx[j], sy[j], sz[j], rx, ry, rz);
+            if (d2 > fl.cutsq) continue;
+            const double mj0 = mu[j], mj1 = mu[n + j], mj2 = mu[2 * n + j];
+            const double d = sqrt(d2);
+            const double dm1 = 1.0 / d, dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2, dm7 = dm5 * dm2;
+            const double expon = exp(-a2 * d2) * rsqpi;
+            const double F0 = fl.erfc_ref ? erfc_fit(a * d) : erfc(a * d);
+            const double F1 = F0 + 2.0 * a * d * expon;
+            const double F2 = F1 + 4.0 * a3 * d2 * d * expon / 3.0;
+            const double A1 = F1 * dm3;
+            const double B2 = 3.0 * F2 * dm5;
+            const double rmj = rx * mj0 + ry * mj1 + rz * mj2;
+            if (MODE == 1) {
+                E[0] += rx * rmj * B2 - mj0 * A1;
+                E[1] += ry * rmj * B2 - mj1 * A1;
+                E[2] += rz * rmj * B2 - mj2 * A1;
+                continue;
+            }
+            const int tj = type[j];
+            const double qj = q[j];
+            const double rmi = rx * mi0 + ry * mi1 + rz * mi2;
+            const double F3 = F2 + 8.0 * a5 * d2 * d2 * d * expon / 15.0;
+            const double C3 = 15.0 * F3 * dm7;
+            // Tang-Toennies damping of the charge-dipole terms (src/field.f90:2205-2217).
+            double gi = 0.0, gdi = 0.0, gj = 0.0, gdj = 0.0;
+            bool ldamp = false;
+            if (fl.damp) {
+                const PairConst& P = pc[ti * NT + tj];
+                if (P.ldamp) {
+                    ldamp = true;
+                    double f1, f2;
+                    tt_damp_d(P.db_i, P.dc_i, d, P.dk_i, f1, gdi);
+                    tt_damp_d(P.db_j, P.dc_j, d, P.dk_j, f2, gdj);
+                    gi = 1.0 - f1;
+                    gj = 1.0 - f2;
+                }
+            }
+            double fi0 = 0.0, fi1 = 0.0, fi2 = 0.0;
+            if (fl.qq) {
+                u += 0.5 * qi * qj * F0 * dm1;
+                if (fl.field) {
+                    const double s = qj * (F1 - gi) * dm3;
+                    E[0] += s * rx; E[1] += s * ry; E[2] += s * rz;
+                }
+                if (fl.efg) {
+                    const double b = -qj * B2, dg = qj * A1;
+                    Gd[0] += b * rx * rx + dg; Gd[1] += b * ry * ry + dg; Gd[2] += b * rz * rz + dg;
+                    Gd[3] += b * rx * ry; Gd[4] += b * rx * rz; Gd[5] += b * ry * rz;
+                }
+                const double s = qi * qj * A1;
+                fi0 += s * rx; fi1 += s * ry; fi2 += s * rz;
+            }
+            if (fl.dd) {
+                const double mimj = mi0 * mj0 + mi1 * mj1 + mi2 * mj2;
+                u -= 0.5 * (rmi * rmj * B2 - mimj * A1);
+                if (fl.field) {
+                    E[0] += rx * rmj * B2 - mj0 * A1;
+                    E[1] += ry * rmj * B2 - mj1 * A1;
+                    E[2] += rz * rmj * B2 - mj2 * A1;
+                }
+                if (fl.efg) {
+                    const double t = -rmj * C3;
+                    Gd[0] += t * rx * rx + rmj * B2 + 2.0 * rx * mj0 * B2;
+                    Gd[1] += t * ry * ry + rmj * B2 + 2.0 * ry * mj1 * B2;
+                    Gd[2] += t * rz * rz + rmj * B2 + 2.0 * rz * mj2 * B2;
+                    Gd[3] += t * rx * ry + (ry * mj0 + rx * mj1) * B2;
+                    Gd[4] += t * rx * rz + (rz * mj0 + rx * mj2) * B2;
+                    Gd[5] += t * ry * rz + (rz * mj1 + ry * mj2) * B2;
+                }
+                const double t3 = -rmi * rmj * C3 + mimj * B2;
+                fi0 += t3 * rx + (mi0 * rmj + mj0 * rmi) * B2;
+                fi1 += t3 * ry + (mi1 * rmj + mj1 * rmi) * B2;
+                fi2 += t3 * rz + (mi2 * rmj + mj2 * rmi) * B2;
+            }
+            if (fl.qd) {
+                u += 0.5 * (qi * A1 * rmj - qj * A1 * rmi);
+                // qi T2 mu_j - qj T2 mu_i
+                const double s = (qi * rmj - qj * rmi) * B2;
+                fi0 += rx * s - (qi * mj0 - qj * mi0) * A1;
+                fi1 += ry * s - (qi * mj1 - qj * mi1) * A1;
+                fi2 += rz * s - (qi * mj2 - qj * mi2) * A1;
+                if (ldamp) {
+                    u += 0.5 * (-qi * gj * dm3 * rmj + qj * gi * dm3 * rmi);
+                    const double F2d = gi + (d / 3.0) * gdi, F2d2 = gj + (d / 3.0) * gdj;
+                    const double Bi = 3.0 * F2d * dm5, Ai = gi * dm3;     // T2d  (damping at i)
+                    const double Bj = 3.0 * F2d2 * dm5, Aj = gj * dm3;    // T2d2 (damping at j)
+                    // qj T2d mu_i - qi T2d2 mu_j
+                    fi0 += qj * (rx * rmi * Bi - mi0 * Ai) - qi * (rx * rmj * Bj - mj0 * Aj);
+                    fi1 += qj * (ry * rmi * Bi - mi1 * Ai) - qi * (ry * rmj * Bj - mj1 * Aj);
+                    fi2 += qj * (rz * rmi * Bi - mi2 * Ai) - qi * (rz * rmj * Bj - mj2 * Aj);
+                }
+            }
+            if (fl.forces) {
+                F[0] += fi0; F[1] += fi1; F[2] += fi2;
+                S[0] += 2.0 * rx * fi0; S[1] += 2.0 * ry * fi1; S[2] += 2.0 * rz * fi2;
+                S[3] += rx * fi1 + ry * fi0; S[4] += rx * fi2 + rz * fi0; S[5] += ry * fi2 + rz * fi1;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) E[k] = group_sum<G>(E[k]);
+    if (MODE == 0) {
+        if (fl.efg) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) Gd[k] = group_sum<G>(Gd[k]);
+        }
+        if (fl.forces) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) F[k] = group_sum<G>(F[k]);
+        }
+    }
+    if (active && sub == 0) {
+        if (MODE == 1 || fl.field) { ef[i] = E[0]; ef[n + i] = E[1]; ef[2 * n + i] = E[2]; }
+        if (MODE == 0 && fl.efg)
+            for (int k = 0; k < 6; ++k) efg[(size_t)k * n + i] = Gd[k];
+        if (MODE == 0 && fl.forces) { fo[i] = F[0]; fo[n + i] = F[1]; fo[2 * n + i] = F[2]; }
+    }
+    if (MODE == 0) {
+        double v[8] = {u, S[0], S[1], S[2], S[3], S[4], S[5], 0.0};
+        block_partials<8>(v, part);
+    }
+}
+
+void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
+                      const int* type, const double* q, const double* mu, CellP c, const NList& l,
+                      const PairConst* pc, DirFlags fl, double* ef, double* efg, double* f, Partials& part,
+                      DevScalars* d) {
+    constexpr int G = 16;
+    const int threads = 256;
+    const int blocks = (int)(((size_t)n * G + threads - 1) / threads);
+    if (!q) {
+        k_ewald_dir<G, 1><<<blocks, threads, 0, st>>>(n, sx, sy, sz, type, q, mu, c, l.nbr, l.cnt, l.cap, pc, fl, ef,
+                                                      efg, f, nullptr);
+        return;
+    }
+    k_ewald_dir<G, 0><<<blocks, threads, 0, st>>>(n, sx, sy, sz, type, q, mu, c, l.nbr, l.cnt, l.cap, pc, fl, ef,
+                                                  efg, f, part.buf);
+    launch_reduce_partials(st, part.buf, blocks, 8, d->dir, 0);
+}
+
+}  // namespace mdff

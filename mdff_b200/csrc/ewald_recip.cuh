@@ -1,0 +1,319 @@
+// ewald_recip.cu -- reciprocal-space part of the multipole Ewald sum.
+//
+// Replaces multipole_ES_rec (src/field.f90:2646-2873) and the k-vector set of
+// kpoint_sum_init (src/kspace.f90:142-207).  The reference loops over k in the
+// outer loop and over all atoms twice inside, with one sin/cos per (k, atom).
+// Here:
+//   pass 1 (k_sfac):  S(k) = sum_i (q_i + i k.mu_i) e^{i k.r_i}
+//       one thread per (k-column (nx,ny), chunk of CH consecutive nz); the
+//       phase is exact from direct coordinates, e^{ik.r} = e^{2 pi i n.s},
+//       with one sincospi per (atom, chunk) and a complex rotation by
+//       e^{2 pi i s_z} per further nz.  The atoms are split over blockIdx.y;
+//       the per-chunk partial sums are added in a fixed order (k_sfac_reduce),
+//       which also forms A_k S(k), the energy and the stress per k.
+//   pass 2 (k_kfield): per atom, E_i = -sum_k k A_k Im(S* e^{ik.r_i}) and the
+//       field gradient sum_k k k^T A_k Re(S* e^{ik.r_i}); one thread per atom,
+//       k-columns staged in shared memory, split over blockIdx.y and reduced
+//       in a fixed order (k_kfield_reduce), which also forms the forces
+//       F_i = q_i E_i + G_i mu_i (src/field.f90:2776-2789).
+// The k set is the full rectangle nx in [0,kx], ny in [-ky,ky], nz in
+// [-kz,kz] with A_k = 0 on the half that the reference skips.
+#include "common.cuh"
+
+namespace mdff {
+
+constexpr int SF_THREADS = 128;
+constexpr int SF_TILE = 64;
+
+template <int CH>
+__global__ void __launch_bounds__(SF_THREADS) k_sfac(int n, int natom_chunk, const double* __restrict__ sx,
+                                                     const double* __restrict__ sy, const double* __restrict__ sz,
+                                                     const double* __restrict__ q, const double* __restrict__ mu,
+                                                     CellP c, int kx, int ky, int kz, int ncol, int ncolblk,
+                                                     int nchunk, int with_q, int with_mu, double* __restrict__ part_re,
+                                                     double* __restrict__ part_im) {
+    __shared__ double t_s1[SF_TILE], t_s2[SF_TILE], t_s3[SF_TILE], t_q[SF_TILE];
+    __shared__ double t_m1[SF_TILE], t_m2[SF_TILE], t_m3[SF_TILE], t_cs[SF_TILE], t_sn[SF_TILE];
+    const int h = blockIdx.x / ncolblk;
+    const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
+    const int p = blockIdx.y;
+    const int ny_n = 2 * ky + 1;
+    const int colc = col < ncol ? col : ncol - 1;
+    const double nx = (double)(colc / ny_n);
+    const double ny = (double)(colc % ny_n - ky);
+    const double nz0 = (double)(-kz + h * CH);
+    double are[CH], aim[CH];
+#pragma unroll
+    for (int m = 0; m < CH; ++m) { are[m] = 0.0; aim[m] = 0.0; }
+    const int a0 = p * natom_chunk;
+    const int a1 = min(n, a0 + natom_chunk);
+    for (int base = a0; base < a1; base += SF_TILE) {
+        __syncthreads();
+        if (threadIdx.x < SF_TILE) {
+            int ia = base + threadIdx.x;
+            if (ia < a1) {
+                double s1 = sx[ia], s2 = sy[ia], s3 = sz[ia];
+                t_s1[threadIdx.x] = s1; t_s2[threadIdx.x] = s2; t_s3[threadIdx.x] = s3;
+                t_q[threadIdx.x] = with_q ? q[ia] : 0.0;
+                double m0 = 0, m1 = 0, m2 = 0;
+                if (with_mu) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
+                // 2 pi (b_j . mu), b_j = column j of B: k.mu = nx*t_m1 + ny*t_m2 + nz*t_m3
+                t_m1[threadIdx.x] = 2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2);
+                t_m2[threadIdx.x] = 2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2);
+                t_m3[threadIdx.x] = 2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2);
+                double fz = s3 - rint(s3);
+                double sn, cs;
+                sincospi(2.0 * fz, &sn, &cs);
+                t_cs[threadIdx.x] = cs; t_sn[threadIdx.x] = sn;
+            }
+        }
+        __syncthreads();
+        const int tn = min(SF_TILE, a1 - base);
+        for (int t = 0; t < tn; ++t) {
+            double ph = fma(nx, t_s1[t], fma(ny, t_s2[t], nz0 * t_s3[t]));
+            ph -= rint(ph);
+            double sn, cs;
+            sincospi(2.0 * ph, &sn, &cs);
+            const double qa = t_q[t];
+            double km = fma(nx, t_m1[t], fma(ny, t_m2[t], nz0 * t_m3[t]));
+            const double dm = t_m3[t], rc = t_cs[t], rs = t_sn[t];
+#pragma unroll
+            for (int m = 0; m < CH; ++m) {
+                are[m] = fma(qa, cs, fma(-km, sn, are[m]));
+                aim[m] = fma(qa, sn, fma(km, cs, aim[m]));
+                const double cn = cs * rc - sn * rs;
+                sn = fma(sn, rc, cs * rs);
+                cs = cn;
+                km += dm;
+            }
+        }
+    }
+    if (col < ncol) {
+        const size_t plane = (size_t)ncol * CH * nchunk;
+#pragma unroll
+        for (int m = 0; m < CH; ++m) {
+            size_t idx = (size_t)p * plane + ((size_t)h * CH + m) * ncol + col;
+            part_re[idx] = are[m];
+            part_im[idx] = aim[m];
+        }
+    }
+}
+
+// Sum the atom-chunk partials in order; A_k S(k); energy and stress per k
+// (src/field.f90:2742-2745, 2803-2815).
+__global__ void k_sfac_reduce(int P, int ch, int nchunk, int ncol, int nzl, int kx, int ky, int kz,
+                              const double* __restrict__ part_re, const double* __restrict__ part_im,
+                              const double* __restrict__ Ak, const double* __restrict__ kcoe, CellP c,
+                              double* __restrict__ aks, int nrect, int energy, double* partials) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int total = ncol * nzl;
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (t < total) {
+        const int col = t % ncol;
+        const int mz = t / ncol;          // 0 .. nzl-1
+        const size_t plane = (size_t)ncol * ch * nchunk;
+        const size_t off = (size_t)mz * ncol + col;   // (h*ch + m) == mz
+        double sr = 0.0, si = 0.0;
+        for (int p = 0; p < P; ++p) {
+            sr += part_re[(size_t)p * plane + off];
+            si += part_im[(size_t)p * plane + off];
+        }
+        const int r = col * nzl + mz;
+        const double ak = Ak[r];
+        aks[r] = ak * sr;
+        aks[nrect + r] = ak * si;
+        if (energy && ak != 0.0) {
+            const int ny_n = 2 * ky + 1;
+            const double nx = (double)(col / ny_n), ny = (double)(col % ny_n - ky), nz = (double)(mz - kz);
+            const double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz * c.B[2]);
+            const double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz * c.B[5]);
+            const double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz * c.B[8]);
+            const double str = (sr * sr + si * si) * ak;
+            const double kc = kcoe[r];
+            v[0] = str;
+            v[1] = (1.0 - kc * k0 * k0) * str;
+            v[2] = (1.0 - kc * k1 * k1) * str;
+            v[3] = (1.0 - kc * k2 * k2) * str;
+            v[4] = -kc * k0 * k1 * str;
+            v[5] = -kc * k0 * k2 * str;
+            v[6] = -kc * k1 * k2 * str;
+        }
+    }
+    if (energy) block_partials<7>(v, partials);
+}
+
+constexpr int KF_THREADS = 128;
+constexpr int KF_COLS = 4;   // columns staged per shared-memory round
+
+template <int GRAD>
+__global__ void __launch_bounds__(KF_THREADS) k_kfield(int n, const double* __restrict__ sx, const double* __restrict__ sy,
+                                                       const double* __restrict__ sz, CellP c, int kx, int ky, int kz,
+                                                       int ncol, int nzl, int cols_per_split,
+                                                       const double* __restrict__ aks, int nrect,
+                                                       double* __restrict__ fpart) {
+    extern __shared__ double sm[];
+    double* s_re = sm;
+    double* s_im = sm + KF_COLS * nzl;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int split = blockIdx.y;
+    const int c0 = split * cols_per_split;
+    const int c1 = min(ncol, c0 + cols_per_split);
+    const bool active = i < n;
+    const int ii = active ? i : 0;
+    const double s1 = sx[ii], s2 = sy[ii], s3 = sz[ii];
+    double rs, rc;
+    sincospi(2.0 * (s3 - rint(s3)), &rs, &rc);
+    const double dk0 = 2.0 * PI * c.B[2], dk1 = 2.0 * PI * c.B[5], dk2 = 2.0 * PI * c.B[8];
+    const int ny_n = 2 * ky + 1;
+    double E0 = 0, E1 = 0, E2 = 0;
+    double G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
+    for (int cb = c0; cb < c1; cb += KF_COLS) {
+        const int nc = min(KF_COLS, c1 - cb);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nc * nzl; t += blockDim.x) {
+            s_re[t] = aks[(size_t)cb * nzl + t];
+            s_im[t] = aks[(size_t)nrect + (size_t)cb * nzl + t];
+        }
+        __syncthreads();
+        for (int cc = 0; cc < nc; ++cc) {
+            const int col = cb + cc;
+            const double nx = (double)(col / ny_n), ny = (double)(col % ny_n - ky), nz0 = (double)(-kz);
+            double ph = fma(nx, s1, fma(ny, s2, nz0 * s3));
+            ph -= rint(ph);
+            double sn, cs;
+            sincospi(2.0 * ph, &sn, &cs);
+            double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz0 * c.B[2]);
+            double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz0 * c.B[5]);
+            double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz0 * c.B[8]);
+            const double* pr = s_re + cc * nzl;
+            const double* pi = s_im + cc * nzl;
+            for (int m = 0; m < nzl; ++m) {
+                const double ar = pr[m], ai = pi[m];
+                const double recarg = ai * cs - ar * sn;
+                E0 = fma(-k0, recarg, E0);
+                E1 = fma(-k1, recarg, E1);
+                E2 = fma(-k2, recarg, E2);
+                if (GRAD) {
+                    const double r2 = ar * cs + ai * sn;
+                    const double a0 = k0 * r2, a1 = k1 * r2;
+                    G0 = fma(k0, a0, G0);
+                    G1 = fma(k1, a1, G1);
+                    G2 = fma(k2, k2 * r2, G2);
+                    G3 = fma(k1, a0, G3);
+                    G4 = fma(k2, a0, G4);
+                    G5 = fma(k2, a1, G5);
+                }
+                const double cn = cs * rc - sn * rs;
+                sn = fma(sn, rc, cs * rs);
+                cs = cn;
+                k0 += dk0; k1 += dk1; k2 += dk2;
+            }
+        }
+    }
+    if (active) {
+        const int nv = GRAD ? 9 : 3;
+        double* o = fpart + (size_t)split * nv * n;
+        o[i] = E0; o[n + i] = E1; o[2 * n + i] = E2;
+        if (GRAD) {
+            o[3 * n + i] = G0; o[4 * n + i] = G1; o[5 * n + i] = G2;
+            o[6 * n + i] = G3; o[7 * n + i] = G4; o[8 * n + i] = G5;
+        }
+    }
+}
+
+// Sum the column splits in order and scale by 2 (half mesh) * 4 pi / V.
+// ef (3n) += E_rec; efg (6n: xx yy zz xy xz yz) += G_rec; fo (3n) +=
+// q E_rec + G_rec mu.
+__global__ void k_kfield_reduce(int n, int nsplit, int grad, const double* __restrict__ fpart, double scale,
+                                const double* __restrict__ q, const double* __restrict__ mu, double* ef,
+                                double* efg, double* fo) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int nv = grad ? 9 : 3;
+    double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < nsplit; ++s)
+        for (int k = 0; k < nv; ++k) v[k] += fpart[((size_t)s * nv + k) * n + i];
+    for (int k = 0; k < nv; ++k) v[k] *= scale;
+    if (ef) { ef[i] += v[0]; ef[n + i] += v[1]; ef[2 * n + i] += v[2]; }
+    if (grad && efg)
+        for (int k = 0; k < 6; ++k) efg[(size_t)k * n + i] += v[3 + k];
+    if (fo) {
+        const double qi = q ? q[i] : 0.0;
+        double f0 = qi * v[0], f1 = qi * v[1], f2 = qi * v[2];
+        if (grad && mu) {
+            const double m0 = mu[i], m1 = mu[n + i], m2 = mu[2 * n + i];
+            f0 += v[3] * m0 + v[6] * m1 + v[7] * m2;
+            f1 += v[6] * m0 + v[4] * m1 + v[8] * m2;
+            f2 += v[7] * m0 + v[8] * m1 + v[5] * m2;
+        }
+        fo[i] += f0; fo[n + i] += f1; fo[2 * n + i] += f2;
+    }
+}
+
+struct RecLaunch {
+    int CH, nchunk, ncolblk, P, natom_chunk, nsplit, cols_per_split;
+};
+
+static RecLaunch plan(int n, const KGrid& kg) {
+    RecLaunch L;
+    L.CH = 16;
+    if (kg.nzl <= 8) L.CH = 8;
+    else if (kg.nzl <= 12) L.CH = 12;
+    L.nchunk = (kg.nzl + L.CH - 1) / L.CH;
+    L.ncolblk = (kg.ncol + SF_THREADS - 1) / SF_THREADS;
+    long threads1 = (long)L.nchunk * L.ncolblk * SF_THREADS;
+    long want = 148L * 1536;
+    int P = (int)((want + threads1 - 1) / threads1);
+    P = std::max(1, std::min(P, (n + 63) / 64));
+    L.natom_chunk = (n + P - 1) / P;
+    L.P = (n + L.natom_chunk - 1) / L.natom_chunk;
+    long threads2 = (long)((n + KF_THREADS - 1) / KF_THREADS) * KF_THREADS;
+    int S = (int)((want + threads2 - 1) / threads2);
+    S = std::max(1, std::min(S, kg.ncol));
+    L.cols_per_split = (kg.ncol + S - 1) / S;
+    L.nsplit = (kg.ncol + L.cols_per_split - 1) / L.cols_per_split;
+    return L;
+}
+
+size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart) {
+    RecLaunch L = plan(n, kg);
+    *fpart = (size_t)L.nsplit * 9 * n;
+    return (size_t)L.P * L.nchunk * L.CH * kg.ncol * 2;
+}
+
+void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
+                      const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl, RecScratch& rs,
+                      double* ef, double* efg, double* fo, Partials& part, DevScalars* d) {
+    RecLaunch L = plan(n, kg);
+    const size_t plane = (size_t)L.P * L.nchunk * L.CH * kg.ncol;
+    double* pre = rs.part;
+    double* pim = rs.part + plane;
+    dim3 g1(L.nchunk * L.ncolblk, L.P);
+    const int kx = kg.kmax[0], ky = kg.kmax[1], kz = kg.kmax[2];
+#define SFAC(CHV) k_sfac<CHV><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, sx, sy, sz, q, mu, c, kx, ky, kz, kg.ncol, \
+                                                     L.ncolblk, L.nchunk, fl.with_q, fl.with_mu, pre, pim)
+    if (L.CH == 16) SFAC(16);
+    else if (L.CH == 12) SFAC(12);
+    else SFAC(8);
+#undef SFAC
+    const int total = kg.ncol * kg.nzl;
+    const int rb = (total + 255) / 256;
+    k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, L.CH, L.nchunk, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak, kg.kcoe, c,
+                                      rs.aks, kg.nrect, fl.energy, part.buf);
+    if (fl.energy) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
+    if (!fl.field && !fl.grad) return;
+    dim3 g2((n + KF_THREADS - 1) / KF_THREADS, L.nsplit);
+    size_t smem = sizeof(double) * 2 * KF_COLS * kg.nzl;
+    if (fl.grad)
+        k_kfield<1><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
+                                                  rs.aks, kg.nrect, rs.fpart);
+    else
+        k_kfield<0><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
+                                                  rs.aks, kg.nrect, rs.fpart);
+    const double scale = 2.0 * 4.0 * PI / c.omega;
+    k_kfield_reduce<<<(n + 255) / 256, 256, 0, st>>>(n, L.nsplit, fl.grad, rs.fpart, scale, fl.with_q ? q : nullptr,
+                                                    fl.with_mu ? mu : nullptr, fl.field ? ef : nullptr, efg,
+                                                    fo);
+}
+
+}  // namespace mdff

@@ -1,0 +1,215 @@
+// solve.cu -- deterministic reductions and the induced-dipole solver's vector
+// kernels.
+//
+// The reference iterates mu <- alpha (E_stat + T mu) (moment_from_pola_scf,
+// src/field.f90:3200-3458) and stops on the RMS of mu/alpha - E
+// (src/field.f90:3378-3400).  Both that fixed-point iteration and a
+// Jacobi-preconditioned conjugate-gradient solve of (1/alpha - T) mu = E_stat
+// are driven from the host with these kernels; every dot product is an FP64
+// block reduction summed in block order, so runs are bit-reproducible.
+#include "common.cuh"
+
+namespace mdff {
+
+// out[k] (+)= sum_b buf[b*K + k]; one warp per k, lanes stride over blocks,
+// fixed shuffle tree.
+__global__ void k_reduce_partials(const double* __restrict__ buf, int nblocks, int K, double* out, int accumulate) {
+    const int k = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    if (k >= K) return;
+    double s = 0.0;
+    for (int b = lane; b < nblocks; b += 32) s += buf[(size_t)b * K + k];
+    s = warp_sum(s);
+    if (lane == 0) out[k] = accumulate ? out[k] + s : s;
+}
+
+void launch_reduce_partials(cudaStream_t st, const double* buf, int nblocks, int K, double* out, int accumulate) {
+    k_reduce_partials<<<1, 32 * K, 0, st>>>(buf, nblocks, K, out, accumulate);
+}
+
+constexpr int VB = 256;
+static int vblocks(int n) { int b = (n + VB - 1) / VB; return b > 592 ? 592 : b; }
+
+__global__ void k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double* part) {
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] = fma(a[i], b[i], v[0]);
+    block_partials<1>(v, part);
+}
+
+void launch_dot(cudaStream_t st, int n, const double* a, const double* b, Partials& part, double* out) {
+    int nb = vblocks(n);
+    k_dot<<<nb, VB, 0, st>>>(n, a, b, part.buf);
+    launch_reduce_partials(st, part.buf, nb, 1, out, 0);
+}
+
+// Ad = d/alpha - Eind on polarisable atoms, 0 elsewhere (n3 = 3n, component-major).
+__global__ void k_apply_A(int n, const double* __restrict__ d, const double* __restrict__ Eind,
+                          const double* __restrict__ inv_alpha, double* Ad) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * n) return;
+    int i = t % n;
+    double ia = inv_alpha[i];
+    Ad[t] = ia != 0.0 ? d[t] * ia - Eind[t] : 0.0;
+}
+
+// r = b - Ax on polarisable atoms; z = alpha r; partial sums of r.r and r.z.
+__global__ void k_cg_init(int n, const double* __restrict__ b, const double* __restrict__ Ax,
+                          const double* __restrict__ alpha, const double* __restrict__ inv_alpha, double* r, double* z,
+                          double* dvec, double* part) {
+    double v[2] = {0.0, 0.0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * n; t += gridDim.x * blockDim.x) {
+        int i = t % n;
+        double rr = inv_alpha[i] != 0.0 ? b[t] - Ax[t] : 0.0;
+        double zz = alpha[i] * rr;
+        r[t] = rr;
+        z[t] = zz;
+        dvec[t] = zz;
+        v[0] = fma(rr, rr, v[0]);
+        v[1] = fma(rr, zz, v[1]);
+    }
+    block_partials<2>(v, part);
+}
+
+// x += a d; r -= a Ad; z = alpha r; partial sums of r.r and r.z, with
+// a = rz / dAd read from the device scalars.
+__global__ void k_cg_update(int n, const double* __restrict__ dvec, const double* __restrict__ Ad,
+                            const double* __restrict__ alpha, double* x, double* r, double* z, const DevScalars* sc,
+                            double* part) {
+    const double a = sc->rz / sc->dAd;
+    double v[2] = {0.0, 0.0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * n; t += gridDim.x * blockDim.x) {
+        int i = t % n;
+        double xx = fma(a, dvec[t], x[t]);
+        double rr = fma(-a, Ad[t], r[t]);
+        double zz = alpha[i] * rr;
+        x[t] = xx;
+        r[t] = rr;
+        z[t] = zz;
+        v[0] = fma(rr, rr, v[0]);
+        v[1] = fma(rr, zz, v[1]);
+    }
+    block_partials<2>(v, part);
+}
+
+// beta = rz_new / rz; rz = rz_new; rmsd = sqrt(r.r / npol).
+__global__ void k_cg_scalars(DevScalars* sc, double inv_npol, double tol) {
+    if (threadIdx.x != 0) return;
+    double rr = sc->rr;     // written by the reduction: rr, rz_new
+    sc->beta_cg = sc->rz_new / sc->rz;
+    sc->rz = sc->rz_new;
+    sc->rmsd = sqrt(rr * inv_npol);
+    sc->converged = sc->rmsd <= tol;
+    sc->iter += 1;
+}
+
+__global__ void k_cg_direction(int n3, const double* __restrict__ z, double* dvec, const DevScalars* sc) {
+    const double b = sc->beta_cg;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n3) dvec[t] = fma(b, dvec[t], z[t]);
+}
+
+__global__ void k_cg_first(DevScalars* sc, double inv_npol) {
+    if (threadIdx.x != 0) return;
+    sc->rz = sc->rz_new;
+    sc->rmsd = sqrt(sc->rr * inv_npol);
+    sc->iter = 0;
+}
+
+// Fixed-point step (induced_moment, src/field.f90:1716-1803): mu = alpha E.
+__global__ void k_induced_moment(int n, const double* __restrict__ E, const double* __restrict__ alpha, double* mu) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 3 * n) mu[t] = alpha[t % n] * E[t];
+}
+
+// ASPC corrector (src/field.f90:3986-3991): mu = w alpha (Estat + Eind) + (1-w) mu_p.
+__global__ void k_aspc_correct(int n, const double* __restrict__ Estat, const double* __restrict__ Eind,
+                               const double* __restrict__ alpha, double w, double* mu) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 3 * n) mu[t] = w * (alpha[t % n] * (Estat[t] + Eind[t])) + (1.0 - w) * mu[t];
+}
+
+// E = Estat + Eind; partial sums of (mu/alpha - E)^2 over polarisable atoms.
+__global__ void k_scf_residual(int n, const double* __restrict__ Estat, const double* __restrict__ Eind,
+                               const double* __restrict__ mu, const double* __restrict__ inv_alpha, double* E,
+                               double* part) {
+    double v[1] = {0.0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * n; t += gridDim.x * blockDim.x) {
+        int i = t % n;
+        double e = Estat[t] + Eind[t];
+        E[t] = e;
+        if (inv_alpha[i] != 0.0) {
+            double r = mu[t] * inv_alpha[i] - e;
+            v[0] = fma(r, r, v[0]);
+        }
+    }
+    block_partials<1>(v, part);
+}
+
+// u_pol = 1/2 sum mu . alpha^-1 mu over polarisable atoms.
+__global__ void k_upol(int n, const double* __restrict__ mu, const double* __restrict__ inv_alpha, double* part) {
+    double v[1] = {0.0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * n; t += gridDim.x * blockDim.x) {
+        int i = t % n;
+        v[0] = fma(mu[t] * inv_alpha[i], mu[t], v[0]);
+    }
+    block_partials<1>(v, part);
+}
+
+// Sums needed by the self and surface terms (src/field.f90:1869-1880):
+// qsq, musq, qtot (sum q r), mutot.
+__global__ void k_coul_sums(int n, const double* __restrict__ q, const double* __restrict__ mu,
+                            const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                            double* part) {
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double qi = q ? q[i] : 0.0;
+        double m0 = mu[i], m1 = mu[n + i], m2 = mu[2 * n + i];
+        v[0] += qi * qi;
+        v[1] += m0 * m0 + m1 * m1 + m2 * m2;
+        v[2] += qi * x[i]; v[3] += qi * y[i]; v[4] += qi * z[i];
+        v[5] += m0; v[6] += m1; v[7] += m2;
+    }
+    block_partials<8>(v, part);
+}
+
+// Extrapolation of the induced dipoles from previous steps.
+// mode 0: x = sum_k coef[k] hist[k]   (polynomial of order <= 1 and ASPC predictor)
+// mode 1: Neville interpolation polint (src/field.f90:3995-4042) at x = 1 from
+//         npt points at xa = 0, -1, -2, ...
+__global__ void k_extrapolate(int n3, int mode, int npt, const double* __restrict__ hist, const double* __restrict__ coef,
+                              double* x) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    if (mode == 0) {
+        double s = 0.0;
+        for (int k = 0; k < npt; ++k) s += coef[k] * hist[(size_t)k * n3 + t];
+        x[t] = s;
+        return;
+    }
+    double c[16], d[16];
+    int xa[16];
+    for (int k = 0; k < npt; ++k) { xa[k] = -k; c[k] = d[k] = hist[(size_t)k * n3 + t]; }
+    int ns = 1;
+    double dif = fabs(1.0 - xa[0]);
+    for (int k = 1; k <= npt; ++k) {
+        double dift = fabs(1.0 - xa[k - 1]);
+        if (dift < dif) { ns = k; dif = dift; }
+    }
+    double y = c[ns - 1], dy;
+    ns = ns - 1;
+    for (int m = 1; m <= npt - 1; ++m) {
+        for (int k = 1; k <= npt - m; ++k) {
+            double ho = double(xa[k - 1] - 1), hp = double(xa[k] - 1);
+            double w = c[k] - d[k - 1];
+            double den = w / (ho - hp);
+            d[k - 1] = hp * den;
+            c[k - 1] = ho * den;
+        }
+        if (2 * ns < npt - m) dy = c[ns];
+        else { dy = d[ns - 1]; ns = ns - 1; }
+        y = y + dy;
+    }
+    x[t] = y;
+}
+
+}  // namespace mdff

@@ -27,6 +27,12 @@
 //       initial vnlist_pbc (src/mdff.f90:192); here every build records them.
 //   D11 Positions are not round-tripped in place through kardir/dirkar on
 //       every force call (src/field.f90:1237,1341 and similar).
+//   D13 chain_nhcn (src/integration.f90:617-649) uses G(2..M-1) before
+//       computing them on the first downward pass of every call (they are 0,
+//       then stale), so for chains longer than 2 the extended energy is not
+//       conserved.  Here the inner chain forces are refreshed first (the
+//       Martyna-Tuckerman-Klein order); identical to the reference for M = 2.
+//       nhc_literal = 1 restores the reference's order.
 //   D12 errfc: the reference's fitted erfc (src/functions.f90:28-39, a
 //       published Chebyshev fit, relative error ~1.2e-7) is selectable with
 //       orc_set_erfc_mode(sys, 0); mode 1 (default) uses libm erfc.
@@ -1189,6 +1195,8 @@ void chain_nhcn(orc_sys* s, double& kin, const std::vector<double>& Q, double L)
             double dts = yw[j] * s->dt / double(p.nhc_mults);
             double dts2 = dts * 0.5, dts4 = dts2 * 0.5, dts8 = dts4 * 0.5;
             G[nhc - 1] = (vxi[nhc - 2] * vxi[nhc - 2] / Q[nhc - 2] - temp);
+            if (!p.nhc_literal)   // D13: refresh the inner chain forces before the downward pass
+                for (int inh = 1; inh < nhc - 1; ++inh) G[inh] = vxi[inh - 1] * vxi[inh - 1] / Q[inh - 1] - temp;
             vxi[nhc - 1] = vxi[nhc - 1] + G[nhc - 1] * dts4;
             for (int inh = nhc - 2; inh >= 0; --inh) {
                 vxi[inh] = vxi[inh] * std::exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);

@@ -164,6 +164,11 @@ typedef struct mdff_thermo {
  * reference counterpart. */
 int  mdff_struct_size(int which);
 
+/* Measured FMA throughput of the device in TFLOP/s: out[0] FP64, out[1]
+ * FP32, out[2] packed FP32x2 (fma.rn.f32x2).  The roofline denominators of
+ * the engine's FMA-bound kernels; no reference counterpart. */
+int  mdff_measure_pipes(int device, double out[3]);
+
 /* Fill p with the reference defaults (control_default_tag, src/control.f90:199-243;
  * field_default_tag, src/field.f90:192-273; md_default_tag, src/md.f90:178-205). */
 void mdff_params_default(mdff_params* p);
@@ -180,6 +185,20 @@ void mdff_destroy(mdff_ctx* ctx);
 
 /* Message of the last failing call on ctx (never NULL). */
 const char* mdff_last_error(const mdff_ctx* ctx);
+
+/* The context's CUDA stream (cudaStream_t), so a caller can order its own
+ * work or timing events against the engine's; no reference counterpart. */
+int  mdff_stream(mdff_ctx* ctx, void** stream);
+
+/* Kernel timing with CUDA events on the context's stream, per kernel group:
+ * 0 Verlet list, 1 pair loop, 2 Ewald real space, 3 structure factor,
+ * 4 reciprocal field, 5 dipole solver vectors, 6 integrator, 7 other.
+ * The counterpart of the reference's MPI_WTIME accumulators
+ * (src/time.f90:35-73, src/symbol.h:2-17).  mdff_profile_get returns the
+ * accumulated milliseconds and kernel launches per group and in total, and
+ * clears them when reset != 0. */
+int  mdff_profile(mdff_ctx* ctx, int enable);
+int  mdff_profile_get(mdff_ctx* ctx, double ms[8], long long count[8], long long* launches, int reset);
 
 /* Define the system: natm atoms, 1-based types, Cartesian positions and the
  * cell.  Replaces read_pos + typeinfo_init (src/read_pos.f90:35-219): the cell
@@ -198,6 +217,9 @@ int  mdff_set_positions(mdff_ctx* ctx, const double* rx, const double* ry, const
 
 /* Wrapped positions as the engine holds them. */
 int  mdff_get_positions(mdff_ctx* ctx, double* rx, double* ry, double* rz);
+
+/* Current velocities (internal units). */
+int  mdff_get_velocities(mdff_ctx* ctx, double* vx, double* vy, double* vz);
 
 /* One force evaluation at the current positions with the current lists:
  * replaces engforce_driver (src/field.f90:1111-1166), i.e. the LJ / BMH(FTD) /

@@ -57,6 +57,12 @@ def lib():
         L.mdff_nlist_get.argtypes = [vp, C.c_int, ip, ip, C.c_int, ip]
         L.mdff_md_start.argtypes = [vp, dp, dp, dp, C.POINTER(abi.Thermo)]
         L.mdff_step.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
+        L.mdff_get_velocities.argtypes = [vp, dp, dp, dp]
+        L.mdff_stream.argtypes = [vp, C.POINTER(vp)]
+        L.mdff_profile.argtypes = [vp, C.c_int]
+        L.mdff_profile_get.argtypes = [vp, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int]
+        L.mdff_measure_pipes.argtypes = [C.c_int, dp]
+        L.mdff_struct_size.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -67,6 +73,18 @@ def _dp(a):
 
 def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+
+
+PROFILE_GROUPS = ("nlist", "pair", "dir", "sfac", "kfield", "solver", "integrate", "other")
+
+
+def measure_pipes(device=0):
+    """Measured FMA throughput (TFLOP/s): (fp64, fp32, fp32x2)."""
+    out = np.zeros(3)
+    rc = lib().mdff_measure_pipes(int(device), _dp(out))
+    if rc != 0:
+        raise EngineError(rc, "mdff_measure_pipes failed")
+    return tuple(float(x) for x in out)
 
 
 def params_default():
@@ -117,6 +135,34 @@ class Engine:
         pos = np.asarray(pos, dtype=np.float64)
         r = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
         self._check(lib().mdff_set_positions(self._h, *(_dp(a) for a in r)))
+
+    def velocities(self):
+        v = [np.empty(self.n) for _ in range(3)]
+        self._check(lib().mdff_get_velocities(self._h, *(_dp(a) for a in v)))
+        return np.stack(v, axis=1)
+
+    state_velocities = velocities
+
+    def stream(self):
+        """The engine's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        ptr = C.c_void_p()
+        self._check(lib().mdff_stream(self._h, C.byref(ptr)))
+        return ptr.value or 0
+
+    def enable_profile(self, on=True):
+        self._check(lib().mdff_profile(self._h, int(bool(on))))
+
+    def profile(self, reset=False):
+        ms = np.zeros(8)
+        cnt = (C.c_longlong * 8)()
+        tot = C.c_longlong()
+        self._check(lib().mdff_profile_get(self._h, _dp(ms), cnt, C.byref(tot), int(bool(reset))))
+        out = {k: {"ms": float(ms[i]), "count": int(cnt[i])} for i, k in enumerate(PROFILE_GROUPS)}
+        out["_launches"] = {"ms": 0.0, "count": int(tot.value)}
+        return out
+
+    def profile_reset(self):
+        self.profile(reset=True)
 
     def nlist_build(self):
         self._check(lib().mdff_nlist_build(self._h))

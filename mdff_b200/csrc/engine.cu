@@ -19,6 +19,7 @@
 #include "ewald_recip.cuh"
 #include "solve.cuh"
 #include "integrate.cuh"
+#include "peaks.cuh"
 
 using namespace mdff;
 
@@ -85,6 +86,7 @@ struct mdff_ctx {
     double tau_nonb[9], tau_coul[9];
     int last_rebuilt = 0;
     int nrebuild = 0;
+    Prof prof;
 };
 
 namespace {
@@ -132,6 +134,7 @@ int check_launch(mdff_ctx* ctx, const char* where) {
 int sync_scalars(mdff_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    ctx->prof.harvest();
     return MDFF_OK;
 }
 
@@ -327,15 +330,19 @@ int build_lists(mdff_ctx* ctx, double skin) {
         TRY(dalloc(ctx, &g.cell_cursor, g.ncell));
         g.ncell_alloc = g.ncell;
     }
+    ctx->prof.begin(PK_NLIST);
     launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
     launch_bin(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, g);
+    ctx->prof.end(5);
     bool nonb = ctx->p.lnmlj || ctx->p.lbmhft || ctx->p.lbmhftd || ctx->p.lmorse;
     double cut_a = nonb ? ctx->cut_vdw : ctx->cut_coul;
     for (int attempt = 0; attempt < 4; ++attempt) {
         double ra = cut_a + skin, rb = ctx->cut_coul + skin;
         CK(cudaMemsetAsync(ctx->d_overflow, 0, sizeof(int), ctx->st));
+        ctx->prof.begin(PK_NLIST);
         launch_nlist(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->cell, g, ra * ra, ctx->lv, rb * rb,
                      ctx->shared_list ? nullptr : &ctx->lc, ctx->d_overflow);
+        ctx->prof.end(1);
         TRY(check_launch(ctx, "nlist"));
         int ovf = 0;
         CK(cudaMemcpyAsync(&ovf, ctx->d_overflow, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
@@ -417,12 +424,16 @@ int induced_field(mdff_ctx* ctx, const double* m, double* out) {
     DirFlags f = dir_flags(ctx);
     f.dd = 1;
     f.field = 1;
+    ctx->prof.begin(PK_DIR);
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, nullptr, m, ctx->cell, coul_list(ctx), ctx->pc,
                      f, out, nullptr, nullptr, ctx->part, ctx->dsc);
-    RecFlags rf{0, 1, 1, 0, 0, ctx->p.precision};
+    ctx->prof.end(1);
+    RecFlags rf{0, 1, 1, 0, 0, 0, ctx->p.precision};
     launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, nullptr, m, ctx->cell, ctx->kg, rf, ctx->rs, out, nullptr,
-                     nullptr, ctx->part, ctx->dsc);
+                     nullptr, ctx->part, ctx->dsc, &ctx->prof);
+    ctx->prof.begin(PK_SOLVER);
     k_axpy<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, 2.0 * selfa2(ctx), m, out);
+    ctx->prof.end(1);
     return check_launch(ctx, "induced_field");
 }
 
@@ -436,12 +447,16 @@ int static_field(mdff_ctx* ctx) {
     f.dd = ctx->any_dip0 ? 1 : 0;
     f.damp = 1;
     f.field = 1;
+    ctx->prof.begin(PK_DIR);
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->dip0, ctx->cell, coul_list(ctx),
                      ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc);
-    RecFlags rf{1, ctx->any_dip0 ? 1 : 0, 1, 0, 0, ctx->p.precision};
+    ctx->prof.end(2);
+    RecFlags rf{1, ctx->any_dip0 ? 1 : 0, 1, 0, 0, 0, ctx->p.precision};
     launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->dip0, ctx->cell, ctx->kg, rf, ctx->rs,
-                     ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc);
+                     ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, &ctx->prof);
+    ctx->prof.begin(PK_SOLVER);
     k_axpy<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, 2.0 * selfa2(ctx), ctx->dip0, ctx->Estat);
+    ctx->prof.end(1);
     return check_launch(ctx, "static_field");
 }
 
@@ -468,6 +483,7 @@ int predict(mdff_ctx* ctx, double* x) {
         coef[0] = 1.0;
     } else if (ord == 1) {
         if (itime > 1) { coef[0] = 2.0; coef[1] = -1.0; npt = 2; }
+        else coef[0] = 1.0;
         shift_from = 1;
     } else {
         if (itime > ord) { mode = 1; npt = ord + 1; }
@@ -477,7 +493,9 @@ int predict(mdff_ctx* ctx, double* x) {
         shift_from = ord;
     }
     CK(cudaMemcpyAsync(ctx->coef, coef, sizeof(coef), cudaMemcpyHostToDevice, ctx->st));
+    ctx->prof.begin(PK_SOLVER);
     k_extrapolate<<<nb(n3), 256, 0, ctx->st>>>(n3, mode, npt, ctx->hist, ctx->coef, x);
+    ctx->prof.end(1);
     for (int k = shift_from; k >= 1; --k)
         CK(cudaMemcpyAsync(ctx->hist + (size_t)k * n3, ctx->hist + (size_t)(k - 1) * n3, sizeof(double) * n3,
                            cudaMemcpyDeviceToDevice, ctx->st));
@@ -498,19 +516,28 @@ int solve_dipoles(mdff_ctx* ctx) {
         bool aspc = p.algo_ext_dipole == MDFF_EXT_ASPC;
         while (((iscf < p.max_scf_pol_iter) && (rmsd > p.conv_tol_ind)) || (iscf < p.min_scf_pol_iter)) {
             iscf++;
-            if (iscf != 1) k_induced_moment<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->E, ctx->alpha, ctx->mu_ind);
-            else TRY(predict(ctx, ctx->mu_ind));
+            if (iscf != 1) {
+                ctx->prof.begin(PK_SOLVER);
+                k_induced_moment<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->E, ctx->alpha, ctx->mu_ind);
+                ctx->prof.end(1);
+            } else {
+                TRY(predict(ctx, ctx->mu_ind));
+            }
             TRY(induced_field(ctx, ctx->mu_ind, ctx->Eind));
             if (iscf == 1 && aspc) {
                 // ASPC corrector: mu = w alpha E + (1-w) mu_p (src/field.f90:3986-3991)
                 int ord = p.extrapolate_order, itime = ctx->itime;
                 int eo = (itime >= ord + 1) ? ord : ((itime == 1 || itime == 0) ? 0 : itime - 1);
                 static const double W[6] = {0.0, 2.0 / 3.0, 0.6, 4.0 / 7.0, 5.0 / 9.0, 6.0 / 11.0};
+                ctx->prof.begin(PK_SOLVER);
                 k_aspc_correct<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->Estat, ctx->Eind, ctx->alpha, W[eo], ctx->mu_ind);
+                ctx->prof.end(1);
             }
+            ctx->prof.begin(PK_SOLVER);
             k_scf_residual<<<vb, 256, 0, ctx->st>>>(n, ctx->Estat, ctx->Eind, ctx->mu_ind, ctx->inv_alpha, ctx->E,
                                                     ctx->part.buf);
             launch_reduce_partials(ctx->st, ctx->part.buf, vb, 1, &d->rr, 0);
+            ctx->prof.end(2);
             TRY(sync_scalars(ctx));
             rmsd = std::sqrt(ctx->hsc->rr * inv_npol);
         }
@@ -518,16 +545,19 @@ int solve_dipoles(mdff_ctx* ctx) {
         TRY(predict(ctx, ctx->mu_ind));
         // zero the guess on non-polarisable atoms: Ad = A x uses the mask
         TRY(induced_field(ctx, ctx->mu_ind, ctx->Eind));
+        ctx->prof.begin(PK_SOLVER);
         k_apply_A<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->mu_ind, ctx->Eind, ctx->inv_alpha, ctx->cg_Ad);
         k_cg_init<<<vb, 256, 0, ctx->st>>>(n, ctx->Estat, ctx->cg_Ad, ctx->alpha, ctx->inv_alpha, ctx->cg_r, ctx->cg_z,
                                            ctx->cg_d, ctx->part.buf);
         launch_reduce_partials(ctx->st, ctx->part.buf, vb, 2, &d->rr, 0);
         k_cg_first<<<1, 32, 0, ctx->st>>>(d, inv_npol);
+        ctx->prof.end(4);
         TRY(sync_scalars(ctx));
         rmsd = ctx->hsc->rmsd;
         while ((iscf < p.max_scf_pol_iter && rmsd > p.conv_tol_ind) || iscf < 1) {
             iscf++;
             TRY(induced_field(ctx, ctx->cg_d, ctx->Eind));
+            ctx->prof.begin(PK_SOLVER);
             k_apply_A<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->Eind, ctx->inv_alpha, ctx->cg_Ad);
             launch_dot(ctx->st, n3, ctx->cg_d, ctx->cg_Ad, ctx->part, &d->dAd);
             k_cg_update<<<vb, 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->cg_Ad, ctx->alpha, ctx->mu_ind, ctx->cg_r, ctx->cg_z,
@@ -535,6 +565,7 @@ int solve_dipoles(mdff_ctx* ctx) {
             launch_reduce_partials(ctx->st, ctx->part.buf, vb, 2, &d->rr, 0);
             k_cg_scalars<<<1, 32, 0, ctx->st>>>(d, inv_npol, p.conv_tol_ind);
             k_cg_direction<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->cg_z, ctx->cg_d, d);
+            ctx->prof.end(8);
             TRY(sync_scalars(ctx));
             rmsd = ctx->hsc->rmsd;
             if (!std::isfinite(rmsd)) return fail(ctx, MDFF_E_NONFINITE, "non-finite residual in the dipole solve");
@@ -542,8 +573,10 @@ int solve_dipoles(mdff_ctx* ctx) {
     }
     TRY(check_launch(ctx, "solve_dipoles"));
     // u_pol = 1/2 mu.alpha^-1.mu (induced_moment, src/field.f90:1780-1790)
+    ctx->prof.begin(PK_SOLVER);
     k_upol<<<vb, 256, 0, ctx->st>>>(n, ctx->mu_ind, ctx->inv_alpha, ctx->part.buf);
     launch_reduce_partials(ctx->st, ctx->part.buf, vb, 1, d->upol, 0);
+    ctx->prof.end(2);
     // store the induced dipoles at t (src/field.f90:3440)
     CK(cudaMemcpyAsync(ctx->hist, ctx->mu_ind, sizeof(double) * n3, cudaMemcpyDeviceToDevice, ctx->st));
     ctx->en.scf_iter = iscf;
@@ -559,13 +592,17 @@ int engforce_device(mdff_ctx* ctx) {
     const int n = ctx->n;
     const mdff_params& p = ctx->p;
     if (!p.lvnlist) TRY(build_lists(ctx, 0.0));
+    ctx->prof.begin(PK_OTHER);
     launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
+    ctx->prof.end(1);
     std::memset(&ctx->en, 0, sizeof ctx->en);
     bool nonb = p.lnmlj || p.lbmhft || p.lbmhftd || p.lmorse;
     if (nonb) {
         PairFlags fl{p.lnmlj, p.lbmhft, p.lbmhftd, p.lmorse, p.trunc, ctx->ntype};
+        ctx->prof.begin(PK_PAIR);
         launch_pair(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->cell, ctx->lv, ctx->pc, fl, ctx->fx, ctx->fy,
                     ctx->fz, ctx->part, ctx->dsc);
+        ctx->prof.end(2);
     } else {
         CK(cudaMemsetAsync(ctx->fx, 0, sizeof(double) * n, ctx->st));
         CK(cudaMemsetAsync(ctx->fy, 0, sizeof(double) * n, ctx->st));
@@ -578,7 +615,9 @@ int engforce_device(mdff_ctx* ctx) {
         const int n3 = 3 * n;
         if (ctx->npol > 0) {
             TRY(solve_dipoles(ctx));
+            ctx->prof.begin(PK_OTHER);
             k_add3<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->dip0, ctx->mu_ind, ctx->mu);
+            ctx->prof.end(1);
         } else {
             CK(cudaMemcpyAsync(ctx->mu, ctx->dip0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, ctx->st));
         }
@@ -593,14 +632,18 @@ int engforce_device(mdff_ctx* ctx) {
         f.forces = 1;
         CK(cudaMemsetAsync(ctx->ef, 0, sizeof(double) * n3, ctx->st));
         if (p.doefg) CK(cudaMemsetAsync(ctx->efg, 0, sizeof(double) * 6 * n, ctx->st));
+        ctx->prof.begin(PK_DIR);
         launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->mu, ctx->cell, coul_list(ctx),
                          ctx->pc, f, ctx->ef, ctx->efg, ctx->fcoul, ctx->part, ctx->dsc);
-        RecFlags rf{ctx->any_q ? 1 : 0, dip ? 1 : 0, p.doefield ? 1 : 0, (p.doefg || dip) ? 1 : 0, 1, p.precision};
+        ctx->prof.end(2);
+        RecFlags rf{ctx->any_q ? 1 : 0, dip ? 1 : 0, p.doefield ? 1 : 0, (p.doefg || dip) ? 1 : 0, 1, 1, p.precision};
         launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->mu, ctx->cell, ctx->kg, rf, ctx->rs, ctx->ef,
-                         p.doefg ? ctx->efg : nullptr, ctx->fcoul, ctx->part, ctx->dsc);
+                         p.doefg ? ctx->efg : nullptr, ctx->fcoul, ctx->part, ctx->dsc, &ctx->prof);
         int vb = std::min(592, nb(n));
+        ctx->prof.begin(PK_OTHER);
         k_coul_sums<<<vb, 256, 0, ctx->st>>>(n, ctx->q, ctx->mu, ctx->x, ctx->y, ctx->z, ctx->part.buf);
         launch_reduce_partials(ctx->st, ctx->part.buf, vb, 8, ctx->dsc->sums, 0);
+        ctx->prof.end(2);
         TRY(check_launch(ctx, "coulomb"));
     }
     TRY(sync_scalars(ctx));
@@ -609,9 +652,11 @@ int engforce_device(mdff_ctx* ctx) {
         double cu = ctx->u.coul;
         double tpi_V = 2.0 * PI / ctx->cell.omega;
         double s[3] = {h.sums[2] + h.sums[5], h.sums[3] + h.sums[6], h.sums[4] + h.sums[7]};
+        ctx->prof.begin(PK_OTHER);
         k_coul_finish<<<nb(n), 256, 0, ctx->st>>>(n, ctx->q, ctx->mu, ctx->ef, ctx->efg, ctx->fcoul, ctx->fx, ctx->fy,
                                                   ctx->fz, selfa2(ctx), cu, p.doefg, p.lsurf, s[0], s[1], s[2],
                                                   2.0 * tpi_V / 3.0);
+        ctx->prof.end(1);
         TRY(check_launch(ctx, "coul_finish"));
         double u_dir = h.dir[0], u_rec = h.rec[0] * 2.0 * tpi_V;
         double u_self = -selfa(ctx) * h.sums[0] - selfa2(ctx) * h.sums[1];
@@ -709,9 +754,11 @@ void nhc_const(const mdff_ctx* ctx, NhcConst& c) {
 
 int ke_reduce(mdff_ctx* ctx, int apply_scale) {
     const int n = ctx->n;
+    ctx->prof.begin(PK_INTEGRATE);
     k_scale_ke<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->mass, ctx->dsc, apply_scale,
                                            ctx->part.buf);
     launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
+    ctx->prof.end(2);
     return check_launch(ctx, "ke");
 }
 
@@ -751,36 +798,50 @@ int md_step(mdff_ctx* ctx) {
     const double dt = p.dt * ctx->u.time;
     ctx->itime++;
     if (p.integrator == MDFF_NVE_VV) {
+        ctx->prof.begin(PK_INTEGRATE);
         k_vv_positions<<<nb(n), 256, 0, ctx->st>>>(n, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy,
                                                    ctx->fz, ctx->fox, ctx->foy, ctx->foz, ctx->mass, dt);
+        ctx->prof.end(1);
         TRY(check_launch(ctx, "vv_positions"));
         TRY(engforce_device(ctx));
+        ctx->prof.begin(PK_INTEGRATE);
         k_vv_velocities<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->fox,
                                                     ctx->foy, ctx->foz, ctx->mass, dt, ctx->part.buf);
         launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
+        ctx->prof.end(2);
     } else {
         NhcConst c;
         nhc_const(ctx, c);
         TRY(ke_reduce(ctx, 0));
+        ctx->prof.begin(PK_INTEGRATE);
         k_nhc_chain<<<1, 1, 0, ctx->st>>>(ctx->dsc, c, ctx->dsc->ke2);
+        ctx->prof.end(1);
         TRY(ke_reduce(ctx, 1));
+        ctx->prof.begin(PK_INTEGRATE);
         k_kick_drift<<<nb(n), 256, 0, ctx->st>>>(n, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy,
                                                  ctx->fz, ctx->mass, dt);
+        ctx->prof.end(1);
         TRY(check_launch(ctx, "kick_drift"));
         TRY(engforce_device(ctx));
+        ctx->prof.begin(PK_INTEGRATE);
         k_kick<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mass, dt,
                                            ctx->part.buf);
         launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
         k_nhc_chain<<<1, 1, 0, ctx->st>>>(ctx->dsc, c, ctx->dsc->ke2);
+        ctx->prof.end(3);
         TRY(ke_reduce(ctx, 1));
+        ctx->prof.begin(PK_INTEGRATE);
         k_nhc_energy<<<1, 1, 0, ctx->st>>>(ctx->dsc, c);
+        ctx->prof.end(1);
     }
     TRY(check_launch(ctx, "step"));
     ctx->last_rebuilt = 0;
     if (p.lvnlist) {
         // positions unchanged since the force call: sx is current
+        ctx->prof.begin(PK_NLIST);
         launch_skin_check(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->xs, ctx->ys, ctx->zs, ctx->cell, p.skindiff,
                           ctx->part, ctx->dsc);
+        ctx->prof.end(2);
         TRY(check_launch(ctx, "skin"));
     }
     TRY(sync_scalars(ctx));
@@ -795,6 +856,79 @@ int md_step(mdff_ctx* ctx) {
 }  // namespace
 
 extern "C" {
+
+int mdff_measure_pipes(int device, double out[3]) {
+    if (!out) return MDFF_E_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return MDFF_E_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int blocks = sms * 8, threads = 256;
+    void* buf = nullptr;
+    if (cudaMalloc(&buf, 64) != cudaSuccess) return MDFF_E_NOMEM;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    double best[3] = {0, 0, 0};
+    const double lanes = (double)blocks * threads * PK_ITERS;
+    for (int rep = 0; rep < 4; ++rep) {
+        for (int kind = 0; kind < 3; ++kind) {
+            cudaEventRecord(a);
+            if (kind == 0) k_peak_f64<<<blocks, threads>>>((double*)buf, 1.0);
+            else if (kind == 1) k_peak_f32<<<blocks, threads>>>((float*)buf, 1.0f);
+            else k_peak_f32x2<<<blocks, threads>>>((float*)buf, 1.0f);
+            cudaEventRecord(b);
+            cudaEventSynchronize(b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            double flops = lanes * (kind == 0 ? 8.0 : 16.0) * 2.0;
+            double tf = flops / (ms * 1e-3) / 1e12;
+            if (rep > 0 && tf > best[kind]) best[kind] = tf;
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(buf);
+    if (e != cudaSuccess) return MDFF_E_CUDA;
+    for (int k = 0; k < 3; ++k) out[k] = best[k];
+    return MDFF_OK;
+}
+
+int mdff_profile(mdff_ctx* ctx, int enable) {
+    if (!ctx) return MDFF_E_ARG;
+    ctx->prof.on = enable != 0;
+    return MDFF_OK;
+}
+
+int mdff_profile_get(mdff_ctx* ctx, double ms[8], long long count[8], long long* launches, int reset) {
+    if (!ctx) return MDFF_E_ARG;
+    cudaSetDevice(ctx->p.device);
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->prof.harvest();
+    for (int k = 0; k < PK_NKIND; ++k) {
+        if (ms) ms[k] = ctx->prof.ms[k];
+        if (count) count[k] = ctx->prof.count[k];
+    }
+    if (launches) *launches = ctx->prof.launches;
+    if (reset) ctx->prof.reset();
+    return MDFF_OK;
+}
+
+int mdff_get_velocities(mdff_ctx* ctx, double* vx, double* vy, double* vz) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    cudaSetDevice(ctx->p.device);
+    TRY(download(ctx, vx, ctx->vx, ctx->n));
+    TRY(download(ctx, vy, ctx->vy, ctx->n));
+    TRY(download(ctx, vz, ctx->vz, ctx->n));
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+int mdff_stream(mdff_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return MDFF_E_ARG;
+    *stream = (void*)ctx->st;
+    return MDFF_OK;
+}
 
 int mdff_struct_size(int which) {
     switch (which) {
@@ -854,6 +988,7 @@ int mdff_create(const mdff_params* p, mdff_ctx** out) {
     cudaSetDevice(p->device);
     e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->hsc, sizeof(DevScalars));
+    ctx->prof.st = ctx->st;
     if (e != cudaSuccess) { ctx->err = std::string("stream/pinned alloc: ") + cudaGetErrorString(e); *out = ctx; return MDFF_E_CUDA; }
     *out = ctx;
     return MDFF_OK;
@@ -864,6 +999,7 @@ void mdff_destroy(mdff_ctx* ctx) {
     if (ctx->st) {
         cudaSetDevice(ctx->p.device);
         cudaStreamSynchronize(ctx->st);
+        ctx->prof.release();
         free_all(ctx);
         cudaStreamDestroy(ctx->st);
     }
@@ -988,6 +1124,9 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
         TRY(dalloc(ctx, &ctx->rs.part, pc));
         TRY(dalloc(ctx, &ctx->rs.fpart, fp));
         TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));
+        TRY(dalloc(ctx, &ctx->rs.aks32, 2 * (size_t)kg.nrect));
+        TRY(dalloc(ctx, &ctx->rs.fixed, 3 * (size_t)n));
+        TRY(dalloc(ctx, &ctx->rs.stepz, (size_t)n));
         ctx->rs.part_cap = pc;
         ctx->rs.fpart_cap = fp;
     }

@@ -42,6 +42,61 @@ struct PairConst {
     int pad;
 };
 
+// Per-kernel-group timing with CUDA events on the context's stream (the
+// counterpart of the reference's MPI_WTIME accumulators, src/time.f90:35-73)
+// and a count of kernel launches.
+enum ProfKind { PK_NLIST = 0, PK_PAIR, PK_DIR, PK_SFAC, PK_KFIELD, PK_SOLVER, PK_INTEGRATE, PK_OTHER, PK_NKIND };
+struct Prof {
+    bool on = false;
+    cudaStream_t st = nullptr;
+    struct Pending { int kind; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    double ms[PK_NKIND] = {0};
+    long count[PK_NKIND] = {0};
+    long launches = 0;
+    int open_kind = -1;
+    cudaEvent_t get() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int kind) {
+        if (!on) return;
+        Pending p{kind, get(), get()};
+        cudaEventRecord(p.a, st);
+        pending.push_back(p);
+        open_kind = kind;
+    }
+    void end(int nkernels) {
+        launches += nkernels;
+        if (!on || pending.empty() || open_kind < 0) return;
+        cudaEventRecord(pending.back().b, st);
+        count[pending.back().kind] += nkernels;
+        open_kind = -1;
+    }
+    void harvest() {   // after the stream has been synchronised
+        for (auto& p : pending) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ms[p.kind] += t;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void reset() {
+        harvest();
+        for (int k = 0; k < PK_NKIND; ++k) { ms[k] = 0.0; count[k] = 0; }
+        launches = 0;
+    }
+    void release() {
+        harvest();
+        for (auto e : pool) cudaEventDestroy(e);
+        pool.clear();
+    }
+};
+
 // Neighbour lists in ELL layout: row i holds cnt[i] entries at nbr[i*cap ...].
 // The row is the FULL list (every j != i within cut+skin); the reference's
 // half list is the subset satisfying its parity ownership rule.
@@ -139,19 +194,22 @@ struct RecScratch {
     double* aks = nullptr;     // [2][nrect] Ak*S (re, im)
     double* fpart = nullptr;   // per-atom field partials [split][9][n]
     size_t fpart_cap = 0;
-    float* part32 = nullptr;
-    float* aks32 = nullptr;
+    float* aks32 = nullptr;     // [2][nrect] Ak*S rounded to FP32 (mixed path)
+    uint32_t* fixed = nullptr;  // [3][n] fractional coordinates as 32-bit fixed point
+    float2* stepz = nullptr;    // [n] e^{2 pi i s_z}
 };
 struct RecFlags {
     int with_q, with_mu;
     int field;     // E
     int grad;      // full field gradient (for EFG and dipole forces)
     int energy;    // energy + stress
+    int forces;    // forces q E + G mu
     int prec;      // MDFF_PREC_*
 };
 void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl,
-                      RecScratch& rs, double* ef, double* efg6, double* fo, Partials& part, DevScalars* d);
+                      RecScratch& rs, double* ef, double* efg6, double* fo, Partials& part, DevScalars* d,
+                      Prof* prof);
 size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart);
 
 // Solver vector kernels.

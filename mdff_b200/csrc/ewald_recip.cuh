@@ -250,6 +250,211 @@ __global__ void k_kfield_reduce(int n, int nsplit, int grad, const double* __res
     }
 }
 
+// ------------------------------------------------------------------------
+// Mixed-precision (FP32) variants.  The phase is exact: fractional
+// coordinates as 32-bit fixed point, so n.s mod 1 is an integer
+// multiply-add that wraps mod 2^32.  e^{2 pi i t} comes from FP32 sincospif of
+// the top 24 bits (exact in a float) with a first-order correction for the
+// low 8 bits (|delta| < 3.7e-7 rad).  FP32 partial sums are flushed into FP64
+// accumulators every tile of atoms (pass 1) or every 8 k-vectors (pass 2).
+
+__global__ void k_fixed_point(int n, const double* __restrict__ sx, const double* __restrict__ sy,
+                              const double* __restrict__ sz, uint32_t* __restrict__ fx, float2* __restrict__ stepz) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double s[3] = {sx[i], sy[i], sz[i]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double w = s[d] - floor(s[d]);
+        unsigned long long u = (unsigned long long)llrint(w * 4294967296.0);
+        fx[(size_t)d * n + i] = (uint32_t)(u & 0xffffffffull);
+    }
+    double sn, cs;
+    sincospi(2.0 * (s[2] - rint(s[2])), &sn, &cs);
+    stepz[i] = make_float2((float)cs, (float)sn);
+}
+
+__device__ __forceinline__ void phase32(uint32_t ph, float& cs, float& sn) {
+    const int p = (int)ph;
+    const float hi = (float)(p & ~0xff) * 4.656612873077393e-10f;   // 2^-31: sin(pi*hi) = sin(2 pi t)
+    sincospif(hi, &sn, &cs);
+    const float d = (float)(p & 0xff) * 1.4629180792671596e-09f;    // 2 pi 2^-32
+    const float c2 = fmaf(-sn, d, cs);
+    sn = fmaf(cs, d, sn);
+    cs = c2;
+}
+
+constexpr int SF32_TILE = 32;
+
+template <int CH>
+__global__ void __launch_bounds__(SF_THREADS) k_sfac32(int n, int natom_chunk, const uint32_t* __restrict__ fx,
+                                                       const float2* __restrict__ stepz, const double* __restrict__ q,
+                                                       const double* __restrict__ mu, CellP c, int kx, int ky, int kz,
+                                                       int ncol, int ncolblk, int nchunk, int with_q, int with_mu,
+                                                       double* __restrict__ part_re, double* __restrict__ part_im) {
+    __shared__ uint32_t t_u1[SF32_TILE], t_u2[SF32_TILE], t_u3[SF32_TILE];
+    __shared__ float t_q[SF32_TILE], t_m1[SF32_TILE], t_m2[SF32_TILE], t_m3[SF32_TILE], t_rc[SF32_TILE], t_rs[SF32_TILE];
+    const int h = blockIdx.x / ncolblk;
+    const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
+    const int p = blockIdx.y;
+    const int ny_n = 2 * ky + 1;
+    const int colc = col < ncol ? col : ncol - 1;
+    const int inx = colc / ny_n, iny = colc % ny_n - ky, inz0 = -kz + h * CH;
+    const float fnx = (float)inx, fny = (float)iny, fnz0 = (float)inz0;
+    double dre[CH], dim[CH];
+#pragma unroll
+    for (int m = 0; m < CH; ++m) { dre[m] = 0.0; dim[m] = 0.0; }
+    const int a0 = p * natom_chunk;
+    const int a1 = min(n, a0 + natom_chunk);
+    for (int base = a0; base < a1; base += SF32_TILE) {
+        __syncthreads();
+        if (threadIdx.x < SF32_TILE) {
+            int ia = base + threadIdx.x;
+            if (ia < a1) {
+                t_u1[threadIdx.x] = fx[ia];
+                t_u2[threadIdx.x] = fx[n + ia];
+                t_u3[threadIdx.x] = fx[2 * n + ia];
+                t_q[threadIdx.x] = with_q ? (float)q[ia] : 0.f;
+                double m0 = 0, m1 = 0, m2 = 0;
+                if (with_mu) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
+                t_m1[threadIdx.x] = (float)(2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2));
+                t_m2[threadIdx.x] = (float)(2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2));
+                t_m3[threadIdx.x] = (float)(2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2));
+                float2 st = stepz[ia];
+                t_rc[threadIdx.x] = st.x;
+                t_rs[threadIdx.x] = st.y;
+            }
+        }
+        __syncthreads();
+        const int tn = min(SF32_TILE, a1 - base);
+        float are[CH], aim[CH];
+#pragma unroll
+        for (int m = 0; m < CH; ++m) { are[m] = 0.f; aim[m] = 0.f; }
+        for (int t = 0; t < tn; ++t) {
+            const uint32_t ph = (uint32_t)inx * t_u1[t] + (uint32_t)iny * t_u2[t] + (uint32_t)inz0 * t_u3[t];
+            float cs, sn;
+            phase32(ph, cs, sn);
+            const float qa = t_q[t];
+            float km = fmaf(fnx, t_m1[t], fmaf(fny, t_m2[t], fnz0 * t_m3[t]));
+            const float dm = t_m3[t], rc = t_rc[t], rs = t_rs[t];
+#pragma unroll
+            for (int m = 0; m < CH; ++m) {
+                are[m] = fmaf(qa, cs, fmaf(-km, sn, are[m]));
+                aim[m] = fmaf(qa, sn, fmaf(km, cs, aim[m]));
+                const float cn = fmaf(cs, rc, -sn * rs);
+                sn = fmaf(sn, rc, cs * rs);
+                cs = cn;
+                km += dm;
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < CH; ++m) { dre[m] += (double)are[m]; dim[m] += (double)aim[m]; }
+    }
+    if (col < ncol) {
+        const size_t plane = (size_t)ncol * CH * nchunk;
+#pragma unroll
+        for (int m = 0; m < CH; ++m) {
+            size_t idx = (size_t)p * plane + ((size_t)h * CH + m) * ncol + col;
+            part_re[idx] = dre[m];
+            part_im[idx] = dim[m];
+        }
+    }
+}
+
+__global__ void k_aks32(int nrect, const double* __restrict__ aks, float* __restrict__ aks32) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 2 * nrect) aks32[t] = (float)aks[t];
+}
+
+constexpr int KF32_SUB = 8;
+
+template <int GRAD>
+__global__ void __launch_bounds__(KF_THREADS) k_kfield32(int n, const uint32_t* __restrict__ fx,
+                                                         const float2* __restrict__ stepz, CellP c, int kx, int ky,
+                                                         int kz, int ncol, int nzl, int cols_per_split,
+                                                         const float* __restrict__ aks, int nrect,
+                                                         double* __restrict__ fpart) {
+    extern __shared__ float smf[];
+    float* s_re = smf;
+    float* s_im = smf + KF_COLS * nzl;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int split = blockIdx.y;
+    const int c0 = split * cols_per_split;
+    const int c1 = min(ncol, c0 + cols_per_split);
+    const bool active = i < n;
+    const int ii = active ? i : 0;
+    const uint32_t u1 = fx[ii], u2 = fx[n + ii], u3 = fx[2 * n + ii];
+    const float2 st = stepz[ii];
+    const float rc = st.x, rs = st.y;
+    const float dk0 = (float)(2.0 * PI * c.B[2]), dk1 = (float)(2.0 * PI * c.B[5]), dk2 = (float)(2.0 * PI * c.B[8]);
+    const int ny_n = 2 * ky + 1;
+    double E0 = 0, E1 = 0, E2 = 0;
+    double G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
+    for (int cb = c0; cb < c1; cb += KF_COLS) {
+        const int nc = min(KF_COLS, c1 - cb);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nc * nzl; t += blockDim.x) {
+            s_re[t] = aks[(size_t)cb * nzl + t];
+            s_im[t] = aks[(size_t)nrect + (size_t)cb * nzl + t];
+        }
+        __syncthreads();
+        for (int cc = 0; cc < nc; ++cc) {
+            const int col = cb + cc;
+            const int inx = col / ny_n, iny = col % ny_n - ky;
+            const double bx = 2.0 * PI * (inx * c.B[0] + iny * c.B[1] - kz * c.B[2]);
+            const double by = 2.0 * PI * (inx * c.B[3] + iny * c.B[4] - kz * c.B[5]);
+            const double bz = 2.0 * PI * (inx * c.B[6] + iny * c.B[7] - kz * c.B[8]);
+            const float* pr = s_re + cc * nzl;
+            const float* pi = s_im + cc * nzl;
+            for (int m0 = 0; m0 < nzl; m0 += KF32_SUB) {
+                const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)(m0 - kz) * u3;
+                float cs, sn;
+                phase32(ph, cs, sn);
+                float k0 = (float)(bx + m0 * 2.0 * PI * c.B[2]);
+                float k1 = (float)(by + m0 * 2.0 * PI * c.B[5]);
+                float k2 = (float)(bz + m0 * 2.0 * PI * c.B[8]);
+                float e0 = 0.f, e1 = 0.f, e2 = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f, g3 = 0.f, g4 = 0.f, g5 = 0.f;
+                const int mend = min(KF32_SUB, nzl - m0);
+#pragma unroll
+                for (int mm = 0; mm < KF32_SUB; ++mm) {
+                    if (mm < mend) {
+                        const float ar = pr[m0 + mm], ai = pi[m0 + mm];
+                        const float recarg = fmaf(ai, cs, -ar * sn);
+                        e0 = fmaf(-k0, recarg, e0);
+                        e1 = fmaf(-k1, recarg, e1);
+                        e2 = fmaf(-k2, recarg, e2);
+                        if (GRAD) {
+                            const float r2 = fmaf(ar, cs, ai * sn);
+                            const float a0 = k0 * r2, a1 = k1 * r2;
+                            g0 = fmaf(k0, a0, g0);
+                            g1 = fmaf(k1, a1, g1);
+                            g2 = fmaf(k2, k2 * r2, g2);
+                            g3 = fmaf(k1, a0, g3);
+                            g4 = fmaf(k2, a0, g4);
+                            g5 = fmaf(k2, a1, g5);
+                        }
+                        const float cn = fmaf(cs, rc, -sn * rs);
+                        sn = fmaf(sn, rc, cs * rs);
+                        cs = cn;
+                        k0 += dk0; k1 += dk1; k2 += dk2;
+                    }
+                }
+                E0 += e0; E1 += e1; E2 += e2;
+                if (GRAD) { G0 += g0; G1 += g1; G2 += g2; G3 += g3; G4 += g4; G5 += g5; }
+            }
+        }
+    }
+    if (active) {
+        const int nv = GRAD ? 9 : 3;
+        double* o = fpart + (size_t)split * nv * n;
+        o[i] = E0; o[n + i] = E1; o[2 * n + i] = E2;
+        if (GRAD) {
+            o[3 * n + i] = G0; o[4 * n + i] = G1; o[5 * n + i] = G2;
+            o[6 * n + i] = G3; o[7 * n + i] = G4; o[8 * n + i] = G5;
+        }
+    }
+}
+
 struct RecLaunch {
     int CH, nchunk, ncolblk, P, natom_chunk, nsplit, cols_per_split;
 };
@@ -283,37 +488,64 @@ size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart) {
 
 void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl, RecScratch& rs,
-                      double* ef, double* efg, double* fo, Partials& part, DevScalars* d) {
+                      double* ef, double* efg, double* fo, Partials& part, DevScalars* d, Prof* prof) {
     RecLaunch L = plan(n, kg);
     const size_t plane = (size_t)L.P * L.nchunk * L.CH * kg.ncol;
     double* pre = rs.part;
     double* pim = rs.part + plane;
     dim3 g1(L.nchunk * L.ncolblk, L.P);
     const int kx = kg.kmax[0], ky = kg.kmax[1], kz = kg.kmax[2];
+    const bool mixed = fl.prec == MDFF_PREC_MIXED;
+    prof->begin(PK_SFAC);
+    if (mixed) {
+        k_fixed_point<<<(n + 255) / 256, 256, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.stepz);
+#define SFAC32(CHV) k_sfac32<CHV><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.stepz, q, mu, c, kx, ky, kz, \
+                                                         kg.ncol, L.ncolblk, L.nchunk, fl.with_q, fl.with_mu, pre, pim)
+        if (L.CH == 16) SFAC32(16);
+        else if (L.CH == 12) SFAC32(12);
+        else SFAC32(8);
+#undef SFAC32
+    } else {
 #define SFAC(CHV) k_sfac<CHV><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, sx, sy, sz, q, mu, c, kx, ky, kz, kg.ncol, \
                                                      L.ncolblk, L.nchunk, fl.with_q, fl.with_mu, pre, pim)
-    if (L.CH == 16) SFAC(16);
-    else if (L.CH == 12) SFAC(12);
-    else SFAC(8);
+        if (L.CH == 16) SFAC(16);
+        else if (L.CH == 12) SFAC(12);
+        else SFAC(8);
 #undef SFAC
+    }
     const int total = kg.ncol * kg.nzl;
     const int rb = (total + 255) / 256;
     k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, L.CH, L.nchunk, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak, kg.kcoe, c,
                                       rs.aks, kg.nrect, fl.energy, part.buf);
     if (fl.energy) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
-    if (!fl.field && !fl.grad) return;
+    prof->end((mixed ? 3 : 2) + (fl.energy ? 1 : 0));
+    if (!fl.field && !fl.grad && !fl.forces) return;
+    prof->begin(PK_KFIELD);
     dim3 g2((n + KF_THREADS - 1) / KF_THREADS, L.nsplit);
+    const bool grad = fl.grad || (fl.forces && fl.with_mu);
+    if (mixed) {
+        k_aks32<<<(2 * kg.nrect + 255) / 256, 256, 0, st>>>(kg.nrect, rs.aks, rs.aks32);
+        size_t smem32 = sizeof(float) * 2 * KF_COLS * kg.nzl;
+        if (grad)
+            k_kfield32<1><<<g2, KF_THREADS, smem32, st>>>(n, rs.fixed, rs.stepz, c, kx, ky, kz, kg.ncol, kg.nzl,
+                                                          L.cols_per_split, rs.aks32, kg.nrect, rs.fpart);
+        else
+            k_kfield32<0><<<g2, KF_THREADS, smem32, st>>>(n, rs.fixed, rs.stepz, c, kx, ky, kz, kg.ncol, kg.nzl,
+                                                          L.cols_per_split, rs.aks32, kg.nrect, rs.fpart);
+    } else {
     size_t smem = sizeof(double) * 2 * KF_COLS * kg.nzl;
-    if (fl.grad)
+    if (grad)
         k_kfield<1><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
                                                   rs.aks, kg.nrect, rs.fpart);
     else
         k_kfield<0><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
                                                   rs.aks, kg.nrect, rs.fpart);
+    }
     const double scale = 2.0 * 4.0 * PI / c.omega;
-    k_kfield_reduce<<<(n + 255) / 256, 256, 0, st>>>(n, L.nsplit, fl.grad, rs.fpart, scale, fl.with_q ? q : nullptr,
+    k_kfield_reduce<<<(n + 255) / 256, 256, 0, st>>>(n, L.nsplit, grad ? 1 : 0, rs.fpart, scale, fl.with_q ? q : nullptr,
                                                     fl.with_mu ? mu : nullptr, fl.field ? ef : nullptr, efg,
-                                                    fo);
+                                                    fl.forces ? fo : nullptr);
+    prof->end(mixed ? 3 : 2);
 }
 
 }  // namespace mdff

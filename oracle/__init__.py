@@ -46,6 +46,8 @@ def lib():
         L.orc_nlist_get.argtypes = [C.c_void_p, C.c_int, ip, ip, C.c_int, ip]
         L.orc_engforce.argtypes = [C.c_void_p, dp, dp, dp, C.POINTER(abi.Energies), dp, dp, dp, dp, dp]
         L.orc_coulomb_field.argtypes = [C.c_void_p, dp, dp, C.c_int, dp, dp, dp]
+        L.orc_field_time.argtypes = [C.c_void_p, C.c_int, dp, dp, dp]
+        L.orc_max_threads.restype = C.c_int
         L.orc_md_start.argtypes = [C.c_void_p, dp, dp, dp, C.POINTER(abi.Thermo)]
         L.orc_step.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
         _lib = L
@@ -58,6 +60,10 @@ def _dp(a):
 
 def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+
+
+def max_threads():
+    return lib().orc_max_threads()
 
 
 def set_threads(n):
@@ -160,6 +166,13 @@ class Oracle:
         u = C.c_double()
         lib().orc_coulomb_field(self._h, _dp(q), _dp(m), int(damp), _dp(ef), _dp(efg), C.byref(u))
         return ef.reshape(3, n).T.copy(), efg.reshape(6, n).T.copy(), u.value
+
+    def field_time(self, kstride=1):
+        """Seconds of one Ewald field evaluation (real space, reciprocal space
+        over every kstride-th k-vector) and one short-range pair loop."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        lib().orc_field_time(self._h, int(kstride), C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
 
     def md_start(self, vel):
         vel = np.asarray(vel, dtype=np.float64)

@@ -1477,6 +1477,50 @@ int orc_coulomb_field(orc_sys* s, const double* q, const double* mu, int damp, d
     return 0;
 }
 
+// Wall time of one Ewald field evaluation of the reference path on the host
+// cores (CPU baseline): multipole_ES_dir over the Coulomb list and
+// multipole_ES_rec over every kstride-th k-vector (the caller scales the
+// reciprocal time by kstride), with the current dipoles; plus one BMHFTD /
+// LJ pair loop.
+int orc_field_time(orc_sys* s, int kstride, double* t_dir, double* t_rec, double* t_pair) {
+    int n = s->natm;
+    std::vector<double> mu(3 * (size_t)n, 0.0);
+    for (int i = 0; i < n; ++i) mu[i] = 0.01 * (i % 7);
+    std::vector<double> ef(3 * (size_t)n, 0.0), efg(9 * (size_t)n, 0.0), f(3 * (size_t)n, 0.0);
+    bool task[6] = {true, true, true, false, false, false};
+    double tau[3][3] = {{0}}, u = 0.0;
+    auto now = []() {
+#ifdef _OPENMP
+        return omp_get_wtime();
+#else
+        return 0.0;
+#endif
+    };
+    double t0 = now();
+    multipole_ES_dir(s, s->qia, mu, task, true, true, false, false, false, u, ef, efg, f, tau);
+    double t1 = now();
+    KMesh full = s->km;
+    KMesh sub;
+    for (int k = 0; k < full.nk; k += kstride) {
+        sub.kx.push_back(full.kx[k]); sub.ky.push_back(full.ky[k]); sub.kz.push_back(full.kz[k]);
+        sub.kk.push_back(full.kk[k]); sub.Ak.push_back(full.Ak[k]); sub.kcoe.push_back(full.kcoe[k]);
+    }
+    sub.nk = (int)sub.kx.size();
+    s->km = sub;
+    multipole_ES_rec(s, s->qia, mu, task, true, false, false, false, u, ef, efg, f, tau);
+    s->km = full;
+    double t2 = now();
+    std::vector<double> sx, sy, sz;
+    direct_coords(s, sx, sy, sz);
+    if (s->p.lbmhftd || s->p.lbmhft) engforce_bmhftd(s, sx, sy, sz);
+    else if (s->p.lnmlj) engforce_nmlj(s, sx, sy, sz);
+    double t3 = now();
+    *t_dir = t1 - t0;
+    *t_rec = t2 - t1;
+    *t_pair = t3 - t2;
+    return 0;
+}
+
 int orc_md_start(orc_sys* s, const double* vx, const double* vy, const double* vz, mdff_thermo* t0) {
     std::memcpy(s->vx.data(), vx, sizeof(double) * s->natm);
     std::memcpy(s->vy.data(), vy, sizeof(double) * s->natm);

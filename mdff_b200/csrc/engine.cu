@@ -595,6 +595,7 @@ int engforce_device(mdff_ctx* ctx) {
     ctx->prof.begin(PK_OTHER);
     launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
     ctx->prof.end(1);
+    ctx->rs.want_epoch++;   // positions may have changed: rebuild the phase tables
     std::memset(&ctx->en, 0, sizeof ctx->en);
     bool nonb = p.lnmlj || p.lbmhft || p.lbmhftd || p.lmorse;
     if (nonb) {
@@ -1127,6 +1128,8 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
         TRY(dalloc(ctx, &ctx->rs.aks32, 2 * (size_t)kg.nrect));
         TRY(dalloc(ctx, &ctx->rs.fixed, 3 * (size_t)n));
         TRY(dalloc(ctx, &ctx->rs.stepz, (size_t)n));
+        TRY(dalloc(ctx, &ctx->rs.tab, (size_t)n * 16));
+        TRY(dalloc(ctx, &ctx->rs.aks2, (size_t)kg.ncol * (((kg.nzl + 15) / 16) * 16)));
         ctx->rs.part_cap = pc;
         ctx->rs.fpart_cap = fp;
     }

@@ -197,6 +197,10 @@ struct RecScratch {
     float* aks32 = nullptr;     // [2][nrect] Ak*S rounded to FP32 (mixed path)
     uint32_t* fixed = nullptr;  // [3][n] fractional coordinates as 32-bit fixed point
     float2* stepz = nullptr;    // [n] e^{2 pi i s_z}
+    float2* tab = nullptr;      // [n][16] e^{2 pi i m s_z}
+    float2* aks2 = nullptr;     // [ncol][nzp] A_k S(k) padded, FP32
+    long tab_epoch = -1;        // position epoch the table was built for
+    long want_epoch = 0;        // current position epoch (set by the engine)
 };
 struct RecFlags {
     int with_q, with_mu;

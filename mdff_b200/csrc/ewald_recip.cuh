@@ -455,6 +455,212 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32(int n, const uint32_t* 
     }
 }
 
+// ---- second-generation FP32 kernels --------------------------------------
+// e^{ik.r} = e0 * T_m with T_m = e^{2 pi i m s_z} (m = 0..15) tabulated per atom
+// once per position update from FP64, so the error does not grow along nz.
+constexpr int TM = 16;     // table length = nz chunk of both passes
+
+// Per-atom phase table T_m, fixed-point coordinates.
+__global__ void k_phase_table(int n, const double* __restrict__ sx, const double* __restrict__ sy,
+                              const double* __restrict__ sz, uint32_t* __restrict__ fx, float2* __restrict__ tab) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double s[3] = {sx[i], sy[i], sz[i]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double w = s[d] - floor(s[d]);
+        unsigned long long u = (unsigned long long)llrint(w * 4294967296.0);
+        fx[(size_t)d * n + i] = (uint32_t)(u & 0xffffffffull);
+    }
+    const double z = s[2] - rint(s[2]);
+#pragma unroll 4
+    for (int m = 0; m < TM; ++m) {
+        double t = m * z;
+        t -= rint(t);
+        double sn, cs;
+        sincospi(2.0 * t, &sn, &cs);
+        tab[(size_t)i * TM + m] = make_float2((float)cs, (float)sn);
+    }
+}
+
+constexpr int SF2_TILE = 32;
+
+// Pass 1: thread = (column, chunk of TM nz).  Contribution of atom t to the
+// chunk: sum_m (w0 + m dw) T_m with w0 = (q + i k0.mu) e0, dw = i (2 pi b3.mu) e0.
+__global__ void __launch_bounds__(SF_THREADS) k_sfac32v2(int n, int natom_chunk, const uint32_t* __restrict__ fx,
+                                                         const float2* __restrict__ tab, const double* __restrict__ q,
+                                                         const double* __restrict__ mu, CellP c, int kx, int ky, int kz,
+                                                         int ncol, int ncolblk, int nchunk, int with_q, int with_mu,
+                                                         double* __restrict__ part_re, double* __restrict__ part_im) {
+    __shared__ uint32_t t_u1[SF2_TILE], t_u2[SF2_TILE], t_u3[SF2_TILE];
+    __shared__ float t_q[SF2_TILE], t_m1[SF2_TILE], t_m2[SF2_TILE], t_m3[SF2_TILE];
+    __shared__ float2 t_tab[SF2_TILE][TM];
+    const int h = blockIdx.x / ncolblk;
+    const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
+    const int p = blockIdx.y;
+    const int ny_n = 2 * ky + 1;
+    const int colc = col < ncol ? col : ncol - 1;
+    const int inx = colc / ny_n, iny = colc % ny_n - ky, inz0 = -kz + h * TM;
+    const float fnx = (float)inx, fny = (float)iny, fnz0 = (float)inz0;
+    double dre[TM], dim[TM];
+#pragma unroll
+    for (int m = 0; m < TM; ++m) { dre[m] = 0.0; dim[m] = 0.0; }
+    const int a0 = p * natom_chunk;
+    const int a1 = min(n, a0 + natom_chunk);
+    for (int base = a0; base < a1; base += SF2_TILE) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < SF2_TILE * TM; t += blockDim.x) {
+            int ia = base + t / TM;
+            if (ia < a1) t_tab[t / TM][t % TM] = tab[(size_t)ia * TM + (t % TM)];
+        }
+        if (threadIdx.x < SF2_TILE) {
+            int ia = base + threadIdx.x;
+            if (ia < a1) {
+                t_u1[threadIdx.x] = fx[ia];
+                t_u2[threadIdx.x] = fx[n + ia];
+                t_u3[threadIdx.x] = fx[2 * n + ia];
+                t_q[threadIdx.x] = with_q ? (float)q[ia] : 0.f;
+                double m0 = 0, m1 = 0, m2 = 0;
+                if (with_mu) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
+                t_m1[threadIdx.x] = (float)(2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2));
+                t_m2[threadIdx.x] = (float)(2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2));
+                t_m3[threadIdx.x] = (float)(2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2));
+            }
+        }
+        __syncthreads();
+        const int tn = min(SF2_TILE, a1 - base);
+        float are[TM], aim[TM];
+#pragma unroll
+        for (int m = 0; m < TM; ++m) { are[m] = 0.f; aim[m] = 0.f; }
+        for (int t = 0; t < tn; ++t) {
+            const uint32_t ph = (uint32_t)inx * t_u1[t] + (uint32_t)iny * t_u2[t] + (uint32_t)inz0 * t_u3[t];
+            float c0, s0;
+            phase32(ph, c0, s0);
+            const float qa = t_q[t];
+            const float km = fmaf(fnx, t_m1[t], fmaf(fny, t_m2[t], fnz0 * t_m3[t]));
+            const float m3 = t_m3[t];
+            const float w0r = fmaf(qa, c0, -km * s0), w0i = fmaf(qa, s0, km * c0);
+            const float dwr = -m3 * s0, dwi = m3 * c0;
+#pragma unroll
+            for (int m = 0; m < TM; ++m) {
+                const float wr = fmaf((float)m, dwr, w0r), wi = fmaf((float)m, dwi, w0i);
+                const float2 T = t_tab[t][m];
+                are[m] = fmaf(wr, T.x, fmaf(-wi, T.y, are[m]));
+                aim[m] = fmaf(wr, T.y, fmaf(wi, T.x, aim[m]));
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < TM; ++m) { dre[m] += (double)are[m]; dim[m] += (double)aim[m]; }
+    }
+    if (col < ncol) {
+        const size_t plane = (size_t)ncol * TM * nchunk;
+#pragma unroll
+        for (int m = 0; m < TM; ++m) {
+            size_t idx = (size_t)p * plane + ((size_t)h * TM + m) * ncol + col;
+            part_re[idx] = dre[m];
+            part_im[idx] = dim[m];
+        }
+    }
+}
+
+// A_k S(k) as float2, each column padded to nzp (a multiple of TM) with zeros.
+__global__ void k_aks32_pad(int ncol, int nzl, int nzp, int nrect, const double* __restrict__ aks,
+                            float2* __restrict__ out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ncol * nzp) return;
+    int col = t / nzp, m = t % nzp;
+    float2 v = make_float2(0.f, 0.f);
+    if (m < nzl) {
+        size_t r = (size_t)col * nzl + m;
+        v = make_float2((float)aks[r], (float)aks[nrect + r]);
+    }
+    out[t] = v;
+}
+
+// Pass 2: thread = atom.  Along a chunk of TM k-vectors k_m = kb + m dk, so
+// sum_m k_m r_m = kb R0 + dk R1 with R0 = sum r_m, R1 = sum m r_m (and the
+// second moment for the field gradient): the k-vector is applied once per chunk.
+template <int GRAD>
+__global__ void __launch_bounds__(KF_THREADS) k_kfield32v2(int n, const uint32_t* __restrict__ fx,
+                                                           const float2* __restrict__ tab, CellP c, int kx, int ky,
+                                                           int kz, int ncol, int nzp, int cols_per_split,
+                                                           const float2* __restrict__ aks, double* __restrict__ fpart) {
+    extern __shared__ float2 sm2[];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int split = blockIdx.y;
+    const int c0 = split * cols_per_split;
+    const int c1 = min(ncol, c0 + cols_per_split);
+    const bool active = i < n;
+    const int ii = active ? i : 0;
+    const uint32_t u1 = fx[ii], u2 = fx[n + ii], u3 = fx[2 * n + ii];
+    float2 T[TM];
+#pragma unroll
+    for (int m = 0; m < TM; ++m) T[m] = tab[(size_t)ii * TM + m];
+    const double dkx = 2.0 * PI * c.B[2], dky = 2.0 * PI * c.B[5], dkz = 2.0 * PI * c.B[8];
+    const float dk0 = (float)dkx, dk1 = (float)dky, dk2 = (float)dkz;
+    const int ny_n = 2 * ky + 1;
+    double E0 = 0, E1 = 0, E2 = 0;
+    double G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
+    for (int cb = c0; cb < c1; cb += KF_COLS) {
+        const int nc = min(KF_COLS, c1 - cb);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nc * nzp; t += blockDim.x) sm2[t] = aks[(size_t)cb * nzp + t];
+        __syncthreads();
+        for (int cc = 0; cc < nc; ++cc) {
+            const int col = cb + cc;
+            const int inx = col / ny_n, iny = col % ny_n - ky;
+            const double bx = 2.0 * PI * (inx * c.B[0] + iny * c.B[1]);
+            const double by = 2.0 * PI * (inx * c.B[3] + iny * c.B[4]);
+            const double bz = 2.0 * PI * (inx * c.B[6] + iny * c.B[7]);
+            const float2* pk = sm2 + cc * nzp;
+            for (int m0 = 0; m0 < nzp; m0 += TM) {
+                const int nzb = m0 - kz;
+                const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)nzb * u3;
+                float ec, es;
+                phase32(ph, ec, es);
+                float R0 = 0.f, R1 = 0.f, Q0 = 0.f, Q1 = 0.f, Q2 = 0.f;
+#pragma unroll
+                for (int m = 0; m < TM; ++m) {
+                    const float cs = fmaf(ec, T[m].x, -es * T[m].y);
+                    const float sn = fmaf(es, T[m].x, ec * T[m].y);
+                    const float2 a = pk[m0 + m];
+                    const float r = fmaf(a.y, cs, -a.x * sn);
+                    R0 += r;
+                    R1 = fmaf((float)m, r, R1);
+                    if (GRAD) {
+                        const float r2 = fmaf(a.x, cs, a.y * sn);
+                        Q0 += r2;
+                        Q1 = fmaf((float)m, r2, Q1);
+                        Q2 = fmaf((float)(m * m), r2, Q2);
+                    }
+                }
+                const float kb0 = (float)(bx + nzb * dkx), kb1 = (float)(by + nzb * dky), kb2 = (float)(bz + nzb * dkz);
+                E0 -= (double)fmaf(kb0, R0, dk0 * R1);
+                E1 -= (double)fmaf(kb1, R0, dk1 * R1);
+                E2 -= (double)fmaf(kb2, R0, dk2 * R1);
+                if (GRAD) {
+                    // sum_m (kb + m dk)_a (kb + m dk)_b r2_m
+                    G0 += (double)(kb0 * kb0 * Q0 + 2.f * kb0 * dk0 * Q1 + dk0 * dk0 * Q2);
+                    G1 += (double)(kb1 * kb1 * Q0 + 2.f * kb1 * dk1 * Q1 + dk1 * dk1 * Q2);
+                    G2 += (double)(kb2 * kb2 * Q0 + 2.f * kb2 * dk2 * Q1 + dk2 * dk2 * Q2);
+                    G3 += (double)(kb0 * kb1 * Q0 + (kb0 * dk1 + dk0 * kb1) * Q1 + dk0 * dk1 * Q2);
+                    G4 += (double)(kb0 * kb2 * Q0 + (kb0 * dk2 + dk0 * kb2) * Q1 + dk0 * dk2 * Q2);
+                    G5 += (double)(kb1 * kb2 * Q0 + (kb1 * dk2 + dk1 * kb2) * Q1 + dk1 * dk2 * Q2);
+                }
+            }
+        }
+    }
+    if (active) {
+        const int nv = GRAD ? 9 : 3;
+        double* o = fpart + (size_t)split * nv * n;
+        o[i] = E0; o[n + i] = E1; o[2 * n + i] = E2;
+        if (GRAD) {
+            o[3 * n + i] = G0; o[4 * n + i] = G1; o[5 * n + i] = G2;
+            o[6 * n + i] = G3; o[7 * n + i] = G4; o[8 * n + i] = G5;
+        }
+    }
+}
+
 struct RecLaunch {
     int CH, nchunk, ncolblk, P, natom_chunk, nsplit, cols_per_split;
 };
@@ -483,7 +689,8 @@ static RecLaunch plan(int n, const KGrid& kg) {
 size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart) {
     RecLaunch L = plan(n, kg);
     *fpart = (size_t)L.nsplit * 9 * n;
-    return (size_t)L.P * L.nchunk * L.CH * kg.ncol * 2;
+    size_t rows = std::max((size_t)L.nchunk * L.CH, (size_t)((kg.nzl + TM - 1) / TM) * TM);
+    return (size_t)L.P * rows * kg.ncol * 2;
 }
 
 void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
@@ -494,17 +701,19 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     double* pre = rs.part;
     double* pim = rs.part + plane;
     dim3 g1(L.nchunk * L.ncolblk, L.P);
+    RecLaunch L2 = L;
+    L2.nchunk = (kg.nzl + TM - 1) / TM;
+    dim3 g1v2(L2.nchunk * L.ncolblk, L.P);
     const int kx = kg.kmax[0], ky = kg.kmax[1], kz = kg.kmax[2];
     const bool mixed = fl.prec == MDFF_PREC_MIXED;
     prof->begin(PK_SFAC);
     if (mixed) {
-        k_fixed_point<<<(n + 255) / 256, 256, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.stepz);
-#define SFAC32(CHV) k_sfac32<CHV><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.stepz, q, mu, c, kx, ky, kz, \
-                                                         kg.ncol, L.ncolblk, L.nchunk, fl.with_q, fl.with_mu, pre, pim)
-        if (L.CH == 16) SFAC32(16);
-        else if (L.CH == 12) SFAC32(12);
-        else SFAC32(8);
-#undef SFAC32
+        if (rs.tab_epoch != rs.want_epoch) {
+            k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab);
+            rs.tab_epoch = rs.want_epoch;
+        }
+        k_sfac32v2<<<g1v2, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
+                                               L.ncolblk, L2.nchunk, fl.with_q, fl.with_mu, pre, pim);
     } else {
 #define SFAC(CHV) k_sfac<CHV><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, sx, sy, sz, q, mu, c, kx, ky, kz, kg.ncol, \
                                                      L.ncolblk, L.nchunk, fl.with_q, fl.with_mu, pre, pim)
@@ -515,23 +724,24 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     }
     const int total = kg.ncol * kg.nzl;
     const int rb = (total + 255) / 256;
-    k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, L.CH, L.nchunk, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak, kg.kcoe, c,
+    k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, mixed ? TM : L.CH, mixed ? L2.nchunk : L.nchunk, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak, kg.kcoe, c,
                                       rs.aks, kg.nrect, fl.energy, part.buf);
     if (fl.energy) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
-    prof->end((mixed ? 3 : 2) + (fl.energy ? 1 : 0));
+    prof->end(2 + (fl.energy ? 1 : 0));
     if (!fl.field && !fl.grad && !fl.forces) return;
     prof->begin(PK_KFIELD);
     dim3 g2((n + KF_THREADS - 1) / KF_THREADS, L.nsplit);
     const bool grad = fl.grad || (fl.forces && fl.with_mu);
     if (mixed) {
-        k_aks32<<<(2 * kg.nrect + 255) / 256, 256, 0, st>>>(kg.nrect, rs.aks, rs.aks32);
-        size_t smem32 = sizeof(float) * 2 * KF_COLS * kg.nzl;
+        const int nzp = ((kg.nzl + TM - 1) / TM) * TM;
+        k_aks32_pad<<<(kg.ncol * nzp + 255) / 256, 256, 0, st>>>(kg.ncol, kg.nzl, nzp, kg.nrect, rs.aks, rs.aks2);
+        size_t smem2 = sizeof(float2) * KF_COLS * nzp;
         if (grad)
-            k_kfield32<1><<<g2, KF_THREADS, smem32, st>>>(n, rs.fixed, rs.stepz, c, kx, ky, kz, kg.ncol, kg.nzl,
-                                                          L.cols_per_split, rs.aks32, kg.nrect, rs.fpart);
+            k_kfield32v2<1><<<g2, KF_THREADS, smem2, st>>>(n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp,
+                                                           L.cols_per_split, rs.aks2, rs.fpart);
         else
-            k_kfield32<0><<<g2, KF_THREADS, smem32, st>>>(n, rs.fixed, rs.stepz, c, kx, ky, kz, kg.ncol, kg.nzl,
-                                                          L.cols_per_split, rs.aks32, kg.nrect, rs.fpart);
+            k_kfield32v2<0><<<g2, KF_THREADS, smem2, st>>>(n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp,
+                                                           L.cols_per_split, rs.aks2, rs.fpart);
     } else {
     size_t smem = sizeof(double) * 2 * KF_COLS * kg.nzl;
     if (grad)

@@ -41,6 +41,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ncell", type=int, default=16)
+    ap.add_argument("--accuracy", action="store_true",
+                    help="error of the mixed path against the FP64 path on snapshots of an FP64 trajectory")
+    ap.add_argument("--snapshots", type=int, default=3)
+    ap.add_argument("--snap-every", type=int, default=100)
     return ap.parse_args()
 
 
@@ -268,6 +272,55 @@ def cpu_baseline(s, p, iters_per_step, kstride=16):
             "seconds": {"dir": td, "rec_sampled": tr, "pair": tp}}
 
 
+def run_accuracy(args):
+    """Error of each mixed-precision result against the FP64 path at identical
+    positions: snapshots every --snap-every steps of an FP64 NVT trajectory of
+    the production cell.  Global relative norms ||x_mixed - x_fp64|| / ||x_fp64||
+    for forces, dipoles, EFG, stresses; energies relative; also the per-atom
+    maximum force deviation relative to the RMS force."""
+    import torch
+    import mdff_b200
+    from mdff_b200 import abi, systems
+    s = systems.mgo_production(ncell=args.ncell)
+    p = s["params"]
+    p.precision = abi.PREC_FP64
+    traj = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+    traj.md_start(s["vel"])
+    pm = abi.Params()
+    C.pointer(pm)[0] = p
+    pm.precision = abi.PREC_MIXED
+    pf = abi.Params()
+    C.pointer(pf)[0] = p
+    snaps = []
+    for k in range(args.snapshots + 1):
+        if k > 0:
+            traj.step(args.snap_every, thermo=False)
+        pos = traj.positions()
+        res = {}
+        for name, pp in (("fp64", pf), ("mixed", pm)):
+            e = mdff_b200.Engine(pp, s["itype"], pos, s["cell"])
+            res[name] = e.engforce()
+            e.close()
+        a, b = res["mixed"], res["fp64"]
+        rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+        df = np.linalg.norm(a["f"] - b["f"], axis=1)
+        snaps.append({
+            "step": k * args.snap_every,
+            "eps_F": rel(a["f"], b["f"]),
+            "max_atom_dF_over_rms_F": float(df.max() / np.sqrt((b["f"] ** 2).sum(1).mean())),
+            "rms_F_eV_per_A": float(np.sqrt((b["f"] ** 2).sum(1).mean())),
+            "eps_mu": rel(a["mu"], b["mu"]),
+            "eps_efg": rel(a["efg"], b["efg"]),
+            "eps_tau_coul": rel(a["tau_coul"], b["tau_coul"]),
+            "rel_u_coul": abs(a["e"]["u_coul"] - b["e"]["u_coul"]) / abs(b["e"]["u_coul"]),
+            "rel_u_bmhft": abs(a["e"]["u_bmhft"] - b["e"]["u_bmhft"]) / abs(b["e"]["u_bmhft"]),
+            "du_per_atom_eV": abs(a["e"]["u_coul"] - b["e"]["u_coul"]) / len(pos),
+            "iters": [a["e"]["scf_iter"], b["e"]["scf_iter"]],
+        })
+    return {"mode": "accuracy", "workload": "mgo-pim-production", "natm": len(s["itype"]), "snapshots": snaps,
+            "eps_F_max": max(x["eps_F"] for x in snaps)}
+
+
 def run_reference(args):
     """Reference arm: the CPU oracle (C++ port of the reference's FP64 path;
     the Fortran/MPI reference cannot be built on this image) on all host cores,
@@ -330,7 +383,9 @@ def run_reference(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.accuracy:
+        r = run_accuracy(args)
+    elif args.impl == "reference":
         r = run_reference(args)
     else:
         r = run_engine(args)

@@ -130,6 +130,7 @@ typedef struct mdff_params {
     int    device;                             /* CUDA device ordinal */
     int    erfc_ref;                           /* 1: the reference's fitted erfc (src/functions.f90:28-39) */
     int    nhc_literal;                        /* 1: chain_nhcn's literal force order (stale G(2..M-1)) */
+    double mixed_ksplit;                       /* mixed path: |k| < mixed_ksplit*alpha summed in FP64 (0: none) */
 } mdff_params;
 
 /* Energies and scalar outputs of one force evaluation (thermodynamic module

@@ -54,7 +54,7 @@ class Params(C.Structure):
         ("nhc_n", C.c_int), ("nhc_yosh_order", C.c_int), ("nhc_mults", C.c_int),
         ("timesca_thermo", C.c_double),
         ("precision", C.c_int), ("efg_period", C.c_int), ("nlist_capacity", C.c_int), ("device", C.c_int),
-        ("erfc_ref", C.c_int), ("nhc_literal", C.c_int),
+        ("erfc_ref", C.c_int), ("nhc_literal", C.c_int), ("mixed_ksplit", C.c_double),
     ]
 
 
@@ -123,4 +123,5 @@ def default_params():
     p.efg_period = 0
     p.nlist_capacity = 0
     p.device = 0
+    p.mixed_ksplit = 3.4
     return p

@@ -967,6 +967,7 @@ void mdff_params_default(mdff_params* p) {
     p->nhc_mults = 2;
     p->timesca_thermo = 1.0;
     p->precision = MDFF_PREC_FP64;
+    p->mixed_ksplit = 3.4;
 }
 
 int mdff_create(const mdff_params* p, mdff_ctx** out) {
@@ -1120,14 +1121,82 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
         TRY(dalloc(ctx, &kg.kcoe, kg.nrect));
         TRY(upload(ctx, kg.Ak, ak.data(), kg.nrect));
         TRY(upload(ctx, kg.kcoe, kc.data(), kg.nrect));
+        // Mixed path: the k-vectors with |k| < mixed_ksplit * alpha form the
+        // FP64 low set (one contiguous nz interval per column, |k|^2 being
+        // convex in nz) and are removed from the FP32 set.
+        ctx->rs.low = LowK();
+        if (p.precision == MDFF_PREC_MIXED && p.mixed_ksplit > 0.0) {
+            const double ks2 = std::pow(p.mixed_ksplit * ctx->alphaES, 2);
+            std::vector<int> cols;
+            std::vector<double> akl, kcl;
+            std::vector<double> akhi = ak;
+            int nzmax = 0;
+            struct Col { int nx, ny, lo, nn; };
+            std::vector<Col> cl;
+            for (int col = 0; col < kg.ncol; ++col) {
+                int nx = col / (2 * kg.kmax[1] + 1), ny = col % (2 * kg.kmax[1] + 1) - kg.kmax[1];
+                int lo = -1, hi = -2;
+                for (int m = 0; m < kg.nzl; ++m) {
+                    size_t r = (size_t)col * kg.nzl + m;
+                    if (ak[r] == 0.0) continue;
+                    int nz = m - kg.kmax[2];
+                    double kx = 2.0 * PI * (double(nx) * c.B[0] + double(ny) * c.B[1] + double(nz) * c.B[2]);
+                    double ky = 2.0 * PI * (double(nx) * c.B[3] + double(ny) * c.B[4] + double(nz) * c.B[5]);
+                    double kz = 2.0 * PI * (double(nx) * c.B[6] + double(ny) * c.B[7] + double(nz) * c.B[8]);
+                    if (kx * kx + ky * ky + kz * kz < ks2) {
+                        if (lo < 0) lo = m;
+                        hi = m;
+                    }
+                }
+                if (lo < 0) continue;
+                cl.push_back({nx, ny, lo, hi - lo + 1});
+                nzmax = std::max(nzmax, hi - lo + 1);
+            }
+            LowK& lk = ctx->rs.low;
+            lk.ncol = (int)cl.size();
+            lk.nzmax = nzmax;
+            if (lk.ncol > 0) {
+                cols.resize(4 * (size_t)lk.ncol);
+                akl.assign((size_t)lk.ncol * nzmax, 0.0);
+                kcl.assign((size_t)lk.ncol * nzmax, 0.0);
+                for (int q = 0; q < lk.ncol; ++q) {
+                    const Col& C_ = cl[q];
+                    int col = C_.nx * (2 * kg.kmax[1] + 1) + (C_.ny + kg.kmax[1]);
+                    cols[4 * q] = C_.nx;
+                    cols[4 * q + 1] = C_.ny;
+                    cols[4 * q + 2] = C_.lo - kg.kmax[2];
+                    cols[4 * q + 3] = C_.nn;
+                    for (int m = 0; m < C_.nn; ++m) {
+                        size_t r = (size_t)col * kg.nzl + C_.lo + m;
+                        akl[(size_t)q * nzmax + m] = ak[r];
+                        kcl[(size_t)q * nzmax + m] = kc[r];
+                        akhi[r] = 0.0;
+                    }
+                }
+                long long thr = (long long)((lk.ncol + 127) / 128) * 128 * ((nzmax + 7) / 8);
+                int P = (int)std::max<long long>(1, (148LL * 1536 + thr - 1) / thr);
+                P = std::min(P, std::max(1, n / 32));
+                lk.natom_chunk = (n + P - 1) / P;
+                lk.P = (n + lk.natom_chunk - 1) / lk.natom_chunk;
+                TRY(dalloc(ctx, &lk.col, cols.size()));
+                CK(cudaMemcpyAsync(lk.col, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice, ctx->st));
+                TRY(dalloc(ctx, &lk.Ak, akl.size()));
+                TRY(dalloc(ctx, &lk.kcoe, kcl.size()));
+                TRY(upload(ctx, lk.Ak, akl.data(), (int)akl.size()));
+                TRY(upload(ctx, lk.kcoe, kcl.data(), (int)kcl.size()));
+                TRY(dalloc(ctx, &lk.part, 2 * (size_t)lk.P * nzmax * lk.ncol));
+                TRY(dalloc(ctx, &lk.aks, 2 * (size_t)lk.ncol * nzmax));
+                TRY(dalloc(ctx, &lk.fpart, 4 * 9 * (size_t)n));
+                TRY(dalloc(ctx, &kg.Ak_hi, kg.nrect));
+                TRY(upload(ctx, kg.Ak_hi, akhi.data(), kg.nrect));
+            }
+        }
         size_t fp = 0;
         size_t pc = rec_scratch_doubles(n, kg, &fp);
         TRY(dalloc(ctx, &ctx->rs.part, pc));
         TRY(dalloc(ctx, &ctx->rs.fpart, fp));
         TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));
-        TRY(dalloc(ctx, &ctx->rs.aks32, 2 * (size_t)kg.nrect));
         TRY(dalloc(ctx, &ctx->rs.fixed, 3 * (size_t)n));
-        TRY(dalloc(ctx, &ctx->rs.stepz, (size_t)n));
         TRY(dalloc(ctx, &ctx->rs.tab, (size_t)n * 16));
         TRY(dalloc(ctx, &ctx->rs.aks2, (size_t)kg.ncol * (((kg.nzl + 15) / 16) * 16)));
         ctx->rs.part_cap = pc;

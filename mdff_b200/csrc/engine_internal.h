@@ -187,20 +187,34 @@ struct KGrid {
     int nrect;           // ncol*nzl
     double* Ak = nullptr;      // [nrect], 0 for excluded k
     double* kcoe = nullptr;    // [nrect]
+    double* Ak_hi = nullptr;   // [nrect], Ak without the low-|k| set (mixed path)
 };
+// The low-|k| set of the mixed path, summed in FP64 (see ewald_recip.cuh):
+// columns (nx, ny) with a contiguous nz range [nzlo, nzlo + nzn).
+struct LowK {
+    int ncol = 0;          // columns in the list
+    int nzmax = 0;         // longest column
+    int* col = nullptr;    // [ncol][4]: nx, ny, nzlo, nzn
+    double* Ak = nullptr;  // [ncol][nzmax]
+    double* kcoe = nullptr;
+    double* part = nullptr;   // pass-1 partials [2][P][nzmax][ncol]
+    double* aks = nullptr;    // [2][ncol][nzmax]
+    double* fpart = nullptr;  // [9][n]
+    int P = 1, natom_chunk = 0;
+};
+
 struct RecScratch {
     double* part = nullptr;    // structure-factor partials
     size_t part_cap = 0;       // doubles
     double* aks = nullptr;     // [2][nrect] Ak*S (re, im)
     double* fpart = nullptr;   // per-atom field partials [split][9][n]
     size_t fpart_cap = 0;
-    float* aks32 = nullptr;     // [2][nrect] Ak*S rounded to FP32 (mixed path)
     uint32_t* fixed = nullptr;  // [3][n] fractional coordinates as 32-bit fixed point
-    float2* stepz = nullptr;    // [n] e^{2 pi i s_z}
     float2* tab = nullptr;      // [n][16] e^{2 pi i m s_z}
     float2* aks2 = nullptr;     // [ncol][nzp] A_k S(k) padded, FP32
     long tab_epoch = -1;        // position epoch the table was built for
     long want_epoch = 0;        // current position epoch (set by the engine)
+    LowK low;
 };
 struct RecFlags {
     int with_q, with_mu;

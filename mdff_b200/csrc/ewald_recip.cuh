@@ -226,13 +226,15 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield(int n, const double* __re
 // q E_rec + G_rec mu.
 __global__ void k_kfield_reduce(int n, int nsplit, int grad, const double* __restrict__ fpart, double scale,
                                 const double* __restrict__ q, const double* __restrict__ mu, double* ef,
-                                double* efg, double* fo) {
+                                double* efg, double* fo, const double* __restrict__ flow, int nlow) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int nv = grad ? 9 : 3;
     double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int s = 0; s < nsplit; ++s)
         for (int k = 0; k < nv; ++k) v[k] += fpart[((size_t)s * nv + k) * n + i];
+    for (int s = 0; s < nlow; ++s)
+        for (int k = 0; k < nv; ++k) v[k] += flow[((size_t)s * 9 + k) * n + i];
     for (int k = 0; k < nv; ++k) v[k] *= scale;
     if (ef) { ef[i] += v[0]; ef[n + i] += v[1]; ef[2 * n + i] += v[2]; }
     if (grad && efg)
@@ -251,28 +253,15 @@ __global__ void k_kfield_reduce(int n, int nsplit, int grad, const double* __res
 }
 
 // ------------------------------------------------------------------------
-// Mixed-precision (FP32) variants.  The phase is exact: fractional
-// coordinates as 32-bit fixed point, so n.s mod 1 is an integer
-// multiply-add that wraps mod 2^32.  e^{2 pi i t} comes from FP32 sincospif of
-// the top 24 bits (exact in a float) with a first-order correction for the
-// low 8 bits (|delta| < 3.7e-7 rad).  FP32 partial sums are flushed into FP64
-// accumulators every tile of atoms (pass 1) or every 8 k-vectors (pass 2).
-
-__global__ void k_fixed_point(int n, const double* __restrict__ sx, const double* __restrict__ sy,
-                              const double* __restrict__ sz, uint32_t* __restrict__ fx, float2* __restrict__ stepz) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double s[3] = {sx[i], sy[i], sz[i]};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        double w = s[d] - floor(s[d]);
-        unsigned long long u = (unsigned long long)llrint(w * 4294967296.0);
-        fx[(size_t)d * n + i] = (uint32_t)(u & 0xffffffffull);
-    }
-    double sn, cs;
-    sincospi(2.0 * (s[2] - rint(s[2])), &sn, &cs);
-    stepz[i] = make_float2((float)cs, (float)sn);
-}
+// Mixed-precision (FP32) kernels.  The phase is exact: fractional coordinates
+// as 32-bit fixed point, so n.s mod 1 is an integer multiply-add that wraps
+// mod 2^32.  e^{2 pi i t} comes from FP32 sincospif of the top 24 bits (exact
+// in a float) with a first-order correction for the low 8 bits
+// (|delta| < 3.7e-7 rad); further nz use a per-atom table T_m = e^{2 pi i m s_z}
+// built in FP64, so errors do not grow along a column.  The inner loops run on
+// packed pairs (fma.rn.f32x2, sm_100): the complex multiply-accumulates are two
+// packed FMAs each.  FP32 partial sums are flushed to FP64 every tile of atoms
+// (pass 1) or every chunk of 16 k-vectors (pass 2).
 
 __device__ __forceinline__ void phase32(uint32_t ph, float& cs, float& sn) {
     const int p = (int)ph;
@@ -282,177 +271,6 @@ __device__ __forceinline__ void phase32(uint32_t ph, float& cs, float& sn) {
     const float c2 = fmaf(-sn, d, cs);
     sn = fmaf(cs, d, sn);
     cs = c2;
-}
-
-constexpr int SF32_TILE = 32;
-
-template <int CH>
-__global__ void __launch_bounds__(SF_THREADS) k_sfac32(int n, int natom_chunk, const uint32_t* __restrict__ fx,
-                                                       const float2* __restrict__ stepz, const double* __restrict__ q,
-                                                       const double* __restrict__ mu, CellP c, int kx, int ky, int kz,
-                                                       int ncol, int ncolblk, int nchunk, int with_q, int with_mu,
-                                                       double* __restrict__ part_re, double* __restrict__ part_im) {
-    __shared__ uint32_t t_u1[SF32_TILE], t_u2[SF32_TILE], t_u3[SF32_TILE];
-    __shared__ float t_q[SF32_TILE], t_m1[SF32_TILE], t_m2[SF32_TILE], t_m3[SF32_TILE], t_rc[SF32_TILE], t_rs[SF32_TILE];
-    const int h = blockIdx.x / ncolblk;
-    const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
-    const int p = blockIdx.y;
-    const int ny_n = 2 * ky + 1;
-    const int colc = col < ncol ? col : ncol - 1;
-    const int inx = colc / ny_n, iny = colc % ny_n - ky, inz0 = -kz + h * CH;
-    const float fnx = (float)inx, fny = (float)iny, fnz0 = (float)inz0;
-    double dre[CH], dim[CH];
-#pragma unroll
-    for (int m = 0; m < CH; ++m) { dre[m] = 0.0; dim[m] = 0.0; }
-    const int a0 = p * natom_chunk;
-    const int a1 = min(n, a0 + natom_chunk);
-    for (int base = a0; base < a1; base += SF32_TILE) {
-        __syncthreads();
-        if (threadIdx.x < SF32_TILE) {
-            int ia = base + threadIdx.x;
-            if (ia < a1) {
-                t_u1[threadIdx.x] = fx[ia];
-                t_u2[threadIdx.x] = fx[n + ia];
-                t_u3[threadIdx.x] = fx[2 * n + ia];
-                t_q[threadIdx.x] = with_q ? (float)q[ia] : 0.f;
-                double m0 = 0, m1 = 0, m2 = 0;
-                if (with_mu) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
-                t_m1[threadIdx.x] = (float)(2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2));
-                t_m2[threadIdx.x] = (float)(2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2));
-                t_m3[threadIdx.x] = (float)(2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2));
-                float2 st = stepz[ia];
-                t_rc[threadIdx.x] = st.x;
-                t_rs[threadIdx.x] = st.y;
-            }
-        }
-        __syncthreads();
-        const int tn = min(SF32_TILE, a1 - base);
-        float are[CH], aim[CH];
-#pragma unroll
-        for (int m = 0; m < CH; ++m) { are[m] = 0.f; aim[m] = 0.f; }
-        for (int t = 0; t < tn; ++t) {
-            const uint32_t ph = (uint32_t)inx * t_u1[t] + (uint32_t)iny * t_u2[t] + (uint32_t)inz0 * t_u3[t];
-            float cs, sn;
-            phase32(ph, cs, sn);
-            const float qa = t_q[t];
-            float km = fmaf(fnx, t_m1[t], fmaf(fny, t_m2[t], fnz0 * t_m3[t]));
-            const float dm = t_m3[t], rc = t_rc[t], rs = t_rs[t];
-#pragma unroll
-            for (int m = 0; m < CH; ++m) {
-                are[m] = fmaf(qa, cs, fmaf(-km, sn, are[m]));
-                aim[m] = fmaf(qa, sn, fmaf(km, cs, aim[m]));
-                const float cn = fmaf(cs, rc, -sn * rs);
-                sn = fmaf(sn, rc, cs * rs);
-                cs = cn;
-                km += dm;
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < CH; ++m) { dre[m] += (double)are[m]; dim[m] += (double)aim[m]; }
-    }
-    if (col < ncol) {
-        const size_t plane = (size_t)ncol * CH * nchunk;
-#pragma unroll
-        for (int m = 0; m < CH; ++m) {
-            size_t idx = (size_t)p * plane + ((size_t)h * CH + m) * ncol + col;
-            part_re[idx] = dre[m];
-            part_im[idx] = dim[m];
-        }
-    }
-}
-
-__global__ void k_aks32(int nrect, const double* __restrict__ aks, float* __restrict__ aks32) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < 2 * nrect) aks32[t] = (float)aks[t];
-}
-
-constexpr int KF32_SUB = 8;
-
-template <int GRAD>
-__global__ void __launch_bounds__(KF_THREADS) k_kfield32(int n, const uint32_t* __restrict__ fx,
-                                                         const float2* __restrict__ stepz, CellP c, int kx, int ky,
-                                                         int kz, int ncol, int nzl, int cols_per_split,
-                                                         const float* __restrict__ aks, int nrect,
-                                                         double* __restrict__ fpart) {
-    extern __shared__ float smf[];
-    float* s_re = smf;
-    float* s_im = smf + KF_COLS * nzl;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int split = blockIdx.y;
-    const int c0 = split * cols_per_split;
-    const int c1 = min(ncol, c0 + cols_per_split);
-    const bool active = i < n;
-    const int ii = active ? i : 0;
-    const uint32_t u1 = fx[ii], u2 = fx[n + ii], u3 = fx[2 * n + ii];
-    const float2 st = stepz[ii];
-    const float rc = st.x, rs = st.y;
-    const float dk0 = (float)(2.0 * PI * c.B[2]), dk1 = (float)(2.0 * PI * c.B[5]), dk2 = (float)(2.0 * PI * c.B[8]);
-    const int ny_n = 2 * ky + 1;
-    double E0 = 0, E1 = 0, E2 = 0;
-    double G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
-    for (int cb = c0; cb < c1; cb += KF_COLS) {
-        const int nc = min(KF_COLS, c1 - cb);
-        __syncthreads();
-        for (int t = threadIdx.x; t < nc * nzl; t += blockDim.x) {
-            s_re[t] = aks[(size_t)cb * nzl + t];
-            s_im[t] = aks[(size_t)nrect + (size_t)cb * nzl + t];
-        }
-        __syncthreads();
-        for (int cc = 0; cc < nc; ++cc) {
-            const int col = cb + cc;
-            const int inx = col / ny_n, iny = col % ny_n - ky;
-            const double bx = 2.0 * PI * (inx * c.B[0] + iny * c.B[1] - kz * c.B[2]);
-            const double by = 2.0 * PI * (inx * c.B[3] + iny * c.B[4] - kz * c.B[5]);
-            const double bz = 2.0 * PI * (inx * c.B[6] + iny * c.B[7] - kz * c.B[8]);
-            const float* pr = s_re + cc * nzl;
-            const float* pi = s_im + cc * nzl;
-            for (int m0 = 0; m0 < nzl; m0 += KF32_SUB) {
-                const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)(m0 - kz) * u3;
-                float cs, sn;
-                phase32(ph, cs, sn);
-                float k0 = (float)(bx + m0 * 2.0 * PI * c.B[2]);
-                float k1 = (float)(by + m0 * 2.0 * PI * c.B[5]);
-                float k2 = (float)(bz + m0 * 2.0 * PI * c.B[8]);
-                float e0 = 0.f, e1 = 0.f, e2 = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f, g3 = 0.f, g4 = 0.f, g5 = 0.f;
-                const int mend = min(KF32_SUB, nzl - m0);
-#pragma unroll
-                for (int mm = 0; mm < KF32_SUB; ++mm) {
-                    if (mm < mend) {
-                        const float ar = pr[m0 + mm], ai = pi[m0 + mm];
-                        const float recarg = fmaf(ai, cs, -ar * sn);
-                        e0 = fmaf(-k0, recarg, e0);
-                        e1 = fmaf(-k1, recarg, e1);
-                        e2 = fmaf(-k2, recarg, e2);
-                        if (GRAD) {
-                            const float r2 = fmaf(ar, cs, ai * sn);
-                            const float a0 = k0 * r2, a1 = k1 * r2;
-                            g0 = fmaf(k0, a0, g0);
-                            g1 = fmaf(k1, a1, g1);
-                            g2 = fmaf(k2, k2 * r2, g2);
-                            g3 = fmaf(k1, a0, g3);
-                            g4 = fmaf(k2, a0, g4);
-                            g5 = fmaf(k2, a1, g5);
-                        }
-                        const float cn = fmaf(cs, rc, -sn * rs);
-                        sn = fmaf(sn, rc, cs * rs);
-                        cs = cn;
-                        k0 += dk0; k1 += dk1; k2 += dk2;
-                    }
-                }
-                E0 += e0; E1 += e1; E2 += e2;
-                if (GRAD) { G0 += g0; G1 += g1; G2 += g2; G3 += g3; G4 += g4; G5 += g5; }
-            }
-        }
-    }
-    if (active) {
-        const int nv = GRAD ? 9 : 3;
-        double* o = fpart + (size_t)split * nv * n;
-        o[i] = E0; o[n + i] = E1; o[2 * n + i] = E2;
-        if (GRAD) {
-            o[3 * n + i] = G0; o[4 * n + i] = G1; o[5 * n + i] = G2;
-            o[6 * n + i] = G3; o[7 * n + i] = G4; o[8 * n + i] = G5;
-        }
-    }
 }
 
 // ---- second-generation FP32 kernels --------------------------------------
@@ -483,86 +301,6 @@ __global__ void k_phase_table(int n, const double* __restrict__ sx, const double
     }
 }
 
-constexpr int SF2_TILE = 32;
-
-// Pass 1: thread = (column, chunk of TM nz).  Contribution of atom t to the
-// chunk: sum_m (w0 + m dw) T_m with w0 = (q + i k0.mu) e0, dw = i (2 pi b3.mu) e0.
-__global__ void __launch_bounds__(SF_THREADS) k_sfac32v2(int n, int natom_chunk, const uint32_t* __restrict__ fx,
-                                                         const float2* __restrict__ tab, const double* __restrict__ q,
-                                                         const double* __restrict__ mu, CellP c, int kx, int ky, int kz,
-                                                         int ncol, int ncolblk, int nchunk, int with_q, int with_mu,
-                                                         double* __restrict__ part_re, double* __restrict__ part_im) {
-    __shared__ uint32_t t_u1[SF2_TILE], t_u2[SF2_TILE], t_u3[SF2_TILE];
-    __shared__ float t_q[SF2_TILE], t_m1[SF2_TILE], t_m2[SF2_TILE], t_m3[SF2_TILE];
-    __shared__ float2 t_tab[SF2_TILE][TM];
-    const int h = blockIdx.x / ncolblk;
-    const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
-    const int p = blockIdx.y;
-    const int ny_n = 2 * ky + 1;
-    const int colc = col < ncol ? col : ncol - 1;
-    const int inx = colc / ny_n, iny = colc % ny_n - ky, inz0 = -kz + h * TM;
-    const float fnx = (float)inx, fny = (float)iny, fnz0 = (float)inz0;
-    double dre[TM], dim[TM];
-#pragma unroll
-    for (int m = 0; m < TM; ++m) { dre[m] = 0.0; dim[m] = 0.0; }
-    const int a0 = p * natom_chunk;
-    const int a1 = min(n, a0 + natom_chunk);
-    for (int base = a0; base < a1; base += SF2_TILE) {
-        __syncthreads();
-        for (int t = threadIdx.x; t < SF2_TILE * TM; t += blockDim.x) {
-            int ia = base + t / TM;
-            if (ia < a1) t_tab[t / TM][t % TM] = tab[(size_t)ia * TM + (t % TM)];
-        }
-        if (threadIdx.x < SF2_TILE) {
-            int ia = base + threadIdx.x;
-            if (ia < a1) {
-                t_u1[threadIdx.x] = fx[ia];
-                t_u2[threadIdx.x] = fx[n + ia];
-                t_u3[threadIdx.x] = fx[2 * n + ia];
-                t_q[threadIdx.x] = with_q ? (float)q[ia] : 0.f;
-                double m0 = 0, m1 = 0, m2 = 0;
-                if (with_mu) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
-                t_m1[threadIdx.x] = (float)(2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2));
-                t_m2[threadIdx.x] = (float)(2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2));
-                t_m3[threadIdx.x] = (float)(2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2));
-            }
-        }
-        __syncthreads();
-        const int tn = min(SF2_TILE, a1 - base);
-        float are[TM], aim[TM];
-#pragma unroll
-        for (int m = 0; m < TM; ++m) { are[m] = 0.f; aim[m] = 0.f; }
-        for (int t = 0; t < tn; ++t) {
-            const uint32_t ph = (uint32_t)inx * t_u1[t] + (uint32_t)iny * t_u2[t] + (uint32_t)inz0 * t_u3[t];
-            float c0, s0;
-            phase32(ph, c0, s0);
-            const float qa = t_q[t];
-            const float km = fmaf(fnx, t_m1[t], fmaf(fny, t_m2[t], fnz0 * t_m3[t]));
-            const float m3 = t_m3[t];
-            const float w0r = fmaf(qa, c0, -km * s0), w0i = fmaf(qa, s0, km * c0);
-            const float dwr = -m3 * s0, dwi = m3 * c0;
-#pragma unroll
-            for (int m = 0; m < TM; ++m) {
-                const float wr = fmaf((float)m, dwr, w0r), wi = fmaf((float)m, dwi, w0i);
-                const float2 T = t_tab[t][m];
-                are[m] = fmaf(wr, T.x, fmaf(-wi, T.y, are[m]));
-                aim[m] = fmaf(wr, T.y, fmaf(wi, T.x, aim[m]));
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < TM; ++m) { dre[m] += (double)are[m]; dim[m] += (double)aim[m]; }
-    }
-    if (col < ncol) {
-        const size_t plane = (size_t)ncol * TM * nchunk;
-#pragma unroll
-        for (int m = 0; m < TM; ++m) {
-            size_t idx = (size_t)p * plane + ((size_t)h * TM + m) * ncol + col;
-            part_re[idx] = dre[m];
-            part_im[idx] = dim[m];
-        }
-    }
-}
-
 // A_k S(k) as float2, each column padded to nzp (a multiple of TM) with zeros.
 __global__ void k_aks32_pad(int ncol, int nzl, int nzp, int nrect, const double* __restrict__ aks,
                             float2* __restrict__ out) {
@@ -577,15 +315,147 @@ __global__ void k_aks32_pad(int ncol, int nzl, int nzp, int nrect, const double*
     out[t] = v;
 }
 
-// Pass 2: thread = atom.  Along a chunk of TM k-vectors k_m = kb + m dk, so
-// sum_m k_m r_m = kb R0 + dk R1 with R0 = sum r_m, R1 = sum m r_m (and the
-// second moment for the field gradient): the k-vector is applied once per chunk.
+typedef unsigned long long u64;
+
+__device__ __forceinline__ u64 pk2(float a, float b) {
+    u64 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(u64 v) {
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return make_float2(a, b);
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+    u64 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+constexpr int SF3_TILE = 32;
+
+// Pass 1: thread = (column, chunk of TM nz values).  Atom t contributes
+// sum_m (w0 + m dw) T_m with w0 = (q + i k0.mu) e0 and dw = i (2 pi b3.mu) e0.
+// Packed: acc_m += (wr,wr)(Tx,Ty) + (wi,wi)(-Ty,Tx).
+template <int WITH_MU>
+__global__ void __launch_bounds__(SF_THREADS) k_sfac32v3(int n, int natom_chunk, const uint32_t* __restrict__ fx,
+                                                         const float2* __restrict__ tab, const double* __restrict__ q,
+                                                         const double* __restrict__ mu, CellP c, int kx, int ky, int kz,
+                                                         int ncol, int ncolblk, int nchunk, int with_q,
+                                                         double* __restrict__ part_re, double* __restrict__ part_im) {
+    __shared__ uint32_t t_u1[SF3_TILE], t_u2[SF3_TILE], t_u3[SF3_TILE];
+    __shared__ float t_q[SF3_TILE], t_m1[SF3_TILE], t_m2[SF3_TILE], t_m3[SF3_TILE];
+    __shared__ u64 t_T[SF3_TILE][TM];    // (Tx, Ty)
+    __shared__ u64 t_iT[SF3_TILE][TM];   // (-Ty, Tx) = i T
+    const int h = blockIdx.x / ncolblk;
+    const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
+    const int p = blockIdx.y;
+    const int ny_n = 2 * ky + 1;
+    const int colc = col < ncol ? col : ncol - 1;
+    const int inx = colc / ny_n, iny = colc % ny_n - ky, inz0 = -kz + h * TM;
+    const float fnx = (float)inx, fny = (float)iny, fnz0 = (float)inz0;
+    u64 MM[TM];
+#pragma unroll
+    for (int m = 0; m < TM; ++m) MM[m] = pk2((float)m, (float)m);
+    double dre[TM], dim[TM];
+#pragma unroll
+    for (int m = 0; m < TM; ++m) { dre[m] = 0.0; dim[m] = 0.0; }
+    const int a0 = p * natom_chunk;
+    const int a1 = min(n, a0 + natom_chunk);
+    for (int base = a0; base < a1; base += SF3_TILE) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < SF3_TILE * TM; t += blockDim.x) {
+            int ia = base + t / TM;
+            if (ia < a1) {
+                float2 T = tab[(size_t)ia * TM + (t % TM)];
+                t_T[t / TM][t % TM] = pk2(T.x, T.y);
+                t_iT[t / TM][t % TM] = pk2(-T.y, T.x);
+            }
+        }
+        if (threadIdx.x < SF3_TILE) {
+            int ia = base + threadIdx.x;
+            if (ia < a1) {
+                t_u1[threadIdx.x] = fx[ia];
+                t_u2[threadIdx.x] = fx[n + ia];
+                t_u3[threadIdx.x] = fx[2 * n + ia];
+                t_q[threadIdx.x] = with_q ? (float)q[ia] : 0.f;
+                double m0 = 0, m1 = 0, m2 = 0;
+                if (WITH_MU) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
+                t_m1[threadIdx.x] = (float)(2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2));
+                t_m2[threadIdx.x] = (float)(2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2));
+                t_m3[threadIdx.x] = (float)(2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2));
+            }
+        }
+        __syncthreads();
+        const int tn = min(SF3_TILE, a1 - base);
+        u64 acc[TM];
+#pragma unroll
+        for (int m = 0; m < TM; ++m) acc[m] = 0ull;
+        for (int t = 0; t < tn; ++t) {
+            const uint32_t ph = (uint32_t)inx * t_u1[t] + (uint32_t)iny * t_u2[t] + (uint32_t)inz0 * t_u3[t];
+            float c0, s0;
+            phase32(ph, c0, s0);
+            const float qa = t_q[t];
+            if (WITH_MU) {
+                const float km = fmaf(fnx, t_m1[t], fmaf(fny, t_m2[t], fnz0 * t_m3[t]));
+                const float m3 = t_m3[t];
+                const float w0r = fmaf(qa, c0, -km * s0), w0i = fmaf(qa, s0, km * c0);
+                const u64 W0R = pk2(w0r, w0r), W0I = pk2(w0i, w0i);
+                const u64 DWR = pk2(-m3 * s0, -m3 * s0), DWI = pk2(m3 * c0, m3 * c0);
+#pragma unroll
+                for (int m = 0; m < TM; ++m) {
+                    const u64 WR = fma2(MM[m], DWR, W0R);
+                    const u64 WI = fma2(MM[m], DWI, W0I);
+                    acc[m] = fma2(WR, t_T[t][m], acc[m]);
+                    acc[m] = fma2(WI, t_iT[t][m], acc[m]);
+                }
+            } else {
+                const float w0r = qa * c0, w0i = qa * s0;
+                const u64 WR = pk2(w0r, w0r), WI = pk2(w0i, w0i);
+#pragma unroll
+                for (int m = 0; m < TM; ++m) {
+                    acc[m] = fma2(WR, t_T[t][m], acc[m]);
+                    acc[m] = fma2(WI, t_iT[t][m], acc[m]);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < TM; ++m) {
+            float2 v = upk2(acc[m]);
+            dre[m] += (double)v.x;
+            dim[m] += (double)v.y;
+        }
+    }
+    if (col < ncol) {
+        const size_t plane = (size_t)ncol * TM * nchunk;
+#pragma unroll
+        for (int m = 0; m < TM; ++m) {
+            size_t idx = (size_t)p * plane + ((size_t)h * TM + m) * ncol + col;
+            part_re[idx] = dre[m];
+            part_im[idx] = dim[m];
+        }
+    }
+}
+
+// Pass 2: thread = atom.  Per chunk of TM k-vectors along nz,
+//   Z_j = sum_m m^j conj(A_k S)_m T_m    (j = 0, 1 [, 2 for the gradient])
+// in packed FMAs: conj(a) T = (ar,ar)(Tx,Ty) + (ai,-ai)(Ty,Tx).  With the
+// chunk's base phase e0 and k_m = kb + m dk:
+//   sum_m k_m recarg_m = -(kb Im(e0 Z0) + dk Im(e0 Z1)),
+//   sum_m k_m k_m^T recarg2_m = kb kb^T Re(e0 Z0) + (kb dk^T + dk kb^T) Re(e0 Z1) + dk dk^T Re(e0 Z2).
+// The column's base phase is computed once; chunk bases follow by
+// multiplication with e^{2 pi i 16 s_z}.  The shared-memory k data holds, per
+// k, (ar,ar),(ai,-ai) and the m- (and m^2-) weighted copies.
+constexpr int KF3_COLS = 4;
+
 template <int GRAD>
-__global__ void __launch_bounds__(KF_THREADS) k_kfield32v2(int n, const uint32_t* __restrict__ fx,
+__global__ void __launch_bounds__(KF_THREADS) k_kfield32v3(int n, const uint32_t* __restrict__ fx,
                                                            const float2* __restrict__ tab, CellP c, int kx, int ky,
                                                            int kz, int ncol, int nzp, int cols_per_split,
                                                            const float2* __restrict__ aks, double* __restrict__ fpart) {
-    extern __shared__ float2 sm2[];
+    extern __shared__ u64 skd[];
+    constexpr int NW = GRAD ? 6 : 4;     // packed words per k
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int split = blockIdx.y;
     const int c0 = split * cols_per_split;
@@ -593,60 +463,86 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v2(int n, const uint32_t
     const bool active = i < n;
     const int ii = active ? i : 0;
     const uint32_t u1 = fx[ii], u2 = fx[n + ii], u3 = fx[2 * n + ii];
-    float2 T[TM];
+    u64 T[TM], Ts[TM];
 #pragma unroll
-    for (int m = 0; m < TM; ++m) T[m] = tab[(size_t)ii * TM + m];
+    for (int m = 0; m < TM; ++m) {
+        float2 t = tab[(size_t)ii * TM + m];
+        T[m] = pk2(t.x, t.y);
+        Ts[m] = pk2(t.y, t.x);
+    }
+    // e^{2 pi i 16 s_z} from the fixed-point coordinate (exact phase)
+    float e16c, e16s;
+    phase32(u3 * 16u, e16c, e16s);
     const double dkx = 2.0 * PI * c.B[2], dky = 2.0 * PI * c.B[5], dkz = 2.0 * PI * c.B[8];
     const float dk0 = (float)dkx, dk1 = (float)dky, dk2 = (float)dkz;
     const int ny_n = 2 * ky + 1;
     double E0 = 0, E1 = 0, E2 = 0;
     double G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
-    for (int cb = c0; cb < c1; cb += KF_COLS) {
-        const int nc = min(KF_COLS, c1 - cb);
+    for (int cb = c0; cb < c1; cb += KF3_COLS) {
+        const int nc = min(KF3_COLS, c1 - cb);
         __syncthreads();
-        for (int t = threadIdx.x; t < nc * nzp; t += blockDim.x) sm2[t] = aks[(size_t)cb * nzp + t];
+        for (int t = threadIdx.x; t < nc * nzp; t += blockDim.x) {
+            const float2 a = aks[(size_t)cb * nzp + t];
+            const float m = (float)(t % TM);
+            u64* o = skd + (size_t)t * NW;
+            o[0] = pk2(a.x, a.x);
+            o[1] = pk2(a.y, -a.y);
+            o[2] = pk2(m * a.x, m * a.x);
+            o[3] = pk2(m * a.y, -m * a.y);
+            if (GRAD) {
+                o[4] = pk2(m * m * a.x, m * m * a.x);
+                o[5] = pk2(m * m * a.y, -m * m * a.y);
+            }
+        }
         __syncthreads();
         for (int cc = 0; cc < nc; ++cc) {
             const int col = cb + cc;
             const int inx = col / ny_n, iny = col % ny_n - ky;
-            const double bx = 2.0 * PI * (inx * c.B[0] + iny * c.B[1]);
-            const double by = 2.0 * PI * (inx * c.B[3] + iny * c.B[4]);
-            const double bz = 2.0 * PI * (inx * c.B[6] + iny * c.B[7]);
-            const float2* pk = sm2 + cc * nzp;
+            const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)(-kz) * u3;
+            float ec, es;
+            phase32(ph, ec, es);
+            float kb0 = (float)(2.0 * PI * (inx * c.B[0] + iny * c.B[1]) - kz * dkx);
+            float kb1 = (float)(2.0 * PI * (inx * c.B[3] + iny * c.B[4]) - kz * dky);
+            float kb2 = (float)(2.0 * PI * (inx * c.B[6] + iny * c.B[7]) - kz * dkz);
+            const u64* kd = skd + (size_t)cc * nzp * NW;
             for (int m0 = 0; m0 < nzp; m0 += TM) {
-                const int nzb = m0 - kz;
-                const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)nzb * u3;
-                float ec, es;
-                phase32(ph, ec, es);
-                float R0 = 0.f, R1 = 0.f, Q0 = 0.f, Q1 = 0.f, Q2 = 0.f;
+                u64 Z0 = 0ull, Z1 = 0ull, Z2 = 0ull;
 #pragma unroll
                 for (int m = 0; m < TM; ++m) {
-                    const float cs = fmaf(ec, T[m].x, -es * T[m].y);
-                    const float sn = fmaf(es, T[m].x, ec * T[m].y);
-                    const float2 a = pk[m0 + m];
-                    const float r = fmaf(a.y, cs, -a.x * sn);
-                    R0 += r;
-                    R1 = fmaf((float)m, r, R1);
+                    const u64* w = kd + (size_t)(m0 + m) * NW;
+                    Z0 = fma2(w[0], T[m], Z0);
+                    Z0 = fma2(w[1], Ts[m], Z0);
+                    Z1 = fma2(w[2], T[m], Z1);
+                    Z1 = fma2(w[3], Ts[m], Z1);
                     if (GRAD) {
-                        const float r2 = fmaf(a.x, cs, a.y * sn);
-                        Q0 += r2;
-                        Q1 = fmaf((float)m, r2, Q1);
-                        Q2 = fmaf((float)(m * m), r2, Q2);
+                        Z2 = fma2(w[4], T[m], Z2);
+                        Z2 = fma2(w[5], Ts[m], Z2);
                     }
                 }
-                const float kb0 = (float)(bx + nzb * dkx), kb1 = (float)(by + nzb * dky), kb2 = (float)(bz + nzb * dkz);
-                E0 -= (double)fmaf(kb0, R0, dk0 * R1);
-                E1 -= (double)fmaf(kb1, R0, dk1 * R1);
-                E2 -= (double)fmaf(kb2, R0, dk2 * R1);
+                const float2 z0 = upk2(Z0), z1 = upk2(Z1);
+                // e0 * Z: real and imaginary parts
+                const float p0r = fmaf(ec, z0.x, -es * z0.y), p0i = fmaf(ec, z0.y, es * z0.x);
+                const float p1r = fmaf(ec, z1.x, -es * z1.y), p1i = fmaf(ec, z1.y, es * z1.x);
+                E0 += (double)fmaf(kb0, p0i, dk0 * p1i);
+                E1 += (double)fmaf(kb1, p0i, dk1 * p1i);
+                E2 += (double)fmaf(kb2, p0i, dk2 * p1i);
                 if (GRAD) {
-                    // sum_m (kb + m dk)_a (kb + m dk)_b r2_m
-                    G0 += (double)(kb0 * kb0 * Q0 + 2.f * kb0 * dk0 * Q1 + dk0 * dk0 * Q2);
-                    G1 += (double)(kb1 * kb1 * Q0 + 2.f * kb1 * dk1 * Q1 + dk1 * dk1 * Q2);
-                    G2 += (double)(kb2 * kb2 * Q0 + 2.f * kb2 * dk2 * Q1 + dk2 * dk2 * Q2);
-                    G3 += (double)(kb0 * kb1 * Q0 + (kb0 * dk1 + dk0 * kb1) * Q1 + dk0 * dk1 * Q2);
-                    G4 += (double)(kb0 * kb2 * Q0 + (kb0 * dk2 + dk0 * kb2) * Q1 + dk0 * dk2 * Q2);
-                    G5 += (double)(kb1 * kb2 * Q0 + (kb1 * dk2 + dk1 * kb2) * Q1 + dk1 * dk2 * Q2);
+                    const float2 z2 = upk2(Z2);
+                    const float p2r = fmaf(ec, z2.x, -es * z2.y);
+                    G0 += (double)(kb0 * kb0 * p0r + 2.f * kb0 * dk0 * p1r + dk0 * dk0 * p2r);
+                    G1 += (double)(kb1 * kb1 * p0r + 2.f * kb1 * dk1 * p1r + dk1 * dk1 * p2r);
+                    G2 += (double)(kb2 * kb2 * p0r + 2.f * kb2 * dk2 * p1r + dk2 * dk2 * p2r);
+                    G3 += (double)(kb0 * kb1 * p0r + (kb0 * dk1 + dk0 * kb1) * p1r + dk0 * dk1 * p2r);
+                    G4 += (double)(kb0 * kb2 * p0r + (kb0 * dk2 + dk0 * kb2) * p1r + dk0 * dk2 * p2r);
+                    G5 += (double)(kb1 * kb2 * p0r + (kb1 * dk2 + dk1 * kb2) * p1r + dk1 * dk2 * p2r);
                 }
+                // next chunk: e0 *= e^{2 pi i 16 s_z}, kb += 16 dk
+                const float nc_ = fmaf(ec, e16c, -es * e16s);
+                es = fmaf(es, e16c, ec * e16s);
+                ec = nc_;
+                kb0 = fmaf(16.f, dk0, kb0);
+                kb1 = fmaf(16.f, dk1, kb1);
+                kb2 = fmaf(16.f, dk2, kb2);
             }
         }
     }
@@ -657,6 +553,183 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v2(int n, const uint32_t
         if (GRAD) {
             o[3 * n + i] = G0; o[4 * n + i] = G1; o[5 * n + i] = G2;
             o[6 * n + i] = G3; o[7 * n + i] = G4; o[8 * n + i] = G5;
+        }
+    }
+}
+
+// ---- FP64 low-|k| set of the mixed path ------------------------------------
+// The error of an FP32 reciprocal sum is weighted by A_k |k|, which peaks at
+// |k| ~ alpha; the short list of k-vectors with |k| < ksplit (about 5 % of the
+// half space at ksplit = 3.4 alpha) is therefore summed in FP64 and removed
+// from the FP32 set.  The list is stored as columns (nx, ny) with a
+// contiguous nz range [nzlo, nzlo + nzn).
+
+constexpr int LK_CH = 8;
+constexpr int LK_SPLIT = 4;   // column splits of the low-|k| field pass
+
+__global__ void __launch_bounds__(SF_THREADS) k_sfac64_low(int n, int natom_chunk, const double* __restrict__ sx,
+                                                           const double* __restrict__ sy, const double* __restrict__ sz,
+                                                           const double* __restrict__ q, const double* __restrict__ mu,
+                                                           CellP c, const int* __restrict__ cols, int ncol, int nzmax,
+                                                           int nchunk, int with_q, int with_mu,
+                                                           double* __restrict__ part_re, double* __restrict__ part_im) {
+    __shared__ double t_s1[SF_TILE], t_s2[SF_TILE], t_s3[SF_TILE], t_q[SF_TILE];
+    __shared__ double t_m1[SF_TILE], t_m2[SF_TILE], t_m3[SF_TILE], t_cs[SF_TILE], t_sn[SF_TILE];
+    const int h = blockIdx.x % nchunk;
+    const int cidx = (blockIdx.x / nchunk) * SF_THREADS + threadIdx.x;
+    const int p = blockIdx.y;
+    const int cc = cidx < ncol ? cidx : ncol - 1;
+    const double nx = (double)cols[4 * cc], ny = (double)cols[4 * cc + 1];
+    const double nz0 = (double)(cols[4 * cc + 2] + h * LK_CH);
+    double are[LK_CH], aim[LK_CH];
+#pragma unroll
+    for (int m = 0; m < LK_CH; ++m) { are[m] = 0.0; aim[m] = 0.0; }
+    const int a0 = p * natom_chunk;
+    const int a1 = min(n, a0 + natom_chunk);
+    for (int base = a0; base < a1; base += SF_TILE) {
+        __syncthreads();
+        if (threadIdx.x < SF_TILE) {
+            int ia = base + threadIdx.x;
+            if (ia < a1) {
+                double s1 = sx[ia], s2 = sy[ia], s3 = sz[ia];
+                t_s1[threadIdx.x] = s1; t_s2[threadIdx.x] = s2; t_s3[threadIdx.x] = s3;
+                t_q[threadIdx.x] = with_q ? q[ia] : 0.0;
+                double m0 = 0, m1 = 0, m2 = 0;
+                if (with_mu) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
+                t_m1[threadIdx.x] = 2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2);
+                t_m2[threadIdx.x] = 2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2);
+                t_m3[threadIdx.x] = 2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2);
+                double sn, cs;
+                sincospi(2.0 * (s3 - rint(s3)), &sn, &cs);
+                t_cs[threadIdx.x] = cs; t_sn[threadIdx.x] = sn;
+            }
+        }
+        __syncthreads();
+        const int tn = min(SF_TILE, a1 - base);
+        for (int t = 0; t < tn; ++t) {
+            double ph = fma(nx, t_s1[t], fma(ny, t_s2[t], nz0 * t_s3[t]));
+            ph -= rint(ph);
+            double sn, cs;
+            sincospi(2.0 * ph, &sn, &cs);
+            const double qa = t_q[t];
+            double km = fma(nx, t_m1[t], fma(ny, t_m2[t], nz0 * t_m3[t]));
+            const double dm = t_m3[t], rc = t_cs[t], rs = t_sn[t];
+#pragma unroll
+            for (int m = 0; m < LK_CH; ++m) {
+                are[m] = fma(qa, cs, fma(-km, sn, are[m]));
+                aim[m] = fma(qa, sn, fma(km, cs, aim[m]));
+                const double cn = cs * rc - sn * rs;
+                sn = fma(sn, rc, cs * rs);
+                cs = cn;
+                km += dm;
+            }
+        }
+    }
+    if (cidx < ncol) {
+        const size_t plane = (size_t)nzmax * ncol;
+#pragma unroll
+        for (int m = 0; m < LK_CH; ++m) {
+            int mz = h * LK_CH + m;
+            if (mz < nzmax) {
+                size_t idx = (size_t)p * plane + (size_t)mz * ncol + cidx;
+                part_re[idx] = are[m];
+                part_im[idx] = aim[m];
+            }
+        }
+    }
+}
+
+__global__ void k_sfac64_low_reduce(int P, int ncol, int nzmax, const int* __restrict__ cols,
+                                    const double* __restrict__ part_re, const double* __restrict__ part_im,
+                                    const double* __restrict__ Ak, const double* __restrict__ kcoe, CellP c,
+                                    double* __restrict__ aks, int energy, double* partials) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (t < ncol * nzmax) {
+        const int cidx = t % ncol, mz = t / ncol;
+        const size_t plane = (size_t)nzmax * ncol;
+        double sr = 0.0, si = 0.0;
+        for (int p = 0; p < P; ++p) {
+            sr += part_re[(size_t)p * plane + (size_t)mz * ncol + cidx];
+            si += part_im[(size_t)p * plane + (size_t)mz * ncol + cidx];
+        }
+        const size_t r = (size_t)cidx * nzmax + mz;
+        const double ak = (mz < cols[4 * cidx + 3]) ? Ak[r] : 0.0;
+        aks[r] = ak * sr;
+        aks[(size_t)ncol * nzmax + r] = ak * si;
+        if (energy && ak != 0.0) {
+            const double nx = cols[4 * cidx], ny = cols[4 * cidx + 1], nz = cols[4 * cidx + 2] + mz;
+            const double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz * c.B[2]);
+            const double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz * c.B[5]);
+            const double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz * c.B[8]);
+            const double str = (sr * sr + si * si) * ak;
+            const double kc = kcoe[r];
+            v[0] = str;
+            v[1] = (1.0 - kc * k0 * k0) * str;
+            v[2] = (1.0 - kc * k1 * k1) * str;
+            v[3] = (1.0 - kc * k2 * k2) * str;
+            v[4] = -kc * k0 * k1 * str;
+            v[5] = -kc * k0 * k2 * str;
+            v[6] = -kc * k1 * k2 * str;
+        }
+    }
+    if (energy) block_partials<7>(v, partials);
+}
+
+// Pass 2 over the low set: thread = atom, every column of the list; written
+// (not accumulated) into fpart[9][n] (E and, with GRAD, the field gradient).
+template <int GRAD>
+__global__ void __launch_bounds__(KF_THREADS) k_kfield64_low(int n, const double* __restrict__ sx,
+                                                             const double* __restrict__ sy, const double* __restrict__ sz,
+                                                             CellP c, const int* __restrict__ cols, int ncol, int nzmax,
+                                                             const double* __restrict__ aks, double* __restrict__ fpart) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int per = (ncol + gridDim.y - 1) / gridDim.y;
+    const int cbeg = blockIdx.y * per, cend = min(ncol, cbeg + per);
+    fpart += (size_t)blockIdx.y * 9 * n;
+    const bool active = i < n;
+    const int ii = active ? i : 0;
+    const double s1 = sx[ii], s2 = sy[ii], s3 = sz[ii];
+    double rs, rc;
+    sincospi(2.0 * (s3 - rint(s3)), &rs, &rc);
+    const double dk0 = 2.0 * PI * c.B[2], dk1 = 2.0 * PI * c.B[5], dk2 = 2.0 * PI * c.B[8];
+    double E0 = 0, E1 = 0, E2 = 0, G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
+    const double* aim_base = aks + (size_t)ncol * nzmax;
+    for (int cc = cbeg; cc < cend; ++cc) {
+        const double nx = cols[4 * cc], ny = cols[4 * cc + 1], nz0 = cols[4 * cc + 2];
+        const int nzn = cols[4 * cc + 3];
+        double ph = fma(nx, s1, fma(ny, s2, nz0 * s3));
+        ph -= rint(ph);
+        double sn, cs;
+        sincospi(2.0 * ph, &sn, &cs);
+        double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz0 * c.B[2]);
+        double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz0 * c.B[5]);
+        double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz0 * c.B[8]);
+        const double* pr = aks + (size_t)cc * nzmax;
+        const double* pi = aim_base + (size_t)cc * nzmax;
+        for (int m = 0; m < nzn; ++m) {
+            const double ar = __ldg(pr + m), ai = __ldg(pi + m);
+            const double recarg = ai * cs - ar * sn;
+            E0 = fma(-k0, recarg, E0);
+            E1 = fma(-k1, recarg, E1);
+            E2 = fma(-k2, recarg, E2);
+            if (GRAD) {
+                const double r2 = ar * cs + ai * sn;
+                const double a0 = k0 * r2, a1 = k1 * r2;
+                G0 = fma(k0, a0, G0); G1 = fma(k1, a1, G1); G2 = fma(k2, k2 * r2, G2);
+                G3 = fma(k1, a0, G3); G4 = fma(k2, a0, G4); G5 = fma(k2, a1, G5);
+            }
+            const double cn = cs * rc - sn * rs;
+            sn = fma(sn, rc, cs * rs);
+            cs = cn;
+            k0 += dk0; k1 += dk1; k2 += dk2;
+        }
+    }
+    if (active) {
+        fpart[i] = E0; fpart[n + i] = E1; fpart[2 * n + i] = E2;
+        if (GRAD) {
+            fpart[3 * n + i] = G0; fpart[4 * n + i] = G1; fpart[5 * n + i] = G2;
+            fpart[6 * n + i] = G3; fpart[7 * n + i] = G4; fpart[8 * n + i] = G5;
         }
     }
 }
@@ -697,65 +770,101 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
                       const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl, RecScratch& rs,
                       double* ef, double* efg, double* fo, Partials& part, DevScalars* d, Prof* prof) {
     RecLaunch L = plan(n, kg);
-    const size_t plane = (size_t)L.P * L.nchunk * L.CH * kg.ncol;
+    const size_t plane = (size_t)L.P * std::max(L.nchunk * L.CH, ((kg.nzl + TM - 1) / TM) * TM) * kg.ncol;
     double* pre = rs.part;
     double* pim = rs.part + plane;
-    dim3 g1(L.nchunk * L.ncolblk, L.P);
-    RecLaunch L2 = L;
-    L2.nchunk = (kg.nzl + TM - 1) / TM;
-    dim3 g1v2(L2.nchunk * L.ncolblk, L.P);
     const int kx = kg.kmax[0], ky = kg.kmax[1], kz = kg.kmax[2];
     const bool mixed = fl.prec == MDFF_PREC_MIXED;
+    const bool low = mixed && rs.low.ncol > 0;
+    const int nchunk32 = (kg.nzl + TM - 1) / TM;
+    const int total = kg.ncol * kg.nzl;
+    const int rb = (total + 255) / 256;
     prof->begin(PK_SFAC);
+    int nk = 2 + (fl.energy ? 1 : 0);
     if (mixed) {
         if (rs.tab_epoch != rs.want_epoch) {
             k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab);
             rs.tab_epoch = rs.want_epoch;
+            nk++;
         }
-        k_sfac32v2<<<g1v2, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
-                                               L.ncolblk, L2.nchunk, fl.with_q, fl.with_mu, pre, pim);
+        dim3 g1(nchunk32 * L.ncolblk, L.P);
+        if (fl.with_mu)
+            k_sfac32v3<1><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
+                                                     L.ncolblk, nchunk32, fl.with_q, pre, pim);
+        else
+            k_sfac32v3<0><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
+                                                     L.ncolblk, nchunk32, fl.with_q, pre, pim);
+        // the FP32 set excludes the low-|k| vectors (A_k = 0 there)
+        k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, TM, nchunk32, kg.ncol, kg.nzl, kx, ky, kz, pre, pim,
+                                          low ? kg.Ak_hi : kg.Ak, kg.kcoe, c, rs.aks, kg.nrect, fl.energy, part.buf);
     } else {
+        dim3 g1(L.nchunk * L.ncolblk, L.P);
 #define SFAC(CHV) k_sfac<CHV><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, sx, sy, sz, q, mu, c, kx, ky, kz, kg.ncol, \
                                                      L.ncolblk, L.nchunk, fl.with_q, fl.with_mu, pre, pim)
         if (L.CH == 16) SFAC(16);
         else if (L.CH == 12) SFAC(12);
         else SFAC(8);
 #undef SFAC
+        k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, L.CH, L.nchunk, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak, kg.kcoe,
+                                          c, rs.aks, kg.nrect, fl.energy, part.buf);
     }
-    const int total = kg.ncol * kg.nzl;
-    const int rb = (total + 255) / 256;
-    k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, mixed ? TM : L.CH, mixed ? L2.nchunk : L.nchunk, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak, kg.kcoe, c,
-                                      rs.aks, kg.nrect, fl.energy, part.buf);
     if (fl.energy) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
-    prof->end(2 + (fl.energy ? 1 : 0));
+    if (low) {
+        LowK& lk = rs.low;
+        const int nch = (lk.nzmax + LK_CH - 1) / LK_CH;
+        const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;
+        dim3 gl(nch * cb, lk.P);
+        const size_t lplane = (size_t)lk.P * lk.nzmax * lk.ncol;
+        k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, sx, sy, sz, q, mu, c, lk.col, lk.ncol, lk.nzmax, nch,
+                                                fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
+        const int lb = (lk.ncol * lk.nzmax + 255) / 256;
+        k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane, lk.Ak,
+                                                lk.kcoe, c, lk.aks, fl.energy, part.buf);
+        if (fl.energy) launch_reduce_partials(st, part.buf, lb, 7, d->rec, 1);
+        nk += 2 + (fl.energy ? 1 : 0);
+    }
+    prof->end(nk);
     if (!fl.field && !fl.grad && !fl.forces) return;
     prof->begin(PK_KFIELD);
+    nk = 1;
     dim3 g2((n + KF_THREADS - 1) / KF_THREADS, L.nsplit);
     const bool grad = fl.grad || (fl.forces && fl.with_mu);
     if (mixed) {
-        const int nzp = ((kg.nzl + TM - 1) / TM) * TM;
+        const int nzp = nchunk32 * TM;
         k_aks32_pad<<<(kg.ncol * nzp + 255) / 256, 256, 0, st>>>(kg.ncol, kg.nzl, nzp, kg.nrect, rs.aks, rs.aks2);
-        size_t smem2 = sizeof(float2) * KF_COLS * nzp;
         if (grad)
-            k_kfield32v2<1><<<g2, KF_THREADS, smem2, st>>>(n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp,
-                                                           L.cols_per_split, rs.aks2, rs.fpart);
+            k_kfield32v3<1><<<g2, KF_THREADS, sizeof(u64) * 6 * KF3_COLS * nzp, st>>>(
+                n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, rs.fpart);
         else
-            k_kfield32v2<0><<<g2, KF_THREADS, smem2, st>>>(n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp,
-                                                           L.cols_per_split, rs.aks2, rs.fpart);
+            k_kfield32v3<0><<<g2, KF_THREADS, sizeof(u64) * 4 * KF3_COLS * nzp, st>>>(
+                n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, rs.fpart);
+        nk += 2;
+        if (low) {
+            LowK& lk = rs.low;
+            if (grad)
+                k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+                    n, sx, sy, sz, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+            else
+                k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+                    n, sx, sy, sz, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+            nk++;
+        }
     } else {
-    size_t smem = sizeof(double) * 2 * KF_COLS * kg.nzl;
-    if (grad)
-        k_kfield<1><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
-                                                  rs.aks, kg.nrect, rs.fpart);
-    else
-        k_kfield<0><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
-                                                  rs.aks, kg.nrect, rs.fpart);
+        size_t smem = sizeof(double) * 2 * KF_COLS * kg.nzl;
+        if (grad)
+            k_kfield<1><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
+                                                      rs.aks, kg.nrect, rs.fpart);
+        else
+            k_kfield<0><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
+                                                      rs.aks, kg.nrect, rs.fpart);
+        nk++;
     }
     const double scale = 2.0 * 4.0 * PI / c.omega;
     k_kfield_reduce<<<(n + 255) / 256, 256, 0, st>>>(n, L.nsplit, grad ? 1 : 0, rs.fpart, scale, fl.with_q ? q : nullptr,
                                                     fl.with_mu ? mu : nullptr, fl.field ? ef : nullptr, efg,
-                                                    fl.forces ? fo : nullptr);
-    prof->end(mixed ? 3 : 2);
+                                                    fl.forces ? fo : nullptr, low ? rs.low.fpart : nullptr,
+                                                    low ? LK_SPLIT : 0);
+    prof->end(nk);
 }
 
 }  // namespace mdff

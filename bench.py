@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ncell", type=int, default=16)
+    ap.add_argument("--ext", default="aspc", choices=["aspc", "poly"],
+                    help="induced-dipole predictor (algo_ext_dipole)")
+    ap.add_argument("--ext-order", type=int, default=3, help="extrapolate_order of the predictor")
     ap.add_argument("--accuracy", action="store_true",
                     help="error of the mixed path against the FP64 path on snapshots of an FP64 trajectory")
     ap.add_argument("--snapshots", type=int, default=3)
@@ -141,6 +144,8 @@ def run_engine(args):
     p = s["params"]
     p.precision = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
     p.device = local
+    p.algo_ext_dipole = abi.EXT_ASPC if args.ext == "aspc" else abi.EXT_POLY
+    p.extrapolate_order = args.ext_order
     natm = len(s["itype"])
     eng = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
     eng.enable_profile(True)
@@ -222,6 +227,7 @@ def run_engine(args):
             "config": {"workload": "mgo-pim-production", "natm": natm, "kmax": list(p.kES), "nk_half": None,
                        "rc": p.cutlongrange, "alpha": p.alphaES, "ensemble": "nvt-nhcn", "nhc_n": p.nhc_n,
                        "dt_ps": p.dt, "efg_period": p.efg_period, "solver": "pcg", "tol": p.conv_tol_ind,
+                       "predictor": "%s order %d" % (args.ext, args.ext_order),
                        "precision": args.precision, "parallelism": f"replicas{world}",
                        "l2": "per-step working set > 126 MB L2 (k-space partials, Verlet lists)"},
             "gpu_launches": int(prof["_launches"]["count"]),

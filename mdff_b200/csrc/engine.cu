@@ -1173,7 +1173,7 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                         akhi[r] = 0.0;
                     }
                 }
-                long long thr = (long long)((lk.ncol + 127) / 128) * 128 * ((nzmax + 7) / 8);
+                long long thr = (long long)((lk.ncol + 127) / 128) * 128 * ((nzmax + 15) / 16);
                 int P = (int)std::max<long long>(1, (148LL * 1536 + thr - 1) / thr);
                 P = std::min(P, std::max(1, n / 32));
                 lk.natom_chunk = (n + P - 1) / P;
@@ -1187,6 +1187,7 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 TRY(dalloc(ctx, &lk.part, 2 * (size_t)lk.P * nzmax * lk.ncol));
                 TRY(dalloc(ctx, &lk.aks, 2 * (size_t)lk.ncol * nzmax));
                 TRY(dalloc(ctx, &lk.fpart, 4 * 9 * (size_t)n));
+                TRY(dalloc(ctx, &lk.tab, 16 * (size_t)n));
                 TRY(dalloc(ctx, &kg.Ak_hi, kg.nrect));
                 TRY(upload(ctx, kg.Ak_hi, akhi.data(), kg.nrect));
             }

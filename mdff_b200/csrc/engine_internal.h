@@ -199,7 +199,8 @@ struct LowK {
     double* kcoe = nullptr;
     double* part = nullptr;   // pass-1 partials [2][P][nzmax][ncol]
     double* aks = nullptr;    // [2][ncol][nzmax]
-    double* fpart = nullptr;  // [9][n]
+    double* fpart = nullptr;  // [LK_SPLIT][9][n]
+    double2* tab = nullptr;   // [n][16] e^{2 pi i m s_z} in FP64
     int P = 1, natom_chunk = 0;
 };
 

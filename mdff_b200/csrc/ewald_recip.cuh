@@ -280,7 +280,8 @@ constexpr int TM = 16;     // table length = nz chunk of both passes
 
 // Per-atom phase table T_m, fixed-point coordinates.
 __global__ void k_phase_table(int n, const double* __restrict__ sx, const double* __restrict__ sy,
-                              const double* __restrict__ sz, uint32_t* __restrict__ fx, float2* __restrict__ tab) {
+                              const double* __restrict__ sz, uint32_t* __restrict__ fx, float2* __restrict__ tab,
+                              double2* __restrict__ tab64) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double s[3] = {sx[i], sy[i], sz[i]};
@@ -298,6 +299,7 @@ __global__ void k_phase_table(int n, const double* __restrict__ sx, const double
         double sn, cs;
         sincospi(2.0 * t, &sn, &cs);
         tab[(size_t)i * TM + m] = make_float2((float)cs, (float)sn);
+        if (tab64) tab64[(size_t)i * TM + m] = make_double2(cs, sn);
     }
 }
 
@@ -315,39 +317,21 @@ __global__ void k_aks32_pad(int ncol, int nzl, int nzp, int nrect, const double*
     out[t] = v;
 }
 
-typedef unsigned long long u64;
-
-__device__ __forceinline__ u64 pk2(float a, float b) {
-    u64 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ float2 upk2(u64 v) {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-    return make_float2(a, b);
-}
-__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
-    u64 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-
-constexpr int SF3_TILE = 32;
+constexpr int SF4_TILE = 32;
 
 // Pass 1: thread = (column, chunk of TM nz values).  Atom t contributes
 // sum_m (w0 + m dw) T_m with w0 = (q + i k0.mu) e0 and dw = i (2 pi b3.mu) e0.
-// Packed: acc_m += (wr,wr)(Tx,Ty) + (wi,wi)(-Ty,Tx).
+// FP32 sums over a tile of atoms are added into FP32 block sums (a two-level
+// tree, at most a few dozen tiles per block) and written as FP64 partials.
 template <int WITH_MU>
-__global__ void __launch_bounds__(SF_THREADS) k_sfac32v3(int n, int natom_chunk, const uint32_t* __restrict__ fx,
+__global__ void __launch_bounds__(SF_THREADS) k_sfac32v4(int n, int natom_chunk, const uint32_t* __restrict__ fx,
                                                          const float2* __restrict__ tab, const double* __restrict__ q,
                                                          const double* __restrict__ mu, CellP c, int kx, int ky, int kz,
                                                          int ncol, int ncolblk, int nchunk, int with_q,
                                                          double* __restrict__ part_re, double* __restrict__ part_im) {
-    __shared__ uint32_t t_u1[SF3_TILE], t_u2[SF3_TILE], t_u3[SF3_TILE];
-    __shared__ float t_q[SF3_TILE], t_m1[SF3_TILE], t_m2[SF3_TILE], t_m3[SF3_TILE];
-    __shared__ u64 t_T[SF3_TILE][TM];    // (Tx, Ty)
-    __shared__ u64 t_iT[SF3_TILE][TM];   // (-Ty, Tx) = i T
+    __shared__ uint32_t t_u1[SF4_TILE], t_u2[SF4_TILE], t_u3[SF4_TILE];
+    __shared__ float t_q[SF4_TILE], t_m1[SF4_TILE], t_m2[SF4_TILE], t_m3[SF4_TILE];
+    __shared__ float4 t_T[SF4_TILE][TM / 2];    // (T_m, T_m+1) pairs
     const int h = blockIdx.x / ncolblk;
     const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
     const int p = blockIdx.y;
@@ -355,25 +339,22 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac32v3(int n, int natom_chunk,
     const int colc = col < ncol ? col : ncol - 1;
     const int inx = colc / ny_n, iny = colc % ny_n - ky, inz0 = -kz + h * TM;
     const float fnx = (float)inx, fny = (float)iny, fnz0 = (float)inz0;
-    u64 MM[TM];
+    float ore[TM], oim[TM];
 #pragma unroll
-    for (int m = 0; m < TM; ++m) MM[m] = pk2((float)m, (float)m);
-    double dre[TM], dim[TM];
-#pragma unroll
-    for (int m = 0; m < TM; ++m) { dre[m] = 0.0; dim[m] = 0.0; }
+    for (int m = 0; m < TM; ++m) { ore[m] = 0.f; oim[m] = 0.f; }
     const int a0 = p * natom_chunk;
     const int a1 = min(n, a0 + natom_chunk);
-    for (int base = a0; base < a1; base += SF3_TILE) {
+    for (int base = a0; base < a1; base += SF4_TILE) {
         __syncthreads();
-        for (int t = threadIdx.x; t < SF3_TILE * TM; t += blockDim.x) {
-            int ia = base + t / TM;
+        for (int t = threadIdx.x; t < SF4_TILE * (TM / 2); t += blockDim.x) {
+            int ia = base + t / (TM / 2);
             if (ia < a1) {
-                float2 T = tab[(size_t)ia * TM + (t % TM)];
-                t_T[t / TM][t % TM] = pk2(T.x, T.y);
-                t_iT[t / TM][t % TM] = pk2(-T.y, T.x);
+                const float2* src = tab + (size_t)ia * TM + 2 * (t % (TM / 2));
+                float2 A = src[0], B = src[1];
+                t_T[t / (TM / 2)][t % (TM / 2)] = make_float4(A.x, A.y, B.x, B.y);
             }
         }
-        if (threadIdx.x < SF3_TILE) {
+        if (threadIdx.x < SF4_TILE) {
             int ia = base + threadIdx.x;
             if (ia < a1) {
                 t_u1[threadIdx.x] = fx[ia];
@@ -388,74 +369,68 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac32v3(int n, int natom_chunk,
             }
         }
         __syncthreads();
-        const int tn = min(SF3_TILE, a1 - base);
-        u64 acc[TM];
+        const int tn = min(SF4_TILE, a1 - base);
+        float are[TM], aim[TM];
 #pragma unroll
-        for (int m = 0; m < TM; ++m) acc[m] = 0ull;
+        for (int m = 0; m < TM; ++m) { are[m] = 0.f; aim[m] = 0.f; }
         for (int t = 0; t < tn; ++t) {
             const uint32_t ph = (uint32_t)inx * t_u1[t] + (uint32_t)iny * t_u2[t] + (uint32_t)inz0 * t_u3[t];
             float c0, s0;
             phase32(ph, c0, s0);
             const float qa = t_q[t];
+            float w0r, w0i, dwr = 0.f, dwi = 0.f;
             if (WITH_MU) {
                 const float km = fmaf(fnx, t_m1[t], fmaf(fny, t_m2[t], fnz0 * t_m3[t]));
                 const float m3 = t_m3[t];
-                const float w0r = fmaf(qa, c0, -km * s0), w0i = fmaf(qa, s0, km * c0);
-                const u64 W0R = pk2(w0r, w0r), W0I = pk2(w0i, w0i);
-                const u64 DWR = pk2(-m3 * s0, -m3 * s0), DWI = pk2(m3 * c0, m3 * c0);
-#pragma unroll
-                for (int m = 0; m < TM; ++m) {
-                    const u64 WR = fma2(MM[m], DWR, W0R);
-                    const u64 WI = fma2(MM[m], DWI, W0I);
-                    acc[m] = fma2(WR, t_T[t][m], acc[m]);
-                    acc[m] = fma2(WI, t_iT[t][m], acc[m]);
-                }
+                w0r = fmaf(qa, c0, -km * s0);
+                w0i = fmaf(qa, s0, km * c0);
+                dwr = -m3 * s0;
+                dwi = m3 * c0;
             } else {
-                const float w0r = qa * c0, w0i = qa * s0;
-                const u64 WR = pk2(w0r, w0r), WI = pk2(w0i, w0i);
+                w0r = qa * c0;
+                w0i = qa * s0;
+            }
 #pragma unroll
-                for (int m = 0; m < TM; ++m) {
-                    acc[m] = fma2(WR, t_T[t][m], acc[m]);
-                    acc[m] = fma2(WI, t_iT[t][m], acc[m]);
+            for (int m2 = 0; m2 < TM / 2; ++m2) {
+                const float4 TT = t_T[t][m2];
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int m = 2 * m2 + j;
+                    const float tx = j ? TT.z : TT.x, ty = j ? TT.w : TT.y;
+                    const float wr = WITH_MU ? fmaf((float)m, dwr, w0r) : w0r;
+                    const float wi = WITH_MU ? fmaf((float)m, dwi, w0i) : w0i;
+                    are[m] = fmaf(wr, tx, fmaf(-wi, ty, are[m]));
+                    aim[m] = fmaf(wr, ty, fmaf(wi, tx, aim[m]));
                 }
             }
         }
 #pragma unroll
-        for (int m = 0; m < TM; ++m) {
-            float2 v = upk2(acc[m]);
-            dre[m] += (double)v.x;
-            dim[m] += (double)v.y;
-        }
+        for (int m = 0; m < TM; ++m) { ore[m] += are[m]; oim[m] += aim[m]; }
     }
     if (col < ncol) {
         const size_t plane = (size_t)ncol * TM * nchunk;
 #pragma unroll
         for (int m = 0; m < TM; ++m) {
             size_t idx = (size_t)p * plane + ((size_t)h * TM + m) * ncol + col;
-            part_re[idx] = dre[m];
-            part_im[idx] = dim[m];
+            part_re[idx] = (double)ore[m];
+            part_im[idx] = (double)oim[m];
         }
     }
 }
 
 // Pass 2: thread = atom.  Per chunk of TM k-vectors along nz,
-//   Z_j = sum_m m^j conj(A_k S)_m T_m    (j = 0, 1 [, 2 for the gradient])
-// in packed FMAs: conj(a) T = (ar,ar)(Tx,Ty) + (ai,-ai)(Ty,Tx).  With the
-// chunk's base phase e0 and k_m = kb + m dk:
+//   Z_j = sum_m m^j conj(A_k S)_m T_m    (j = 0, 1 [, 2 for the gradient]),
+// then with the chunk's base phase e0 and k_m = kb + m dk:
 //   sum_m k_m recarg_m = -(kb Im(e0 Z0) + dk Im(e0 Z1)),
 //   sum_m k_m k_m^T recarg2_m = kb kb^T Re(e0 Z0) + (kb dk^T + dk kb^T) Re(e0 Z1) + dk dk^T Re(e0 Z2).
 // The column's base phase is computed once; chunk bases follow by
-// multiplication with e^{2 pi i 16 s_z}.  The shared-memory k data holds, per
-// k, (ar,ar),(ai,-ai) and the m- (and m^2-) weighted copies.
-constexpr int KF3_COLS = 4;
-
+// multiplication with e^{2 pi i 16 s_z}.  The chunk sums go to FP64.
 template <int GRAD>
-__global__ void __launch_bounds__(KF_THREADS) k_kfield32v3(int n, const uint32_t* __restrict__ fx,
+__global__ void __launch_bounds__(KF_THREADS) k_kfield32v4(int n, const uint32_t* __restrict__ fx,
                                                            const float2* __restrict__ tab, CellP c, int kx, int ky,
                                                            int kz, int ncol, int nzp, int cols_per_split,
                                                            const float2* __restrict__ aks, double* __restrict__ fpart) {
-    extern __shared__ u64 skd[];
-    constexpr int NW = GRAD ? 6 : 4;     // packed words per k
+    extern __shared__ float2 ska[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int split = blockIdx.y;
     const int c0 = split * cols_per_split;
@@ -463,37 +438,21 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v3(int n, const uint32_t
     const bool active = i < n;
     const int ii = active ? i : 0;
     const uint32_t u1 = fx[ii], u2 = fx[n + ii], u3 = fx[2 * n + ii];
-    u64 T[TM], Ts[TM];
+    float2 T[TM];
 #pragma unroll
-    for (int m = 0; m < TM; ++m) {
-        float2 t = tab[(size_t)ii * TM + m];
-        T[m] = pk2(t.x, t.y);
-        Ts[m] = pk2(t.y, t.x);
-    }
-    // e^{2 pi i 16 s_z} from the fixed-point coordinate (exact phase)
+    for (int m = 0; m < TM; ++m) T[m] = tab[(size_t)ii * TM + m];
     float e16c, e16s;
     phase32(u3 * 16u, e16c, e16s);
-    const double dkx = 2.0 * PI * c.B[2], dky = 2.0 * PI * c.B[5], dkz = 2.0 * PI * c.B[8];
-    const float dk0 = (float)dkx, dk1 = (float)dky, dk2 = (float)dkz;
+    const float b1x = (float)(2.0 * PI * c.B[0]), b1y = (float)(2.0 * PI * c.B[3]), b1z = (float)(2.0 * PI * c.B[6]);
+    const float b2x = (float)(2.0 * PI * c.B[1]), b2y = (float)(2.0 * PI * c.B[4]), b2z = (float)(2.0 * PI * c.B[7]);
+    const float dk0 = (float)(2.0 * PI * c.B[2]), dk1 = (float)(2.0 * PI * c.B[5]), dk2 = (float)(2.0 * PI * c.B[8]);
     const int ny_n = 2 * ky + 1;
     double E0 = 0, E1 = 0, E2 = 0;
     double G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
-    for (int cb = c0; cb < c1; cb += KF3_COLS) {
-        const int nc = min(KF3_COLS, c1 - cb);
+    for (int cb = c0; cb < c1; cb += KF_COLS) {
+        const int nc = min(KF_COLS, c1 - cb);
         __syncthreads();
-        for (int t = threadIdx.x; t < nc * nzp; t += blockDim.x) {
-            const float2 a = aks[(size_t)cb * nzp + t];
-            const float m = (float)(t % TM);
-            u64* o = skd + (size_t)t * NW;
-            o[0] = pk2(a.x, a.x);
-            o[1] = pk2(a.y, -a.y);
-            o[2] = pk2(m * a.x, m * a.x);
-            o[3] = pk2(m * a.y, -m * a.y);
-            if (GRAD) {
-                o[4] = pk2(m * m * a.x, m * m * a.x);
-                o[5] = pk2(m * m * a.y, -m * m * a.y);
-            }
-        }
+        for (int t = threadIdx.x; t < nc * nzp; t += blockDim.x) ska[t] = aks[(size_t)cb * nzp + t];
         __syncthreads();
         for (int cc = 0; cc < nc; ++cc) {
             const int col = cb + cc;
@@ -501,34 +460,30 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v3(int n, const uint32_t
             const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)(-kz) * u3;
             float ec, es;
             phase32(ph, ec, es);
-            float kb0 = (float)(2.0 * PI * (inx * c.B[0] + iny * c.B[1]) - kz * dkx);
-            float kb1 = (float)(2.0 * PI * (inx * c.B[3] + iny * c.B[4]) - kz * dky);
-            float kb2 = (float)(2.0 * PI * (inx * c.B[6] + iny * c.B[7]) - kz * dkz);
-            const u64* kd = skd + (size_t)cc * nzp * NW;
+            const float fnx = (float)inx, fny = (float)iny, fnz = (float)(-kz);
+            float kb0 = fmaf(fnx, b1x, fmaf(fny, b2x, fnz * dk0));
+            float kb1 = fmaf(fnx, b1y, fmaf(fny, b2y, fnz * dk1));
+            float kb2 = fmaf(fnx, b1z, fmaf(fny, b2z, fnz * dk2));
+            const float2* pk = ska + cc * nzp;
             for (int m0 = 0; m0 < nzp; m0 += TM) {
-                u64 Z0 = 0ull, Z1 = 0ull, Z2 = 0ull;
+                float z0r = 0.f, z0i = 0.f, z1r = 0.f, z1i = 0.f, z2r = 0.f, z2i = 0.f;
 #pragma unroll
                 for (int m = 0; m < TM; ++m) {
-                    const u64* w = kd + (size_t)(m0 + m) * NW;
-                    Z0 = fma2(w[0], T[m], Z0);
-                    Z0 = fma2(w[1], Ts[m], Z0);
-                    Z1 = fma2(w[2], T[m], Z1);
-                    Z1 = fma2(w[3], Ts[m], Z1);
-                    if (GRAD) {
-                        Z2 = fma2(w[4], T[m], Z2);
-                        Z2 = fma2(w[5], Ts[m], Z2);
-                    }
+                    const float2 a = pk[m0 + m];
+                    // conj(a) T_m
+                    const float pr = fmaf(a.x, T[m].x, a.y * T[m].y);
+                    const float pi = fmaf(a.x, T[m].y, -a.y * T[m].x);
+                    z0r += pr; z0i += pi;
+                    z1r = fmaf((float)m, pr, z1r); z1i = fmaf((float)m, pi, z1i);
+                    if (GRAD) { z2r = fmaf((float)(m * m), pr, z2r); z2i = fmaf((float)(m * m), pi, z2i); }
                 }
-                const float2 z0 = upk2(Z0), z1 = upk2(Z1);
-                // e0 * Z: real and imaginary parts
-                const float p0r = fmaf(ec, z0.x, -es * z0.y), p0i = fmaf(ec, z0.y, es * z0.x);
-                const float p1r = fmaf(ec, z1.x, -es * z1.y), p1i = fmaf(ec, z1.y, es * z1.x);
+                const float p0r = fmaf(ec, z0r, -es * z0i), p0i = fmaf(ec, z0i, es * z0r);
+                const float p1r = fmaf(ec, z1r, -es * z1i), p1i = fmaf(ec, z1i, es * z1r);
                 E0 += (double)fmaf(kb0, p0i, dk0 * p1i);
                 E1 += (double)fmaf(kb1, p0i, dk1 * p1i);
                 E2 += (double)fmaf(kb2, p0i, dk2 * p1i);
                 if (GRAD) {
-                    const float2 z2 = upk2(Z2);
-                    const float p2r = fmaf(ec, z2.x, -es * z2.y);
+                    const float p2r = fmaf(ec, z2r, -es * z2i);
                     G0 += (double)(kb0 * kb0 * p0r + 2.f * kb0 * dk0 * p1r + dk0 * dk0 * p2r);
                     G1 += (double)(kb1 * kb1 * p0r + 2.f * kb1 * dk1 * p1r + dk1 * dk1 * p2r);
                     G2 += (double)(kb2 * kb2 * p0r + 2.f * kb2 * dk2 * p1r + dk2 * dk2 * p2r);
@@ -536,7 +491,6 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v3(int n, const uint32_t
                     G4 += (double)(kb0 * kb2 * p0r + (kb0 * dk2 + dk0 * kb2) * p1r + dk0 * dk2 * p2r);
                     G5 += (double)(kb1 * kb2 * p0r + (kb1 * dk2 + dk1 * kb2) * p1r + dk1 * dk2 * p2r);
                 }
-                // next chunk: e0 *= e^{2 pi i 16 s_z}, kb += 16 dk
                 const float nc_ = fmaf(ec, e16c, -es * e16s);
                 es = fmaf(es, e16c, ec * e16s);
                 ec = nc_;
@@ -564,72 +518,77 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v3(int n, const uint32_t
 // from the FP32 set.  The list is stored as columns (nx, ny) with a
 // contiguous nz range [nzlo, nzlo + nzn).
 
-constexpr int LK_CH = 8;
 constexpr int LK_SPLIT = 4;   // column splits of the low-|k| field pass
 
-__global__ void __launch_bounds__(SF_THREADS) k_sfac64_low(int n, int natom_chunk, const double* __restrict__ sx,
-                                                           const double* __restrict__ sy, const double* __restrict__ sz,
-                                                           const double* __restrict__ q, const double* __restrict__ mu,
-                                                           CellP c, const int* __restrict__ cols, int ncol, int nzmax,
-                                                           int nchunk, int with_q, int with_mu,
-                                                           double* __restrict__ part_re, double* __restrict__ part_im) {
-    __shared__ double t_s1[SF_TILE], t_s2[SF_TILE], t_s3[SF_TILE], t_q[SF_TILE];
-    __shared__ double t_m1[SF_TILE], t_m2[SF_TILE], t_m3[SF_TILE], t_cs[SF_TILE], t_sn[SF_TILE];
+// Pass 1 over the low set: thread = (list column, chunk of TM nz).  Same
+// scheme as the FP32 pass (exact fixed-point base phase, per-atom table T_m),
+// in FP64.
+constexpr int LK_TILE = 32;
+__global__ void __launch_bounds__(SF_THREADS) k_sfac64_low(int n, int natom_chunk, const uint32_t* __restrict__ fx,
+                                                           const double2* __restrict__ tab, const double* __restrict__ q,
+                                                           const double* __restrict__ mu, CellP c,
+                                                           const int* __restrict__ cols, int ncol, int nzmax, int nchunk,
+                                                           int with_q, int with_mu, double* __restrict__ part_re,
+                                                           double* __restrict__ part_im) {
+    __shared__ uint32_t t_u1[LK_TILE], t_u2[LK_TILE], t_u3[LK_TILE];
+    __shared__ double t_q[LK_TILE], t_m1[LK_TILE], t_m2[LK_TILE], t_m3[LK_TILE];
+    __shared__ double2 t_T[LK_TILE][TM];
     const int h = blockIdx.x % nchunk;
     const int cidx = (blockIdx.x / nchunk) * SF_THREADS + threadIdx.x;
     const int p = blockIdx.y;
     const int cc = cidx < ncol ? cidx : ncol - 1;
-    const double nx = (double)cols[4 * cc], ny = (double)cols[4 * cc + 1];
-    const double nz0 = (double)(cols[4 * cc + 2] + h * LK_CH);
-    double are[LK_CH], aim[LK_CH];
+    const int inx = cols[4 * cc], iny = cols[4 * cc + 1], inz0 = cols[4 * cc + 2] + h * TM;
+    const double fnx = inx, fny = iny, fnz0 = inz0;
+    double are[TM], aim[TM];
 #pragma unroll
-    for (int m = 0; m < LK_CH; ++m) { are[m] = 0.0; aim[m] = 0.0; }
+    for (int m = 0; m < TM; ++m) { are[m] = 0.0; aim[m] = 0.0; }
     const int a0 = p * natom_chunk;
     const int a1 = min(n, a0 + natom_chunk);
-    for (int base = a0; base < a1; base += SF_TILE) {
+    for (int base = a0; base < a1; base += LK_TILE) {
         __syncthreads();
-        if (threadIdx.x < SF_TILE) {
+        for (int t = threadIdx.x; t < LK_TILE * TM; t += blockDim.x) {
+            int ia = base + t / TM;
+            if (ia < a1) t_T[t / TM][t % TM] = tab[(size_t)ia * TM + (t % TM)];
+        }
+        if (threadIdx.x < LK_TILE) {
             int ia = base + threadIdx.x;
             if (ia < a1) {
-                double s1 = sx[ia], s2 = sy[ia], s3 = sz[ia];
-                t_s1[threadIdx.x] = s1; t_s2[threadIdx.x] = s2; t_s3[threadIdx.x] = s3;
+                t_u1[threadIdx.x] = fx[ia];
+                t_u2[threadIdx.x] = fx[n + ia];
+                t_u3[threadIdx.x] = fx[2 * n + ia];
                 t_q[threadIdx.x] = with_q ? q[ia] : 0.0;
                 double m0 = 0, m1 = 0, m2 = 0;
                 if (with_mu) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
                 t_m1[threadIdx.x] = 2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2);
                 t_m2[threadIdx.x] = 2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2);
                 t_m3[threadIdx.x] = 2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2);
-                double sn, cs;
-                sincospi(2.0 * (s3 - rint(s3)), &sn, &cs);
-                t_cs[threadIdx.x] = cs; t_sn[threadIdx.x] = sn;
             }
         }
         __syncthreads();
-        const int tn = min(SF_TILE, a1 - base);
+        const int tn = min(LK_TILE, a1 - base);
         for (int t = 0; t < tn; ++t) {
-            double ph = fma(nx, t_s1[t], fma(ny, t_s2[t], nz0 * t_s3[t]));
-            ph -= rint(ph);
-            double sn, cs;
-            sincospi(2.0 * ph, &sn, &cs);
+            const uint32_t ph = (uint32_t)inx * t_u1[t] + (uint32_t)iny * t_u2[t] + (uint32_t)inz0 * t_u3[t];
+            double s0, c0;
+            sincospi((double)(int)ph * 4.656612873077393e-10, &s0, &c0);   // 2 pi t, t = ph / 2^32
             const double qa = t_q[t];
-            double km = fma(nx, t_m1[t], fma(ny, t_m2[t], nz0 * t_m3[t]));
-            const double dm = t_m3[t], rc = t_cs[t], rs = t_sn[t];
+            const double km = fma(fnx, t_m1[t], fma(fny, t_m2[t], fnz0 * t_m3[t]));
+            const double m3 = t_m3[t];
+            const double w0r = fma(qa, c0, -km * s0), w0i = fma(qa, s0, km * c0);
+            const double dwr = -m3 * s0, dwi = m3 * c0;
 #pragma unroll
-            for (int m = 0; m < LK_CH; ++m) {
-                are[m] = fma(qa, cs, fma(-km, sn, are[m]));
-                aim[m] = fma(qa, sn, fma(km, cs, aim[m]));
-                const double cn = cs * rc - sn * rs;
-                sn = fma(sn, rc, cs * rs);
-                cs = cn;
-                km += dm;
+            for (int m = 0; m < TM; ++m) {
+                const double wr = fma((double)m, dwr, w0r), wi = fma((double)m, dwi, w0i);
+                const double2 T = t_T[t][m];
+                are[m] = fma(wr, T.x, fma(-wi, T.y, are[m]));
+                aim[m] = fma(wr, T.y, fma(wi, T.x, aim[m]));
             }
         }
     }
     if (cidx < ncol) {
         const size_t plane = (size_t)nzmax * ncol;
 #pragma unroll
-        for (int m = 0; m < LK_CH; ++m) {
-            int mz = h * LK_CH + m;
+        for (int m = 0; m < TM; ++m) {
+            int mz = h * TM + m;
             if (mz < nzmax) {
                 size_t idx = (size_t)p * plane + (size_t)mz * ncol + cidx;
                 part_re[idx] = are[m];
@@ -639,20 +598,27 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac64_low(int n, int natom_chun
     }
 }
 
+// One warp per low-set k-vector: sum of the atom-chunk partials, A_k S(k),
+// energy and stress terms.
 __global__ void k_sfac64_low_reduce(int P, int ncol, int nzmax, const int* __restrict__ cols,
                                     const double* __restrict__ part_re, const double* __restrict__ part_im,
                                     const double* __restrict__ Ak, const double* __restrict__ kcoe, CellP c,
                                     double* __restrict__ aks, int energy, double* partials) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     double v[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (t < ncol * nzmax) {
-        const int cidx = t % ncol, mz = t / ncol;
-        const size_t plane = (size_t)nzmax * ncol;
-        double sr = 0.0, si = 0.0;
-        for (int p = 0; p < P; ++p) {
+    const bool valid = t < ncol * nzmax;
+    const int cidx = valid ? t % ncol : 0, mz = valid ? t / ncol : 0;
+    const size_t plane = (size_t)nzmax * ncol;
+    double sr = 0.0, si = 0.0;
+    if (valid)
+        for (int p = lane; p < P; p += 32) {
             sr += part_re[(size_t)p * plane + (size_t)mz * ncol + cidx];
             si += part_im[(size_t)p * plane + (size_t)mz * ncol + cidx];
         }
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    if (valid && lane == 0) {
         const size_t r = (size_t)cidx * nzmax + mz;
         const double ak = (mz < cols[4 * cidx + 3]) ? Ak[r] : 0.0;
         aks[r] = ak * sr;
@@ -676,12 +642,14 @@ __global__ void k_sfac64_low_reduce(int P, int ncol, int nzmax, const int* __res
     if (energy) block_partials<7>(v, partials);
 }
 
-// Pass 2 over the low set: thread = atom, every column of the list; written
-// (not accumulated) into fpart[9][n] (E and, with GRAD, the field gradient).
+// Pass 2 over the low set: thread = atom, blockIdx.y = range of list columns.
+// Along a column the phase advances by the per-atom FP64 step e^{2 pi i s_z};
+// the k-vector is applied once per column through the moments
+// R0 = sum r_m, R1 = sum m r_m (Q0..Q2 for the field gradient).
 template <int GRAD>
-__global__ void __launch_bounds__(KF_THREADS) k_kfield64_low(int n, const double* __restrict__ sx,
-                                                             const double* __restrict__ sy, const double* __restrict__ sz,
-                                                             CellP c, const int* __restrict__ cols, int ncol, int nzmax,
+__global__ void __launch_bounds__(KF_THREADS) k_kfield64_low(int n, const uint32_t* __restrict__ fx,
+                                                             const double2* __restrict__ tab, CellP c,
+                                                             const int* __restrict__ cols, int ncol, int nzmax,
                                                              const double* __restrict__ aks, double* __restrict__ fpart) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int per = (ncol + gridDim.y - 1) / gridDim.y;
@@ -689,40 +657,49 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield64_low(int n, const double
     fpart += (size_t)blockIdx.y * 9 * n;
     const bool active = i < n;
     const int ii = active ? i : 0;
-    const double s1 = sx[ii], s2 = sy[ii], s3 = sz[ii];
-    double rs, rc;
-    sincospi(2.0 * (s3 - rint(s3)), &rs, &rc);
+    const uint32_t u1 = fx[ii], u2 = fx[n + ii], u3 = fx[2 * n + ii];
+    const double2 st = tab[(size_t)ii * TM + 1];   // e^{2 pi i s_z}
+    const double rc = st.x, rs = st.y;
     const double dk0 = 2.0 * PI * c.B[2], dk1 = 2.0 * PI * c.B[5], dk2 = 2.0 * PI * c.B[8];
     double E0 = 0, E1 = 0, E2 = 0, G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
     const double* aim_base = aks + (size_t)ncol * nzmax;
     for (int cc = cbeg; cc < cend; ++cc) {
-        const double nx = cols[4 * cc], ny = cols[4 * cc + 1], nz0 = cols[4 * cc + 2];
+        const int inx = cols[4 * cc], iny = cols[4 * cc + 1], inz0 = cols[4 * cc + 2];
         const int nzn = cols[4 * cc + 3];
-        double ph = fma(nx, s1, fma(ny, s2, nz0 * s3));
-        ph -= rint(ph);
+        const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)inz0 * u3;
         double sn, cs;
-        sincospi(2.0 * ph, &sn, &cs);
-        double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz0 * c.B[2]);
-        double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz0 * c.B[5]);
-        double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz0 * c.B[8]);
+        sincospi((double)(int)ph * 4.656612873077393e-10, &sn, &cs);
+        const double kb0 = 2.0 * PI * (inx * c.B[0] + iny * c.B[1] + inz0 * c.B[2]);
+        const double kb1 = 2.0 * PI * (inx * c.B[3] + iny * c.B[4] + inz0 * c.B[5]);
+        const double kb2 = 2.0 * PI * (inx * c.B[6] + iny * c.B[7] + inz0 * c.B[8]);
         const double* pr = aks + (size_t)cc * nzmax;
         const double* pi = aim_base + (size_t)cc * nzmax;
+        double R0 = 0, R1 = 0, Q0 = 0, Q1 = 0, Q2 = 0;
         for (int m = 0; m < nzn; ++m) {
             const double ar = __ldg(pr + m), ai = __ldg(pi + m);
-            const double recarg = ai * cs - ar * sn;
-            E0 = fma(-k0, recarg, E0);
-            E1 = fma(-k1, recarg, E1);
-            E2 = fma(-k2, recarg, E2);
+            const double r = ai * cs - ar * sn;
+            R0 += r;
+            R1 = fma((double)m, r, R1);
             if (GRAD) {
                 const double r2 = ar * cs + ai * sn;
-                const double a0 = k0 * r2, a1 = k1 * r2;
-                G0 = fma(k0, a0, G0); G1 = fma(k1, a1, G1); G2 = fma(k2, k2 * r2, G2);
-                G3 = fma(k1, a0, G3); G4 = fma(k2, a0, G4); G5 = fma(k2, a1, G5);
+                Q0 += r2;
+                Q1 = fma((double)m, r2, Q1);
+                Q2 = fma((double)(m * m), r2, Q2);
             }
             const double cn = cs * rc - sn * rs;
             sn = fma(sn, rc, cs * rs);
             cs = cn;
-            k0 += dk0; k1 += dk1; k2 += dk2;
+        }
+        E0 -= fma(kb0, R0, dk0 * R1);
+        E1 -= fma(kb1, R0, dk1 * R1);
+        E2 -= fma(kb2, R0, dk2 * R1);
+        if (GRAD) {
+            G0 += kb0 * kb0 * Q0 + 2.0 * kb0 * dk0 * Q1 + dk0 * dk0 * Q2;
+            G1 += kb1 * kb1 * Q0 + 2.0 * kb1 * dk1 * Q1 + dk1 * dk1 * Q2;
+            G2 += kb2 * kb2 * Q0 + 2.0 * kb2 * dk2 * Q1 + dk2 * dk2 * Q2;
+            G3 += kb0 * kb1 * Q0 + (kb0 * dk1 + dk0 * kb1) * Q1 + dk0 * dk1 * Q2;
+            G4 += kb0 * kb2 * Q0 + (kb0 * dk2 + dk0 * kb2) * Q1 + dk0 * dk2 * Q2;
+            G5 += kb1 * kb2 * Q0 + (kb1 * dk2 + dk1 * kb2) * Q1 + dk1 * dk2 * Q2;
         }
     }
     if (active) {
@@ -783,16 +760,17 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     int nk = 2 + (fl.energy ? 1 : 0);
     if (mixed) {
         if (rs.tab_epoch != rs.want_epoch) {
-            k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab);
+            k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab,
+                                                           rs.low.ncol > 0 ? rs.low.tab : nullptr);
             rs.tab_epoch = rs.want_epoch;
             nk++;
         }
         dim3 g1(nchunk32 * L.ncolblk, L.P);
         if (fl.with_mu)
-            k_sfac32v3<1><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
+            k_sfac32v4<1><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
                                                      L.ncolblk, nchunk32, fl.with_q, pre, pim);
         else
-            k_sfac32v3<0><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
+            k_sfac32v4<0><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
                                                      L.ncolblk, nchunk32, fl.with_q, pre, pim);
         // the FP32 set excludes the low-|k| vectors (A_k = 0 there)
         k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, TM, nchunk32, kg.ncol, kg.nzl, kx, ky, kz, pre, pim,
@@ -811,13 +789,13 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     if (fl.energy) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
     if (low) {
         LowK& lk = rs.low;
-        const int nch = (lk.nzmax + LK_CH - 1) / LK_CH;
+        const int nch = (lk.nzmax + TM - 1) / TM;
         const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;
         dim3 gl(nch * cb, lk.P);
         const size_t lplane = (size_t)lk.P * lk.nzmax * lk.ncol;
-        k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, sx, sy, sz, q, mu, c, lk.col, lk.ncol, lk.nzmax, nch,
-                                                fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
-        const int lb = (lk.ncol * lk.nzmax + 255) / 256;
+        k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, rs.fixed, lk.tab, q, mu, c, lk.col, lk.ncol, lk.nzmax,
+                                                nch, fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
+        const int lb = (lk.ncol * lk.nzmax * 32 + 255) / 256;
         k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane, lk.Ak,
                                                 lk.kcoe, c, lk.aks, fl.energy, part.buf);
         if (fl.energy) launch_reduce_partials(st, part.buf, lb, 7, d->rec, 1);
@@ -833,20 +811,20 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         const int nzp = nchunk32 * TM;
         k_aks32_pad<<<(kg.ncol * nzp + 255) / 256, 256, 0, st>>>(kg.ncol, kg.nzl, nzp, kg.nrect, rs.aks, rs.aks2);
         if (grad)
-            k_kfield32v3<1><<<g2, KF_THREADS, sizeof(u64) * 6 * KF3_COLS * nzp, st>>>(
+            k_kfield32v4<1><<<g2, KF_THREADS, sizeof(float2) * KF_COLS * nzp, st>>>(
                 n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, rs.fpart);
         else
-            k_kfield32v3<0><<<g2, KF_THREADS, sizeof(u64) * 4 * KF3_COLS * nzp, st>>>(
+            k_kfield32v4<0><<<g2, KF_THREADS, sizeof(float2) * KF_COLS * nzp, st>>>(
                 n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, rs.fpart);
         nk += 2;
         if (low) {
             LowK& lk = rs.low;
             if (grad)
                 k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, sx, sy, sz, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
             else
                 k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, sx, sy, sz, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
             nk++;
         }
     } else {

@@ -160,9 +160,31 @@ typedef struct mdff_thermo {
     double scf_rmsd;
 } mdff_thermo;
 
-/* sizeof(mdff_params), sizeof(mdff_energies), sizeof(mdff_thermo) for
- * which = 0, 1, 2 (lets a binding check its mirror of these structs); no
- * reference counterpart. */
+/* Derivative of a scalar loss with respect to the force-field tables (no
+ * reference counterpart; the reference has no derivatives).  Layout mirrors
+ * the tables of mdff_params.  The tables are taken as symmetric in their pair
+ * indices (symmetric_pot): the derivative with respect to an unordered entry
+ * {a,b} is returned in the upper-triangle slot [a][b] with a <= b (for the
+ * damping tables [p][a][b] with a <= b), and the lower-triangle slots are 0.
+ * Bbmhftd is the inverse range 1/rho as in the reference
+ * (src/field.f90:2952); d/d(rho) = -B^2 d/dB. */
+typedef struct mdff_param_grad {
+    double Abmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double Bbmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double Cbmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double Dbmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double BDbmhftd[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double epsmor[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double sigmamor[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double rhomor[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double poldip_iso[MDFF_NTYPE_MAX];
+    double dip_pol_damp_b[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+    double dip_pol_damp_c[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
+} mdff_param_grad;
+
+/* sizeof(mdff_params), sizeof(mdff_energies), sizeof(mdff_thermo),
+ * sizeof(mdff_param_grad) for which = 0, 1, 2, 3 (lets a binding check its
+ * mirror of these structs); no reference counterpart. */
 int  mdff_struct_size(int which);
 
 /* Measured FMA throughput of the device in TFLOP/s: out[0] FP64, out[1]

@@ -89,6 +89,21 @@ class Thermo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ParamGrad(C.Structure):
+    """mdff_param_grad: derivative of a loss with respect to the force-field
+    tables, unordered pairs in the upper-triangle slot [a][b], a <= b."""
+    _fields_ = [
+        ("Abmhftd", _D2), ("Bbmhftd", _D2), ("Cbmhftd", _D2), ("Dbmhftd", _D2), ("BDbmhftd", _D2),
+        ("epsmor", _D2), ("sigmamor", _D2), ("rhomor", _D2),
+        ("poldip_iso", _D1),
+        ("dip_pol_damp_b", _D3), ("dip_pol_damp_c", _D3),
+    ]
+
+    def array(self, name):
+        import numpy as np
+        return np.ctypeslib.as_array(getattr(self, name)).copy()
+
+
 def default_params():
     """Reference defaults: control_default_tag (src/control.f90:199-243),
     field_default_tag (src/field.f90:192-273), md_default_tag

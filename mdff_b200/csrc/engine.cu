@@ -936,6 +936,7 @@ int mdff_struct_size(int which) {
         case 0: return (int)sizeof(mdff_params);
         case 1: return (int)sizeof(mdff_energies);
         case 2: return (int)sizeof(mdff_thermo);
+        case 3: return (int)sizeof(mdff_param_grad);
         default: return -1;
     }
 }

@@ -286,23 +286,57 @@ def mgo_production(ncell=16, vacancy_frac=0.01, seed=11):
     return s
 
 
-def mgo_batch(nconf=64, nmin=200, nmax=2000, dens=(3.3, 3.8), seed=99, dmin=1.7):
-    """Batch of MgO PIM configurations for force matching: atom counts drawn
-    uniformly from [nmin, nmax] (rounded to even, half O half Mg), random
-    uniform positions with a minimum separation dmin in a cubic box at a
-    density drawn from dens (g/cm3); rc = min(10, half box width),
-    alpha chosen as 3.2 / rc, kmax from the reference's estimate at 1e-6."""
+def _grid_for(n, max_aspect=2.0):
+    """Even site-grid dimensions (nx <= ny <= nz, nz/nx <= max_aspect) whose
+    product P >= n is smallest, P - n even."""
+    best = None
+    for nx in range(2, 40, 2):
+        for ny in range(nx, 40, 2):
+            for nz in range(ny, int(max_aspect * nx) + 1, 2):
+                P = nx * ny * nz
+                if P < n or (P - n) % 2:
+                    continue
+                if best is None or P < best[0]:
+                    best = (P, (nx, ny, nz))
+    return best[1]
+
+
+def mgo_batch(nconf=64, nmin=200, nmax=2000, dens=(3.3, 3.8), seed=99, jitter=0.12):
+    """Batch of MgO PIM configurations for force matching.
+
+    Atom counts are drawn uniformly from [nmin, nmax] (rounded down to even,
+    half O and half Mg) and densities uniformly from dens (g/cm3).  Each
+    configuration is a rock-salt site grid (spacing h, rock-salt occupation)
+    in the smallest orthorhombic box of even grid dimensions holding at least
+    n sites, with the surplus sites removed as equal numbers of O and Mg
+    vacancies, h scaled so that the n atoms have the drawn density, and
+    positions jittered by N(0, jitter^2): disordered hot-crystal snapshots,
+    which keep the induced-dipole system well conditioned (uniformly random
+    positions put O-O pairs within the polarisation-catastrophe distance).
+    rc = min(10, half the smallest box width), alpha = 3.2 / rc, kmax from
+    the reference's estimate at 1e-6."""
     rng = np.random.default_rng(seed)
     confs = []
     for c in range(nconf):
         n = int(rng.integers(nmin, nmax + 1)) // 2 * 2
         d = float(rng.uniform(*dens))
+        nx, ny, nz = _grid_for(n)
         m = (n // 2) * (MASS_O + MASS_MG)
-        L = (m * AMU_G / d * 1e24) ** (1.0 / 3.0)
-        rc = min(10.0, 0.5 * L - 1e-9)
+        vol = m * AMU_G / d * 1e24
+        h = (vol / (nx * ny * nz)) ** (1.0 / 3.0)
+        sites, is_o = rocksalt_sites(nx, ny, nz, 2.0 * h)
+        nvac = (len(sites) - n) // 2
+        keep = np.ones(len(sites), bool)
+        if nvac:
+            keep[rng.choice(np.flatnonzero(is_o), nvac, replace=False)] = False
+            keep[rng.choice(np.flatnonzero(~is_o), nvac, replace=False)] = False
+        sites, is_o = sites[keep], is_o[keep]
+        order = np.concatenate([np.flatnonzero(is_o), np.flatnonzero(~is_o)])
+        pos = sites[order] + rng.normal(0.0, jitter, (n, 3))
+        box = np.array([nx, ny, nz], float) * h
+        rc = min(10.0, 0.5 * box.min() - 1e-9)
         alpha = 3.2 / rc
-        kmax = max(3, ewald_kmax_for(alpha, L, 1e-6, rc))
-        pos = random_min_sep(rng, n, L, dmin)
+        kmax = [max(3, ewald_kmax_for(alpha, float(L), 1e-6, rc)) for L in box]
         itype = np.array([1] * (n // 2) + [2] * (n // 2), np.int32)
-        confs.append(dict(itype=itype, pos=pos, cell=np.eye(3) * L, rc=rc, alpha=alpha, kmax=kmax, density=d))
+        confs.append(dict(itype=itype, pos=pos, cell=np.diag(box), rc=rc, alpha=alpha, kmax=kmax, density=d))
     return confs

@@ -49,6 +49,8 @@ def lib():
         L.orc_field_time.argtypes = [C.c_void_p, C.c_int, dp, dp, dp]
         L.orc_max_threads.restype = C.c_int
         L.orc_md_start.argtypes = [C.c_void_p, dp, dp, dp, C.POINTER(abi.Thermo)]
+        L.orc_loss_grad.argtypes = [C.c_void_p, dp, dp, dp, dp, C.c_double, C.c_double, dp,
+                                    C.POINTER(abi.ParamGrad), ip]
         L.orc_step.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
         _lib = L
     return _lib
@@ -173,6 +175,23 @@ class Oracle:
         a, b, c = C.c_double(), C.c_double(), C.c_double()
         lib().orc_field_time(self._h, int(kstride), C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
+
+    def loss_grad(self, f_target, tau_target, c_force, c_stress, grad=None):
+        """Force-matching loss c_force*sum|F-F*|^2 + c_stress*sum(tau-tau*)^2
+        of this configuration (a fresh induced-dipole solve) and its gradient
+        with respect to the force-field tables, accumulated into grad (an
+        abi.ParamGrad, created zeroed when None).  Returns (loss, grad,
+        (forward iterations, adjoint iterations))."""
+        ft = np.asarray(f_target, dtype=np.float64)
+        f = [np.ascontiguousarray(ft[:, k]) for k in range(3)]
+        tt = np.ascontiguousarray(np.asarray(tau_target, dtype=np.float64).T.reshape(9))
+        if grad is None:
+            grad = abi.ParamGrad()
+        loss = C.c_double(0.0)
+        it = (C.c_int * 2)()
+        lib().orc_loss_grad(self._h, *(_dp(a) for a in f), _dp(tt), float(c_force), float(c_stress),
+                            C.byref(loss), C.byref(grad), it)
+        return loss.value, grad, (it[0], it[1])
 
     def md_start(self, vel):
         vel = np.asarray(vel, dtype=np.float64)

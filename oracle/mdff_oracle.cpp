@@ -1329,6 +1329,316 @@ void copy_out(orc_sys* s, double* fx, double* fy, double* fz, mdff_energies* e, 
     if (mu) { if (s->mu.size() == 3 * (size_t)n) std::memcpy(mu, s->mu.data(), sizeof(double) * 3 * n); else std::memset(mu, 0, sizeof(double) * 3 * n); }
 }
 
+
+// ---------------------------------------------------------------------------
+// Force-matching loss and its gradient with respect to the force-field
+// parameters.  The reference has no derivatives: this is the FP64 checker of
+// the engine's adjoint kernels, written from the engine's own force
+// expressions (the ones restated above) by hand differentiation.
+//
+// Loss of one configuration:  L = cF sum_i |F_i - F*_i|^2 + cS sum_ab (tau_ab - tau*_ab)^2
+// with F the total force (eV/A) and tau = tau_nonb + tau_coul (GPa).
+// With R_i = dL/dF_i and S = dL/dtau held fixed, dL/dtheta is the derivative
+// of J = sum_i R_i.F_i + S:tau.  J depends on theta directly and through the
+// induced dipoles mu, which solve A mu = b with A = 1/alpha - T (T the
+// undamped dipole field operator, symmetric) and b the damped static field.
+// The adjoint lambda = A^{-1} dJ/dmu gives
+//   dL/dtheta = dJ/dtheta|_mu + lambda.(db/dtheta - dA/dtheta mu).
+// ---------------------------------------------------------------------------
+
+// Tang-Toennies pieces and their parameter derivatives:
+// g = 1 - f = c e^{-x} sum_{m<=k} x^m/m!,  gd = f' = c b e^{-x} x^k/k!,  x = b r.
+struct TTDeriv { double g, gd, dg_db, dg_dc, dgd_db, dgd_dc; };
+TTDeriv tt_deriv(double b, double c, double r, int k) {
+    double x = b * r, e = std::exp(-x);
+    double sum = E_TT[k];
+    for (int m = k - 1; m >= 0; --m) sum = sum * x + E_TT[m];
+    double tk = E_TT[k] * std::pow(x, k);
+    TTDeriv t;
+    t.g = c * e * sum;
+    t.gd = c * b * e * tk;
+    t.dg_dc = e * sum;
+    t.dg_db = -c * r * e * tk;
+    t.dgd_dc = b * e * tk;
+    t.dgd_db = c * e * tk * (1.0 + k - x);
+    return t;
+}
+
+// Upper-triangle slot of an unordered type pair.
+inline void upper(int& a, int& b) { if (a > b) std::swap(a, b); }
+
+// Jacobi-preconditioned CG on the polarisable atoms: (1/alpha - T) x = rhs.
+int adjoint_solve(orc_sys* s, const std::vector<double>& rhs, std::vector<double>& x, const std::vector<char>& pol,
+                  int npol) {
+    int n = s->natm;
+    const mdff_params& p = s->p;
+    std::vector<double> Eind(3 * (size_t)n, 0.0);
+    auto apply = [&](const std::vector<double>& v, std::vector<double>& out) {
+        induced_field(s, v, Eind);
+        out.assign(3 * (size_t)n, 0.0);
+        for (int c = 0; c < 3; ++c) for (int ia = 0; ia < n; ++ia)
+            if (pol[ia]) out[(size_t)c * n + ia] = v[(size_t)c * n + ia] * s->invpoldia[ia] - Eind[(size_t)c * n + ia];
+    };
+    auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) { double t = 0; for (size_t k = 0; k < a.size(); ++k) t += a[k] * b[k]; return t; };
+    x.assign(3 * (size_t)n, 0.0);
+    for (int c = 0; c < 3; ++c) for (int ia = 0; ia < n; ++ia)
+        if (pol[ia]) x[(size_t)c * n + ia] = s->poldia[ia] * rhs[(size_t)c * n + ia];
+    std::vector<double> r(3 * (size_t)n), z(3 * (size_t)n), d, Ad;
+    apply(x, Ad);
+    for (size_t k = 0; k < r.size(); ++k) r[k] = pol[k % n] ? rhs[k] - Ad[k] : 0.0;
+    for (size_t k = 0; k < r.size(); ++k) z[k] = s->poldia[k % n] * r[k];
+    d = z;
+    double rz = dot(r, z);
+    double rmsd = std::sqrt(dot(r, r) / double(npol));
+    int it = 0;
+    while (it < p.max_scf_pol_iter && rmsd > p.conv_tol_ind) {
+        it++;
+        apply(d, Ad);
+        double a = rz / dot(d, Ad);
+        for (size_t k = 0; k < x.size(); ++k) { x[k] += a * d[k]; r[k] -= a * Ad[k]; }
+        for (size_t k = 0; k < r.size(); ++k) z[k] = s->poldia[k % n] * r[k];
+        double rz2 = dot(r, z);
+        rmsd = std::sqrt(dot(r, r) / double(npol));
+        double beta = rz2 / rz;
+        rz = rz2;
+        for (size_t k = 0; k < d.size(); ++k) d[k] = z[k] + beta * d[k];
+    }
+    return it;
+}
+
+int loss_grad(orc_sys* s, const double* fxt, const double* fyt, const double* fzt, const double* taut, double cF,
+              double cS, double* loss, mdff_param_grad* g, int* iters) {
+    const int n = s->natm;
+    const mdff_params& p = s->p;
+    // a fresh solve: no predictor history
+    std::fill(s->dip_hist.begin(), s->dip_hist.end(), 0.0);
+    s->itime = 0;
+    engforce(s);
+    iters[0] = s->en.scf_iter;
+    iters[1] = 0;
+    std::vector<double> R(3 * (size_t)n);
+    double L = 0.0;
+    const double* ft[3] = {fxt, fyt, fzt};
+    const std::vector<double>* fv[3] = {&s->fx, &s->fy, &s->fz};
+    for (int c = 0; c < 3; ++c)
+        for (int i = 0; i < n; ++i) {
+            double dlt = (*fv[c])[i] - ft[c][i];
+            L += cF * dlt * dlt;
+            R[(size_t)c * n + i] = 2.0 * cF * dlt;
+        }
+    double S[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            double dlt = s->tau_nonb[a][b] + s->tau_coul[a][b] - taut[3 * b + a];
+            L += cS * dlt * dlt;
+            S[a][b] = 2.0 * cS * dlt;
+        }
+    *loss += L;
+    const double so = 1.0 / (s->cell.omega * s->u.press);   // stress per unit pair virial
+    std::vector<double> sx, sy, sz;
+    direct_coords(s, sx, sy, sz);
+    auto RR = [&](int c, int i) { return R[(size_t)c * n + i]; };
+    auto Sr = [&](const double r[3], double out[3]) {
+        for (int a = 0; a < 3; ++a) out[a] = S[a][0] * r[0] + S[a][1] * r[1] + S[a][2] * r[2];
+    };
+    // --- short-range pairs: dJ/dtheta = sum_pairs dw/dtheta [(R_i - R_j).r + r.S.r/(omega press)]
+    if (p.lbmhft || p.lbmhftd || p.lmorse) {
+        for_pairs(s, s->vdw, sx, sy, sz, [&](int ia, int ja) {
+            double r[3];
+            double rsq = pairvec(s->cell, sx[ia], sy[ia], sz[ia], sx[ja], sy[ja], sz[ja], r[0], r[1], r[2]);
+            double srv[3];
+            Sr(r, srv);
+            double geo = 0.0;
+            for (int c = 0; c < 3; ++c) geo += (RR(c, ia) - RR(c, ja)) * r[c] + so * r[c] * srv[c];
+            int t1 = s->itype[ia], t2 = s->itype[ja];
+            if ((p.lbmhft || p.lbmhftd) && p.Abmhftd[t1][t2] != 0.0 && rsq < s->rcutsq[t1][t2]) {
+                double d = std::sqrt(rsq);
+                double A = p.Abmhftd[t1][t2], B = p.Bbmhftd[t1][t2], C = p.Cbmhftd[t1][t2], D = p.Dbmhftd[t1][t2];
+                double e1 = std::exp(-B * d), erh = A * e1;
+                double d6 = 1.0 / (rsq * rsq * rsq), d8 = d6 / rsq;
+                double f6 = 1.0, f8 = 1.0, fd6 = 0.0, fd8 = 0.0, df6 = 0.0, df8 = 0.0, dfd6 = 0.0, dfd8 = 0.0;
+                if (p.lbmhftd) {
+                    double bd = p.BDbmhftd[t1][t2];
+                    TTDeriv a6 = tt_deriv(bd, 1.0, d, 6), a8 = tt_deriv(bd, 1.0, d, 8);
+                    f6 = 1.0 - a6.g; fd6 = a6.gd; df6 = -a6.dg_db; dfd6 = a6.dgd_db;
+                    f8 = 1.0 - a8.g; fd8 = a8.gd; df8 = -a8.dg_db; dfd8 = a8.dgd_db;
+                }
+                int a = t1, b = t2;
+                upper(a, b);
+                g->Abmhftd[a][b] += geo * B * e1 / d;
+                g->Bbmhftd[a][b] += geo * erh * (1.0 - B * d) / d;
+                g->Cbmhftd[a][b] += geo * (-6.0 * f6 * d6 / d + fd6 * d6) / d;
+                g->Dbmhftd[a][b] += geo * (-8.0 * f8 * d8 / d + fd8 * d8) / d;
+                if (p.lbmhftd)
+                    g->BDbmhftd[a][b] += geo * (-6.0 * C * d6 / d * df6 - 8.0 * D * d8 / d * df8 + C * d6 * dfd6 + D * d8 * dfd8) / d;
+            }
+            int m1 = s->itype[ja], m2 = s->itype[ia];
+            if (p.lmorse && rsq < s->rcutsq[m1][m2]) {
+                double d = std::sqrt(rsq);
+                double eps = p.epsmor[m1][m2], rho = p.rhomor[m1][m2], sig = p.sigmamor[m1][m2];
+                double e = std::exp(-d * rho) * s->rs[m1][m2];
+                int a = m1, b = m2;
+                upper(a, b);
+                g->epsmor[a][b] += geo * 2.0 * rho * e * (e - 1.0) / d;
+                g->rhomor[a][b] += geo * 2.0 * eps / d * (e * (e - 1.0) + rho * (sig - d) * e * (2.0 * e - 1.0));
+                g->sigmamor[a][b] += geo * 2.0 * eps * rho / d * rho * e * (2.0 * e - 1.0);
+            }
+        });
+    }
+    if (!p.lcoulomb || !any_polar(s)) return 0;
+    // --- electrostatics: h = dJ/dmu (real + reciprocal space), damping terms of dJ/dtheta
+    const double cu = s->u.coul;
+    std::vector<char> pol(n, 0);
+    int npol = 0;
+    for (int ia = 0; ia < n; ++ia) if (p.ldip_polar[s->itype[ia]] && s->poldia[ia] != 0.0) { pol[ia] = 1; npol++; }
+    const std::vector<double>& mu = s->mu;
+    const std::vector<double>& q = s->qia;
+    std::vector<double> h(3 * (size_t)n, 0.0);
+    const double aES = s->alphaES, a2 = aES * aES, a3 = a2 * aES, a5 = a3 * a2;
+    const double cutsq = s->coul.cut * s->coul.cut;
+    auto MU = [&](int c, int i) { return mu[(size_t)c * n + i]; };
+    struct PairGeo { double r[3], d, A1, B2, C3; };
+    auto geom = [&](int ia, int ja, PairGeo& G) -> bool {
+        double d2 = pairvec(s->cell, sx[ia], sy[ia], sz[ia], sx[ja], sy[ja], sz[ja], G.r[0], G.r[1], G.r[2]);
+        if (d2 > cutsq) return false;
+        double d = std::sqrt(d2);
+        double expon = std::exp(-a2 * d2) / PIROOT;
+        double F0 = erfc_sel(s, aES * d);
+        double F1 = F0 + 2.0 * aES * d * expon;
+        double F2 = F1 + 4.0 * a3 * d2 * d * expon / 3.0;
+        double F3 = F2 + 8.0 * a5 * d2 * d2 * d * expon / 15.0;
+        G.d = d;
+        G.A1 = F1 / (d2 * d);
+        G.B2 = 3.0 * F2 / (d2 * d2 * d);
+        G.C3 = 15.0 * F3 / (d2 * d2 * d2 * d);
+        return true;
+    };
+    for_pairs(s, s->coul, sx, sy, sz, [&](int ia, int ja) {
+        PairGeo G;
+        if (!geom(ia, ja, G)) return;
+        const double* r = G.r;
+        int ti = s->itype[ia], tj = s->itype[ja];
+        double qi = q[ia], qj = q[ja];
+        double mi[3] = {MU(0, ia), MU(1, ia), MU(2, ia)}, mj[3] = {MU(0, ja), MU(1, ja), MU(2, ja)};
+        double srv[3], W[3];
+        Sr(r, srv);
+        for (int c = 0; c < 3; ++c) W[c] = cu * (RR(c, ia) - RR(c, ja)) + cu * so * srv[c];
+        double wr = W[0] * r[0] + W[1] * r[1] + W[2] * r[2];
+        double rmi = r[0] * mi[0] + r[1] * mi[1] + r[2] * mi[2], rmj = r[0] * mj[0] + r[1] * mj[1] + r[2] * mj[2];
+        double Wmi = W[0] * mi[0] + W[1] * mi[1] + W[2] * mi[2], Wmj = W[0] * mj[0] + W[1] * mj[1] + W[2] * mj[2];
+        double hi[3], hj[3];
+        for (int c = 0; c < 3; ++c) {
+            // dipole-dipole
+            hi[c] = wr * (-r[c] * rmj * G.C3 + mj[c] * G.B2) + W[c] * rmj * G.B2 + Wmj * r[c] * G.B2;
+            hj[c] = wr * (-r[c] * rmi * G.C3 + mi[c] * G.B2) + Wmi * r[c] * G.B2 + W[c] * rmi * G.B2;
+            // charge-dipole
+            hi[c] += -wr * qj * r[c] * G.B2 + qj * W[c] * G.A1;
+            hj[c] += wr * qi * r[c] * G.B2 - qi * W[c] * G.A1;
+        }
+        bool ldamp = p.ldip_damping[ti][ti][tj] || p.ldip_damping[tj][ti][tj];
+        if (ldamp) {
+            double d = G.d, d3 = d * d * d, d5 = d3 * d * d;
+            TTDeriv Ti = tt_deriv(p.dip_pol_damp_b[ti][ti][tj], p.dip_pol_damp_c[ti][ti][tj], d, p.dip_pol_damp_k[ti][ti][tj]);
+            TTDeriv Tj = tt_deriv(p.dip_pol_damp_b[tj][ti][tj], p.dip_pol_damp_c[tj][ti][tj], d, p.dip_pol_damp_k[tj][ti][tj]);
+            double Ai = Ti.g / d3, Bi = 3.0 * (Ti.g + d / 3.0 * Ti.gd) / d5;
+            double Aj = Tj.g / d3, Bj = 3.0 * (Tj.g + d / 3.0 * Tj.gd) / d5;
+            for (int c = 0; c < 3; ++c) {
+                hi[c] += qj * (wr * r[c] * Bi - W[c] * Ai);
+                hj[c] += -qi * (wr * r[c] * Bj - W[c] * Aj);
+            }
+            // dJ/d(b,c) at fixed mu: the damped charge-dipole force
+            double dAi_b = Ti.dg_db / d3, dBi_b = (3.0 * Ti.dg_db + d * Ti.dgd_db) / d5;
+            double dAi_c = Ti.dg_dc / d3, dBi_c = (3.0 * Ti.dg_dc + d * Ti.dgd_dc) / d5;
+            double dAj_b = Tj.dg_db / d3, dBj_b = (3.0 * Tj.dg_db + d * Tj.dgd_db) / d5;
+            double dAj_c = Tj.dg_dc / d3, dBj_c = (3.0 * Tj.dg_dc + d * Tj.dgd_dc) / d5;
+            int a = ti, b = tj;
+            upper(a, b);
+            g->dip_pol_damp_b[ti][a][b] += qj * (wr * rmi * dBi_b - Wmi * dAi_b);
+            g->dip_pol_damp_c[ti][a][b] += qj * (wr * rmi * dBi_c - Wmi * dAi_c);
+            g->dip_pol_damp_b[tj][a][b] += -qi * (wr * rmj * dBj_b - Wmj * dAj_b);
+            g->dip_pol_damp_c[tj][a][b] += -qi * (wr * rmj * dBj_c - Wmj * dAj_c);
+        }
+        for (int c = 0; c < 3; ++c) { h[(size_t)c * n + ia] += hi[c]; h[(size_t)c * n + ja] += hj[c]; }
+    });
+    // reciprocal space: forces F = -fpi_V grad sum_k A_k |rho_k|^2 (half mesh), stress
+    // (2 tpi_V / omega) sum_k (delta - kcoe k k) A_k |rho_k|^2.
+    {
+        const KMesh& km = s->km;
+        double tpi_V = TPI / s->cell.omega, fpi_V = 2.0 * tpi_V;
+        double cs = cu / s->u.press * 2.0 * tpi_V / s->cell.omega;
+        double trS = S[0][0] + S[1][1] + S[2][2];
+        int nth = 1;
+#ifdef _OPENMP
+        nth = omp_get_max_threads();
+#endif
+        std::vector<std::vector<double>> th(nth, std::vector<double>(3 * (size_t)n, 0.0));
+#pragma omp parallel
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            std::vector<double>& lh = th[t];
+            std::vector<double> ck(n), sk(n);
+#pragma omp for schedule(static)
+            for (int ik = 0; ik < km.nk; ++ik) {
+                if (km.kk[ik] == 0.0) continue;
+                double k[3] = {km.kx[ik], km.ky[ik], km.kz[ik]}, Ak = km.Ak[ik];
+                double rhoR = 0, rhoI = 0, sgR = 0, sgI = 0;
+                for (int ia = 0; ia < n; ++ia) {
+                    double kr = k[0] * s->rx[ia] + k[1] * s->ry[ia] + k[2] * s->rz[ia];
+                    ck[ia] = std::cos(kr);
+                    sk[ia] = std::sin(kr);
+                    double m = k[0] * MU(0, ia) + k[1] * MU(1, ia) + k[2] * MU(2, ia);
+                    double kR = k[0] * RR(0, ia) + k[1] * RR(1, ia) + k[2] * RR(2, ia);
+                    double aR = q[ia] * ck[ia] - m * sk[ia], aI = q[ia] * sk[ia] + m * ck[ia];
+                    rhoR += aR; rhoI += aI;
+                    sgR += kR * aR; sgI += kR * aI;
+                }
+                double kSk = 0.0;
+                for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) kSk += k[a] * S[a][b] * k[b];
+                double sk_ = trS - km.kcoe[ik] * kSk;
+                for (int ja = 0; ja < n; ++ja) {
+                    double kR = k[0] * RR(0, ja) + k[1] * RR(1, ja) + k[2] * RR(2, ja);
+                    double v = 2.0 * cu * fpi_V * Ak * (kR * (rhoR * ck[ja] + rhoI * sk[ja]) - (sgR * ck[ja] + sgI * sk[ja]))
+                             - 2.0 * cs * sk_ * Ak * (rhoR * sk[ja] - rhoI * ck[ja]);
+                    for (int c = 0; c < 3; ++c) lh[(size_t)c * n + ja] += k[c] * v;
+                }
+            }
+        }
+        for (int t = 0; t < nth; ++t) for (size_t k = 0; k < h.size(); ++k) h[k] += th[t][k];
+    }
+    for (size_t k = 0; k < h.size(); ++k) if (!pol[k % n]) h[k] = 0.0;
+    std::vector<double> lam;
+    iters[1] = adjoint_solve(s, h, lam, pol, npol);
+    // polarisabilities: dA/dalpha_t = -1/alpha_t^2 on type-t atoms
+    for (int ia = 0; ia < n; ++ia) {
+        if (!pol[ia]) continue;
+        double lm = 0.0;
+        for (int c = 0; c < 3; ++c) lm += lam[(size_t)c * n + ia] * (MU(c, ia) - (c == 0 ? s->dipx[ia] : c == 1 ? s->dipy[ia] : s->dipz[ia]));
+        g->poldip_iso[s->itype[ia]] += lm * s->invpoldia[ia] * s->invpoldia[ia];
+    }
+    // damping in the static field b: E_i += qj (F1 - g_i) r/d^3, E_j -= qi (F1 - g_j) r/d^3
+    for_pairs(s, s->coul, sx, sy, sz, [&](int ia, int ja) {
+        int ti = s->itype[ia], tj = s->itype[ja];
+        if (!(p.ldip_damping[ti][ti][tj] || p.ldip_damping[tj][ti][tj])) return;
+        PairGeo G;
+        if (!geom(ia, ja, G)) return;
+        double d = G.d, d3 = d * d * d;
+        double li = 0.0, lj = 0.0;
+        for (int c = 0; c < 3; ++c) { li += lam[(size_t)c * n + ia] * G.r[c]; lj += lam[(size_t)c * n + ja] * G.r[c]; }
+        TTDeriv Ti = tt_deriv(p.dip_pol_damp_b[ti][ti][tj], p.dip_pol_damp_c[ti][ti][tj], d, p.dip_pol_damp_k[ti][ti][tj]);
+        TTDeriv Tj = tt_deriv(p.dip_pol_damp_b[tj][ti][tj], p.dip_pol_damp_c[tj][ti][tj], d, p.dip_pol_damp_k[tj][ti][tj]);
+        int a = ti, b = tj;
+        upper(a, b);
+        g->dip_pol_damp_b[ti][a][b] += -q[ja] * li / d3 * Ti.dg_db;
+        g->dip_pol_damp_c[ti][a][b] += -q[ja] * li / d3 * Ti.dg_dc;
+        g->dip_pol_damp_b[tj][a][b] += q[ia] * lj / d3 * Tj.dg_db;
+        g->dip_pol_damp_c[tj][a][b] += q[ia] * lj / d3 * Tj.dg_dc;
+    });
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1449,6 +1759,14 @@ int orc_nlist_get(orc_sys* s, int which, int* point, int* list, int cap, int* nl
     for (int i = 0; i <= s->natm; ++i) point[i] = L.point[i] + 1;
     for (size_t k = 0; k < L.list.size(); ++k) list[k] = L.list[k] + 1;
     return 0;
+}
+
+// Force-matching loss of this configuration and its parameter gradient,
+// ADDED to *loss and *g (see loss_grad).  iters[0], iters[1]: iterations of
+// the forward and adjoint solves.
+int orc_loss_grad(orc_sys* s, const double* fxt, const double* fyt, const double* fzt, const double taut[9],
+                  double cF, double cS, double* loss, mdff_param_grad* g, int iters[2]) {
+    return loss_grad(s, fxt, fyt, fzt, taut, cF, cS, loss, g, iters);
 }
 
 int orc_engforce(orc_sys* s, double* fx, double* fy, double* fz, mdff_energies* e, double tau_nonb[9],

@@ -290,6 +290,53 @@ int  mdff_step(mdff_ctx* ctx, int nsteps,
                double* fx, double* fy, double* fz,
                mdff_thermo* thermo);
 
+/*
+ * Batched force matching (no reference counterpart: the reference evaluates
+ * one configuration at a time and has no derivatives).  A batch holds nconf
+ * fixed configurations of uneven atom counts sharing one force field; every
+ * kernel of an evaluation is one launch over the whole batch.  The physics per
+ * configuration is that of mdff_engforce in FP64 (BMH / BMHFTD, Morse,
+ * multipole Ewald with polarisable ions solved by PCG to conv_tol_ind), with
+ * one neighbour cutoff rc[c] for both the short-range and the real-space
+ * Coulomb sums, Ewald alpha[c] and k rectangle kmax[3c..3c+2] per
+ * configuration.  Lennard-Jones, static dipoles and lsurf are not supported
+ * (MDFF_E_UNSUPPORTED); at most 2 atom types.
+ *
+ * Loss:  L = 1/nconf sum_c [ w_force/(3 N_c) sum_i |F_i - F*_i|^2
+ *                           + w_stress/9 sum_ab (tau_ab - tau*_ab)^2 ]
+ * with F the total force (eV/A) and tau = tau_nonb + tau_coul (GPa).
+ */
+typedef struct mdff_batch mdff_batch;
+
+/* natm[c] atoms per configuration; itype (1-based), rx, ry, rz concatenated
+ * over the configurations; cells[9c..9c+8] the column-major cell of
+ * configuration c.  *out is set even when the call fails (read
+ * mdff_batch_last_error, then mdff_batch_destroy). */
+int  mdff_batch_create(const mdff_params* p, int nconf, const int* natm, const int* itype,
+                       const double* rx, const double* ry, const double* rz, const double* cells,
+                       const double* rc, const double* alpha, const int* kmax, mdff_batch** out);
+void mdff_batch_destroy(mdff_batch* b);
+const char* mdff_batch_last_error(const mdff_batch* b);
+int  mdff_batch_stream(mdff_batch* b, void** stream);
+
+/* Replace the force-field tables (same ntype and lcoulomb as at creation). */
+int  mdff_batch_set_params(mdff_batch* b, const mdff_params* p);
+
+/* Forces (concatenated, eV/A), total stress tau[9c..9c+8] (GPa, column-major)
+ * and potential energy energy[c] (eV) of every configuration; iters receives
+ * the iterations of the dipole solve.  Any output may be NULL. */
+int  mdff_batch_forces(mdff_batch* b, double* fx, double* fy, double* fz, double* tau, double* energy,
+                       int* iters);
+
+/* Target forces (concatenated) and stresses (9 per configuration) of the loss. */
+int  mdff_batch_set_targets(mdff_batch* b, const double* fx, const double* fy, const double* fz,
+                            const double* tau, double w_force, double w_stress);
+
+/* The loss and, when grad != NULL, its gradient with respect to the force-field
+ * tables (adjoint method: one forward and one adjoint induced-dipole solve).
+ * iters (may be NULL) receives the forward and adjoint solve iterations. */
+int  mdff_batch_loss_grad(mdff_batch* b, double* loss, mdff_param_grad* grad, int iters[2]);
+
 #ifdef __cplusplus
 }
 #endif

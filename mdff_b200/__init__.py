@@ -63,6 +63,16 @@ def lib():
         L.mdff_profile_get.argtypes = [vp, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int]
         L.mdff_measure_pipes.argtypes = [C.c_int, dp]
         L.mdff_struct_size.argtypes = [C.c_int]
+        L.mdff_batch_create.argtypes = [C.POINTER(abi.Params), C.c_int, ip, ip, dp, dp, dp, dp, dp, dp, ip, C.POINTER(vp)]
+        L.mdff_batch_destroy.argtypes = [vp]
+        L.mdff_batch_destroy.restype = None
+        L.mdff_batch_last_error.argtypes = [vp]
+        L.mdff_batch_last_error.restype = C.c_char_p
+        L.mdff_batch_stream.argtypes = [vp, C.POINTER(vp)]
+        L.mdff_batch_set_params.argtypes = [vp, C.POINTER(abi.Params)]
+        L.mdff_batch_forces.argtypes = [vp, dp, dp, dp, dp, dp, ip]
+        L.mdff_batch_set_targets.argtypes = [vp, dp, dp, dp, dp, C.c_double, C.c_double]
+        L.mdff_batch_loss_grad.argtypes = [vp, dp, C.POINTER(abi.ParamGrad), ip]
         _lib = L
     return _lib
 
@@ -232,3 +242,91 @@ class Engine:
         self._check(lib().mdff_step(self._h, nsteps, *(_dp(pos[k]) for k in range(3)), *(_dp(vel[k]) for k in range(3)),
                                     *(_dp(a) for a in f), thermo))
         return f
+
+
+class Batch:
+    """A batch of fixed configurations sharing one force field: forces and
+    stress of all of them, and the force-matching loss with its adjoint
+    gradient, each in one set of launches (mdff_batch_* in
+    include/mdff_engine.h).
+
+    confs: list of dicts with itype (1-based), pos [n,3], cell [3,3] (rows
+    are the basis vectors), rc, alpha, kmax (int or 3 ints)."""
+
+    def __init__(self, params, confs):
+        L = lib()
+        self.params = params
+        self.nconf = len(confs)
+        self.natm = np.array([len(c["itype"]) for c in confs], dtype=np.int32)
+        self.N = int(self.natm.sum())
+        self.offsets = np.concatenate([[0], np.cumsum(self.natm)])
+        itype = np.ascontiguousarray(np.concatenate([c["itype"] for c in confs]), dtype=np.int32)
+        pos = np.concatenate([np.asarray(c["pos"], dtype=np.float64) for c in confs])
+        r = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+        cells = np.ascontiguousarray(np.concatenate(
+            [np.asarray(c["cell"], dtype=np.float64).T.reshape(9) for c in confs]))
+        rc = np.ascontiguousarray([float(c["rc"]) for c in confs])
+        alpha = np.ascontiguousarray([float(c["alpha"]) for c in confs])
+        km = np.ascontiguousarray(np.concatenate(
+            [np.broadcast_to(np.asarray(c["kmax"], dtype=np.int32), (3,)) for c in confs]), dtype=np.int32)
+        self._h = C.c_void_p()
+        rc_ = L.mdff_batch_create(C.byref(params), self.nconf, _ip(self.natm), _ip(itype), *(_dp(a) for a in r),
+                                  _dp(cells), _dp(rc), _dp(alpha), _ip(km), C.byref(self._h))
+        self._check(rc_)
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = lib().mdff_batch_last_error(self._h).decode() if self._h else "no batch"
+            raise EngineError(rc, msg)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().mdff_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stream(self):
+        s = C.c_void_p()
+        self._check(lib().mdff_batch_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def set_params(self, params):
+        self.params = params
+        self._check(lib().mdff_batch_set_params(self._h, C.byref(params)))
+
+    def split(self, a):
+        return [a[self.offsets[c]:self.offsets[c + 1]] for c in range(self.nconf)]
+
+    def forces(self):
+        """Per configuration: forces [n,3] (eV/A), total stress [3,3] (GPa)
+        and potential energy (eV); and the dipole-solve iterations."""
+        f = [np.empty(self.N) for _ in range(3)]
+        tau = np.empty(9 * self.nconf)
+        e = np.empty(self.nconf)
+        it = C.c_int()
+        self._check(lib().mdff_batch_forces(self._h, *(_dp(a) for a in f), _dp(tau), _dp(e), C.byref(it)))
+        F = np.stack(f, axis=1)
+        taus = [tau[9 * c:9 * c + 9].reshape(3, 3).T.copy() for c in range(self.nconf)]
+        return {"f": self.split(F), "tau": taus, "energy": e, "iters": it.value}
+
+    def set_targets(self, f_target, tau_target, w_force=1.0, w_stress=1.0):
+        """Targets of the loss: forces per configuration [n,3] and stresses [3,3]."""
+        F = np.concatenate([np.asarray(x, dtype=np.float64) for x in f_target])
+        f = [np.ascontiguousarray(F[:, k]) for k in range(3)]
+        tau = np.ascontiguousarray(np.concatenate(
+            [np.asarray(t, dtype=np.float64).T.reshape(9) for t in tau_target]))
+        self._check(lib().mdff_batch_set_targets(self._h, *(_dp(a) for a in f), _dp(tau), float(w_force),
+                                                 float(w_stress)))
+
+    def loss_grad(self, want_grad=True):
+        """(loss, abi.ParamGrad or None, (forward iterations, adjoint iterations))."""
+        loss = C.c_double()
+        g = abi.ParamGrad() if want_grad else None
+        it = (C.c_int * 2)()
+        self._check(lib().mdff_batch_loss_grad(self._h, C.byref(loss), C.byref(g) if g is not None else None, it))
+        return loss.value, g, (it[0], it[1])

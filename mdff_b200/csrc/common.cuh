@@ -23,6 +23,30 @@ __device__ __forceinline__ double pairvec_exact(const CellP& c, double si1, doub
     return __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
 }
 
+// errfc (src/functions.f90:28-39): the reference's fitted erfc (Numerical
+// Recipes' Chebyshev approximation), selectable for bit-level parity studies.
+__device__ __forceinline__ double erfc_fit(double x) {
+    double z = fabs(x);
+    double t = 1.0 / (1.0 + 0.5 * z);
+    double r = t * exp(-z * z - 1.26551223 + t * (1.00002368 + t * (.37409196 + t * (.09678418 +
+               t * (-.18628806 + t * (.27886807 + t * (-1.13520398 + t * (1.48851587 +
+               t * (-.82215223 + t * .17087277)))))))));
+    return x < 0.0 ? 2.0 - r : r;
+}
+
+__device__ __forceinline__ void tt_damp_d(double b, double c, double r, int k, double& f, double& fd) {
+    const double br = b * r;
+    const double e = exp(-br) * c;
+    double term = 1.0, sum = 1.0, inv = 1.0;
+    for (int m = 1; m <= k; ++m) {
+        inv = inv / (double)m;
+        term = term * br;
+        sum = fma(term, inv, sum);
+    }
+    f = 1.0 - sum * e;
+    fd = term * inv * e * b;
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -17,30 +17,6 @@
 
 namespace mdff {
 
-// errfc (src/functions.f90:28-39): the reference's fitted erfc (Numerical
-// Recipes' Chebyshev approximation), selectable for bit-level parity studies.
-__device__ __forceinline__ double erfc_fit(double x) {
-    double z = fabs(x);
-    double t = 1.0 / (1.0 + 0.5 * z);
-    double r = t * exp(-z * z - 1.26551223 + t * (1.00002368 + t * (.37409196 + t * (.09678418 +
-               t * (-.18628806 + t * (.27886807 + t * (-1.13520398 + t * (1.48851587 +
-               t * (-.82215223 + t * .17087277)))))))));
-    return x < 0.0 ? 2.0 - r : r;
-}
-
-__device__ __forceinline__ void tt_damp_d(double b, double c, double r, int k, double& f, double& fd) {
-    const double br = b * r;
-    const double e = exp(-br) * c;
-    double term = 1.0, sum = 1.0, inv = 1.0;
-    for (int m = 1; m <= k; ++m) {
-        inv = inv / (double)m;
-        term = term * br;
-        sum = fma(term, inv, sum);
-    }
-    f = 1.0 - sum * e;
-    fd = term * inv * e * b;
-}
-
 // MODE 0: full evaluation (tasks from flags; field / efg / forces from flags)
 // MODE 1: induced-dipole field operator E_i = sum_j T2(r_ij) mu_j (no damping),
 //         the dipole-dipole field of src/field.f90:3354.

@@ -131,3 +131,39 @@ def batch_constants(natm, w_force, w_stress):
     """Per-configuration weights (c_force, c_stress) of the batch loss."""
     B = len(natm)
     return [(w_force / (3.0 * n * B), w_stress / (9.0 * B)) for n in natm]
+
+
+def _autograd_function():
+    import torch
+
+    class ForceMatchLoss(torch.autograd.Function):
+        """loss(theta) of a Batch at the force field space.apply(base, theta).
+        The forward pass runs the batch's forward and adjoint solves once and
+        keeps dL/dtheta; backward returns it times the incoming gradient."""
+
+        @staticmethod
+        def forward(ctx, theta, batch, space, base):
+            th = theta.detach().cpu().double().numpy()
+            batch.set_params(space.apply(base, th))
+            loss, g, _ = batch.loss_grad(want_grad=True)
+            grad = torch.as_tensor(space.project(g, th), dtype=theta.dtype, device=theta.device)
+            ctx.save_for_backward(grad)
+            return theta.new_tensor(loss)
+
+        @staticmethod
+        def backward(ctx, gout):
+            (grad,) = ctx.saved_tensors
+            return gout * grad, None, None, None
+
+    return ForceMatchLoss
+
+
+_FML = None
+
+
+def force_match_loss(theta, batch, space, base):
+    """Differentiable force-matching loss (torch scalar) of batch at theta."""
+    global _FML
+    if _FML is None:
+        _FML = _autograd_function()
+    return _FML.apply(theta, batch, space, base)

@@ -32,6 +32,7 @@ def test_struct_sizes_match():
     assert L.mdff_struct_size(0) == C.sizeof(abi.Params)
     assert L.mdff_struct_size(1) == C.sizeof(abi.Energies)
     assert L.mdff_struct_size(2) == C.sizeof(abi.Thermo)
+    assert L.mdff_struct_size(3) == C.sizeof(abi.ParamGrad)
 
 
 def test_defaults_match_library():
@@ -53,3 +54,18 @@ def test_error_codes_match_header():
     for name in ("OK", "E_ARG", "E_CUDA", "E_NOCONV", "E_LISTOVF", "E_NONFINITE", "E_STATE", "E_UNSUPPORTED", "E_NOMEM"):
         m = re.search(r"#define MDFF_%s\s+(-?\d+)" % name, src)
         assert int(m.group(1)) == getattr(abi, name), name
+
+
+def test_batch_rejects_unsupported_models_without_gpu():
+    from mdff_b200 import systems
+    confs = systems.mgo_batch(nconf=2, nmin=120, nmax=140, seed=1)
+    p = systems.mgo_params(6.0, 0.5, 6)
+    p.lnmlj = 1
+    with pytest.raises(mdff_b200.EngineError) as e:
+        mdff_b200.Batch(p, confs)
+    assert e.value.code == abi.E_UNSUPPORTED
+    p = systems.mgo_params(6.0, 0.5, 6)
+    p.ntype = 3
+    with pytest.raises(mdff_b200.EngineError) as e:
+        mdff_b200.Batch(p, confs)
+    assert e.value.code == abi.E_UNSUPPORTED

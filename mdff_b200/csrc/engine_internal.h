@@ -200,6 +200,7 @@ struct LowK {
     double* part = nullptr;   // pass-1 partials [2][P][nzmax][ncol]
     double* aks = nullptr;    // [2][ncol][nzmax]
     double* fpart = nullptr;  // [LK_SPLIT][9][n]
+    double* aks_acc = nullptr;   // solver accumulator of aks (reuse of structure factors)
     double2* tab = nullptr;   // [n][16] e^{2 pi i m s_z} in FP64
     int P = 1, natom_chunk = 0;
 };
@@ -208,6 +209,7 @@ struct RecScratch {
     double* part = nullptr;    // structure-factor partials
     size_t part_cap = 0;       // doubles
     double* aks = nullptr;     // [2][nrect] Ak*S (re, im)
+    double* aks_acc = nullptr; // [2][nrect] solver accumulator of Ak*S (reuse of structure factors)
     double* fpart = nullptr;   // per-atom field partials [split][9][n]
     size_t fpart_cap = 0;
     uint32_t* fixed = nullptr;  // [3][n] fractional coordinates as 32-bit fixed point
@@ -224,12 +226,14 @@ struct RecFlags {
     int energy;    // energy + stress
     int forces;    // forces q E + G mu
     int prec;      // MDFF_PREC_*
+    int reuse;     // take A_k S from the solver's accumulators (no structure-factor pass)
 };
 void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl,
                       RecScratch& rs, double* ef, double* efg6, double* fo, Partials& part, DevScalars* d,
                       Prof* prof);
 size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart);
+void launch_aks_accumulate(cudaStream_t st, const KGrid& kg, RecScratch& rs, const DevScalars* d, int copy);
 
 // Solver vector kernels.
 void launch_dot(cudaStream_t st, int n3, const double* a, const double* b, Partials& part, double* out);

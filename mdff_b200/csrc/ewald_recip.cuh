@@ -715,6 +715,94 @@ struct RecLaunch {
     int CH, nchunk, ncolblk, P, natom_chunk, nsplit, cols_per_split;
 };
 
+// ---- reuse of the solver's structure factors ------------------------------
+// The structure factor is linear in the sources: with the PCG iterate
+// x = x0 + sum_k a_k d_k, S(q + x) = S(q + x0) + sum_k a_k S(d_k).  The
+// solver accumulates A_k S over its own evaluations (k_aks_axpy), so the
+// final force evaluation needs no structure-factor pass.
+
+// acc = src (copy), or acc += a src with a = rz / dAd, the step of the
+// current PCG iteration (read before k_cg_scalars advances rz).
+__global__ void k_aks_axpy(int m, const DevScalars* __restrict__ sc, int copy, const double* __restrict__ src,
+                           double* __restrict__ acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    if (copy) acc[t] = src[t];
+    else acc[t] = fma(sc->rz / sc->dAd, src[t], acc[t]);
+}
+
+// Energy and stress sums (as k_sfac_reduce) of a given A_k S(k) set of the
+// rectangle: A |S|^2 = |A S|^2 / A.
+__global__ void k_aks_energy(int ncol, int nzl, int ky, int kz, const double* __restrict__ aks, int nrect,
+                             const double* __restrict__ Ak, const double* __restrict__ kcoe, CellP c,
+                             double* partials) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (r < ncol * nzl) {
+        const double ak = Ak[r];
+        if (ak != 0.0) {
+            const int col = r / nzl, mz = r % nzl;
+            const int ny_n = 2 * ky + 1;
+            const double nx = (double)(col / ny_n), ny = (double)(col % ny_n - ky), nz = (double)(mz - kz);
+            const double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz * c.B[2]);
+            const double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz * c.B[5]);
+            const double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz * c.B[8]);
+            const double ar = aks[r], ai = aks[nrect + r];
+            const double str = (ar * ar + ai * ai) / ak;
+            const double kc = kcoe[r];
+            v[0] = str;
+            v[1] = (1.0 - kc * k0 * k0) * str;
+            v[2] = (1.0 - kc * k1 * k1) * str;
+            v[3] = (1.0 - kc * k2 * k2) * str;
+            v[4] = -kc * k0 * k1 * str;
+            v[5] = -kc * k0 * k2 * str;
+            v[6] = -kc * k1 * k2 * str;
+        }
+    }
+    block_partials<7>(v, partials);
+}
+
+// The same over the FP64 low-|k| list.
+__global__ void k_aks_energy_low(int ncol, int nzmax, const int* __restrict__ cols, const double* __restrict__ aks,
+                                 const double* __restrict__ Ak, const double* __restrict__ kcoe, CellP c,
+                                 double* partials) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (r < ncol * nzmax) {
+        const int cidx = r / nzmax, mz = r % nzmax;
+        const double ak = (mz < cols[4 * cidx + 3]) ? Ak[r] : 0.0;
+        if (ak != 0.0) {
+            const double nx = cols[4 * cidx], ny = cols[4 * cidx + 1], nz = cols[4 * cidx + 2] + mz;
+            const double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz * c.B[2]);
+            const double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz * c.B[5]);
+            const double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz * c.B[8]);
+            const double ar = aks[r], ai = aks[(size_t)ncol * nzmax + r];
+            const double str = (ar * ar + ai * ai) / ak;
+            const double kc = kcoe[r];
+            v[0] = str;
+            v[1] = (1.0 - kc * k0 * k0) * str;
+            v[2] = (1.0 - kc * k1 * k1) * str;
+            v[3] = (1.0 - kc * k2 * k2) * str;
+            v[4] = -kc * k0 * k1 * str;
+            v[5] = -kc * k0 * k2 * str;
+            v[6] = -kc * k1 * k2 * str;
+        }
+    }
+    block_partials<7>(v, partials);
+}
+
+// Snapshot (copy != 0) or PCG-step accumulation of the current A_k S sets
+// (rectangle and, on the mixed path, the low-|k| list) into the solver's
+// accumulators.
+void launch_aks_accumulate(cudaStream_t st, const KGrid& kg, RecScratch& rs, const DevScalars* d, int copy) {
+    const int m = 2 * kg.nrect;
+    k_aks_axpy<<<(m + 255) / 256, 256, 0, st>>>(m, d, copy, rs.aks, rs.aks_acc);
+    if (rs.low.ncol > 0 && rs.low.aks_acc) {
+        const int ml = 2 * rs.low.ncol * rs.low.nzmax;
+        k_aks_axpy<<<(ml + 255) / 256, 256, 0, st>>>(ml, d, copy, rs.low.aks, rs.low.aks_acc);
+    }
+}
+
 static RecLaunch plan(int n, const KGrid& kg) {
     RecLaunch L;
     L.CH = 16;
@@ -743,6 +831,8 @@ size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart) {
     return (size_t)L.P * rows * kg.ncol * 2;
 }
 
+#define CUDA_COPY_ACC(st, dst, src, bytes) cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (st))
+
 void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl, RecScratch& rs,
                       double* ef, double* efg, double* fo, Partials& part, DevScalars* d, Prof* prof) {
@@ -758,7 +848,28 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     const int rb = (total + 255) / 256;
     prof->begin(PK_SFAC);
     int nk = 2 + (fl.energy ? 1 : 0);
-    if (mixed) {
+    if (fl.reuse) {
+        // A_k S from the solver's accumulators: no structure-factor pass
+        CUDA_COPY_ACC(st, rs.aks, rs.aks_acc, sizeof(double) * 2 * kg.nrect);
+        nk = 0;
+        if (fl.energy) {
+            const double* akr = low ? kg.Ak_hi : kg.Ak;
+            k_aks_energy<<<rb, 256, 0, st>>>(kg.ncol, kg.nzl, ky, kz, rs.aks, kg.nrect, akr, kg.kcoe, c, part.buf);
+            launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
+            nk += 2;
+        }
+        if (low) {
+            LowK& lk = rs.low;
+            const int ml = lk.ncol * lk.nzmax;
+            CUDA_COPY_ACC(st, lk.aks, lk.aks_acc, sizeof(double) * 2 * ml);
+            if (fl.energy) {
+                const int lb = (ml + 255) / 256;
+                k_aks_energy_low<<<lb, 256, 0, st>>>(lk.ncol, lk.nzmax, lk.col, lk.aks, lk.Ak, lk.kcoe, c, part.buf);
+                launch_reduce_partials(st, part.buf, lb, 7, d->rec, 1);
+                nk += 2;
+            }
+        }
+    } else if (mixed) {
         if (rs.tab_epoch != rs.want_epoch) {
             k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab,
                                                            rs.low.ncol > 0 ? rs.low.tab : nullptr);
@@ -786,8 +897,8 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, L.CH, L.nchunk, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak, kg.kcoe,
                                           c, rs.aks, kg.nrect, fl.energy, part.buf);
     }
-    if (fl.energy) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
-    if (low) {
+    if (fl.energy && !fl.reuse) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
+    if (low && !fl.reuse) {
         LowK& lk = rs.low;
         const int nch = (lk.nzmax + TM - 1) / TM;
         const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;

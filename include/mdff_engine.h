@@ -337,6 +337,31 @@ int  mdff_batch_set_targets(mdff_batch* b, const double* fx, const double* fy, c
  * iters (may be NULL) receives the forward and adjoint solve iterations. */
 int  mdff_batch_loss_grad(mdff_batch* b, double* loss, mdff_param_grad* grad, int iters[2]);
 
+/*
+ * Reciprocal-space Ewald energy of point charges that allocates no device
+ * memory (no reference counterpart).  For callers that cannot let a library
+ * allocate device memory while they run: a host code whose device memory is
+ * held entirely by its own pool, or one that must not enter the CUDA
+ * allocator inside a time step.  Inputs are the caller's DEVICE arrays (rx,
+ * ry, rz Cartesian positions and q charges, natm each) on `device`; A is the
+ * host cell matrix (column-major, as in mdff_set_system), kmax the host k
+ * rectangle; stream is a cudaStream_t (NULL: the legacy default stream).
+ * *u_rec receives the energy in eV with coul_unit applied, the same quantity
+ * as mdff_energies.u_rec of mdff_engforce for a charges-only system.  The call
+ * returns after the result is on the host.
+ *
+ * Scratch is a fixed 16 MiB array in device memory per device (2^21 doubles):
+ * a problem needing more (3 natm + the structure-factor partials) returns
+ * MDFF_E_NOMEM, and *scratch_needed (may be NULL) receives the doubles it
+ * would need.  The first call on a device looks up the scratch's address
+ * (one-time set-up), so make that first call before any stream capture.  All
+ * calls on one device share the scratch: overlapping calls race and must be
+ * serialised by the caller.
+ */
+int  mdff_rec_energy_noalloc(int device, int natm, const double* rx, const double* ry, const double* rz,
+                             const double* q, const double A[9], double alpha, const int kmax[3],
+                             void* stream, double* u_rec, long long* scratch_needed);
+
 #ifdef __cplusplus
 }
 #endif

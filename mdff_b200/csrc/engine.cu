@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1365,3 +1366,134 @@ int mdff_step(mdff_ctx* ctx, int nsteps, double* rx, double* ry, double* rz, dou
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Reciprocal-space energy of point charges without any device allocation.
+//
+// Some callers cannot let the library allocate device memory during a run:
+// a host code whose device memory is entirely held by its own pool (a Fortran
+// code that reserves the GPU at start-up, or a PyTorch process whose caching
+// allocator already owns the free memory), or code that must not enter the
+// CUDA allocator in the middle of a time step.  mdff_rec_energy_noalloc reads
+// the caller's own device arrays and keeps all of its scratch in one fixed
+// array in device global memory, so it calls neither cudaMalloc nor cudaFree.
+//
+// The scratch holds the fractional coordinates, the structure-factor partials
+// and the energy partials of one call; nothing in it has to start at zero
+// (every word a call reads is written earlier in the same call).  There is one
+// scratch per device, so two calls that overlap on the same device (two host
+// threads, or two streams without ordering between them) race on it and must
+// be serialised by the caller.
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_DOUBLES = (size_t)1 << 21;   // 16 MiB of device memory per device
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Energy sum over the k rectangle from the structure-factor partials, with
+// A_k = exp(-k^2/4 alpha^2)/k^2 evaluated in place (no k table): the energy
+// part of k_sfac_reduce.
+__global__ void k_sfac_energy_inplace(int P, int ch, int nchunk, int ncol, int nzl, int ky, int kz,
+                                      const double* __restrict__ part_re, const double* __restrict__ part_im,
+                                      double inv4a2, CellP c, double* partials) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[1] = {0.0};
+    if (t < ncol * nzl) {
+        const int col = t % ncol;
+        const int mz = t / ncol;
+        const int ny_n = 2 * ky + 1;
+        const int nx = col / ny_n, ny = col % ny_n - ky, nz = mz - kz;
+        const bool keep = nx > 0 || (nx == 0 && ny > 0) || (nx == 0 && ny == 0 && nz > 0);
+        if (keep) {
+            const size_t plane = (size_t)ncol * ch * nchunk;
+            const size_t off = (size_t)mz * ncol + col;
+            double sr = 0.0, si = 0.0;
+            for (int p = 0; p < P; ++p) {
+                sr += part_re[(size_t)p * plane + off];
+                si += part_im[(size_t)p * plane + off];
+            }
+            const double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz * c.B[2]);
+            const double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz * c.B[5]);
+            const double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz * c.B[8]);
+            const double kk = k0 * k0 + k1 * k1 + k2 * k2;
+            if (kk != 0.0) v[0] = (sr * sr + si * si) * (exp(-kk * inv4a2) / kk);
+        }
+    }
+    block_partials<1>(v, partials);
+}
+
+// Device address of this device's scratch, looked up once per device with
+// that device current.
+int noalloc_scratch(int device, double** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MDFF_E_CUDA;
+        g_noalloc_ptr[device] = (double*)p;
+    }
+    *out = g_noalloc_ptr[device];
+    return MDFF_OK;
+}
+
+}  // namespace
+
+extern "C" int mdff_rec_energy_noalloc(int device, int natm, const double* rx, const double* ry, const double* rz,
+                                       const double* q, const double A[9], double alpha, const int kmax[3],
+                                       void* stream, double* u_rec, long long* scratch_needed) {
+    if (!rx || !ry || !rz || !q || !A || !kmax || !u_rec || natm < 1 || !(alpha > 0.0)) return MDFF_E_ARG;
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) return MDFF_E_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (kmax[d] < 0 || kmax[d] > 64) return MDFF_E_ARG;
+    // scratch layout: sx sy sz (3 natm), partials (2 plane), energy partials, result
+    KGrid kg;
+    for (int d = 0; d < 3; ++d) kg.kmax[d] = kmax[d];
+    kg.ncol = (kmax[0] + 1) * (2 * kmax[1] + 1);
+    kg.nzl = 2 * kmax[2] + 1;
+    kg.nrect = kg.ncol * kg.nzl;
+    const RecLaunch L = plan(natm, kg);
+    const size_t plane = (size_t)L.P * L.nchunk * L.CH * kg.ncol;
+    const int rb = (kg.nrect + 255) / 256;
+    const size_t need = 3 * (size_t)natm + 2 * plane + (size_t)rb + 1;
+    if (scratch_needed) *scratch_needed = (long long)need;
+    if (need > NOALLOC_SCRATCH_DOUBLES) return MDFF_E_NOMEM;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return MDFF_E_CUDA;
+    if (prev != device && cudaSetDevice(device) != cudaSuccess) return MDFF_E_CUDA;
+    int rc = MDFF_OK;
+    double* scr = nullptr;
+    if ((rc = noalloc_scratch(device, &scr)) == MDFF_OK) {
+        cudaStream_t st = (cudaStream_t)stream;
+        CellP c;
+        double W[3], anorm[3];
+        lattice(A, c, W, anorm);
+        double *sx = scr, *sy = scr + natm, *sz = scr + 2 * (size_t)natm;
+        double* pre = scr + 3 * (size_t)natm;
+        double* pim = pre + plane;
+        double* epart = pim + plane;
+        double* res = epart + rb;
+        launch_frac(st, natm, rx, ry, rz, c, sx, sy, sz);
+        dim3 g1(L.nchunk * L.ncolblk, L.P);
+#define SFAC_NA(CHV) k_sfac<CHV><<<g1, SF_THREADS, 0, st>>>(natm, L.natom_chunk, sx, sy, sz, q, nullptr, c, kmax[0], \
+                                                        kmax[1], kmax[2], kg.ncol, L.ncolblk, L.nchunk, 1, 0, pre, pim)
+        if (L.CH == 16) SFAC_NA(16);
+        else if (L.CH == 12) SFAC_NA(12);
+        else SFAC_NA(8);
+#undef SFAC_NA
+        k_sfac_energy_inplace<<<rb, 256, 0, st>>>(L.P, L.CH, L.nchunk, kg.ncol, kg.nzl, kmax[1], kmax[2], pre, pim,
+                                                  0.25 / (alpha * alpha), c, epart);
+        launch_reduce_partials(st, epart, rb, 1, res, 0);
+        double h = 0.0;
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            rc = MDFF_E_CUDA;
+        else
+            *u_rec = h * 2.0 * (2.0 * PI / c.omega) * 14.3996441494161;   // eV, as mdff_energies.u_rec
+    }
+    if (prev != device) cudaSetDevice(prev);
+    return rc;
+}

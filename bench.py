@@ -44,6 +44,12 @@ def parse():
     ap.add_argument("--ext", default="aspc", choices=["aspc", "poly"],
                     help="induced-dipole predictor (algo_ext_dipole)")
     ap.add_argument("--ext-order", type=int, default=3, help="extrapolate_order of the predictor")
+    ap.add_argument("--ksplit", type=float, default=None,
+                    help="mixed path: |k| below ksplit*alpha summed in FP64 (default: the library's)")
+    ap.add_argument("--keps", type=float, default=None,
+                    help="mixed path: leave out k with exp(-k^2/4 alpha^2) below keps (0: all; default: the library's)")
+    ap.add_argument("--reuse", default="auto", choices=["auto", "0", "1"],
+                    help="kspace_reuse (auto: on for the mixed path, off for the plain FP64 path)")
     ap.add_argument("--accuracy", action="store_true",
                     help="error of the mixed path against the FP64 path on snapshots of an FP64 trajectory")
     ap.add_argument("--snapshots", type=int, default=3)
@@ -131,17 +137,6 @@ def barrier(dist, device):
         dist.barrier(device_ids=[device.index])
 
 
-def flop_model(natm, nk_rect, iters, with_efg):
-    """Algorithmic FP work of the reciprocal-space kernels per MD step, counted
-    from the kernel source: per (atom, k) pair, structure factor 15 flops
-    (4 FMA accumulate, complex rotation, k.mu update); field 18 flops (E only)
-    or 36 (E and field gradient).  Evaluations per step: static field, one per
-    solver iteration (+1 for the initial residual) and the final forces."""
-    evals_e = 2 + iters          # static + initial residual + iterations (field only)
-    per_pair = evals_e * (15 + 18) + (15 + 36)
-    return float(natm) * nk_rect * per_pair
-
-
 def run_engine(args):
     import torch
     world, rank, local, dist = dist_setup(args.gpus)
@@ -155,6 +150,11 @@ def run_engine(args):
     p.device = local
     p.algo_ext_dipole = abi.EXT_ASPC if args.ext == "aspc" else abi.EXT_POLY
     p.extrapolate_order = args.ext_order
+    p.kspace_reuse = (1 if args.precision == "mixed" else 0) if args.reuse == "auto" else int(args.reuse)
+    if args.ksplit is not None:
+        p.mixed_ksplit = args.ksplit
+    if args.keps is not None:
+        p.mixed_keps = args.keps
     natm = len(s["itype"])
     eng = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
     eng.enable_profile(True)
@@ -207,15 +207,26 @@ def run_engine(args):
     result = None
     if rank == 0:
         pipes = mdff_b200.measure_pipes(local)
-        nk_rect = (p.kES[0] + 1) * (2 * p.kES[1] + 1) * (2 * p.kES[2] + 1)
+        ki = eng.kspace_info()
+        # algorithmic k-vectors per evaluation: the reference's half space on
+        # the FP64 path; the FP32 set plus the FP64 low set on the mixed path
+        nk_eff = (ki["fp32"] + ki["low"]) if args.precision == "mixed" else ki["half"]
         mean_it = float(np.mean(iters))
         kern = {k: v for k, v in prof.items() if v["count"] > 0 and not k.startswith("_")}
         ksf = kern.get("sfac", {"ms": 0.0, "count": 0})
         kkf = kern.get("kfield", {"ms": 0.0, "count": 0})
-        # algorithmic flops of the dominant pair of kernels over the timed region
-        n_e = 2 + mean_it
-        sf_flops = natm * nk_rect * 15.0 * (n_e + 1) * args.steps
-        kf_flops = natm * nk_rect * (18.0 * n_e + 36.0) * args.steps
+        # algorithmic flops of the dominant pair of kernels over the timed region.
+        # Evaluations per step: plain sequence: structure factor for the static
+        # field, the first residual, each iteration and the forces; field for
+        # all but the forces (E) plus one with the field gradient.  With
+        # kspace_reuse the static field and first residual share one
+        # evaluation and the forces take no structure-factor pass.
+        if p.kspace_reuse:
+            n_sf, n_e = 1 + mean_it, 1 + mean_it
+        else:
+            n_sf, n_e = 3 + mean_it, 2 + mean_it
+        sf_flops = natm * nk_eff * 15.0 * n_sf * args.steps
+        kf_flops = natm * nk_eff * (18.0 * n_e + 36.0) * args.steps
         k_ms = ksf["ms"] + kkf["ms"]
         achieved = (sf_flops + kf_flops) / (k_ms / 1e3) / 1e12 if k_ms > 0 else None
         peak = pipes[1] if args.precision == "mixed" else pipes[0]
@@ -233,10 +244,13 @@ def run_engine(args):
             "vs_baseline": None,
             "dtype": "fp32+fp64" if args.precision == "mixed" else "fp64",
             "data": "synthetic (seeded MgO polarisable-ion cell, mdff_b200.systems.mgo_production)",
-            "config": {"workload": "mgo-pim-production", "natm": natm, "kmax": list(p.kES), "nk_half": None,
+            "config": {"workload": "mgo-pim-production", "natm": natm, "kmax": list(p.kES), "k_vectors": ki,
                        "rc": p.cutlongrange, "alpha": p.alphaES, "ensemble": "nvt-nhcn", "nhc_n": p.nhc_n,
                        "dt_ps": p.dt, "efg_period": p.efg_period, "solver": "pcg", "tol": p.conv_tol_ind,
                        "predictor": "%s order %d" % (args.ext, args.ext_order),
+                       "kspace_reuse": int(p.kspace_reuse),
+                       "mixed_ksplit": p.mixed_ksplit if args.precision == "mixed" else None,
+                       "mixed_keps": p.mixed_keps if args.precision == "mixed" else None,
                        "precision": args.precision, "parallelism": f"replicas{world}",
                        "l2": "per-step working set > 126 MB L2 (k-space partials, Verlet lists)"},
             "gpu_launches": int(prof["_launches"]["count"]),
@@ -304,6 +318,11 @@ def run_accuracy(args):
     pm = abi.Params()
     C.pointer(pm)[0] = p
     pm.precision = abi.PREC_MIXED
+    pm.kspace_reuse = 1 if args.reuse in ("auto", "1") else 0
+    if args.ksplit is not None:
+        pm.mixed_ksplit = args.ksplit
+    if args.keps is not None:
+        pm.mixed_keps = args.keps
     pf = abi.Params()
     C.pointer(pf)[0] = p
     snaps = []
@@ -332,7 +351,9 @@ def run_accuracy(args):
             "du_per_atom_eV": abs(a["e"]["u_coul"] - b["e"]["u_coul"]) / len(pos),
             "iters": [a["e"]["scf_iter"], b["e"]["scf_iter"]],
         })
-    return {"mode": "accuracy", "workload": "mgo-pim-production", "natm": len(s["itype"]), "snapshots": snaps,
+    return {"mode": "accuracy", "workload": "mgo-pim-production", "natm": len(s["itype"]),
+            "mixed": {"kspace_reuse": int(pm.kspace_reuse), "mixed_ksplit": pm.mixed_ksplit,
+                      "mixed_keps": pm.mixed_keps}, "snapshots": snaps,
             "eps_F_max": max(x["eps_F"] for x in snaps)}
 
 

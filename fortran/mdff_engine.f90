@@ -76,6 +76,8 @@ module mdff_engine
     integer(c_int) :: erfc_ref
     integer(c_int) :: nhc_literal
     real(c_double) :: mixed_ksplit
+    integer(c_int) :: kspace_reuse
+    real(c_double) :: mixed_keps
   end type mdff_params_t
 
   type, bind(C) :: mdff_energies_t

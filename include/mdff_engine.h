@@ -131,6 +131,11 @@ typedef struct mdff_params {
     int    erfc_ref;                           /* 1: the reference's fitted erfc (src/functions.f90:28-39) */
     int    nhc_literal;                        /* 1: chain_nhcn's literal force order (stale G(2..M-1)) */
     double mixed_ksplit;                       /* mixed path: |k| < mixed_ksplit*alpha summed in FP64 (0: none) */
+    int    kspace_reuse;                       /* PCG: one reciprocal evaluation for the static field and the first
+                                                  residual, and the final structure factor from the solver's by
+                                                  linearity (0: the reference's sequence of evaluations) */
+    double mixed_keps;                         /* mixed path: k-vectors whose Gaussian factor exp(-k^2/4 alpha^2)
+                                                  is below mixed_keps are left out (0: the whole rectangle) */
 } mdff_params;
 
 /* Energies and scalar outputs of one force evaluation (thermodynamic module
@@ -222,6 +227,13 @@ int  mdff_stream(mdff_ctx* ctx, void** stream);
  * clears them when reset != 0. */
 int  mdff_profile(mdff_ctx* ctx, int enable);
 int  mdff_profile_get(mdff_ctx* ctx, double ms[8], long long count[8], long long* launches, int reset);
+
+/* Sizes of the reciprocal-space sums of the context (no reference
+ * counterpart): out[0] the k rectangle the kernels sweep, out[1] the k-vectors
+ * of the reference's half space (kpoint_sum_init, src/kspace.f90:142-207),
+ * out[2] the FP32 set and out[3] the FP64 low-|k| set of the mixed path (both
+ * 0 on the FP64 path). */
+int  mdff_kspace_info(mdff_ctx* ctx, long long out[4]);
 
 /* Define the system: natm atoms, 1-based types, Cartesian positions and the
  * cell.  Replaces read_pos + typeinfo_init (src/read_pos.f90:35-219): the cell

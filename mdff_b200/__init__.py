@@ -63,6 +63,7 @@ def lib():
         L.mdff_profile_get.argtypes = [vp, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int]
         L.mdff_measure_pipes.argtypes = [C.c_int, dp]
         L.mdff_struct_size.argtypes = [C.c_int]
+        L.mdff_kspace_info.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.mdff_batch_create.argtypes = [C.POINTER(abi.Params), C.c_int, ip, ip, dp, dp, dp, dp, dp, dp, ip, C.POINTER(vp)]
         L.mdff_batch_destroy.argtypes = [vp]
         L.mdff_batch_destroy.restype = None
@@ -124,6 +125,13 @@ class Engine:
         if rc != 0:
             msg = lib().mdff_last_error(self._h).decode() if self._h else "no context"
             raise EngineError(rc, msg)
+
+    def kspace_info(self):
+        """k-vector counts: rectangle, reference half space, mixed FP32 set,
+        mixed FP64 low set."""
+        out = (C.c_longlong * 4)()
+        self._check(lib().mdff_kspace_info(self._h, out))
+        return {"rect": out[0], "half": out[1], "fp32": out[2], "low": out[3]}
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

@@ -55,6 +55,7 @@ class Params(C.Structure):
         ("timesca_thermo", C.c_double),
         ("precision", C.c_int), ("efg_period", C.c_int), ("nlist_capacity", C.c_int), ("device", C.c_int),
         ("erfc_ref", C.c_int), ("nhc_literal", C.c_int), ("mixed_ksplit", C.c_double),
+        ("kspace_reuse", C.c_int), ("mixed_keps", C.c_double),
     ]
 
 
@@ -138,5 +139,6 @@ def default_params():
     p.efg_period = 0
     p.nlist_capacity = 0
     p.device = 0
-    p.mixed_ksplit = 3.4
+    p.mixed_ksplit = 2.5
+    p.mixed_keps = 1e-7
     return p

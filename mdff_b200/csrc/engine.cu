@@ -87,6 +87,8 @@ struct mdff_ctx {
     double tau_nonb[9], tau_coul[9];
     int last_rebuilt = 0;
     int nrebuild = 0;
+    bool rec_acc_ready = false;   // rs.aks_acc holds A_k S of the charges + final dipoles
+    long long kinfo[4] = {0, 0, 0, 0};   // rectangle, half space, FP32 set, FP64 low set
     Prof prof;
 };
 
@@ -420,16 +422,32 @@ DirFlags dir_flags(const mdff_ctx* ctx) {
 
 // Field of the induced dipoles: real space (dipole-dipole, undamped) +
 // reciprocal space + self term; src/field.f90:3354-3357.
-int induced_field(mdff_ctx* ctx, const double* m, double* out) {
+// Real-space part of the dipole field operator: FP64 (MODE 1 of
+// k_ewald_dir) or, on the mixed path, FP32 arithmetic from the fixed-point
+// coordinates (k_ewald_dd32).
+void dd_field_real(mdff_ctx* ctx, const double* m, double* out) {
     const int n = ctx->n;
+    ctx->prof.begin(PK_DIR);
+    if (ctx->p.precision == MDFF_PREC_MIXED) {
+        int k = ctx->rs.tab_epoch != ctx->rs.want_epoch ? 2 : 1;
+        ensure_phase_tables(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->rs);
+        launch_ewald_dd32(ctx->st, n, ctx->rs.fixed, m, ctx->cell, coul_list(ctx), ctx->cut_coul * ctx->cut_coul,
+                          ctx->alphaES, out);
+        ctx->prof.end(k);
+        return;
+    }
     DirFlags f = dir_flags(ctx);
     f.dd = 1;
     f.field = 1;
-    ctx->prof.begin(PK_DIR);
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, nullptr, m, ctx->cell, coul_list(ctx), ctx->pc,
                      f, out, nullptr, nullptr, ctx->part, ctx->dsc);
     ctx->prof.end(1);
-    RecFlags rf{0, 1, 1, 0, 0, 0, ctx->p.precision};
+}
+
+int induced_field(mdff_ctx* ctx, const double* m, double* out) {
+    const int n = ctx->n;
+    dd_field_real(ctx, m, out);
+    RecFlags rf{0, 1, 1, 0, 0, 0, ctx->p.precision, 0};
     launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, nullptr, m, ctx->cell, ctx->kg, rf, ctx->rs, out, nullptr,
                      nullptr, ctx->part, ctx->dsc, &ctx->prof);
     ctx->prof.begin(PK_SOLVER);
@@ -452,13 +470,45 @@ int static_field(mdff_ctx* ctx) {
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->dip0, ctx->cell, coul_list(ctx),
                      ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc);
     ctx->prof.end(2);
-    RecFlags rf{1, ctx->any_dip0 ? 1 : 0, 1, 0, 0, 0, ctx->p.precision};
+    RecFlags rf{1, ctx->any_dip0 ? 1 : 0, 1, 0, 0, 0, ctx->p.precision, 0};
     launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->dip0, ctx->cell, ctx->kg, rf, ctx->rs,
                      ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, &ctx->prof);
     ctx->prof.begin(PK_SOLVER);
     k_axpy<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, 2.0 * selfa2(ctx), ctx->dip0, ctx->Estat);
     ctx->prof.end(1);
     return check_launch(ctx, "static_field");
+}
+
+// Static field and the field of the initial guess x0 (mu_ind) together, for
+// the PCG's first residual r0 = b - A x0 (kspace_reuse): the real-space parts
+// are the same two sums as static_field / induced_field, the reciprocal part is
+// ONE evaluation of the sources q + dip0 + x0 added to Estat (r0 only needs the
+// sum), and its A_k S is the starting value of the solver's accumulator.
+int fused_initial_field(mdff_ctx* ctx) {
+    const int n = ctx->n, n3 = 3 * n;
+    DirFlags f = dir_flags(ctx);
+    f.qq = 1;
+    f.qd = ctx->any_dip0 ? 1 : 0;
+    f.dd = ctx->any_dip0 ? 1 : 0;
+    f.damp = 1;
+    f.field = 1;
+    ctx->prof.begin(PK_DIR);
+    launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->dip0, ctx->cell, coul_list(ctx),
+                     ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc);
+    ctx->prof.end(2);
+    dd_field_real(ctx, ctx->mu_ind, ctx->Eind);
+    ctx->prof.begin(PK_OTHER);
+    k_add3<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->dip0, ctx->mu_ind, ctx->mu);   // ctx->mu as scratch
+    ctx->prof.end(1);
+    RecFlags rf{1, 1, 1, 0, 0, 0, ctx->p.precision, 0};
+    launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->mu, ctx->cell, ctx->kg, rf, ctx->rs,
+                     ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, &ctx->prof);
+    ctx->prof.begin(PK_SOLVER);
+    launch_aks_accumulate(ctx->st, ctx->kg, ctx->rs, ctx->dsc, 1);
+    k_axpy<<<nb(n3), 256, 0, ctx->st>>>(n3, 2.0 * selfa2(ctx), ctx->dip0, ctx->Estat);
+    k_axpy<<<nb(n3), 256, 0, ctx->st>>>(n3, 2.0 * selfa2(ctx), ctx->mu_ind, ctx->Eind);
+    ctx->prof.end(ctx->rs.low.ncol > 0 ? 4 : 3);
+    return check_launch(ctx, "fused_initial_field");
 }
 
 // Extrapolated initial guess from the stored history (extrapolate_dipole_poly,
@@ -508,7 +558,9 @@ int solve_dipoles(mdff_ctx* ctx) {
     const int n = ctx->n, n3 = 3 * n;
     const mdff_params& p = ctx->p;
     DevScalars* d = ctx->dsc;
-    TRY(static_field(ctx));
+    const bool reuse = p.kspace_reuse && p.algo_moment_from_pola == MDFF_POLA_PCG;
+    ctx->rec_acc_ready = false;
+    if (!reuse) TRY(static_field(ctx));
     const double inv_npol = 1.0 / (double)ctx->npol;
     int iscf = 0;
     double rmsd = 1e300;
@@ -545,7 +597,8 @@ int solve_dipoles(mdff_ctx* ctx) {
     } else {
         TRY(predict(ctx, ctx->mu_ind));
         // zero the guess on non-polarisable atoms: Ad = A x uses the mask
-        TRY(induced_field(ctx, ctx->mu_ind, ctx->Eind));
+        if (reuse) TRY(fused_initial_field(ctx));
+        else TRY(induced_field(ctx, ctx->mu_ind, ctx->Eind));
         ctx->prof.begin(PK_SOLVER);
         k_apply_A<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->mu_ind, ctx->Eind, ctx->inv_alpha, ctx->cg_Ad);
         k_cg_init<<<vb, 256, 0, ctx->st>>>(n, ctx->Estat, ctx->cg_Ad, ctx->alpha, ctx->inv_alpha, ctx->cg_r, ctx->cg_z,
@@ -563,10 +616,12 @@ int solve_dipoles(mdff_ctx* ctx) {
             launch_dot(ctx->st, n3, ctx->cg_d, ctx->cg_Ad, ctx->part, &d->dAd);
             k_cg_update<<<vb, 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->cg_Ad, ctx->alpha, ctx->mu_ind, ctx->cg_r, ctx->cg_z,
                                                  d, ctx->part.buf);
+            // the same step on the structure factors (before rz advances)
+            if (reuse) launch_aks_accumulate(ctx->st, ctx->kg, ctx->rs, d, 0);
             launch_reduce_partials(ctx->st, ctx->part.buf, vb, 2, &d->rr, 0);
             k_cg_scalars<<<1, 32, 0, ctx->st>>>(d, inv_npol, p.conv_tol_ind);
             k_cg_direction<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->cg_z, ctx->cg_d, d);
-            ctx->prof.end(8);
+            ctx->prof.end(8 + (reuse ? (ctx->rs.low.ncol > 0 ? 2 : 1) : 0));
             TRY(sync_scalars(ctx));
             rmsd = ctx->hsc->rmsd;
             if (!std::isfinite(rmsd)) return fail(ctx, MDFF_E_NONFINITE, "non-finite residual in the dipole solve");
@@ -584,6 +639,7 @@ int solve_dipoles(mdff_ctx* ctx) {
     ctx->en.scf_rmsd = rmsd;
     if (iscf >= p.max_scf_pol_iter && rmsd > p.conv_tol_ind && p.algo_moment_from_pola == MDFF_POLA_PCG)
         return fail(ctx, MDFF_E_NOCONV, "induced-dipole solve did not converge within max_scf_pol_iter");
+    ctx->rec_acc_ready = reuse;
     return MDFF_OK;
 }
 
@@ -638,7 +694,9 @@ int engforce_device(mdff_ctx* ctx) {
         launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->mu, ctx->cell, coul_list(ctx),
                          ctx->pc, f, ctx->ef, ctx->efg, ctx->fcoul, ctx->part, ctx->dsc);
         ctx->prof.end(2);
-        RecFlags rf{ctx->any_q ? 1 : 0, dip ? 1 : 0, p.doefield ? 1 : 0, (p.doefg || dip) ? 1 : 0, 1, 1, p.precision};
+        RecFlags rf{ctx->any_q ? 1 : 0, dip ? 1 : 0, p.doefield ? 1 : 0, (p.doefg || dip) ? 1 : 0, 1, 1, p.precision,
+                    ctx->rec_acc_ready ? 1 : 0};
+        ctx->rec_acc_ready = false;
         launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->mu, ctx->cell, ctx->kg, rf, ctx->rs, ctx->ef,
                          p.doefg ? ctx->efg : nullptr, ctx->fcoul, ctx->part, ctx->dsc, &ctx->prof);
         int vb = std::min(592, nb(n));
@@ -932,6 +990,13 @@ int mdff_stream(mdff_ctx* ctx, void** stream) {
     return MDFF_OK;
 }
 
+int mdff_kspace_info(mdff_ctx* ctx, long long out[4]) {
+    if (!ctx || !out) return MDFF_E_ARG;
+    if (!ctx->have_system) return fail(ctx, MDFF_E_STATE, "set_system first");
+    for (int k = 0; k < 4; ++k) out[k] = ctx->kinfo[k];
+    return MDFF_OK;
+}
+
 int mdff_struct_size(int which) {
     switch (which) {
         case 0: return (int)sizeof(mdff_params);
@@ -969,7 +1034,8 @@ void mdff_params_default(mdff_params* p) {
     p->nhc_mults = 2;
     p->timesca_thermo = 1.0;
     p->precision = MDFF_PREC_FP64;
-    p->mixed_ksplit = 3.4;
+    p->mixed_ksplit = 2.5;
+    p->mixed_keps = 1e-7;
 }
 
 int mdff_create(const mdff_params* p, mdff_ctx** out) {
@@ -1119,6 +1185,10 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 kc[(size_t)col * kg.nzl + m] = 2.0 * (1.0 / kk + 1.0 / a2 / 4.0);
             }
         }
+        ctx->kinfo[0] = kg.nrect;
+        ctx->kinfo[1] = 0;
+        for (double v : ak) ctx->kinfo[1] += v != 0.0;
+        ctx->kinfo[2] = ctx->kinfo[3] = 0;
         TRY(dalloc(ctx, &kg.Ak, kg.nrect));
         TRY(dalloc(ctx, &kg.kcoe, kg.nrect));
         TRY(upload(ctx, kg.Ak, ak.data(), kg.nrect));
@@ -1127,11 +1197,11 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
         // FP64 low set (one contiguous nz interval per column, |k|^2 being
         // convex in nz) and are removed from the FP32 set.
         ctx->rs.low = LowK();
+        std::vector<double> akhi = ak;   // the FP32 set of the mixed path
         if (p.precision == MDFF_PREC_MIXED && p.mixed_ksplit > 0.0) {
             const double ks2 = std::pow(p.mixed_ksplit * ctx->alphaES, 2);
             std::vector<int> cols;
             std::vector<double> akl, kcl;
-            std::vector<double> akhi = ak;
             int nzmax = 0;
             struct Col { int nx, ny, lo, nn; };
             std::vector<Col> cl;
@@ -1188,17 +1258,69 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 TRY(upload(ctx, lk.kcoe, kcl.data(), (int)kcl.size()));
                 TRY(dalloc(ctx, &lk.part, 2 * (size_t)lk.P * nzmax * lk.ncol));
                 TRY(dalloc(ctx, &lk.aks, 2 * (size_t)lk.ncol * nzmax));
+                TRY(dalloc(ctx, &lk.aks_acc, 2 * (size_t)lk.ncol * nzmax));
                 TRY(dalloc(ctx, &lk.fpart, 4 * 9 * (size_t)n));
                 TRY(dalloc(ctx, &lk.tab, 16 * (size_t)n));
-                TRY(dalloc(ctx, &kg.Ak_hi, kg.nrect));
-                TRY(upload(ctx, kg.Ak_hi, akhi.data(), kg.nrect));
             }
+        }
+        if (p.precision == MDFF_PREC_MIXED) {
+            // Leave out the k-vectors whose Gaussian factor exp(-k^2 / 4 alpha^2)
+            // is below mixed_keps (a sphere |k|^2 > -4 alpha^2 ln mixed_keps).
+            if (p.mixed_keps > 0.0) {
+                const double R2 = -4.0 * ctx->alphaES * ctx->alphaES * std::log(p.mixed_keps);
+                for (int col = 0; col < kg.ncol; ++col) {
+                    int nx = col / (2 * kg.kmax[1] + 1), ny = col % (2 * kg.kmax[1] + 1) - kg.kmax[1];
+                    for (int m = 0; m < kg.nzl; ++m) {
+                        int nz = m - kg.kmax[2];
+                        double kx = 2.0 * PI * (double(nx) * c.B[0] + double(ny) * c.B[1] + double(nz) * c.B[2]);
+                        double ky = 2.0 * PI * (double(nx) * c.B[3] + double(ny) * c.B[4] + double(nz) * c.B[5]);
+                        double kz = 2.0 * PI * (double(nx) * c.B[6] + double(ny) * c.B[7] + double(nz) * c.B[8]);
+                        if (kx * kx + ky * ky + kz * kz > R2) akhi[(size_t)col * kg.nzl + m] = 0.0;
+                    }
+                }
+            }
+            // per column the range of 16-wide nz chunks holding a nonzero entry,
+            // and the (column, chunk) work list of the FP32 structure factor
+            std::vector<int> crange(2 * (size_t)kg.ncol, 0), items;
+            for (int col = 0; col < kg.ncol; ++col) {
+                int lo = -1, hi = -1;
+                for (int m = 0; m < kg.nzl; ++m)
+                    if (akhi[(size_t)col * kg.nzl + m] != 0.0) { if (lo < 0) lo = m; hi = m; }
+                if (lo < 0) continue;
+                crange[2 * col] = lo / 16;
+                crange[2 * col + 1] = hi / 16 - lo / 16 + 1;
+                for (int h = lo / 16; h <= hi / 16; ++h) { items.push_back(col); items.push_back(h); }
+            }
+            kg.nitems = (int)(items.size() / 2);
+            for (double v : akhi) ctx->kinfo[2] += v != 0.0;
+            ctx->kinfo[3] = 0;
+            for (int col = 0; col < kg.ncol; ++col)
+                for (int m = 0; m < kg.nzl; ++m)
+                    if (ak[(size_t)col * kg.nzl + m] != 0.0 && akhi[(size_t)col * kg.nzl + m] == 0.0 &&
+                        ctx->rs.low.ncol > 0) {
+                        // in the low set when below the split (the rest is outside the sphere)
+                        int nx = col / (2 * kg.kmax[1] + 1), ny = col % (2 * kg.kmax[1] + 1) - kg.kmax[1];
+                        int nz = m - kg.kmax[2];
+                        double kx = 2.0 * PI * (double(nx) * c.B[0] + double(ny) * c.B[1] + double(nz) * c.B[2]);
+                        double ky = 2.0 * PI * (double(nx) * c.B[3] + double(ny) * c.B[4] + double(nz) * c.B[5]);
+                        double kz = 2.0 * PI * (double(nx) * c.B[6] + double(ny) * c.B[7] + double(nz) * c.B[8]);
+                        if (kx * kx + ky * ky + kz * kz < std::pow(p.mixed_ksplit * ctx->alphaES, 2)) ctx->kinfo[3]++;
+                    }
+            TRY(dalloc(ctx, &kg.colrange, crange.size()));
+            CK(cudaMemcpyAsync(kg.colrange, crange.data(), sizeof(int) * crange.size(), cudaMemcpyHostToDevice, ctx->st));
+            TRY(dalloc(ctx, &kg.items, std::max<size_t>(2, items.size())));
+            if (!items.empty())
+                CK(cudaMemcpyAsync(kg.items, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice, ctx->st));
+            TRY(dalloc(ctx, &kg.Ak_hi, kg.nrect));
+            TRY(upload(ctx, kg.Ak_hi, akhi.data(), kg.nrect));
+            CK(cudaStreamSynchronize(ctx->st));   // the host vectors above go out of scope
         }
         size_t fp = 0;
         size_t pc = rec_scratch_doubles(n, kg, &fp);
         TRY(dalloc(ctx, &ctx->rs.part, pc));
         TRY(dalloc(ctx, &ctx->rs.fpart, fp));
         TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));
+        TRY(dalloc(ctx, &ctx->rs.aks_acc, 2 * (size_t)kg.nrect));
         TRY(dalloc(ctx, &ctx->rs.fixed, 3 * (size_t)n));
         TRY(dalloc(ctx, &ctx->rs.tab, (size_t)n * 16));
         TRY(dalloc(ctx, &ctx->rs.aks2, (size_t)kg.ncol * (((kg.nzl + 15) / 16) * 16)));

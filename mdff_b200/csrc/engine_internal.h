@@ -187,7 +187,10 @@ struct KGrid {
     int nrect;           // ncol*nzl
     double* Ak = nullptr;      // [nrect], 0 for excluded k
     double* kcoe = nullptr;    // [nrect]
-    double* Ak_hi = nullptr;   // [nrect], Ak without the low-|k| set (mixed path)
+    double* Ak_hi = nullptr;   // [nrect], Ak of the FP32 set: without the low-|k| set and outside the sphere (mixed path)
+    int* colrange = nullptr;   // [ncol][2]: first 16-wide nz chunk and chunk count of the FP32 set (mixed path)
+    int* items = nullptr;      // [nitems][2]: (column, chunk) work list of the FP32 structure factor
+    int nitems = 0;
 };
 // The low-|k| set of the mixed path, summed in FP64 (see ewald_recip.cuh):
 // columns (nx, ny) with a contiguous nz range [nzlo, nzlo + nzn).
@@ -234,6 +237,9 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
                       Prof* prof);
 size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart);
 void launch_aks_accumulate(cudaStream_t st, const KGrid& kg, RecScratch& rs, const DevScalars* d, int copy);
+void ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs);
+void launch_ewald_dd32(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
+                       double cutsq, double alpha, double* ef);
 
 // Solver vector kernels.
 void launch_dot(cudaStream_t st, int n3, const double* a, const double* b, Partials& part, double* out);

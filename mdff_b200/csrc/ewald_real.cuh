@@ -169,6 +169,70 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
     }
 }
 
+// Mixed path: the dipole field operator E_i = sum_j T2(r_ij) mu_j in FP32
+// arithmetic with FP64 accumulation.  The minimum image comes exactly from the
+// 32-bit fixed-point fractional coordinates (the wrapped integer difference is
+// d - NINT(d)), r = A d in FP32; erfc, exp and the contraction in FP32.  r_ji
+// is exactly -r_ij, so the operator stays symmetric, which the conjugate
+// gradient needs.
+template <int G>
+__global__ void __launch_bounds__(256) k_ewald_dd32(int n, const uint32_t* __restrict__ fx,
+                                                    const double* __restrict__ mu, CellP c,
+                                                    const int* __restrict__ nbr, const int* __restrict__ cnt, int cap,
+                                                    float cutsq, float alpha, double* __restrict__ ef) {
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int sub = threadIdx.x & (G - 1);
+    const bool active = gid < n;
+    const int i = active ? gid : 0;
+    const float sc = 2.3283064365386963e-10f;   // 2^-32
+    const float A0 = (float)c.A[0], A1 = (float)c.A[1], A2 = (float)c.A[2];
+    const float A3 = (float)c.A[3], A4 = (float)c.A[4], A5 = (float)c.A[5];
+    const float A6 = (float)c.A[6], A7 = (float)c.A[7], A8 = (float)c.A[8];
+    const float a2 = alpha * alpha;
+    const float two_a_rpi = 2.0f * alpha * 0.5641895835477563f;          // 2 a / sqrt(pi)
+    const float four3_a3_rpi = 4.0f / 3.0f * a2 * alpha * 0.5641895835477563f;
+    double E0 = 0.0, E1 = 0.0, E2 = 0.0;
+    if (active) {
+        const uint32_t u1 = fx[i], u2 = fx[n + i], u3 = fx[2 * n + i];
+        const int m = cnt[i];
+        const int* row = nbr + (size_t)i * cap;
+        for (int k = sub; k < m; k += G) {
+            const int j = row[k];
+            const float d0 = (float)(int)(u1 - fx[j]) * sc;
+            const float d1 = (float)(int)(u2 - fx[n + j]) * sc;
+            const float d2 = (float)(int)(u3 - fx[2 * n + j]) * sc;
+            const float rx = fmaf(d0, A0, fmaf(d1, A1, d2 * A2));
+            const float ry = fmaf(d0, A3, fmaf(d1, A4, d2 * A5));
+            const float rz = fmaf(d0, A6, fmaf(d1, A7, d2 * A8));
+            const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+            if (r2 > cutsq) continue;
+            const float dm1 = rsqrtf(r2);
+            const float d = r2 * dm1;
+            const float dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2;
+            const float ex = __expf(-a2 * r2);
+            const float F1 = erfcf(alpha * d) + two_a_rpi * d * ex;
+            const float F2 = F1 + four3_a3_rpi * r2 * d * ex;
+            const float a1c = F1 * dm3, b2c = 3.0f * F2 * dm5;
+            const float mj0 = (float)mu[j], mj1 = (float)mu[n + j], mj2 = (float)mu[2 * n + j];
+            const float rb = fmaf(rx, mj0, fmaf(ry, mj1, rz * mj2)) * b2c;
+            E0 += (double)fmaf(rx, rb, -mj0 * a1c);
+            E1 += (double)fmaf(ry, rb, -mj1 * a1c);
+            E2 += (double)fmaf(rz, rb, -mj2 * a1c);
+        }
+    }
+    E0 = group_sum<G>(E0);
+    E1 = group_sum<G>(E1);
+    E2 = group_sum<G>(E2);
+    if (active && sub == 0) { ef[i] = E0; ef[n + i] = E1; ef[2 * n + i] = E2; }
+}
+
+void launch_ewald_dd32(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
+                       double cutsq, double alpha, double* ef) {
+    constexpr int G = 16;
+    const int blocks = (int)(((size_t)n * G + 255) / 256);
+    k_ewald_dd32<G><<<blocks, 256, 0, st>>>(n, fx, mu, c, l.nbr, l.cnt, l.cap, (float)cutsq, (float)alpha, ef);
+}
+
 void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const int* type, const double* q, const double* mu, CellP c, const NList& l,
                       const PairConst* pc, DirFlags fl, double* ef, double* efg, double* f, Partials& part,

@@ -113,13 +113,14 @@ __global__ void k_sfac_reduce(int P, int ch, int nchunk, int ncol, int nzl, int 
         const int mz = t / ncol;          // 0 .. nzl-1
         const size_t plane = (size_t)ncol * ch * nchunk;
         const size_t off = (size_t)mz * ncol + col;   // (h*ch + m) == mz
-        double sr = 0.0, si = 0.0;
-        for (int p = 0; p < P; ++p) {
-            sr += part_re[(size_t)p * plane + off];
-            si += part_im[(size_t)p * plane + off];
-        }
         const int r = col * nzl + mz;
         const double ak = Ak[r];
+        double sr = 0.0, si = 0.0;
+        if (ak != 0.0)   // entries outside the work list have no partials
+            for (int p = 0; p < P; ++p) {
+                sr += part_re[(size_t)p * plane + off];
+                si += part_im[(size_t)p * plane + off];
+            }
         aks[r] = ak * sr;
         aks[nrect + r] = ak * si;
         if (energy && ak != 0.0) {
@@ -328,15 +329,25 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac32v4(int n, int natom_chunk,
                                                          const float2* __restrict__ tab, const double* __restrict__ q,
                                                          const double* __restrict__ mu, CellP c, int kx, int ky, int kz,
                                                          int ncol, int ncolblk, int nchunk, int with_q,
+                                                         const int* __restrict__ items, int nitems,
                                                          double* __restrict__ part_re, double* __restrict__ part_im) {
     __shared__ uint32_t t_u1[SF4_TILE], t_u2[SF4_TILE], t_u3[SF4_TILE];
     __shared__ float t_q[SF4_TILE], t_m1[SF4_TILE], t_m2[SF4_TILE], t_m3[SF4_TILE];
     __shared__ float4 t_T[SF4_TILE][TM / 2];    // (T_m, T_m+1) pairs
-    const int h = blockIdx.x / ncolblk;
-    const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
+    // work item: (column, chunk of TM nz), from the work list when given
+    int h, col;
+    if (items) {
+        const int it = blockIdx.x * SF_THREADS + threadIdx.x;
+        const int itc = it < nitems ? it : nitems - 1;
+        col = it < nitems ? items[2 * itc] : ncol;
+        h = items[2 * itc + 1];
+    } else {
+        h = blockIdx.x / ncolblk;
+        col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
+    }
     const int p = blockIdx.y;
     const int ny_n = 2 * ky + 1;
-    const int colc = col < ncol ? col : ncol - 1;
+    const int colc = col < ncol ? col : (items ? items[2 * (nitems - 1)] : ncol - 1);
     const int inx = colc / ny_n, iny = colc % ny_n - ky, inz0 = -kz + h * TM;
     const float fnx = (float)inx, fny = (float)iny, fnz0 = (float)inz0;
     float ore[TM], oim[TM];
@@ -429,7 +440,8 @@ template <int GRAD>
 __global__ void __launch_bounds__(KF_THREADS) k_kfield32v4(int n, const uint32_t* __restrict__ fx,
                                                            const float2* __restrict__ tab, CellP c, int kx, int ky,
                                                            int kz, int ncol, int nzp, int cols_per_split,
-                                                           const float2* __restrict__ aks, double* __restrict__ fpart) {
+                                                           const float2* __restrict__ aks, const int* __restrict__ colrange,
+                                                           double* __restrict__ fpart) {
     extern __shared__ float2 ska[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int split = blockIdx.y;
@@ -456,16 +468,21 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v4(int n, const uint32_t
         __syncthreads();
         for (int cc = 0; cc < nc; ++cc) {
             const int col = cb + cc;
+            // the column's chunks of the FP32 set (all of them without a range table)
+            int clo = 0, cn = nzp / TM;
+            if (colrange) { clo = colrange[2 * col]; cn = colrange[2 * col + 1]; }
+            if (cn == 0) continue;
             const int inx = col / ny_n, iny = col % ny_n - ky;
-            const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)(-kz) * u3;
+            const int nzb = -kz + TM * clo;
+            const uint32_t ph = (uint32_t)inx * u1 + (uint32_t)iny * u2 + (uint32_t)nzb * u3;
             float ec, es;
             phase32(ph, ec, es);
-            const float fnx = (float)inx, fny = (float)iny, fnz = (float)(-kz);
+            const float fnx = (float)inx, fny = (float)iny, fnz = (float)nzb;
             float kb0 = fmaf(fnx, b1x, fmaf(fny, b2x, fnz * dk0));
             float kb1 = fmaf(fnx, b1y, fmaf(fny, b2y, fnz * dk1));
             float kb2 = fmaf(fnx, b1z, fmaf(fny, b2z, fnz * dk2));
             const float2* pk = ska + cc * nzp;
-            for (int m0 = 0; m0 < nzp; m0 += TM) {
+            for (int m0 = TM * clo; m0 < TM * (clo + cn); m0 += TM) {
                 float z0r = 0.f, z0i = 0.f, z1r = 0.f, z1i = 0.f, z2r = 0.f, z2i = 0.f;
 #pragma unroll
                 for (int m = 0; m < TM; ++m) {
@@ -831,6 +848,14 @@ size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart) {
     return (size_t)L.P * rows * kg.ncol * 2;
 }
 
+// The mixed path's fixed-point coordinates and phase tables for the current
+// positions (built once per position update).
+void ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs) {
+    if (rs.tab_epoch == rs.want_epoch) return;
+    k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab, rs.low.ncol > 0 ? rs.low.tab : nullptr);
+    rs.tab_epoch = rs.want_epoch;
+}
+
 #define CUDA_COPY_ACC(st, dst, src, bytes) cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (st))
 
 void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
@@ -853,7 +878,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         CUDA_COPY_ACC(st, rs.aks, rs.aks_acc, sizeof(double) * 2 * kg.nrect);
         nk = 0;
         if (fl.energy) {
-            const double* akr = low ? kg.Ak_hi : kg.Ak;
+            const double* akr = mixed ? kg.Ak_hi : kg.Ak;
             k_aks_energy<<<rb, 256, 0, st>>>(kg.ncol, kg.nzl, ky, kz, rs.aks, kg.nrect, akr, kg.kcoe, c, part.buf);
             launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
             nk += 2;
@@ -876,16 +901,19 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             rs.tab_epoch = rs.want_epoch;
             nk++;
         }
-        dim3 g1(nchunk32 * L.ncolblk, L.P);
-        if (fl.with_mu)
-            k_sfac32v4<1><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
-                                                     L.ncolblk, nchunk32, fl.with_q, pre, pim);
-        else
-            k_sfac32v4<0><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
-                                                     L.ncolblk, nchunk32, fl.with_q, pre, pim);
-        // the FP32 set excludes the low-|k| vectors (A_k = 0 there)
-        k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, TM, nchunk32, kg.ncol, kg.nzl, kx, ky, kz, pre, pim,
-                                          low ? kg.Ak_hi : kg.Ak, kg.kcoe, c, rs.aks, kg.nrect, fl.energy, part.buf);
+        // the FP32 set's (column, chunk) work list: the low-|k| vectors and
+        // those outside the sphere are not in it (A_k = 0 there)
+        dim3 g1((kg.nitems + SF_THREADS - 1) / SF_THREADS, L.P);
+        if (kg.nitems > 0) {
+            if (fl.with_mu)
+                k_sfac32v4<1><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
+                                                         L.ncolblk, nchunk32, fl.with_q, kg.items, kg.nitems, pre, pim);
+            else
+                k_sfac32v4<0><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
+                                                         L.ncolblk, nchunk32, fl.with_q, kg.items, kg.nitems, pre, pim);
+        }
+        k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, TM, nchunk32, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak_hi, kg.kcoe, c,
+                                          rs.aks, kg.nrect, fl.energy, part.buf);
     } else {
         dim3 g1(L.nchunk * L.ncolblk, L.P);
 #define SFAC(CHV) k_sfac<CHV><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, sx, sy, sz, q, mu, c, kx, ky, kz, kg.ncol, \
@@ -923,10 +951,10 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         k_aks32_pad<<<(kg.ncol * nzp + 255) / 256, 256, 0, st>>>(kg.ncol, kg.nzl, nzp, kg.nrect, rs.aks, rs.aks2);
         if (grad)
             k_kfield32v4<1><<<g2, KF_THREADS, sizeof(float2) * KF_COLS * nzp, st>>>(
-                n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, rs.fpart);
+                n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
         else
             k_kfield32v4<0><<<g2, KF_THREADS, sizeof(float2) * KF_COLS * nzp, st>>>(
-                n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, rs.fpart);
+                n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
         nk += 2;
         if (low) {
             LowK& lk = rs.low;

@@ -76,3 +76,24 @@ def test_pim_nve_with_extrapolation(ext):
         assert abs(a["e_tot"] - b["e_tot"]) < 1e-9 * abs(b["e_tot"])
         assert a["scf_iter"] == b["scf_iter"]
     assert rel(re["f"], ro["f"]) < 1e-8
+
+
+@pytest.mark.parametrize("ext", [(abi.EXT_POLY, 0), (abi.EXT_ASPC, 3)])
+def test_pim_pcg_kspace_reuse_vs_oracle(ext):
+    """kspace_reuse (one reciprocal evaluation for the static field and the
+    first residual; final structure factor from the solver's by linearity):
+    the same trajectory as the oracle's plain sequence of evaluations."""
+    s = systems.mgo_pim(grid=(6, 6, 6), rc=6.0, alpha=0.55, kmax=8, temp=1000.0)
+    p = s["params"]
+    p.algo_ext_dipole, p.extrapolate_order = ext
+    p.algo_moment_from_pola = abi.POLA_PCG
+    p.conv_tol_ind = 1e-11
+    p.doefg = 1
+    p.kspace_reuse = 1
+    te0, to0, re, ro = run_both(s, 8)
+    assert abs(te0["e_tot"] - to0["e_tot"]) < 1e-10 * abs(to0["e_tot"])
+    for a, b in zip(re["thermo"], ro["thermo"]):
+        assert abs(a["e_tot"] - b["e_tot"]) < 1e-9 * abs(b["e_tot"])
+        assert abs(a["pressure_tot"] - b["pressure_tot"]) < 1e-8 * max(1.0, abs(b["pressure_tot"]))
+    assert rel(re["f"], ro["f"]) < 1e-8
+

@@ -61,3 +61,23 @@ def test_mixed_md_energy_tracks_fp64():
         res[prec] = e.step(20)
     for a, b in zip(res[abi.PREC_MIXED]["thermo"], res[abi.PREC_FP64]["thermo"]):
         assert abs(a["e_tot"] - b["e_tot"]) < 1e-6 * abs(b["e_tot"])
+
+
+def test_mixed_kspace_reuse_matches_fp64():
+    """The mixed path with kspace_reuse and the FP32 real-space dipole operator
+    against the plain FP64 path."""
+    s = systems.mgo_pim(grid=(16, 16, 16), rc=10.0, alpha=0.3, kmax=12, vacancy_frac=0.01, seed=3, jitter=0.1)
+    out = {}
+    for prec, reuse in ((abi.PREC_FP64, 0), (abi.PREC_MIXED, 1)):
+        p = s["params"]
+        p.precision = prec
+        p.kspace_reuse = reuse
+        p.doefg = 1
+        p.conv_tol_ind = 1e-10
+        out[prec] = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"]).engforce()
+    m, d = out[abi.PREC_MIXED], out[abi.PREC_FP64]
+    assert rel(m["f"], d["f"]) < 1e-6
+    assert rel(m["mu"], d["mu"]) < 1e-6
+    assert rel(m["efg"], d["efg"]) < 1e-6
+    assert abs(m["e"]["u_coul"] - d["e"]["u_coul"]) < 1e-6 * abs(d["e"]["u_coul"])
+    assert rel(m["tau_coul"], d["tau_coul"]) < 1e-6

@@ -1078,6 +1078,70 @@ __global__ void k_b_alpha_grad(int N, const int* __restrict__ type, const double
     block_partials<NTYB>(v, part);
 }
 
+// Condition of the lockstep PCG loop (a conditional WHILE node of the batch's
+// CUDA graph): iterate while some configuration has not converged and fewer
+// than max_it iterations have run.  reset != 0 starts the count (before the
+// loop); otherwise one iteration has just finished.  The cap makes the loop
+// finite whatever the residuals do.
+__global__ void k_b_cg_cond(int nconf, const int* __restrict__ conv, int* loop_it, int max_it, int reset,
+                            cudaGraphConditionalHandle h) {
+    __shared__ int open_;
+    if (threadIdx.x == 0) open_ = 0;
+    __syncthreads();
+    for (int c = threadIdx.x; c < nconf; c += blockDim.x)
+        if (!conv[c]) open_ = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int it = reset ? 0 : *loop_it + 1;
+        *loop_it = it;
+        cudaGraphSetConditional(h, (open_ && it < max_it) ? 1u : 0u);
+    }
+}
+
+// After a solve: out[0] = largest iteration count, out[1] = configurations
+// not converged.
+__global__ void k_b_cg_summary(int nconf, const int* __restrict__ conv, const BScal* __restrict__ sc, int* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int it = 0, bad = 0;
+    for (int c = 0; c < nconf; ++c) {
+        it = max(it, sc[c].iter);
+        bad += conv[c] ? 0 : 1;
+    }
+    out[0] = it;
+    out[1] = bad;
+}
+
+// Per configuration: total stress tau = tau_nonb + tau_coul (GPa, column-major,
+// the assembly of engforce: pair sums / omega / press; real-space sums
+// 0.25/omega and reciprocal sums 2 tpi_V/omega, times cu / press), the loss
+// cF sum|dF|^2 + cS sum dtau^2 and S = dL/dtau (symmetrised).
+__global__ void k_b_loss_tail(int nconf, const BCfg* __restrict__ cf, const double* __restrict__ red_pair,
+                              const double* __restrict__ red_dir, const double* __restrict__ red_rec,
+                              const double* __restrict__ lossF, const double* __restrict__ tau_t, double cu,
+                              double press, int coul, double* loss_c, double* tau_c, double* Sres) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nconf) return;
+    const BCfg& C = cf[c];
+    const double om = C.cell.omega, tpi_V = 2.0 * PI / om;
+    const int map[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    double tau[9];
+    for (int k = 0; k < 6; ++k) {
+        double v = red_pair[7 * c + 1 + k] / om / press;
+        if (coul) v += (red_dir[7 * c + 1 + k] * 0.25 / om + red_rec[8 * c + 1 + k] * 2.0 * tpi_V / om) * cu / press;
+        tau[3 * map[k][1] + map[k][0]] = v;
+        tau[3 * map[k][0] + map[k][1]] = v;
+    }
+    double L = lossF[c], D[9];
+    for (int k = 0; k < 9; ++k) {
+        D[k] = tau[k] - tau_t[9 * c + k];
+        L += C.cS * D[k] * D[k];
+        tau_c[9 * c + k] = tau[k];
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int bb = 0; bb < 3; ++bb) Sres[9 * c + 3 * a + bb] = C.cS * (D[3 * a + bb] + D[3 * bb + a]);
+    loss_c[c] = L;
+}
+
 }  // namespace
 
 // ==========================================================================
@@ -1132,6 +1196,19 @@ struct mdff_batch {
     std::vector<double> energy;  // [nconf]
     int fwd_iters = 0, adj_iters = 0;
     std::vector<int> hconv;
+    // the loss + gradient evaluation as one CUDA graph (built on first use and
+    // whenever the flags of the force field change)
+    cudaStream_t st2 = nullptr;          // stream used to capture the loop bodies
+    cudaGraphExec_t gexec = nullptr, gexec_loss = nullptr;   // loss + gradient; loss only
+    cudaGraph_t graph = nullptr, graph_loss = nullptr;
+    BFlags gflags[2];                    // flags each graph was built with
+    bool gpol[2] = {false, false};
+    cudaGraphConditionalHandle hcond[2] = {0, 0};
+    int* loop_it = nullptr;              // device loop counter of the running solve
+    int* solve_out = nullptr;            // [4]: forward iterations, not converged; adjoint iterations, not converged
+    double* tau_t_dev = nullptr;         // [nconf][9]
+    double* loss_c = nullptr;            // [nconf]
+    double* tau_c = nullptr;             // [nconf][9]
 };
 
 namespace {
@@ -1358,8 +1435,19 @@ int pcg(mdff_batch* b, const double* rhs, double* x, int* iters) {
     return MDFF_OK;
 }
 
-// Forces, per-configuration energy and stress at the current parameters.
-int forward(mdff_batch* b) {
+int pcg_captured(mdff_batch* b, const double* rhs, double* x, int slot);
+
+bool any_polarisable(const mdff_batch* b) {
+    for (auto& C : b->hcfg)
+        if (C.npol > 0) return true;
+    return false;
+}
+
+// The launches of one force evaluation (no host synchronisation when the
+// dipole solve is captured): forces into b->f, per-configuration sums of the
+// pair and real-space energy and stress into b->red (+16 nconf, +24 nconf),
+// reciprocal sums (+8 nconf).
+int forward_launches(mdff_batch* b, bool captured) {
     const int N = b->N;
     const mdff_params& p = b->p;
     if (p.lbmhft || p.lbmhftd || p.lmorse) {
@@ -1372,7 +1460,7 @@ int forward(mdff_batch* b) {
         BCK(cudaMemsetAsync(b->e_pair, 0, sizeof(double) * N, b->st));
         BCK(cudaMemsetAsync(b->s_pair, 0, sizeof(double) * 6 * N, b->st));
     }
-    b->fwd_iters = 0;
+    if (!captured) b->fwd_iters = 0;
     if (p.lcoulomb) {
         // static field b: damped charges, real + reciprocal
         k_b_dir<16, 0><<<dir_blocks(N, 16), 256, 0, b->st>>>(N, b->cfg_of, b->cfg, nullptr, b->sx, b->sy, b->sz, b->type,
@@ -1381,10 +1469,12 @@ int forward(mdff_batch* b) {
         BTRY(blaunch(b, "static field"));
         BTRY((structure_factor<0, 0>(b, nullptr, nullptr)));
         BTRY((kfield<0, 1, 1>(b, nullptr, b->Estat, nullptr)));
-        bool pol = false;
-        for (auto& C : b->hcfg) pol = pol || C.npol > 0;
-        if (pol) BTRY(pcg(b, b->Estat, b->mu, &b->fwd_iters));
-        else BCK(cudaMemsetAsync(b->mu, 0, sizeof(double) * 3 * N, b->st));
+        if (any_polarisable(b)) {
+            if (captured) BTRY(pcg_captured(b, b->Estat, b->mu, 0));
+            else BTRY(pcg(b, b->Estat, b->mu, &b->fwd_iters));
+        } else {
+            BCK(cudaMemsetAsync(b->mu, 0, sizeof(double) * 3 * N, b->st));
+        }
         // final multipole Ewald: forces, energy, stress
         k_b_dir<16, 2><<<dir_blocks(N, 16), 256, 0, b->st>>>(N, b->cfg_of, b->cfg, nullptr, b->sx, b->sy, b->sz, b->type,
                                                              b->q, b->mu, b->nbr, b->cnt, b->cap, b->pc, b->fl, b->fdir,
@@ -1398,24 +1488,33 @@ int forward(mdff_batch* b) {
     k_b_forces<<<nblk(N, 256), 256, 0, b->st>>>(N, b->fpair, b->fdir, b->Erec, b->G, b->q, b->mu, b->cu, p.lcoulomb,
                                                 b->f);
     BTRY(blaunch(b, "forces"));
-    // per-configuration sums: pair energy + stress (7), then dir energy +
-    // stress (7) and the self / polarisation sums (q^2, mu^2, mu.mu/alpha)
+    // per-configuration sums: pair energy + stress, real-space energy + stress
     SegSpec a;
     std::memset(&a, 0, sizeof a);
     a.t[0] = {b->e_pair, nullptr, 1};
     for (int k = 0; k < 6; ++k) a.t[1 + k] = {b->s_pair + (size_t)k * N, nullptr, 1};
-    double* red_pair = b->red + 16 * b->nconf;   // [nconf][8]
-    BTRY(segsum<7>(b, a, red_pair));
-    std::vector<double> hp((size_t)b->nconf * 7), hd((size_t)b->nconf * 7, 0.0), hs((size_t)b->nconf * 3, 0.0),
-        hr((size_t)b->nconf * 8, 0.0);
-    BCK(cudaMemcpyAsync(hp.data(), red_pair, sizeof(double) * 7 * b->nconf, cudaMemcpyDeviceToHost, b->st));
+    BTRY(segsum<7>(b, a, b->red + 16 * b->nconf));
     if (p.lcoulomb) {
         std::memset(&a, 0, sizeof a);
         a.t[0] = {b->e_dir, nullptr, 1};
         for (int k = 0; k < 6; ++k) a.t[1 + k] = {b->s_dir + (size_t)k * N, nullptr, 1};
-        double* red_dir = b->red + 24 * b->nconf;
-        BTRY(segsum<7>(b, a, red_dir));
-        BCK(cudaMemcpyAsync(hd.data(), red_dir, sizeof(double) * 7 * b->nconf, cudaMemcpyDeviceToHost, b->st));
+        BTRY(segsum<7>(b, a, b->red + 24 * b->nconf));
+    }
+    return MDFF_OK;
+}
+
+// Forces, per-configuration energy and stress at the current parameters.
+int forward(mdff_batch* b) {
+    const mdff_params& p = b->p;
+    BTRY(forward_launches(b, false));
+    std::vector<double> hp((size_t)b->nconf * 7), hd((size_t)b->nconf * 7, 0.0), hs((size_t)b->nconf * 3, 0.0),
+        hr((size_t)b->nconf * 8, 0.0);
+    BCK(cudaMemcpyAsync(hp.data(), b->red + 16 * b->nconf, sizeof(double) * 7 * b->nconf, cudaMemcpyDeviceToHost, b->st));
+    if (p.lcoulomb) {
+        BCK(cudaMemcpyAsync(hd.data(), b->red + 24 * b->nconf, sizeof(double) * 7 * b->nconf, cudaMemcpyDeviceToHost,
+                            b->st));
+        // self-term sums q^2 and mu^2
+        SegSpec a;
         std::memset(&a, 0, sizeof a);
         a.t[0] = {b->q, b->q, 1};
         a.t[1] = {b->mu, b->mu, 3};
@@ -1458,70 +1557,194 @@ int forward(mdff_batch* b) {
     return MDFF_OK;
 }
 
-int loss_and_gradient(mdff_batch* b, double* loss, mdff_param_grad* grad) {
+// Body of one lockstep PCG iteration (captured into a WHILE node's graph).
+int pcg_body(mdff_batch* b, double* x, int slot) {
+    const int N = b->N, n3 = 3 * N;
+    BTRY(dd_field(b, b->cg_d, b->Eind));
+    k_b_apply_A<<<nblk(n3, 256), 256, 0, b->st>>>(N, b->cfg_of, b->cfg, b->conv, b->cg_d, b->Eind, b->inv_alpha,
+                                                  b->cg_Ad);
+    SegSpec s1;
+    std::memset(&s1, 0, sizeof s1);
+    s1.t[0] = {b->cg_d, b->cg_Ad, 3};
+    BTRY(segsum<1>(b, s1, b->red + 2 * b->nconf));
+    k_b_cg_update<<<nblk(n3, 256), 256, 0, b->st>>>(N, b->cfg_of, b->conv, b->sc, b->red + 2 * b->nconf, b->cg_d,
+                                                    b->cg_Ad, b->alpha, x, b->cg_r, b->cg_z);
+    SegSpec s2;
+    std::memset(&s2, 0, sizeof s2);
+    s2.t[0] = {b->cg_r, b->cg_r, 3};
+    s2.t[1] = {b->cg_r, b->cg_z, 3};
+    BTRY(segsum<2>(b, s2, b->red));
+    k_b_cg_scalars<<<nblk(b->nconf, 64), 64, 0, b->st>>>(b->nconf, b->cfg, b->red, b->sc, b->conv, b->p.conv_tol_ind);
+    k_b_cg_direction<<<nblk(n3, 256), 256, 0, b->st>>>(N, b->cfg_of, b->conv, b->sc, b->cg_z, b->cg_d);
+    k_b_cg_cond<<<1, 256, 0, b->st>>>(b->nconf, b->conv, b->loop_it, b->p.max_scf_pol_iter, 0, b->hcond[slot]);
+    return blaunch(b, "pcg iteration");
+}
+
+// Lockstep PCG inside a stream capture: the initial residual, then a
+// conditional WHILE node whose body is one iteration; the loop ends on the
+// device when every configuration has converged or after max_scf_pol_iter
+// iterations.  solve_out[2 slot .. 2 slot + 1] receive the iteration count
+// and the number of configurations that did not converge.
+int pcg_captured(mdff_batch* b, const double* rhs, double* x, int slot) {
+    const int N = b->N, n3 = 3 * N;
+    const double tol = b->p.conv_tol_ind;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    // the loop's condition handle, owned by the graph under capture
+    BCK(cudaStreamGetCaptureInfo(b->st, &cs, nullptr, &g, nullptr, nullptr));
+    BCK(cudaGraphConditionalHandleCreate(&b->hcond[slot], g, 0, 0));
+    k_b_cg_x0<<<nblk(n3, 256), 256, 0, b->st>>>(N, rhs, b->alpha, x);
+    BCK(cudaMemsetAsync(b->conv, 0, sizeof(int) * b->nconf, b->st));
+    BTRY(dd_field(b, x, b->Eind));
+    k_b_apply_A<<<nblk(n3, 256), 256, 0, b->st>>>(N, b->cfg_of, b->cfg, nullptr, x, b->Eind, b->inv_alpha, b->cg_Ad);
+    k_b_cg_init<<<nblk(n3, 256), 256, 0, b->st>>>(N, rhs, b->cg_Ad, b->alpha, b->inv_alpha, b->cg_r, b->cg_z, b->cg_d);
+    SegSpec s2;
+    std::memset(&s2, 0, sizeof s2);
+    s2.t[0] = {b->cg_r, b->cg_r, 3};
+    s2.t[1] = {b->cg_r, b->cg_z, 3};
+    BTRY(segsum<2>(b, s2, b->red));
+    k_b_cg_first<<<nblk(b->nconf, 64), 64, 0, b->st>>>(b->nconf, b->cfg, b->red, b->sc, b->conv, tol);
+    k_b_cg_cond<<<1, 256, 0, b->st>>>(b->nconf, b->conv, b->loop_it, b->p.max_scf_pol_iter, 1, b->hcond[slot]);
+    BTRY(blaunch(b, "pcg init"));
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    BCK(cudaStreamGetCaptureInfo(b->st, &cs, nullptr, &g, &deps, &nd));
+    alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];   // the struct holds a union
+    std::memset(cp_raw, 0, sizeof cp_raw);                                           // with no default constructor
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = b->hcond[slot];
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    BCK(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    BCK(cudaStreamUpdateCaptureDependencies(b->st, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t main_st = b->st;
+    b->st = b->st2;
+    cudaError_t e = cudaStreamBeginCaptureToGraph(b->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    int r = e == cudaSuccess ? pcg_body(b, x, slot)
+                             : bfail(b, MDFF_E_CUDA, std::string("capture of the PCG body: ") + cudaGetErrorString(e));
+    if (e == cudaSuccess) {
+        cudaGraph_t out = body;
+        cudaError_t e2 = cudaStreamEndCapture(b->st, &out);
+        if (r == MDFF_OK && e2 != cudaSuccess)
+            r = bfail(b, MDFF_E_CUDA, std::string("capture of the PCG body: ") + cudaGetErrorString(e2));
+    }
+    b->st = main_st;
+    BTRY(r);
+    k_b_cg_summary<<<1, 32, 0, b->st>>>(b->nconf, b->conv, b->sc, b->solve_out + 2 * slot);
+    return blaunch(b, "pcg summary");
+}
+
+// The loss (and, with_grad, its gradient) as launches on b->st, for capture.
+int loss_grad_launches(mdff_batch* b, bool with_grad) {
     const int N = b->N;
-    BTRY(forward(b));
-    // loss
+    const mdff_params& p = b->p;
+    BCK(cudaMemsetAsync(b->solve_out, 0, sizeof(int) * 4, b->st));
+    BCK(cudaMemsetAsync(b->gsum, 0, sizeof(double) * 64, b->st));
+    BTRY(forward_launches(b, true));
     k_b_residual<<<nblk(N, 256), 256, 0, b->st>>>(N, b->cfg_of, b->cfg, b->f, b->ft, b->R, b->lossa);
     SegSpec a;
     std::memset(&a, 0, sizeof a);
     a.t[0] = {b->lossa, nullptr, 1};
-    BTRY(segsum<1>(b, a, b->red));
-    std::vector<double> lf(b->nconf);
-    BCK(cudaMemcpyAsync(lf.data(), b->red, sizeof(double) * b->nconf, cudaMemcpyDeviceToHost, b->st));
-    BCK(cudaStreamSynchronize(b->st));
-    std::vector<double> S((size_t)b->nconf * 9);
-    double L = 0.0;
-    for (int c = 0; c < b->nconf; ++c) {
-        L += lf[c];
-        const double cS = b->hcfg[c].cS;
-        double D[9];
-        for (int k = 0; k < 9; ++k) {
-            D[k] = b->tau[9 * c + k] - b->tau_t[9 * c + k];
-            L += cS * D[k] * D[k];
-        }
-        // dL/dtau, symmetrised (tau is symmetric, so only the symmetric part acts)
-        for (int a0 = 0; a0 < 3; ++a0)
-            for (int b0 = 0; b0 < 3; ++b0) S[9 * c + 3 * a0 + b0] = cS * (D[3 * a0 + b0] + D[3 * b0 + a0]);
-    }
-    *loss = L;
-    if (!grad) return MDFF_OK;
-    std::memset(grad, 0, sizeof(mdff_param_grad));
-    BCK(cudaMemcpyAsync(b->Sres, S.data(), sizeof(double) * 9 * b->nconf, cudaMemcpyHostToDevice, b->st));
-    const mdff_params& p = b->p;
+    double* lossF = b->red + 35 * b->nconf;
+    BTRY(segsum<1>(b, a, lossF));
+    k_b_loss_tail<<<nblk(b->nconf, 64), 64, 0, b->st>>>(b->nconf, b->cfg, b->red + 16 * b->nconf,
+                                                        b->red + 24 * b->nconf, b->red + 8 * b->nconf, lossF,
+                                                        b->tau_t_dev, b->cu, b->press, p.lcoulomb, b->loss_c, b->tau_c,
+                                                        b->Sres);
+    BTRY(blaunch(b, "loss"));
+    if (!with_grad) return MDFF_OK;
     constexpr int KA = NTYB * NTYB * 4, KR = NTYB * NTYB * 10;
     const int blk16 = dir_blocks(N, 16);
-    std::vector<double> gA(KA, 0.0), gR(KR, 0.0), gP(NTYB, 0.0);
-    b->adj_iters = 0;
-    bool pol = false;
-    for (auto& C : b->hcfg) pol = pol || C.npol > 0;
-    if (p.lcoulomb && pol) {
+    if (p.lcoulomb && any_polarisable(b)) {
         // adjoint right-hand side h = dJ/dmu
         k_b_dir_adj<16><<<blk16, 256, 0, b->st>>>(N, b->cfg_of, b->cfg, b->sx, b->sy, b->sz, b->type, b->q, b->mu, b->R,
                                                   b->Sres, b->nbr, b->cnt, b->cap, b->pc, b->fl, b->h, b->gpart);
-        BTRY(blaunch(b, "adjoint real space"));
         k_b_reduce_cols<<<nblk(KA, 8), 256, 0, b->st>>>(b->gpart, blk16, KA, b->gsum);
-        BCK(cudaMemcpyAsync(gA.data(), b->gsum, sizeof(double) * KA, cudaMemcpyDeviceToHost, b->st));
+        BTRY(blaunch(b, "adjoint real space"));
         BTRY((structure_factor<3, 2>(b, nullptr, b->mu)));
         BTRY((kfield<0, 1, 0>(b, nullptr, b->h, nullptr)));
         k_b_h_finish<<<nblk(N, 256), 256, 0, b->st>>>(N, b->G, b->R, b->inv_alpha, b->cu, b->h);
         BTRY(blaunch(b, "adjoint rhs"));
-        BTRY(pcg(b, b->h, b->lam, &b->adj_iters));
-        // polarisabilities
-        int ab = std::min(592, nblk(N, 256));
+        BTRY(pcg_captured(b, b->h, b->lam, 1));
+        const int ab = std::min(592, nblk(N, 256));
         k_b_alpha_grad<<<ab, 256, 0, b->st>>>(N, b->type, b->lam, b->mu, b->inv_alpha, b->gpart);
-        k_b_reduce_cols<<<1, 256, 0, b->st>>>(b->gpart, ab, NTYB, b->gsum);
-        BCK(cudaMemcpyAsync(gP.data(), b->gsum, sizeof(double) * NTYB, cudaMemcpyDeviceToHost, b->st));
+        k_b_reduce_cols<<<1, 256, 0, b->st>>>(b->gpart, ab, NTYB, b->gsum + KA + KR);
         BTRY(blaunch(b, "alpha gradient"));
     } else {
         BCK(cudaMemsetAsync(b->lam, 0, sizeof(double) * 3 * N, b->st));
     }
     k_b_grad_rows<16><<<blk16, 256, 0, b->st>>>(N, b->cfg_of, b->cfg, b->sx, b->sy, b->sz, b->type, b->q, b->R, b->Sres,
                                                 b->lam, b->nbr, b->cnt, b->cap, b->pc, b->fl, b->gpart);
-    BTRY(blaunch(b, "row gradient"));
-    k_b_reduce_cols<<<nblk(KR, 8), 256, 0, b->st>>>(b->gpart, blk16, KR, b->gsum);
-    BCK(cudaMemcpyAsync(gR.data(), b->gsum, sizeof(double) * KR, cudaMemcpyDeviceToHost, b->st));
+    k_b_reduce_cols<<<nblk(KR, 8), 256, 0, b->st>>>(b->gpart, blk16, KR, b->gsum + KA);
+    return blaunch(b, "row gradient");
+}
+
+void drop_graph(mdff_batch* b, int which) {
+    cudaGraphExec_t& ge = which ? b->gexec : b->gexec_loss;
+    cudaGraph_t& g = which ? b->graph : b->graph_loss;
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    ge = nullptr;
+    g = nullptr;
+}
+
+// Capture the evaluation (which = 1: loss and gradient; 0: loss only) as one
+// CUDA graph and instantiate it.
+int build_graph(mdff_batch* b, int which) {
+    drop_graph(b, which);
+    BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+    int r = loss_grad_launches(b, which == 1);
+    cudaGraph_t out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->st, &out);
+    if (r == MDFF_OK && e != cudaSuccess) r = bfail(b, MDFF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    if (r != MDFF_OK) {
+        if (out) cudaGraphDestroy(out);
+        cudaGetLastError();
+        return r;
+    }
+    cudaGraphExec_t ge = nullptr;
+    e = cudaGraphInstantiate(&ge, out, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(out);
+        return bfail(b, MDFF_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    (which ? b->graph : b->graph_loss) = out;
+    (which ? b->gexec : b->gexec_loss) = ge;
+    b->gflags[which] = b->fl;
+    b->gpol[which] = any_polarisable(b);
+    return MDFF_OK;
+}
+
+int loss_and_gradient(mdff_batch* b, double* loss, mdff_param_grad* grad) {
+    const int which = grad ? 1 : 0;
+    const bool stale = (which ? !b->gexec : !b->gexec_loss) ||
+                       std::memcmp(&b->gflags[which], &b->fl, sizeof(BFlags)) != 0 ||
+                       b->gpol[which] != any_polarisable(b);
+    if (stale) BTRY(build_graph(b, which));
+    BCK(cudaGraphLaunch(which ? b->gexec : b->gexec_loss, b->st));
+    constexpr int KA = NTYB * NTYB * 4, KR = NTYB * NTYB * 10;
+    std::vector<double> lc(b->nconf), gs(64);
+    int so[4];
+    BCK(cudaMemcpyAsync(lc.data(), b->loss_c, sizeof(double) * b->nconf, cudaMemcpyDeviceToHost, b->st));
+    BCK(cudaMemcpyAsync(b->tau.data(), b->tau_c, sizeof(double) * 9 * b->nconf, cudaMemcpyDeviceToHost, b->st));
+    BCK(cudaMemcpyAsync(gs.data(), b->gsum, sizeof(double) * 64, cudaMemcpyDeviceToHost, b->st));
+    BCK(cudaMemcpyAsync(so, b->solve_out, sizeof(int) * 4, cudaMemcpyDeviceToHost, b->st));
     BCK(cudaStreamSynchronize(b->st));
+    b->fwd_iters = so[0];
+    b->adj_iters = so[2];
+    if (so[1] || so[3])
+        return bfail(b, MDFF_E_NOCONV, "batch: induced-dipole solve did not converge within max_scf_pol_iter");
+    double L = 0.0;
+    for (int c = 0; c < b->nconf; ++c) L += lc[c];
+    *loss = L;
+    if (!grad) return MDFF_OK;
+    std::memset(grad, 0, sizeof(mdff_param_grad));
+    const double* gA = gs.data();
+    const double* gR = gs.data() + KA;
+    const double* gP = gs.data() + KA + KR;
     // fold ordered slots (ti,tj) into the upper-triangle parameter slots
     for (int ti = 0; ti < b->ntype; ++ti)
         for (int tj = 0; tj < b->ntype; ++tj) {
@@ -1567,6 +1790,7 @@ int mdff_batch_create(const mdff_params* p, int nconf, const int* natm, const in
     cudaError_t e = cudaSetDevice(p->device);
     if (e != cudaSuccess) return bad(bfail(b, MDFF_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e)));
     e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st2, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bad(bfail(b, MDFF_E_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)));
     if (p->lreduced) { b->cu = 1.0; b->press = 1.0; }
     else { b->cu = 14.3996441494161; b->press = 0.00624150964712042; }
@@ -1652,6 +1876,11 @@ int mdff_batch_create(const mdff_params* p, int nconf, const int* natm, const in
     A(&b->red, 40 * nconf);
     A(&b->Sres, 9 * nconf);
     A(&b->overflow, 1);
+    A(&b->loop_it, 1);
+    A(&b->solve_out, 4);
+    A(&b->tau_t_dev, 9 * nconf);
+    A(&b->loss_c, nconf);
+    A(&b->tau_c, 9 * nconf);
     b->gpart_cap = dir_blocks(b->N, 16) * NTYB * NTYB * 10 + 1024;
     A(&b->gpart, b->gpart_cap);
     A(&b->gsum, 64);
@@ -1700,6 +1929,7 @@ int mdff_batch_create(const mdff_params* p, int nconf, const int* natm, const in
         (e = cudaMemsetAsync(b->Sres, 0, sizeof(double) * 9 * nconf, b->st)))
         return bad(bfail(b, MDFF_E_CUDA, std::string("batch upload: ") + cudaGetErrorString(e)));
     b->tau_t.assign((size_t)9 * nconf, 0.0);
+    b->tau.assign((size_t)9 * nconf, 0.0);
     if (int r2 = upload_params(b, *p)) return bad(r2);
     k_b_wrap_frac<<<nblk(N, 256), 256, 0, b->st>>>(b->N, b->cfg_of, b->cfg, b->x, b->y, b->z, b->sx, b->sy, b->sz);
     if (int r2 = blaunch(b, "wrap")) return bad(r2);
@@ -1734,8 +1964,11 @@ int mdff_batch_create(const mdff_params* p, int nconf, const int* natm, const in
 void mdff_batch_destroy(mdff_batch* b) {
     if (!b) return;
     if (b->st) cudaStreamSynchronize(b->st);
+    drop_graph(b, 0);
+    drop_graph(b, 1);
     for (void* p : b->allocs) cudaFree(p);
     if (b->st) cudaStreamDestroy(b->st);
+    if (b->st2) cudaStreamDestroy(b->st2);
     delete b;
 }
 
@@ -1782,6 +2015,7 @@ int mdff_batch_set_targets(mdff_batch* b, const double* fx, const double* fy, co
     BCK(cudaMemcpyAsync(b->ft + N, fy, sizeof(double) * N, cudaMemcpyHostToDevice, b->st));
     BCK(cudaMemcpyAsync(b->ft + 2 * (size_t)N, fz, sizeof(double) * N, cudaMemcpyHostToDevice, b->st));
     std::memcpy(b->tau_t.data(), tau, sizeof(double) * 9 * b->nconf);
+    BCK(cudaMemcpyAsync(b->tau_t_dev, tau, sizeof(double) * 9 * b->nconf, cudaMemcpyHostToDevice, b->st));
     b->w_force = w_force;
     b->w_stress = w_stress;
     for (auto& C : b->hcfg) {

@@ -48,6 +48,7 @@ def parse():
                     help="mixed path: |k| below ksplit*alpha summed in FP64 (default: the library's)")
     ap.add_argument("--keps", type=float, default=None,
                     help="mixed path: leave out k with exp(-k^2/4 alpha^2) below keps (0: all; default: the library's)")
+    ap.add_argument("--autotune", type=int, default=1, choices=[0, 1], help="autotune the launch shapes")
     ap.add_argument("--reuse", default="auto", choices=["auto", "0", "1"],
                     help="kspace_reuse (auto: on for the mixed path, off for the plain FP64 path)")
     ap.add_argument("--workload", default="production", choices=["production", "batch"],
@@ -175,6 +176,7 @@ def run_engine(args):
         p.mixed_ksplit = args.ksplit
     if args.keps is not None:
         p.mixed_keps = args.keps
+    p.autotune = args.autotune
     natm = len(s["itype"])
     eng = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
     eng.enable_profile(True)
@@ -273,6 +275,7 @@ def run_engine(args):
                        "precision": args.precision, "parallelism": f"replicas{world}",
                        "l2": "per-step working set > 126 MB L2 (k-space partials, Verlet lists)"},
             "gpu_launches": int(prof["_launches"]["count"]),
+            "launch_shape": eng.launch_shape(),
             "solver_iters_mean": mean_it,
             "h_tot_drift_per_step": (h[-1] - h[0]) / max(1, len(h) - 1) / natm,
             "kernels_ms": {k: round(v["ms"], 3) for k, v in kern.items()},

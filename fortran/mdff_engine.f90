@@ -78,6 +78,7 @@ module mdff_engine
     real(c_double) :: mixed_ksplit
     integer(c_int) :: kspace_reuse
     real(c_double) :: mixed_keps
+    integer(c_int) :: autotune
   end type mdff_params_t
 
   type, bind(C) :: mdff_energies_t

@@ -136,6 +136,8 @@ typedef struct mdff_params {
                                                   linearity (0: the reference's sequence of evaluations) */
     double mixed_keps;                         /* mixed path: k-vectors whose Gaussian factor exp(-k^2/4 alpha^2)
                                                   is below mixed_keps are left out (0: the whole rectangle) */
+    int    autotune;                           /* 1: time the candidate launch shapes of the Ewald kernels on the
+                                                  first force evaluation and keep the fastest */
 } mdff_params;
 
 /* Energies and scalar outputs of one force evaluation (thermodynamic module
@@ -234,6 +236,12 @@ int  mdff_profile_get(mdff_ctx* ctx, double ms[8], long long count[8], long long
  * out[2] the FP32 set and out[3] the FP64 low-|k| set of the mixed path (both
  * 0 on the FP64 path). */
 int  mdff_kspace_info(mdff_ctx* ctx, long long out[4]);
+
+/* Launch shape in use (the autotuner's choice, or the defaults): out[0] lanes
+ * per atom of the FP64 real-space Ewald kernel, out[1] of the FP32 dipole
+ * operator, out[2] and out[3] the FP32 structure-factor atom split and field
+ * column split in halves of the default (no reference counterpart). */
+int  mdff_launch_shape(mdff_ctx* ctx, int out[4]);
 
 /* Define the system: natm atoms, 1-based types, Cartesian positions and the
  * cell.  Replaces read_pos + typeinfo_init (src/read_pos.f90:35-219): the cell

@@ -64,6 +64,7 @@ def lib():
         L.mdff_measure_pipes.argtypes = [C.c_int, dp]
         L.mdff_struct_size.argtypes = [C.c_int]
         L.mdff_kspace_info.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.mdff_launch_shape.argtypes = [vp, C.POINTER(C.c_int)]
         L.mdff_batch_create.argtypes = [C.POINTER(abi.Params), C.c_int, ip, ip, dp, dp, dp, dp, dp, dp, ip, C.POINTER(vp)]
         L.mdff_batch_destroy.argtypes = [vp]
         L.mdff_batch_destroy.restype = None
@@ -132,6 +133,13 @@ class Engine:
         out = (C.c_longlong * 4)()
         self._check(lib().mdff_kspace_info(self._h, out))
         return {"rect": out[0], "half": out[1], "fp32": out[2], "low": out[3]}
+
+    def launch_shape(self):
+        """Launch shape in use: real-space lanes per atom (FP64, FP32) and the
+        FP32 structure-factor / field splits (in halves of the default)."""
+        out = (C.c_int * 4)()
+        self._check(lib().mdff_launch_shape(self._h, out))
+        return {"g_dir": out[0], "g_dd32": out[1], "sfac_split_x2": out[2], "field_split_x2": out[3]}
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

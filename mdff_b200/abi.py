@@ -55,7 +55,7 @@ class Params(C.Structure):
         ("timesca_thermo", C.c_double),
         ("precision", C.c_int), ("efg_period", C.c_int), ("nlist_capacity", C.c_int), ("device", C.c_int),
         ("erfc_ref", C.c_int), ("nhc_literal", C.c_int), ("mixed_ksplit", C.c_double),
-        ("kspace_reuse", C.c_int), ("mixed_keps", C.c_double),
+        ("kspace_reuse", C.c_int), ("mixed_keps", C.c_double), ("autotune", C.c_int),
     ]
 
 

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -89,6 +90,8 @@ struct mdff_ctx {
     int nrebuild = 0;
     bool rec_acc_ready = false;   // rs.aks_acc holds A_k S of the charges + final dipoles
     long long kinfo[4] = {0, 0, 0, 0};   // rectangle, half space, FP32 set, FP64 low set
+    int g_dir = 16, g_dd = 16;           // lanes per atom of the real-space Ewald kernels (autotuned)
+    bool tuned = false;
     Prof prof;
 };
 
@@ -432,7 +435,7 @@ void dd_field_real(mdff_ctx* ctx, const double* m, double* out) {
         int k = ctx->rs.tab_epoch != ctx->rs.want_epoch ? 2 : 1;
         ensure_phase_tables(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->rs);
         launch_ewald_dd32(ctx->st, n, ctx->rs.fixed, m, ctx->cell, coul_list(ctx), ctx->cut_coul * ctx->cut_coul,
-                          ctx->alphaES, out);
+                          ctx->alphaES, out, ctx->g_dd);
         ctx->prof.end(k);
         return;
     }
@@ -440,7 +443,7 @@ void dd_field_real(mdff_ctx* ctx, const double* m, double* out) {
     f.dd = 1;
     f.field = 1;
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, nullptr, m, ctx->cell, coul_list(ctx), ctx->pc,
-                     f, out, nullptr, nullptr, ctx->part, ctx->dsc);
+                     f, out, nullptr, nullptr, ctx->part, ctx->dsc, ctx->g_dir);
     ctx->prof.end(1);
 }
 
@@ -468,7 +471,7 @@ int static_field(mdff_ctx* ctx) {
     f.field = 1;
     ctx->prof.begin(PK_DIR);
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->dip0, ctx->cell, coul_list(ctx),
-                     ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc);
+                     ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, ctx->g_dir);
     ctx->prof.end(2);
     RecFlags rf{1, ctx->any_dip0 ? 1 : 0, 1, 0, 0, 0, ctx->p.precision, 0};
     launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->dip0, ctx->cell, ctx->kg, rf, ctx->rs,
@@ -494,7 +497,7 @@ int fused_initial_field(mdff_ctx* ctx) {
     f.field = 1;
     ctx->prof.begin(PK_DIR);
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->dip0, ctx->cell, coul_list(ctx),
-                     ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc);
+                     ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, ctx->g_dir);
     ctx->prof.end(2);
     dd_field_real(ctx, ctx->mu_ind, ctx->Eind);
     ctx->prof.begin(PK_OTHER);
@@ -643,6 +646,84 @@ int solve_dipoles(mdff_ctx* ctx) {
     return MDFF_OK;
 }
 
+// Autotuner (autotune != 0): on the first force evaluation, time every
+// candidate launch shape of the Ewald kernels on this system's own data with
+// CUDA events on the context's stream (one warm-up launch, then three timed
+// ones) and keep the fastest: lanes per atom of the real-space kernels
+// (8, 16, 32), and on the mixed path the atom split of the FP32 structure
+// factor and the column split of the FP32 field (x 1/2, 1, 2 of the default).
+// The candidates compute the same sums in a different order; the launches
+// write only scratch that the evaluation overwrites.
+float time_launch(mdff_ctx* ctx, const std::function<void()>& fn) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    fn();
+    cudaEventRecord(a, ctx->st);
+    for (int r = 0; r < 3; ++r) fn();
+    cudaEventRecord(b, ctx->st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms / 3.f;
+}
+
+int autotune(mdff_ctx* ctx) {
+    ctx->tuned = true;
+    if (!ctx->p.lcoulomb) return MDFF_OK;
+    const int n = ctx->n;
+    const bool prof_on = ctx->prof.on;
+    const long launches = ctx->prof.launches;
+    ctx->prof.on = false;
+    CK(cudaMemsetAsync(ctx->mu, 0, sizeof(double) * 3 * n, ctx->st));
+    const int gs[3] = {8, 16, 32};
+    auto pick = [&](const std::function<void(int)>& run, const int* cand, int nc) {
+        int best = cand[0];
+        float tb = 1e30f;
+        for (int k = 0; k < nc; ++k) {
+            float t = time_launch(ctx, [&] { run(cand[k]); });
+            if (t < tb) { tb = t; best = cand[k]; }
+        }
+        return best;
+    };
+    DirFlags f = dir_flags(ctx);
+    f.qq = 1;
+    f.qd = 1;
+    f.dd = 1;
+    f.damp = 1;
+    f.field = 1;
+    f.forces = 1;
+    ctx->g_dir = pick([&](int g) {
+        launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->mu, ctx->cell, coul_list(ctx),
+                         ctx->pc, f, ctx->ef, nullptr, ctx->fcoul, ctx->part, ctx->dsc, g);
+    }, gs, 3);
+    if (ctx->p.precision == MDFF_PREC_MIXED) {
+        ensure_phase_tables(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->rs);
+        ctx->g_dd = pick([&](int g) {
+            launch_ewald_dd32(ctx->st, n, ctx->rs.fixed, ctx->mu, ctx->cell, coul_list(ctx),
+                              ctx->cut_coul * ctx->cut_coul, ctx->alphaES, ctx->Eind, g);
+        }, gs, 3);
+        const int muls[3] = {1, 2, 4};
+        RecFlags sf{1, 1, 0, 0, 0, 0, MDFF_PREC_MIXED, 0};   // structure factor only
+        ctx->rs.p_mul = pick([&](int m) {
+            ctx->rs.p_mul = m;
+            launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->mu, ctx->cell, ctx->kg, sf, ctx->rs,
+                             nullptr, nullptr, nullptr, ctx->part, ctx->dsc, &ctx->prof);
+        }, muls, 3);
+        RecFlags fe{1, 1, 1, 0, 0, 0, MDFF_PREC_MIXED, 0};   // with the field pass
+        ctx->rs.s_mul = pick([&](int m) {
+            ctx->rs.s_mul = m;
+            launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->mu, ctx->cell, ctx->kg, fe, ctx->rs,
+                             ctx->ef, nullptr, nullptr, ctx->part, ctx->dsc, &ctx->prof);
+        }, muls, 3);
+    }
+    ctx->prof.on = prof_on;
+    ctx->prof.launches = launches;
+    return check_launch(ctx, "autotune");
+}
+
 // engforce_driver (src/field.f90:1111-1166) on the device; results stay in
 // device memory and ctx->hsc/en after the trailing sync.
 int engforce_device(mdff_ctx* ctx) {
@@ -653,6 +734,7 @@ int engforce_device(mdff_ctx* ctx) {
     launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
     ctx->prof.end(1);
     ctx->rs.want_epoch++;   // positions may have changed: rebuild the phase tables
+    if (p.autotune && !ctx->tuned) TRY(autotune(ctx));
     std::memset(&ctx->en, 0, sizeof ctx->en);
     bool nonb = p.lnmlj || p.lbmhft || p.lbmhftd || p.lmorse;
     if (nonb) {
@@ -692,7 +774,7 @@ int engforce_device(mdff_ctx* ctx) {
         if (p.doefg) CK(cudaMemsetAsync(ctx->efg, 0, sizeof(double) * 6 * n, ctx->st));
         ctx->prof.begin(PK_DIR);
         launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->mu, ctx->cell, coul_list(ctx),
-                         ctx->pc, f, ctx->ef, ctx->efg, ctx->fcoul, ctx->part, ctx->dsc);
+                         ctx->pc, f, ctx->ef, ctx->efg, ctx->fcoul, ctx->part, ctx->dsc, ctx->g_dir);
         ctx->prof.end(2);
         RecFlags rf{ctx->any_q ? 1 : 0, dip ? 1 : 0, p.doefield ? 1 : 0, (p.doefg || dip) ? 1 : 0, 1, 1, p.precision,
                     ctx->rec_acc_ready ? 1 : 0};
@@ -987,6 +1069,15 @@ int mdff_get_velocities(mdff_ctx* ctx, double* vx, double* vy, double* vz) {
 int mdff_stream(mdff_ctx* ctx, void** stream) {
     if (!ctx || !stream) return MDFF_E_ARG;
     *stream = (void*)ctx->st;
+    return MDFF_OK;
+}
+
+int mdff_launch_shape(mdff_ctx* ctx, int out[4]) {
+    if (!ctx || !out) return MDFF_E_ARG;
+    out[0] = ctx->g_dir;
+    out[1] = ctx->g_dd;
+    out[2] = ctx->rs.p_mul;
+    out[3] = ctx->rs.s_mul;
     return MDFF_OK;
 }
 
@@ -1316,7 +1407,7 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
             CK(cudaStreamSynchronize(ctx->st));   // the host vectors above go out of scope
         }
         size_t fp = 0;
-        size_t pc = rec_scratch_doubles(n, kg, &fp);
+        size_t pc = rec_scratch_doubles(n, kg, &fp, p.precision == MDFF_PREC_MIXED);
         TRY(dalloc(ctx, &ctx->rs.part, pc));
         TRY(dalloc(ctx, &ctx->rs.fpart, fp));
         TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));

@@ -177,7 +177,7 @@ struct DirFlags {
 void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const int* type, const double* q, const double* mu, CellP c, const NList& l,
                       const PairConst* pc, DirFlags fl,
-                      double* ef, double* efg, double* f, Partials& part, DevScalars* d);
+                      double* ef, double* efg, double* f, Partials& part, DevScalars* d, int g = 16);
 
 // Reciprocal-space multipole Ewald.
 struct KGrid {
@@ -218,6 +218,7 @@ struct RecScratch {
     uint32_t* fixed = nullptr;  // [3][n] fractional coordinates as 32-bit fixed point
     float2* tab = nullptr;      // [n][16] e^{2 pi i m s_z}
     float2* aks2 = nullptr;     // [ncol][nzp] A_k S(k) padded, FP32
+    int p_mul = 2, s_mul = 2;   // mixed path: FP32 structure-factor atom split and field column split, x mul/2
     long tab_epoch = -1;        // position epoch the table was built for
     long want_epoch = 0;        // current position epoch (set by the engine)
     LowK low;
@@ -235,11 +236,11 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
                       const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl,
                       RecScratch& rs, double* ef, double* efg6, double* fo, Partials& part, DevScalars* d,
                       Prof* prof);
-size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart);
+size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart, int mixed);
 void launch_aks_accumulate(cudaStream_t st, const KGrid& kg, RecScratch& rs, const DevScalars* d, int copy);
 void ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs);
 void launch_ewald_dd32(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
-                       double cutsq, double alpha, double* ef);
+                       double cutsq, double alpha, double* ef, int g = 16);
 
 // Solver vector kernels.
 void launch_dot(cudaStream_t st, int n3, const double* a, const double* b, Partials& part, double* out);

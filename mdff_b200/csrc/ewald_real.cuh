@@ -226,27 +226,36 @@ __global__ void __launch_bounds__(256) k_ewald_dd32(int n, const uint32_t* __res
     if (active && sub == 0) { ef[i] = E0; ef[n + i] = E1; ef[2 * n + i] = E2; }
 }
 
+// g: lanes per atom (8, 16 or 32; the autotuner's choice).
 void launch_ewald_dd32(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
-                       double cutsq, double alpha, double* ef) {
-    constexpr int G = 16;
-    const int blocks = (int)(((size_t)n * G + 255) / 256);
-    k_ewald_dd32<G><<<blocks, 256, 0, st>>>(n, fx, mu, c, l.nbr, l.cnt, l.cap, (float)cutsq, (float)alpha, ef);
+                       double cutsq, double alpha, double* ef, int g) {
+    const int blocks = (int)(((size_t)n * g + 255) / 256);
+#define DD32(G) k_ewald_dd32<G><<<blocks, 256, 0, st>>>(n, fx, mu, c, l.nbr, l.cnt, l.cap, (float)cutsq, (float)alpha, ef)
+    if (g == 8) DD32(8);
+    else if (g == 32) DD32(32);
+    else DD32(16);
+#undef DD32
 }
 
+// g: lanes per atom (8, 16 or 32; the autotuner's choice).
 void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const int* type, const double* q, const double* mu, CellP c, const NList& l,
                       const PairConst* pc, DirFlags fl, double* ef, double* efg, double* f, Partials& part,
-                      DevScalars* d) {
-    constexpr int G = 16;
+                      DevScalars* d, int g) {
     const int threads = 256;
-    const int blocks = (int)(((size_t)n * G + threads - 1) / threads);
+    const int blocks = (int)(((size_t)n * g + threads - 1) / threads);
+#define DIR(G, M, P) k_ewald_dir<G, M><<<blocks, threads, 0, st>>>(n, sx, sy, sz, type, q, mu, c, l.nbr, l.cnt, l.cap, \
+                                                                   pc, fl, ef, efg, f, P)
     if (!q) {
-        k_ewald_dir<G, 1><<<blocks, threads, 0, st>>>(n, sx, sy, sz, type, q, mu, c, l.nbr, l.cnt, l.cap, pc, fl, ef,
-                                                      efg, f, nullptr);
+        if (g == 8) DIR(8, 1, nullptr);
+        else if (g == 32) DIR(32, 1, nullptr);
+        else DIR(16, 1, nullptr);
         return;
     }
-    k_ewald_dir<G, 0><<<blocks, threads, 0, st>>>(n, sx, sy, sz, type, q, mu, c, l.nbr, l.cnt, l.cap, pc, fl, ef,
-                                                  efg, f, part.buf);
+    if (g == 8) DIR(8, 0, part.buf);
+    else if (g == 32) DIR(32, 0, part.buf);
+    else DIR(16, 0, part.buf);
+#undef DIR
     launch_reduce_partials(st, part.buf, blocks, 8, d->dir, 0);
 }
 

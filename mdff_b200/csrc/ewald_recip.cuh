@@ -841,11 +841,40 @@ static RecLaunch plan(int n, const KGrid& kg) {
     return L;
 }
 
-size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart) {
+// Launch shape of the mixed path's FP32 passes: the atom split of the
+// structure factor sized for its (column, chunk) work list and the column
+// split of the field, each scaled by mul/2 (mul = 1, 2 or 4; chosen by the
+// autotuner, 2 by default).
+static RecLaunch plan_mixed(int n, const KGrid& kg, int p_mul, int s_mul) {
     RecLaunch L = plan(n, kg);
-    *fpart = (size_t)L.nsplit * 9 * n;
+    const long want = 148L * 1536;
+    const int nitems = kg.nitems > 0 ? kg.nitems : kg.ncol * ((kg.nzl + TM - 1) / TM);
+    const long threads1 = (long)((nitems + SF_THREADS - 1) / SF_THREADS) * SF_THREADS;
+    int P = (int)((want + threads1 - 1) / threads1);
+    P = std::max(1, std::min(P * p_mul / 2, (n + 31) / 32));
+    L.natom_chunk = (n + P - 1) / P;
+    L.P = (n + L.natom_chunk - 1) / L.natom_chunk;
+    const long threads2 = (long)((n + KF_THREADS - 1) / KF_THREADS) * KF_THREADS;
+    int S = (int)((want + threads2 - 1) / threads2);
+    S = std::max(1, std::min(S * s_mul / 2, kg.ncol));
+    L.cols_per_split = (kg.ncol + S - 1) / S;
+    L.nsplit = (kg.ncol + L.cols_per_split - 1) / L.cols_per_split;
+    return L;
+}
+
+// Scratch for every launch shape the path may use (on the mixed path up to
+// the autotuner's largest splits).
+size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart, int mixed) {
+    RecLaunch L = plan(n, kg);
     size_t rows = std::max((size_t)L.nchunk * L.CH, (size_t)((kg.nzl + TM - 1) / TM) * TM);
-    return (size_t)L.P * rows * kg.ncol * 2;
+    size_t part = (size_t)L.P * rows * kg.ncol * 2;
+    *fpart = (size_t)L.nsplit * 9 * n;
+    if (mixed) {
+        RecLaunch M = plan_mixed(n, kg, 4, 4);
+        part = std::max(part, (size_t)M.P * rows * kg.ncol * 2);
+        *fpart = std::max(*fpart, (size_t)M.nsplit * 9 * n);
+    }
+    return part;
 }
 
 // The mixed path's fixed-point coordinates and phase tables for the current
@@ -861,12 +890,12 @@ void ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double*
 void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const double* q, const double* mu, CellP c, const KGrid& kg, RecFlags fl, RecScratch& rs,
                       double* ef, double* efg, double* fo, Partials& part, DevScalars* d, Prof* prof) {
-    RecLaunch L = plan(n, kg);
+    const bool mixed = fl.prec == MDFF_PREC_MIXED;
+    RecLaunch L = mixed ? plan_mixed(n, kg, rs.p_mul, rs.s_mul) : plan(n, kg);
     const size_t plane = (size_t)L.P * std::max(L.nchunk * L.CH, ((kg.nzl + TM - 1) / TM) * TM) * kg.ncol;
     double* pre = rs.part;
     double* pim = rs.part + plane;
     const int kx = kg.kmax[0], ky = kg.kmax[1], kz = kg.kmax[2];
-    const bool mixed = fl.prec == MDFF_PREC_MIXED;
     const bool low = mixed && rs.low.ncol > 0;
     const int nchunk32 = (kg.nzl + TM - 1) / TM;
     const int total = kg.ncol * kg.nzl;

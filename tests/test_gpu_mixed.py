@@ -81,3 +81,24 @@ def test_mixed_kspace_reuse_matches_fp64():
     assert rel(m["efg"], d["efg"]) < 1e-6
     assert abs(m["e"]["u_coul"] - d["e"]["u_coul"]) < 1e-6 * abs(d["e"]["u_coul"])
     assert rel(m["tau_coul"], d["tau_coul"]) < 1e-6
+
+
+@pytest.mark.parametrize("prec,tol", [(abi.PREC_FP64, 1e-12), (abi.PREC_MIXED, 1e-8)])
+def test_autotuned_launch_shapes_same_results(prec, tol):
+    """The autotuner's launch shapes change only the summation order."""
+    s = systems.mgo_pim(grid=(12, 12, 12), rc=8.0, alpha=0.4, kmax=10, vacancy_frac=0.01, seed=5, jitter=0.1)
+    out, shape = {}, None
+    for at in (0, 1):
+        p = s["params"]
+        p.precision = prec
+        p.autotune = at
+        p.kspace_reuse = 1
+        p.conv_tol_ind = 1e-11
+        e = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+        out[at] = e.engforce()
+        if at:
+            shape = e.launch_shape()
+    assert shape["g_dir"] in (8, 16, 32) and shape["g_dd32"] in (8, 16, 32)
+    assert shape["sfac_split_x2"] in (1, 2, 4) and shape["field_split_x2"] in (1, 2, 4)
+    assert rel(out[1]["f"], out[0]["f"]) < tol
+    assert rel(out[1]["mu"], out[0]["mu"]) < tol

@@ -47,6 +47,33 @@ __device__ __forceinline__ void tt_damp_d(double b, double c, double r, int k, d
     fd = term * inv * e * b;
 }
 
+// Packed two-lane FP32 arithmetic of sm_100 (add / mul / fma .rn.f32x2): a
+// 64-bit register holds the pair (lo, hi).
+typedef unsigned long long f2p;
+__device__ __forceinline__ f2p pk2(float lo, float hi) {
+    f2p r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk2(f2p v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2p ffma2(f2p a, f2p b, f2p c) {
+    f2p d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2p fmul2(f2p a, f2p b) {
+    f2p d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2p fadd2(f2p a, f2p b) {
+    f2p d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

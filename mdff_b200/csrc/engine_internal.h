@@ -217,7 +217,7 @@ struct RecScratch {
     size_t fpart_cap = 0;
     uint32_t* fixed = nullptr;  // [3][n] fractional coordinates as 32-bit fixed point
     float2* tab = nullptr;      // [n][16] e^{2 pi i m s_z}
-    float2* aks2 = nullptr;     // [ncol][nzp] A_k S(k) padded, FP32
+    float4* aks2 = nullptr;     // [ncol][nzp] A_k S(k) padded, FP32 pairs (re, re, im, im)
     int p_mul = 2, s_mul = 2;   // mixed path: FP32 structure-factor atom split and field column split, x mul/2
     long tab_epoch = -1;        // position epoch the table was built for
     long want_epoch = 0;        // current position epoch (set by the engine)

@@ -145,6 +145,7 @@ __global__ void k_sfac_reduce(int P, int ch, int nchunk, int ncol, int nzl, int 
 
 constexpr int KF_THREADS = 128;
 constexpr int KF_COLS = 4;   // columns staged per shared-memory round
+constexpr int KF_COLS32 = 16;   // the same for the packed FP32 field kernel
 
 template <int GRAD>
 __global__ void __launch_bounds__(KF_THREADS) k_kfield(int n, const double* __restrict__ sx, const double* __restrict__ sy,
@@ -304,16 +305,19 @@ __global__ void k_phase_table(int n, const double* __restrict__ sx, const double
     }
 }
 
-// A_k S(k) as float2, each column padded to nzp (a multiple of TM) with zeros.
+// conj-ready FP32 copy of A_k S(k) for the packed field kernel: per k the
+// pairs (re, re) and (im, im), each column padded to nzp (a multiple of TM)
+// with zeros.
 __global__ void k_aks32_pad(int ncol, int nzl, int nzp, int nrect, const double* __restrict__ aks,
-                            float2* __restrict__ out) {
+                            float4* __restrict__ out) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ncol * nzp) return;
     int col = t / nzp, m = t % nzp;
-    float2 v = make_float2(0.f, 0.f);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
     if (m < nzl) {
         size_t r = (size_t)col * nzl + m;
-        v = make_float2((float)aks[r], (float)aks[nrect + r]);
+        const float re = (float)aks[r], im = (float)aks[nrect + r];
+        v = make_float4(re, re, im, im);
     }
     out[t] = v;
 }
@@ -429,20 +433,24 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac32v4(int n, int natom_chunk,
     }
 }
 
-// Pass 2: thread = atom.  Per chunk of TM k-vectors along nz,
-//   Z_j = sum_m m^j conj(A_k S)_m T_m    (j = 0, 1 [, 2 for the gradient]),
+// Pass 2: thread = atom.  Per chunk of TM k-vectors along nz, with
+// P_m = conj(a_m) T_m (a_m = A_k S(k), T_m = e^{2 pi i m s_z}):
+//   Z0 = sum_m P_m,  Z1 = sum_m m P_m  (and Z2 = sum_m m^2 P_m for the gradient),
 // then with the chunk's base phase e0 and k_m = kb + m dk:
 //   sum_m k_m recarg_m = -(kb Im(e0 Z0) + dk Im(e0 Z1)),
 //   sum_m k_m k_m^T recarg2_m = kb kb^T Re(e0 Z0) + (kb dk^T + dk kb^T) Re(e0 Z1) + dk dk^T Re(e0 Z2).
-// The column's base phase is computed once; chunk bases follow by
-// multiplication with e^{2 pi i 16 s_z}.  The chunk sums go to FP64.
+// The inner loop is packed FP32 (f32x2): P_m = a_re (T) + a_im (T_im, -T_re)
+// from a 16-byte shared-memory load of (a_re, a_re, a_im, a_im), and the
+// m-weighted sums come from running suffix sums over m descending
+// (R = sum_{m>=j} P_m, Q = sum R, W = sum Q: Z1 = Q, Z2 = 2W - Q), so no
+// per-m constants are needed.  Each column's FP32 sum is flushed to FP64.
 template <int GRAD>
-__global__ void __launch_bounds__(KF_THREADS) k_kfield32v4(int n, const uint32_t* __restrict__ fx,
+__global__ void __launch_bounds__(KF_THREADS) k_kfield32v5(int n, const uint32_t* __restrict__ fx,
                                                            const float2* __restrict__ tab, CellP c, int kx, int ky,
                                                            int kz, int ncol, int nzp, int cols_per_split,
-                                                           const float2* __restrict__ aks, const int* __restrict__ colrange,
+                                                           const float4* __restrict__ aks, const int* __restrict__ colrange,
                                                            double* __restrict__ fpart) {
-    extern __shared__ float2 ska[];
+    extern __shared__ float4 ska4[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int split = blockIdx.y;
     const int c0 = split * cols_per_split;
@@ -450,9 +458,13 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v4(int n, const uint32_t
     const bool active = i < n;
     const int ii = active ? i : 0;
     const uint32_t u1 = fx[ii], u2 = fx[n + ii], u3 = fx[2 * n + ii];
-    float2 T[TM];
+    f2p T[TM], Tn[TM];
 #pragma unroll
-    for (int m = 0; m < TM; ++m) T[m] = tab[(size_t)ii * TM + m];
+    for (int m = 0; m < TM; ++m) {
+        const float2 t = tab[(size_t)ii * TM + m];
+        T[m] = pk2(t.x, t.y);
+        Tn[m] = pk2(t.y, -t.x);
+    }
     float e16c, e16s;
     phase32(u3 * 16u, e16c, e16s);
     const float b1x = (float)(2.0 * PI * c.B[0]), b1y = (float)(2.0 * PI * c.B[3]), b1z = (float)(2.0 * PI * c.B[6]);
@@ -461,14 +473,13 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v4(int n, const uint32_t
     const int ny_n = 2 * ky + 1;
     double E0 = 0, E1 = 0, E2 = 0;
     double G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
-    for (int cb = c0; cb < c1; cb += KF_COLS) {
-        const int nc = min(KF_COLS, c1 - cb);
+    for (int cb = c0; cb < c1; cb += KF_COLS32) {
+        const int nc = min(KF_COLS32, c1 - cb);
         __syncthreads();
-        for (int t = threadIdx.x; t < nc * nzp; t += blockDim.x) ska[t] = aks[(size_t)cb * nzp + t];
+        for (int t = threadIdx.x; t < nc * nzp; t += blockDim.x) ska4[t] = aks[(size_t)cb * nzp + t];
         __syncthreads();
         for (int cc = 0; cc < nc; ++cc) {
             const int col = cb + cc;
-            // the column's chunks of the FP32 set (all of them without a range table)
             int clo = 0, cn = nzp / TM;
             if (colrange) { clo = colrange[2 * col]; cn = colrange[2 * col + 1]; }
             if (cn == 0) continue;
@@ -481,32 +492,42 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v4(int n, const uint32_t
             float kb0 = fmaf(fnx, b1x, fmaf(fny, b2x, fnz * dk0));
             float kb1 = fmaf(fnx, b1y, fmaf(fny, b2y, fnz * dk1));
             float kb2 = fmaf(fnx, b1z, fmaf(fny, b2z, fnz * dk2));
-            const float2* pk = ska + cc * nzp;
+            const ulonglong2* pk = reinterpret_cast<const ulonglong2*>(ska4 + cc * nzp);
+            float e0 = 0.f, e1 = 0.f, e2 = 0.f;
+            float g0 = 0.f, g1 = 0.f, g2 = 0.f, g3 = 0.f, g4 = 0.f, g5 = 0.f;
             for (int m0 = TM * clo; m0 < TM * (clo + cn); m0 += TM) {
-                float z0r = 0.f, z0i = 0.f, z1r = 0.f, z1i = 0.f, z2r = 0.f, z2i = 0.f;
+                f2p R = 0ull, Q = 0ull, W = 0ull;
 #pragma unroll
-                for (int m = 0; m < TM; ++m) {
-                    const float2 a = pk[m0 + m];
-                    // conj(a) T_m
-                    const float pr = fmaf(a.x, T[m].x, a.y * T[m].y);
-                    const float pi = fmaf(a.x, T[m].y, -a.y * T[m].x);
-                    z0r += pr; z0i += pi;
-                    z1r = fmaf((float)m, pr, z1r); z1i = fmaf((float)m, pi, z1i);
-                    if (GRAD) { z2r = fmaf((float)(m * m), pr, z2r); z2i = fmaf((float)(m * m), pi, z2i); }
+                for (int m = TM - 1; m >= 1; --m) {
+                    const ulonglong2 a = pk[m0 + m];
+                    const f2p P = ffma2(a.x, T[m], fmul2(a.y, Tn[m]));
+                    R = fadd2(R, P);
+                    Q = fadd2(Q, R);
+                    if (GRAD) W = fadd2(W, Q);
                 }
+                {
+                    const ulonglong2 a = pk[m0];
+                    R = fadd2(R, ffma2(a.x, T[0], fmul2(a.y, Tn[0])));
+                }
+                float z0r, z0i, z1r, z1i;
+                upk2(R, z0r, z0i);
+                upk2(Q, z1r, z1i);
                 const float p0r = fmaf(ec, z0r, -es * z0i), p0i = fmaf(ec, z0i, es * z0r);
                 const float p1r = fmaf(ec, z1r, -es * z1i), p1i = fmaf(ec, z1i, es * z1r);
-                E0 += (double)fmaf(kb0, p0i, dk0 * p1i);
-                E1 += (double)fmaf(kb1, p0i, dk1 * p1i);
-                E2 += (double)fmaf(kb2, p0i, dk2 * p1i);
+                e0 = fmaf(kb0, p0i, fmaf(dk0, p1i, e0));
+                e1 = fmaf(kb1, p0i, fmaf(dk1, p1i, e1));
+                e2 = fmaf(kb2, p0i, fmaf(dk2, p1i, e2));
                 if (GRAD) {
+                    float wr, wi;
+                    upk2(W, wr, wi);
+                    const float z2r = 2.f * wr - z1r, z2i = 2.f * wi - z1i;
                     const float p2r = fmaf(ec, z2r, -es * z2i);
-                    G0 += (double)(kb0 * kb0 * p0r + 2.f * kb0 * dk0 * p1r + dk0 * dk0 * p2r);
-                    G1 += (double)(kb1 * kb1 * p0r + 2.f * kb1 * dk1 * p1r + dk1 * dk1 * p2r);
-                    G2 += (double)(kb2 * kb2 * p0r + 2.f * kb2 * dk2 * p1r + dk2 * dk2 * p2r);
-                    G3 += (double)(kb0 * kb1 * p0r + (kb0 * dk1 + dk0 * kb1) * p1r + dk0 * dk1 * p2r);
-                    G4 += (double)(kb0 * kb2 * p0r + (kb0 * dk2 + dk0 * kb2) * p1r + dk0 * dk2 * p2r);
-                    G5 += (double)(kb1 * kb2 * p0r + (kb1 * dk2 + dk1 * kb2) * p1r + dk1 * dk2 * p2r);
+                    g0 += kb0 * kb0 * p0r + 2.f * kb0 * dk0 * p1r + dk0 * dk0 * p2r;
+                    g1 += kb1 * kb1 * p0r + 2.f * kb1 * dk1 * p1r + dk1 * dk1 * p2r;
+                    g2 += kb2 * kb2 * p0r + 2.f * kb2 * dk2 * p1r + dk2 * dk2 * p2r;
+                    g3 += kb0 * kb1 * p0r + (kb0 * dk1 + dk0 * kb1) * p1r + dk0 * dk1 * p2r;
+                    g4 += kb0 * kb2 * p0r + (kb0 * dk2 + dk0 * kb2) * p1r + dk0 * dk2 * p2r;
+                    g5 += kb1 * kb2 * p0r + (kb1 * dk2 + dk1 * kb2) * p1r + dk1 * dk2 * p2r;
                 }
                 const float nc_ = fmaf(ec, e16c, -es * e16s);
                 es = fmaf(es, e16c, ec * e16s);
@@ -514,6 +535,11 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield32v4(int n, const uint32_t
                 kb0 = fmaf(16.f, dk0, kb0);
                 kb1 = fmaf(16.f, dk1, kb1);
                 kb2 = fmaf(16.f, dk2, kb2);
+            }
+            E0 += (double)e0; E1 += (double)e1; E2 += (double)e2;
+            if (GRAD) {
+                G0 += (double)g0; G1 += (double)g1; G2 += (double)g2;
+                G3 += (double)g3; G4 += (double)g4; G5 += (double)g5;
             }
         }
     }
@@ -978,12 +1004,13 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     if (mixed) {
         const int nzp = nchunk32 * TM;
         k_aks32_pad<<<(kg.ncol * nzp + 255) / 256, 256, 0, st>>>(kg.ncol, kg.nzl, nzp, kg.nrect, rs.aks, rs.aks2);
+        const size_t sm32 = sizeof(float4) * KF_COLS32 * nzp;
         if (grad)
-            k_kfield32v4<1><<<g2, KF_THREADS, sizeof(float2) * KF_COLS * nzp, st>>>(
-                n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
+            k_kfield32v5<1><<<g2, KF_THREADS, sm32, st>>>(n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp,
+                                                         L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
         else
-            k_kfield32v4<0><<<g2, KF_THREADS, sizeof(float2) * KF_COLS * nzp, st>>>(
-                n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp, L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
+            k_kfield32v5<0><<<g2, KF_THREADS, sm32, st>>>(n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp,
+                                                         L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
         nk += 2;
         if (low) {
             LowK& lk = rs.low;

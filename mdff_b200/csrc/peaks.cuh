@@ -40,13 +40,6 @@ __global__ void __launch_bounds__(256) k_peak_f32(float* out, float seed) {
     if (s == 1234.5678f) out[0] = s;
 }
 
-// Packed two-lane FP32 FMA (fma.rn.f32x2, sm_100).
-__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b, unsigned long long c) {
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-
 __global__ void __launch_bounds__(256) k_peak_f32x2(float* out, float seed) {
     unsigned long long a[8];
 #pragma unroll

@@ -322,113 +322,138 @@ __global__ void k_aks32_pad(int ncol, int nzl, int nzp, int nrect, const double*
     out[t] = v;
 }
 
-constexpr int SF4_TILE = 32;
-
-// Pass 1: thread = (column, chunk of TM nz values).  Atom t contributes
-// sum_m (w0 + m dw) T_m with w0 = (q + i k0.mu) e0 and dw = i (2 pi b3.mu) e0.
-// FP32 sums over a tile of atoms are added into FP32 block sums (a two-level
-// tree, at most a few dozen tiles per block) and written as FP64 partials.
+// Pass 1: each thread sweeps two (column, chunk) work items over the same
+// atoms, so one shared-memory load of the atom's table entry T_m serves both.
+// The amplitude of item k at nz index m is w_m = w0 + m dw (w0 = (q + i k0.mu)
+// e0, dw = i (2 pi b3.mu) e0, e0 the item's base phase): six scalar FMAs per
+// (atom, k), the minimum for a complex multiply-accumulate with a linearly
+// advancing amplitude.  When the second item is the next chunk of the same
+// column its base phase is the first one's times e^{2 pi i 16 s_z} (tabulated
+// per atom) instead of a second sin/cos.  FP32 sums over a tile of atoms go to
+// FP32 block sums in shared memory (a two-level tree) and are written as FP64
+// partials.
+constexpr int SF32_TILE = 32;
 template <int WITH_MU>
-__global__ void __launch_bounds__(SF_THREADS) k_sfac32v4(int n, int natom_chunk, const uint32_t* __restrict__ fx,
+__global__ void __launch_bounds__(SF_THREADS) k_sfac32(int n, int natom_chunk, const uint32_t* __restrict__ fx,
                                                          const float2* __restrict__ tab, const double* __restrict__ q,
-                                                         const double* __restrict__ mu, CellP c, int kx, int ky, int kz,
-                                                         int ncol, int ncolblk, int nchunk, int with_q,
-                                                         const int* __restrict__ items, int nitems,
-                                                         double* __restrict__ part_re, double* __restrict__ part_im) {
-    __shared__ uint32_t t_u1[SF4_TILE], t_u2[SF4_TILE], t_u3[SF4_TILE];
-    __shared__ float t_q[SF4_TILE], t_m1[SF4_TILE], t_m2[SF4_TILE], t_m3[SF4_TILE];
-    __shared__ float4 t_T[SF4_TILE][TM / 2];    // (T_m, T_m+1) pairs
-    // work item: (column, chunk of TM nz), from the work list when given
-    int h, col;
-    if (items) {
-        const int it = blockIdx.x * SF_THREADS + threadIdx.x;
-        const int itc = it < nitems ? it : nitems - 1;
-        col = it < nitems ? items[2 * itc] : ncol;
-        h = items[2 * itc + 1];
-    } else {
-        h = blockIdx.x / ncolblk;
-        col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
-    }
+                                                         const double* __restrict__ mu, CellP c, int ky, int kz,
+                                                         int ncol, int nchunk, int with_q, const int* __restrict__ items,
+                                                         int nitems, double* __restrict__ part_re,
+                                                         double* __restrict__ part_im) {
+    __shared__ uint4 t_a[SF32_TILE];                 // u1, u2, u3, q (float bits)
+    __shared__ float4 t_m[SF32_TILE];                // 2 pi b_d . mu (d = 1..3), unused
+    __shared__ float2 t_16[SF32_TILE];               // e^{2 pi i 16 s_z}
+    __shared__ float4 t_T[SF32_TILE][TM / 2];        // (T_m, T_m+1)
+    __shared__ float s_acc[4 * TM][SF_THREADS];     // second-level sums: [item][re/im][m] x thread
+    const int t0 = 2 * (blockIdx.x * SF_THREADS + threadIdx.x);
     const int p = blockIdx.y;
     const int ny_n = 2 * ky + 1;
-    const int colc = col < ncol ? col : (items ? items[2 * (nitems - 1)] : ncol - 1);
-    const int inx = colc / ny_n, iny = colc % ny_n - ky, inz0 = -kz + h * TM;
-    const float fnx = (float)inx, fny = (float)iny, fnz0 = (float)inz0;
-    float ore[TM], oim[TM];
+    int inx[2], iny[2], inz0[2];
 #pragma unroll
-    for (int m = 0; m < TM; ++m) { ore[m] = 0.f; oim[m] = 0.f; }
+    for (int it = 0; it < 2; ++it) {
+        const int kc = min(t0 + it, nitems - 1);
+        const int cl = items[2 * kc];
+        inx[it] = cl / ny_n;
+        iny[it] = cl % ny_n - ky;
+        inz0[it] = -kz + items[2 * kc + 1] * TM;
+    }
+    // the second item continues the first one's column: rotate instead of sin/cos
+    const bool chain = inx[1] == inx[0] && iny[1] == iny[0] && inz0[1] == inz0[0] + TM;
+#pragma unroll
+    for (int k = 0; k < 4 * TM; ++k) s_acc[k][threadIdx.x] = 0.f;
     const int a0 = p * natom_chunk;
     const int a1 = min(n, a0 + natom_chunk);
-    for (int base = a0; base < a1; base += SF4_TILE) {
+    for (int base = a0; base < a1; base += SF32_TILE) {
         __syncthreads();
-        for (int t = threadIdx.x; t < SF4_TILE * (TM / 2); t += blockDim.x) {
-            int ia = base + t / (TM / 2);
-            if (ia < a1) {
-                const float2* src = tab + (size_t)ia * TM + 2 * (t % (TM / 2));
-                float2 A = src[0], B = src[1];
-                t_T[t / (TM / 2)][t % (TM / 2)] = make_float4(A.x, A.y, B.x, B.y);
-            }
+        const int tn = min(SF32_TILE, a1 - base);
+        for (int t = threadIdx.x; t < tn * (TM / 2); t += blockDim.x) {
+            const int a = t / (TM / 2), m2 = t % (TM / 2);
+            const float2* src = tab + (size_t)(base + a) * TM + 2 * m2;
+            const float2 A = src[0], B = src[1];
+            t_T[a][m2] = make_float4(A.x, A.y, B.x, B.y);
         }
-        if (threadIdx.x < SF4_TILE) {
-            int ia = base + threadIdx.x;
-            if (ia < a1) {
-                t_u1[threadIdx.x] = fx[ia];
-                t_u2[threadIdx.x] = fx[n + ia];
-                t_u3[threadIdx.x] = fx[2 * n + ia];
-                t_q[threadIdx.x] = with_q ? (float)q[ia] : 0.f;
-                double m0 = 0, m1 = 0, m2 = 0;
-                if (WITH_MU) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
-                t_m1[threadIdx.x] = (float)(2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2));
-                t_m2[threadIdx.x] = (float)(2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2));
-                t_m3[threadIdx.x] = (float)(2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2));
-            }
+        if (threadIdx.x < tn) {
+            const int ia = base + threadIdx.x;
+            const float qa = with_q ? (float)q[ia] : 0.f;
+            const uint32_t u3 = fx[2 * n + ia];
+            t_a[threadIdx.x] = make_uint4(fx[ia], fx[n + ia], u3, __float_as_uint(qa));
+            double m0 = 0, m1 = 0, m2 = 0;
+            if (WITH_MU) { m0 = mu[ia]; m1 = mu[n + ia]; m2 = mu[2 * n + ia]; }
+            t_m[threadIdx.x] = make_float4((float)(2.0 * PI * (c.B[0] * m0 + c.B[3] * m1 + c.B[6] * m2)),
+                                           (float)(2.0 * PI * (c.B[1] * m0 + c.B[4] * m1 + c.B[7] * m2)),
+                                           (float)(2.0 * PI * (c.B[2] * m0 + c.B[5] * m1 + c.B[8] * m2)), 0.f);
+            float c16, s16;
+            phase32(u3 * 16u, c16, s16);
+            t_16[threadIdx.x] = make_float2(c16, s16);
         }
         __syncthreads();
-        const int tn = min(SF4_TILE, a1 - base);
-        float are[TM], aim[TM];
+        float ar0[TM], ai0[TM], ar1[TM], ai1[TM];
 #pragma unroll
-        for (int m = 0; m < TM; ++m) { are[m] = 0.f; aim[m] = 0.f; }
-        for (int t = 0; t < tn; ++t) {
-            const uint32_t ph = (uint32_t)inx * t_u1[t] + (uint32_t)iny * t_u2[t] + (uint32_t)inz0 * t_u3[t];
-            float c0, s0;
-            phase32(ph, c0, s0);
-            const float qa = t_q[t];
-            float w0r, w0i, dwr = 0.f, dwi = 0.f;
-            if (WITH_MU) {
-                const float km = fmaf(fnx, t_m1[t], fmaf(fny, t_m2[t], fnz0 * t_m3[t]));
-                const float m3 = t_m3[t];
-                w0r = fmaf(qa, c0, -km * s0);
-                w0i = fmaf(qa, s0, km * c0);
-                dwr = -m3 * s0;
-                dwi = m3 * c0;
+        for (int m = 0; m < TM; ++m) { ar0[m] = 0.f; ai0[m] = 0.f; ar1[m] = 0.f; ai1[m] = 0.f; }
+        for (int a = 0; a < tn; ++a) {
+            const uint4 A = t_a[a];
+            const float qa = __uint_as_float(A.w);
+            float c0[2], s0[2];
+            phase32((uint32_t)inx[0] * A.x + (uint32_t)iny[0] * A.y + (uint32_t)inz0[0] * A.z, c0[0], s0[0]);
+            if (chain) {
+                const float2 e16 = t_16[a];
+                c0[1] = fmaf(c0[0], e16.x, -s0[0] * e16.y);
+                s0[1] = fmaf(s0[0], e16.x, c0[0] * e16.y);
             } else {
-                w0r = qa * c0;
-                w0i = qa * s0;
+                phase32((uint32_t)inx[1] * A.x + (uint32_t)iny[1] * A.y + (uint32_t)inz0[1] * A.z, c0[1], s0[1]);
+            }
+            float w0r[2], w0i[2], dwr[2] = {0.f, 0.f}, dwi[2] = {0.f, 0.f};
+            const float4 M = t_m[a];
+#pragma unroll
+            for (int it = 0; it < 2; ++it) {
+                if (WITH_MU) {
+                    const float km = fmaf((float)inx[it], M.x, fmaf((float)iny[it], M.y, (float)inz0[it] * M.z));
+                    w0r[it] = fmaf(qa, c0[it], -km * s0[it]);
+                    w0i[it] = fmaf(qa, s0[it], km * c0[it]);
+                    dwr[it] = -M.z * s0[it];
+                    dwi[it] = M.z * c0[it];
+                } else {
+                    w0r[it] = qa * c0[it];
+                    w0i[it] = qa * s0[it];
+                }
             }
 #pragma unroll
             for (int m2 = 0; m2 < TM / 2; ++m2) {
-                const float4 TT = t_T[t][m2];
+                const float4 TT = t_T[a][m2];
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
                     const int m = 2 * m2 + j;
                     const float tx = j ? TT.z : TT.x, ty = j ? TT.w : TT.y;
-                    const float wr = WITH_MU ? fmaf((float)m, dwr, w0r) : w0r;
-                    const float wi = WITH_MU ? fmaf((float)m, dwi, w0i) : w0i;
-                    are[m] = fmaf(wr, tx, fmaf(-wi, ty, are[m]));
-                    aim[m] = fmaf(wr, ty, fmaf(wi, tx, aim[m]));
+                    const float wr0 = WITH_MU ? fmaf((float)m, dwr[0], w0r[0]) : w0r[0];
+                    const float wi0 = WITH_MU ? fmaf((float)m, dwi[0], w0i[0]) : w0i[0];
+                    const float wr1 = WITH_MU ? fmaf((float)m, dwr[1], w0r[1]) : w0r[1];
+                    const float wi1 = WITH_MU ? fmaf((float)m, dwi[1], w0i[1]) : w0i[1];
+                    ar0[m] = fmaf(wr0, tx, fmaf(-wi0, ty, ar0[m]));
+                    ai0[m] = fmaf(wr0, ty, fmaf(wi0, tx, ai0[m]));
+                    ar1[m] = fmaf(wr1, tx, fmaf(-wi1, ty, ar1[m]));
+                    ai1[m] = fmaf(wr1, ty, fmaf(wi1, tx, ai1[m]));
                 }
             }
         }
 #pragma unroll
-        for (int m = 0; m < TM; ++m) { ore[m] += are[m]; oim[m] += aim[m]; }
+        for (int m = 0; m < TM; ++m) {
+            s_acc[2 * m][threadIdx.x] += ar0[m];
+            s_acc[2 * m + 1][threadIdx.x] += ai0[m];
+            s_acc[2 * TM + 2 * m][threadIdx.x] += ar1[m];
+            s_acc[2 * TM + 2 * m + 1][threadIdx.x] += ai1[m];
+        }
     }
-    if (col < ncol) {
-        const size_t plane = (size_t)ncol * TM * nchunk;
+    const size_t plane = (size_t)ncol * TM * nchunk;
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+        const int k = t0 + it;
+        if (k >= nitems) continue;
+        const int cl = items[2 * k], hh = items[2 * k + 1];
 #pragma unroll
         for (int m = 0; m < TM; ++m) {
-            size_t idx = (size_t)p * plane + ((size_t)h * TM + m) * ncol + col;
-            part_re[idx] = (double)ore[m];
-            part_im[idx] = (double)oim[m];
+            const size_t idx = (size_t)p * plane + ((size_t)hh * TM + m) * ncol + cl;
+            part_re[idx] = (double)s_acc[2 * TM * it + 2 * m][threadIdx.x];
+            part_im[idx] = (double)s_acc[2 * TM * it + 2 * m + 1][threadIdx.x];
         }
     }
 }
@@ -875,7 +900,8 @@ static RecLaunch plan_mixed(int n, const KGrid& kg, int p_mul, int s_mul) {
     RecLaunch L = plan(n, kg);
     const long want = 148L * 1536;
     const int nitems = kg.nitems > 0 ? kg.nitems : kg.ncol * ((kg.nzl + TM - 1) / TM);
-    const long threads1 = (long)((nitems + SF_THREADS - 1) / SF_THREADS) * SF_THREADS;
+    const int nthr = (nitems + 1) / 2;   // two work items per thread
+    const long threads1 = (long)((nthr + SF_THREADS - 1) / SF_THREADS) * SF_THREADS;
     int P = (int)((want + threads1 - 1) / threads1);
     P = std::max(1, std::min(P * p_mul / 2, (n + 31) / 32));
     L.natom_chunk = (n + P - 1) / P;
@@ -958,14 +984,14 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         }
         // the FP32 set's (column, chunk) work list: the low-|k| vectors and
         // those outside the sphere are not in it (A_k = 0 there)
-        dim3 g1((kg.nitems + SF_THREADS - 1) / SF_THREADS, L.P);
+        dim3 g1(((kg.nitems + 1) / 2 + SF_THREADS - 1) / SF_THREADS, L.P);
         if (kg.nitems > 0) {
             if (fl.with_mu)
-                k_sfac32v4<1><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
-                                                         L.ncolblk, nchunk32, fl.with_q, kg.items, kg.nitems, pre, pim);
+                k_sfac32<1><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, ky, kz, kg.ncol,
+                                                         nchunk32, fl.with_q, kg.items, kg.nitems, pre, pim);
             else
-                k_sfac32v4<0><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, kx, ky, kz, kg.ncol,
-                                                         L.ncolblk, nchunk32, fl.with_q, kg.items, kg.nitems, pre, pim);
+                k_sfac32<0><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, ky, kz, kg.ncol,
+                                                         nchunk32, fl.with_q, kg.items, kg.nitems, pre, pim);
         }
         k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, TM, nchunk32, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak_hi, kg.kcoe, c,
                                           rs.aks, kg.nrect, fl.energy, part.buf);

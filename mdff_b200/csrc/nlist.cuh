@@ -110,16 +110,33 @@ __global__ void k_bin_fill(int n, const int* cell_of, int* cursor, int* atoms) {
 }
 
 // Atomic fill leaves an arbitrary order inside each cell; sort each cell's
-// atoms by index so that the list layout is deterministic.
-__global__ void k_sort_cells(int ncell, const int* start, int* atoms) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+// atoms by index so that the list layout is deterministic.  One block per
+// cell: the cell's atoms are staged in shared memory and each element is
+// written to its rank (the number of smaller indices; indices are distinct).
+// A cell of more than SORT_CAP atoms is sorted by one thread (insertion).
+constexpr int SORT_CAP = 4096;
+__global__ void k_sort_cells(int ncell, const int* __restrict__ start, int* atoms) {
+    __shared__ int s_at[SORT_CAP];
+    const int c = blockIdx.x;
     if (c >= ncell) return;
-    int b = start[c], e = start[c + 1];
+    const int b = start[c], e = start[c + 1], m = e - b;
+    if (m <= SORT_CAP) {
+        for (int t = threadIdx.x; t < m; t += blockDim.x) s_at[t] = atoms[b + t];
+        __syncthreads();
+        for (int t = threadIdx.x; t < m; t += blockDim.x) {
+            const int v = s_at[t];
+            int r = 0;
+            for (int k = 0; k < m; ++k) r += s_at[k] < v;
+            atoms[b + r] = v;
+        }
+        return;
+    }
+    if (threadIdx.x != 0) return;
     for (int k = b + 1; k < e; ++k) {
         int v = atoms[k];
-        int m = k - 1;
-        while (m >= b && atoms[m] > v) { atoms[m + 1] = atoms[m]; --m; }
-        atoms[m + 1] = v;
+        int q = k - 1;
+        while (q >= b && atoms[q] > v) { atoms[q + 1] = atoms[q]; --q; }
+        atoms[q + 1] = v;
     }
 }
 
@@ -128,7 +145,7 @@ void launch_bin(cudaStream_t st, int n, const double* sx, const double* sy, cons
     k_bin_count<<<(n + 255) / 256, 256, 0, st>>>(n, sx, sy, sz, g.nc[0], g.nc[1], g.nc[2], g.cell_of, g.cell_count);
     k_scan<<<1, 1024, 0, st>>>(g.ncell, g.cell_count, g.cell_start, g.cell_cursor);
     k_bin_fill<<<(n + 255) / 256, 256, 0, st>>>(n, g.cell_of, g.cell_cursor, g.cell_atoms);
-    k_sort_cells<<<(g.ncell + 127) / 128, 128, 0, st>>>(g.ncell, g.cell_start, g.cell_atoms);
+    k_sort_cells<<<g.ncell, 128, 0, st>>>(g.ncell, g.cell_start, g.cell_atoms);
 }
 
 // ------------------------------------------------------------ list build --

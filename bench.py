@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--keps", type=float, default=None,
                     help="mixed path: leave out k with exp(-k^2/4 alpha^2) below keps (0: all; default: the library's)")
     ap.add_argument("--autotune", type=int, default=1, choices=[0, 1], help="autotune the launch shapes")
+    ap.add_argument("--tc", type=int, default=1, choices=[0, 1],
+                    help="mixed path: structure factor on the tensor cores (1) or the FP32 CUDA-core kernel (0)")
     ap.add_argument("--reuse", default="auto", choices=["auto", "0", "1"],
                     help="kspace_reuse (auto: on for the mixed path, off for the plain FP64 path)")
     ap.add_argument("--workload", default="production", choices=["production", "batch"],
@@ -177,6 +179,7 @@ def run_engine(args):
     if args.keps is not None:
         p.mixed_keps = args.keps
     p.autotune = args.autotune
+    p.kspace_tc = args.tc
     natm = len(s["itype"])
     eng = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
     eng.enable_profile(True)
@@ -272,6 +275,7 @@ def run_engine(args):
                        "kspace_reuse": int(p.kspace_reuse),
                        "mixed_ksplit": p.mixed_ksplit if args.precision == "mixed" else None,
                        "mixed_keps": p.mixed_keps if args.precision == "mixed" else None,
+                       "kspace_tc": int(p.kspace_tc) if args.precision == "mixed" else None,
                        "precision": args.precision, "parallelism": f"replicas{world}",
                        "l2": "per-step working set > 126 MB L2 (k-space partials, Verlet lists)"},
             "gpu_launches": int(prof["_launches"]["count"]),
@@ -345,6 +349,7 @@ def run_accuracy(args):
         pm.mixed_ksplit = args.ksplit
     if args.keps is not None:
         pm.mixed_keps = args.keps
+    pm.kspace_tc = args.tc
     pf = abi.Params()
     C.pointer(pf)[0] = p
     snaps = []
@@ -375,7 +380,7 @@ def run_accuracy(args):
         })
     return {"mode": "accuracy", "workload": "mgo-pim-production", "natm": len(s["itype"]),
             "mixed": {"kspace_reuse": int(pm.kspace_reuse), "mixed_ksplit": pm.mixed_ksplit,
-                      "mixed_keps": pm.mixed_keps}, "snapshots": snaps,
+                      "mixed_keps": pm.mixed_keps, "kspace_tc": int(pm.kspace_tc)}, "snapshots": snaps,
             "eps_F_max": max(x["eps_F"] for x in snaps)}
 
 

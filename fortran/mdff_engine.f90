@@ -79,6 +79,7 @@ module mdff_engine
     integer(c_int) :: kspace_reuse
     real(c_double) :: mixed_keps
     integer(c_int) :: autotune
+    integer(c_int) :: kspace_tc
   end type mdff_params_t
 
   type, bind(C) :: mdff_energies_t

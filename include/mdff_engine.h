@@ -138,6 +138,9 @@ typedef struct mdff_params {
                                                   is below mixed_keps are left out (0: the whole rectangle) */
     int    autotune;                           /* 1: time the candidate launch shapes of the Ewald kernels on the
                                                   first force evaluation and keep the fastest */
+    int    kspace_tc;                          /* mixed path: 1 = structure factor on the tensor cores (exact int8
+                                                  digit products of 24-bit fixed point) when nz rows <= 80;
+                                                  0 = FP32 CUDA-core kernel */
 } mdff_params;
 
 /* Energies and scalar outputs of one force evaluation (thermodynamic module

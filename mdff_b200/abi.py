@@ -56,6 +56,7 @@ class Params(C.Structure):
         ("precision", C.c_int), ("efg_period", C.c_int), ("nlist_capacity", C.c_int), ("device", C.c_int),
         ("erfc_ref", C.c_int), ("nhc_literal", C.c_int), ("mixed_ksplit", C.c_double),
         ("kspace_reuse", C.c_int), ("mixed_keps", C.c_double), ("autotune", C.c_int),
+        ("kspace_tc", C.c_int),
     ]
 
 
@@ -141,4 +142,5 @@ def default_params():
     p.device = 0
     p.mixed_ksplit = 2.5
     p.mixed_keps = 1e-7
+    p.kspace_tc = 1
     return p

@@ -141,6 +141,9 @@ int sync_scalars(mdff_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     ctx->prof.harvest();
+    if (ctx->hsc->tc_err)
+        return fail(ctx, MDFF_E_CUDA, "tensor-core structure factor: a pipeline wait gave up (code " +
+                                          std::to_string(ctx->hsc->tc_err) + ")");
     return MDFF_OK;
 }
 
@@ -432,8 +435,7 @@ void dd_field_real(mdff_ctx* ctx, const double* m, double* out) {
     const int n = ctx->n;
     ctx->prof.begin(PK_DIR);
     if (ctx->p.precision == MDFF_PREC_MIXED) {
-        int k = ctx->rs.tab_epoch != ctx->rs.want_epoch ? 2 : 1;
-        ensure_phase_tables(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->rs);
+        const int k = 1 + ensure_phase_tables(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->rs);
         launch_ewald_dd32(ctx->st, n, ctx->rs.fixed, m, ctx->cell, coul_list(ctx), ctx->cut_coul * ctx->cut_coul,
                           ctx->alphaES, out, ctx->g_dd);
         ctx->prof.end(k);
@@ -1127,6 +1129,7 @@ void mdff_params_default(mdff_params* p) {
     p->precision = MDFF_PREC_FP64;
     p->mixed_ksplit = 2.5;
     p->mixed_keps = 1e-7;
+    p->kspace_tc = 1;
 }
 
 int mdff_create(const mdff_params* p, mdff_ctx** out) {
@@ -1354,6 +1357,7 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 TRY(dalloc(ctx, &lk.tab, 16 * (size_t)n));
             }
         }
+        size_t tc_part = 0;
         if (p.precision == MDFF_PREC_MIXED) {
             // Leave out the k-vectors whose Gaussian factor exp(-k^2 / 4 alpha^2)
             // is below mixed_keps (a sphere |k|^2 > -4 alpha^2 ln mixed_keps).
@@ -1404,10 +1408,43 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 CK(cudaMemcpyAsync(kg.items, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice, ctx->st));
             TRY(dalloc(ctx, &kg.Ak_hi, kg.nrect));
             TRY(upload(ctx, kg.Ak_hi, akhi.data(), kg.nrect));
+            // tensor-core structure factor: GEMM rows = the columns of the work
+            // list, N = 2 x (nz rows padded to 8), atoms split so that the grid
+            // covers the 148 SMs about once
+            TcK& tc = ctx->rs.tc;
+            const int N = ((2 * kg.nzl + 15) / 16) * 16;
+            tc.on = p.kspace_tc && !items.empty() && N <= tcs::LSTRIDE;
+            if (tc.on) {
+                std::vector<int> sph;
+                for (size_t i = 0; i < items.size(); i += 2)
+                    if (sph.empty() || sph.back() != items[i]) sph.push_back(items[i]);
+                tc.nsph = (int)sph.size();
+                tc.ntile = (tc.nsph + 127) / 128;
+                tc.N = N;
+                tc.kx = kg.kmax[0]; tc.ky = kg.kmax[1]; tc.kz = kg.kmax[2]; tc.nzl = kg.nzl;
+                tc.XYW = ((kg.kmax[0] + 2 + 2 * kg.kmax[1]) + 1) / 2 * 2;
+                tc.nblk = (n + tcs::SA - 1) / tcs::SA;
+                tc.npad = tc.nblk * tcs::SA;
+                int S = std::max(1, 148 / tc.ntile);
+                tc.bps = std::max(1, (tc.nblk + S - 1) / S);
+                tc.bps = std::min(tc.bps, 600);      // int32 headroom of the digit accumulators
+                tc.nsplit = (tc.nblk + tc.bps - 1) / tc.bps;
+                const tcs::Layout lay(N, tc.XYW);
+                tc.smem = lay.smem_bytes();
+                TRY(dalloc(ctx, &tc.cols, tc.nsph));
+                CK(cudaMemcpyAsync(tc.cols, sph.data(), sizeof(int) * tc.nsph, cudaMemcpyHostToDevice, ctx->st));
+                CK(cudaStreamSynchronize(ctx->st));
+                TRY(dalloc(ctx, &tc.xy, (size_t)tc.npad * tc.XYW));
+                TRY(dalloc(ctx, &tc.bimg, (size_t)tc.nblk * lay.b_bytes()));
+                TRY(dalloc(ctx, &tc.prm, (size_t)tc.npad));
+                TRY(dalloc(ctx, &tc.amax, (size_t)tc.npad));
+                CK(cudaFuncSetAttribute(tcs::k_sfac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc.smem));
+                tc_part = 2 * (size_t)tc.nsplit * kg.ncol * (((kg.nzl + TM - 1) / TM) * TM);
+            }
             CK(cudaStreamSynchronize(ctx->st));   // the host vectors above go out of scope
         }
         size_t fp = 0;
-        size_t pc = rec_scratch_doubles(n, kg, &fp, p.precision == MDFF_PREC_MIXED);
+        size_t pc = std::max(tc_part, rec_scratch_doubles(n, kg, &fp, p.precision == MDFF_PREC_MIXED));
         TRY(dalloc(ctx, &ctx->rs.part, pc));
         TRY(dalloc(ctx, &ctx->rs.fpart, fp));
         TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));

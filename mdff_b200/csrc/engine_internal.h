@@ -134,6 +134,7 @@ struct DevScalars {
     double dmax1, dmax2;
     int rebuild;
     int overflow;
+    int tc_err;         // tensor-core pipeline: a bounded wait gave up (bit per wait site)
 };
 
 // Launchers (kernels live in the *.cuh files, compiled as one unit by engine.cu).
@@ -208,6 +209,22 @@ struct LowK {
     int P = 1, natom_chunk = 0;
 };
 
+// Tensor-core structure factor of the mixed path (ewald_tc.cuh).
+struct TcK {
+    int on = 0;
+    int nsph = 0;             // sphere columns (rows of the GEMM)
+    int* cols = nullptr;      // [nsph] rectangle column index of each row
+    int ntile = 0, nsplit = 0, bps = 0;   // 128-row tiles, atom splits, 16-atom blocks per split
+    int nblk = 0, npad = 0;   // 16-atom blocks, padded atom count
+    int N = 0, XYW = 0;       // GEMM N (2 x padded nz rows), per-atom X/Y table width
+    int kx = 0, ky = 0, kz = 0, nzl = 0;
+    size_t smem = 0;
+    float2* xy = nullptr;     // [npad][XYW] X_a[nx], Y_a[ny]
+    uint8_t* bimg = nullptr;  // [nblk] B digit images
+    float4* prm = nullptr;    // [npad] (q, m1, m2, m3)
+    float* amax = nullptr;    // [npad]
+};
+
 struct RecScratch {
     double* part = nullptr;    // structure-factor partials
     size_t part_cap = 0;       // doubles
@@ -222,6 +239,7 @@ struct RecScratch {
     long tab_epoch = -1;        // position epoch the table was built for
     long want_epoch = 0;        // current position epoch (set by the engine)
     LowK low;
+    TcK tc;
 };
 struct RecFlags {
     int with_q, with_mu;
@@ -238,7 +256,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
                       Prof* prof);
 size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart, int mixed);
 void launch_aks_accumulate(cudaStream_t st, const KGrid& kg, RecScratch& rs, const DevScalars* d, int copy);
-void ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs);
+int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs);
 void launch_ewald_dd32(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
                        double cutsq, double alpha, double* ef, int g = 16);
 

@@ -19,6 +19,7 @@
 // The k set is the full rectangle nx in [0,kx], ny in [-ky,ky], nz in
 // [-kz,kz] with A_k = 0 on the half that the reference skips.
 #include "common.cuh"
+#include "ewald_tc.cuh"
 
 namespace mdff {
 
@@ -931,10 +932,18 @@ size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart, int mixed) {
 
 // The mixed path's fixed-point coordinates and phase tables for the current
 // positions (built once per position update).
-void ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs) {
-    if (rs.tab_epoch == rs.want_epoch) return;
+// (plus, with the tensor-core structure factor, its X/Y tables and B digit
+// images); returns the number of kernels launched.
+int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs) {
+    if (rs.tab_epoch == rs.want_epoch) return 0;
     k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab, rs.low.ncol > 0 ? rs.low.tab : nullptr);
     rs.tab_epoch = rs.want_epoch;
+    if (!rs.tc.on) return 1;
+    const TcK& t = rs.tc;
+    const long nxy = (long)t.npad * t.XYW, nb = (long)t.npad * (t.N / 2);
+    tcs::k_tc_xy<<<(unsigned)((nxy + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kx, t.ky, t.XYW, t.xy);
+    tcs::k_tc_bimage<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kz, t.nzl, t.N, t.bimg);
+    return 3;
 }
 
 #define CUDA_COPY_ACC(st, dst, src, bytes) cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (st))
@@ -976,16 +985,25 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             }
         }
     } else if (mixed) {
-        if (rs.tab_epoch != rs.want_epoch) {
-            k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab,
-                                                           rs.low.ncol > 0 ? rs.low.tab : nullptr);
-            rs.tab_epoch = rs.want_epoch;
-            nk++;
-        }
+        nk += ensure_phase_tables(st, n, sx, sy, sz, rs);
         // the FP32 set's (column, chunk) work list: the low-|k| vectors and
         // those outside the sphere are not in it (A_k = 0 there)
         dim3 g1(((kg.nitems + 1) / 2 + SF_THREADS - 1) / SF_THREADS, L.P);
-        if (kg.nitems > 0) {
+        int Pr = L.P;
+        if (rs.tc.on) {
+            // tensor-core structure factor: one partial per atom split
+            const TcK& t = rs.tc;
+            const size_t tplane = (size_t)kg.ncol * nchunk32 * TM;
+            pre = rs.part;
+            pim = rs.part + (size_t)t.nsplit * tplane;
+            tcs::k_tc_params<<<(t.npad + 255) / 256, 256, 0, st>>>(n, t.npad, q, mu, c, fl.with_q, fl.with_mu, kx, ky,
+                                                                   kz, t.prm, t.amax);
+            tcs::k_sfac_tc<<<dim3(t.ntile, t.nsplit), tcs::THREADS, t.smem, st>>>(
+                t.nblk, t.bps, t.bimg, t.xy, t.prm, t.amax, t.cols, t.nsph, kx, ky, kz, kg.nzl, t.N, t.XYW, kg.ncol,
+                tplane, pre, pim, &d->tc_err);
+            Pr = t.nsplit;
+            nk += 2;
+        } else if (kg.nitems > 0) {
             if (fl.with_mu)
                 k_sfac32<1><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, ky, kz, kg.ncol,
                                                          nchunk32, fl.with_q, kg.items, kg.nitems, pre, pim);
@@ -993,7 +1011,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
                 k_sfac32<0><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, rs.fixed, rs.tab, q, mu, c, ky, kz, kg.ncol,
                                                          nchunk32, fl.with_q, kg.items, kg.nitems, pre, pim);
         }
-        k_sfac_reduce<<<rb, 256, 0, st>>>(L.P, TM, nchunk32, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak_hi, kg.kcoe, c,
+        k_sfac_reduce<<<rb, 256, 0, st>>>(Pr, TM, nchunk32, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak_hi, kg.kcoe, c,
                                           rs.aks, kg.nrect, fl.energy, part.buf);
     } else {
         dim3 g1(L.nchunk * L.ncolblk, L.P);

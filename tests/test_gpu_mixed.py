@@ -102,3 +102,41 @@ def test_autotuned_launch_shapes_same_results(prec, tol):
     assert shape["sfac_split_x2"] in (1, 2, 4) and shape["field_split_x2"] in (1, 2, 4)
     assert rel(out[1]["f"], out[0]["f"]) < tol
     assert rel(out[1]["mu"], out[0]["mu"]) < tol
+
+
+@pytest.mark.parametrize("case", ["mgo_pim", "silica_rigid", "mgo_small_kz"])
+def test_tensor_core_structure_factor(case):
+    """The tensor-core structure factor (exact int8 digit products of 24-bit
+    fixed point) against the FP64 path, and no less accurate than the FP32
+    CUDA-core kernel it replaces.  Covers charges with dipoles and field
+    gradient, charges only, atom counts that are not a multiple of the
+    16-atom pipeline block, and a short nz range."""
+    if case == "mgo_pim":
+        s = systems.mgo_pim(grid=(16, 16, 16), rc=10.0, alpha=0.3, kmax=12, vacancy_frac=0.01, seed=3, jitter=0.1)
+        over = dict(doefg=1, conv_tol_ind=1e-10)
+    elif case == "silica_rigid":
+        s = systems.silica_bmh()
+        over = dict(doefield=1)
+    else:
+        s = systems.mgo_pim(grid=(10, 10, 6), rc=6.0, alpha=0.5, kmax=9, vacancy_frac=0.02, seed=5, jitter=0.1)
+        s["params"].kES[2] = 4
+        over = dict(doefg=1, conv_tol_ind=1e-10)
+    assert len(s["itype"]) % 16 != 0 or case == "silica_rigid"
+    out = {}
+    for key, prec, tc in (("fp64", abi.PREC_FP64, 0), ("fp32", abi.PREC_MIXED, 0), ("tc", abi.PREC_MIXED, 1)):
+        p = s["params"]
+        p.precision = prec
+        p.kspace_tc = tc
+        for k, v in over.items():
+            setattr(p, k, v)
+        out[key] = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"]).engforce()
+    d = out["fp64"]
+    e_tc = rel(out["tc"]["f"], d["f"])
+    e_32 = rel(out["fp32"]["f"], d["f"])
+    assert e_tc < 1e-6, (e_tc, e_32)
+    assert e_tc < 2.0 * e_32 + 1e-8, (e_tc, e_32)
+    assert abs(out["tc"]["e"]["u_coul"] - d["e"]["u_coul"]) < 1e-6 * abs(d["e"]["u_coul"])
+    assert rel(out["tc"]["tau_coul"], d["tau_coul"]) < 1e-6
+    if over.get("doefg"):
+        assert rel(out["tc"]["mu"], d["mu"]) < 1e-6
+        assert rel(out["tc"]["efg"], d["efg"]) < 1e-6

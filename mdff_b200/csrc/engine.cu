@@ -1440,11 +1440,28 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 TRY(dalloc(ctx, &tc.amax, (size_t)tc.npad));
                 CK(cudaFuncSetAttribute(tcs::k_sfac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc.smem));
                 tc_part = 2 * (size_t)tc.nsplit * kg.ncol * (((kg.nzl + TM - 1) / TM) * TM);
+                // field pass
+                tc.KZ = ((2 * kg.nzl + 31) / 32) * 32;
+                tc.ntile_f = (n + 127) / 128;
+                const tcf::FLayout f2(tc.KZ, tc.XYW, tcf::Cfg<2>::NB, tcf::Cfg<2>::CB);
+                const tcf::FLayout f3(tc.KZ, tc.XYW, tcf::Cfg<3>::NB, tcf::Cfg<3>::CB);
+                tc.smem_f2 = f2.smem_bytes();
+                tc.smem_f3 = f3.smem_bytes();
+                const size_t ncb2 = (tc.nsph + tcf::Cfg<2>::CB - 1) / tcf::Cfg<2>::CB;
+                const size_t ncb3 = (tc.nsph + tcf::Cfg<3>::CB - 1) / tcf::Cfg<3>::CB;
+                TRY(dalloc(ctx, &tc.aimg, (size_t)tc.ntile_f * f2.a_bytes()));
+                TRY(dalloc(ctx, &tc.xyt, (size_t)tc.ntile_f * tc.XYW * 128));
+                TRY(dalloc(ctx, &tc.fimg, std::max(ncb2 * f2.stage_bytes, ncb3 * f3.stage_bytes)));
+                CK(cudaFuncSetAttribute(tcf::k_kfield_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tc.smem_f2));
+                CK(cudaFuncSetAttribute(tcf::k_kfield_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tc.smem_f3));
             }
             CK(cudaStreamSynchronize(ctx->st));   // the host vectors above go out of scope
         }
         size_t fp = 0;
         size_t pc = std::max(tc_part, rec_scratch_doubles(n, kg, &fp, p.precision == MDFF_PREC_MIXED));
+        fp = std::max(fp, (size_t)2 * 9 * n);   // the tensor-core field pass writes two halves
         TRY(dalloc(ctx, &ctx->rs.part, pc));
         TRY(dalloc(ctx, &ctx->rs.fpart, fp));
         TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));

@@ -223,6 +223,12 @@ struct TcK {
     uint8_t* bimg = nullptr;  // [nblk] B digit images
     float4* prm = nullptr;    // [npad] (q, m1, m2, m3)
     float* amax = nullptr;    // [npad]
+    // field pass
+    int ntile_f = 0, KZ = 0;  // 128-atom tiles, K bytes (nz, re/im) per atom row
+    uint8_t* aimg = nullptr;  // [ntile_f] Z digit images
+    float2* xyt = nullptr;    // [ntile_f][XYW][128] X/Y tables
+    uint8_t* fimg = nullptr;  // per evaluation: B digit images + column constants
+    size_t smem_f2 = 0, smem_f3 = 0;
 };
 
 struct RecScratch {

@@ -943,7 +943,10 @@ int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* 
     const long nxy = (long)t.npad * t.XYW, nb = (long)t.npad * (t.N / 2);
     tcs::k_tc_xy<<<(unsigned)((nxy + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kx, t.ky, t.XYW, t.xy);
     tcs::k_tc_bimage<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kz, t.nzl, t.N, t.bimg);
-    return 3;
+    const long na = (long)t.ntile_f * 128 * (t.KZ / 16), nt = (long)t.ntile_f * 128 * t.XYW;
+    tcf::k_tcf_aimage<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(n, t.ntile_f, rs.fixed, t.kz, t.nzl, t.KZ, t.aimg);
+    tcf::k_tcf_xyt<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(t.npad, t.ntile_f, t.xy, t.XYW, t.xyt);
+    return 5;
 }
 
 #define CUDA_COPY_ACC(st, dst, src, bytes) cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (st))
@@ -1045,7 +1048,39 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     nk = 1;
     dim3 g2((n + KF_THREADS - 1) / KF_THREADS, L.nsplit);
     const bool grad = fl.grad || (fl.forces && fl.with_mu);
-    if (mixed) {
+    int nsplit_f = L.nsplit;
+    if (mixed && rs.tc.on) {
+        // field pass on the tensor cores: two column halves per atom
+        const TcK& t = rs.tc;
+        const int nch = t.KZ / 16;
+        if (grad) {
+            using C3 = tcf::Cfg<3>;
+            const int ncb = (t.nsph + C3::CB - 1) / C3::CB;
+            tcf::k_tcf_bimage<3><<<ncb, C3::NB * nch, 0, st>>>(t.nsph, t.cols, kx, ky, kz, kg.nzl, t.KZ, rs.aks,
+                                                                kg.nrect, c, t.fimg);
+            tcf::k_kfield_tc<3><<<t.ntile_f, tcf::THREADS, t.smem_f3, st>>>(n, ncb, t.aimg, t.xyt, t.fimg, t.KZ, t.XYW,
+                                                                             c, rs.fpart, &d->tc_err);
+        } else {
+            using C2 = tcf::Cfg<2>;
+            const int ncb = (t.nsph + C2::CB - 1) / C2::CB;
+            tcf::k_tcf_bimage<2><<<ncb, C2::NB * nch, 0, st>>>(t.nsph, t.cols, kx, ky, kz, kg.nzl, t.KZ, rs.aks,
+                                                                kg.nrect, c, t.fimg);
+            tcf::k_kfield_tc<2><<<t.ntile_f, tcf::THREADS, t.smem_f2, st>>>(n, ncb, t.aimg, t.xyt, t.fimg, t.KZ, t.XYW,
+                                                                             c, rs.fpart, &d->tc_err);
+        }
+        nsplit_f = 2;
+        nk += 1;
+        if (low) {
+            LowK& lk = rs.low;
+            if (grad)
+                k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+            else
+                k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+            nk++;
+        }
+    } else if (mixed) {
         const int nzp = nchunk32 * TM;
         k_aks32_pad<<<(kg.ncol * nzp + 255) / 256, 256, 0, st>>>(kg.ncol, kg.nzl, nzp, kg.nrect, rs.aks, rs.aks2);
         const size_t sm32 = sizeof(float4) * KF_COLS32 * nzp;
@@ -1077,7 +1112,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         nk++;
     }
     const double scale = 2.0 * 4.0 * PI / c.omega;
-    k_kfield_reduce<<<(n + 255) / 256, 256, 0, st>>>(n, L.nsplit, grad ? 1 : 0, rs.fpart, scale, fl.with_q ? q : nullptr,
+    k_kfield_reduce<<<(n + 255) / 256, 256, 0, st>>>(n, nsplit_f, grad ? 1 : 0, rs.fpart, scale, fl.with_q ? q : nullptr,
                                                     fl.with_mu ? mu : nullptr, fl.field ? ef : nullptr, efg,
                                                     fl.forces ? fo : nullptr, low ? rs.low.fpart : nullptr,
                                                     low ? LK_SPLIT : 0);

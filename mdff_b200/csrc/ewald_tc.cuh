@@ -319,3 +319,383 @@ __global__ void __launch_bounds__(THREADS, 1)
 
 }  // namespace tcs
 }  // namespace mdff
+
+// ===========================================================================
+// Field pass on the tensor cores (mixed path).
+//
+// With a[c, nz] = A_k S(k) on the FP32 set and the same factorisation,
+//   sum_k k Im(conj(a_k) e^{i k.r_i}) = sum_c [kc Im(W F0) + b3 Im(W F1)],
+//   sum_k k k^T Re(conj(a_k) e^{i k.r_i})
+//       = sum_c [kc kc^T Re(W F0) + (kc b3^T + b3 kc^T) Re(W F1) + b3 b3^T Re(W F2)],
+// W = X_i[nx] Y_i[ny], kc = nx b1 + ny b2 (b_j = 2 pi (column j of B)),
+//   F_j[i, c] = sum_nz Z_i[nz] nz^j conj(a[c, nz])          (j = 0, 1 [, 2]).
+// F is a complex GEMM: M = 128 atoms per CTA, K = (nz, re/im), N = (column,
+// moment, re/im) in blocks of 16 columns (8 with the field gradient).  As in
+// the structure factor the operands are 24-bit fixed point in three int8
+// digits with exact S32 accumulation; A (Z of the tile's atoms) is a digit
+// image built per position update, B (nz^j conj(a)) is quantised per
+// evaluation with one scale per (column, moment).  The contraction over
+// columns runs in the epilogue (8 warps: each atom's row is split over two
+// warps by column halves) from the accumulators in tensor memory, double
+// buffered so the MMAs of the next column block overlap it; FP32 sums are
+// flushed to FP64 after every block.
+namespace mdff {
+namespace tcf {
+
+constexpr int EPW = 8;                   // epilogue warps
+constexpr int THREADS = 32 * (EPW + 2);  // + MMA warp + copy warp
+constexpr int NBS = 3;                   // B stages
+constexpr int LVL = 64;                  // tensor-memory columns per digit level
+constexpr int BUFC = 3 * LVL;            // per accumulator buffer (two buffers)
+constexpr int NCONST = 16;               // floats of per-column constants
+constexpr uint32_t WAIT_LIMIT = 1u << 22;
+
+template <int NMOM>
+struct Cfg {
+    static constexpr int CB = NMOM == 2 ? 16 : 8;   // columns per block
+    static constexpr int NB = CB * NMOM * 2;        // GEMM N per block
+    static constexpr int HC = CB / 2;               // columns per epilogue warp
+};
+
+struct FLayout {
+    int KZ, XYW, NB, CB;
+    uint32_t a_off, xy_off, b_off, stage_bytes, img_bytes;
+    __host__ __device__ static uint32_t up128(uint32_t x) { return (x + 127u) & ~127u; }
+    __host__ __device__ FLayout(int KZ_, int XYW_, int NB_, int CB_) : KZ(KZ_), XYW(XYW_), NB(NB_), CB(CB_) {
+        a_off = 0;
+        xy_off = up128(3u * 128u * KZ);
+        b_off = up128(xy_off + (uint32_t)XYW * 128u * 8u);
+        img_bytes = 3u * NB * KZ + (uint32_t)CB * NCONST * 4u;   // B digits + per-column constants
+        stage_bytes = up128(img_bytes);
+    }
+    __host__ __device__ uint32_t a_bytes() const { return 3u * 128u * KZ; }
+    __host__ __device__ uint32_t xy_bytes() const { return (uint32_t)XYW * 128u * 8u; }
+    __host__ __device__ uint32_t smem_bytes() const { return b_off + NBS * stage_bytes + 128u; }
+};
+
+// Per position update: the A digit image of each 128-atom tile, rows = atoms,
+// K = (nz row m, re/im) of Z_i[nz]; KZ bytes per row (zero past 2 nzl).
+__global__ void k_tcf_aimage(int n, int ntile, const uint32_t* __restrict__ fx, int kz, int nzl, int KZ,
+                             uint8_t* __restrict__ img) {
+    const int nch = KZ / 16;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ntile * 128 * nch) return;
+    const int kc = (int)(t % nch);
+    const int a = (int)(t / nch);
+    const int tile = a / 128, r = a % 128;
+    float v[16];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int m = 8 * kc + u;
+        double zs = 0.0, zc = 0.0;
+        if (a < n && m < nzl) {
+            const uint32_t ph = (uint32_t)(m - kz) * fx[2 * n + a];
+            sincospi((double)(int)ph * 4.656612873077393e-10, &zs, &zc);
+        }
+        v[2 * u] = (float)(zc * (double)umma::QS);
+        v[2 * u + 1] = (float)(zs * (double)umma::QS);
+    }
+    uint32_t s1[4], s2[4], s3[4];
+#pragma unroll
+    for (int g = 0; g < 4; ++g)
+        umma::slices4(umma::digits24(__float2int_rn(v[4 * g])), umma::digits24(__float2int_rn(v[4 * g + 1])),
+                      umma::digits24(__float2int_rn(v[4 * g + 2])), umma::digits24(__float2int_rn(v[4 * g + 3])),
+                      s1[g], s2[g], s3[g]);
+    uint8_t* base = img + (size_t)tile * 3 * 128 * KZ;
+    const uint32_t off = (uint32_t)kc * (16 * 128) + (uint32_t)(r >> 3) * 128 + (r & 7) * 16;
+    *reinterpret_cast<uint4*>(base + off) = make_uint4(s1[0], s1[1], s1[2], s1[3]);
+    *reinterpret_cast<uint4*>(base + 128 * KZ + off) = make_uint4(s2[0], s2[1], s2[2], s2[3]);
+    *reinterpret_cast<uint4*>(base + 2 * 128 * KZ + off) = make_uint4(s3[0], s3[1], s3[2], s3[3]);
+}
+
+// Per position update: X/Y tables of each tile transposed to [tile][entry][128].
+__global__ void k_tcf_xyt(int npad, int ntile, const float2* __restrict__ xy, int XYW, float2* __restrict__ xyt) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ntile * 128 * XYW) return;
+    const int r = (int)(t % 128);
+    const long te = t / 128;
+    const int e = (int)(te % XYW), tile = (int)(te / XYW);
+    const int a = tile * 128 + r;
+    xyt[t] = a < npad ? xy[(size_t)a * XYW + e] : make_float2(0.f, 0.f);
+}
+
+// Per evaluation: the B digit image and per-column constants of each column
+// block.  Block = one column block, thread = (GEMM row n, 16-byte K chunk).
+// Constants per column: kc s0 (3), s1, kc_d kc_e s0 (00 11 22 01 02 12),
+// kc s1 (3), s2, X entry, Y entry; s_j = (scale of moment j) 2^16 / QS^2.
+template <int NMOM>
+__global__ void k_tcf_bimage(int nsph, const int* __restrict__ cols, int kx, int ky, int kz, int nzl, int KZ,
+                             const double* __restrict__ aks, int nrect, CellP c, uint8_t* __restrict__ img) {
+    using C = Cfg<NMOM>;
+    const int nch = KZ / 16;
+    const FLayout L(KZ, 0, C::NB, C::CB);
+    __shared__ unsigned smax[C::CB * NMOM];
+    const int q = blockIdx.x, t = threadIdx.x;
+    if (t < C::CB * NMOM) smax[t] = 0u;
+    __syncthreads();
+    const int n = t / nch, kc = t % nch;
+    const int cl = n / (2 * NMOM), j = (n >> 1) % NMOM, part = n & 1;
+    const int li = q * C::CB + cl;
+    const int col = li < nsph ? cols[li] : -1;
+    double br[8], bi[8];   // nz^j conj(a) over the chunk's 8 rows
+    float mx = 0.f;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int m = 8 * kc + u;
+        br[u] = 0.0; bi[u] = 0.0;
+        if (col >= 0 && m < nzl) {
+            const double w = j == 0 ? 1.0 : (j == 1 ? (double)(m - kz) : (double)(m - kz) * (double)(m - kz));
+            const size_t r = (size_t)col * nzl + m;
+            br[u] = w * aks[r];
+            bi[u] = -w * aks[nrect + r];
+        }
+        mx = fmaxf(mx, (float)fmax(fabs(br[u]), fabs(bi[u])));
+    }
+    if (t < nch * C::NB) atomicMax(&smax[cl * NMOM + j], __float_as_uint(mx * 1.0000002f));
+    __syncthreads();
+    uint8_t* base = img + (size_t)q * L.stage_bytes;
+    if (t < nch * C::NB) {
+        const float sg = __uint_as_float(smax[cl * NMOM + j]);
+        const double qsc = sg > 0.f ? (double)umma::QS / (double)sg : 0.0;
+        float v[16];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            // part re: (Re B, -Im B); part im: (Im B, Re B)
+            v[2 * u] = (float)((part ? bi[u] : br[u]) * qsc);
+            v[2 * u + 1] = (float)((part ? br[u] : -bi[u]) * qsc);
+        }
+        uint32_t s1[4], s2[4], s3[4];
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+            umma::slices4(umma::digits24(__float2int_rn(v[4 * g])), umma::digits24(__float2int_rn(v[4 * g + 1])),
+                          umma::digits24(__float2int_rn(v[4 * g + 2])), umma::digits24(__float2int_rn(v[4 * g + 3])),
+                          s1[g], s2[g], s3[g]);
+        const uint32_t lbo = (uint32_t)(C::NB / 8) * 128;
+        const uint32_t off = (uint32_t)kc * lbo + (uint32_t)(n >> 3) * 128 + (n & 7) * 16;
+        *reinterpret_cast<uint4*>(base + off) = make_uint4(s1[0], s1[1], s1[2], s1[3]);
+        *reinterpret_cast<uint4*>(base + C::NB * KZ + off) = make_uint4(s2[0], s2[1], s2[2], s2[3]);
+        *reinterpret_cast<uint4*>(base + 2 * C::NB * KZ + off) = make_uint4(s3[0], s3[1], s3[2], s3[3]);
+    }
+    if (t < C::CB) {
+        float* k = reinterpret_cast<float*>(base + 3 * C::NB * KZ) + t * NCONST;
+        const int li2 = q * C::CB + t;
+        const int col2 = li2 < nsph ? cols[li2] : -1;
+        float cv[NCONST];
+#pragma unroll
+        for (int e = 0; e < NCONST; ++e) cv[e] = 0.f;
+        if (col2 >= 0) {
+            const int ny_n = 2 * ky + 1;
+            const int nx = col2 / ny_n, ny = col2 % ny_n - ky;
+            const double w = 65536.0 / ((double)umma::QS * (double)umma::QS);
+            double s[3];
+            for (int jj = 0; jj < 3; ++jj) s[jj] = jj < NMOM ? (double)__uint_as_float(smax[t * NMOM + jj]) * w : 0.0;
+            double kc3[3];
+            for (int d = 0; d < 3; ++d) kc3[d] = 2.0 * PI * (nx * c.B[3 * d] + ny * c.B[3 * d + 1]);
+            cv[0] = (float)(kc3[0] * s[0]); cv[1] = (float)(kc3[1] * s[0]); cv[2] = (float)(kc3[2] * s[0]);
+            cv[3] = (float)s[1];
+            cv[4] = (float)(kc3[0] * kc3[0] * s[0]); cv[5] = (float)(kc3[1] * kc3[1] * s[0]);
+            cv[6] = (float)(kc3[2] * kc3[2] * s[0]); cv[7] = (float)(kc3[0] * kc3[1] * s[0]);
+            cv[8] = (float)(kc3[0] * kc3[2] * s[0]); cv[9] = (float)(kc3[1] * kc3[2] * s[0]);
+            cv[10] = (float)(kc3[0] * s[1]); cv[11] = (float)(kc3[1] * s[1]); cv[12] = (float)(kc3[2] * s[1]);
+            cv[13] = (float)s[2];
+            cv[14] = __int_as_float(nx);
+            cv[15] = __int_as_float(kx + 1 + ny + ky);
+        }
+#pragma unroll
+        for (int e = 0; e < NCONST; ++e) k[e] = cv[e];
+    }
+}
+
+__device__ __forceinline__ bool f_wait(uint64_t* b, uint32_t parity, int* err, int code, volatile int* abort_) {
+    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+        if (umma::mbar_test(b, parity)) return true;
+        if (*abort_) return false;
+        if (it > 32) __nanosleep(64);
+    }
+    atomicOr(err, code);
+    *abort_ = 1;
+    return false;
+}
+
+// exact digit-level sums -> FP32: (D0 2^8 + D1) 2^8 + D2 (the common 2^16 and
+// the column scale live in the per-column constants)
+__device__ __forceinline__ float comb3(float d0, float d1, float d2) {
+    const int t = __float_as_int(d0) * 256 + __float_as_int(d1);
+    return fmaf((float)t, 256.f, (float)__float_as_int(d2));
+}
+
+// grid = 128-atom tiles; THREADS threads; dynamic shared memory FLayout::smem_bytes().
+// Writes fpart[(half * nv + component) * n + i] for the two column halves
+// (nv = 3, or 9 with the field gradient).
+template <int NMOM>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_kfield_tc(int n, int ncb, const uint8_t* __restrict__ aimg, const float2* __restrict__ xyt,
+                const uint8_t* __restrict__ bimg, int KZ, int XYW, CellP c, double* __restrict__ fpart,
+                int* __restrict__ err) {
+    using C = Cfg<NMOM>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t ares, bfull[NBS], bempty[NBS], accfull[2], accfree[2], fin;
+    __shared__ uint32_t tslot;
+    __shared__ volatile int abort_;
+    const FLayout L(KZ, XYW, C::NB, C::CB);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tile = blockIdx.x;
+    if (tid == 0) {
+        umma::mbar_init(&ares, 1);
+        for (int b = 0; b < NBS; ++b) {
+            umma::mbar_init(&bfull[b], 1);
+            umma::mbar_init(&bempty[b], 1 + EPW);
+        }
+        for (int b = 0; b < 2; ++b) {
+            umma::mbar_init(&accfull[b], 1);
+            umma::mbar_init(&accfree[b], EPW);
+        }
+        umma::mbar_init(&fin, 1);
+        abort_ = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) umma::tmem_alloc(&tslot, 512);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t sbase = umma::smem_u32(smem);
+
+    if (warp == EPW + 1) {
+        // ---- copies: the tile's A image and X/Y table, then the B stages
+        if (lane == 0) {
+            umma::mbar_arrive_expect_tx(&ares, L.a_bytes() + L.xy_bytes());
+            umma::bulk_g2s(smem + L.a_off, aimg + (size_t)tile * L.a_bytes(), L.a_bytes(), &ares);
+            umma::bulk_g2s(smem + L.xy_off, xyt + (size_t)tile * XYW * 128, L.xy_bytes(), &ares);
+            for (int q = 0; q < ncb; ++q) {
+                const int bs = q % NBS;
+                if (q >= NBS && !f_wait(&bempty[bs], ((q / NBS) - 1) & 1, err, 1, &abort_)) break;
+                umma::mbar_arrive_expect_tx(&bfull[bs], L.img_bytes);
+                umma::bulk_g2s(smem + L.b_off + bs * L.stage_bytes, bimg + (size_t)q * L.stage_bytes, L.img_bytes,
+                               &bfull[bs]);
+            }
+        }
+    } else if (warp == EPW) {
+        // ---- MMA issue: per column block KZ/32 K-steps x 6 digit products
+        if (lane == 0) {
+            const uint32_t idesc = umma::idesc_s8(128, C::NB);
+            const uint32_t lboA = 16 * 128, lboB = (uint32_t)(C::NB / 8) * 128;
+            if (f_wait(&ares, 0, err, 2, &abort_)) {
+                for (int q = 0; q < ncb; ++q) {
+                    const int bs = q % NBS, tb = q & 1;
+                    if (!f_wait(&bfull[bs], (q / NBS) & 1, err, 4, &abort_)) break;
+                    if (q >= 2 && !f_wait(&accfree[tb], ((q >> 1) - 1) & 1, err, 8, &abort_)) break;
+                    umma::fence_after_sync();
+                    const uint32_t a0 = sbase + L.a_off, b0 = sbase + L.b_off + bs * L.stage_bytes;
+                    for (int ks = 0; ks < KZ / 32; ++ks) {
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int j = 0; j < 3 - i; ++j) {
+                                const int lvl = i + j;
+                                const uint64_t ad = umma::desc_kmajor(a0 + i * 128 * KZ + 2 * ks * lboA, lboA, 128);
+                                const uint64_t bd =
+                                    umma::desc_kmajor(b0 + j * C::NB * KZ + 2 * ks * lboB, lboB, 128);
+                                const uint32_t acc = (ks > 0 || (lvl == 1 && i == 1) || (lvl == 2 && i > 0)) ? 1u : 0u;
+                                umma::mma_s8(tmem + tb * BUFC + lvl * LVL, ad, bd, idesc, acc);
+                            }
+                    }
+                    umma::commit(&accfull[tb]);
+                    umma::commit(&bempty[bs]);
+                }
+            }
+            umma::commit(&fin);
+        }
+    } else {
+        // ---- epilogue: atom row = 32 (warp % 4) + lane, column half = warp / 4
+        const int qd = warp & 3, half = warp >> 2;
+        const int r = 32 * qd + lane;
+        const int i = tile * 128 + r;
+        const float2* sxy = reinterpret_cast<const float2*>(smem + L.xy_off);
+        double E[3] = {0, 0, 0}, G[6] = {0, 0, 0, 0, 0, 0}, H[3] = {0, 0, 0}, SI1 = 0, SR2 = 0;
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * qd) << 16);
+        constexpr int WN = C::HC * NMOM * 2;   // accumulator columns per warp per level (32 or 24)
+        bool ok = f_wait(&ares, 0, err, 16, &abort_);
+        for (int q = 0; q < ncb && ok; ++q) {
+            const int bs = q % NBS, tb = q & 1;
+            if (!f_wait(&accfull[tb], (q >> 1) & 1, err, 32, &abort_)) break;
+            umma::fence_after_sync();
+            float d[3][WN];
+#pragma unroll
+            for (int lv = 0; lv < 3; ++lv) {
+                const uint32_t ta = lane_base + tb * BUFC + lv * LVL + half * WN;
+                umma::tmem_ld16(ta, d[lv]);
+                if (WN == 32) umma::tmem_ld16(ta + 16, d[lv] + 16);
+                else umma::tmem_ld8(ta + 16, d[lv] + 16);
+            }
+            umma::tmem_wait_ld();
+            umma::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) umma::mbar_arrive(&accfree[tb]);
+            const float* kcst = reinterpret_cast<const float*>(smem + L.b_off + bs * L.stage_bytes + 3 * C::NB * KZ);
+            float e0 = 0.f, e1 = 0.f, e2 = 0.f, si1 = 0.f;
+            float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, h[3] = {0.f, 0.f, 0.f}, sr2 = 0.f;
+#pragma unroll
+            for (int cc = 0; cc < C::HC; ++cc) {
+                const float* k = kcst + (half * C::HC + cc) * NCONST;
+                const float4 k0 = *reinterpret_cast<const float4*>(k);
+                const int ex = __float_as_int(k[14]), ey = __float_as_int(k[15]);
+                const float2 X = sxy[ex * 128 + r], Y = sxy[ey * 128 + r];
+                const float wr = fmaf(X.x, Y.x, -X.y * Y.y), wi = fmaf(X.x, Y.y, X.y * Y.x);
+                const int o = cc * NMOM * 2;
+                const float f0r = comb3(d[0][o], d[1][o], d[2][o]), f0i = comb3(d[0][o + 1], d[1][o + 1], d[2][o + 1]);
+                const float f1r = comb3(d[0][o + 2], d[1][o + 2], d[2][o + 2]);
+                const float f1i = comb3(d[0][o + 3], d[1][o + 3], d[2][o + 3]);
+                const float i0 = fmaf(wr, f0i, wi * f0r), i1 = fmaf(wr, f1i, wi * f1r);
+                e0 = fmaf(k0.x, i0, e0);
+                e1 = fmaf(k0.y, i0, e1);
+                e2 = fmaf(k0.z, i0, e2);
+                si1 = fmaf(k0.w, i1, si1);
+                if (NMOM == 3) {
+                    const float f2r = comb3(d[0][o + 4], d[1][o + 4], d[2][o + 4]);
+                    const float f2i = comb3(d[0][o + 5], d[1][o + 5], d[2][o + 5]);
+                    const float r0 = fmaf(wr, f0r, -wi * f0i), r1 = fmaf(wr, f1r, -wi * f1i);
+                    const float r2 = fmaf(wr, f2r, -wi * f2i);
+                    const float4 k1 = *reinterpret_cast<const float4*>(k + 4);
+                    const float4 k2 = *reinterpret_cast<const float4*>(k + 8);
+                    const float4 k3 = *reinterpret_cast<const float4*>(k + 12);
+                    g[0] = fmaf(k1.x, r0, g[0]); g[1] = fmaf(k1.y, r0, g[1]); g[2] = fmaf(k1.z, r0, g[2]);
+                    g[3] = fmaf(k1.w, r0, g[3]); g[4] = fmaf(k2.x, r0, g[4]); g[5] = fmaf(k2.y, r0, g[5]);
+                    h[0] = fmaf(k2.z, r1, h[0]); h[1] = fmaf(k2.w, r1, h[1]); h[2] = fmaf(k3.x, r1, h[2]);
+                    sr2 = fmaf(k3.y, r2, sr2);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) umma::mbar_arrive(&bempty[bs]);
+            E[0] += e0; E[1] += e1; E[2] += e2; SI1 += si1;
+            if (NMOM == 3) {
+                for (int e = 0; e < 6; ++e) G[e] += g[e];
+                for (int e = 0; e < 3; ++e) H[e] += h[e];
+                SR2 += sr2;
+            }
+        }
+        if (i < n && !abort_) {
+            const double b3[3] = {2.0 * PI * c.B[2], 2.0 * PI * c.B[5], 2.0 * PI * c.B[8]};
+            const int nv = NMOM == 3 ? 9 : 3;
+            double* o = fpart + (size_t)half * nv * n;
+            for (int dd = 0; dd < 3; ++dd) o[(size_t)dd * n + i] = E[dd] + b3[dd] * SI1;
+            if (NMOM == 3) {
+                const int pd[6] = {0, 1, 2, 0, 0, 1}, pe[6] = {0, 1, 2, 1, 2, 2};
+                for (int e = 0; e < 6; ++e)
+                    o[(size_t)(3 + e) * n + i] =
+                        G[e] + b3[pe[e]] * H[pd[e]] + b3[pd[e]] * H[pe[e]] + b3[pd[e]] * b3[pe[e]] * SR2;
+            }
+        }
+    }
+    // every MMA has completed before the tensor memory is released
+    if (warp == 0) f_wait(&fin, 0, err, 64, &abort_);
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tmem, 512);
+    }
+}
+
+}  // namespace tcf
+}  // namespace mdff

@@ -23,7 +23,7 @@
 // Operands.  B (Z and i (nz/kz) Z) depends on the positions only: its digit
 // image is built once per position update in exactly the shared-memory
 // layout of a stage and streamed in by plain bulk copies.  A is generated per
-// evaluation by eight producer warps from per-atom tables X, Y (FP32, built
+// evaluation by sixteen producer warps from per-atom tables X, Y (FP32, built
 // per position update from the exact fixed-point phase in FP64) and the
 // per-atom source parameters.  One thread issues the MMAs.  Each CTA covers
 // one 128-column tile and one contiguous range of atoms; its accumulators are
@@ -36,12 +36,12 @@ namespace tcs {
 
 constexpr int SA = 16;                 // atoms per pipeline stage
 constexpr int KB = 4 * SA;             // K bytes per operand row per stage
-constexpr int NBUF = 3;                // pipeline depth
-constexpr int NPW = 8;                 // producer warps
-constexpr int THREADS = 32 * (NPW + 1);
+constexpr int NBUF = 4;                // pipeline depth
+constexpr int NPW = 16;                // producer warps (row x 4-atom chunk per thread)
+constexpr int THREADS = 32 * (NPW + 2);   // + MMA warp + copy warp
 constexpr int LSTRIDE = 160;           // tensor-memory columns per digit level (N <= 160)
 constexpr int A_SLICE = 128 * KB;      // bytes of one A digit slice per stage
-constexpr uint32_t WAIT_LIMIT = 1u << 22;
+constexpr uint64_t WAIT_NS = 200000000ull;   // 0.2 s: a pipeline wait longer than this is an error
 
 struct Layout {
     int N, XYW;
@@ -142,9 +142,10 @@ __global__ void k_tc_params(int n, int npad, const double* __restrict__ q, const
     amax[a] = (float)fmax(fabs(qa) + kx * fabs(m1) + ky * fabs(m2), kz * fabs(m3));
 }
 
-__device__ __forceinline__ bool tc_wait(uint64_t* b, uint32_t parity, int* err, int code) {
-    if (umma::mbar_wait(b, parity, WAIT_LIMIT)) return true;
-    atomicOr(err, code);
+__device__ __forceinline__ bool tc_wait(uint64_t* b, uint32_t parity, int* err, int code, volatile int* stop) {
+    if (umma::mbar_wait_ns(b, parity, WAIT_NS, stop)) return true;
+    if (!*stop) atomicOr(err, code);
+    *stop = 1;
     return false;
 }
 
@@ -158,6 +159,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     __shared__ __align__(8) uint64_t full[NBUF], aready[NBUF], empty[NBUF], done;
     __shared__ uint32_t tslot;
     __shared__ float red[THREADS / 32];
+    __shared__ volatile int stop;
     const Layout L(N, XYW);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tile = blockIdx.x, split = blockIdx.y;
@@ -176,6 +178,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             umma::mbar_init(&empty[b], 1);
         }
         umma::mbar_init(&done, 1);
+        stop = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) umma::tmem_alloc(&tslot, 512);
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t sbase = umma::smem_u32(smem);
 
     if (warp < NPW) {
-        // ---- producers: row r of the A tile, atoms [8h, 8h + 8) of each stage
+        // ---- producers: row r of the A tile, atoms [4h, 4h + 4) of each stage
         const int r = tid & 127, h = tid >> 7;
         const int li = tile * 128 + r;
         const int col = li < nsph ? cols[li] : -1;
@@ -199,35 +202,17 @@ __global__ void __launch_bounds__(THREADS, 1)
         const float rinv = col >= 0 ? inv : 0.f;
         const float fnx = (float)nx * rinv, fny = (float)ny * rinv, gk = (float)kz * rinv;
         const int ex = nx, ey = kx + 1 + ny + ky;
-        bool ok = true;
-        for (int s = 0; s < nst && ok; ++s) {
+        for (int s = 0; s < nst; ++s) {
             const int b = s % NBUF;
-            if (tid == 0 && s == 0) {
-                const int blk = blk0;
-                umma::mbar_arrive_expect_tx(&full[0], L.b_bytes() + SA * XYW * 8u + SA * 16u);
-                umma::bulk_g2s(smem + L.b_off, bimg + (size_t)blk * L.b_bytes(), L.b_bytes(), &full[0]);
-                umma::bulk_g2s(smem + L.xy_off, xy + (size_t)blk * SA * XYW, SA * XYW * 8u, &full[0]);
-                umma::bulk_g2s(smem + L.p_off, prm + (size_t)blk * SA, SA * 16u, &full[0]);
-            }
-            if (tid == 0 && s + 1 < nst) {
-                const int bn = (s + 1) % NBUF, blk = blk0 + s + 1;
-                if (s + 1 >= NBUF && !tc_wait(&empty[bn], ((s + 1) / NBUF - 1) & 1, err, 1)) ok = false;
-                uint8_t* bb = smem + bn * L.buf_bytes;
-                umma::mbar_arrive_expect_tx(&full[bn], L.b_bytes() + SA * XYW * 8u + SA * 16u);
-                umma::bulk_g2s(bb + L.b_off, bimg + (size_t)blk * L.b_bytes(), L.b_bytes(), &full[bn]);
-                umma::bulk_g2s(bb + L.xy_off, xy + (size_t)blk * SA * XYW, SA * XYW * 8u, &full[bn]);
-                umma::bulk_g2s(bb + L.p_off, prm + (size_t)blk * SA, SA * 16u, &full[bn]);
-            }
-            if (!tc_wait(&full[b], (s / NBUF) & 1, err, 2)) { ok = false; break; }
+            if (!tc_wait(&full[b], (s / NBUF) & 1, err, 2, &stop)) break;
             uint8_t* bb = smem + b * L.buf_bytes;
             const float2* sxy = reinterpret_cast<const float2*>(bb + L.xy_off);
             const float4* sp = reinterpret_cast<const float4*>(bb + L.p_off);
-#pragma unroll
-            for (int g = 0; g < 2; ++g) {          // two groups of 4 atoms = one 16-byte chunk each
+            {                                      // 4 atoms = one 16-byte chunk per slice
                 uint32_t w1[4], w2[4], w3[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    const int al = 8 * h + 4 * g + u;
+                    const int al = 4 * h + u;
                     const float2 X = sxy[al * XYW + ex], Y = sxy[al * XYW + ey];
                     const float4 P = sp[al];
                     const float xr = fmaf(X.x, Y.x, -X.y * Y.y), xi = fmaf(X.x, Y.y, X.y * Y.x);
@@ -238,7 +223,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                                   umma::digits24(__float2int_rn(a1r)), umma::digits24(__float2int_rn(a1i)), w1[u],
                                   w2[u], w3[u]);
                 }
-                const int kc = 2 * h + g;          // core-matrix column (16 K bytes)
+                const int kc = h;                  // core-matrix column (16 K bytes)
                 const uint32_t off = (uint32_t)kc * (16 * 128) + (uint32_t)(r >> 3) * 128 + (r & 7) * 16;
                 *reinterpret_cast<uint4*>(bb + L.a_off + off) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
                 *reinterpret_cast<uint4*>(bb + L.a_off + A_SLICE + off) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
@@ -248,6 +233,21 @@ __global__ void __launch_bounds__(THREADS, 1)
             __syncwarp();
             if (lane == 0) umma::mbar_arrive(&aready[b]);
         }
+    } else if (warp == NPW + 1) {
+        // ---- copies: B digit image, X/Y tables and parameters of each stage,
+        // as far ahead as the buffers allow
+        if (lane == 0) {
+            const uint32_t bytes = L.b_bytes() + SA * XYW * 8u + SA * 16u;
+            for (int s = 0; s < nst; ++s) {
+                const int b = s % NBUF, blk = blk0 + s;
+                if (s >= NBUF && !tc_wait(&empty[b], ((s / NBUF) - 1) & 1, err, 1, &stop)) break;
+                uint8_t* bb = smem + b * L.buf_bytes;
+                umma::mbar_arrive_expect_tx(&full[b], bytes);
+                umma::bulk_g2s(bb + L.b_off, bimg + (size_t)blk * L.b_bytes(), L.b_bytes(), &full[b]);
+                umma::bulk_g2s(bb + L.xy_off, xy + (size_t)blk * SA * XYW, SA * XYW * 8u, &full[b]);
+                umma::bulk_g2s(bb + L.p_off, prm + (size_t)blk * SA, SA * 16u, &full[b]);
+            }
+        }
     } else if (lane == 0) {
         // ---- MMA issue: per stage 2 K-steps of 32 x 6 digit products
         const uint32_t idesc = umma::idesc_s8(128, N);
@@ -255,8 +255,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         uint32_t started = 0;
         for (int s = 0; s < nst; ++s) {
             const int b = s % NBUF;
-            if (!tc_wait(&full[b], (s / NBUF) & 1, err, 4)) break;
-            if (!tc_wait(&aready[b], (s / NBUF) & 1, err, 8)) break;
+            if (!tc_wait(&full[b], (s / NBUF) & 1, err, 4, &stop)) break;
+            if (!tc_wait(&aready[b], (s / NBUF) & 1, err, 8, &stop)) break;
             umma::fence_after_sync();
             const uint32_t a0 = sbase + b * L.buf_bytes + L.a_off, b0 = sbase + b * L.buf_bytes + L.b_off;
 #pragma unroll
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     // ---- epilogue: warps 0-3 (tensor-memory lane quarters 0-3), row = lane
     if (warp < 4) {
-        const bool ok = nst == 0 || tc_wait(&done, 0, err, 16);
+        const bool ok = nst == 0 || tc_wait(&done, 0, err, 16, &stop);
         umma::fence_after_sync();
         const int r = tid;
         const int li = tile * 128 + r;
@@ -348,7 +348,7 @@ constexpr int NBS = 3;                   // B stages
 constexpr int LVL = 64;                  // tensor-memory columns per digit level
 constexpr int BUFC = 3 * LVL;            // per accumulator buffer (two buffers)
 constexpr int NCONST = 16;               // floats of per-column constants
-constexpr uint32_t WAIT_LIMIT = 1u << 22;
+constexpr uint64_t WAIT_NS = 200000000ull;
 
 template <int NMOM>
 struct Cfg {
@@ -507,12 +507,8 @@ __global__ void k_tcf_bimage(int nsph, const int* __restrict__ cols, int kx, int
 }
 
 __device__ __forceinline__ bool f_wait(uint64_t* b, uint32_t parity, int* err, int code, volatile int* abort_) {
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
-        if (umma::mbar_test(b, parity)) return true;
-        if (*abort_) return false;
-        if (it > 32) __nanosleep(64);
-    }
-    atomicOr(err, code);
+    if (umma::mbar_wait_ns(b, parity, WAIT_NS, abort_)) return true;
+    if (!*abort_) atomicOr(err, code);
     *abort_ = 1;
     return false;
 }

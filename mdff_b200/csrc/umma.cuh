@@ -153,6 +153,35 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint32_t
     }
     return false;
 }
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// try_wait suspends the warp in hardware until the phase completes or a
+// short system-defined limit passes, so waiting costs almost no issue slots
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Bounded wait by elapsed time: false once `limit_ns` has passed (or *stop
+// became nonzero) without the phase completing.
+__device__ __forceinline__ bool mbar_wait_ns(uint64_t* b, uint32_t parity, uint64_t limit_ns,
+                                             const volatile int* stop = nullptr) {
+    if (mbar_try(b, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (!mbar_try(b, parity)) {
+        if (stop && *stop) return false;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    }
+    return true;
+}
 
 // Two FP32 values as one BF16 pair (round to nearest): e0 in the low half
 // (lower address, even K index), e1 in the high half.

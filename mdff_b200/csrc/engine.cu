@@ -91,6 +91,12 @@ struct mdff_ctx {
     bool rec_acc_ready = false;   // rs.aks_acc holds A_k S of the charges + final dipoles
     long long kinfo[4] = {0, 0, 0, 0};   // rectangle, half space, FP32 set, FP64 low set
     int g_dir = 16, g_dd = 16;           // lanes per atom of the real-space Ewald kernels (autotuned)
+    // mixed path: per-step pair table of the dipole-dipole operator (A1, B2 per
+    // Coulomb list entry), written by the charge pass of each force evaluation
+    float2* ddtab = nullptr;
+    size_t ddtab_cap = 0;                // entries allocated
+    long ddtab_epoch = -1;               // position epoch it was written for
+    int ddtab_lcap = 0;                  // list capacity it was written with
     bool tuned = false;
     Prof prof;
 };
@@ -436,8 +442,12 @@ void dd_field_real(mdff_ctx* ctx, const double* m, double* out) {
     ctx->prof.begin(PK_DIR);
     if (ctx->p.precision == MDFF_PREC_MIXED) {
         const int k = 1 + ensure_phase_tables(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->rs);
-        launch_ewald_dd32(ctx->st, n, ctx->rs.fixed, m, ctx->cell, coul_list(ctx), ctx->cut_coul * ctx->cut_coul,
-                          ctx->alphaES, out, ctx->g_dd);
+        const NList& L = coul_list(ctx);
+        if (ctx->ddtab_epoch == ctx->rs.want_epoch && ctx->ddtab_lcap == L.cap)
+            launch_ewald_ddtab(ctx->st, n, ctx->rs.fixed, m, ctx->cell, L, ctx->ddtab, out, ctx->g_dd);
+        else
+            launch_ewald_dd32(ctx->st, n, ctx->rs.fixed, m, ctx->cell, L, ctx->cut_coul * ctx->cut_coul,
+                              ctx->alphaES, out, ctx->g_dd);
         ctx->prof.end(k);
         return;
     }
@@ -461,6 +471,26 @@ int induced_field(mdff_ctx* ctx, const double* m, double* out) {
     return check_launch(ctx, "induced_field");
 }
 
+// On the mixed path, let this charge pass also write the dipole-dipole pair
+// table for the solver's operator (allocated for the current list capacity).
+int arm_ddtab(mdff_ctx* ctx, DirFlags& f) {
+    if (ctx->p.precision != MDFF_PREC_MIXED) return MDFF_OK;
+    const NList& L = coul_list(ctx);
+    const size_t need = (size_t)ctx->n * L.cap;
+    if (need > ctx->ddtab_cap) {
+        if (ctx->ddtab) CK(cudaFree(ctx->ddtab));
+        ctx->ddtab = nullptr;
+        ctx->ddtab_cap = 0;
+        cudaError_t e = cudaMalloc(&ctx->ddtab, sizeof(float2) * need);
+        if (e != cudaSuccess) return fail(ctx, MDFF_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        ctx->ddtab_cap = need;
+    }
+    f.ddtab = ctx->ddtab;
+    ctx->ddtab_epoch = ctx->rs.want_epoch;
+    ctx->ddtab_lcap = L.cap;
+    return MDFF_OK;
+}
+
 // Static field of the charges (and static dipoles), damped
 // (src/field.f90:3270-3272).
 int static_field(mdff_ctx* ctx) {
@@ -471,6 +501,7 @@ int static_field(mdff_ctx* ctx) {
     f.dd = ctx->any_dip0 ? 1 : 0;
     f.damp = 1;
     f.field = 1;
+    TRY(arm_ddtab(ctx, f));
     ctx->prof.begin(PK_DIR);
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->dip0, ctx->cell, coul_list(ctx),
                      ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, ctx->g_dir);
@@ -497,6 +528,7 @@ int fused_initial_field(mdff_ctx* ctx) {
     f.dd = ctx->any_dip0 ? 1 : 0;
     f.damp = 1;
     f.field = 1;
+    TRY(arm_ddtab(ctx, f));
     ctx->prof.begin(PK_DIR);
     launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->dip0, ctx->cell, coul_list(ctx),
                      ctx->pc, f, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, ctx->g_dir);
@@ -703,9 +735,17 @@ int autotune(mdff_ctx* ctx) {
     }, gs, 3);
     if (ctx->p.precision == MDFF_PREC_MIXED) {
         ensure_phase_tables(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->rs);
+        // the pair table of this step, then the lanes per atom of its operator
+        DirFlags fs = dir_flags(ctx);
+        fs.qq = 1;
+        fs.damp = 1;
+        fs.field = 1;
+        TRY(arm_ddtab(ctx, fs));
+        launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->mu, ctx->cell, coul_list(ctx),
+                         ctx->pc, fs, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, ctx->g_dir);
         ctx->g_dd = pick([&](int g) {
-            launch_ewald_dd32(ctx->st, n, ctx->rs.fixed, ctx->mu, ctx->cell, coul_list(ctx),
-                              ctx->cut_coul * ctx->cut_coul, ctx->alphaES, ctx->Eind, g);
+            launch_ewald_ddtab(ctx->st, n, ctx->rs.fixed, ctx->mu, ctx->cell, coul_list(ctx), ctx->ddtab, ctx->Eind,
+                               g);
         }, gs, 3);
         const int muls[3] = {1, 2, 4};
         RecFlags sf{1, 1, 0, 0, 0, 0, MDFF_PREC_MIXED, 0};   // structure factor only
@@ -1165,6 +1205,7 @@ void mdff_destroy(mdff_ctx* ctx) {
         cudaStreamSynchronize(ctx->st);
         ctx->prof.release();
         free_all(ctx);
+        if (ctx->ddtab) cudaFree(ctx->ddtab);
         cudaStreamDestroy(ctx->st);
     }
     if (ctx->hsc) cudaFreeHost(ctx->hsc);

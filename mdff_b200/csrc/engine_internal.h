@@ -174,6 +174,8 @@ struct DirFlags {
     double alpha;          // Ewald alpha
     double cutsq;          // verlet_coul%cut^2
     int erfc_ref;          // use the reference's fitted erfc
+    float2* ddtab;         // optional output (charge pass): per list entry (A1, B2) of the
+                           // undamped dipole-dipole tensor in FP32, zero beyond the cutoff
 };
 void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const int* type, const double* q, const double* mu, CellP c, const NList& l,
@@ -265,6 +267,8 @@ void launch_aks_accumulate(cudaStream_t st, const KGrid& kg, RecScratch& rs, con
 int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs);
 void launch_ewald_dd32(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
                        double cutsq, double alpha, double* ef, int g = 16);
+void launch_ewald_ddtab(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
+                        const float2* tab, double* ef, int g = 16);
 
 // Solver vector kernels.
 void launch_dot(cudaStream_t st, int n3, const double* a, const double* b, Partials& part, double* out);

@@ -47,7 +47,10 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
             const int j = row[k];
             double rx, ry, rz;
             const double d2 = pairvec_exact(c, si1, si2, si3, sx[j], sy[j], sz[j], rx, ry, rz);
-            if (d2 > fl.cutsq) continue;
+            if (d2 > fl.cutsq) {
+                if (MODE == 0 && fl.ddtab) fl.ddtab[(size_t)i * cap + k] = make_float2(0.f, 0.f);
+                continue;
+            }
             const double mj0 = mu[j], mj1 = mu[n + j], mj2 = mu[2 * n + j];
             const double d = sqrt(d2);
             const double dm1 = 1.0 / d, dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2, dm7 = dm5 * dm2;
@@ -58,6 +61,7 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
             const double A1 = F1 * dm3;
             const double B2 = 3.0 * F2 * dm5;
             const double rmj = rx * mj0 + ry * mj1 + rz * mj2;
+            if (MODE == 0 && fl.ddtab) fl.ddtab[(size_t)i * cap + k] = make_float2((float)A1, (float)B2);
             if (MODE == 1) {
                 E[0] += rx * rmj * B2 - mj0 * A1;
                 E[1] += ry * rmj * B2 - mj1 * A1;
@@ -224,6 +228,61 @@ __global__ void __launch_bounds__(256) k_ewald_dd32(int n, const uint32_t* __res
     E1 = group_sum<G>(E1);
     E2 = group_sum<G>(E2);
     if (active && sub == 0) { ef[i] = E0; ef[n + i] = E1; ef[2 * n + i] = E2; }
+}
+
+// The same operator from the per-step pair table written by the charge pass
+// (A1 = F1/r^3, B2 = 3 F2/r^5 per list entry, FP64 rounded to FP32, zero
+// beyond the cutoff): no special functions per iteration, r from the exact
+// fixed-point difference, so the operator stays symmetric.
+template <int G>
+__global__ void __launch_bounds__(256) k_ewald_ddtab(int n, const uint32_t* __restrict__ fx,
+                                                     const double* __restrict__ mu, CellP c,
+                                                     const int* __restrict__ nbr, const int* __restrict__ cnt, int cap,
+                                                     const float2* __restrict__ tab, double* __restrict__ ef) {
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int sub = threadIdx.x & (G - 1);
+    const bool active = gid < n;
+    const int i = active ? gid : 0;
+    const float sc = 2.3283064365386963e-10f;   // 2^-32
+    const float A0 = (float)c.A[0], A1 = (float)c.A[1], A2 = (float)c.A[2];
+    const float A3 = (float)c.A[3], A4 = (float)c.A[4], A5 = (float)c.A[5];
+    const float A6 = (float)c.A[6], A7 = (float)c.A[7], A8 = (float)c.A[8];
+    double E0 = 0.0, E1 = 0.0, E2 = 0.0;
+    if (active) {
+        const uint32_t u1 = fx[i], u2 = fx[n + i], u3 = fx[2 * n + i];
+        const int m = cnt[i];
+        const int* row = nbr + (size_t)i * cap;
+        const float2* trow = tab + (size_t)i * cap;
+        for (int k = sub; k < m; k += G) {
+            const int j = row[k];
+            const float2 t = trow[k];
+            const float d0 = (float)(int)(u1 - fx[j]) * sc;
+            const float d1 = (float)(int)(u2 - fx[n + j]) * sc;
+            const float d2 = (float)(int)(u3 - fx[2 * n + j]) * sc;
+            const float rx = fmaf(d0, A0, fmaf(d1, A1, d2 * A2));
+            const float ry = fmaf(d0, A3, fmaf(d1, A4, d2 * A5));
+            const float rz = fmaf(d0, A6, fmaf(d1, A7, d2 * A8));
+            const float mj0 = (float)mu[j], mj1 = (float)mu[n + j], mj2 = (float)mu[2 * n + j];
+            const float rb = fmaf(rx, mj0, fmaf(ry, mj1, rz * mj2)) * t.y;
+            E0 += (double)fmaf(rx, rb, -mj0 * t.x);
+            E1 += (double)fmaf(ry, rb, -mj1 * t.x);
+            E2 += (double)fmaf(rz, rb, -mj2 * t.x);
+        }
+    }
+    E0 = group_sum<G>(E0);
+    E1 = group_sum<G>(E1);
+    E2 = group_sum<G>(E2);
+    if (active && sub == 0) { ef[i] = E0; ef[n + i] = E1; ef[2 * n + i] = E2; }
+}
+
+void launch_ewald_ddtab(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
+                        const float2* tab, double* ef, int g) {
+    const int blocks = (int)(((size_t)n * g + 255) / 256);
+#define DDT(G) k_ewald_ddtab<G><<<blocks, 256, 0, st>>>(n, fx, mu, c, l.nbr, l.cnt, l.cap, tab, ef)
+    if (g == 8) DDT(8);
+    else if (g == 32) DDT(32);
+    else DDT(16);
+#undef DDT
 }
 
 // g: lanes per atom (8, 16 or 32; the autotuner's choice).

@@ -94,6 +94,9 @@ struct mdff_ctx {
     // mixed path: per-step pair table of the dipole-dipole operator (A1, B2 per
     // Coulomb list entry), written by the charge pass of each force evaluation
     float2* ddtab = nullptr;
+    int* ddnbr = nullptr;
+    int* ddcnt = nullptr;
+    uint4* ddrec = nullptr;              // [2n] gather records of the operator
     size_t ddtab_cap = 0;                // entries allocated
     long ddtab_epoch = -1;               // position epoch it was written for
     int ddtab_lcap = 0;                  // list capacity it was written with
@@ -444,7 +447,8 @@ void dd_field_real(mdff_ctx* ctx, const double* m, double* out) {
         const int k = 1 + ensure_phase_tables(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->rs);
         const NList& L = coul_list(ctx);
         if (ctx->ddtab_epoch == ctx->rs.want_epoch && ctx->ddtab_lcap == L.cap)
-            launch_ewald_ddtab(ctx->st, n, ctx->rs.fixed, m, ctx->cell, L, ctx->ddtab, out, ctx->g_dd);
+            launch_ewald_ddtab(ctx->st, n, ctx->rs.fixed, m, ctx->cell, ctx->ddnbr, ctx->ddcnt, L.cap, ctx->ddtab,
+                               ctx->ddrec, out, ctx->g_dd);
         else
             launch_ewald_dd32(ctx->st, n, ctx->rs.fixed, m, ctx->cell, L, ctx->cut_coul * ctx->cut_coul,
                               ctx->alphaES, out, ctx->g_dd);
@@ -479,13 +483,20 @@ int arm_ddtab(mdff_ctx* ctx, DirFlags& f) {
     const size_t need = (size_t)ctx->n * L.cap;
     if (need > ctx->ddtab_cap) {
         if (ctx->ddtab) CK(cudaFree(ctx->ddtab));
+        if (ctx->ddnbr) CK(cudaFree(ctx->ddnbr));
         ctx->ddtab = nullptr;
+        ctx->ddnbr = nullptr;
         ctx->ddtab_cap = 0;
         cudaError_t e = cudaMalloc(&ctx->ddtab, sizeof(float2) * need);
+        if (e == cudaSuccess) e = cudaMalloc(&ctx->ddnbr, sizeof(int) * need);
         if (e != cudaSuccess) return fail(ctx, MDFF_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
         ctx->ddtab_cap = need;
     }
+    if (!ctx->ddcnt) TRY(dalloc(ctx, &ctx->ddcnt, ctx->n));
+    if (!ctx->ddrec) TRY(dalloc(ctx, &ctx->ddrec, 2 * (size_t)ctx->n));
     f.ddtab = ctx->ddtab;
+    f.ddnbr = ctx->ddnbr;
+    f.ddcnt = ctx->ddcnt;
     ctx->ddtab_epoch = ctx->rs.want_epoch;
     ctx->ddtab_lcap = L.cap;
     return MDFF_OK;
@@ -744,8 +755,8 @@ int autotune(mdff_ctx* ctx) {
         launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->mu, ctx->cell, coul_list(ctx),
                          ctx->pc, fs, ctx->Estat, nullptr, nullptr, ctx->part, ctx->dsc, ctx->g_dir);
         ctx->g_dd = pick([&](int g) {
-            launch_ewald_ddtab(ctx->st, n, ctx->rs.fixed, ctx->mu, ctx->cell, coul_list(ctx), ctx->ddtab, ctx->Eind,
-                               g);
+            launch_ewald_ddtab(ctx->st, n, ctx->rs.fixed, ctx->mu, ctx->cell, ctx->ddnbr, ctx->ddcnt,
+                               coul_list(ctx).cap, ctx->ddtab, ctx->ddrec, ctx->Eind, g);
         }, gs, 3);
         const int muls[3] = {1, 2, 4};
         RecFlags sf{1, 1, 0, 0, 0, 0, MDFF_PREC_MIXED, 0};   // structure factor only
@@ -1206,6 +1217,7 @@ void mdff_destroy(mdff_ctx* ctx) {
         ctx->prof.release();
         free_all(ctx);
         if (ctx->ddtab) cudaFree(ctx->ddtab);
+        if (ctx->ddnbr) cudaFree(ctx->ddnbr);
         cudaStreamDestroy(ctx->st);
     }
     if (ctx->hsc) cudaFreeHost(ctx->hsc);

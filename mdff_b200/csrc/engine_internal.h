@@ -174,8 +174,12 @@ struct DirFlags {
     double alpha;          // Ewald alpha
     double cutsq;          // verlet_coul%cut^2
     int erfc_ref;          // use the reference's fitted erfc
-    float2* ddtab;         // optional output (charge pass): per list entry (A1, B2) of the
-                           // undamped dipole-dipole tensor in FP32, zero beyond the cutoff
+    // optional output of the charge pass: the Coulomb list compacted to the
+    // entries inside the cutoff (ddnbr, ddcnt) with the undamped
+    // dipole-dipole radial factors (A1, B2) of each entry in FP32 (ddtab)
+    float2* ddtab;
+    int* ddnbr;
+    int* ddcnt;
 };
 void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz,
                       const int* type, const double* q, const double* mu, CellP c, const NList& l,
@@ -267,8 +271,10 @@ void launch_aks_accumulate(cudaStream_t st, const KGrid& kg, RecScratch& rs, con
 int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs);
 void launch_ewald_dd32(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
                        double cutsq, double alpha, double* ef, int g = 16);
-void launch_ewald_ddtab(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
-                        const float2* tab, double* ef, int g = 16);
+// The solver's real-space dipole operator from the charge pass's pair table;
+// rec is per-atom scratch of 8 words (fixed-point coordinates, FP32 dipole).
+void launch_ewald_ddtab(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const int* nbr,
+                        const int* cnt, int cap, const float2* tab, uint4* rec, double* ef, int g = 16);
 
 // Solver vector kernels.
 void launch_dot(cudaStream_t st, int n3, const double* a, const double* b, Partials& part, double* out);

@@ -43,14 +43,25 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
         const double mi0 = mu[i], mi1 = mu[n + i], mi2 = mu[2 * n + i];
         const int m = cnt[i];
         const int* row = nbr + (size_t)i * cap;
-        for (int k = sub; k < m; k += G) {
-            const int j = row[k];
-            double rx, ry, rz;
-            const double d2 = pairvec_exact(c, si1, si2, si3, sx[j], sy[j], sz[j], rx, ry, rz);
-            if (d2 > fl.cutsq) {
-                if (MODE == 0 && fl.ddtab) fl.ddtab[(size_t)i * cap + k] = make_float2(0.f, 0.f);
-                continue;
+        // pair table: the lanes of the group compact the entries inside the
+        // cutoff in list order (a ballot per sweep of G entries)
+        const int g0 = (threadIdx.x & 31) & ~(G - 1);
+        const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << g0);
+        int cbase = 0, pos = 0;
+        for (int k0 = 0; k0 < m; k0 += G) {
+            const int k = k0 + sub;
+            const bool valid = k < m;
+            const int j = valid ? row[k] : i;
+            double rx = 0.0, ry = 0.0, rz = 0.0, d2 = 0.0;
+            if (valid) d2 = pairvec_exact(c, si1, si2, si3, sx[j], sy[j], sz[j], rx, ry, rz);
+            const bool in = valid && d2 <= fl.cutsq;
+            if (MODE == 0 && fl.ddtab) {
+                const unsigned bal = (__ballot_sync(gmask, in) & gmask) >> g0;
+                pos = cbase + __popc(bal & ((1u << sub) - 1u));
+                if (in) fl.ddnbr[(size_t)i * cap + pos] = j;
+                cbase += __popc(bal);
             }
+            if (!in) continue;
             const double mj0 = mu[j], mj1 = mu[n + j], mj2 = mu[2 * n + j];
             const double d = sqrt(d2);
             const double dm1 = 1.0 / d, dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2, dm7 = dm5 * dm2;
@@ -61,7 +72,7 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
             const double A1 = F1 * dm3;
             const double B2 = 3.0 * F2 * dm5;
             const double rmj = rx * mj0 + ry * mj1 + rz * mj2;
-            if (MODE == 0 && fl.ddtab) fl.ddtab[(size_t)i * cap + k] = make_float2((float)A1, (float)B2);
+            if (MODE == 0 && fl.ddtab) fl.ddtab[(size_t)i * cap + pos] = make_float2((float)A1, (float)B2);
             if (MODE == 1) {
                 E[0] += rx * rmj * B2 - mj0 * A1;
                 E[1] += ry * rmj * B2 - mj1 * A1;
@@ -148,6 +159,7 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
                 S[3] += rx * fi1 + ry * fi0; S[4] += rx * fi2 + rz * fi0; S[5] += ry * fi2 + rz * fi1;
             }
         }
+        if (MODE == 0 && fl.ddtab && sub == 0) fl.ddcnt[i] = cbase;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) E[k] = group_sum<G>(E[k]);
@@ -230,13 +242,24 @@ __global__ void __launch_bounds__(256) k_ewald_dd32(int n, const uint32_t* __res
     if (active && sub == 0) { ef[i] = E0; ef[n + i] = E1; ef[2 * n + i] = E2; }
 }
 
-// The same operator from the per-step pair table written by the charge pass
-// (A1 = F1/r^3, B2 = 3 F2/r^5 per list entry, FP64 rounded to FP32, zero
-// beyond the cutoff): no special functions per iteration, r from the exact
-// fixed-point difference, so the operator stays symmetric.
+// The same operator from the per-step pair table written by the charge pass:
+// the Coulomb list compacted to the entries inside the cutoff, with
+// A1 = F1/r^3 and B2 = 3 F2/r^5 per entry (FP64 rounded to FP32), so no
+// special functions per iteration.  Each neighbour is one 32-byte gather of
+// its record (fixed-point coordinates, FP32 dipole); r comes from the exact
+// fixed-point difference, so the operator stays symmetric.  Two entries per
+// lane are in flight per sweep.
+__global__ void k_dd_records(int n, const uint32_t* __restrict__ fx, const double* __restrict__ mu,
+                             uint4* __restrict__ rec) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    rec[2 * i] = make_uint4(fx[i], fx[n + i], fx[2 * n + i], 0u);
+    rec[2 * i + 1] = make_uint4(__float_as_uint((float)mu[i]), __float_as_uint((float)mu[n + i]),
+                                __float_as_uint((float)mu[2 * n + i]), 0u);
+}
+
 template <int G>
-__global__ void __launch_bounds__(256) k_ewald_ddtab(int n, const uint32_t* __restrict__ fx,
-                                                     const double* __restrict__ mu, CellP c,
+__global__ void __launch_bounds__(256) k_ewald_ddtab(int n, const uint4* __restrict__ rec, CellP c,
                                                      const int* __restrict__ nbr, const int* __restrict__ cnt, int cap,
                                                      const float2* __restrict__ tab, double* __restrict__ ef) {
     const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -249,24 +272,34 @@ __global__ void __launch_bounds__(256) k_ewald_ddtab(int n, const uint32_t* __re
     const float A6 = (float)c.A[6], A7 = (float)c.A[7], A8 = (float)c.A[8];
     double E0 = 0.0, E1 = 0.0, E2 = 0.0;
     if (active) {
-        const uint32_t u1 = fx[i], u2 = fx[n + i], u3 = fx[2 * n + i];
+        const uint4 ri = rec[2 * i];
         const int m = cnt[i];
         const int* row = nbr + (size_t)i * cap;
         const float2* trow = tab + (size_t)i * cap;
-        for (int k = sub; k < m; k += G) {
-            const int j = row[k];
-            const float2 t = trow[k];
-            const float d0 = (float)(int)(u1 - fx[j]) * sc;
-            const float d1 = (float)(int)(u2 - fx[n + j]) * sc;
-            const float d2 = (float)(int)(u3 - fx[2 * n + j]) * sc;
+        auto term = [&](float2 t, const uint4& p, const uint4& q) {
+            const float d0 = (float)(int)(ri.x - p.x) * sc;
+            const float d1 = (float)(int)(ri.y - p.y) * sc;
+            const float d2 = (float)(int)(ri.z - p.z) * sc;
             const float rx = fmaf(d0, A0, fmaf(d1, A1, d2 * A2));
             const float ry = fmaf(d0, A3, fmaf(d1, A4, d2 * A5));
             const float rz = fmaf(d0, A6, fmaf(d1, A7, d2 * A8));
-            const float mj0 = (float)mu[j], mj1 = (float)mu[n + j], mj2 = (float)mu[2 * n + j];
+            const float mj0 = __uint_as_float(q.x), mj1 = __uint_as_float(q.y), mj2 = __uint_as_float(q.z);
             const float rb = fmaf(rx, mj0, fmaf(ry, mj1, rz * mj2)) * t.y;
             E0 += (double)fmaf(rx, rb, -mj0 * t.x);
             E1 += (double)fmaf(ry, rb, -mj1 * t.x);
             E2 += (double)fmaf(rz, rb, -mj2 * t.x);
+        };
+        int k = sub;
+        for (; k + G < m; k += 2 * G) {
+            const int ja = row[k], jb = row[k + G];
+            const float2 ta = trow[k], tb = trow[k + G];
+            const uint4 pa = rec[2 * ja], qa = rec[2 * ja + 1], pb = rec[2 * jb], qb = rec[2 * jb + 1];
+            term(ta, pa, qa);
+            term(tb, pb, qb);
+        }
+        if (k < m) {
+            const int ja = row[k];
+            term(trow[k], rec[2 * ja], rec[2 * ja + 1]);
         }
     }
     E0 = group_sum<G>(E0);
@@ -275,10 +308,11 @@ __global__ void __launch_bounds__(256) k_ewald_ddtab(int n, const uint32_t* __re
     if (active && sub == 0) { ef[i] = E0; ef[n + i] = E1; ef[2 * n + i] = E2; }
 }
 
-void launch_ewald_ddtab(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const NList& l,
-                        const float2* tab, double* ef, int g) {
+void launch_ewald_ddtab(cudaStream_t st, int n, const uint32_t* fx, const double* mu, CellP c, const int* nbr,
+                        const int* cnt, int cap, const float2* tab, uint4* rec, double* ef, int g) {
+    k_dd_records<<<(n + 255) / 256, 256, 0, st>>>(n, fx, mu, rec);
     const int blocks = (int)(((size_t)n * g + 255) / 256);
-#define DDT(G) k_ewald_ddtab<G><<<blocks, 256, 0, st>>>(n, fx, mu, c, l.nbr, l.cnt, l.cap, tab, ef)
+#define DDT(G) k_ewald_ddtab<G><<<blocks, 256, 0, st>>>(n, rec, c, nbr, cnt, cap, tab, ef)
     if (g == 8) DDT(8);
     else if (g == 32) DDT(32);
     else DDT(16);

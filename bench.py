@@ -203,6 +203,7 @@ def run_engine(args):
     torch.cuda.synchronize(device)
     ms = ev0.elapsed_time(ev1)
     prof = eng.profile()
+    det = eng.profile_detail()
     ms_max = max_over_ranks(ms, dist, device)
     value = whole_job_rate(natm * args.steps, ms / 1e3, dist, device)
     iters = [t["scf_iter"] for t in out["thermo"]]
@@ -252,9 +253,50 @@ def run_engine(args):
         sf_flops = natm * nk_eff * 15.0 * n_sf * args.steps
         kf_flops = natm * nk_eff * (18.0 * n_e + 36.0) * args.steps
         k_ms = ksf["ms"] + kkf["ms"]
-        achieved = (sf_flops + kf_flops) / (k_ms / 1e3) / 1e12 if k_ms > 0 else None
-        peak = pipes[1] if args.precision == "mixed" else pipes[0]
         total_ms = sum(v["ms"] for v in kern.values())
+        tc_ms = det["sfac_tc"]["ms"] + det["kfield_tc"]["ms"]
+        if args.precision == "mixed" and det["sfac_tc"]["count"] > 0:
+            # dominant kernels: the tensor-core structure factor and field,
+            # timed alone (CUDA events around each launch); achieved = the int8
+            # digit-product operations of the unpadded GEMMs / their time
+            tens = mdff_b200.measure_tensor(local)
+            ops = det["sfac_tc"]["ops"] + det["kfield_tc"]["ops"]
+            achieved = ops / (tc_ms / 1e3) / 1e12
+            per = {}
+            for k, v in det.items():
+                if v["count"]:
+                    per[k] = {"launches": v["count"], "ms_per_launch": v["ms"] / v["count"],
+                              "tops": v["ops"] / (v["ms"] / 1e3) / 1e12}
+            roof = {
+                "bound": "tensor",
+                "kernels": "k_sfac_tc + k_kfield_tc (tcgen05 kind::i8 digit GEMMs of the reciprocal sum)",
+                "achieved": achieved,
+                "peak": tens[0],
+                "unit": "TOPS (int8, dense)",
+                "frac": achieved / tens[0],
+                "peak_source": "measured tcgen05 kind::i8 throughput on this GPU (mdff_measure_tensor): "
+                               "N=256 %.0f, N=96 %.0f, N=64 %.0f TOPS" % tuple(tens),
+                "per_kernel": per,
+                "share_of_step": tc_ms / total_ms if total_ms else None,
+                # algorithmic FP32-equivalent rate of the k-space sum these two kernels perform
+                "kspace_fp32_equiv_tflops": (sf_flops + kf_flops) / (tc_ms / 1e3) / 1e12,
+                "traffic": None,
+            }
+        else:
+            achieved = (sf_flops + kf_flops) / (k_ms / 1e3) / 1e12 if k_ms > 0 else None
+            peak = pipes[1] if args.precision == "mixed" else pipes[0]
+            roof = {
+                "bound": "fp32" if args.precision == "mixed" else "fp64",
+                "kernels": "k-space structure factor + field (k_sfac*, k_kfield*)",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / peak if achieved and peak else None,
+                "peak_source": "measured FMA throughput on this GPU (mdff_measure_pipes): fp64 %.1f, fp32 %.1f, "
+                               "fp32x2 %.1f TFLOP/s" % tuple(pipes),
+                "share_of_step": k_ms / total_ms if total_ms else None,
+                "traffic": None,
+            }
         result = {
             "metric": METRIC,
             "value": value,
@@ -277,24 +319,14 @@ def run_engine(args):
                        "mixed_keps": p.mixed_keps if args.precision == "mixed" else None,
                        "kspace_tc": int(p.kspace_tc) if args.precision == "mixed" else None,
                        "precision": args.precision, "parallelism": f"replicas{world}",
-                       "l2": "per-step working set > 126 MB L2 (k-space partials, Verlet lists)"},
+                       "l2": "per-step working set > 126 MB L2 (Verlet and pair-table lists, k-space digit "
+                             "images, partials)"},
             "gpu_launches": int(prof["_launches"]["count"]),
             "launch_shape": eng.launch_shape(),
             "solver_iters_mean": mean_it,
             "h_tot_drift_per_step": (h[-1] - h[0]) / max(1, len(h) - 1) / natm,
             "kernels_ms": {k: round(v["ms"], 3) for k, v in kern.items()},
-            "roofline": {
-                "bound": "fp32" if args.precision == "mixed" else "fp64",
-                "kernels": "k-space structure factor + field (k_sfac*, k_kfield*)",
-                "achieved": achieved,
-                "peak": peak,
-                "unit": "TFLOP/s",
-                "frac": achieved / peak if achieved and peak else None,
-                "peak_source": "measured FMA throughput on this GPU (mdff_measure_pipes): fp64 %.1f, fp32 %.1f, fp32x2 %.1f TFLOP/s"
-                               % tuple(pipes),
-                "share_of_step": k_ms / total_ms if total_ms else None,
-                "traffic": None,
-            },
+            "roofline": roof,
             "e2e": e2e,
             "step0": {"h_tot": t0["h_tot"], "temp_r": t0["temp_r"], "scf_iter": t0["scf_iter"]},
         }

@@ -202,6 +202,12 @@ int  mdff_struct_size(int which);
  * the engine's FMA-bound kernels; no reference counterpart. */
 int  mdff_measure_pipes(int device, double out[3]);
 
+/* Measured tcgen05 kind::i8 tensor-core throughput of the device in TOPS
+ * (dense, S32 accumulate, operands resident in shared memory): out[0] with
+ * N = 256 (the peak), out[1] N = 96 and out[2] N = 64 (the tile widths of the
+ * structure-factor and field GEMMs).  No reference counterpart. */
+int  mdff_measure_tensor(int device, double out[3]);
+
 /* Fill p with the reference defaults (control_default_tag, src/control.f90:199-243;
  * field_default_tag, src/field.f90:192-273; md_default_tag, src/md.f90:178-205). */
 void mdff_params_default(mdff_params* p);
@@ -232,6 +238,12 @@ int  mdff_stream(mdff_ctx* ctx, void** stream);
  * clears them when reset != 0. */
 int  mdff_profile(mdff_ctx* ctx, int enable);
 int  mdff_profile_get(mdff_ctx* ctx, double ms[8], long long count[8], long long* launches, int reset);
+/* Detail timers inside groups 3 and 4 (mixed path, tensor-core k-space): the
+ * structure-factor kernel [0] and the field kernel [1] alone -- accumulated
+ * milliseconds, launches, and the int8 digit-product operations (2 M N K per
+ * product, six products, unpadded problem) they were launched for; cleared
+ * with the groups.  No reference counterpart. */
+int  mdff_profile_detail(mdff_ctx* ctx, double ms[2], long long count[2], double ops[2]);
 
 /* Sizes of the reciprocal-space sums of the context (no reference
  * counterpart): out[0] the k rectangle the kernels sweep, out[1] the k-vectors

@@ -62,6 +62,8 @@ def lib():
         L.mdff_profile.argtypes = [vp, C.c_int]
         L.mdff_profile_get.argtypes = [vp, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int]
         L.mdff_measure_pipes.argtypes = [C.c_int, dp]
+        L.mdff_measure_tensor.argtypes = [C.c_int, dp]
+        L.mdff_profile_detail.argtypes = [vp, dp, C.POINTER(C.c_longlong), dp]
         L.mdff_struct_size.argtypes = [C.c_int]
         L.mdff_kspace_info.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.mdff_launch_shape.argtypes = [vp, C.POINTER(C.c_int)]
@@ -88,6 +90,15 @@ def _ip(a):
 
 
 PROFILE_GROUPS = ("nlist", "pair", "dir", "sfac", "kfield", "solver", "integrate", "other")
+
+
+def measure_tensor(device=0):
+    """Measured tcgen05 kind::i8 throughput (TOPS, dense): (N=256 peak, N=96, N=64)."""
+    out = np.zeros(3)
+    rc = lib().mdff_measure_tensor(int(device), _dp(out))
+    if rc != 0:
+        raise EngineError(rc, "mdff_measure_tensor failed")
+    return tuple(float(x) for x in out)
 
 
 def measure_pipes(device=0):
@@ -189,6 +200,15 @@ class Engine:
 
     def profile_reset(self):
         self.profile(reset=True)
+
+    def profile_detail(self):
+        """The tensor-core k-space kernels alone (mixed path): per kernel the
+        accumulated ms, launches and int8 digit-product operations."""
+        ms, ops = np.zeros(2), np.zeros(2)
+        cnt = (C.c_longlong * 2)()
+        self._check(lib().mdff_profile_detail(self._h, _dp(ms), cnt, _dp(ops)))
+        return {k: {"ms": float(ms[i]), "count": int(cnt[i]), "ops": float(ops[i])}
+                for i, k in enumerate(("sfac_tc", "kfield_tc"))}
 
     def nlist_build(self):
         self._check(lib().mdff_nlist_build(self._h))

@@ -1089,6 +1089,61 @@ int mdff_measure_pipes(int device, double out[3]) {
     return MDFF_OK;
 }
 
+int mdff_measure_tensor(int device, double out[3]) {
+    if (!out) return MDFF_E_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return MDFF_E_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    int* err = nullptr;
+    if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return MDFF_E_NOMEM;
+    cudaMemset(err, 0, sizeof(int));
+    const int niter = 4096;
+    cudaFuncSetAttribute(k_peak_i8<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (128 + 256) * 64);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int ns[3] = {256, 96, 64};
+    double best[3] = {0, 0, 0};
+    for (int rep = 0; rep < 3; ++rep)
+        for (int k = 0; k < 3; ++k) {
+            const int N = ns[k];
+            const size_t smem = (size_t)(128 + N) * 64;
+            cudaEventRecord(a);
+            if (N == 256) k_peak_i8<256><<<sms, 128, smem>>>(niter, err);
+            else if (N == 96) k_peak_i8<96><<<sms, 128, smem>>>(niter, err);
+            else k_peak_i8<64><<<sms, 128, smem>>>(niter, err);
+            cudaEventRecord(b);
+            cudaEventSynchronize(b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            const double ops = 2.0 * 128 * N * 64 * (double)niter * sms;
+            const double tops = ops / (ms * 1e-3) / 1e12;
+            if (rep > 0 && tops > best[k]) best[k] = tops;
+        }
+    int herr = 0;
+    cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(err);
+    if (e != cudaSuccess || herr) return MDFF_E_CUDA;
+    for (int k = 0; k < 3; ++k) out[k] = best[k];
+    return MDFF_OK;
+}
+
+int mdff_profile_detail(mdff_ctx* ctx, double ms[2], long long count[2], double ops[2]) {
+    if (!ctx) return MDFF_E_ARG;
+    cudaSetDevice(ctx->p.device);
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->prof.harvest();
+    for (int k = 0; k < PD_NDETAIL; ++k) {
+        if (ms) ms[k] = ctx->prof.dms[k];
+        if (count) count[k] = ctx->prof.dcount[k];
+        if (ops) ops[k] = ctx->prof.dops[k];
+    }
+    return MDFF_OK;
+}
+
 int mdff_profile(mdff_ctx* ctx, int enable) {
     if (!ctx) return MDFF_E_ARG;
     ctx->prof.on = enable != 0;

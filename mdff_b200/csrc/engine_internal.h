@@ -46,16 +46,35 @@ struct PairConst {
 // counterpart of the reference's MPI_WTIME accumulators, src/time.f90:35-73)
 // and a count of kernel launches.
 enum ProfKind { PK_NLIST = 0, PK_PAIR, PK_DIR, PK_SFAC, PK_KFIELD, PK_SOLVER, PK_INTEGRATE, PK_OTHER, PK_NKIND };
+// Detail timers (inside the groups): the tensor-core structure factor and
+// field kernels alone, with the int8 MMA operations they were launched for.
+enum ProfDetail { PD_TC_SFAC = 0, PD_TC_FIELD, PD_NDETAIL };
 struct Prof {
     bool on = false;
     cudaStream_t st = nullptr;
-    struct Pending { int kind; cudaEvent_t a, b; };
+    struct Pending { int kind; cudaEvent_t a, b; };   // kind >= PK_NKIND: detail PK_NKIND + d
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> pool;
     double ms[PK_NKIND] = {0};
     long count[PK_NKIND] = {0};
+    double dms[PD_NDETAIL] = {0}, dops[PD_NDETAIL] = {0};
+    long dcount[PD_NDETAIL] = {0};
     long launches = 0;
     int open_kind = -1;
+    size_t open_idx = 0, detail_idx = 0;
+    void detail_begin(int d) {
+        if (!on) return;
+        Pending p{PK_NKIND + d, get(), get()};
+        cudaEventRecord(p.a, st);
+        pending.push_back(p);
+        detail_idx = pending.size() - 1;
+    }
+    void detail_end(int d, double ops) {
+        if (!on) return;
+        cudaEventRecord(pending[detail_idx].b, st);
+        dcount[d] += 1;
+        dops[d] += ops;
+    }
     cudaEvent_t get() {
         if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
         cudaEvent_t e;
@@ -68,18 +87,22 @@ struct Prof {
         cudaEventRecord(p.a, st);
         pending.push_back(p);
         open_kind = kind;
+        open_idx = pending.size() - 1;
     }
     void end(int nkernels) {
         launches += nkernels;
         if (!on || pending.empty() || open_kind < 0) return;
-        cudaEventRecord(pending.back().b, st);
-        count[pending.back().kind] += nkernels;
+        cudaEventRecord(pending[open_idx].b, st);
+        count[pending[open_idx].kind] += nkernels;
         open_kind = -1;
     }
     void harvest() {   // after the stream has been synchronised
         for (auto& p : pending) {
             float t = 0.f;
-            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ms[p.kind] += t;
+            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) {
+                if (p.kind < PK_NKIND) ms[p.kind] += t;
+                else dms[p.kind - PK_NKIND] += t;
+            }
             pool.push_back(p.a);
             pool.push_back(p.b);
         }
@@ -88,6 +111,7 @@ struct Prof {
     void reset() {
         harvest();
         for (int k = 0; k < PK_NKIND; ++k) { ms[k] = 0.0; count[k] = 0; }
+        for (int k = 0; k < PD_NDETAIL; ++k) { dms[k] = 0.0; dops[k] = 0.0; dcount[k] = 0; }
         launches = 0;
     }
     void release() {

@@ -1001,9 +1001,13 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             pim = rs.part + (size_t)t.nsplit * tplane;
             tcs::k_tc_params<<<(t.npad + 255) / 256, 256, 0, st>>>(n, t.npad, q, mu, c, fl.with_q, fl.with_mu, kx, ky,
                                                                    kz, t.prm, t.amax);
+            // int8 digit-product operations of the unpadded GEMM: 6 products of
+            // 2 M N K, M = sphere columns, N = 2 nz rows, K = 4 per atom
+            prof->detail_begin(PD_TC_SFAC);
             tcs::k_sfac_tc<<<dim3(t.ntile, t.nsplit), tcs::THREADS, t.smem, st>>>(
                 t.nblk, t.bps, t.bimg, t.xy, t.prm, t.amax, t.cols, t.nsph, kx, ky, kz, kg.nzl, t.N, t.XYW, kg.ncol,
                 tplane, pre, pim, &d->tc_err);
+            prof->detail_end(PD_TC_SFAC, 6.0 * 2.0 * t.nsph * (2.0 * kg.nzl) * (4.0 * n));
             Pr = t.nsplit;
             nk += 2;
         } else if (kg.nitems > 0) {
@@ -1058,15 +1062,19 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             const int ncb = (t.nsph + C3::CB - 1) / C3::CB;
             tcf::k_tcf_bimage<3><<<ncb, C3::NB * nch, 0, st>>>(t.nsph, t.cols, kx, ky, kz, kg.nzl, t.KZ, rs.aks,
                                                                 kg.nrect, c, t.fimg);
+            prof->detail_begin(PD_TC_FIELD);
             tcf::k_kfield_tc<3><<<t.ntile_f, tcf::THREADS, t.smem_f3, st>>>(n, ncb, t.aimg, t.xyt, t.fimg, t.KZ, t.XYW,
                                                                              c, rs.fpart, &d->tc_err);
+            prof->detail_end(PD_TC_FIELD, 6.0 * 2.0 * n * (6.0 * t.nsph) * (2.0 * kg.nzl));
         } else {
             using C2 = tcf::Cfg<2>;
             const int ncb = (t.nsph + C2::CB - 1) / C2::CB;
             tcf::k_tcf_bimage<2><<<ncb, C2::NB * nch, 0, st>>>(t.nsph, t.cols, kx, ky, kz, kg.nzl, t.KZ, rs.aks,
                                                                 kg.nrect, c, t.fimg);
+            prof->detail_begin(PD_TC_FIELD);
             tcf::k_kfield_tc<2><<<t.ntile_f, tcf::THREADS, t.smem_f2, st>>>(n, ncb, t.aimg, t.xyt, t.fimg, t.KZ, t.XYW,
                                                                              c, rs.fpart, &d->tc_err);
+            prof->detail_end(PD_TC_FIELD, 6.0 * 2.0 * n * (4.0 * t.nsph) * (2.0 * kg.nzl));
         }
         nsplit_f = 2;
         nk += 1;

@@ -1,10 +1,12 @@
 // peaks.cuh -- measured arithmetic-pipe throughput of the device.
 //
-// The engine's hot kernels are bound by the FP64 or FP32 FMA pipes (no
-// tensor-core contraction, working sets in L2), so their roofline denominators
-// are FMA throughputs, measured here with long chains of independent FMAs
-// (8 chains per thread, every SM filled), timed with CUDA events.
+// Roofline denominators of the engine's kernels: FMA throughputs (FP64,
+// FP32, packed FP32x2) measured with long chains of independent FMAs (every
+// SM filled), and the tcgen05 kind::i8 tensor-core throughput of the
+// reciprocal-space GEMMs, measured with back-to-back MMAs from resident
+// shared-memory operands (one CTA per SM); all timed with CUDA events.
 #include "common.cuh"
+#include "umma.cuh"
 
 namespace mdff {
 
@@ -61,6 +63,43 @@ __global__ void __launch_bounds__(256) k_peak_f32x2(float* out, float seed) {
         s += v.x + v.y;
     }
     if (s == 1234.5678f) out[0] = s;
+}
+
+// tcgen05 kind::i8 throughput: M = 128, N as given, K = 64 bytes per
+// iteration (two MMAs), accumulating into tensor memory; every wait bounded.
+template <int N>
+__global__ void __launch_bounds__(128) k_peak_i8(int niter, int* err) {
+    constexpr int KB = 64;
+    extern __shared__ __align__(128) uint8_t pk_smem[];
+    uint8_t* sm = pk_smem;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int i = tid; i < (128 + N) * KB / 4; i += 128) reinterpret_cast<uint32_t*>(sm)[i] = 0x01010101u;
+    if (warp == 0) umma::tmem_alloc(&slot, 256);
+    if (tid == 0) umma::mbar_init(&mbar, 1);
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tm = slot;
+    if (tid == 0) {
+        const uint32_t a0 = umma::smem_u32(sm), b0 = a0 + 128 * KB;
+        const uint32_t lboA = 16 * 128, lboB = (N / 8) * 128;
+        for (int r = 0; r < niter; ++r)
+            for (int s = 0; s < KB / 32; ++s)
+                umma::mma_s8(tm, umma::desc_kmajor(a0 + 2 * s * lboA, lboA, 128),
+                             umma::desc_kmajor(b0 + 2 * s * lboB, lboB, 128), umma::idesc_s8(128, N), (r | s) != 0);
+        umma::commit(&mbar);
+    }
+    __syncwarp();
+    if (!umma::mbar_wait_ns(&mbar, 0, 2000000000ull) && tid == 0) atomicOr(err, 1);
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tm, 256);
+    }
 }
 
 }  // namespace mdff

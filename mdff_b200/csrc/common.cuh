@@ -34,14 +34,42 @@ __device__ __forceinline__ double erfc_fit(double x) {
     return x < 0.0 ? 2.0 - r : r;
 }
 
+// Inverse factorials 1/m! by the recurrence inv_m = inv_{m-1} / m in IEEE
+// double, evaluated at compile time: the values a division loop produces, so
+// the damping below is bit-identical to it without a division per term.
+struct InvFact {
+    double v[17];
+    constexpr InvFact() : v() {
+        double inv = 1.0;
+        v[0] = 1.0;
+        for (int m = 1; m < 17; ++m) {
+            inv = inv / (double)m;
+            v[m] = inv;
+        }
+    }
+};
+
+// Tang-Toennies damping of order k (TT_damping_functions, src/field.f90:3775-3805):
+// f = 1 - c e^{-br} sum_{m<=k} (br)^m/m!,  f' = c b e^{-br} (br)^k / k!.
 __device__ __forceinline__ void tt_damp_d(double b, double c, double r, int k, double& f, double& fd) {
+    constexpr InvFact IF;
     const double br = b * r;
     const double e = exp(-br) * c;
     double term = 1.0, sum = 1.0, inv = 1.0;
-    for (int m = 1; m <= k; ++m) {
-        inv = inv / (double)m;
-        term = term * br;
-        sum = fma(term, inv, sum);
+    if (k <= 16) {
+#pragma unroll
+        for (int m = 1; m <= 16; ++m) {
+            if (m > k) break;
+            inv = IF.v[m];
+            term = term * br;
+            sum = fma(term, inv, sum);
+        }
+    } else {
+        for (int m = 1; m <= k; ++m) {
+            inv = inv / (double)m;
+            term = term * br;
+            sum = fma(term, inv, sum);
+        }
     }
     f = 1.0 - sum * e;
     fd = term * inv * e * b;

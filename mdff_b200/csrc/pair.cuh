@@ -11,19 +11,8 @@
 
 namespace mdff {
 
-// Tang-Toennies damping of order k (TT_damping_functions, src/field.f90:3775-3805):
-// f = 1 - c e^{-br} sum_{m<=k} (br)^m/m!,  f' = c b e^{-br} (br)^k / k!.
 __device__ __forceinline__ void tt_damp(double b, double c, double r, int k, double& f, double& fd) {
-    const double br = b * r;
-    const double e = exp(-br) * c;
-    double term = 1.0, sum = 1.0, inv = 1.0;
-    for (int m = 1; m <= k; ++m) {
-        inv = inv / (double)m;
-        term = term * br;
-        sum = fma(term, inv, sum);
-    }
-    f = 1.0 - sum * e;
-    fd = term * inv * e * b;
+    tt_damp_d(b, c, r, k, f, fd);
 }
 
 __device__ __forceinline__ double ipow_half(double x, double p) {

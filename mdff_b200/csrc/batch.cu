@@ -245,11 +245,11 @@ __device__ __forceinline__ PairG ewald_radial(double d2, double a, int erfc_ref)
     PairG g;
     const double d = sqrt(d2);
     const double dm1 = 1.0 / d, dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2, dm7 = dm5 * dm2;
-    const double expon = exp(-a2 * d2) * rsqpi;
-    const double F0 = erfc_ref ? erfc_fit(a * d) : erfc(a * d);
+    const double ex2 = exp(-a2 * d2), expon = ex2 * rsqpi;
+    const double F0 = erfc_ref ? erfc_fit(a * d) : erfc_ex2(a * d, ex2);
     const double F1 = F0 + 2.0 * a * d * expon;
-    const double F2 = F1 + 4.0 * a3 * d2 * d * expon / 3.0;
-    const double F3 = F2 + 8.0 * a5 * d2 * d2 * d * expon / 15.0;
+    const double F2 = F1 + (4.0 * a3 / 3.0) * d2 * d * expon;
+    const double F3 = F2 + (8.0 * a5 / 15.0) * d2 * d2 * d * expon;
     g.d = d;
     g.F0 = F0 * dm1;
     g.A1 = F1 * dm3;

@@ -21,7 +21,7 @@ namespace mdff {
 // MODE 1: induced-dipole field operator E_i = sum_j T2(r_ij) mu_j (no damping),
 //         the dipole-dipole field of src/field.f90:3354.
 template <int G, int MODE>
-__global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restrict__ sx, const double* __restrict__ sy,
+__global__ void __launch_bounds__(256, 2) k_ewald_dir(int n, const double* __restrict__ sx, const double* __restrict__ sy,
                                                    const double* __restrict__ sz, const int* __restrict__ type,
                                                    const double* __restrict__ q, const double* __restrict__ mu,
                                                    CellP c, const int* __restrict__ nbr, const int* __restrict__ cnt,
@@ -33,6 +33,7 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
     const bool active = gid < n;
     const int i = active ? gid : 0;
     const double a = fl.alpha, a2 = a * a, a3 = a2 * a, a5 = a3 * a2;
+    const double c43a3 = 4.0 * a3 / 3.0, c815a5 = 8.0 * a5 / 15.0;
     const double rsqpi = 0.56418958354775628695;   // 1/sqrt(pi)
     double E[3] = {0, 0, 0}, Gd[6] = {0, 0, 0, 0, 0, 0}, F[3] = {0, 0, 0};
     double u = 0.0, S[6] = {0, 0, 0, 0, 0, 0};
@@ -65,10 +66,10 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
             const double mj0 = mu[j], mj1 = mu[n + j], mj2 = mu[2 * n + j];
             const double d = sqrt(d2);
             const double dm1 = 1.0 / d, dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2, dm7 = dm5 * dm2;
-            const double expon = exp(-a2 * d2) * rsqpi;
-            const double F0 = fl.erfc_ref ? erfc_fit(a * d) : erfc(a * d);
+            const double ex2 = exp(-a2 * d2), expon = ex2 * rsqpi;
+            const double F0 = fl.erfc_ref ? erfc_fit(a * d) : erfc_ex2(a * d, ex2);
             const double F1 = F0 + 2.0 * a * d * expon;
-            const double F2 = F1 + 4.0 * a3 * d2 * d * expon / 3.0;
+            const double F2 = F1 + c43a3 * d2 * d * expon;
             const double A1 = F1 * dm3;
             const double B2 = 3.0 * F2 * dm5;
             const double rmj = rx * mj0 + ry * mj1 + rz * mj2;
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(256) k_ewald_dir(int n, const double* __restri
             const int tj = type[j];
             const double qj = q[j];
             const double rmi = rx * mi0 + ry * mi1 + rz * mi2;
-            const double F3 = F2 + 8.0 * a5 * d2 * d2 * d * expon / 15.0;
+            const double F3 = F2 + c815a5 * d2 * d2 * d * expon;
             const double C3 = 15.0 * F3 * dm7;
             // Tang-Toennies damping of the charge-dipole terms (src/field.f90:2205-2217).
             double gi = 0.0, gdi = 0.0, gj = 0.0, gdj = 0.0;

@@ -1569,7 +1569,7 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
         }
         size_t fp = 0;
         size_t pc = std::max(tc_part, rec_scratch_doubles(n, kg, &fp, p.precision == MDFF_PREC_MIXED));
-        fp = std::max(fp, (size_t)2 * 9 * n);   // the tensor-core field pass writes two halves
+        fp = std::max(fp, (size_t)tcf::NQ * 9 * n);   // the tensor-core field pass writes NQ column parts
         TRY(dalloc(ctx, &ctx->rs.part, pc));
         TRY(dalloc(ctx, &ctx->rs.fpart, fp));
         TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));

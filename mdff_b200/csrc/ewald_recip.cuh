@@ -1054,7 +1054,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     const bool grad = fl.grad || (fl.forces && fl.with_mu);
     int nsplit_f = L.nsplit;
     if (mixed && rs.tc.on) {
-        // field pass on the tensor cores: two column halves per atom
+        // field pass on the tensor cores: NQ column parts per atom
         const TcK& t = rs.tc;
         const int nch = t.KZ / 16;
         if (grad) {
@@ -1076,7 +1076,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
                                                                              c, rs.fpart, &d->tc_err);
             prof->detail_end(PD_TC_FIELD, 6.0 * 2.0 * n * (4.0 * t.nsph) * (2.0 * kg.nzl));
         }
-        nsplit_f = 2;
+        nsplit_f = tcf::NQ;
         nk += 1;
         if (low) {
             LowK& lk = rs.low;

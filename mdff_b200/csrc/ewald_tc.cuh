@@ -336,15 +336,16 @@ __global__ void __launch_bounds__(THREADS, 1)
 // image built per position update, B (nz^j conj(a)) is quantised per
 // evaluation with one scale per (column, moment).  The contraction over
 // columns runs in the epilogue (8 warps: each atom's row is split over two
-// warps by column halves) from the accumulators in tensor memory, double
+// warps by column parts) from the accumulators in tensor memory, double
 // buffered so the MMAs of the next column block overlap it; FP32 sums are
 // flushed to FP64 after every block.
 namespace mdff {
 namespace tcf {
 
-constexpr int EPW = 8;                   // epilogue warps
+constexpr int EPW = 8;                   // epilogue warps: 2 per tensor-memory lane quarter
+constexpr int NQ = EPW / 4;              // column parts per block (one per epilogue warp of a quarter)
 constexpr int THREADS = 32 * (EPW + 2);  // + MMA warp + copy warp
-constexpr int NBS = 3;                   // B stages
+constexpr int NBS = 6;                   // B stages (the epilogue holds a stage until it has read its constants)
 constexpr int LVL = 64;                  // tensor-memory columns per digit level
 constexpr int BUFC = 3 * LVL;            // per accumulator buffer (two buffers)
 constexpr int NCONST = 16;               // floats of per-column constants
@@ -354,7 +355,7 @@ template <int NMOM>
 struct Cfg {
     static constexpr int CB = NMOM == 2 ? 16 : 8;   // columns per block
     static constexpr int NB = CB * NMOM * 2;        // GEMM N per block
-    static constexpr int HC = CB / 2;               // columns per epilogue warp
+    static constexpr int HC = CB / NQ;              // columns per epilogue warp
 };
 
 struct FLayout {
@@ -521,7 +522,7 @@ __device__ __forceinline__ float comb3(float d0, float d1, float d2) {
 }
 
 // grid = 128-atom tiles; THREADS threads; dynamic shared memory FLayout::smem_bytes().
-// Writes fpart[(half * nv + component) * n + i] for the two column halves
+// Writes fpart[(part * nv + component) * n + i] for the NQ column parts
 // (nv = 3, or 9 with the field gradient).
 template <int NMOM>
 __global__ void __launch_bounds__(THREADS, 1)
@@ -603,27 +604,26 @@ __global__ void __launch_bounds__(THREADS, 1)
             umma::commit(&fin);
         }
     } else {
-        // ---- epilogue: atom row = 32 (warp % 4) + lane, column half = warp / 4
-        const int qd = warp & 3, half = warp >> 2;
+        // ---- epilogue: atom row = 32 (warp % 4) + lane, column part = warp / 4
+        const int qd = warp & 3, part = warp >> 2;
         const int r = 32 * qd + lane;
         const int i = tile * 128 + r;
         const float2* sxy = reinterpret_cast<const float2*>(smem + L.xy_off);
         double E[3] = {0, 0, 0}, G[6] = {0, 0, 0, 0, 0, 0}, H[3] = {0, 0, 0}, SI1 = 0, SR2 = 0;
         const uint32_t lane_base = tmem + ((uint32_t)(32 * qd) << 16);
         constexpr int WN = C::HC * NMOM * 2;   // accumulator columns per warp per level (32 or 24)
+        static_assert(WN <= 32 && C::HC * NQ == C::CB, "two 16-column loads per digit level at most");
         bool ok = f_wait(&ares, 0, err, 16, &abort_);
         for (int q = 0; q < ncb && ok; ++q) {
             const int bs = q % NBS, tb = q & 1;
             if (!f_wait(&accfull[tb], (q >> 1) & 1, err, 32, &abort_)) break;
             umma::fence_after_sync();
-            float d[3][WN];
+            float d[3][32];
 #pragma unroll
-            for (int lv = 0; lv < 3; ++lv) {
-                const uint32_t ta = lane_base + tb * BUFC + lv * LVL + half * WN;
-                umma::tmem_ld16(ta, d[lv]);
-                if (WN == 32) umma::tmem_ld16(ta + 16, d[lv] + 16);
-                else umma::tmem_ld8(ta + 16, d[lv] + 16);
-            }
+            for (int lv = 0; lv < 3; ++lv)
+#pragma unroll
+                for (int h = 0; h < (WN + 15) / 16; ++h)
+                    umma::tmem_ld16(lane_base + tb * BUFC + lv * LVL + part * WN + 16 * h, d[lv] + 16 * h);
             umma::tmem_wait_ld();
             umma::fence_before_sync();
             __syncwarp();
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, h[3] = {0.f, 0.f, 0.f}, sr2 = 0.f;
 #pragma unroll
             for (int cc = 0; cc < C::HC; ++cc) {
-                const float* k = kcst + (half * C::HC + cc) * NCONST;
+                const float* k = kcst + (part * C::HC + cc) * NCONST;
                 const float4 k0 = *reinterpret_cast<const float4*>(k);
                 const int ex = __float_as_int(k[14]), ey = __float_as_int(k[15]);
                 const float2 X = sxy[ex * 128 + r], Y = sxy[ey * 128 + r];
@@ -673,7 +673,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (i < n && !abort_) {
             const double b3[3] = {2.0 * PI * c.B[2], 2.0 * PI * c.B[5], 2.0 * PI * c.B[8]};
             const int nv = NMOM == 3 ? 9 : 3;
-            double* o = fpart + (size_t)half * nv * n;
+            double* o = fpart + (size_t)part * nv * n;
             for (int dd = 0; dd < 3; ++dd) o[(size_t)dd * n + i] = E[dd] + b3[dd] * SI1;
             if (NMOM == 3) {
                 const int pd[6] = {0, 1, 2, 0, 0, 1}, pe[6] = {0, 1, 2, 1, 2, 2};

@@ -182,7 +182,10 @@ def run_engine(args):
     p.kspace_tc = args.tc
     natm = len(s["itype"])
     eng = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
-    eng.enable_profile(True)
+    # the timed region runs without the per-kernel-group CUDA events (they
+    # cost ~0.7 ms of gaps per step); a separate profiled pass afterwards
+    # gives the kernel breakdown and the roofline's detail timers
+    eng.enable_profile(False)
     stream_ptr = eng.stream()
     ext = torch.cuda.ExternalStream(stream_ptr, device=device)
     t0 = eng.md_start(s["vel"])
@@ -202,8 +205,7 @@ def run_engine(args):
         ev1.synchronize()
     torch.cuda.synchronize(device)
     ms = ev0.elapsed_time(ev1)
-    prof = eng.profile()
-    det = eng.profile_detail()
+    launches = eng.profile()["_launches"]["count"]   # counted with the timers off too
     ms_max = max_over_ranks(ms, dist, device)
     value = whole_job_rate(natm * args.steps, ms / 1e3, dist, device)
     iters = [t["scf_iter"] for t in out["thermo"]]
@@ -229,6 +231,15 @@ def run_engine(args):
         t2 = time.perf_counter()
         e2e = {"value": whole_job_rate(natm * ke, t2 - t1, dist, device), "unit": "atom-steps/s", "steps": ke,
                "h2d_bytes_per_step": 6 * 8 * natm, "d2h_bytes_per_step": 9 * 8 * natm}
+    # profiled pass (not part of the timed region)
+    kp = max(2, min(args.steps, 10))
+    eng.enable_profile(True)
+    eng.profile_reset()
+    outp = eng.step(kp, thermo=True)
+    prof = eng.profile()
+    det = eng.profile_detail()
+    eng.enable_profile(False)
+    iters_p = [t["scf_iter"] for t in outp["thermo"]]
     result = None
     if rank == 0:
         pipes = mdff_b200.measure_pipes(local)
@@ -237,6 +248,7 @@ def run_engine(args):
         # the FP64 path; the FP32 set plus the FP64 low set on the mixed path
         nk_eff = (ki["fp32"] + ki["low"]) if args.precision == "mixed" else ki["half"]
         mean_it = float(np.mean(iters))
+        mean_it_p = float(np.mean(iters_p))
         kern = {k: v for k, v in prof.items() if v["count"] > 0 and not k.startswith("_")}
         ksf = kern.get("sfac", {"ms": 0.0, "count": 0})
         kkf = kern.get("kfield", {"ms": 0.0, "count": 0})
@@ -247,11 +259,11 @@ def run_engine(args):
         # kspace_reuse the static field and first residual share one
         # evaluation and the forces take no structure-factor pass.
         if p.kspace_reuse:
-            n_sf, n_e = 1 + mean_it, 1 + mean_it
+            n_sf, n_e = 1 + mean_it_p, 1 + mean_it_p
         else:
-            n_sf, n_e = 3 + mean_it, 2 + mean_it
-        sf_flops = natm * nk_eff * 15.0 * n_sf * args.steps
-        kf_flops = natm * nk_eff * (18.0 * n_e + 36.0) * args.steps
+            n_sf, n_e = 3 + mean_it_p, 2 + mean_it_p
+        sf_flops = natm * nk_eff * 15.0 * n_sf * kp
+        kf_flops = natm * nk_eff * (18.0 * n_e + 36.0) * kp
         k_ms = ksf["ms"] + kkf["ms"]
         total_ms = sum(v["ms"] for v in kern.values())
         tc_ms = det["sfac_tc"]["ms"] + det["kfield_tc"]["ms"]
@@ -321,11 +333,12 @@ def run_engine(args):
                        "precision": args.precision, "parallelism": f"replicas{world}",
                        "l2": "per-step working set > 126 MB L2 (Verlet and pair-table lists, k-space digit "
                              "images, partials)"},
-            "gpu_launches": int(prof["_launches"]["count"]),
+            "gpu_launches": int(launches),
             "launch_shape": eng.launch_shape(),
             "solver_iters_mean": mean_it,
             "h_tot_drift_per_step": (h[-1] - h[0]) / max(1, len(h) - 1) / natm,
-            "kernels_ms": {k: round(v["ms"], 3) for k, v in kern.items()},
+            "profile_steps": kp,
+            "kernels_ms_per_step": {k: round(v["ms"] / kp, 4) for k, v in kern.items()},
             "roofline": roof,
             "e2e": e2e,
             "step0": {"h_tot": t0["h_tot"], "temp_r": t0["temp_r"], "scf_iter": t0["scf_iter"]},

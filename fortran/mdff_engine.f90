@@ -106,6 +106,11 @@ module mdff_engine
     real(c_double) :: scf_rmsd
   end type mdff_thermo_t
 
+  type, bind(C) :: mdff_opt_result_t
+    real(c_double) :: u_initial, u_final, phigrad
+    integer(c_int) :: iterations, nforce, status, pad
+  end type mdff_opt_result_t
+
   interface
     subroutine mdff_params_default(p) bind(C, name="mdff_params_default")
       import :: mdff_params_t
@@ -156,6 +161,13 @@ module mdff_engine
       type(mdff_energies_t), intent(out) :: e
       real(c_double), intent(out) :: tau_nonb(9), tau_coul(9)
       real(c_double), intent(out) :: ef(*), efg(*), mu(*)
+    end function
+
+    integer(c_int) function mdff_opt_sastry(ctx, itmax, res) bind(C, name="mdff_opt_sastry")
+      import :: c_int, c_ptr, mdff_opt_result_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: itmax
+      type(mdff_opt_result_t), intent(out) :: res
     end function
 
     integer(c_int) function mdff_nlist_build(ctx) bind(C, name="mdff_nlist_build")

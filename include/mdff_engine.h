@@ -192,8 +192,21 @@ typedef struct mdff_param_grad {
     double dip_pol_damp_c[MDFF_NTYPE_MAX][MDFF_NTYPE_MAX][MDFF_NTYPE_MAX];
 } mdff_param_grad;
 
+/* Result of a structure optimisation (opt_main's per-configuration report,
+ * src/opt.f90:369-380: Eis, phigrad, iter, neng, pot0). */
+typedef struct mdff_opt_result {
+    double u_initial;   /* u_tot at the starting positions (eV), pot0 */
+    double u_final;     /* u_tot at the returned positions (eV), Eis */
+    double phigrad;     /* sum of the squared force components at the end (eV^2/A^2) */
+    int    iterations;  /* conjugate-gradient iterations (its) */
+    int    nforce;      /* force evaluations (neng) */
+    int    status;      /* 0: minimum reached (energy unchanged to ftol); 1: itmax iterations;
+                           2: zero gradient; 3: the line search made no progress in 100 steps */
+    int    pad;
+} mdff_opt_result;
+
 /* sizeof(mdff_params), sizeof(mdff_energies), sizeof(mdff_thermo),
- * sizeof(mdff_param_grad) for which = 0, 1, 2, 3 (lets a binding check its
+ * sizeof(mdff_param_grad), sizeof(mdff_opt_result) for which = 0 .. 4 (lets a binding check its
  * mirror of these structs); no reference counterpart. */
 int  mdff_struct_size(int which);
 
@@ -291,6 +304,16 @@ int  mdff_get_velocities(mdff_ctx* ctx, double* vx, double* vy, double* vz);
 int  mdff_engforce(mdff_ctx* ctx, double* fx, double* fy, double* fz,
                    mdff_energies* e, double tau_nonb[9], double tau_coul[9],
                    double* ef, double* efg, double* mu);
+
+/* Structure optimisation of the current positions by conjugate gradients
+ * with cubic line minimisation: sastry + eforce1d (src/opt.f90:452-933), the
+ * default optalgo of opt_main (src/opt.f90:251-439; epsilon, dutol, ds and
+ * the energy test with ftol = tiny(1.0_dp) as there).  Every function value
+ * is one mdff_engforce at trial positions on the lists of the starting
+ * configuration.  On return the context's positions (mdff_get_positions) and
+ * forces are those of the minimum; *out gets pot0, Eis, phigrad, iter, neng.
+ * itmax: the reference's 10000. */
+int  mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out);
 
 /* Rebuild the Verlet lists at the current positions: vnlist_pbc
  * (src/tools.f90:274-370). */

@@ -63,6 +63,7 @@ def lib():
         L.mdff_profile_get.argtypes = [vp, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int]
         L.mdff_measure_pipes.argtypes = [C.c_int, dp]
         L.mdff_measure_tensor.argtypes = [C.c_int, dp]
+        L.mdff_opt_sastry.argtypes = [vp, C.c_int, C.POINTER(abi.OptResult)]
         L.mdff_profile_detail.argtypes = [vp, dp, C.POINTER(C.c_longlong), dp]
         L.mdff_struct_size.argtypes = [C.c_int]
         L.mdff_kspace_info.argtypes = [vp, C.POINTER(C.c_longlong)]
@@ -200,6 +201,14 @@ class Engine:
 
     def profile_reset(self):
         self.profile(reset=True)
+
+    def opt_sastry(self, itmax=10000):
+        """Structure optimisation from the current positions (conjugate
+        gradients with cubic line minimisation, the reference's sastry);
+        the engine's positions are left at the minimum."""
+        r = abi.OptResult()
+        self._check(lib().mdff_opt_sastry(self._h, int(itmax), C.byref(r)))
+        return r.as_dict()
 
     def profile_detail(self):
         """The tensor-core k-space kernels alone (mixed path): per kernel the

@@ -91,6 +91,15 @@ class Thermo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class OptResult(C.Structure):
+    """mdff_opt_result: one structure optimisation (opt_main's report)."""
+    _fields_ = [("u_initial", C.c_double), ("u_final", C.c_double), ("phigrad", C.c_double),
+                ("iterations", C.c_int), ("nforce", C.c_int), ("status", C.c_int), ("pad", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
 class ParamGrad(C.Structure):
     """mdff_param_grad: derivative of a loss with respect to the force-field
     tables, unordered pairs in the upper-triangle slot [a][b], a <= b."""

@@ -21,6 +21,7 @@
 #include "ewald_recip.cuh"
 #include "solve.cuh"
 #include "integrate.cuh"
+#include "opt.cuh"
 #include "peaks.cuh"
 
 using namespace mdff;
@@ -68,6 +69,7 @@ struct mdff_ctx {
     double *cg_r = nullptr, *cg_z = nullptr, *cg_d = nullptr, *cg_Ad = nullptr, *mu_save = nullptr;
     double* hist = nullptr;
     double* coef = nullptr;
+    double *opt_xi = nullptr, *opt_g = nullptr, *opt_h = nullptr, *opt_r0 = nullptr;   // structure optimisation
     double *ef = nullptr, *efg = nullptr, *fcoul = nullptr;
     PairConst* pc = nullptr;
     NList lv, lc;
@@ -1050,7 +1052,226 @@ int md_step(mdff_ctx* ctx) {
 
 }  // namespace
 
+// ---- structure optimisation ------------------------------------------------
+// sastry (src/opt.f90:452-849): conjugate gradients on U(r) = u_tot with the
+// direction normalised to unit length and each line minimised by cubic
+// interpolation along it; eforce1d (:864-933) is one engforce at r + x xi.
+// The scalar control flow is the reference's, statement for statement
+// (labels 777, 524, 525, 676 become loops); the vectors and their dot
+// products stay on the device.  As in the reference, the Verlet lists are
+// the ones of the starting configuration (engforce does not rebuild them),
+// trial evaluations leave their forces behind, and u_tot changes only where
+// the reference assigns it.
+namespace {
+
+double opt_utot(const mdff_ctx* ctx) { return ctx->en.u_lj + ctx->en.u_coul + ctx->en.u_morse + ctx->en.u_bmhft; }
+
+int opt_sum(mdff_ctx* ctx, int K, double out[2]) {
+    launch_reduce_partials(ctx->st, ctx->part.buf, nb(ctx->n), K, ctx->dsc->opt, 0);
+    TRY(sync_scalars(ctx));
+    out[0] = ctx->hsc->opt[0];
+    out[1] = K > 1 ? ctx->hsc->opt[1] : 0.0;
+    return MDFF_OK;
+}
+
+int opt_dot(mdff_ctx* ctx, int mode, double out[2]) {
+    const int n = ctx->n;
+    if (mode == 0) k_opt_dots<0><<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->opt_xi, ctx->opt_g, ctx->part.buf);
+    else if (mode == 1) k_opt_dots<1><<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->opt_xi, ctx->opt_g, ctx->part.buf);
+    else k_opt_dots<2><<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->opt_xi, ctx->opt_g, ctx->part.buf);
+    return opt_sum(ctx, 2, out);
+}
+
+// the unit steepest-descent direction from the current forces
+int opt_steepest(mdff_ctx* ctx) {
+    const int n = ctx->n;
+    double s[2];
+    k_opt_steepest<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->opt_xi, ctx->opt_g, ctx->opt_h,
+                                               ctx->part.buf);
+    TRY(opt_sum(ctx, 1, s));
+    const double umag = std::sqrt(s[0]);
+    k_opt_div<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, ctx->opt_xi, umag);
+    return check_launch(ctx, "opt_steepest");
+}
+
+// r = r0 + x xi on the device positions
+void opt_place(mdff_ctx* ctx, double x) {
+    const int n = ctx->n;
+    k_opt_move<<<nb(n), 256, 0, ctx->st>>>(n, ctx->opt_r0, ctx->opt_r0 + n, ctx->opt_r0 + 2 * (size_t)n, ctx->opt_xi,
+                                           x, ctx->x, ctx->y, ctx->z);
+}
+
+// eforce1d: U and dU/dx at r0 + x xi; the positions are r0 again afterwards,
+// the forces stay those of the trial point
+int opt_eforce1d(mdff_ctx* ctx, double x, double& pot, double& f1d, int& neng) {
+    opt_place(ctx, x);
+    TRY(engforce_device(ctx));
+    pot = opt_utot(ctx);
+    neng = neng + 1;
+    opt_place(ctx, 0.0);
+    double s[2];
+    TRY(opt_dot(ctx, 0, s));
+    f1d = -s[0];
+    return MDFF_OK;
+}
+
+// the accepted move r0 += x xi (kept in r0 and in the device positions)
+int opt_accept(mdff_ctx* ctx, double x) {
+    const int n = ctx->n;
+    opt_place(ctx, x);
+    CK(cudaMemcpyAsync(ctx->opt_r0, ctx->x, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->opt_r0 + n, ctx->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->opt_r0 + 2 * (size_t)n, ctx->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    return MDFF_OK;
+}
+
+int opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* R) {
+    const int n = ctx->n;
+    if (!ctx->opt_xi) {
+        TRY(dalloc(ctx, &ctx->opt_xi, 3 * (size_t)n));
+        TRY(dalloc(ctx, &ctx->opt_g, 3 * (size_t)n));
+        TRY(dalloc(ctx, &ctx->opt_h, 3 * (size_t)n));
+        TRY(dalloc(ctx, &ctx->opt_r0, 3 * (size_t)n));
+    }
+    CK(cudaMemcpyAsync(ctx->opt_r0, ctx->x, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->opt_r0 + n, ctx->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->opt_r0 + 2 * (size_t)n, ctx->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    const double ftol = 2.2250738585072014e-308, epsilon = 1.0e-14;   // tiny(1.0_dp)
+    int neng = 0;
+    TRY(engforce_device(ctx));
+    neng = neng + 1;
+    double u_tot = opt_utot(ctx);
+    R->u_initial = u_tot;
+    R->status = 1;
+    TRY(opt_steepest(ctx));
+    double ds = 0.2, dutol = 1.0e-12, phigrad = 0.0, Eis = u_tot, xsol = 0.0, t[2];
+    for (int its = 1; its <= itmax; ++its) {
+        TRY(opt_dot(ctx, 1, t));
+        phigrad = t[0];
+        R->iterations = its;
+        double ukeep = u_tot, x0 = 0.0, u0 = u_tot, f1_dp;
+        TRY(opt_dot(ctx, 0, t));
+        f1_dp = -t[0];
+        if (f1_dp >= 0.0) {   // reset to the steepest-descent direction
+            TRY(opt_steepest(ctx));
+            ukeep = u_tot; x0 = 0.0; u0 = u_tot;
+            TRY(opt_dot(ctx, 0, t));
+            f1_dp = -t[0];
+        }
+        double x1 = ds, u1, f1d1, u2 = 0.0, f1ds = 0.0;
+        TRY(opt_eforce1d(ctx, x1, u1, f1d1, neng));
+        int nstep = 0;
+        double uprev = std::min(u1, u0);
+        for (;;) {   // label 777
+            nstep = nstep + 1;
+            const double dx = x1 - x0, dx2 = dx * dx, dx3 = dx * dx2;
+            if (nstep > 100) {
+                if (std::min(u0, u1) > ukeep) {
+                    Eis = u0;
+                    R->u_final = Eis; R->phigrad = phigrad; R->nforce = neng; R->status = 3;
+                    return MDFF_OK;
+                }
+                if (u0 < u1) {
+                    TRY(opt_eforce1d(ctx, x0, u0, f1_dp, neng));
+                    xsol = x0; u_tot = u0; f1ds = f1_dp;
+                } else {
+                    xsol = x1; u_tot = u1; f1ds = f1d1;
+                }
+                TRY(opt_accept(ctx, xsol));
+                break;
+            }
+            if (f1_dp * f1d1 < 0.0) {
+                const double uppcub = (2.0 / dx2) * (3.0 * (u1 - u0) - (f1d1 + 2.0 * f1_dp) * dx);
+                const double u3pcub = (-12.0 / dx3) * ((u1 - u0) - (f1d1 + f1_dp) * (dx / 2.0));
+                double x1sol = -uppcub + std::sqrt(uppcub * uppcub - 2.0 * u3pcub * f1_dp);
+                x1sol = x1sol / u3pcub;
+                double x2sol = -uppcub - std::sqrt(uppcub * uppcub - 2.0 * u3pcub * f1_dp);
+                x2sol = x2sol / u3pcub;
+                const double curv1 = uppcub + u3pcub * x1sol, curv2 = uppcub + u3pcub * x2sol;
+                if (curv1 > 0.0) xsol = x1sol + x0;
+                if (curv2 > 0.0) xsol = x2sol + x0;
+                for (;;) {   // label 524: keep u2 below ukeep
+                    TRY(opt_eforce1d(ctx, xsol, u2, f1ds, neng));
+                    if (u2 > ukeep) { xsol = x0 + (xsol - x0) / 2.0; continue; }
+                    break;
+                }
+                if (std::fabs((uprev - u2) / u2) < dutol) {
+                    TRY(opt_accept(ctx, xsol));
+                    u_tot = u2; ds = xsol;
+                    if (xsol <= 1.0e-8) ds = 1.0e-8;
+                    break;
+                }
+                if (f1_dp * f1ds <= 0.0) { x1 = xsol; u1 = u2; f1d1 = f1ds; }
+                else { x0 = xsol; u0 = u2; f1_dp = f1ds; }
+                uprev = std::min(u0, u1);
+            } else {
+                const double u2pdis = (f1d1 - f1_dp) / (x1 - x0), adx = std::fabs(x1 - x0);
+                if (u2pdis > 0.0) {
+                    xsol = x0 - f1_dp / u2pdis;
+                    if (std::fabs(xsol - x0) > 3.0 * adx) xsol = x0 + 3.0 * adx;
+                } else {
+                    xsol = x0 + 1.50 * adx;
+                }
+                for (;;) {   // label 525
+                    TRY(opt_eforce1d(ctx, xsol, u2, f1ds, neng));
+                    if (u2 > ukeep) { xsol = x0 + (xsol - x0) / 2.0; continue; }
+                    break;
+                }
+                if (std::fabs((uprev - u2) / u2) < dutol) {
+                    TRY(opt_accept(ctx, xsol));
+                    u_tot = u2; ds = xsol;
+                    if (xsol <= 1.0e-8) ds = 1.0e-8;
+                    break;
+                }
+                if (u1 < u0) { x0 = x1; u0 = u1; f1_dp = f1d1; }
+                x1 = xsol; u1 = u2; f1d1 = f1ds;
+                uprev = std::min(u0, u1);
+            }
+        }
+        // label 676
+        const double DD1 = 2.0 * std::fabs(ukeep - u_tot);
+        const double DD2 = ftol * (std::fabs(ukeep) + std::fabs(u_tot) + epsilon);
+        if (DD1 <= DD2) {
+            TRY(engforce_device(ctx));
+            neng = neng + 1;
+            Eis = u_tot;
+            TRY(opt_dot(ctx, 1, t));
+            phigrad = t[0];
+            R->u_final = Eis; R->phigrad = phigrad; R->nforce = neng; R->status = 0;
+            return MDFF_OK;
+        } else if (std::fabs(1.0 - u_tot / ukeep) < dutol) {
+            dutol = std::fabs(1.0 - u_tot / ukeep);
+        }
+        TRY(opt_dot(ctx, 2, t));
+        const double gg = t[0], dgg = t[1];
+        if (gg == 0.0) {
+            R->u_final = u_tot; R->phigrad = phigrad; R->nforce = neng; R->status = 2;
+            return MDFF_OK;
+        }
+        const double gam = dgg / gg;
+        k_opt_cg<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->opt_xi, ctx->opt_g, ctx->opt_h, gam,
+                                             ctx->part.buf);
+        TRY(opt_sum(ctx, 1, t));
+        k_opt_div<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, ctx->opt_xi, std::sqrt(t[0]));
+        TRY(check_launch(ctx, "opt_cg"));
+    }
+    R->u_final = u_tot; R->phigrad = phigrad; R->nforce = neng; R->status = 1;
+    R->iterations = itmax;
+    return MDFF_OK;
+}
+
+}  // namespace
+
 extern "C" {
+
+int mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!out || itmax < 1) return fail(ctx, MDFF_E_ARG, "mdff_opt_sastry: out must be given and itmax >= 1");
+    cudaSetDevice(ctx->p.device);
+    std::memset(out, 0, sizeof *out);
+    return opt_sastry(ctx, itmax, out);
+}
+
 
 int mdff_measure_pipes(int device, double out[3]) {
     if (!out) return MDFF_E_ARG;
@@ -1202,6 +1423,7 @@ int mdff_struct_size(int which) {
         case 1: return (int)sizeof(mdff_energies);
         case 2: return (int)sizeof(mdff_thermo);
         case 3: return (int)sizeof(mdff_param_grad);
+        case 4: return (int)sizeof(mdff_opt_result);
         default: return -1;
     }
 }

@@ -159,6 +159,8 @@ struct DevScalars {
     int rebuild;
     int overflow;
     int tc_err;         // tensor-core pipeline: a bounded wait gave up (bit per wait site)
+    int pad_;
+    double opt[2];      // structure optimisation: reduced dot products
 };
 
 // Launchers (kernels live in the *.cuh files, compiled as one unit by engine.cu).

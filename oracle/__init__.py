@@ -52,6 +52,7 @@ def lib():
         L.orc_loss_grad.argtypes = [C.c_void_p, dp, dp, dp, dp, C.c_double, C.c_double, dp,
                                     C.POINTER(abi.ParamGrad), ip]
         L.orc_step.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
+        L.orc_opt_sastry.argtypes = [C.c_void_p, C.c_int, C.POINTER(abi.OptResult)]
         _lib = L
     return _lib
 
@@ -192,6 +193,13 @@ class Oracle:
         lib().orc_loss_grad(self._h, *(_dp(a) for a in f), _dp(tt), float(c_force), float(c_stress),
                             C.byref(loss), C.byref(grad), it)
         return loss.value, grad, (it[0], it[1])
+
+    def opt_sastry(self, itmax=10000):
+        """Structure optimisation from the current positions (sastry,
+        src/opt.f90:452-849); the positions are left at the minimum."""
+        r = abi.OptResult()
+        lib().orc_opt_sastry(self._h, int(itmax), C.byref(r))
+        return r.as_dict()
 
     def md_start(self, vel):
         vel = np.asarray(vel, dtype=np.float64)

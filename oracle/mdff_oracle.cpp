@@ -1641,6 +1641,195 @@ int loss_grad(orc_sys* s, const double* fxt, const double* fyt, const double* fz
 
 }  // namespace
 
+
+// ---- structure optimisation ------------------------------------------------
+// sastry (src/opt.f90:452-849): conjugate gradients on U(r) with the search
+// direction normalised to unit length, each line minimised by cubic
+// interpolation of U along it (eforce1d, :864-933, evaluates U and dU/dx at
+// r + x xi).  Stated as the reference runs it: trial evaluations leave their
+// forces in fx (the next direction uses the forces of the last accepted
+// trial point), u_tot is reassigned only where the reference assigns it, and
+// the energy test uses ftol = tiny(1.0_dp).
+static double opt_utot(const orc_sys* s) { return s->en.u_lj + s->en.u_coul + s->en.u_morse + s->en.u_bmhft; }
+
+static void opt_eforce1d(orc_sys* s, double x, double& pot, double& f1d, const std::vector<double>& xix,
+                         const std::vector<double>& xiy, const std::vector<double>& xiz, int& neng) {
+    const int n = s->natm;
+    std::vector<double> tx = s->rx, ty = s->ry, tz = s->rz;
+    for (int ia = 0; ia < n; ++ia) {
+        s->rx[ia] = tx[ia] + x * xix[ia];
+        s->ry[ia] = ty[ia] + x * xiy[ia];
+        s->rz[ia] = tz[ia] + x * xiz[ia];
+    }
+    engforce(s);
+    pot = opt_utot(s);
+    neng = neng + 1;
+    s->rx = tx; s->ry = ty; s->rz = tz;
+    f1d = 0.0;
+    for (int ia = 0; ia < n; ++ia) f1d = f1d + s->fx[ia] * xix[ia] + s->fy[ia] * xiy[ia] + s->fz[ia] * xiz[ia];
+    f1d = -f1d;
+}
+
+static int opt_sastry(orc_sys* s, int itmax, mdff_opt_result* R) {
+    const int n = s->natm;
+    std::vector<double> gx(n), gy(n), gz(n), hx(n), hy(n), hz(n), xix(n), xiy(n), xiz(n);
+    const double ftol = 2.2250738585072014e-308, epsilon = 1.0e-14;   // tiny(1.0_dp)
+    int neng = 0;
+    engforce(s);
+    neng = neng + 1;
+    double u_tot = opt_utot(s);
+    R->u_initial = u_tot;
+    R->status = 1;
+    auto steepest = [&]() {
+        double umag = 0.0;
+        for (int ja = 0; ja < n; ++ja) {
+            xix[ja] = -s->fx[ja]; xiy[ja] = -s->fy[ja]; xiz[ja] = -s->fz[ja];
+            gx[ja] = -xix[ja]; gy[ja] = -xiy[ja]; gz[ja] = -xiz[ja];
+            hx[ja] = gx[ja]; hy[ja] = gy[ja]; hz[ja] = gz[ja];
+            xix[ja] = hx[ja]; xiy[ja] = hy[ja]; xiz[ja] = hz[ja];
+            umag = umag + xix[ja] * xix[ja] + xiy[ja] * xiy[ja] + xiz[ja] * xiz[ja];
+        }
+        umag = std::sqrt(umag);
+        for (int ja = 0; ja < n; ++ja) { xix[ja] = xix[ja] / umag; xiy[ja] = xiy[ja] / umag; xiz[ja] = xiz[ja] / umag; }
+    };
+    auto fdotxi = [&]() {
+        double f = 0.0;
+        for (int ia = 0; ia < n; ++ia) f = f + s->fx[ia] * xix[ia] + s->fy[ia] * xiy[ia] + s->fz[ia] * xiz[ia];
+        return -f;
+    };
+    auto sumf2 = [&]() {
+        double g = 0.0;
+        for (int ia = 0; ia < n; ++ia) g = g + s->fx[ia] * s->fx[ia] + s->fy[ia] * s->fy[ia] + s->fz[ia] * s->fz[ia];
+        return g;
+    };
+    auto move = [&](double x) {
+        for (int ia = 0; ia < n; ++ia) {
+            s->rx[ia] = s->rx[ia] + x * xix[ia];
+            s->ry[ia] = s->ry[ia] + x * xiy[ia];
+            s->rz[ia] = s->rz[ia] + x * xiz[ia];
+        }
+    };
+    steepest();
+    double ds = 0.2, dutol = 1.0e-12, phigrad = 0.0, Eis = u_tot, xsol = 0.0;
+    int its;
+    for (its = 1; its <= itmax; ++its) {
+        phigrad = sumf2();
+        R->iterations = its;
+        double ukeep = u_tot, x0 = 0.0, u0 = u_tot, f1_dp = fdotxi();
+        if (f1_dp >= 0.0) {   // reset to the steepest-descent direction
+            steepest();
+            ukeep = u_tot; x0 = 0.0; u0 = u_tot; f1_dp = fdotxi();
+        }
+        double x1 = ds, u1, f1d1, u2 = 0.0, f1ds = 0.0;
+        opt_eforce1d(s, x1, u1, f1d1, xix, xiy, xiz, neng);
+        int nstep = 0;
+        double uprev = std::min(u1, u0);
+        for (;;) {   // label 777
+            nstep = nstep + 1;
+            double dx = x1 - x0, dx2 = dx * dx, dx3 = dx * dx2;
+            (void)dx3;
+            if (nstep > 100) {
+                if (std::min(u0, u1) > ukeep) {
+                    Eis = u0;
+                    R->u_final = Eis; R->phigrad = phigrad; R->nforce = neng; R->status = 3;
+                    return 0;
+                }
+                if (u0 < u1) {
+                    opt_eforce1d(s, x0, u0, f1_dp, xix, xiy, xiz, neng);
+                    xsol = x0; u_tot = u0; f1ds = f1_dp;
+                } else {
+                    xsol = x1; u_tot = u1; f1ds = f1d1;
+                }
+                move(xsol);
+                break;
+            }
+            if (f1_dp * f1d1 < 0.0) {
+                const double uppcub = (2.0 / dx2) * (3.0 * (u1 - u0) - (f1d1 + 2.0 * f1_dp) * dx);
+                const double u3pcub = (-12.0 / dx3) * ((u1 - u0) - (f1d1 + f1_dp) * (dx / 2.0));
+                double x1sol = -uppcub + std::sqrt(uppcub * uppcub - 2.0 * u3pcub * f1_dp);
+                x1sol = x1sol / u3pcub;
+                double x2sol = -uppcub - std::sqrt(uppcub * uppcub - 2.0 * u3pcub * f1_dp);
+                x2sol = x2sol / u3pcub;
+                const double curv1 = uppcub + u3pcub * x1sol, curv2 = uppcub + u3pcub * x2sol;
+                if (curv1 > 0.0) xsol = x1sol + x0;
+                if (curv2 > 0.0) xsol = x2sol + x0;
+                for (;;) {   // label 524: keep u2 below ukeep
+                    opt_eforce1d(s, xsol, u2, f1ds, xix, xiy, xiz, neng);
+                    if (u2 > ukeep) { xsol = x0 + (xsol - x0) / 2.0; continue; }
+                    break;
+                }
+                if (std::fabs((uprev - u2) / u2) < dutol) {
+                    move(xsol);
+                    u_tot = u2; ds = xsol;
+                    if (xsol <= 1.0e-8) ds = 1.0e-8;
+                    break;
+                }
+                if (f1_dp * f1ds <= 0.0) { x1 = xsol; u1 = u2; f1d1 = f1ds; }
+                else { x0 = xsol; u0 = u2; f1_dp = f1ds; }
+                uprev = std::min(u0, u1);
+            } else {
+                const double u2pdis = (f1d1 - f1_dp) / (x1 - x0), adx = std::fabs(x1 - x0);
+                if (u2pdis > 0.0) {
+                    xsol = x0 - f1_dp / u2pdis;
+                    if (std::fabs(xsol - x0) > 3.0 * adx) xsol = x0 + 3.0 * adx;
+                } else {
+                    xsol = x0 + 1.50 * adx;
+                }
+                for (;;) {   // label 525
+                    opt_eforce1d(s, xsol, u2, f1ds, xix, xiy, xiz, neng);
+                    if (u2 > ukeep) { xsol = x0 + (xsol - x0) / 2.0; continue; }
+                    break;
+                }
+                if (std::fabs((uprev - u2) / u2) < dutol) {
+                    move(xsol);
+                    u_tot = u2; ds = xsol;
+                    if (xsol <= 1.0e-8) ds = 1.0e-8;
+                    break;
+                }
+                if (u1 < u0) { x0 = x1; u0 = u1; f1_dp = f1d1; }
+                x1 = xsol; u1 = u2; f1d1 = f1ds;
+                uprev = std::min(u0, u1);
+            }
+        }
+        // label 676
+        const double DD1 = 2.0 * std::fabs(ukeep - u_tot);
+        const double DD2 = ftol * (std::fabs(ukeep) + std::fabs(u_tot) + epsilon);
+        if (DD1 <= DD2) {
+            engforce(s);
+            neng = neng + 1;
+            Eis = u_tot;
+            phigrad = sumf2();
+            R->u_final = Eis; R->phigrad = phigrad; R->nforce = neng; R->status = 0;
+            return 0;
+        } else if (std::fabs(1.0 - u_tot / ukeep) < dutol) {
+            dutol = std::fabs(1.0 - u_tot / ukeep);
+        }
+        double gg = 0.0, dgg = 0.0;
+        for (int ja = 0; ja < n; ++ja) {
+            xix[ja] = -s->fx[ja]; xiy[ja] = -s->fy[ja]; xiz[ja] = -s->fz[ja];
+            gg = gg + gx[ja] * gx[ja] + gy[ja] * gy[ja] + gz[ja] * gz[ja];
+            dgg = dgg + (xix[ja] + gx[ja]) * xix[ja] + (xiy[ja] + gy[ja]) * xiy[ja] + (xiz[ja] + gz[ja]) * xiz[ja];
+        }
+        if (gg == 0.0) {
+            R->u_final = u_tot; R->phigrad = phigrad; R->nforce = neng; R->status = 2;
+            return 0;
+        }
+        const double gam = dgg / gg;
+        double umag = 0.0;
+        for (int ja = 0; ja < n; ++ja) {
+            gx[ja] = -xix[ja]; gy[ja] = -xiy[ja]; gz[ja] = -xiz[ja];
+            hx[ja] = gx[ja] + gam * hx[ja]; hy[ja] = gy[ja] + gam * hy[ja]; hz[ja] = gz[ja] + gam * hz[ja];
+            xix[ja] = hx[ja]; xiy[ja] = hy[ja]; xiz[ja] = hz[ja];
+            umag = umag + xix[ja] * xix[ja] + xiy[ja] * xiy[ja] + xiz[ja] * xiz[ja];
+        }
+        umag = std::sqrt(umag);
+        for (int ja = 0; ja < n; ++ja) { xix[ja] = xix[ja] / umag; xiy[ja] = xiy[ja] / umag; xiz[ja] = xiz[ja] / umag; }
+    }
+    R->u_final = u_tot; R->phigrad = phigrad; R->nforce = neng; R->status = 1;
+    R->iterations = itmax;
+    return 0;
+}
+
 extern "C" {
 
 orc_sys* orc_create(const mdff_params* p, int natm, const int* itype, const double* rx, const double* ry,
@@ -1767,6 +1956,11 @@ int orc_nlist_get(orc_sys* s, int which, int* point, int* list, int cap, int* nl
 int orc_loss_grad(orc_sys* s, const double* fxt, const double* fyt, const double* fzt, const double taut[9],
                   double cF, double cS, double* loss, mdff_param_grad* g, int iters[2]) {
     return loss_grad(s, fxt, fyt, fzt, taut, cF, cS, loss, g, iters);
+}
+
+int orc_opt_sastry(orc_sys* s, int itmax, mdff_opt_result* r) {
+    std::memset(r, 0, sizeof *r);
+    return opt_sastry(s, itmax, r);
 }
 
 int orc_engforce(orc_sys* s, double* fx, double* fy, double* fz, mdff_energies* e, double tau_nonb[9],

@@ -53,7 +53,8 @@ def parse():
                     help="mixed path: structure factor on the tensor cores (1) or the FP32 CUDA-core kernel (0)")
     ap.add_argument("--reuse", default="auto", choices=["auto", "0", "1"],
                     help="kspace_reuse (auto: on for the mixed path, off for the plain FP64 path)")
-    ap.add_argument("--workload", default="production", choices=["production", "batch"],
+    ap.add_argument("--opt-iters", type=int, default=10, help="opt workload: conjugate-gradient iterations")
+    ap.add_argument("--workload", default="production", choices=["production", "batch", "opt"],
                     help="production: the 32 440-ion PIM NVT cell (the headline metric); batch: the 64-configuration "
                          "force-matching loss and adjoint gradient")
     ap.add_argument("--accuracy", action="store_true",
@@ -567,6 +568,93 @@ def run_batch(args):
     return result
 
 
+def run_opt(args):
+    """Structure-optimisation workload: the reference's conjugate-gradient
+    minimiser (sastry) on the production cell from its jittered start, capped
+    at --opt-iters iterations.  Every line-search point is one full force
+    evaluation (pair loop, real and reciprocal Ewald, induced-dipole solve), so
+    value = atoms x force evaluations / device time; e2e adds loading the
+    positions from host memory and reading the minimised ones back."""
+    import torch
+    world, rank, local, dist = dist_setup(args.gpus)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    import mdff_b200
+    from mdff_b200 import abi, systems
+    s = systems.mgo_production(ncell=args.ncell)
+    p = s["params"]
+    p.precision = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    p.device = local
+    p.kspace_reuse = (1 if args.precision == "mixed" else 0) if args.reuse == "auto" else int(args.reuse)
+    p.autotune = args.autotune
+    p.kspace_tc = args.tc
+    natm = len(s["itype"])
+    pos0 = np.ascontiguousarray(s["pos"])
+    eng = mdff_b200.Engine(p, s["itype"], pos0, s["cell"])
+    ext = torch.cuda.ExternalStream(eng.stream(), device=device)
+    for _ in range(max(args.warmup, 1)):
+        eng.set_positions(pos0)
+        eng.opt_sastry(2)
+    eng.set_positions(pos0)
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(ext)
+        r = eng.opt_sastry(args.opt_iters)
+        ev1.record(ext)
+        ev1.synchronize()
+    torch.cuda.synchronize(device)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, dist, device)
+    value = whole_job_rate(natm * r["nforce"], ms / 1e3, dist, device)
+    # end to end: positions from pinned host memory in, minimised positions out
+    hp = torch.empty((natm, 3), dtype=torch.float64, pin_memory=True).numpy()
+    hp[:] = pos0
+    barrier(dist, device)
+    t1 = time.perf_counter()
+    eng.set_positions(hp)
+    r2 = eng.opt_sastry(args.opt_iters)
+    out = eng.positions()
+    t2 = time.perf_counter()
+    e2e_v = whole_job_rate(natm * r2["nforce"], t2 - t1, dist, device)
+    result = None
+    if rank == 0:
+        result = {
+            "metric": "structure-optimisation atom-force-evaluations/s, 32k-ion MgO PIM (conjugate gradients, "
+                      "cubic line search)",
+            "value": value,
+            "unit": "atom-evaluations/s",
+            "n_gpus": world,
+            "steps": r["iterations"],
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / max(r["nforce"], 1),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "fp32+fp64" if args.precision == "mixed" else "fp64",
+            "data": "synthetic (seeded MgO polarisable-ion cell, mdff_b200.systems.mgo_production)",
+            "config": {"workload": "mgo-pim-opt", "natm": natm, "algorithm": "sastry (cg + cubic line search)",
+                       "opt_iters": args.opt_iters, "precision": args.precision, "kspace_tc": int(p.kspace_tc),
+                       "parallelism": f"replicas{world}",
+                       "l2": "per-evaluation working set > 126 MB L2"},
+            "opt": r,
+            "e2e": {"value": e2e_v, "unit": "atom-evaluations/s", "h2d_bytes_per_step": 24 * natm,
+                    "d2h_bytes_per_step": 24 * natm + 48},
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu:
+            cb = cpu_baseline(s, p, 8.0)
+            cb["unit"] = "atom-evaluations/s"
+            cb["sample"] = cb["sample"].replace("per MD step", "per force evaluation")
+            result["cpu_baseline"] = cb
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
 def main():
     args = parse()
     if args.accuracy:
@@ -575,6 +663,8 @@ def main():
         r = run_reference(args)
     elif args.workload == "batch":
         r = run_batch(args)
+    elif args.workload == "opt":
+        r = run_opt(args)
     else:
         r = run_engine(args)
     if r is not None:

@@ -205,10 +205,17 @@ typedef struct mdff_opt_result {
     int    pad;
 } mdff_opt_result;
 
+/* Distribution settings of efg_stat (the efgtag namelist, src/efg.f90:171-190):
+ * bins PANvzz = int(2|vzzmin|/resvzz), PANeta = int(1/reseta),
+ * PANU = int(2|umin|/resu), PANS = int(smax/resu) (src/efg.f90:233-236). */
+typedef struct mdff_efg_dist_params {
+    double vzzmin, resvzz, reseta, umin, resu, smax;
+} mdff_efg_dist_params;
+
 /* sizeof(mdff_params), sizeof(mdff_energies), sizeof(mdff_thermo),
  * sizeof(mdff_param_grad), sizeof(mdff_opt_result) for which = 0 .. 4 (lets a binding check its
  * mirror of these structs); no reference counterpart. */
-int  mdff_struct_size(int which);
+int  mdff_struct_size(int which);   /* 5 = mdff_efg_dist_params */
 
 /* Measured FMA throughput of the device in TFLOP/s: out[0] FP64, out[1]
  * FP32, out[2] packed FP32x2 (fma.rn.f32x2).  The roofline denominators of
@@ -314,6 +321,30 @@ int  mdff_engforce(mdff_ctx* ctx, double* fx, double* fy, double* fz,
  * forces are those of the minimum; *out gets pot0, Eis, phigrad, iter, neng.
  * itmax: the reference's 10000. */
 int  mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out);
+
+/* EFG post-processing (efg_stat's per-site part, src/efg.f90:2225-2270, and
+ * nmr_convention, :2546-2650) on the device.  efg6: host tensors [6][natm]
+ * (xx yy zz xy xz yz), or NULL for the context's EFG of its last force
+ * evaluation (doefg).  Out (host, any may be NULL): nmr[4][natm] = Vxx, Vyy,
+ * Vzz, eta (|Vzz| >= |Vyy| >= |Vxx|); U[5][natm] the Czjzek components
+ * (Vzz/2, Vxz/sqrt3, Vyz/sqrt3, Vxy/sqrt3, (Vxx-Vyy)/(2 sqrt3)); S[natm] = |U|.
+ * The principal values come from a cyclic Jacobi iteration in FP64 in place
+ * of LAPACK's DSYEV. */
+int  mdff_efg_nmr(mdff_ctx* ctx, const double* efg6, double* nmr, double* U, double* S);
+/* efg_stat's statistics and distributions of one configuration
+ * (src/efg.f90:2272-2440).  Rows t = 0 (all sites), 1..ntype.  stats[(ntype+1)][8]:
+ * vzzmin, vzzmax (running extrema started at 0, as there), <Vzz>, <|Vzz|>,
+ * <eta>, fraction Vzz >= 0, rho_z = sigma/<|Vzz|>, sigma = sqrt(<Vzz^2> - <|Vzz|>^2)
+ * (0 where a row has no sites or <|Vzz|> = 0).  The isotropy test
+ * (:2435-2469): mU[(ntype+1)][5] = <U_k>, m2U[(ntype+1)][5][5] = <U_k U_l> on
+ * the upper triangle (k <= l, zero below), row 0 of m2U left as the plain sum
+ * over sites as there.  Counts: dib_vzz[(ntype+1)][PANvzz+1],
+ * dib_eta[(ntype+1)][PANeta+1], dib_u[6][(ntype+1)][PANU+1] (U1..U5, then
+ * U2..U5 together), dib_s[(ntype+1)][PANS+1]; over several configurations the
+ * reference's totals are the sums of the per-call counts.  A value outside the
+ * ranges returns MDFF_E_ARG (the reference STOPs).  Any output may be NULL. */
+int  mdff_efg_dist(mdff_ctx* ctx, const double* efg6, const mdff_efg_dist_params* dp, double* stats,
+                   double* mU, double* m2U, int* dib_vzz, int* dib_eta, int* dib_u, int* dib_s);
 
 /* Rebuild the Verlet lists at the current positions: vnlist_pbc
  * (src/tools.f90:274-370). */

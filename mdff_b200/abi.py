@@ -100,6 +100,18 @@ class OptResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
+class EfgDistParams(C.Structure):
+    """mdff_efg_dist_params: efg_stat's distribution settings (efgtag:
+    vzzmin, resvzz, reseta, umin, resu, smax; src/efg.f90:171-190)."""
+    _fields_ = [("vzzmin", C.c_double), ("resvzz", C.c_double), ("reseta", C.c_double),
+                ("umin", C.c_double), ("resu", C.c_double), ("smax", C.c_double)]
+
+    def bins(self):
+        """(PANvzz, PANeta, PANU, PANS) as efg_check_tag sets them (src/efg.f90:233-236)."""
+        return (int((2.0 * abs(self.vzzmin)) / self.resvzz), int(1.0 / self.reseta),
+                int((2.0 * abs(self.umin)) / self.resu), int(self.smax / self.resu))
+
+
 class ParamGrad(C.Structure):
     """mdff_param_grad: derivative of a loss with respect to the force-field
     tables, unordered pairs in the upper-triangle slot [a][b], a <= b."""

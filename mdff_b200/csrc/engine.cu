@@ -22,6 +22,7 @@
 #include "solve.cuh"
 #include "integrate.cuh"
 #include "opt.cuh"
+#include "efg_post.cuh"
 #include "peaks.cuh"
 
 using namespace mdff;
@@ -70,6 +71,7 @@ struct mdff_ctx {
     double* hist = nullptr;
     double* coef = nullptr;
     double *opt_xi = nullptr, *opt_g = nullptr, *opt_h = nullptr, *opt_r0 = nullptr;   // structure optimisation
+    double *efgp_t = nullptr, *efgp_nmr = nullptr, *efgp_u = nullptr, *efgp_s = nullptr;   // EFG post-processing
     double *ef = nullptr, *efg = nullptr, *fcoul = nullptr;
     PairConst* pc = nullptr;
     NList lv, lc;
@@ -1264,6 +1266,131 @@ int opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* R) {
 
 extern "C" {
 
+// EFG post-processing: the tensors (the caller's, or the context's own from
+// the last force evaluation) through k_efg_nmr into device scratch.
+static int efg_post_sites(mdff_ctx* ctx, const double* efg6) {
+    const int n = ctx->n;
+    if (!ctx->efgp_nmr) {
+        TRY(dalloc(ctx, &ctx->efgp_t, 6 * (size_t)n));
+        TRY(dalloc(ctx, &ctx->efgp_nmr, 4 * (size_t)n));
+        TRY(dalloc(ctx, &ctx->efgp_u, 5 * (size_t)n));
+        TRY(dalloc(ctx, &ctx->efgp_s, (size_t)n));
+    }
+    const double* src = ctx->efg;
+    if (efg6) {
+        CK(cudaMemcpyAsync(ctx->efgp_t, efg6, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, ctx->st));
+        src = ctx->efgp_t;
+    } else if (!(ctx->p.lcoulomb && ctx->p.doefg)) {
+        return fail(ctx, MDFF_E_STATE, "no EFG in the context: pass tensors or evaluate forces with doefg");
+    }
+    k_efg_nmr<<<nb(n), 256, 0, ctx->st>>>(n, src, ctx->efgp_nmr, ctx->efgp_u, ctx->efgp_s);
+    return check_launch(ctx, "efg_nmr");
+}
+
+int mdff_efg_nmr(mdff_ctx* ctx, const double* efg6, double* nmr, double* U, double* S) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    cudaSetDevice(ctx->p.device);
+    TRY(efg_post_sites(ctx, efg6));
+    const int n = ctx->n;
+    if (nmr) CK(cudaMemcpyAsync(nmr, ctx->efgp_nmr, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, ctx->st));
+    if (U) CK(cudaMemcpyAsync(U, ctx->efgp_u, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, ctx->st));
+    if (S) CK(cudaMemcpyAsync(S, ctx->efgp_s, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+int mdff_efg_dist(mdff_ctx* ctx, const double* efg6, const mdff_efg_dist_params* dp, double* stats, double* mU,
+                  double* m2U, int* dib_vzz, int* dib_eta, int* dib_u, int* dib_s) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!dp || !(dp->resvzz > 0.0) || !(dp->reseta > 0.0) || !(dp->resu > 0.0))
+        return fail(ctx, MDFF_E_ARG, "mdff_efg_dist: resolutions must be positive");
+    if (ctx->ntype > EFG_NT_MAX) return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_efg_dist: at most 16 types");
+    cudaSetDevice(ctx->p.device);
+    TRY(efg_post_sites(ctx, efg6));
+    const int n = ctx->n, nt1 = ctx->ntype + 1;
+    EfgBins b;
+    b.vzzmin = dp->vzzmin; b.resvzz = dp->resvzz; b.reseta = dp->reseta; b.umin = dp->umin; b.resu = dp->resu;
+    b.PANeta = (int)(1.0 / dp->reseta);                       // efg_check_tag, src/efg.f90:233-236
+    b.PANvzz = (int)((2.0 * std::fabs(dp->vzzmin)) / dp->resvzz);
+    b.PANU = (int)((2.0 * std::fabs(dp->umin)) / dp->resu);
+    b.PANS = (int)(dp->smax / dp->resu);
+    b.ntype = ctx->ntype;
+    const size_t nvzz = (size_t)nt1 * (b.PANvzz + 1), neta = (size_t)nt1 * (b.PANeta + 1);
+    const size_t nu = (size_t)6 * nt1 * (b.PANU + 1), ns = (size_t)nt1 * (b.PANS + 1);
+    const int nblk = nb(n);
+    int* hist = nullptr;
+    double* part = nullptr;
+    // histogram and partial scratch for this call only (sizes depend on the bins)
+    CK(cudaMallocAsync((void**)&hist, sizeof(int) * (nvzz + neta + nu + ns + 1), ctx->st));
+    CK(cudaMallocAsync((void**)&part, sizeof(double) * (size_t)nblk * nt1 * EFG_NACC, ctx->st));
+    CK(cudaMemsetAsync(hist, 0, sizeof(int) * (nvzz + neta + nu + ns + 1), ctx->st));
+    int* hv = hist;
+    int* he = hv + nvzz;
+    int* hu = he + neta;
+    int* hs = hu + nu;
+    int* bad = hs + ns;
+    k_efg_dist<<<nblk, 256, 0, ctx->st>>>(n, ctx->type, ctx->efgp_nmr, ctx->efgp_u, ctx->efgp_s, b, hv, he, hu, hs, bad);
+    k_efg_stats<<<nblk, 256, 0, ctx->st>>>(n, ctx->ntype, ctx->type, ctx->efgp_nmr, ctx->efgp_u, part);
+    std::vector<int> hh(nvzz + neta + nu + ns + 1);
+    std::vector<double> pp((size_t)nblk * nt1 * EFG_NACC);
+    CK(cudaMemcpyAsync(hh.data(), hist, sizeof(int) * hh.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(pp.data(), part, sizeof(double) * pp.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaFreeAsync(hist, ctx->st));
+    CK(cudaFreeAsync(part, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    TRY(check_launch(ctx, "efg_dist"));
+    if (dib_vzz) std::memcpy(dib_vzz, hh.data(), sizeof(int) * nvzz);
+    if (dib_eta) std::memcpy(dib_eta, hh.data() + nvzz, sizeof(int) * neta);
+    if (dib_u) std::memcpy(dib_u, hh.data() + nvzz + neta, sizeof(int) * nu);
+    if (dib_s) std::memcpy(dib_s, hh.data() + nvzz + neta + nu, sizeof(int) * ns);
+    // statistics per type row: blocks summed in order; the running extrema of
+    // the reference start at 0 (src/efg.f90:2163-2164)
+    for (int t = 0; t < nt1; ++t) {
+        double a[EFG_NACC] = {};
+        for (int bl = 0; bl < nblk; ++bl) {
+            const double* q = &pp[((size_t)bl * nt1 + t) * EFG_NACC];
+            for (int k = 0; k < EFG_NACC; ++k)
+                if (k != 6 && k != 7) a[k] += q[k];
+            a[6] = std::min(a[6], q[6]);
+            a[7] = std::max(a[7], q[7]);
+        }
+        const double cnt = a[5];
+        // <U_k> per row; <U_k U_l> (k <= l) per type, left as the plain sum for
+        // row 0 as the reference leaves it (src/efg.f90:2435-2439)
+        if (mU)
+            for (int k = 0; k < 5; ++k) mU[(size_t)t * 5 + k] = cnt > 0 ? a[8 + k] / cnt : 0.0;
+        if (m2U) {
+            int m = 13;
+            for (int k = 0; k < 5; ++k)
+                for (int l = 0; l < 5; ++l) {
+                    double v = 0.0;
+                    if (l >= k) {
+                        v = a[m++];
+                        if (t > 0) v = cnt > 0 ? v / cnt : 0.0;
+                    }
+                    m2U[((size_t)t * 5 + k) * 5 + l] = v;
+                }
+        }
+        if (stats) {
+            double* o = stats + (size_t)t * 8;
+            o[0] = a[6];                                  // vzzmini
+            o[1] = a[7];                                  // vzzmaxi
+            o[2] = cnt > 0 ? a[0] / cnt : 0.0;            // vzzm
+            o[3] = cnt > 0 ? a[1] / cnt : 0.0;            // vzzma
+            o[4] = cnt > 0 ? a[2] / cnt : 0.0;            // etam
+            o[5] = cnt > 0 ? a[4] / cnt : 0.0;            // pvzz
+            const double vzzsq = cnt > 0 ? a[3] / cnt : 0.0;
+            const double sig = std::sqrt(vzzsq - o[3] * o[3]);
+            o[7] = sig;                                   // sigmavzz
+            o[6] = o[3] != 0.0 ? sig / o[3] : 0.0;        // rho_z
+        }
+    }
+    const int flag = hh[nvzz + neta + nu + ns];
+    if (flag) return fail(ctx, MDFF_E_ARG, "EFG value outside the distribution range (vzzmin, umin, smax) -- code " +
+                                               std::to_string(flag));
+    return MDFF_OK;
+}
+
 int mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out) {
     if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
     if (!out || itmax < 1) return fail(ctx, MDFF_E_ARG, "mdff_opt_sastry: out must be given and itmax >= 1");
@@ -1424,6 +1551,7 @@ int mdff_struct_size(int which) {
         case 2: return (int)sizeof(mdff_thermo);
         case 3: return (int)sizeof(mdff_param_grad);
         case 4: return (int)sizeof(mdff_opt_result);
+        case 5: return (int)sizeof(mdff_efg_dist_params);
         default: return -1;
     }
 }

@@ -34,6 +34,7 @@ def test_struct_sizes_match():
     assert L.mdff_struct_size(2) == C.sizeof(abi.Thermo)
     assert L.mdff_struct_size(3) == C.sizeof(abi.ParamGrad)
     assert L.mdff_struct_size(4) == C.sizeof(abi.OptResult)
+    assert L.mdff_struct_size(5) == C.sizeof(abi.EfgDistParams)
 
 
 def test_defaults_match_library():

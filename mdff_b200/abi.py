@@ -107,7 +107,10 @@ class EfgDistParams(C.Structure):
                 ("umin", C.c_double), ("resu", C.c_double), ("smax", C.c_double)]
 
     def bins(self):
-        """(PANvzz, PANeta, PANU, PANS) as efg_check_tag sets them (src/efg.f90:233-236)."""
+        """(PANvzz, PANeta, PANU, PANS) as efg_check_tag sets them (src/efg.f90:233-236);
+        zeros where a resolution is not positive (the engine rejects those)."""
+        if not (self.resvzz > 0 and self.reseta > 0 and self.resu > 0):
+            return (0, 0, 0, 0)
         return (int((2.0 * abs(self.vzzmin)) / self.resvzz), int(1.0 / self.reseta),
                 int((2.0 * abs(self.umin)) / self.resu), int(self.smax / self.resu))
 

@@ -175,20 +175,23 @@ module mdff_engine
       type(mdff_opt_result_t), intent(out) :: res
     end function
 
-    ! efg_stat on the device: efg6 = c_loc(efg(1,1)) of efg(natm,6) or c_null_ptr
-    ! for the context's own tensors; nmr(natm,4), u(natm,5), s(natm)
-    integer(c_int) function mdff_efg_nmr(ctx, efg6, nmr, u, s) bind(C, name="mdff_efg_nmr")
+    ! efg_stat on the device over nconf configurations: efg6 = c_loc(efg(1,1,1))
+    ! of efg(natm,6,nconf), or c_null_ptr with nconf = 1 for the context's own
+    ! tensors; nmr(natm,4,nconf), u(natm,5,nconf), s(natm,nconf)
+    integer(c_int) function mdff_efg_nmr(ctx, nconf, efg6, nmr, u, s) bind(C, name="mdff_efg_nmr")
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: ctx, efg6
+      integer(c_int), value :: nconf
       real(c_double), intent(out) :: nmr(*), u(*), s(*)
     end function
 
-    ! stats(8,0:ntype), mu(5,0:ntype), m2u(5,5,0:ntype), dibvzz(0:PANvzz,0:ntype),
+    ! stats(8,0:ntype,nconf), mu(5,0:ntype), m2u(5,5,0:ntype), dibvzz(0:PANvzz,0:ntype),
     ! dibeta(0:PANeta,0:ntype), dibu(0:PANU,0:ntype,6), dibs(0:PANS,0:ntype)
-    integer(c_int) function mdff_efg_dist(ctx, efg6, dp, stats, mu, m2u, dibvzz, dibeta, dibu, dibs) &
+    integer(c_int) function mdff_efg_dist(ctx, nconf, efg6, dp, stats, mu, m2u, dibvzz, dibeta, dibu, dibs) &
         bind(C, name="mdff_efg_dist")
       import :: c_int, c_ptr, c_double, mdff_efg_dist_params_t
       type(c_ptr), value :: ctx, efg6
+      integer(c_int), value :: nconf
       type(mdff_efg_dist_params_t), intent(in) :: dp
       real(c_double), intent(out) :: stats(*), mu(*), m2u(*)
       integer(c_int), intent(out) :: dibvzz(*), dibeta(*), dibu(*), dibs(*)

@@ -322,28 +322,32 @@ int  mdff_engforce(mdff_ctx* ctx, double* fx, double* fy, double* fz,
  * itmax: the reference's 10000. */
 int  mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out);
 
-/* EFG post-processing (efg_stat's per-site part, src/efg.f90:2225-2270, and
- * nmr_convention, :2546-2650) on the device.  efg6: host tensors [6][natm]
- * (xx yy zz xy xz yz), or NULL for the context's EFG of its last force
- * evaluation (doefg).  Out (host, any may be NULL): nmr[4][natm] = Vxx, Vyy,
- * Vzz, eta (|Vzz| >= |Vyy| >= |Vxx|); U[5][natm] the Czjzek components
- * (Vzz/2, Vxz/sqrt3, Vyz/sqrt3, Vxy/sqrt3, (Vxx-Vyy)/(2 sqrt3)); S[natm] = |U|.
- * The principal values come from a cyclic Jacobi iteration in FP64 in place
- * of LAPACK's DSYEV. */
-int  mdff_efg_nmr(mdff_ctx* ctx, const double* efg6, double* nmr, double* U, double* S);
-/* efg_stat's statistics and distributions of one configuration
- * (src/efg.f90:2272-2440).  Rows t = 0 (all sites), 1..ntype.  stats[(ntype+1)][8]:
- * vzzmin, vzzmax (running extrema started at 0, as there), <Vzz>, <|Vzz|>,
- * <eta>, fraction Vzz >= 0, rho_z = sigma/<|Vzz|>, sigma = sqrt(<Vzz^2> - <|Vzz|>^2)
- * (0 where a row has no sites or <|Vzz|> = 0).  The isotropy test
- * (:2435-2469): mU[(ntype+1)][5] = <U_k>, m2U[(ntype+1)][5][5] = <U_k U_l> on
- * the upper triangle (k <= l, zero below), row 0 of m2U left as the plain sum
- * over sites as there.  Counts: dib_vzz[(ntype+1)][PANvzz+1],
- * dib_eta[(ntype+1)][PANeta+1], dib_u[6][(ntype+1)][PANU+1] (U1..U5, then
- * U2..U5 together), dib_s[(ntype+1)][PANS+1]; over several configurations the
- * reference's totals are the sums of the per-call counts.  A value outside the
- * ranges returns MDFF_E_ARG (the reference STOPs).  Any output may be NULL. */
-int  mdff_efg_dist(mdff_ctx* ctx, const double* efg6, const mdff_efg_dist_params* dp, double* stats,
+/* EFG post-processing (efg_stat, src/efg.f90:2057-2440, and nmr_convention,
+ * :2546-2650) on the device, over nconf configurations of the context's
+ * system at once (the configurations of an EFGALL file).  efg6: host tensors
+ * [nconf][6][natm] (xx yy zz xy xz yz), or NULL with nconf = 1 for the
+ * context's EFG of its last force evaluation (doefg).
+ * mdff_efg_nmr, per site (any output may be NULL): nmr[nconf][4][natm] = Vxx,
+ * Vyy, Vzz, eta (|Vzz| >= |Vyy| >= |Vxx|); U[nconf][5][natm] the Czjzek
+ * components (Vzz/2, Vxz/sqrt3, Vyz/sqrt3, Vxy/sqrt3, (Vxx-Vyy)/(2 sqrt3));
+ * S[nconf][natm] = |U|.  The principal values come from a cyclic Jacobi
+ * iteration in FP64 in place of LAPACK's DSYEV. */
+int  mdff_efg_nmr(mdff_ctx* ctx, int nconf, const double* efg6, double* nmr, double* U, double* S);
+/* efg_stat's statistics and distributions.  Rows t = 0 (all sites), 1..ntype.
+ * stats[nconf][ntype+1][8] per configuration: vzzmin, vzzmax, <Vzz>, <|Vzz|>,
+ * <eta>, fraction Vzz >= 0, rho_z = sigma/<|Vzz|>, sigma = sqrt(<Vzz^2> -
+ * <|Vzz|>^2), formed as the reference's loop forms them (averages zeroed once
+ * before the loop, so each configuration's sums add to the previous
+ * configuration's averages; extrema running from 0 over all configurations;
+ * 0 where a row has no sites or <|Vzz|> = 0).  The isotropy test (:2435-2469)
+ * over all configurations: mU[ntype+1][5] = <U_k>, m2U[ntype+1][5][5] =
+ * <U_k U_l> on the upper triangle (k <= l, zero below), row 0 of m2U left as
+ * the plain sum as there.  Counts summed over the configurations:
+ * dib_vzz[ntype+1][PANvzz+1], dib_eta[ntype+1][PANeta+1],
+ * dib_u[6][ntype+1][PANU+1] (U1..U5, then U2..U5 together),
+ * dib_s[ntype+1][PANS+1].  A value outside the ranges returns MDFF_E_ARG (the
+ * reference STOPs).  Any output may be NULL. */
+int  mdff_efg_dist(mdff_ctx* ctx, int nconf, const double* efg6, const mdff_efg_dist_params* dp, double* stats,
                    double* mU, double* m2U, int* dib_vzz, int* dib_eta, int* dib_u, int* dib_s);
 
 /* Rebuild the Verlet lists at the current positions: vnlist_pbc

@@ -65,8 +65,8 @@ def lib():
         L.mdff_measure_tensor.argtypes = [C.c_int, dp]
         L.mdff_opt_sastry.argtypes = [vp, C.c_int, C.POINTER(abi.OptResult)]
         L.mdff_profile_detail.argtypes = [vp, dp, C.POINTER(C.c_longlong), dp]
-        L.mdff_efg_nmr.argtypes = [vp, dp, dp, dp, dp]
-        L.mdff_efg_dist.argtypes = [vp, dp, C.POINTER(abi.EfgDistParams), dp, dp, dp, ip, ip, ip, ip]
+        L.mdff_efg_nmr.argtypes = [vp, C.c_int, dp, dp, dp, dp]
+        L.mdff_efg_dist.argtypes = [vp, C.c_int, dp, C.POINTER(abi.EfgDistParams), dp, dp, dp, ip, ip, ip, ip]
         L.mdff_struct_size.argtypes = [C.c_int]
         L.mdff_kspace_info.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.mdff_launch_shape.argtypes = [vp, C.POINTER(C.c_int)]
@@ -212,34 +212,52 @@ class Engine:
         self._check(lib().mdff_opt_sastry(self._h, int(itmax), C.byref(r)))
         return r.as_dict()
 
+    def _efg_input(self, efg):
+        """[nconf][6][natm] contiguous from [natm][6] or [nconf][natm][6]; None stays None."""
+        if efg is None:
+            return None, 1
+        e = np.asarray(efg, dtype=np.float64)
+        if e.ndim == 2:
+            e = e[None]
+        return np.ascontiguousarray(e.transpose(0, 2, 1)), e.shape[0]
+
     def efg_nmr(self, efg=None):
-        """Per-site EFG analysis (efg_stat, src/efg.f90:2225-2270): efg is
-        [natm][6] (xx yy zz xy xz yz) or None for the tensors of the last
-        engforce (doefg).  Returns nmr [natm][4] (Vxx, Vyy, Vzz, eta in the
-        NMR convention), U [natm][5] (Czjzek components) and S [natm]."""
+        """Per-site EFG analysis (efg_stat, src/efg.f90:2225-2270).  efg:
+        [natm][6] or [nconf][natm][6] (xx yy zz xy xz yz), or None for the
+        tensors of the last engforce (doefg).  Returns nmr [..][natm][4]
+        (Vxx, Vyy, Vzz, eta in the NMR convention), U [..][natm][5] (Czjzek
+        components) and S [..][natm], with the configuration axis only when
+        efg has one."""
         n = self.n
-        e6 = None if efg is None else np.ascontiguousarray(np.asarray(efg, dtype=np.float64).T)
-        nmr, U, S = np.empty(4 * n), np.empty(5 * n), np.empty(n)
-        self._check(lib().mdff_efg_nmr(self._h, _dp(e6), _dp(nmr), _dp(U), _dp(S)))
-        return nmr.reshape(4, n).T.copy(), U.reshape(5, n).T.copy(), S
+        e6, nc = self._efg_input(efg)
+        nmr, U, S = np.empty(4 * n * nc), np.empty(5 * n * nc), np.empty(n * nc)
+        self._check(lib().mdff_efg_nmr(self._h, nc, _dp(e6), _dp(nmr), _dp(U), _dp(S)))
+        nmr = nmr.reshape(nc, 4, n).transpose(0, 2, 1).copy()
+        U = U.reshape(nc, 5, n).transpose(0, 2, 1).copy()
+        S = S.reshape(nc, n)
+        if efg is None or np.ndim(efg) == 2:
+            return nmr[0], U[0], S[0]
+        return nmr, U, S
 
     def efg_dist(self, dist, efg=None):
-        """efg_stat's statistics and distributions of one configuration
-        (src/efg.f90:2272-2440).  dist: abi.EfgDistParams.  Rows 0 (all
-        sites), 1..ntype.  Returns a dict with stats [ntype+1][8] (vzzmin,
-        vzzmax, <Vzz>, <|Vzz|>, <eta>, P(Vzz>=0), rho_z, sigma), mU
-        [ntype+1][5], m2U [ntype+1][5][5] and the integer histograms
-        vzz, eta, u [6][ntype+1][PANU+1], s."""
-        n, nt1 = self.n, self.params.ntype + 1
+        """efg_stat's statistics and distributions (src/efg.f90:2272-2440)
+        over one configuration ([natm][6]) or several ([nconf][natm][6]); None
+        for the context's own EFG.  dist: abi.EfgDistParams.  Rows 0 (all
+        sites), 1..ntype.  Returns a dict with stats [nconf][ntype+1][8]
+        (vzzmin, vzzmax, <Vzz>, <|Vzz|>, <eta>, P(Vzz>=0), rho_z, sigma per
+        configuration, as the reference's loop forms them), mU [ntype+1][5],
+        m2U [ntype+1][5][5] and the integer histograms summed over the
+        configurations: vzz, eta, u [6][ntype+1][PANU+1], s."""
+        nt1 = self.params.ntype + 1
         PV, PE, PU, PS = dist.bins()
-        e6 = None if efg is None else np.ascontiguousarray(np.asarray(efg, dtype=np.float64).T)
-        stats, mU, m2U = np.empty((nt1, 8)), np.empty((nt1, 5)), np.empty((nt1, 5, 5))
+        e6, nc = self._efg_input(efg)
+        stats, mU, m2U = np.empty((nc, nt1, 8)), np.empty((nt1, 5)), np.empty((nt1, 5, 5))
         hv = np.empty((nt1, PV + 1), dtype=np.int32)
         he = np.empty((nt1, PE + 1), dtype=np.int32)
         hu = np.empty((6, nt1, PU + 1), dtype=np.int32)
         hs = np.empty((nt1, PS + 1), dtype=np.int32)
-        self._check(lib().mdff_efg_dist(self._h, _dp(e6), C.byref(dist), _dp(stats), _dp(mU), _dp(m2U), _ip(hv),
-                                        _ip(he), _ip(hu), _ip(hs)))
+        self._check(lib().mdff_efg_dist(self._h, nc, _dp(e6), C.byref(dist), _dp(stats), _dp(mU), _dp(m2U),
+                                        _ip(hv), _ip(he), _ip(hu), _ip(hs)))
         return {"stats": stats, "mU": mU, "m2U": m2U, "vzz": hv, "eta": he, "u": hu, "s": hs}
 
     def profile_detail(self):

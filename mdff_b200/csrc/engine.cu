@@ -71,7 +71,9 @@ struct mdff_ctx {
     double* hist = nullptr;
     double* coef = nullptr;
     double *opt_xi = nullptr, *opt_g = nullptr, *opt_h = nullptr, *opt_r0 = nullptr;   // structure optimisation
-    double *efgp_t = nullptr, *efgp_nmr = nullptr, *efgp_u = nullptr, *efgp_s = nullptr;   // EFG post-processing
+    double *efgp_t = nullptr, *efgp_nmr = nullptr, *efgp_part = nullptr;   // EFG post-processing scratch
+    int* efgp_hist = nullptr;
+    size_t efgp_tcap = 0, efgp_ncap = 0, efgp_pcap = 0, efgp_hcap = 0;
     double *ef = nullptr, *efg = nullptr, *fcoul = nullptr;
     PairConst* pc = nullptr;
     NList lv, lc;
@@ -136,6 +138,21 @@ int dalloc(mdff_ctx* ctx, T** ptr, size_t count) {
     if (e != cudaSuccess) return fail(ctx, MDFF_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     ctx->allocs.push_back(p);
     *ptr = (T*)p;
+    return MDFF_OK;
+}
+
+// Grow-only device scratch owned by the context.
+template <class T>
+int dgrow(mdff_ctx* ctx, T** ptr, size_t* cap, size_t need) {
+    if (*ptr && need <= *cap) return MDFF_OK;
+    if (*ptr) {
+        CK(cudaStreamSynchronize(ctx->st));
+        cudaFree(*ptr);
+        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void*)*ptr));
+        *ptr = nullptr;
+    }
+    TRY(dalloc(ctx, ptr, need));
+    *cap = need;
     return MDFF_OK;
 }
 
@@ -1266,128 +1283,159 @@ int opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* R) {
 
 extern "C" {
 
-// EFG post-processing: the tensors (the caller's, or the context's own from
-// the last force evaluation) through k_efg_nmr into device scratch.
-static int efg_post_sites(mdff_ctx* ctx, const double* efg6) {
-    const int n = ctx->n;
-    if (!ctx->efgp_nmr) {
-        TRY(dalloc(ctx, &ctx->efgp_t, 6 * (size_t)n));
-        TRY(dalloc(ctx, &ctx->efgp_nmr, 4 * (size_t)n));
-        TRY(dalloc(ctx, &ctx->efgp_u, 5 * (size_t)n));
-        TRY(dalloc(ctx, &ctx->efgp_s, (size_t)n));
-    }
-    const double* src = ctx->efg;
+// EFG post-processing input: nconf configurations of the caller's tensors
+// [nconf][6][natm] uploaded into context scratch, or (efg6 NULL, nconf 1) the
+// context's EFG of its last force evaluation.
+static int efg_post_input(mdff_ctx* ctx, int nconf, const double* efg6, const double** src) {
+    const size_t n = (size_t)ctx->n;
+    if (nconf < 1) return fail(ctx, MDFF_E_ARG, "EFG post-processing: nconf must be >= 1");
     if (efg6) {
-        CK(cudaMemcpyAsync(ctx->efgp_t, efg6, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, ctx->st));
-        src = ctx->efgp_t;
-    } else if (!(ctx->p.lcoulomb && ctx->p.doefg)) {
-        return fail(ctx, MDFF_E_STATE, "no EFG in the context: pass tensors or evaluate forces with doefg");
+        TRY(dgrow(ctx, &ctx->efgp_t, &ctx->efgp_tcap, 6 * n * nconf));
+        CK(cudaMemcpyAsync(ctx->efgp_t, efg6, sizeof(double) * 6 * n * nconf, cudaMemcpyHostToDevice, ctx->st));
+        *src = ctx->efgp_t;
+    } else {
+        if (nconf != 1) return fail(ctx, MDFF_E_ARG, "EFG post-processing: the context holds one configuration");
+        if (!(ctx->p.lcoulomb && ctx->p.doefg))
+            return fail(ctx, MDFF_E_STATE, "no EFG in the context: pass tensors or evaluate forces with doefg");
+        *src = ctx->efg;
     }
-    k_efg_nmr<<<nb(n), 256, 0, ctx->st>>>(n, src, ctx->efgp_nmr, ctx->efgp_u, ctx->efgp_s);
-    return check_launch(ctx, "efg_nmr");
+    return MDFF_OK;
 }
 
-int mdff_efg_nmr(mdff_ctx* ctx, const double* efg6, double* nmr, double* U, double* S) {
+int mdff_efg_nmr(mdff_ctx* ctx, int nconf, const double* efg6, double* nmr, double* U, double* S) {
     if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
     cudaSetDevice(ctx->p.device);
-    TRY(efg_post_sites(ctx, efg6));
-    const int n = ctx->n;
-    if (nmr) CK(cudaMemcpyAsync(nmr, ctx->efgp_nmr, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, ctx->st));
-    if (U) CK(cudaMemcpyAsync(U, ctx->efgp_u, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, ctx->st));
-    if (S) CK(cudaMemcpyAsync(S, ctx->efgp_s, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+    const double* src = nullptr;
+    TRY(efg_post_input(ctx, nconf, efg6, &src));
+    const size_t n = (size_t)ctx->n;
+    TRY(dgrow(ctx, &ctx->efgp_nmr, &ctx->efgp_ncap, 10 * n * nconf));
+    double* dn = ctx->efgp_nmr;
+    double* du = dn + 4 * n * nconf;
+    double* ds = du + 5 * n * nconf;
+    EfgBins b{};
+    const dim3 grid((unsigned)((n + EFG_THREADS - 1) / EFG_THREADS), (unsigned)nconf);
+    k_efg_sites<false, false><<<grid, EFG_THREADS, 0, ctx->st>>>(ctx->n, src, ctx->type, b, nullptr, nullptr, dn, du,
+                                                                  ds, nullptr);
+    TRY(check_launch(ctx, "efg_sites"));
+    if (nmr) CK(cudaMemcpyAsync(nmr, dn, sizeof(double) * 4 * n * nconf, cudaMemcpyDeviceToHost, ctx->st));
+    if (U) CK(cudaMemcpyAsync(U, du, sizeof(double) * 5 * n * nconf, cudaMemcpyDeviceToHost, ctx->st));
+    if (S) CK(cudaMemcpyAsync(S, ds, sizeof(double) * n * nconf, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return MDFF_OK;
 }
 
-int mdff_efg_dist(mdff_ctx* ctx, const double* efg6, const mdff_efg_dist_params* dp, double* stats, double* mU,
-                  double* m2U, int* dib_vzz, int* dib_eta, int* dib_u, int* dib_s) {
+int mdff_efg_dist(mdff_ctx* ctx, int nconf, const double* efg6, const mdff_efg_dist_params* dp, double* stats,
+                  double* mU, double* m2U, int* dib_vzz, int* dib_eta, int* dib_u, int* dib_s) {
     if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
     if (!dp || !(dp->resvzz > 0.0) || !(dp->reseta > 0.0) || !(dp->resu > 0.0))
         return fail(ctx, MDFF_E_ARG, "mdff_efg_dist: resolutions must be positive");
     if (ctx->ntype > EFG_NT_MAX) return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_efg_dist: at most 16 types");
     cudaSetDevice(ctx->p.device);
-    TRY(efg_post_sites(ctx, efg6));
+    const double* src = nullptr;
+    TRY(efg_post_input(ctx, nconf, efg6, &src));
     const int n = ctx->n, nt1 = ctx->ntype + 1;
-    EfgBins b;
+    EfgBins b{};
     b.vzzmin = dp->vzzmin; b.resvzz = dp->resvzz; b.reseta = dp->reseta; b.umin = dp->umin; b.resu = dp->resu;
-    b.PANeta = (int)(1.0 / dp->reseta);                       // efg_check_tag, src/efg.f90:233-236
-    b.PANvzz = (int)((2.0 * std::fabs(dp->vzzmin)) / dp->resvzz);
-    b.PANU = (int)((2.0 * std::fabs(dp->umin)) / dp->resu);
-    b.PANS = (int)(dp->smax / dp->resu);
+    const double pv = (2.0 * std::fabs(dp->vzzmin)) / dp->resvzz, pe = 1.0 / dp->reseta;
+    const double pu = (2.0 * std::fabs(dp->umin)) / dp->resu, ps = dp->smax / dp->resu;
+    if (!(pv < 1e8 && pe < 1e8 && pu < 1e8 && ps < 1e8 && ps >= 0.0))
+        return fail(ctx, MDFF_E_ARG, "mdff_efg_dist: bin counts out of range");
+    b.PANvzz = (int)pv;                                      // efg_check_tag, src/efg.f90:233-236
+    b.PANeta = (int)pe;
+    b.PANU = (int)pu;
+    b.PANS = (int)ps;
     b.ntype = ctx->ntype;
     const size_t nvzz = (size_t)nt1 * (b.PANvzz + 1), neta = (size_t)nt1 * (b.PANeta + 1);
     const size_t nu = (size_t)6 * nt1 * (b.PANU + 1), ns = (size_t)nt1 * (b.PANS + 1);
-    const int nblk = nb(n);
-    int* hist = nullptr;
-    double* part = nullptr;
-    // histogram and partial scratch for this call only (sizes depend on the bins)
-    CK(cudaMallocAsync((void**)&hist, sizeof(int) * (nvzz + neta + nu + ns + 1), ctx->st));
-    CK(cudaMallocAsync((void**)&part, sizeof(double) * (size_t)nblk * nt1 * EFG_NACC, ctx->st));
-    CK(cudaMemsetAsync(hist, 0, sizeof(int) * (nvzz + neta + nu + ns + 1), ctx->st));
-    int* hv = hist;
-    int* he = hv + nvzz;
-    int* hu = he + neta;
-    int* hs = hu + nu;
-    int* bad = hs + ns;
-    k_efg_dist<<<nblk, 256, 0, ctx->st>>>(n, ctx->type, ctx->efgp_nmr, ctx->efgp_u, ctx->efgp_s, b, hv, he, hu, hs, bad);
-    k_efg_stats<<<nblk, 256, 0, ctx->st>>>(n, ctx->ntype, ctx->type, ctx->efgp_nmr, ctx->efgp_u, part);
-    std::vector<int> hh(nvzz + neta + nu + ns + 1);
-    std::vector<double> pp((size_t)nblk * nt1 * EFG_NACC);
+    const size_t nbins = nvzz + neta + nu + ns;
+    if (nbins > (size_t)1 << 30) return fail(ctx, MDFF_E_ARG, "mdff_efg_dist: too many bins");
+    b.ov = 0; b.oe = (int)nvzz; b.ou = (int)(nvzz + neta); b.os = (int)(nvzz + neta + nu); b.nbins = (int)nbins;
+    const int nblk = (n + EFG_THREADS - 1) / EFG_THREADS;
+    const size_t npart = (size_t)nconf * nblk * nt1 * EFG_NACC, nfin = (size_t)nconf * nt1 * EFG_NACC;
+    TRY(dgrow(ctx, &ctx->efgp_hist, &ctx->efgp_hcap, nbins + 1));
+    TRY(dgrow(ctx, &ctx->efgp_part, &ctx->efgp_pcap, npart + nfin));
+    int* hist = ctx->efgp_hist;
+    double* part = ctx->efgp_part;
+    double* fin = part + npart;
+    CK(cudaMemsetAsync(hist, 0, sizeof(int) * (nbins + 1), ctx->st));
+    const dim3 grid((unsigned)nblk, (unsigned)nconf);
+    if (nbins <= (size_t)EFG_SMEM_BINS)
+        k_efg_sites<true, true><<<grid, EFG_THREADS, sizeof(int) * nbins, ctx->st>>>(
+            n, src, ctx->type, b, hist, part, nullptr, nullptr, nullptr, hist + nbins);
+    else
+        k_efg_sites<true, false><<<grid, EFG_THREADS, 0, ctx->st>>>(n, src, ctx->type, b, hist, part, nullptr,
+                                                                     nullptr, nullptr, hist + nbins);
+    TRY(check_launch(ctx, "efg_sites"));
+    k_efg_stats_fin<<<dim3((unsigned)nt1, (unsigned)nconf), 32, 0, ctx->st>>>(nblk, part, fin);
+    TRY(check_launch(ctx, "efg_stats_fin"));
+    std::vector<int> hh(nbins + 1);
+    std::vector<double> ff(nfin);
     CK(cudaMemcpyAsync(hh.data(), hist, sizeof(int) * hh.size(), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(pp.data(), part, sizeof(double) * pp.size(), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaFreeAsync(hist, ctx->st));
-    CK(cudaFreeAsync(part, ctx->st));
+    CK(cudaMemcpyAsync(ff.data(), fin, sizeof(double) * nfin, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    TRY(check_launch(ctx, "efg_dist"));
-    if (dib_vzz) std::memcpy(dib_vzz, hh.data(), sizeof(int) * nvzz);
-    if (dib_eta) std::memcpy(dib_eta, hh.data() + nvzz, sizeof(int) * neta);
-    if (dib_u) std::memcpy(dib_u, hh.data() + nvzz + neta, sizeof(int) * nu);
-    if (dib_s) std::memcpy(dib_s, hh.data() + nvzz + neta + nu, sizeof(int) * ns);
-    // statistics per type row: blocks summed in order; the running extrema of
-    // the reference start at 0 (src/efg.f90:2163-2164)
-    for (int t = 0; t < nt1; ++t) {
-        double a[EFG_NACC] = {};
-        for (int bl = 0; bl < nblk; ++bl) {
-            const double* q = &pp[((size_t)bl * nt1 + t) * EFG_NACC];
-            for (int k = 0; k < EFG_NACC; ++k)
-                if (k != 6 && k != 7) a[k] += q[k];
-            a[6] = std::min(a[6], q[6]);
-            a[7] = std::max(a[7], q[7]);
+    if (dib_vzz) std::memcpy(dib_vzz, hh.data() + b.ov, sizeof(int) * nvzz);
+    if (dib_eta) std::memcpy(dib_eta, hh.data() + b.oe, sizeof(int) * neta);
+    if (dib_u) std::memcpy(dib_u, hh.data() + b.ou, sizeof(int) * nu);
+    if (dib_s) std::memcpy(dib_s, hh.data() + b.os, sizeof(int) * ns);
+    // Statistics as efg_stat forms them over its configuration loop
+    // (src/efg.f90:2159-2330): the averages are zeroed once before the loop,
+    // so each configuration's sums add to the previous configuration's
+    // averages before the division; the extrema run over all configurations
+    // from 0; <U> and <U U> are totals over all configurations divided by
+    // nconf x sites at the end (:2435-2439), row 0 of <U U> left undivided.
+    std::vector<double> vzzm(nt1, 0.0), vzzma(nt1, 0.0), etam(nt1, 0.0), vzzsq(nt1, 0.0), pvzz(nt1, 0.0);
+    std::vector<double> vmin(nt1, 0.0), vmax(nt1, 0.0), cnt(nt1, 0.0), su(nt1 * 20, 0.0);
+    for (int c = 0; c < nconf; ++c) {
+        for (int t = 0; t < nt1; ++t) {
+            const double* a = &ff[((size_t)c * nt1 + t) * EFG_NACC];
+            const double k = a[5];
+            vzzm[t] += a[0];
+            vzzma[t] += a[1];
+            etam[t] += a[2];
+            vzzsq[t] += a[3];
+            pvzz[t] += a[4];
+            vmin[t] = std::min(vmin[t], a[6]);
+            vmax[t] = std::max(vmax[t], a[7]);
+            for (int q = 0; q < 20; ++q) su[t * 20 + q] += a[8 + q];
+            cnt[t] = k;
+            if (k > 0) {
+                vzzm[t] /= k; vzzsq[t] /= k; vzzma[t] /= k; etam[t] /= k; pvzz[t] /= k;
+            }
+            const double sig = std::sqrt(vzzsq[t] - vzzma[t] * vzzma[t]);
+            if (stats) {
+                double* o = stats + ((size_t)c * nt1 + t) * 8;
+                o[0] = vmin[t];
+                o[1] = vmax[t];
+                o[2] = vzzm[t];
+                o[3] = vzzma[t];
+                o[4] = etam[t];
+                o[5] = pvzz[t];
+                o[6] = vzzma[t] != 0.0 ? sig / vzzma[t] : 0.0;   // rho_z
+                o[7] = sig;                                      // sigmavzz
+            }
         }
-        const double cnt = a[5];
-        // <U_k> per row; <U_k U_l> (k <= l) per type, left as the plain sum for
-        // row 0 as the reference leaves it (src/efg.f90:2435-2439)
+    }
+    for (int t = 0; t < nt1; ++t) {
+        const double den = (double)nconf * cnt[t];
         if (mU)
-            for (int k = 0; k < 5; ++k) mU[(size_t)t * 5 + k] = cnt > 0 ? a[8 + k] / cnt : 0.0;
+            for (int k = 0; k < 5; ++k) mU[(size_t)t * 5 + k] = den > 0 ? su[t * 20 + k] / den : 0.0;
         if (m2U) {
-            int m = 13;
+            int m = 5;
             for (int k = 0; k < 5; ++k)
                 for (int l = 0; l < 5; ++l) {
                     double v = 0.0;
                     if (l >= k) {
-                        v = a[m++];
-                        if (t > 0) v = cnt > 0 ? v / cnt : 0.0;
+                        v = su[t * 20 + m++];
+                        if (t > 0) v = den > 0 ? v / den : 0.0;
                     }
                     m2U[((size_t)t * 5 + k) * 5 + l] = v;
                 }
         }
-        if (stats) {
-            double* o = stats + (size_t)t * 8;
-            o[0] = a[6];                                  // vzzmini
-            o[1] = a[7];                                  // vzzmaxi
-            o[2] = cnt > 0 ? a[0] / cnt : 0.0;            // vzzm
-            o[3] = cnt > 0 ? a[1] / cnt : 0.0;            // vzzma
-            o[4] = cnt > 0 ? a[2] / cnt : 0.0;            // etam
-            o[5] = cnt > 0 ? a[4] / cnt : 0.0;            // pvzz
-            const double vzzsq = cnt > 0 ? a[3] / cnt : 0.0;
-            const double sig = std::sqrt(vzzsq - o[3] * o[3]);
-            o[7] = sig;                                   // sigmavzz
-            o[6] = o[3] != 0.0 ? sig / o[3] : 0.0;        // rho_z
-        }
     }
-    const int flag = hh[nvzz + neta + nu + ns];
-    if (flag) return fail(ctx, MDFF_E_ARG, "EFG value outside the distribution range (vzzmin, umin, smax) -- code " +
-                                               std::to_string(flag));
+    const int flag = hh[nbins];
+    if (flag)
+        return fail(ctx, MDFF_E_ARG,
+                    "EFG value outside the distribution range (vzzmin, umin, smax) -- code " + std::to_string(flag));
     return MDFF_OK;
 }
 

@@ -80,6 +80,38 @@ def test_dist_matches_oracle():
     assert np.allclose(got["m2U"], ref["m2U"], rtol=1e-12, atol=1e-14)
 
 
+def test_dist_over_configurations():
+    # several configurations in one call: histograms summed, statistics formed
+    # as the reference's configuration loop forms them
+    e, s = engine_for()
+    rng = np.random.default_rng(8)
+    efg = np.stack([random_traceless(e.n, rng, scale=0.5 + 0.25 * c) for c in range(5)])
+    kw = dict(vzzmin=-10.0, resvzz=0.05, reseta=0.02, umin=-8.0, resu=0.05, smax=10.0)
+    got = e.efg_dist(dist_params(**kw), efg)
+    ref = efg_stat.efg_dist(efg, s["itype"], s["params"].ntype, **kw)
+    for k in ("vzz", "eta", "u", "s"):
+        assert np.array_equal(got[k], ref[k]), k
+    assert got["stats"].shape == (5, 3, 8)
+    for k in ("stats", "mU", "m2U"):
+        assert np.allclose(got[k], ref[k], rtol=1e-12, atol=1e-14), k
+    nmr, U, S = e.efg_nmr(efg)
+    assert nmr.shape == (5, e.n, 4)
+    assert np.max(np.abs(nmr[:, :, 2] - ref["nmr"][:, :, 2])) <= 1e-12 * np.abs(efg).max()
+    assert np.max(np.abs(U - ref["U"])) <= 1e-15 * np.abs(efg).max()
+
+
+def test_dist_many_bins_global_histograms():
+    # more bins than fit the block-private shared-memory histograms
+    e, s = engine_for()
+    efg = random_traceless(e.n, np.random.default_rng(12))
+    kw = dict(vzzmin=-8.0, resvzz=0.002, reseta=0.001, umin=-6.0, resu=0.002, smax=8.0)
+    got = e.efg_dist(dist_params(**kw), efg)
+    ref = efg_stat.efg_dist(efg, s["itype"], s["params"].ntype, **kw)
+    assert got["u"].size > 12288
+    for k in ("vzz", "eta", "u", "s"):
+        assert np.array_equal(got[k], ref[k]), k
+
+
 def test_dist_of_engine_efg():
     # tensors of a PIM force evaluation (doefg) taken from the context itself
     s = systems.mgo_pim(grid=(8, 8, 8), rc=6.0, alpha=0.5, kmax=7, vacancy_frac=0.02, seed=4)

@@ -96,18 +96,18 @@ def test_statistics_and_histograms_bookkeeping():
             assert d["u"][k, r].sum() == counts[r]
         assert d["u"][5, r].sum() == 4 * counts[r]
     # row statistics from the per-site values
-    nmr = d["nmr"]
+    nmr = d["nmr"][0]
     for r in range(ntype + 1):
         sel = np.ones(n, bool) if r == 0 else itype == r
         v = nmr[sel, 2]
-        st = d["stats"][r]
+        st = d["stats"][0, r]
         assert abs(st[0] - min(0.0, v.min())) < 1e-15 and abs(st[1] - max(0.0, v.max())) < 1e-15
         assert abs(st[2] - v.mean()) < 1e-13 and abs(st[3] - np.abs(v).mean()) < 1e-13
         assert abs(st[4] - nmr[sel, 3].mean()) < 1e-13
         assert abs(st[5] - np.mean(v >= 0)) < 1e-15
         sig = math.sqrt(np.mean(v * v) - np.abs(v).mean() ** 2)
         assert abs(st[7] - sig) < 1e-12 and abs(st[6] - sig / np.abs(v).mean()) < 1e-12
-        U = d["U"][sel]
+        U = d["U"][0][sel]
         assert np.allclose(d["mU"][r], U.mean(axis=0), rtol=0, atol=1e-13)
         m2 = np.triu(U.T @ U)
         if r > 0:
@@ -117,6 +117,27 @@ def test_statistics_and_histograms_bookkeeping():
     ia = 5
     kv = int((nmr[ia, 2] + 8.0) / 0.1) + 1
     assert d["vzz"][0, kv] >= 1 and d["vzz"][itype[ia], kv] >= 1
+
+
+def test_configurations_carry_the_previous_averages():
+    # two configurations: the reference zeroes its sums once, so the second
+    # configuration's averages include the first configuration's averages
+    rng = np.random.default_rng(9)
+    n = 60
+    itype = np.ones(n, int)
+    e = np.stack([random_traceless(n, rng), random_traceless(n, rng)])
+    kw = dict(vzzmin=-8.0, resvzz=0.1, reseta=0.05, umin=-6.0, resu=0.1, smax=8.0)
+    d2 = efg_stat.efg_dist(e, itype, 1, **kw)
+    a = efg_stat.efg_dist(e[0], itype, 1, **kw)
+    b = efg_stat.efg_dist(e[1], itype, 1, **kw)
+    assert np.array_equal(d2["stats"][0], a["stats"][0])
+    v1 = a["nmr"][0][:, 2]
+    v2 = b["nmr"][0][:, 2]
+    assert abs(d2["stats"][1, 0, 2] - (v1.mean() + v2.sum()) / n) < 1e-13
+    assert d2["stats"][1, 0, 0] == min(0.0, v1.min(), v2.min())
+    for k in ("vzz", "eta", "u", "s"):
+        assert np.array_equal(d2[k], a[k] + b[k])
+    assert np.allclose(d2["mU"], (a["mU"] + b["mU"]) / 2, rtol=0, atol=1e-14)
 
 
 def test_out_of_range_raises():

@@ -258,12 +258,16 @@ int  mdff_stream(mdff_ctx* ctx, void** stream);
  * clears them when reset != 0. */
 int  mdff_profile(mdff_ctx* ctx, int enable);
 int  mdff_profile_get(mdff_ctx* ctx, double ms[8], long long count[8], long long* launches, int reset);
-/* Detail timers inside groups 3 and 4 (mixed path, tensor-core k-space): the
- * structure-factor kernel [0] and the field kernel [1] alone -- accumulated
- * milliseconds, launches, and the int8 digit-product operations (2 M N K per
- * product, six products, unpadded problem) they were launched for; cleared
- * with the groups.  No reference counterpart. */
-int  mdff_profile_detail(mdff_ctx* ctx, double ms[2], long long count[2], double ops[2]);
+/* Detail timers of single kernels: the tensor-core structure-factor kernel
+ * [0] and field kernel [1] (mixed path, inside groups 3 and 4) with the int8
+ * digit-product operations they were launched for (2 M N K per product, six
+ * products, unpadded problem), and the EFG post-processing site kernel [2]
+ * with the bytes it must read (52 per site: tensor and type) -- accumulated
+ * milliseconds, launches and work; cleared with the groups.  No reference
+ * counterpart. */
+#define MDFF_NDETAIL 3
+int  mdff_profile_detail(mdff_ctx* ctx, double ms[MDFF_NDETAIL], long long count[MDFF_NDETAIL],
+                         double ops[MDFF_NDETAIL]);
 
 /* Sizes of the reciprocal-space sums of the context (no reference
  * counterpart): out[0] the k rectangle the kernels sweep, out[1] the k-vectors

@@ -260,14 +260,31 @@ class Engine:
                                         _ip(hv), _ip(he), _ip(hu), _ip(hs)))
         return {"stats": stats, "mU": mU, "m2U": m2U, "vzz": hv, "eta": he, "u": hu, "s": hs}
 
+    def efg_dist_ptr(self, dist, ptr, nconf):
+        """efg_dist over tensors at a raw address of [nconf][6][natm] float64:
+        this GPU's memory (read in place, e.g. a torch CUDA tensor's
+        data_ptr()) or host memory (uploaded; pinned memory copies fastest)."""
+        nt1 = self.params.ntype + 1
+        PV, PE, PU, PS = dist.bins()
+        stats, mU, m2U = np.empty((nconf, nt1, 8)), np.empty((nt1, 5)), np.empty((nt1, 5, 5))
+        hv = np.empty((nt1, PV + 1), dtype=np.int32)
+        he = np.empty((nt1, PE + 1), dtype=np.int32)
+        hu = np.empty((6, nt1, PU + 1), dtype=np.int32)
+        hs = np.empty((nt1, PS + 1), dtype=np.int32)
+        self._check(lib().mdff_efg_dist(self._h, int(nconf), C.cast(C.c_void_p(ptr), C.POINTER(C.c_double)),
+                                        C.byref(dist), _dp(stats), _dp(mU), _dp(m2U), _ip(hv), _ip(he), _ip(hu),
+                                        _ip(hs)))
+        return {"stats": stats, "mU": mU, "m2U": m2U, "vzz": hv, "eta": he, "u": hu, "s": hs}
+
     def profile_detail(self):
-        """The tensor-core k-space kernels alone (mixed path): per kernel the
-        accumulated ms, launches and int8 digit-product operations."""
-        ms, ops = np.zeros(2), np.zeros(2)
-        cnt = (C.c_longlong * 2)()
+        """Single-kernel detail timers: the tensor-core k-space kernels (mixed
+        path; ops = int8 digit-product operations) and the EFG site kernel
+        (ops = bytes it reads): accumulated ms, launches and work."""
+        ms, ops = np.zeros(3), np.zeros(3)
+        cnt = (C.c_longlong * 3)()
         self._check(lib().mdff_profile_detail(self._h, _dp(ms), cnt, _dp(ops)))
         return {k: {"ms": float(ms[i]), "count": int(cnt[i]), "ops": float(ops[i])}
-                for i, k in enumerate(("sfac_tc", "kfield_tc"))}
+                for i, k in enumerate(("sfac_tc", "kfield_tc", "efg_sites"))}
 
     def nlist_build(self):
         self._check(lib().mdff_nlist_build(self._h))

@@ -1284,11 +1284,21 @@ int opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* R) {
 extern "C" {
 
 // EFG post-processing input: nconf configurations of the caller's tensors
-// [nconf][6][natm] uploaded into context scratch, or (efg6 NULL, nconf 1) the
-// context's EFG of its last force evaluation.
+// [nconf][6][natm] -- read in place when they are in device memory, else
+// uploaded into context scratch -- or (efg6 NULL, nconf 1) the context's EFG of
+// its last force evaluation.
 static int efg_post_input(mdff_ctx* ctx, int nconf, const double* efg6, const double** src) {
     const size_t n = (size_t)ctx->n;
     if (nconf < 1) return fail(ctx, MDFF_E_ARG, "EFG post-processing: nconf must be >= 1");
+    cudaPointerAttributes pa{};
+    if (efg6 && cudaPointerGetAttributes(&pa, efg6) == cudaSuccess &&
+        (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged)) {
+        if (pa.device != ctx->p.device)
+            return fail(ctx, MDFF_E_ARG, "EFG post-processing: tensors on another device");
+        *src = efg6;
+        return MDFF_OK;
+    }
+    cudaGetLastError();
     if (efg6) {
         TRY(dgrow(ctx, &ctx->efgp_t, &ctx->efgp_tcap, 6 * n * nconf));
         CK(cudaMemcpyAsync(ctx->efgp_t, efg6, sizeof(double) * 6 * n * nconf, cudaMemcpyHostToDevice, ctx->st));
@@ -1302,6 +1312,13 @@ static int efg_post_input(mdff_ctx* ctx, int nconf, const double* efg6, const do
     return MDFF_OK;
 }
 
+// persistent grid of the EFG site kernel: three blocks per SM at most
+static int efg_grid(mdff_ctx* ctx, int nchunk) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->p.device);
+    return std::max(1, std::min(nchunk, 3 * sms));
+}
+
 int mdff_efg_nmr(mdff_ctx* ctx, int nconf, const double* efg6, double* nmr, double* U, double* S) {
     if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
     cudaSetDevice(ctx->p.device);
@@ -1313,9 +1330,9 @@ int mdff_efg_nmr(mdff_ctx* ctx, int nconf, const double* efg6, double* nmr, doub
     double* du = dn + 4 * n * nconf;
     double* ds = du + 5 * n * nconf;
     EfgBins b{};
-    const dim3 grid((unsigned)((n + EFG_THREADS - 1) / EFG_THREADS), (unsigned)nconf);
-    k_efg_sites<false, false><<<grid, EFG_THREADS, 0, ctx->st>>>(ctx->n, src, ctx->type, b, nullptr, nullptr, dn, du,
-                                                                  ds, nullptr);
+    const int nblk = (int)((n + EFG_THREADS - 1) / EFG_THREADS), nchunk = nblk * nconf;
+    k_efg_sites<false, false><<<efg_grid(ctx, nchunk), EFG_THREADS, 0, ctx->st>>>(
+        ctx->n, nblk, nchunk, src, ctx->type, b, nullptr, nullptr, dn, du, ds, nullptr);
     TRY(check_launch(ctx, "efg_sites"));
     if (nmr) CK(cudaMemcpyAsync(nmr, dn, sizeof(double) * 4 * n * nconf, cudaMemcpyDeviceToHost, ctx->st));
     if (U) CK(cudaMemcpyAsync(U, du, sizeof(double) * 5 * n * nconf, cudaMemcpyDeviceToHost, ctx->st));
@@ -1336,6 +1353,7 @@ int mdff_efg_dist(mdff_ctx* ctx, int nconf, const double* efg6, const mdff_efg_d
     const int n = ctx->n, nt1 = ctx->ntype + 1;
     EfgBins b{};
     b.vzzmin = dp->vzzmin; b.resvzz = dp->resvzz; b.reseta = dp->reseta; b.umin = dp->umin; b.resu = dp->resu;
+    b.ivzz = 1.0 / dp->resvzz; b.ieta = 1.0 / dp->reseta; b.iu = 1.0 / dp->resu;
     const double pv = (2.0 * std::fabs(dp->vzzmin)) / dp->resvzz, pe = 1.0 / dp->reseta;
     const double pu = (2.0 * std::fabs(dp->umin)) / dp->resu, ps = dp->smax / dp->resu;
     if (!(pv < 1e8 && pe < 1e8 && pu < 1e8 && ps < 1e8 && ps >= 0.0))
@@ -1350,24 +1368,34 @@ int mdff_efg_dist(mdff_ctx* ctx, int nconf, const double* efg6, const mdff_efg_d
     const size_t nbins = nvzz + neta + nu + ns;
     if (nbins > (size_t)1 << 30) return fail(ctx, MDFF_E_ARG, "mdff_efg_dist: too many bins");
     b.ov = 0; b.oe = (int)nvzz; b.ou = (int)(nvzz + neta); b.os = (int)(nvzz + neta + nu); b.nbins = (int)nbins;
+    const int nt = ctx->ntype;
+    b.cv = 0;
+    b.ce = b.cv + nt * (b.PANvzz + 1);
+    b.cu = b.ce + nt * (b.PANeta + 1);
+    b.cs = b.cu + 5 * nt * (b.PANU + 1);
+    b.ncomp = b.cs + nt * (b.PANS + 1);
     const int nblk = (n + EFG_THREADS - 1) / EFG_THREADS;
-    const size_t npart = (size_t)nconf * nblk * nt1 * EFG_NACC, nfin = (size_t)nconf * nt1 * EFG_NACC;
+    const size_t npart = (size_t)nconf * nblk * nt * EFG_NACC, nfin = (size_t)nconf * nt1 * EFG_NACC;
     TRY(dgrow(ctx, &ctx->efgp_hist, &ctx->efgp_hcap, nbins + 1));
     TRY(dgrow(ctx, &ctx->efgp_part, &ctx->efgp_pcap, npart + nfin));
     int* hist = ctx->efgp_hist;
     double* part = ctx->efgp_part;
     double* fin = part + npart;
     CK(cudaMemsetAsync(hist, 0, sizeof(int) * (nbins + 1), ctx->st));
-    const dim3 grid((unsigned)nblk, (unsigned)nconf);
-    if (nbins <= (size_t)EFG_SMEM_BINS)
-        k_efg_sites<true, true><<<grid, EFG_THREADS, sizeof(int) * nbins, ctx->st>>>(
-            n, src, ctx->type, b, hist, part, nullptr, nullptr, nullptr, hist + nbins);
+    const int nchunk = nblk * nconf, grid = efg_grid(ctx, nchunk);
+    ctx->prof.begin(PK_OTHER);
+    ctx->prof.detail_begin(PD_EFG_SITES);
+    if (b.ncomp <= EFG_SMEM_BINS)
+        k_efg_sites<true, true><<<grid, EFG_THREADS, sizeof(int) * b.ncomp, ctx->st>>>(
+            n, nblk, nchunk, src, ctx->type, b, hist, part, nullptr, nullptr, nullptr, hist + nbins);
     else
-        k_efg_sites<true, false><<<grid, EFG_THREADS, 0, ctx->st>>>(n, src, ctx->type, b, hist, part, nullptr,
-                                                                     nullptr, nullptr, hist + nbins);
+        k_efg_sites<true, false><<<grid, EFG_THREADS, 0, ctx->st>>>(n, nblk, nchunk, src, ctx->type, b, hist, part,
+                                                                     nullptr, nullptr, nullptr, hist + nbins);
     TRY(check_launch(ctx, "efg_sites"));
-    k_efg_stats_fin<<<dim3((unsigned)nt1, (unsigned)nconf), 32, 0, ctx->st>>>(nblk, part, fin);
+    ctx->prof.detail_end(PD_EFG_SITES, 52.0 * n * nconf);
+    k_efg_stats_fin<<<dim3((unsigned)nt1, (unsigned)nconf), EFG_THREADS, 0, ctx->st>>>(nblk, nt, part, fin);
     TRY(check_launch(ctx, "efg_stats_fin"));
+    ctx->prof.end(2);
     std::vector<int> hh(nbins + 1);
     std::vector<double> ff(nfin);
     CK(cudaMemcpyAsync(hh.data(), hist, sizeof(int) * hh.size(), cudaMemcpyDeviceToHost, ctx->st));
@@ -1394,9 +1422,9 @@ int mdff_efg_dist(mdff_ctx* ctx, int nconf, const double* efg6, const mdff_efg_d
             etam[t] += a[2];
             vzzsq[t] += a[3];
             pvzz[t] += a[4];
-            vmin[t] = std::min(vmin[t], a[6]);
-            vmax[t] = std::max(vmax[t], a[7]);
-            for (int q = 0; q < 20; ++q) su[t * 20 + q] += a[8 + q];
+            vmin[t] = std::min(vmin[t], a[26]);
+            vmax[t] = std::max(vmax[t], a[27]);
+            for (int q = 0; q < 20; ++q) su[t * 20 + q] += a[6 + q];
             cnt[t] = k;
             if (k > 0) {
                 vzzm[t] /= k; vzzsq[t] /= k; vzzma[t] /= k; etam[t] /= k; pvzz[t] /= k;
@@ -1527,7 +1555,9 @@ int mdff_measure_tensor(int device, double out[3]) {
     return MDFF_OK;
 }
 
-int mdff_profile_detail(mdff_ctx* ctx, double ms[2], long long count[2], double ops[2]) {
+int mdff_profile_detail(mdff_ctx* ctx, double ms[MDFF_NDETAIL], long long count[MDFF_NDETAIL],
+                        double ops[MDFF_NDETAIL]) {
+    static_assert(PD_NDETAIL == MDFF_NDETAIL, "detail timer count");
     if (!ctx) return MDFF_E_ARG;
     cudaSetDevice(ctx->p.device);
     CK(cudaStreamSynchronize(ctx->st));

@@ -46,9 +46,10 @@ struct PairConst {
 // counterpart of the reference's MPI_WTIME accumulators, src/time.f90:35-73)
 // and a count of kernel launches.
 enum ProfKind { PK_NLIST = 0, PK_PAIR, PK_DIR, PK_SFAC, PK_KFIELD, PK_SOLVER, PK_INTEGRATE, PK_OTHER, PK_NKIND };
-// Detail timers (inside the groups): the tensor-core structure factor and
-// field kernels alone, with the int8 MMA operations they were launched for.
-enum ProfDetail { PD_TC_SFAC = 0, PD_TC_FIELD, PD_NDETAIL };
+// Detail timers of single kernels: the tensor-core structure factor and field
+// kernels with the int8 MMA operations they were launched for, the EFG site
+// kernel with the bytes it reads.
+enum ProfDetail { PD_TC_SFAC = 0, PD_TC_FIELD, PD_EFG_SITES, PD_NDETAIL };
 struct Prof {
     bool on = false;
     cudaStream_t st = nullptr;

@@ -112,6 +112,19 @@ def test_dist_many_bins_global_histograms():
         assert np.array_equal(got[k], ref[k]), k
 
 
+def test_dist_from_device_memory():
+    # tensors already on the GPU are read in place and give the same answer
+    import torch
+    e, s = engine_for()
+    efg = np.stack([random_traceless(e.n, np.random.default_rng(c), scale=0.8) for c in range(3)])
+    kw = dict(vzzmin=-8.0, resvzz=0.05, reseta=0.02, umin=-6.0, resu=0.05, smax=8.0)
+    t = torch.from_numpy(np.ascontiguousarray(efg.transpose(0, 2, 1))).cuda()
+    got = e.efg_dist_ptr(dist_params(**kw), t.data_ptr(), 3)
+    ref = e.efg_dist(dist_params(**kw), efg)
+    for k in ("vzz", "eta", "u", "s", "stats", "mU", "m2U"):
+        assert np.array_equal(got[k], ref[k]), k
+
+
 def test_dist_of_engine_efg():
     # tensors of a PIM force evaluation (doefg) taken from the context itself
     s = systems.mgo_pim(grid=(8, 8, 8), rc=6.0, alpha=0.5, kmax=7, vacancy_frac=0.02, seed=4)

@@ -459,6 +459,69 @@ int  mdff_rec_energy_noalloc(int device, int natm, const double* rx, const doubl
                              const double* q, const double A[9], double alpha, const int kmax[3],
                              void* stream, double* u_rec, long long* scratch_needed);
 
+/* ---- on-disk formats and streaming (TRAJFF, CONTFF, EFGALL, DIPFF, EFALL) ----
+ * File kinds and their reference writers: TRAJFF write_trajff_xyz
+ * (src/config.f90:539-628), CONTFF write_CONTFF (src/config.f90:206-250),
+ * EFGALL write_EFGALL (src/field.f90:4140-4195), DIPFF write_DIPFF
+ * (src/field.f90:4051-4083), EFALL write_EFALL (src/field.f90:4205-4240).
+ * iformat 0 = Fortran unformatted sequential (4-byte record markers; TRAJFF
+ * and EFGALL), else formatted.  data (TRAJFF): trajff_data as bits,
+ * 0 = rnn, MDFF_DATA_V = rvn, MDFF_DATA_F = rnf, both = rvf. */
+#define MDFF_FILE_TRAJFF 0
+#define MDFF_FILE_CONTFF 1
+#define MDFF_FILE_EFGALL 2
+#define MDFF_FILE_DIPFF  3
+#define MDFF_FILE_EFALL  4
+#define MDFF_DATA_V 1
+#define MDFF_DATA_F 2
+
+/* Frame header: the config module's natm, system, simu_cell%A (column-major:
+ * A[0..2] = first lattice vector), ntype, atypei, natmi. */
+typedef struct mdff_frame_header {
+    int natm, ntype;
+    double A[9];
+    char system[60];                 /* blank padded, not NUL terminated */
+    char atypei[MDFF_NTYPE_MAX][3];  /* blank padded */
+    int natmi[MDFF_NTYPE_MAX];
+} mdff_frame_header;
+
+/* One frame formatted on the host (no device use).  itype: 1-based type per
+ * atom.  cols: [ncol][natm] -- TRAJFF: x y z [vx vy vz] [fx fy fz] (by data),
+ * CONTFF: the nine of rvf, EFGALL: xx yy zz xy xz yz, DIPFF: mux muy muz,
+ * EFALL: Ex Ey Ez; positions are written as given (the streaming writer folds
+ * them into the cell first, as the reference's writers do).  out: cap bytes;
+ * *len receives the frame's length (when cap is too small nothing is written
+ * and MDFF_E_ARG is returned with *len the size needed). */
+int  mdff_io_format(int file, int iformat, int data, const mdff_frame_header* h, const int* itype,
+                    const double* cols, char* out, size_t cap, size_t* len);
+
+/* Streaming writer bound to a context: each mdff_writer_frame snapshots the
+ * context's current state on its stream and returns; a copy stream and a
+ * writer thread bring the frame to the file (appended; CONTFF rewritten).
+ * h supplies system and the type labels (natm, ntype, natmi and the cell come
+ * from the context).  nslot frames may be in flight (>= 1).  EFGALL / DIPFF /
+ * EFALL take the tensors, dipoles or fields of the last force evaluation
+ * (doefg / lcoulomb as the reference requires).  Errors of the background
+ * write are returned by the next mdff_writer_frame or by mdff_writer_close,
+ * which drains the queue, closes the file and frees the writer. */
+typedef struct mdff_writer mdff_writer;
+int  mdff_writer_open(mdff_ctx* ctx, const char* path, int file, int iformat, int data, const mdff_frame_header* h,
+                      int nslot, mdff_writer** w);
+int  mdff_writer_frame(mdff_writer* w);
+int  mdff_writer_close(mdff_writer* w);
+
+/* Checkpoint of the whole time-integration state: what the reference restarts
+ * from (CONTFF's positions, velocities, forces) plus what it cannot restore
+ * (Nose-Hoover chain variables, the induced-dipole predictor history, the
+ * neighbour-list reference positions, the step counter, the tuned launch
+ * shapes), so that a restarted run continues bit for bit.
+ * mdff_checkpoint_save writes into buf (cap bytes; *len the size; buf NULL to
+ * query; MDFF_E_ARG when cap is too small).  mdff_checkpoint_load restores it
+ * into a context created with the same parameters and system
+ * (mdff_set_system), in place of mdff_md_start. */
+int  mdff_checkpoint_save(mdff_ctx* ctx, void* buf, size_t cap, size_t* len);
+int  mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,14 @@ def lib():
         L.mdff_measure_tensor.argtypes = [C.c_int, dp]
         L.mdff_opt_sastry.argtypes = [vp, C.c_int, C.POINTER(abi.OptResult)]
         L.mdff_profile_detail.argtypes = [vp, dp, C.POINTER(C.c_longlong), dp]
+        L.mdff_io_format.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(abi.FrameHeader), ip, dp, C.c_char_p,
+                                     C.c_size_t, C.POINTER(C.c_size_t)]
+        L.mdff_writer_open.argtypes = [vp, C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(abi.FrameHeader),
+                                       C.c_int, C.POINTER(vp)]
+        L.mdff_writer_frame.argtypes = [vp]
+        L.mdff_writer_close.argtypes = [vp]
+        L.mdff_checkpoint_save.argtypes = [vp, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]
+        L.mdff_checkpoint_load.argtypes = [vp, C.c_void_p, C.c_size_t]
         L.mdff_efg_nmr.argtypes = [vp, C.c_int, dp, dp, dp, dp]
         L.mdff_efg_dist.argtypes = [vp, C.c_int, dp, C.POINTER(abi.EfgDistParams), dp, dp, dp, ip, ip, ip, ip]
         L.mdff_struct_size.argtypes = [C.c_int]
@@ -259,6 +267,25 @@ class Engine:
         self._check(lib().mdff_efg_dist(self._h, nc, _dp(e6), C.byref(dist), _dp(stats), _dp(mU), _dp(m2U),
                                         _ip(hv), _ip(he), _ip(hu), _ip(hs)))
         return {"stats": stats, "mU": mU, "m2U": m2U, "vzz": hv, "eta": he, "u": hu, "s": hs}
+
+    def checkpoint(self):
+        """The whole time-integration state as bytes (mdff_checkpoint_save)."""
+        n = C.c_size_t()
+        self._check(lib().mdff_checkpoint_save(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        self._check(lib().mdff_checkpoint_save(self._h, buf, n.value, C.byref(n)))
+        return buf.raw[:n.value]
+
+    def restore(self, data):
+        """Continue from a checkpoint of an engine with the same parameters
+        and system (mdff_checkpoint_load), in place of md_start."""
+        buf = C.create_string_buffer(bytes(data), len(data))
+        self._check(lib().mdff_checkpoint_load(self._h, buf, len(data)))
+
+    def writer(self, path, kind, iformat=1, data="rvf", system="", labels=(), nslot=4):
+        """A streaming writer of this engine's frames (mdff_writer_open)."""
+        from .io import Writer
+        return Writer(self, path, kind, iformat, data, system, labels, nslot)
 
     def efg_dist_ptr(self, dist, ptr, nconf):
         """efg_dist over tensors at a raw address of [nconf][6][natm] float64:

@@ -100,6 +100,18 @@ class OptResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
+FILE_TRAJFF, FILE_CONTFF, FILE_EFGALL, FILE_DIPFF, FILE_EFALL = 0, 1, 2, 3, 4
+DATA_V, DATA_F = 1, 2
+TRAJ_DATA = {"rnn": 0, "rvn": DATA_V, "rnf": DATA_F, "rvf": DATA_V | DATA_F}
+
+
+class FrameHeader(C.Structure):
+    """mdff_frame_header: natm, system, simu_cell%A (column-major), ntype,
+    atypei, natmi of one frame."""
+    _fields_ = [("natm", C.c_int), ("ntype", C.c_int), ("A", C.c_double * 9), ("system", C.c_char * 60),
+                ("atypei", (C.c_char * 3) * NTYPE_MAX), ("natmi", C.c_int * NTYPE_MAX)]
+
+
 class EfgDistParams(C.Structure):
     """mdff_efg_dist_params: efg_stat's distribution settings (efgtag:
     vzzmin, resvzz, reseta, umin, resu, smax; src/efg.f90:171-190)."""

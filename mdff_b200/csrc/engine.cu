@@ -23,6 +23,10 @@
 #include "integrate.cuh"
 #include "opt.cuh"
 #include "efg_post.cuh"
+#include "io.cuh"
+#include <condition_variable>
+#include <deque>
+#include <thread>
 #include "peaks.cuh"
 
 using namespace mdff;
@@ -352,8 +356,9 @@ int ensure_lists(mdff_ctx* ctx, int cap) {
     return MDFF_OK;
 }
 
-// vnlist_pbc (src/tools.f90:274-370): both lists at the current positions.
-int build_lists(mdff_ctx* ctx, double skin) {
+// vnlist_pbc (src/tools.f90:274-370): both lists at the current positions
+// (from_frac: at the fractional coordinates already in sx, sy, sz).
+int build_lists(mdff_ctx* ctx, double skin, bool from_frac = false) {
     const int n = ctx->n;
     double rl = rlist_max(ctx, skin);
     if (rl <= 0.0) return MDFF_OK;
@@ -370,7 +375,7 @@ int build_lists(mdff_ctx* ctx, double skin) {
         g.ncell_alloc = g.ncell;
     }
     ctx->prof.begin(PK_NLIST);
-    launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
+    if (!from_frac) launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
     launch_bin(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, g);
     ctx->prof.end(5);
     bool nonb = ctx->p.lnmlj || ctx->p.lbmhft || ctx->p.lbmhftd || ctx->p.lmorse;
@@ -2300,3 +2305,417 @@ extern "C" int mdff_rec_energy_noalloc(int device, int natm, const double* rx, c
     if (prev != device) cudaSetDevice(prev);
     return rc;
 }
+
+// ---------------------------------------------------------------------------
+// On-disk formats, the streaming writer and checkpoints.
+extern "C" {
+
+int mdff_io_format(int file, int iformat, int data, const mdff_frame_header* h, const int* itype,
+                   const double* cols, char* out, size_t cap, size_t* len) {
+    if (!h || !itype || !cols || !len) return MDFF_E_ARG;
+    std::string o;
+    const int rc = mdff::io::format_frame(file, iformat, data, *h, itype, cols, o);
+    if (rc != MDFF_OK) return rc;
+    *len = o.size();
+    if (!out || cap < o.size()) return MDFF_E_ARG;
+    std::memcpy(out, o.data(), o.size());
+    return MDFF_OK;
+}
+
+}  // extern "C"
+
+struct mdff_writer {
+    mdff_ctx* ctx = nullptr;
+    int file = 0, iformat = 1, data = 0, ncol = 0, nslot = 0, device = 0;
+    std::string path;
+    mdff_frame_header h{};
+    std::vector<int> itype;                 // 1-based, host
+    std::FILE* f = nullptr;
+    cudaStream_t cs = nullptr;
+    double* dbuf = nullptr;                 // [nslot][ncol][n] device snapshots
+    std::vector<double*> hbuf;              // pinned host copies
+    std::vector<cudaEvent_t> ev_snap, ev_copy;
+    std::vector<mdff_frame_header> hslot;   // header (cell) of each slot's frame
+    std::thread th;
+    std::mutex m;
+    std::condition_variable cv;
+    std::deque<int> queue;
+    std::vector<int> free_slots;
+    bool stop = false;
+    int err = MDFF_OK;
+    std::string errmsg;
+};
+
+namespace {
+
+void writer_loop(mdff_writer* w) {
+    cudaSetDevice(w->device);
+    std::string out;
+    for (;;) {
+        int s;
+        {
+            std::unique_lock<std::mutex> lk(w->m);
+            w->cv.wait(lk, [&] { return w->stop || !w->queue.empty(); });
+            if (w->queue.empty()) break;
+            s = w->queue.front();
+            w->queue.pop_front();
+        }
+        int rc = MDFF_OK;
+        std::string msg;
+        if (cudaEventSynchronize(w->ev_copy[s]) != cudaSuccess) {
+            rc = MDFF_E_CUDA;
+            msg = "writer: device copy failed";
+        } else {
+            out.clear();
+            rc = mdff::io::format_frame(w->file, w->iformat, w->data, w->hslot[s], w->itype.data(), w->hbuf[s], out);
+            if (rc != MDFF_OK) msg = "writer: frame could not be formatted";
+            if (rc == MDFF_OK && w->file == MDFF_FILE_CONTFF) {   // rewritten at every call
+                std::FILE* g = std::fopen(w->path.c_str(), "wb");
+                if (!g || std::fwrite(out.data(), 1, out.size(), g) != out.size()) {
+                    rc = MDFF_E_ARG;
+                    msg = "writer: cannot write " + w->path;
+                }
+                if (g) std::fclose(g);
+            } else if (rc == MDFF_OK) {
+                if (std::fwrite(out.data(), 1, out.size(), w->f) != out.size() || std::fflush(w->f) != 0) {
+                    rc = MDFF_E_ARG;
+                    msg = "writer: cannot write " + w->path;
+                }
+            }
+        }
+        {
+            std::lock_guard<std::mutex> lk(w->m);
+            if (rc != MDFF_OK && w->err == MDFF_OK) {
+                w->err = rc;
+                w->errmsg = msg;
+            }
+            w->free_slots.push_back(s);
+        }
+        w->cv.notify_all();
+    }
+}
+
+void writer_free(mdff_writer* w) {
+    if (w->th.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(w->m);
+            w->stop = true;
+        }
+        w->cv.notify_all();
+        w->th.join();
+    }
+    if (w->f) std::fclose(w->f);
+    for (auto e : w->ev_snap)
+        if (e) cudaEventDestroy(e);
+    for (auto e : w->ev_copy)
+        if (e) cudaEventDestroy(e);
+    for (auto p : w->hbuf)
+        if (p) cudaFreeHost(p);
+    if (w->dbuf) cudaFree(w->dbuf);
+    if (w->cs) cudaStreamDestroy(w->cs);
+    delete w;
+}
+
+// the snapshot of slot s on the engine's stream and its copy to the host
+int writer_snapshot(mdff_writer* w, int s) {
+    mdff_ctx* ctx = w->ctx;
+    const int n = ctx->n;
+    double* d = w->dbuf + (size_t)s * w->ncol * n;
+    const size_t b = sizeof(double) * n;
+    // the slot's previous device-to-host copy has finished before it is overwritten
+    CK(cudaStreamWaitEvent(ctx->st, w->ev_copy[s], 0));
+    auto dd = [&](int c, const double* src, int k) {
+        return cudaMemcpyAsync(d + (size_t)c * n, src, b * k, cudaMemcpyDeviceToDevice, ctx->st);
+    };
+    if (w->file == MDFF_FILE_TRAJFF || w->file == MDFF_FILE_CONTFF) {
+        const int data = w->file == MDFF_FILE_CONTFF ? (MDFF_DATA_V | MDFF_DATA_F) : w->data;
+        int c = 0;
+        CK(dd(c++, ctx->x, 1));
+        CK(dd(c++, ctx->y, 1));
+        CK(dd(c++, ctx->z, 1));
+        if (data & MDFF_DATA_V) {
+            CK(dd(c++, ctx->vx, 1));
+            CK(dd(c++, ctx->vy, 1));
+            CK(dd(c++, ctx->vz, 1));
+        }
+        if (data & MDFF_DATA_F) {
+            CK(dd(c++, ctx->fx, 1));
+            CK(dd(c++, ctx->fy, 1));
+            CK(dd(c++, ctx->fz, 1));
+        }
+        // kardir, periodicbc, dirkar of the written copy (write_trajff_xyz, src/config.f90:552-554)
+        launch_wrap_positions(ctx->st, n, d, d + n, d + 2 * (size_t)n, ctx->cell);
+        TRY(check_launch(ctx, "writer wrap"));
+    } else if (w->file == MDFF_FILE_EFGALL) {
+        CK(dd(0, ctx->efg, 6));
+    } else if (w->file == MDFF_FILE_DIPFF) {
+        CK(dd(0, ctx->mu, 3));
+    } else {
+        CK(dd(0, ctx->ef, 3));
+    }
+    CK(cudaEventRecord(w->ev_snap[s], ctx->st));
+    CK(cudaStreamWaitEvent(w->cs, w->ev_snap[s], 0));
+    CK(cudaMemcpyAsync(w->hbuf[s], d, b * w->ncol, cudaMemcpyDeviceToHost, w->cs));
+    CK(cudaEventRecord(w->ev_copy[s], w->cs));
+    mdff_frame_header& hs = w->hslot[s];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) hs.A[i + 3 * j] = ctx->cell.A[i * 3 + j];
+    return MDFF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdff_writer_open(mdff_ctx* ctx, const char* path, int file, int iformat, int data, const mdff_frame_header* h,
+                     int nslot, mdff_writer** out) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!path || !h || !out || nslot < 1) return fail(ctx, MDFF_E_ARG, "mdff_writer_open: bad argument");
+    const int ncol = mdff::io::frame_cols(file, data);
+    if (ncol < 0) return fail(ctx, MDFF_E_ARG, "mdff_writer_open: unknown file kind");
+    if (iformat == 0 && file != MDFF_FILE_TRAJFF && file != MDFF_FILE_EFGALL)
+        return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_writer_open: only TRAJFF and EFGALL have an unformatted form");
+    if (file == MDFF_FILE_EFGALL && !(ctx->p.lcoulomb && ctx->p.doefg))
+        return fail(ctx, MDFF_E_STATE, "EFGALL needs lcoulomb and doefg");
+    if ((file == MDFF_FILE_DIPFF || file == MDFF_FILE_EFALL) && !ctx->p.lcoulomb)
+        return fail(ctx, MDFF_E_STATE, "DIPFF / EFALL need lcoulomb");
+    cudaSetDevice(ctx->p.device);
+    const int n = ctx->n;
+    auto* w = new mdff_writer;
+    w->ctx = ctx;
+    w->file = file;
+    w->iformat = iformat;
+    w->data = data;
+    w->ncol = ncol;
+    w->nslot = nslot;
+    w->device = ctx->p.device;
+    w->path = path;
+    w->h = *h;
+    w->h.natm = n;
+    w->h.ntype = ctx->ntype;
+    for (int t = 0; t < ctx->ntype; ++t) w->h.natmi[t] = ctx->natmi[t];
+    std::vector<int> t0(n);
+    cudaError_t e = cudaMemcpyAsync(t0.data(), ctx->type, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    w->itype.resize(n);
+    for (int i = 0; i < n; ++i) w->itype[i] = t0[i] + 1;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&w->dbuf, sizeof(double) * (size_t)nslot * ncol * n);
+    w->hbuf.assign(nslot, nullptr);
+    w->ev_snap.assign(nslot, nullptr);
+    w->ev_copy.assign(nslot, nullptr);
+    w->hslot.assign(nslot, w->h);
+    for (int s = 0; s < nslot && e == cudaSuccess; ++s) {
+        e = cudaHostAlloc((void**)&w->hbuf[s], sizeof(double) * (size_t)ncol * n, cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w->ev_snap[s], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w->ev_copy[s], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(w->ev_copy[s], w->cs);   // the slot starts free
+        w->free_slots.push_back(s);
+    }
+    if (e != cudaSuccess) {
+        writer_free(w);
+        return fail(ctx, MDFF_E_CUDA, std::string("mdff_writer_open: ") + cudaGetErrorString(e));
+    }
+    if (file != MDFF_FILE_CONTFF) {
+        w->f = std::fopen(path, "ab");
+        if (!w->f) {
+            writer_free(w);
+            return fail(ctx, MDFF_E_ARG, std::string("mdff_writer_open: cannot open ") + path);
+        }
+    }
+    w->th = std::thread(writer_loop, w);
+    *out = w;
+    return MDFF_OK;
+}
+
+int mdff_writer_frame(mdff_writer* w) {
+    if (!w) return MDFF_E_ARG;
+    mdff_ctx* ctx = w->ctx;
+    cudaSetDevice(w->device);
+    int s;
+    {
+        std::unique_lock<std::mutex> lk(w->m);
+        w->cv.wait(lk, [&] { return !w->free_slots.empty() || w->err != MDFF_OK; });
+        if (w->err != MDFF_OK) return fail(ctx, w->err, w->errmsg);
+        s = w->free_slots.back();
+        w->free_slots.pop_back();
+    }
+    const int rc = writer_snapshot(w, s);
+    if (rc != MDFF_OK) {   // the slot goes back unused
+        {
+            std::lock_guard<std::mutex> lk(w->m);
+            w->free_slots.push_back(s);
+        }
+        w->cv.notify_all();
+        return rc;
+    }
+    {
+        std::lock_guard<std::mutex> lk(w->m);
+        w->queue.push_back(s);
+    }
+    w->cv.notify_all();
+    return MDFF_OK;
+}
+
+int mdff_writer_close(mdff_writer* w) {
+    if (!w) return MDFF_E_ARG;
+    cudaSetDevice(w->device);
+    {
+        // drain: every queued frame written and its slot returned
+        std::unique_lock<std::mutex> lk(w->m);
+        w->cv.wait(lk, [&] { return (int)w->free_slots.size() == w->nslot; });
+    }
+    const int rc = w->err;
+    if (rc != MDFF_OK && w->ctx) w->ctx->err = w->errmsg;
+    writer_free(w);
+    return rc;
+}
+
+}  // extern "C"
+
+// ---- checkpoint -------------------------------------------------------------
+namespace {
+struct CkHost {
+    char magic[8];
+    int32_t version, n, ntype, nhist, nparam_bytes;
+    int32_t itime, last_rebuilt, nrebuild, md_started, forces_valid, have_list, tuned, g_dir, g_dd, p_mul, s_mul;
+    int32_t pad;
+    double e_kin, temp_r;
+    mdff_energies en;
+    double tau_nonb[9], tau_coul[9];
+};
+constexpr char CK_MAGIC[8] = {'M', 'D', 'F', 'F', 'C', 'K', 'P', '1'};
+
+// the device arrays of the state, in file order
+std::vector<std::pair<double*, size_t>> ck_arrays(mdff_ctx* ctx) {
+    const size_t n = ctx->n;
+    return {{ctx->x, n},         {ctx->y, n},          {ctx->z, n},
+            {ctx->vx, n},        {ctx->vy, n},         {ctx->vz, n},
+            {ctx->fx, n},        {ctx->fy, n},         {ctx->fz, n},
+            {ctx->fox, n},       {ctx->foy, n},        {ctx->foz, n},
+            {ctx->xs, n},        {ctx->ys, n},         {ctx->zs, n},
+            {ctx->mu, 3 * n},    {ctx->mu_ind, 3 * n}, {ctx->hist, (size_t)ctx->nhist * 3 * n},
+            {ctx->ef, 3 * n},    {ctx->efg, 6 * n}};
+}
+
+mdff_params ck_params(const mdff_params& p) {
+    mdff_params q = p;
+    q.device = 0;
+    q.autotune = 0;
+    return q;
+}
+
+size_t ck_size(mdff_ctx* ctx) {
+    size_t need = sizeof(CkHost) + sizeof(mdff_params) + sizeof(DevScalars);
+    for (auto& a : ck_arrays(ctx)) need += sizeof(double) * a.second;
+    return need;
+}
+}  // namespace
+
+extern "C" {
+
+int mdff_checkpoint_save(mdff_ctx* ctx, void* buf, size_t cap, size_t* len) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!len) return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_save: len is NULL");
+    const size_t need = ck_size(ctx);
+    *len = need;
+    if (!buf) return MDFF_OK;
+    if (cap < need) return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_save: buffer too small");
+    cudaSetDevice(ctx->p.device);
+    CkHost hdr{};
+    std::memcpy(hdr.magic, CK_MAGIC, 8);
+    hdr.version = 1;
+    hdr.n = ctx->n;
+    hdr.ntype = ctx->ntype;
+    hdr.nhist = ctx->nhist;
+    hdr.nparam_bytes = (int)sizeof(mdff_params);
+    hdr.itime = ctx->itime;
+    hdr.last_rebuilt = ctx->last_rebuilt;
+    hdr.nrebuild = ctx->nrebuild;
+    hdr.md_started = ctx->md_started;
+    hdr.forces_valid = ctx->forces_valid;
+    hdr.have_list = ctx->have_list;
+    hdr.tuned = ctx->tuned;
+    hdr.g_dir = ctx->g_dir;
+    hdr.g_dd = ctx->g_dd;
+    hdr.p_mul = ctx->rs.p_mul;
+    hdr.s_mul = ctx->rs.s_mul;
+    hdr.e_kin = ctx->e_kin;
+    hdr.temp_r = ctx->temp_r;
+    hdr.en = ctx->en;
+    std::memcpy(hdr.tau_nonb, ctx->tau_nonb, sizeof hdr.tau_nonb);
+    std::memcpy(hdr.tau_coul, ctx->tau_coul, sizeof hdr.tau_coul);
+    char* o = (char*)buf;
+    std::memcpy(o, &hdr, sizeof hdr);
+    o += sizeof hdr;
+    const mdff_params pp = ck_params(ctx->p);
+    std::memcpy(o, &pp, sizeof pp);
+    o += sizeof pp;
+    CK(cudaMemcpyAsync(o, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->st));
+    o += sizeof(DevScalars);
+    for (auto& a : ck_arrays(ctx)) {
+        CK(cudaMemcpyAsync(o, a.first, sizeof(double) * a.second, cudaMemcpyDeviceToHost, ctx->st));
+        o += sizeof(double) * a.second;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+int mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!buf || len < sizeof(CkHost)) return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: no checkpoint");
+    CkHost hdr;
+    std::memcpy(&hdr, buf, sizeof hdr);
+    if (std::memcmp(hdr.magic, CK_MAGIC, 8) != 0 || hdr.version != 1)
+        return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: not a checkpoint of this library");
+    if (hdr.n != ctx->n || hdr.ntype != ctx->ntype || hdr.nhist != ctx->nhist ||
+        hdr.nparam_bytes != (int)sizeof(mdff_params))
+        return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: checkpoint of another system");
+    if (len != ck_size(ctx)) return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: size mismatch");
+    const char* in = (const char*)buf + sizeof hdr;
+    const mdff_params pp = ck_params(ctx->p);
+    if (std::memcmp(in, &pp, sizeof pp) != 0)
+        return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: parameters differ from the checkpoint's");
+    in += sizeof pp;
+    cudaSetDevice(ctx->p.device);
+    CK(cudaMemcpyAsync(ctx->dsc, in, sizeof(DevScalars), cudaMemcpyHostToDevice, ctx->st));
+    std::memcpy((void*)ctx->hsc, in, sizeof(DevScalars));
+    in += sizeof(DevScalars);
+    for (auto& a : ck_arrays(ctx)) {
+        CK(cudaMemcpyAsync(a.first, in, sizeof(double) * a.second, cudaMemcpyHostToDevice, ctx->st));
+        in += sizeof(double) * a.second;
+    }
+    // the neighbour lists as they were built: from the build-time fractional
+    // coordinates, so their pair order (and every sum over them) is unchanged
+    if (hdr.have_list) {
+        CK(cudaMemcpyAsync(ctx->sx, ctx->xs, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->sy, ctx->ys, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->sz, ctx->zs, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
+        TRY(build_lists(ctx, ctx->p.lvnlist ? ctx->p.skindiff : 0.0, true));
+    }
+    launch_frac(ctx->st, ctx->n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
+    TRY(check_launch(ctx, "checkpoint frac"));
+    ctx->itime = hdr.itime;
+    ctx->last_rebuilt = hdr.last_rebuilt;
+    ctx->nrebuild = hdr.nrebuild;
+    ctx->md_started = hdr.md_started != 0;
+    ctx->forces_valid = hdr.forces_valid != 0;
+    ctx->have_list = hdr.have_list != 0;
+    ctx->tuned = hdr.tuned != 0;
+    ctx->g_dir = hdr.g_dir;
+    ctx->g_dd = hdr.g_dd;
+    ctx->rs.p_mul = hdr.p_mul;
+    ctx->rs.s_mul = hdr.s_mul;
+    ctx->e_kin = hdr.e_kin;
+    ctx->temp_r = hdr.temp_r;
+    ctx->en = hdr.en;
+    std::memcpy(ctx->tau_nonb, hdr.tau_nonb, sizeof hdr.tau_nonb);
+    std::memcpy(ctx->tau_coul, hdr.tau_coul, sizeof hdr.tau_coul);
+    ctx->rs.want_epoch++;
+    ctx->rec_acc_ready = false;
+    ctx->ddtab_epoch = -1;
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+}  // extern "C"

@@ -5,6 +5,9 @@ writes small .npz files next to this script.  Run once where the reference is
 available; the fixtures are committed so the GPU tests never read the
 reference at run time.
 
+ex1_contff_head.txt, ex1_contff.sha256 -- the first 24 lines of
+examples/ex1/ref/CONTFF and the SHA-256 of the whole file.
+
 ex1_final.npz -- examples/ex1/ref: the final configuration of the 256-atom
 LJ argon NVE run (CONTFF: positions, velocities and forces at step 5000,
 12 significant digits), its energy (OSZIFF line of step 5000), virial
@@ -42,6 +45,14 @@ def ex1():
              u_lj=u, pvir_gpa=pvir, tau_nonb_printed=tau, cutshortrange=8.5, epslj=0.010323576, sigmalj=3.405,
              mass=39.95)
     print("ex1_final.npz", n, u, pvir)
+    # the CONTFF text itself (write_CONTFF's layout): its first lines and the
+    # digest of the whole file, for the formatter's byte-for-byte check
+    import hashlib
+    raw = open(os.path.join(base, "CONTFF"), "rb").read()
+    head = b"\n".join(raw.split(b"\n")[:24]) + b"\n"
+    open(os.path.join(OUT, "ex1_contff_head.txt"), "wb").write(head)
+    open(os.path.join(OUT, "ex1_contff.sha256"), "w").write(hashlib.sha256(raw).hexdigest() + "\n")
+    print("ex1_contff_head.txt", len(raw))
 
 
 if __name__ == "__main__":

@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-stream", action="store_true",
+                    help="skip the trajectory-streaming measurement of the production workload")
     ap.add_argument("--ncell", type=int, default=16)
     ap.add_argument("--ext", default="aspc", choices=["aspc", "poly"],
                     help="induced-dipole predictor (algo_ext_dipole)")
@@ -234,6 +236,47 @@ def run_engine(args):
         t2 = time.perf_counter()
         e2e = {"value": whole_job_rate(natm * ke, t2 - t1, dist, device), "unit": "atom-steps/s", "steps": ke,
                "h2d_bytes_per_step": 6 * 8 * natm, "d2h_bytes_per_step": 9 * 8 * natm}
+    # trajectory streaming: the same steps with TRAJFF frames written through
+    # the engine's writer (device snapshot, copy stream, writer thread), against
+    # the same loop without frames; wall time includes draining the writer
+    stream = None
+    if not args.no_stream:
+        import shutil
+        import tempfile
+        tmpd = tempfile.mkdtemp(prefix="mdff_stream_")
+        ks = max(10, args.steps)
+
+        def run_stream(iformat, every):
+            w = None
+            if every:
+                w = eng.writer(os.path.join(tmpd, f"TRAJFF{iformat}"), "TRAJFF", iformat, "rvf", system="MgO",
+                               labels=["O", "Mg"], nslot=4)
+            torch.cuda.synchronize(device)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            t1 = time.perf_counter()
+            a.record(ext)
+            for k in range(ks):
+                eng.advance(1)
+                if w is not None and (k + 1) % every == 0:
+                    w.frame()
+            b.record(ext)
+            if w is not None:
+                w.close()
+            b.synchronize()
+            t2 = time.perf_counter()
+            return a.elapsed_time(b), (t2 - t1) * 1e3
+
+        base_ms, base_wall = run_stream(1, 0)
+        stream = {"steps": ks, "no_frames": {"device_ms_per_step": base_ms / ks, "wall_ms_per_step": base_wall / ks}}
+        for label, iformat, every in (("trajff_rvf_unformatted_every_step", 0, 1),
+                                      ("trajff_rvf_formatted_every_10_steps", 1, 10)):
+            d_ms, w_ms = run_stream(iformat, every)
+            nbytes = os.path.getsize(os.path.join(tmpd, f"TRAJFF{iformat}"))
+            stream[label] = {"device_ms_per_step": d_ms / ks, "wall_ms_per_step": w_ms / ks,
+                             "wall_overhead_vs_no_frames": w_ms / base_wall - 1.0,
+                             "bytes_written": nbytes, "file_mb_per_s": nbytes / (w_ms / 1e3) / 1e6}
+        shutil.rmtree(tmpd, ignore_errors=True)
     # profiled pass (not part of the timed region)
     kp = max(2, min(args.steps, 10))
     eng.enable_profile(True)
@@ -344,6 +387,7 @@ def run_engine(args):
             "kernels_ms_per_step": {k: round(v["ms"] / kp, 4) for k, v in kern.items()},
             "roofline": roof,
             "e2e": e2e,
+            "stream": stream,
             "step0": {"h_tot": t0["h_tot"], "temp_r": t0["temp_r"], "scf_iter": t0["scf_iter"]},
         }
         if not args.no_cpu:

@@ -373,6 +373,11 @@ class Engine:
             "thermo": [th[i].as_dict() for i in range(nsteps)] if thermo else [],
         }
 
+    def advance(self, nsteps):
+        """Advance nsteps with the state left on the device (nothing read back)."""
+        self._check(lib().mdff_step(self._h, int(nsteps), None, None, None, None, None, None, None, None, None,
+                                    None))
+
     def step_host(self, nsteps, pos, vel, thermo=None):
         """The host-buffer form of mdff_step: positions and velocities are
         uploaded from, and written back to, the given (N,3)-shaped SoA arrays."""

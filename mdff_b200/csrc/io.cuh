@@ -25,12 +25,15 @@
 // formatted and written by a writer thread, so the time loop never waits for
 // the disk unless every slot of the ring is still in flight.
 #pragma once
+#include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mdff_engine.h"
@@ -48,30 +51,96 @@ inline void pad_left(std::string& o, const std::string& s, int w) {
     o += s;
 }
 
+// Exact powers of ten in x87 extended precision (10^k = 5^k 2^k, 5^27 < 2^64).
+inline long double pow10_exact(int k) {
+    static const long double t[28] = {1e0L,  1e1L,  1e2L,  1e3L,  1e4L,  1e5L,  1e6L,  1e7L,  1e8L,  1e9L,
+                                      1e10L, 1e11L, 1e12L, 1e13L, 1e14L, 1e15L, 1e16L, 1e17L, 1e18L, 1e19L,
+                                      1e20L, 1e21L, 1e22L, 1e23L, 1e24L, 1e25L, 1e26L, 1e27L};
+    return t[k];
+}
+
+// The d significant decimal digits of a > 0 (d <= 17) and its decimal
+// exponent (a = 0.digits x 10^e), correctly rounded, without the general
+// conversion: a times an exact power of ten in extended precision carries a
+// relative error below 2^-64, far less than the distance of its fractional
+// part from 1/2 except near a tie; near one (or outside the exact range)
+// returns false and the caller converts exactly.
+inline bool digits_fast(double a, int d, char* out, int& e) {
+    if (!(a > 1e-25 && a < 1e25) || d > 17) return false;
+    int e10 = (int)std::floor(std::log10(a));           // a in [10^e10, 10^(e10+1)), up to one off
+    const long double top = pow10_exact(d);
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        const int k = d - 1 - e10;                        // scale a by 10^k into [10^(d-1), 10^d)
+        if (k > 27 || k < -27) return false;
+        const long double m = k >= 0 ? (long double)a * pow10_exact(k) : (long double)a / pow10_exact(-k);
+        if (m >= top) { ++e10; continue; }
+        if (m < pow10_exact(d - 1)) { --e10; continue; }
+        long double ip = std::floor(m);
+        const long double frac = m - ip;
+        if (std::fabs(frac - 0.5L) < 1e-3L) return false;
+        if (frac > 0.5L) ip += 1.0L;
+        if (ip >= top) { ip = pow10_exact(d - 1); ++e10; }
+        unsigned long long u = (unsigned long long)ip;
+        for (int j = d - 1; j >= 0; --j) {
+            out[j] = (char)('0' + u % 10);
+            u /= 10;
+        }
+        e = e10 + 1;
+        return true;
+    }
+    return false;
+}
+
 // Ew.d: [-]0.d1..dd E+ee (|exponent| <= 99) or [-]0.d1..dd+eee; the optional
 // leading zero is dropped only when the field is too narrow for it.
 inline void fmt_E(std::string& o, double v, int w, int d) {
     if (std::isnan(v)) { pad_left(o, "NaN", w); return; }
     if (std::isinf(v)) { pad_left(o, v < 0 ? "-Infinity" : "Infinity", w); return; }
-    const bool neg = std::signbit(v);
-    std::string digits;
-    int e = 0;
+    char s[96];
+    int k = 0, e = 0;
+    if (std::signbit(v)) s[k++] = '-';
+    const int zero_at = k;
+    s[k++] = '0';
+    s[k++] = '.';
     if (v == 0.0) {
-        digits.assign(d, '0');
+        for (int j = 0; j < d && k < 80; ++j) s[k++] = '0';
+    } else if (d <= 17 && digits_fast(std::fabs(v), d, s + k, e)) {
+        k += d;
     } else {
+        // d significant digits of the binary value, correctly rounded (as
+        // the Fortran runtime prints them)
         char buf[64];
-        std::snprintf(buf, sizeof buf, "%.*e", d - 1, std::fabs(v));
+        const auto r = std::to_chars(buf, buf + sizeof buf, std::fabs(v), std::chars_format::scientific, d - 1);
         const char* p = buf;
-        for (; *p && *p != 'e'; ++p)
-            if (*p != '.') digits.push_back(*p);
-        e = std::atoi(p + 1) + 1;
+        for (; p < r.ptr && *p != 'e' && k < 80; ++p)
+            if (*p != '.') s[k++] = *p;
+        int ex = 0;
+        const char* q = p + 1;
+        if (q < r.ptr && *q == '+') ++q;
+        std::from_chars(q, (const char*)r.ptr, ex);
+        e = ex + 1;
     }
-    char ex[16];
-    if (std::abs(e) <= 99) std::snprintf(ex, sizeof ex, "E%c%02d", e < 0 ? '-' : '+', std::abs(e));
-    else std::snprintf(ex, sizeof ex, "%c%03d", e < 0 ? '-' : '+', std::abs(e));
-    std::string s = std::string(neg ? "-" : "") + "0." + digits + ex;
-    if ((int)s.size() > w) s = std::string(neg ? "-" : "") + "." + digits + ex;
-    pad_left(o, s, w);
+    const int ae = std::abs(e);
+    if (ae <= 99) {
+        s[k++] = 'E';
+        s[k++] = e < 0 ? '-' : '+';
+    } else {
+        s[k++] = e < 0 ? '-' : '+';
+        s[k++] = (char)('0' + ae / 100 % 10);
+    }
+    s[k++] = (char)('0' + ae / 10 % 10);
+    s[k++] = (char)('0' + ae % 10);
+    const char* beg = s;
+    if (k > w) {   // drop the optional leading zero
+        std::memmove(s + zero_at, s + zero_at + 1, k - zero_at - 1);
+        --k;
+    }
+    if (k > w) {
+        o.append(w, '*');
+        return;
+    }
+    o.append(w - k, ' ');
+    o.append(beg, k);
 }
 
 inline void fmt_F(std::string& o, double v, int w, int d) {
@@ -82,8 +151,14 @@ inline void fmt_F(std::string& o, double v, int w, int d) {
 
 inline void fmt_I(std::string& o, long long v, int w) {
     char buf[32];
-    std::snprintf(buf, sizeof buf, "%lld", v);
-    pad_left(o, buf, w);
+    const auto r = std::to_chars(buf, buf + sizeof buf, v);
+    const int k = (int)(r.ptr - buf);
+    if (k > w) {
+        o.append(w, '*');
+        return;
+    }
+    o.append(w - k, ' ');
+    o.append(buf, k);
 }
 
 // character variable of declared length len (blank padded)
@@ -176,13 +251,40 @@ inline int format_frame(int file, int iformat, int data, const mdff_frame_header
         }
         ld_chars(o, h.atypei, nt);
         ld_ints(o, h.natmi, nt);
-        if (file == MDFF_FILE_TRAJFF || file == MDFF_FILE_CONTFF) {
-            o += "Cartesian\n";
-            for (int i = 0; i < n; ++i) {
-                fmt_A(o, h.atypei[itype[i] - 1], 3);
-                for (int c = 0; c < ncol; ++c) fmt_E(o, col(c, i), 20, 12);
-                o.push_back('\n');
+        // per-atom lines: chunks formatted on host threads, joined in order
+        const bool traj = file == MDFF_FILE_TRAJFF || file == MDFF_FILE_CONTFF;
+        auto line = [&](std::string& s, int i) {
+            if (traj) {
+                fmt_A(s, h.atypei[itype[i] - 1], 3);
+                for (int c = 0; c < ncol; ++c) fmt_E(s, col(c, i), 20, 12);
+            } else {
+                fmt_I(s, i + 1, 8);
+                s += "  ";
+                fmt_A(s, h.atypei[itype[i] - 1], 3);
+                for (int c = 0; c < ncol; ++c) fmt_E(s, col(c, i), 24, 16);
             }
+            s.push_back('\n');
+        };
+        auto lines = [&](std::string& s) {
+            const int nth = n < 4096 ? 1 : (int)std::min<unsigned>(8u, std::max(1u, std::thread::hardware_concurrency()));
+            if (nth == 1) {
+                for (int i = 0; i < n; ++i) line(s, i);
+                return;
+            }
+            std::vector<std::string> part(nth);
+            std::vector<std::thread> th;
+            for (int t = 0; t < nth; ++t)
+                th.emplace_back([&, t] {
+                    const int i0 = (int)((long long)n * t / nth), i1 = (int)((long long)n * (t + 1) / nth);
+                    part[t].reserve((size_t)(i1 - i0) * (traj ? 4 + 20 * ncol : 14 + 24 * ncol));
+                    for (int i = i0; i < i1; ++i) line(part[t], i);
+                });
+            for (auto& x : th) x.join();
+            for (auto& x : part) s += x;
+        };
+        if (traj) {
+            o += "Cartesian\n";
+            lines(o);
         } else {
             const char* head =
                 file == MDFF_FILE_EFGALL
@@ -193,13 +295,7 @@ inline int format_frame(int file, int iformat, int data, const mdff_frame_header
                           : "      ia type                   Ex                      Ey                      Ez";
             o += head;
             o.push_back('\n');
-            for (int i = 0; i < n; ++i) {
-                fmt_I(o, i + 1, 8);
-                o += "  ";
-                fmt_A(o, h.atypei[itype[i] - 1], 3);
-                for (int c = 0; c < ncol; ++c) fmt_E(o, col(c, i), 24, 16);
-                o.push_back('\n');
-            }
+            lines(o);
         }
         return MDFF_OK;
     }

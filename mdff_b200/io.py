@@ -56,11 +56,12 @@ def format_frame(kind, iformat, data, h, itype, cols):
     L = lib()
     args = (_kind(kind), int(iformat), _data(data), C.byref(h), it.ctypes.data_as(C.POINTER(C.c_int)),
             c.ctypes.data_as(C.POINTER(C.c_double)))
-    rc = L.mdff_io_format(*args, None, 0, C.byref(n))
-    if rc not in (0, abi.E_ARG) or n.value == 0:
-        raise ValueError(f"mdff_io_format failed ({rc})")
-    buf = C.create_string_buffer(n.value)
-    rc = L.mdff_io_format(*args, buf, n.value, C.byref(n))
+    guess = 4096 + c.size * 26 + it.size * 16          # above any frame's length: one formatting pass
+    buf = C.create_string_buffer(guess)
+    rc = L.mdff_io_format(*args, buf, guess, C.byref(n))
+    if rc == abi.E_ARG and n.value > guess:
+        buf = C.create_string_buffer(n.value)
+        rc = L.mdff_io_format(*args, buf, n.value, C.byref(n))
     if rc != 0:
         raise ValueError(f"mdff_io_format failed ({rc})")
     return buf.raw[:n.value]

@@ -246,11 +246,13 @@ def run_engine(args):
         tmpd = tempfile.mkdtemp(prefix="mdff_stream_")
         ks = max(10, args.steps)
 
-        def run_stream(iformat, every):
+        shm = tempfile.mkdtemp(prefix="mdff_stream_", dir="/dev/shm") if os.path.isdir("/dev/shm") else None
+
+        def run_stream(iformat, every, where=None):
             w = None
             if every:
-                w = eng.writer(os.path.join(tmpd, f"TRAJFF{iformat}"), "TRAJFF", iformat, "rvf", system="MgO",
-                               labels=["O", "Mg"], nslot=4)
+                w = eng.writer(os.path.join(where or tmpd, f"TRAJFF{iformat}"), "TRAJFF", iformat, "rvf",
+                               system="MgO", labels=["O", "Mg"], nslot=4)
             torch.cuda.synchronize(device)
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
@@ -268,15 +270,22 @@ def run_engine(args):
             return a.elapsed_time(b), (t2 - t1) * 1e3
 
         base_ms, base_wall = run_stream(1, 0)
-        stream = {"steps": ks, "no_frames": {"device_ms_per_step": base_ms / ks, "wall_ms_per_step": base_wall / ks}}
-        for label, iformat, every in (("trajff_rvf_unformatted_every_step", 0, 1),
-                                      ("trajff_rvf_formatted_every_10_steps", 1, 10)):
-            d_ms, w_ms = run_stream(iformat, every)
-            nbytes = os.path.getsize(os.path.join(tmpd, f"TRAJFF{iformat}"))
+        stream = {"steps": ks, "dir": tmpd, "no_frames": {"device_ms_per_step": base_ms / ks,
+                                                          "wall_ms_per_step": base_wall / ks}}
+        cases = [("trajff_rvf_unformatted_every_step", 0, 1, tmpd),
+                 ("trajff_rvf_formatted_every_10_steps", 1, 10, tmpd)]
+        if shm:
+            cases += [("trajff_rvf_unformatted_every_step_to_dev_shm", 0, 1, shm),
+                      ("trajff_rvf_formatted_every_10_steps_to_dev_shm", 1, 10, shm)]
+        for label, iformat, every, where in cases:
+            d_ms, w_ms = run_stream(iformat, every, where)
+            nbytes = os.path.getsize(os.path.join(where, f"TRAJFF{iformat}"))
             stream[label] = {"device_ms_per_step": d_ms / ks, "wall_ms_per_step": w_ms / ks,
                              "wall_overhead_vs_no_frames": w_ms / base_wall - 1.0,
                              "bytes_written": nbytes, "file_mb_per_s": nbytes / (w_ms / 1e3) / 1e6}
         shutil.rmtree(tmpd, ignore_errors=True)
+        if shm:
+            shutil.rmtree(shm, ignore_errors=True)
     # profiled pass (not part of the timed region)
     kp = max(2, min(args.steps, 10))
     eng.enable_profile(True)

@@ -116,6 +116,19 @@ module mdff_engine
     real(c_double) :: vzzmin, resvzz, reseta, umin, resu, smax
   end type mdff_efg_dist_params_t
 
+  ! frame header of the on-disk formats: natm, simu_cell%A (column-major),
+  ! system, atypei, natmi (the config module's values)
+  type, bind(C) :: mdff_frame_header_t
+    integer(c_int) :: natm, ntype
+    real(c_double) :: a(9)
+    character(kind=c_char) :: system(60)
+    character(kind=c_char) :: atypei(3, MDFF_NTYPE_MAX)
+    integer(c_int) :: natmi(MDFF_NTYPE_MAX)
+  end type mdff_frame_header_t
+
+  integer(c_int), parameter :: MDFF_FILE_TRAJFF = 0, MDFF_FILE_CONTFF = 1, MDFF_FILE_EFGALL = 2, &
+                               MDFF_FILE_DIPFF = 3, MDFF_FILE_EFALL = 4, MDFF_DATA_V = 1, MDFF_DATA_F = 2
+
   interface
     subroutine mdff_params_default(p) bind(C, name="mdff_params_default")
       import :: mdff_params_t
@@ -225,6 +238,40 @@ module mdff_engine
       real(c_double), intent(inout) :: rx(*), ry(*), rz(*), vx(*), vy(*), vz(*)
       real(c_double), intent(out) :: fx(*), fy(*), fz(*)
       type(mdff_thermo_t), intent(out) :: thermo(*)
+    end function
+    ! streaming writer: frames of the context's state, written in the background
+    integer(c_int) function mdff_writer_open(ctx, path, file, iformat, data, h, nslot, w) &
+        bind(C, name="mdff_writer_open")
+      import :: c_int, c_ptr, c_char, mdff_frame_header_t
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)     ! NUL terminated
+      integer(c_int), value :: file, iformat, data, nslot
+      type(mdff_frame_header_t), intent(in) :: h
+      type(c_ptr), intent(out) :: w
+    end function
+
+    integer(c_int) function mdff_writer_frame(w) bind(C, name="mdff_writer_frame")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: w
+    end function
+
+    integer(c_int) function mdff_writer_close(w) bind(C, name="mdff_writer_close")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: w
+    end function
+
+    ! whole-state checkpoint into / from a caller's buffer (buf = c_null_ptr to query len)
+    integer(c_int) function mdff_checkpoint_save(ctx, buf, cap, len) bind(C, name="mdff_checkpoint_save")
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ctx, buf
+      integer(c_size_t), value :: cap
+      integer(c_size_t), intent(out) :: len
+    end function
+
+    integer(c_int) function mdff_checkpoint_load(ctx, buf, len) bind(C, name="mdff_checkpoint_load")
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ctx, buf
+      integer(c_size_t), value :: len
     end function
   end interface
 

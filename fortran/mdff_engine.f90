@@ -24,7 +24,7 @@ module mdff_engine
   integer(c_int), parameter :: MDFF_TRUNC_NONE = 0, MDFF_TRUNC_LINEAR = 1, MDFF_TRUNC_QUADRATIC = 2
   integer(c_int), parameter :: MDFF_POLA_SCF = 0, MDFF_POLA_PCG = 1
   integer(c_int), parameter :: MDFF_EXT_POLY = 0, MDFF_EXT_ASPC = 1
-  integer(c_int), parameter :: MDFF_NVE_VV = 0, MDFF_NVT_NHCN = 1
+  integer(c_int), parameter :: MDFF_NVE_VV = 0, MDFF_NVT_NHCN = 1, MDFF_NPT_NHCNP = 2
   integer(c_int), parameter :: MDFF_PREC_FP64 = 0, MDFF_PREC_MIXED = 1
 
   type, bind(C) :: mdff_params_t
@@ -80,6 +80,8 @@ module mdff_engine
     real(c_double) :: mixed_keps
     integer(c_int) :: autotune
     integer(c_int) :: kspace_tc
+    real(c_double) :: press
+    real(c_double) :: timesca_baro
   end type mdff_params_t
 
   type, bind(C) :: mdff_energies_t
@@ -104,6 +106,7 @@ module mdff_engine
     integer(c_int) :: nlist_rebuilt
     integer(c_int) :: scf_iter
     real(c_double) :: scf_rmsd
+    real(c_double) :: volume
   end type mdff_thermo_t
 
   type, bind(C) :: mdff_opt_result_t

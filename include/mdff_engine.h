@@ -65,6 +65,8 @@ extern "C" {
 /* integrator (src/md.f90:71-76); only the two on the hot path */
 #define MDFF_NVE_VV   0
 #define MDFF_NVT_NHCN 1
+#define MDFF_NPT_NHCNP 2           /* isotropic Martyna-Tobias-Klein barostat with Nose-Hoover chains on
+                                      particles and barostat (nhcnp, src/integration.f90:715-1160) */
 
 /* arithmetic of the bulk pair and k-space work */
 #define MDFF_PREC_FP64  0          /* plain FP64 everywhere */
@@ -118,7 +120,7 @@ typedef struct mdff_params {
     int    extrapolate_order;
     int    algo_ext_dipole;                    /* MDFF_EXT_* */
     /* &mdtag */
-    int    integrator;                         /* MDFF_NVE_VV / MDFF_NVT_NHCN */
+    int    integrator;                         /* MDFF_NVE_VV / MDFF_NVT_NHCN / MDFF_NPT_NHCNP */
     double dt;                                 /* ps */
     double temp;                               /* K */
     int    nhc_n, nhc_yosh_order, nhc_mults;
@@ -141,6 +143,9 @@ typedef struct mdff_params {
     int    kspace_tc;                          /* mixed path: 1 = structure factor on the tensor cores (exact int8
                                                   digit products of 24-bit fixed point) when nz rows <= 80;
                                                   0 = FP32 CUDA-core kernel */
+    /* &mdtag, constant pressure (integrator MDFF_NPT_NHCNP) */
+    double press;                              /* GPa (md_check_tag converts with press_unit) */
+    double timesca_baro;                       /* ps */
 } mdff_params;
 
 /* Energies and scalar outputs of one force evaluation (thermodynamic module
@@ -162,12 +167,13 @@ typedef struct mdff_thermo {
     double e_kin, temp_r;                      /* eV, K */
     double u_tot, e_tot, h_tot;                /* eV; h_tot is the conserved quantity */
     double u_lj, u_bmhft, u_morse, u_coul, u_pol;
-    double e_nvt;                              /* NHC thermostat energy (0 for NVE) */
+    double e_nvt;                              /* NHC thermostat energy (NPT: e_npt, thermostats and barostat) */
     double pressure_tot;                       /* GPa */
     double pvirial_tot;                        /* GPa */
     int    nlist_rebuilt;                      /* 1 if the Verlet list was rebuilt after this step */
     int    scf_iter;
     double scf_rmsd;
+    double volume;                             /* A^3 (changes under MDFF_NPT_NHCNP) */
 } mdff_thermo;
 
 /* Derivative of a scalar loss with respect to the force-field tables (no
@@ -295,6 +301,13 @@ int  mdff_set_system(mdff_ctx* ctx, int natm, const int* itype,
 
 /* Replace the positions (no wrap, no list rebuild): the state engforce_driver
  * sees when a caller moved the atoms itself. */
+/* A new cell (column-major, as mdff_set_system) for the same atoms: the
+ * lattice, the tail corrections and the Ewald k tables of the same k
+ * rectangle follow it (the k membership of the mixed path's sets stays as set
+ * up; meant for the percent-level changes of a constant-pressure run).
+ * Positions are kept as given (Cartesian); lists are rebuilt.  No reference
+ * counterpart (the reference moves simu_cell inside nhcnp). */
+int  mdff_set_cell(mdff_ctx* ctx, const double A[9]);
 int  mdff_set_positions(mdff_ctx* ctx, const double* rx, const double* ry, const double* rz);
 
 /* Wrapped positions as the engine holds them. */

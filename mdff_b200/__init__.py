@@ -51,6 +51,7 @@ def lib():
         L.mdff_last_error.restype = C.c_char_p
         L.mdff_set_system.argtypes = [vp, C.c_int, ip, dp, dp, dp, dp]
         L.mdff_set_positions.argtypes = [vp, dp, dp, dp]
+        L.mdff_set_cell.argtypes = [vp, dp]
         L.mdff_get_positions.argtypes = [vp, dp, dp, dp]
         L.mdff_engforce.argtypes = [vp, dp, dp, dp, C.POINTER(abi.Energies), dp, dp, dp, dp, dp]
         L.mdff_nlist_build.argtypes = [vp]
@@ -178,6 +179,11 @@ class Engine:
         r = [np.empty(self.n) for _ in range(3)]
         self._check(lib().mdff_get_positions(self._h, *(_dp(a) for a in r)))
         return np.stack(r, axis=1)
+
+    def set_cell(self, cell):
+        """A new cell (rows = lattice vectors) for the same atoms (mdff_set_cell)."""
+        A = np.ascontiguousarray(np.asarray(cell, dtype=np.float64).T.reshape(9))
+        self._check(lib().mdff_set_cell(self._h, _dp(A)))
 
     def set_positions(self, pos):
         pos = np.asarray(pos, dtype=np.float64)

@@ -23,7 +23,7 @@ E_NOMEM = -8
 TRUNC_NONE, TRUNC_LINEAR, TRUNC_QUADRATIC = 0, 1, 2
 POLA_SCF, POLA_PCG = 0, 1
 EXT_POLY, EXT_ASPC = 0, 1
-NVE_VV, NVT_NHCN = 0, 1
+NVE_VV, NVT_NHCN, NPT_NHCNP = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 
 _T = NTYPE_MAX
@@ -57,6 +57,7 @@ class Params(C.Structure):
         ("erfc_ref", C.c_int), ("nhc_literal", C.c_int), ("mixed_ksplit", C.c_double),
         ("kspace_reuse", C.c_int), ("mixed_keps", C.c_double), ("autotune", C.c_int),
         ("kspace_tc", C.c_int),
+        ("press", C.c_double), ("timesca_baro", C.c_double),
     ]
 
 
@@ -85,6 +86,7 @@ class Thermo(C.Structure):
         ("u_coul", C.c_double), ("u_pol", C.c_double),
         ("e_nvt", C.c_double), ("pressure_tot", C.c_double), ("pvirial_tot", C.c_double),
         ("nlist_rebuilt", C.c_int), ("scf_iter", C.c_int), ("scf_rmsd", C.c_double),
+        ("volume", C.c_double),
     ]
 
     def as_dict(self):
@@ -179,4 +181,6 @@ def default_params():
     p.mixed_ksplit = 2.5
     p.mixed_keps = 1e-7
     p.kspace_tc = 1
+    p.press = 0.0
+    p.timesca_baro = 1.0
     return p

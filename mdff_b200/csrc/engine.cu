@@ -22,6 +22,7 @@
 #include "solve.cuh"
 #include "integrate.cuh"
 #include "opt.cuh"
+#include "npt.cuh"
 #include "efg_post.cuh"
 #include "io.cuh"
 #include <condition_variable>
@@ -112,6 +113,10 @@ struct mdff_ctx {
     int ddtab_lcap = 0;                  // list capacity it was written with
     bool tuned = false;
     Prof prof;
+    // cell (column-major, as given) and the constant-pressure state
+    double A_cur[9] = {0};
+    double omega0 = 0.0, utail0 = 0.0, ptail0 = 0.0;   // set-up cell volume and tail corrections
+    NptState npt;
 };
 
 namespace {
@@ -240,14 +245,17 @@ int check_params(mdff_ctx* ctx, const mdff_params& p) {
             for (int c = 0; c < p.ntype; ++c)
                 if (p.dip_pol_damp_k[a][b][c] > MDFF_TT_MAX_ORDER || p.dip_pol_damp_k[a][b][c] < 0)
                     return fail(ctx, MDFF_E_ARG, "Tang-Toennies expansion order too large (dip_pol_damp_k)");
-    if (p.integrator != MDFF_NVE_VV && p.integrator != MDFF_NVT_NHCN)
-        return fail(ctx, MDFF_E_UNSUPPORTED, "integrator: only nve-vv and nvt-nhcn are on the engine's path");
-    if (p.integrator == MDFF_NVT_NHCN && (p.nhc_n < 2 || p.nhc_n > 16))
+    if (p.integrator != MDFF_NVE_VV && p.integrator != MDFF_NVT_NHCN && p.integrator != MDFF_NPT_NHCNP)
+        return fail(ctx, MDFF_E_UNSUPPORTED, "integrator: nve-vv, nvt-nhcn and npt-nhcnp are on the engine's path");
+    const bool chains = p.integrator == MDFF_NVT_NHCN || p.integrator == MDFF_NPT_NHCNP;
+    if (chains && (p.nhc_n < 2 || p.nhc_n > 16))
         return fail(ctx, MDFF_E_ARG, "nhc_n = 1 is not allowed with Nose Hoover chains thermostats");
     int yo = p.nhc_yosh_order;
-    if (p.integrator == MDFF_NVT_NHCN && !(yo == 1 || yo == 3 || yo == 5 || yo == 7 || yo == 9))
+    if (chains && !(yo == 1 || yo == 3 || yo == 5 || yo == 7 || yo == 9))
         return fail(ctx, MDFF_E_ARG, "value of yoshida order not available");
-    if (p.integrator == MDFF_NVT_NHCN && p.nhc_mults < 1) return fail(ctx, MDFF_E_ARG, "nhc_mults < 1");
+    if (chains && p.nhc_mults < 1) return fail(ctx, MDFF_E_ARG, "nhc_mults < 1");
+    if (p.integrator == MDFF_NPT_NHCNP && !(p.timesca_baro > 0.0))
+        return fail(ctx, MDFF_E_ARG, "mdtag: with integrator in npt_ensemble timesca_baro should be set");
     if (p.extrapolate_order < 0 || p.extrapolate_order > 5)
         return fail(ctx, MDFF_E_ARG, "extrapolate_order should be 0 <= order <= 5");
     if (p.algo_moment_from_pola != MDFF_POLA_SCF && p.algo_moment_from_pola != MDFF_POLA_PCG)
@@ -403,6 +411,7 @@ int build_lists(mdff_ctx* ctx, double skin, bool from_frac = false) {
     CK(cudaMemcpyAsync(ctx->zs, ctx->sz, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
     ctx->have_list = true;
     ctx->nrebuild++;
+    ctx->npt.scale_build = ctx->npt.scale;
     return MDFF_OK;
 }
 
@@ -997,8 +1006,10 @@ void fill_thermo(mdff_ctx* ctx, mdff_thermo* t, int step) {
     t->u_pol = ctx->en.u_pol / nr;
     t->u_tot = t->u_lj + t->u_coul + t->u_morse + t->u_bmhft;
     t->e_tot = t->u_tot + t->e_kin;
-    t->e_nvt = (ctx->p.integrator == MDFF_NVT_NHCN ? ctx->hsc->e_nvt : 0.0) / nr;
-    t->h_tot = ctx->p.integrator == MDFF_NVT_NHCN ? t->e_tot + t->e_nvt : t->e_tot;
+    const int ig = ctx->p.integrator;
+    t->e_nvt = (ig == MDFF_NVT_NHCN ? ctx->hsc->e_nvt : ig == MDFF_NPT_NHCNP ? ctx->npt.e_npt : 0.0) / nr;
+    t->h_tot = ig == MDFF_NVE_VV ? t->e_tot : t->e_tot + t->e_nvt;
+    t->volume = omega;
     double pv = (ctx->en.vir_lj + ctx->en.vir_morse + ctx->en.vir_bmhft) / omega / nr + ctx->en.pvirial_coul / nr;
     t->pvirial_tot = pv / ctx->u.press;
     t->pressure_tot = (pv + ctx->temp_r * ctx->u.boltz / omega) / ctx->u.press;
@@ -1012,13 +1023,149 @@ void set_kin(mdff_ctx* ctx) {
     ctx->temp_r = 2.0 * ctx->e_kin / ctx->u.boltz / (3.0 * (double)ctx->n);
 }
 
+// A new cell of the same k rectangle (constant pressure, mdff_set_cell):
+// lattice, the tail corrections (proportional to 1/V and 1/V^2) and the k
+// tables with their set-up membership.
+int apply_cell(mdff_ctx* ctx, const double A9[9]) {
+    CellP c;
+    double W[3], an[3];
+    lattice(A9, c, W, an);
+    if (!(c.omega > 0.0)) return fail(ctx, MDFF_E_ARG, "cell volume must be positive");
+    ctx->cell = c;
+    for (int d = 0; d < 3; ++d) { ctx->W[d] = W[d]; ctx->anorm[d] = an[d]; }
+    std::memcpy(ctx->A_cur, A9, sizeof ctx->A_cur);
+    const double r = ctx->omega0 / c.omega;
+    ctx->utail = ctx->utail0 * r;
+    ctx->ptail = ctx->ptail0 * r * r;
+    if (ctx->p.lcoulomb && ctx->kg.mask) {
+        KGrid& kg = ctx->kg;
+        const double a2 = ctx->alphaES * ctx->alphaES;
+        k_kgrid_refresh<<<nb(kg.nrect), 256, 0, ctx->st>>>(kg.nrect, kg.nzl, kg.kmax[1], kg.kmax[2], c, a2, kg.mask,
+                                                           kg.Ak, kg.kcoe, kg.Ak_hi);
+        const LowK& lk = ctx->rs.low;
+        if (lk.ncol > 0)
+            k_lowk_refresh<<<nb(lk.ncol * lk.nzmax), 256, 0, ctx->st>>>(lk.ncol, lk.nzmax, c, a2, lk.col, lk.Ak,
+                                                                        lk.kcoe);
+        TRY(check_launch(ctx, "k tables"));
+    }
+    ctx->ddtab_epoch = -1;
+    ctx->rec_acc_ready = false;
+    ctx->forces_valid = false;
+    return MDFF_OK;
+}
+
+void npt_const(const mdff_ctx* ctx, NptConst& c) {
+    const mdff_params& p = ctx->p;
+    NhcConst h;
+    nhc_const(ctx, h);
+    std::memset(&c, 0, sizeof c);
+    c.nhc_n = h.nhc_n;
+    c.yosh = h.yosh;
+    c.mults = h.mults;
+    c.literal = h.literal;
+    c.dt = h.dt;
+    c.temp = h.temp;
+    c.L = h.L;
+    std::memcpy(c.w, h.w, sizeof c.w);
+    std::memcpy(c.Q, h.Q, sizeof c.Q);   // Q = timesca_thermo^2 temp, Q(1) x L
+    const double tb = p.timesca_baro * ctx->u.time;
+    for (int k = 0; k < p.nhc_n; ++k) c.Qb[k] = tb * tb * c.temp;   // Qb(1) x 9 (src/integration.f90:995-996)
+    c.Qb[0] = c.Qb[0] * 9.0;
+    c.W = (c.L + 1.0) * tb * tb * c.temp;
+    c.press = p.press * ctx->u.press;
+}
+
+// sum m v^2 of the current velocities (scaled by s first when apply), on the host
+int npt_ke2(mdff_ctx* ctx, bool apply, double s, double& ke2) {
+    if (apply) CK(cudaMemcpyAsync(&ctx->dsc->s_scale, &s, sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    TRY(ke_reduce(ctx, apply ? 1 : 0));
+    CK(cudaMemcpyAsync(&ctx->hsc->ke2[0], &ctx->dsc->ke2[0], sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ke2 = ctx->hsc->ke2[0];
+    return MDFF_OK;
+}
+
+// virial pressure of the last force evaluation (pvirial_tot, eV / A^3)
+double npt_pvirial(const mdff_ctx* ctx) {
+    return (ctx->en.vir_lj + ctx->en.vir_morse + ctx->en.vir_bmhft) / ctx->cell.omega + ctx->en.pvirial_coul;
+}
+
+// nhcnp (src/integration.f90:966-1042) with the corrections listed in npt.cuh
+int npt_step(mdff_ctx* ctx) {
+    const int n = ctx->n;
+    NptConst c;
+    npt_const(ctx, c);
+    NptState& st = ctx->npt;
+    const double dt = c.dt, dt2 = dt * 0.5, dt4 = dt2 * 0.5;
+    const double odnf = 1.0 + 3.0 / c.L;
+    double ke2, s, sb;
+    auto kick_ve = [&](double ke2_) {   // D15, D17
+        const double omega = ctx->cell.omega;
+        const double P_kin = odnf * ke2_ / (3.0 * omega);
+        const double Ge = 3.0 * omega * (P_kin + npt_pvirial(ctx) - c.press);
+        st.ve = st.ve + Ge * dt2;
+    };
+    // first half: barostat and particle chains, velocities scaled, barostat kick
+    TRY(npt_ke2(ctx, false, 1.0, ke2));
+    npt_chain_half(c, st, 0.5 * ke2, true, s, sb);
+    TRY(npt_ke2(ctx, true, s, ke2));
+    st.ve = st.ve * sb;
+    kick_ve(ke2);
+    // prop_pos_vel_verlet_npt (src/integration.f90:1049-1160)
+    double arg = odnf * st.ve * dt4 / c.W;
+    double aa = std::exp(-arg);
+    double AA2 = aa * aa, BB = aa * dt2 * npt_poly(arg);
+    ctx->prof.begin(PK_INTEGRATE);
+    k_npt_kick<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mass, AA2, BB,
+                                           ctx->part.buf);
+    ctx->prof.end(1);
+    st.xe = st.xe + st.ve * dt / c.W;
+    const double g = std::exp(st.xe - st.xe0);
+    double A[9];
+    for (int k = 0; k < 9; ++k) A[k] = ctx->A_cur[k] * g;
+    st.xe0 = st.xe;
+    st.scale *= g;
+    TRY(apply_cell(ctx, A));
+    arg = st.ve * dt2 / c.W;
+    aa = std::exp(arg);
+    AA2 = aa * aa;
+    BB = aa * npt_poly(arg) * dt;
+    ctx->prof.begin(PK_INTEGRATE);
+    k_npt_drift<<<nb(n), 256, 0, ctx->st>>>(n, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, AA2, BB);
+    ctx->prof.end(1);
+    TRY(check_launch(ctx, "npt drift"));
+    TRY(engforce_device(ctx));
+    arg = odnf * st.ve * dt4 / c.W;
+    aa = std::exp(-arg);
+    AA2 = aa * aa;
+    BB = aa * npt_poly(arg) * dt2;
+    ctx->prof.begin(PK_INTEGRATE);
+    k_npt_kick<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mass, AA2, BB,
+                                           ctx->part.buf);
+    launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
+    ctx->prof.end(2);
+    TRY(check_launch(ctx, "npt kick"));
+    CK(cudaMemcpyAsync(&ctx->hsc->ke2[0], &ctx->dsc->ke2[0], sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ke2 = ctx->hsc->ke2[0];
+    // second half: barostat kick, particle and barostat chains
+    kick_ve(ke2);
+    npt_chain_half(c, st, 0.5 * ke2, false, s, sb);
+    TRY(npt_ke2(ctx, true, s, ke2));
+    st.ve = st.ve * sb;
+    st.e_npt = npt_energy(c, st, ctx->cell.omega);
+    return MDFF_OK;
+}
+
 // One MD step (body of md_run's loop, src/runmd.f90:266-277).
 int md_step(mdff_ctx* ctx) {
     const int n = ctx->n;
     const mdff_params& p = ctx->p;
     const double dt = p.dt * ctx->u.time;
     ctx->itime++;
-    if (p.integrator == MDFF_NVE_VV) {
+    if (p.integrator == MDFF_NPT_NHCNP) {
+        TRY(npt_step(ctx));
+    } else if (p.integrator == MDFF_NVE_VV) {
         ctx->prof.begin(PK_INTEGRATE);
         k_vv_positions<<<nb(n), 256, 0, ctx->st>>>(n, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy,
                                                    ctx->fz, ctx->fox, ctx->foy, ctx->foz, ctx->mass, dt);
@@ -1060,7 +1207,11 @@ int md_step(mdff_ctx* ctx) {
     if (p.lvnlist) {
         // positions unchanged since the force call: sx is current
         ctx->prof.begin(PK_NLIST);
-        launch_skin_check(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->xs, ctx->ys, ctx->zs, ctx->cell, p.skindiff,
+        // a shrinking cell brings pairs beyond the list radius closer by the
+        // same factor: that margin comes off the displacement allowance
+        const double shrink = std::max(0.0, 1.0 - ctx->npt.scale / ctx->npt.scale_build);
+        const double skin_eff = p.skindiff - shrink * rlist_max(ctx, p.skindiff);
+        launch_skin_check(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->xs, ctx->ys, ctx->zs, ctx->cell, skin_eff,
                           ctx->part, ctx->dsc);
         ctx->prof.end(2);
         TRY(check_launch(ctx, "skin"));
@@ -1669,6 +1820,8 @@ void mdff_params_default(mdff_params* p) {
     p->mixed_ksplit = 2.5;
     p->mixed_keps = 1e-7;
     p->kspace_tc = 1;
+    p->press = 0.0;
+    p->timesca_baro = 1.0;   // md_default_tag (src/md.f90:204)
 }
 
 int mdff_create(const mdff_params* p, mdff_ctx** out) {
@@ -1731,6 +1884,8 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
     ctx->ntype = p.ntype;
     lattice(A, ctx->cell, ctx->W, ctx->anorm);
     if (!(ctx->cell.omega > 0.0)) return fail(ctx, MDFF_E_ARG, "cell volume must be positive");
+    std::memcpy(ctx->A_cur, A, sizeof ctx->A_cur);
+    ctx->npt = NptState();
     ctx->natmi.assign(NT, 0);
     std::vector<int> t0(n);
     std::vector<double> hq(n), hm(n), ha(n), hia(n), hd(3 * (size_t)n);
@@ -1758,6 +1913,9 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
     else ctx->cut_coul = p.cutlongrange;
     std::vector<PairConst> tab;
     build_pair_consts(ctx, tab);
+    ctx->omega0 = ctx->cell.omega;
+    ctx->utail0 = ctx->utail;
+    ctx->ptail0 = ctx->ptail;
     // device buffers
     double** d1[] = {&ctx->x, &ctx->y, &ctx->z, &ctx->vx, &ctx->vy, &ctx->vz, &ctx->fx, &ctx->fy, &ctx->fz,
                      &ctx->fox, &ctx->foy, &ctx->foz, &ctx->sx, &ctx->sy, &ctx->sz, &ctx->xs, &ctx->ys, &ctx->zs,
@@ -2000,6 +2158,14 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
             }
             CK(cudaStreamSynchronize(ctx->st));   // the host vectors above go out of scope
         }
+        {   // k membership for cell changes (constant pressure, mdff_set_cell)
+            std::vector<unsigned char> mk(kg.nrect);
+            for (int r = 0; r < kg.nrect; ++r)
+                mk[r] = (unsigned char)((ak[r] != 0.0 ? 1 : 0) | (akhi[r] != 0.0 ? 2 : 0));
+            TRY(dalloc(ctx, &kg.mask, kg.nrect));
+            CK(cudaMemcpyAsync(kg.mask, mk.data(), kg.nrect, cudaMemcpyHostToDevice, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+        }
         size_t fp = 0;
         size_t pc = std::max(tc_part, rec_scratch_doubles(n, kg, &fp, p.precision == MDFF_PREC_MIXED));
         fp = std::max(fp, (size_t)tcf::NQ * 9 * n);   // the tensor-core field pass writes NQ column parts
@@ -2029,6 +2195,16 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
     ctx->itime = 0;
     ctx->have_system = true;
     if (p.lvnlist) TRY(build_lists(ctx, p.skindiff));
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+int mdff_set_cell(mdff_ctx* ctx, const double A[9]) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!A) return fail(ctx, MDFF_E_ARG, "mdff_set_cell: A is NULL");
+    cudaSetDevice(ctx->p.device);
+    TRY(apply_cell(ctx, A));
+    if (ctx->p.lvnlist) TRY(build_lists(ctx, ctx->p.skindiff));
     CK(cudaStreamSynchronize(ctx->st));
     return MDFF_OK;
 }
@@ -2131,6 +2307,13 @@ int mdff_md_start(mdff_ctx* ctx, const double* vx, const double* vy, const doubl
     CK(cudaMemsetAsync(ctx->dsc->xi, 0, sizeof(double) * 16, ctx->st));
     CK(cudaMemsetAsync(ctx->dsc->vxi, 0, sizeof(double) * 16, ctx->st));
     CK(cudaMemsetAsync(&ctx->dsc->e_nvt, 0, sizeof(double), ctx->st));
+    {   // xe = ve = 0 (md_check_tag, src/md.f90:349-350); the cell stays as set
+        const double sc = ctx->npt.scale, sb = ctx->npt.scale_build;
+        ctx->npt = NptState();
+        ctx->npt.scale = sc;
+        ctx->npt.scale_build = sb;
+        if (ctx->p.integrator == MDFF_NPT_NHCNP) ctx->npt.e_npt = ctx->p.press * ctx->u.press * ctx->cell.omega;
+    }
     ctx->itime = 0;
     TRY(ke_reduce(ctx, 0));
     TRY(engforce_device(ctx));   // syncs the scalars
@@ -2583,8 +2766,10 @@ struct CkHost {
     double e_kin, temp_r;
     mdff_energies en;
     double tau_nonb[9], tau_coul[9];
+    double A_cur[9];
+    NptState npt;
 };
-constexpr char CK_MAGIC[8] = {'M', 'D', 'F', 'F', 'C', 'K', 'P', '1'};
+constexpr char CK_MAGIC[8] = {'M', 'D', 'F', 'F', 'C', 'K', 'P', '2'};
 
 // the device arrays of the state, in file order
 std::vector<std::pair<double*, size_t>> ck_arrays(mdff_ctx* ctx) {
@@ -2624,7 +2809,7 @@ int mdff_checkpoint_save(mdff_ctx* ctx, void* buf, size_t cap, size_t* len) {
     cudaSetDevice(ctx->p.device);
     CkHost hdr{};
     std::memcpy(hdr.magic, CK_MAGIC, 8);
-    hdr.version = 1;
+    hdr.version = 2;
     hdr.n = ctx->n;
     hdr.ntype = ctx->ntype;
     hdr.nhist = ctx->nhist;
@@ -2645,6 +2830,8 @@ int mdff_checkpoint_save(mdff_ctx* ctx, void* buf, size_t cap, size_t* len) {
     hdr.en = ctx->en;
     std::memcpy(hdr.tau_nonb, ctx->tau_nonb, sizeof hdr.tau_nonb);
     std::memcpy(hdr.tau_coul, ctx->tau_coul, sizeof hdr.tau_coul);
+    std::memcpy(hdr.A_cur, ctx->A_cur, sizeof hdr.A_cur);
+    hdr.npt = ctx->npt;
     char* o = (char*)buf;
     std::memcpy(o, &hdr, sizeof hdr);
     o += sizeof hdr;
@@ -2666,7 +2853,7 @@ int mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len) {
     if (!buf || len < sizeof(CkHost)) return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: no checkpoint");
     CkHost hdr;
     std::memcpy(&hdr, buf, sizeof hdr);
-    if (std::memcmp(hdr.magic, CK_MAGIC, 8) != 0 || hdr.version != 1)
+    if (std::memcmp(hdr.magic, CK_MAGIC, 8) != 0 || hdr.version != 2)
         return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: not a checkpoint of this library");
     if (hdr.n != ctx->n || hdr.ntype != ctx->ntype || hdr.nhist != ctx->nhist ||
         hdr.nparam_bytes != (int)sizeof(mdff_params))
@@ -2678,6 +2865,9 @@ int mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len) {
         return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: parameters differ from the checkpoint's");
     in += sizeof pp;
     cudaSetDevice(ctx->p.device);
+    // the cell of the checkpoint (constant pressure moves it), then the state
+    if (std::memcmp(hdr.A_cur, ctx->A_cur, sizeof hdr.A_cur) != 0) TRY(apply_cell(ctx, hdr.A_cur));
+    ctx->npt = hdr.npt;
     CK(cudaMemcpyAsync(ctx->dsc, in, sizeof(DevScalars), cudaMemcpyHostToDevice, ctx->st));
     std::memcpy((void*)ctx->hsc, in, sizeof(DevScalars));
     in += sizeof(DevScalars);
@@ -2688,10 +2878,13 @@ int mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len) {
     // the neighbour lists as they were built: from the build-time fractional
     // coordinates, so their pair order (and every sum over them) is unchanged
     if (hdr.have_list) {
+        const double sc = ctx->npt.scale;
+        ctx->npt.scale = hdr.npt.scale_build;   // the list as built, at its build-time cell scale
         CK(cudaMemcpyAsync(ctx->sx, ctx->xs, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->sy, ctx->ys, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->sz, ctx->zs, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
         TRY(build_lists(ctx, ctx->p.lvnlist ? ctx->p.skindiff : 0.0, true));
+        ctx->npt.scale = sc;
     }
     launch_frac(ctx->st, ctx->n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
     TRY(check_launch(ctx, "checkpoint frac"));

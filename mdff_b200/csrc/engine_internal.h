@@ -224,6 +224,7 @@ struct KGrid {
     double* Ak_hi = nullptr;   // [nrect], Ak of the FP32 set: without the low-|k| set and outside the sphere (mixed path)
     int* colrange = nullptr;   // [ncol][2]: first 16-wide nz chunk and chunk count of the FP32 set (mixed path)
     int* items = nullptr;      // [nitems][2]: (column, chunk) work list of the FP32 structure factor
+    unsigned char* mask = nullptr;   // [nrect]: bit 1 in the half space, bit 2 in the FP32 set (fixed at set-up)
     int nitems = 0;
 };
 // The low-|k| set of the mixed path, summed in FP64 (see ewald_recip.cuh):

@@ -33,6 +33,13 @@
 //       conserved.  Here the inner chain forces are refreshed first (the
 //       Martyna-Tuckerman-Klein order); identical to the reference for M = 2.
 //       nhc_literal = 1 restores the reference's order.
+//   D14-D17 constant pressure (nhcnp, src/integration.f90:715-1160): the
+//       k mesh and tail corrections follow the cell (the reference keeps
+//       those of the start-up cell); the barostat momentum gets both half
+//       kicks (the reference's trotter orders -1/+1 give one); chain forces
+//       G = p^2/Q - kT and Gb_1 = ve^2/W - kT (the reference halves them);
+//       kinetic pressure (1 + 3/Nf) 2K/3V (the reference uses K).  With
+//       these the reference's e_npt + e_tot is conserved.
 //   D12 errfc: the reference's fitted erfc (src/functions.f90:28-39, a
 //       published Chebyshev fit, relative error ~1.2e-7) is selectable with
 //       orc_set_erfc_mode(sys, 0); mode 1 (default) uses libm erfc.
@@ -189,6 +196,11 @@ struct orc_sys {
     // MD state (md.f90:60-62)
     std::vector<double> xi, vxi;
     double dt = 0.0, temp = 0.0, timesca = 0.0;
+    // constant pressure (md.f90:60-62): barostat chain, log-volume and momentum
+    std::vector<double> xib, vxib;
+    double xe = 0.0, ve = 0.0, xe0 = 0.0, e_npt = 0.0;
+    double scale = 1.0, scale_build = 1.0;   // linear cell scale now / at the last list build
+    double omega0 = 0.0, utail0 = 0.0, ptail0 = 0.0;
     int erfc_mode = 1;
     // outputs of the last engforce
     mdff_energies en;
@@ -366,6 +378,7 @@ void vnlist_pbc(orc_sys* s) {
     pack(s->coul, lc);
     s->xs = sx; s->ys = sy; s->zs = sz;   // D10
     s->have_list = true;
+    s->scale_build = s->scale;
 }
 
 // vnlistcheck (src/tools.f90:446-535): largest + second largest displacement
@@ -381,7 +394,11 @@ bool vnlistcheck(orc_sys* s) {
         if (drnei > dmax) { dmax2 = dmax; dmax = drnei; }
         else if (drnei > dmax2) dmax2 = drnei;
     }
-    if (dmax + dmax2 > s->p.skindiff) { vnlist_pbc(s); return true; }
+    // a shrinking cell (constant pressure) brings pairs beyond the list radius
+    // closer by the same factor: that margin comes off the allowance
+    const double shrink = std::max(0.0, 1.0 - s->scale / s->scale_build);
+    const double rl = std::max(s->vdw.cut, s->coul.cut) + s->p.skindiff;
+    if (dmax + dmax2 > s->p.skindiff - shrink * rl) { vnlist_pbc(s); return true; }
     return false;
 }
 
@@ -1289,6 +1306,164 @@ void nhcn(orc_sys* s) {
     s->e_nvt = nvt1 + nvt2 + nvt3 + nvt4;
 }
 
+// A new cell for the same atoms (D14): lattice, tail corrections and k mesh.
+void set_cell(orc_sys* s, const double A[3][3]) {
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) s->cell.A[i][j] = A[i][j];
+    lattice(s->cell);
+    const double r = s->omega0 / s->cell.omega;
+    s->utail = s->utail0 * r;
+    s->ptail = s->ptail0 * r * r;
+    if (s->p.lcoulomb) kpoint_sum_init(s);
+}
+
+// chain_nhcnp (src/integration.f90:724-964), one half: first = barostat chain
+// then particle chain (trotter order -1), else particle then barostat (+1);
+// D13 and D16 as in the header.  Velocities scaled by s, ve by sb; kin
+// recomputed from the scaled velocities.
+void chain_nhcnp(orc_sys* s, double& kin, const std::vector<double>& Q, const std::vector<double>& Qb, double W,
+                 double L, bool first) {
+    const mdff_params& p = s->p;
+    const int nhc = p.nhc_n;
+    double yw[9] = {0};
+    switch (p.nhc_yosh_order) {
+        case 1: yw[0] = 1.0; break;
+        case 3: yw[0] = 1.0 / (2.0 - std::pow(2.0, 1.0 / 3.0)); yw[1] = 1.0 - 2.0 * yw[0]; yw[2] = yw[0]; break;
+        case 5: yw[0] = 1.0 / (4.0 - std::pow(4.0, 1.0 / 3.0)); yw[1] = yw[0]; yw[2] = yw[0]; yw[3] = yw[0]; yw[4] = 1.0 - 4.0 * yw[0]; break;
+        case 7:
+            yw[0] = .78451361047756; yw[1] = .235573213359357; yw[2] = -1.17767998417887;
+            yw[3] = 1.0 - 2.0 * (yw[0] + yw[1] + yw[2]); yw[4] = yw[2]; yw[5] = yw[1]; yw[6] = yw[0]; break;
+        default:
+            yw[0] = 0.192; yw[1] = 0.554910818409783619692725006662999; yw[2] = 0.124659619941888644216504240951585;
+            yw[3] = -0.843182063596933505315033808282941; yw[4] = 1.0 - 2.0 * (yw[0] + yw[1] + yw[2] + yw[3]);
+            yw[5] = yw[3]; yw[6] = yw[2]; yw[7] = yw[1]; yw[8] = yw[0]; break;
+    }
+    const double temp = s->temp;
+    std::vector<double> G(nhc, 0.0), Gb(nhc, 0.0);
+    double sc = 1.0, sb = 1.0;
+    G[0] = 2.0 * kin - L * temp;
+    Gb[0] = s->ve * s->ve / W - temp;
+    // one Trotter piece of a chain (src/integration.f90:830-877)
+    auto piece = [&](std::vector<double>& v, std::vector<double>& x, const std::vector<double>& q,
+                     std::vector<double>& g, double& f, bool baro, double dts) {
+        double dts2 = dts * 0.5, dts4 = dts2 * 0.5, dts8 = dts4 * 0.5;
+        g[nhc - 1] = v[nhc - 2] * v[nhc - 2] / q[nhc - 2] - temp;
+        if (!p.nhc_literal)
+            for (int inh = 1; inh < nhc - 1; ++inh) g[inh] = v[inh - 1] * v[inh - 1] / q[inh - 1] - temp;
+        v[nhc - 1] = v[nhc - 1] + g[nhc - 1] * dts4;
+        for (int inh = nhc - 2; inh >= 0; --inh) {
+            v[inh] = v[inh] * std::exp(-v[inh + 1] * dts8 / q[inh + 1]);
+            v[inh] = v[inh] + g[inh] * dts4;
+            v[inh] = v[inh] * std::exp(-v[inh + 1] * dts8 / q[inh + 1]);
+        }
+        f = f * std::exp(-v[0] * dts2 / q[0]);
+        for (int inh = 0; inh < nhc; ++inh) x[inh] = x[inh] + v[inh] * dts2 / q[inh];
+        g[0] = baro ? s->ve * s->ve * f * f / W - temp : 2.0 * kin * f * f - L * temp;
+        for (int inh = 0; inh < nhc - 1; ++inh) {
+            v[inh] = v[inh] * std::exp(-v[inh + 1] * dts8 / q[inh + 1]);
+            v[inh] = v[inh] + g[inh] * dts4;
+            v[inh] = v[inh] * std::exp(-v[inh + 1] * dts8 / q[inh + 1]);
+            g[inh + 1] = v[inh] * v[inh] / q[inh] - temp;
+        }
+        v[nhc - 1] = v[nhc - 1] + g[nhc - 1] * dts4;
+    };
+    for (int k = 0; k < p.nhc_mults; ++k)
+        for (int j = 0; j < p.nhc_yosh_order; ++j) {
+            double dts = yw[j] * s->dt / double(p.nhc_mults);
+            if (first) {
+                piece(s->vxib, s->xib, Qb, Gb, sb, true, dts);
+                piece(s->vxi, s->xi, Q, G, sc, false, dts);
+            } else {
+                piece(s->vxi, s->xi, Q, G, sc, false, dts);
+                piece(s->vxib, s->xib, Qb, Gb, sb, true, dts);
+            }
+        }
+    kin = 0.0;
+    for (int ia = 0; ia < s->natm; ++ia) {
+        s->vx[ia] = sc * s->vx[ia];
+        s->vy[ia] = sc * s->vy[ia];
+        s->vz[ia] = sc * s->vz[ia];
+        kin = kin + (s->vx[ia] * s->vx[ia] + s->vy[ia] * s->vy[ia] + s->vz[ia] * s->vz[ia]) * s->massia[ia];
+    }
+    kin = kin * 0.5;
+    s->ve = s->ve * sb;
+}
+
+// nhcnp (src/integration.f90:966-1042) with prop_pos_vel_verlet_npt
+// (:1049-1160); D15, D17: ve += Ge dt/2 after the first chain half and before
+// the second, Ge = 3V ((1 + 3/L) 2K / 3V + pvirial - press).
+void nhcnp(orc_sys* s) {
+    const mdff_params& p = s->p;
+    const double L = 3.0 * double(s->natm);
+    std::vector<double> Q(p.nhc_n, s->timesca * s->timesca * s->temp), Qb(p.nhc_n);
+    Q[0] = Q[0] * L;
+    const double tb = p.timesca_baro * s->u.time;
+    for (int k = 0; k < p.nhc_n; ++k) Qb[k] = tb * tb * s->temp;
+    Qb[0] = Qb[0] * 9.0;
+    const double W = (L + 1.0) * tb * tb * s->temp;
+    const double press = p.press * s->u.press;
+    const double odnf = 1.0 + 3.0 / L, dt = s->dt, dt2 = dt * 0.5, dt4 = dt2 * 0.5;
+    auto pvirial = [&]() { return (s->en.vir_lj + s->en.vir_morse + s->en.vir_bmhft) / s->cell.omega + s->en.pvirial_coul; };
+    auto kick_ve = [&](double kin) {
+        double P_kin = odnf * 2.0 * kin / (3.0 * s->cell.omega);
+        double Ge = 3.0 * s->cell.omega * (P_kin + pvirial() - press);
+        s->ve = s->ve + Ge * dt2;
+    };
+    auto poly = [](double arg) {
+        const double e2 = 1.0 / 6.0, e4 = e2 / 20.0, e6 = e4 / 42.0, e8 = e6 / 72.0;
+        double a2 = arg * arg;
+        return (((e8 * a2 + e6) * a2 + e4) * a2 + e2) * a2 + 1.0;
+    };
+    double tempi, kin;
+    calc_temp(s, tempi, kin);
+    chain_nhcnp(s, kin, Q, Qb, W, L, true);
+    kick_ve(kin);
+    double arg = odnf * s->ve * dt4 / W;
+    double aa = std::exp(-arg), AA2 = aa * aa, BB = aa * dt2 * poly(arg);
+    for (int ia = 0; ia < s->natm; ++ia) {
+        s->vx[ia] = s->vx[ia] * AA2 + s->fx[ia] * BB / s->massia[ia];
+        s->vy[ia] = s->vy[ia] * AA2 + s->fy[ia] * BB / s->massia[ia];
+        s->vz[ia] = s->vz[ia] * AA2 + s->fz[ia] * BB / s->massia[ia];
+    }
+    s->xe = s->xe + s->ve * dt / W;
+    const double g = std::exp(s->xe - s->xe0);
+    double A[3][3];
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) A[i][j] = s->cell.A[i][j] * g;
+    s->xe0 = s->xe;
+    s->scale = s->scale * g;
+    set_cell(s, A);
+    arg = s->ve * dt2 / W;
+    aa = std::exp(arg);
+    AA2 = aa * aa;
+    BB = aa * poly(arg) * dt;
+    for (int ia = 0; ia < s->natm; ++ia) {
+        s->rx[ia] = s->rx[ia] * AA2 + s->vx[ia] * BB;
+        s->ry[ia] = s->ry[ia] * AA2 + s->vy[ia] * BB;
+        s->rz[ia] = s->rz[ia] * AA2 + s->vz[ia] * BB;
+    }
+    engforce(s);
+    arg = odnf * s->ve * dt4 / W;
+    aa = std::exp(-arg);
+    AA2 = aa * aa;
+    BB = aa * poly(arg) * dt2;
+    kin = 0.0;
+    for (int ia = 0; ia < s->natm; ++ia) {
+        s->vx[ia] = s->vx[ia] * AA2 + s->fx[ia] * BB / s->massia[ia];
+        s->vy[ia] = s->vy[ia] * AA2 + s->fy[ia] * BB / s->massia[ia];
+        s->vz[ia] = s->vz[ia] * AA2 + s->fz[ia] * BB / s->massia[ia];
+        kin = kin + (s->vx[ia] * s->vx[ia] + s->vy[ia] * s->vy[ia] + s->vz[ia] * s->vz[ia]) * s->massia[ia];
+    }
+    kin = kin * 0.5;
+    kick_ve(kin);
+    chain_nhcnp(s, kin, Q, Qb, W, L, false);
+    calc_temp(s, s->temp_r, s->e_kin);
+    double e = press * s->cell.omega + s->ve * s->ve * 0.5 / W + L * s->temp * s->xi[0] + s->temp * s->xib[0] +
+               s->vxi[0] * s->vxi[0] * 0.5 / Q[0] + s->vxib[0] * s->vxib[0] * 0.5 / Qb[0];
+    for (int k = 1; k < p.nhc_n; ++k)
+        e = e + s->vxi[k] * s->vxi[k] * 0.5 / Q[k] + s->vxib[k] * s->vxib[k] * 0.5 / Qb[k] + s->temp * s->xi[k] +
+            s->temp * s->xib[k];
+    s->e_npt = e;
+}
+
 // calc_thermo (src/thermo.f90:116-207), non-reduced output path.
 void calc_thermo(orc_sys* s, mdff_thermo* t, int step) {
     double omega = s->cell.omega;
@@ -1300,8 +1475,9 @@ void calc_thermo(orc_sys* s, mdff_thermo* t, int step) {
     t->u_coul = s->en.u_coul / nr; t->u_pol = s->en.u_pol / nr;
     t->u_tot = t->u_lj + t->u_coul + t->u_morse + t->u_bmhft;
     t->e_tot = t->u_tot + t->e_kin;
-    t->e_nvt = s->e_nvt / nr;
-    t->h_tot = (s->p.integrator == MDFF_NVT_NHCN) ? t->e_tot + t->e_nvt : t->e_tot;
+    t->e_nvt = (s->p.integrator == MDFF_NPT_NHCNP ? s->e_npt : s->e_nvt) / nr;
+    t->h_tot = (s->p.integrator == MDFF_NVE_VV) ? t->e_tot : t->e_tot + t->e_nvt;   // thermo.f90:184-199
+    t->volume = omega;
     double pv = (s->en.vir_lj + s->en.vir_morse + s->en.vir_bmhft) / omega / nr + s->en.pvirial_coul / nr;
     t->pvirial_tot = pv / s->u.press;
     t->pressure_tot = (pv + s->temp_r * s->u.boltz / omega) / s->u.press;
@@ -1878,6 +2054,11 @@ orc_sys* orc_create(const mdff_params* p, int natm, const int* itype, const doub
     s->timesca = s->p.timesca_thermo * s->u.time;
     s->xi.assign(std::max(2, s->p.nhc_n), 0.0);
     s->vxi.assign(std::max(2, s->p.nhc_n), 0.0);
+    s->xib.assign(std::max(2, s->p.nhc_n), 0.0);
+    s->vxib.assign(std::max(2, s->p.nhc_n), 0.0);
+    s->omega0 = s->cell.omega;
+    s->utail0 = s->utail;
+    s->ptail0 = s->ptail;
     if (s->p.lvnlist) vnlist_pbc(s);
     return s;
 }
@@ -2041,6 +2222,10 @@ int orc_md_start(orc_sys* s, const double* vx, const double* vy, const double* v
     s->itime = 0;
     engforce(s);
     s->e_nvt = 0.0;
+    s->xe = s->ve = s->xe0 = 0.0;
+    s->e_npt = s->p.integrator == MDFF_NPT_NHCNP ? s->p.press * s->u.press * s->cell.omega : 0.0;   // P V, at rest
+    std::fill(s->xib.begin(), s->xib.end(), 0.0);
+    std::fill(s->vxib.begin(), s->vxib.end(), 0.0);
     s->step_rebuilt = 0;
     if (t0) calc_thermo(s, t0, 0);
     return 0;
@@ -2058,6 +2243,7 @@ int orc_step(orc_sys* s, int nsteps, double* rx, double* ry, double* rz, double*
     for (int k = 0; k < nsteps; ++k) {
         s->itime++;
         if (s->p.integrator == MDFF_NVT_NHCN) nhcn(s);
+        else if (s->p.integrator == MDFF_NPT_NHCNP) nhcnp(s);
         else prop_velocity_verlet(s);
         s->step_rebuilt = 0;
         if (s->p.lvnlist) s->step_rebuilt = vnlistcheck(s) ? 1 : 0;

@@ -412,6 +412,7 @@ int build_lists(mdff_ctx* ctx, double skin, bool from_frac = false) {
     ctx->have_list = true;
     ctx->nrebuild++;
     ctx->npt.scale_build = ctx->npt.scale;
+    std::memcpy(ctx->npt.A_build, ctx->A_cur, sizeof ctx->A_cur);
     return MDFF_OK;
 }
 
@@ -2215,6 +2216,8 @@ int mdff_set_positions(mdff_ctx* ctx, const double* rx, const double* ry, const 
     TRY(upload(ctx, ctx->x, rx, ctx->n));
     TRY(upload(ctx, ctx->y, ry, ctx->n));
     TRY(upload(ctx, ctx->z, rz, ctx->n));
+    // a list built for other positions is not a list of these
+    if (ctx->p.lvnlist) TRY(build_lists(ctx, ctx->p.skindiff));
     CK(cudaStreamSynchronize(ctx->st));
     ctx->forces_valid = false;
     return MDFF_OK;
@@ -2878,13 +2881,27 @@ int mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len) {
     // the neighbour lists as they were built: from the build-time fractional
     // coordinates, so their pair order (and every sum over them) is unchanged
     if (hdr.have_list) {
-        const double sc = ctx->npt.scale;
-        ctx->npt.scale = hdr.npt.scale_build;   // the list as built, at its build-time cell scale
+        // the build-time cell (it differs from the current one under constant
+        // pressure): the list's binning and distances as they were
+        const CellP cur = ctx->cell;
+        double W[3], an[3], Acur[9];
+        std::memcpy(W, ctx->W, sizeof W);
+        std::memcpy(an, ctx->anorm, sizeof an);
+        std::memcpy(Acur, ctx->A_cur, sizeof Acur);
+        const bool other = std::memcmp(hdr.npt.A_build, Acur, sizeof Acur) != 0 && hdr.npt.A_build[0] != 0.0;
+        if (other) {
+            lattice(hdr.npt.A_build, ctx->cell, ctx->W, ctx->anorm);
+            std::memcpy(ctx->A_cur, hdr.npt.A_build, sizeof Acur);
+        }
         CK(cudaMemcpyAsync(ctx->sx, ctx->xs, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->sy, ctx->ys, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->sz, ctx->zs, sizeof(double) * ctx->n, cudaMemcpyDeviceToDevice, ctx->st));
         TRY(build_lists(ctx, ctx->p.lvnlist ? ctx->p.skindiff : 0.0, true));
-        ctx->npt.scale = sc;
+        ctx->cell = cur;
+        std::memcpy(ctx->W, W, sizeof W);
+        std::memcpy(ctx->anorm, an, sizeof an);
+        std::memcpy(ctx->A_cur, Acur, sizeof Acur);
+        ctx->npt = hdr.npt;   // build_lists recorded its own scale and cell
     }
     launch_frac(ctx->st, ctx->n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
     TRY(check_launch(ctx, "checkpoint frac"));

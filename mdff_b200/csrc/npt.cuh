@@ -102,6 +102,7 @@ struct NptState {
     double xe = 0.0, ve = 0.0, xe0 = 0.0;
     double e_npt = 0.0;
     double scale = 1.0, scale_build = 1.0;   // linear cell scale now / at the last list build
+    double A_build[9] = {0};                 // the cell (column-major) of the last list build
 };
 
 struct NptConst {

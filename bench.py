@@ -61,6 +61,9 @@ def parse():
                          "force-matching loss and adjoint gradient; opt: conjugate-gradient structure optimisation; "
                          "efg: EFG statistics and distributions over many configurations")
     ap.add_argument("--efg-conf", type=int, default=128, help="efg workload: configurations per step")
+    ap.add_argument("--ensemble", default="nvt", choices=["nvt", "npt"],
+                    help="production workload: Nose-Hoover chains at constant volume (the headline) or the "
+                         "isotropic barostat at 0 GPa (timesca_baro 0.5 ps)")
     ap.add_argument("--accuracy", action="store_true",
                     help="error of the mixed path against the FP64 path on snapshots of an FP64 trajectory")
     ap.add_argument("--snapshots", type=int, default=3)
@@ -176,6 +179,10 @@ def run_engine(args):
     p = s["params"]
     p.precision = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
     p.device = local
+    if args.ensemble == "npt":
+        p.integrator = abi.NPT_NHCNP
+        p.press = 0.0
+        p.timesca_baro = 0.5
     p.algo_ext_dipole = abi.EXT_ASPC if args.ext == "aspc" else abi.EXT_POLY
     p.extrapolate_order = args.ext_order
     p.kspace_reuse = (1 if args.precision == "mixed" else 0) if args.reuse == "auto" else int(args.reuse)
@@ -378,7 +385,8 @@ def run_engine(args):
             "dtype": "fp32+fp64" if args.precision == "mixed" else "fp64",
             "data": "synthetic (seeded MgO polarisable-ion cell, mdff_b200.systems.mgo_production)",
             "config": {"workload": "mgo-pim-production", "natm": natm, "kmax": list(p.kES), "k_vectors": ki,
-                       "rc": p.cutlongrange, "alpha": p.alphaES, "ensemble": "nvt-nhcn", "nhc_n": p.nhc_n,
+                       "rc": p.cutlongrange, "alpha": p.alphaES,
+                       "ensemble": "npt-nhcnp (0 GPa)" if args.ensemble == "npt" else "nvt-nhcn", "nhc_n": p.nhc_n,
                        "dt_ps": p.dt, "efg_period": p.efg_period, "solver": "pcg", "tol": p.conv_tol_ind,
                        "predictor": "%s order %d" % (args.ext, args.ext_order),
                        "kspace_reuse": int(p.kspace_reuse),

@@ -242,6 +242,13 @@ module mdff_engine
       real(c_double), intent(out) :: fx(*), fy(*), fz(*)
       type(mdff_thermo_t), intent(out) :: thermo(*)
     end function
+    ! a new cell (column-major) for the same atoms: lattice, tail corrections, k tables
+    integer(c_int) function mdff_set_cell(ctx, a) bind(C, name="mdff_set_cell")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: a(9)
+    end function
+
     ! streaming writer: frames of the context's state, written in the background
     integer(c_int) function mdff_writer_open(ctx, path, file, iformat, data, h, nslot, w) &
         bind(C, name="mdff_writer_open")

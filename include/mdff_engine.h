@@ -535,6 +535,44 @@ int  mdff_writer_close(mdff_writer* w);
 int  mdff_checkpoint_save(mdff_ctx* ctx, void* buf, size_t cap, size_t* len);
 int  mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len);
 
+/* ---- pair distribution and reverse Monte Carlo (rmc.f90, radial_distrib.f90) ----
+ * g(r) as rmc_gr forms it (gr_main, src/radial_distrib.f90, normalised as
+ * src/rmc.f90:1469-1490): nbins = INT(cut/res) + 1; rows mp = 0 (all pairs,
+ * over natm^2) then the type pairs it1 <= it2 (over natmi(it1) natmi(it2)),
+ * grr[(npairs+1)][nbins], npairs = ntype (ntype+1) / 2; at most 4 types.
+ * grr NULL: *nbins only. */
+int  mdff_gr(mdff_ctx* ctx, double cut, double res, double* grr, int* nbins);
+
+/* rmc_main (src/rmc.f90:196-640) on the g(r) chi^2: single-atom trial moves
+ * of up to max_displacement / ANORM per fractional axis (rmc_move), g(r)
+ * chi^2 against grr_exp [(npairs+1)][nbins] (eval_chisq_rmc), the
+ * Metropolis test of each chi^2 component with exp(-dchi^2 / 2 T) and the
+ * total deciding.  temp_rmc[0..4]: the components' temperatures (g(r), var,
+ * U, Vzz, eta), temp_rmc[5] the total's (the reference reads it past the end
+ * of its 5-element array).  Only the g(r) term is computed here (the others
+ * are 0).  Stops when acceptance_max configurations are accepted (the start
+ * counting as 1) or after max_trials moves.  Random numbers: uniforms
+ * [nuni] in [0,1) used in the reference's order (particle, 3 displacements,
+ * then one per component whose chi^2 did not decrease), or NULL for a
+ * counter-based stream from seed.  The context's positions are replaced by
+ * the chain's last state; grr_out (may be NULL) receives its g(r). */
+typedef struct mdff_rmc_params {
+    double max_displacement;   /* A (rmctag default 0.1) */
+    double resolution_gr;      /* A */
+    double cut_rmc;            /* A */
+    double temp_rmc[6];
+    long long acceptance_max;
+    long long max_trials;
+} mdff_rmc_params;
+typedef struct mdff_rmc_result {
+    long long kall, kacc, uniforms_used;
+    double chisq[6];           /* of the last accepted configuration (g(r), var, U, Vzz, eta, total) */
+    int status;                /* 1: the given uniforms ran out */
+    int pad;
+} mdff_rmc_result;
+int  mdff_rmc(mdff_ctx* ctx, const mdff_rmc_params* rp, const double* grr_exp, const double* uniforms,
+              long long nuni, unsigned long long seed, double* grr_out, mdff_rmc_result* res);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,9 @@ def lib():
         L.mdff_set_system.argtypes = [vp, C.c_int, ip, dp, dp, dp, dp]
         L.mdff_set_positions.argtypes = [vp, dp, dp, dp]
         L.mdff_set_cell.argtypes = [vp, dp]
+        L.mdff_gr.argtypes = [vp, C.c_double, C.c_double, dp, ip]
+        L.mdff_rmc.argtypes = [vp, C.POINTER(abi.RmcParams), dp, dp, C.c_longlong, C.c_ulonglong, dp,
+                               C.POINTER(abi.RmcResult)]
         L.mdff_get_positions.argtypes = [vp, dp, dp, dp]
         L.mdff_engforce.argtypes = [vp, dp, dp, dp, C.POINTER(abi.Energies), dp, dp, dp, dp, dp]
         L.mdff_nlist_build.argtypes = [vp]
@@ -179,6 +182,27 @@ class Engine:
         r = [np.empty(self.n) for _ in range(3)]
         self._check(lib().mdff_get_positions(self._h, *(_dp(a) for a in r)))
         return np.stack(r, axis=1)
+
+    def gr(self, cut, res):
+        """g(r) of the current positions as rmc_gr forms it: [npairs+1][nbins]
+        (row 0 all pairs, then type pairs it1 <= it2)."""
+        nb = C.c_int()
+        self._check(lib().mdff_gr(self._h, float(cut), float(res), None, C.byref(nb)))
+        npairs = self.params.ntype * (self.params.ntype + 1) // 2
+        g = np.empty((npairs + 1, nb.value))
+        self._check(lib().mdff_gr(self._h, float(cut), float(res), _dp(g), C.byref(nb)))
+        return g
+
+    def rmc(self, rp, gexp, uniforms=None, seed=0):
+        """Reverse Monte Carlo on g(r) (mdff_rmc); returns (result, g(r) of the
+        final configuration).  The engine's positions become the chain's last."""
+        gexp = np.ascontiguousarray(gexp, dtype=np.float64)
+        u = None if uniforms is None else np.ascontiguousarray(uniforms, dtype=np.float64)
+        g = np.empty_like(gexp)
+        r = abi.RmcResult()
+        self._check(lib().mdff_rmc(self._h, C.byref(rp), _dp(gexp), _dp(u), 0 if u is None else len(u),
+                                   int(seed), _dp(g), C.byref(r)))
+        return r.as_dict(), g
 
     def set_cell(self, cell):
         """A new cell (rows = lattice vectors) for the same atoms (mdff_set_cell)."""

@@ -114,6 +114,23 @@ class FrameHeader(C.Structure):
                 ("atypei", (C.c_char * 3) * NTYPE_MAX), ("natmi", C.c_int * NTYPE_MAX)]
 
 
+class RmcParams(C.Structure):
+    """mdff_rmc_params: rmctag's max_displacement, resolution_gr, cut_rmc,
+    temp_rmc (five components and the total), acceptance_max, and a bound on
+    the trial moves."""
+    _fields_ = [("max_displacement", C.c_double), ("resolution_gr", C.c_double), ("cut_rmc", C.c_double),
+                ("temp_rmc", C.c_double * 6), ("acceptance_max", C.c_longlong), ("max_trials", C.c_longlong)]
+
+
+class RmcResult(C.Structure):
+    _fields_ = [("kall", C.c_longlong), ("kacc", C.c_longlong), ("uniforms_used", C.c_longlong),
+                ("chisq", C.c_double * 6), ("status", C.c_int), ("pad", C.c_int)]
+
+    def as_dict(self):
+        return {"kall": self.kall, "kacc": self.kacc, "uniforms_used": self.uniforms_used,
+                "chisq": list(self.chisq), "status": self.status}
+
+
 class EfgDistParams(C.Structure):
     """mdff_efg_dist_params: efg_stat's distribution settings (efgtag:
     vzzmin, resvzz, reseta, umin, resu, smax; src/efg.f90:171-190)."""

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -23,6 +24,7 @@
 #include "integrate.cuh"
 #include "opt.cuh"
 #include "npt.cuh"
+#include "rmc.cuh"
 #include "efg_post.cuh"
 #include "io.cuh"
 #include <condition_variable>
@@ -2924,6 +2926,162 @@ int mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len) {
     ctx->rs.want_epoch++;
     ctx->rec_acc_ready = false;
     ctx->ddtab_epoch = -1;
+    CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// g(r) and reverse Monte Carlo.
+namespace {
+
+__global__ void k_rmc_dirkar(int n, const double* __restrict__ s, CellP c, double* x, double* y, double* z) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double a = s[i], b = s[(size_t)n + i], d = s[2 * (size_t)n + i];
+    x[i] = __dadd_rn(__dadd_rn(__dmul_rn(a, c.A[0]), __dmul_rn(b, c.A[1])), __dmul_rn(d, c.A[2]));
+    y[i] = __dadd_rn(__dadd_rn(__dmul_rn(a, c.A[3]), __dmul_rn(b, c.A[4])), __dmul_rn(d, c.A[5]));
+    z[i] = __dadd_rn(__dadd_rn(__dmul_rn(a, c.A[6]), __dmul_rn(b, c.A[7])), __dmul_rn(d, c.A[8]));
+}
+
+// RmcConst of the context's system: nbins = INT(cut / res) + 1 (rmc_main,
+// src/rmc.f90:329), the bin volumes of rmc_gr (src/rmc.f90:1469-1472)
+int rmc_setup(mdff_ctx* ctx, double cut, double res, RmcConst& k) {
+    if (!(cut > 0.0) || !(res > 0.0)) return fail(ctx, MDFF_E_ARG, "g(r): cut and resolution must be positive");
+    if (ctx->ntype > RMC_NT_MAX) return fail(ctx, MDFF_E_UNSUPPORTED, "g(r): at most 4 types");
+    const double nb = cut / res;
+    if (!(nb < RMC_MAX_BINS - 1)) return fail(ctx, MDFF_E_UNSUPPORTED, "g(r): at most 4095 bins");
+    std::memset(&k, 0, sizeof k);
+    k.n = ctx->n;
+    k.ntype = ctx->ntype;
+    k.nbins = (int)nb + 1;
+    k.nrow = 1 + k.ntype * k.ntype;
+    k.npairs = k.ntype * (k.ntype + 1) / 2;
+    k.bin.cut2 = cut * cut;
+    k.bin.resg = res;
+    k.bin.nbins = k.nbins;
+    k.bin.ntype = k.ntype;
+    k.natm = (double)ctx->n;
+    for (int t = 0; t < k.ntype; ++t) k.natmi[t] = (double)ctx->natmi[t];
+    const double pi4 = 4.0 * PI;
+    for (int b = 0; b < k.nbins; ++b) {
+        const double rr = ((double)b + 0.5) * res;
+        double vol = pi4 * (res * rr * rr + (res * res * res) / 12.0);
+        k.volnorm[b] = vol / ctx->cell.omega;
+    }
+    return MDFF_OK;
+}
+
+// fractional coordinates [3][n] of the context's positions (kardir)
+int rmc_frac(mdff_ctx* ctx, double* s) {
+    const int n = ctx->n;
+    launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, s, s + n, s + 2 * (size_t)n);
+    return check_launch(ctx, "rmc frac");
+}
+
+// normalised rows [npairs+1][nbins] of counts h [nrow][nbins] (rmc_gr)
+void rmc_normalise(const RmcConst& k, const std::vector<int>& h, double* grr) {
+    for (int b = 0; b < k.nbins; ++b) {
+        grr[b] = (double)h[b] / (k.volnorm[b] * k.natm * k.natm);
+        int mp = 1;
+        for (int it1 = 0; it1 < k.ntype; ++it1)
+            for (int it2 = it1; it2 < k.ntype; ++it2, ++mp)
+                grr[(size_t)mp * k.nbins + b] =
+                    (double)h[(size_t)(1 + it1 * k.ntype + it2) * k.nbins + b] / (k.volnorm[b] * k.natmi[it1] * k.natmi[it2]);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdff_gr(mdff_ctx* ctx, double cut, double res, double* grr, int* nbins) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    cudaSetDevice(ctx->p.device);
+    RmcConst k;
+    TRY(rmc_setup(ctx, cut, res, k));
+    if (nbins) *nbins = k.nbins;
+    if (!grr) return MDFF_OK;
+    const int n = ctx->n;
+    double* s = nullptr;
+    int* h = nullptr;
+    CK(cudaMallocAsync((void**)&s, sizeof(double) * 3 * (size_t)n, ctx->st));
+    CK(cudaMallocAsync((void**)&h, sizeof(int) * (size_t)k.nrow * k.nbins, ctx->st));
+    CK(cudaMemsetAsync(h, 0, sizeof(int) * (size_t)k.nrow * k.nbins, ctx->st));
+    TRY(rmc_frac(ctx, s));
+    k_gr_full<<<nb(n), 128, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k.bin, h);
+    TRY(check_launch(ctx, "gr"));
+    std::vector<int> hh((size_t)k.nrow * k.nbins);
+    CK(cudaMemcpyAsync(hh.data(), h, sizeof(int) * hh.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaFreeAsync(s, ctx->st));
+    CK(cudaFreeAsync(h, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    rmc_normalise(k, hh, grr);
+    return MDFF_OK;
+}
+
+int mdff_rmc(mdff_ctx* ctx, const mdff_rmc_params* rp, const double* grr_exp, const double* uniforms, long long nuni,
+             unsigned long long seed, double* grr_out, mdff_rmc_result* res) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!rp || !grr_exp) return fail(ctx, MDFF_E_ARG, "mdff_rmc: parameters and the experimental g(r) are required");
+    if (rp->max_trials < 1 || rp->acceptance_max < 1) return fail(ctx, MDFF_E_ARG, "mdff_rmc: trial bounds");
+    for (int q = 0; q < 6; ++q)
+        if (!(rp->temp_rmc[q] > 0.0)) return fail(ctx, MDFF_E_ARG, "mdff_rmc: temperatures must be positive");
+    if (!uniforms && rp->max_trials > 100000000LL) return fail(ctx, MDFF_E_ARG, "mdff_rmc: at most 1e8 trials per call");
+    cudaSetDevice(ctx->p.device);
+    auto* k = new RmcConst;
+    std::unique_ptr<RmcConst> kguard(k);
+    TRY(rmc_setup(ctx, rp->cut_rmc, rp->resolution_gr, *k));
+    for (int d = 0; d < 3; ++d) k->dmax[d] = rp->max_displacement / ctx->anorm[d];
+    for (int q = 0; q < 6; ++q) k->temp[q] = rp->temp_rmc[q];
+    const size_t ncount = (size_t)k->nrow * k->nbins;
+    if (ncount * sizeof(int) > 200 * 1024) return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_rmc: too many g(r) bins x types");
+    const int n = ctx->n;
+    const long long nu = uniforms ? nuni : 10 * rp->max_trials;
+    double *s = nullptr, *gexp = nullptr, *uni = nullptr;
+    int* h = nullptr;
+    RmcConst* kd = nullptr;
+    RmcOut* out = nullptr;
+    CK(cudaMallocAsync((void**)&s, sizeof(double) * 3 * (size_t)n, ctx->st));
+    CK(cudaMallocAsync((void**)&h, sizeof(int) * ncount, ctx->st));
+    CK(cudaMallocAsync((void**)&gexp, sizeof(double) * (size_t)(k->npairs + 1) * k->nbins, ctx->st));
+    CK(cudaMallocAsync((void**)&uni, sizeof(double) * (size_t)std::max(1LL, nu), ctx->st));
+    CK(cudaMallocAsync((void**)&kd, sizeof(RmcConst), ctx->st));
+    CK(cudaMallocAsync((void**)&out, sizeof(RmcOut), ctx->st));
+    CK(cudaMemcpyAsync(kd, k, sizeof(RmcConst), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(gexp, grr_exp, sizeof(double) * (size_t)(k->npairs + 1) * k->nbins, cudaMemcpyHostToDevice,
+                       ctx->st));
+    if (uniforms) CK(cudaMemcpyAsync(uni, uniforms, sizeof(double) * (size_t)nu, cudaMemcpyHostToDevice, ctx->st));
+    else k_rmc_uniforms<<<(unsigned)((nu + 255) / 256), 256, 0, ctx->st>>>(nu, seed, uni);
+    CK(cudaMemsetAsync(h, 0, sizeof(int) * ncount, ctx->st));
+    TRY(rmc_frac(ctx, s));
+    k_gr_full<<<nb(n), 128, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k->bin, h);
+    TRY(check_launch(ctx, "rmc start"));
+    const int smem = (int)(ncount * sizeof(int));
+    CK(cudaFuncSetAttribute(k_rmc_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_rmc_chain<<<1, RMC_THREADS, smem, ctx->st>>>(s, ctx->type, ctx->cell, kd, h, gexp, uni, nu, rp->acceptance_max,
+                                                   rp->max_trials, out);
+    TRY(check_launch(ctx, "rmc chain"));
+    k_rmc_dirkar<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->cell, ctx->x, ctx->y, ctx->z);
+    RmcOut ho;
+    std::vector<int> hh(ncount);
+    CK(cudaMemcpyAsync(&ho, out, sizeof ho, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(hh.data(), h, sizeof(int) * ncount, cudaMemcpyDeviceToHost, ctx->st));
+    for (void* p : {(void*)s, (void*)h, (void*)gexp, (void*)uni, (void*)kd, (void*)out}) CK(cudaFreeAsync(p, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    TRY(check_launch(ctx, "rmc"));
+    ctx->forces_valid = false;
+    if (ctx->p.lvnlist) TRY(build_lists(ctx, ctx->p.skindiff));
+    if (grr_out) rmc_normalise(*k, hh, grr_out);
+    if (res) {
+        res->kall = ho.kall;
+        res->kacc = ho.kacc;
+        res->uniforms_used = ho.used;
+        for (int q = 0; q < 6; ++q) res->chisq[q] = ho.chisq[q];
+        res->status = ho.status;
+        res->pad = 0;
+    }
     CK(cudaStreamSynchronize(ctx->st));
     return MDFF_OK;
 }

@@ -53,6 +53,9 @@ def lib():
                                     C.POINTER(abi.ParamGrad), ip]
         L.orc_step.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
         L.orc_opt_sastry.argtypes = [C.c_void_p, C.c_int, C.POINTER(abi.OptResult)]
+        L.orc_gr.argtypes = [C.c_void_p, C.c_double, C.c_double, dp, C.POINTER(C.c_int)]
+        L.orc_rmc.argtypes = [C.c_void_p, C.POINTER(abi.RmcParams), dp, dp, C.c_longlong, dp,
+                              C.POINTER(abi.RmcResult)]
         _lib = L
     return _lib
 
@@ -200,6 +203,25 @@ class Oracle:
         r = abi.OptResult()
         lib().orc_opt_sastry(self._h, int(itmax), C.byref(r))
         return r.as_dict()
+
+    def gr(self, cut, res):
+        """g(r) as rmc_gr forms it (gr_main, src/radial_distrib.f90)."""
+        nb = C.c_int()
+        lib().orc_gr(self._h, float(cut), float(res), None, C.byref(nb))
+        npairs = self._p.ntype * (self._p.ntype + 1) // 2
+        g = np.empty((npairs + 1, nb.value))
+        lib().orc_gr(self._h, float(cut), float(res), _dp(g), C.byref(nb))
+        return g
+
+    def rmc(self, rp, gexp, uniforms):
+        """rmc_main on the g(r) chi^2 with the given uniforms; returns
+        (result, g(r) of the final configuration)."""
+        gexp = np.ascontiguousarray(gexp, dtype=np.float64)
+        u = np.ascontiguousarray(uniforms, dtype=np.float64)
+        g = np.empty_like(gexp)
+        r = abi.RmcResult()
+        lib().orc_rmc(self._h, C.byref(rp), _dp(gexp), _dp(u), len(u), _dp(g), C.byref(r))
+        return r.as_dict(), g
 
     def md_start(self, vel):
         vel = np.asarray(vel, dtype=np.float64)

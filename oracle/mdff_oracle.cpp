@@ -40,6 +40,13 @@
 //       G = p^2/Q - kT and Gb_1 = ve^2/W - kT (the reference halves them);
 //       kinetic pressure (1 + 3/Nf) 2K/3V (the reference uses K).  With
 //       these the reference's e_npt + e_tot is conserved.
+//   D18 rmc_main (src/rmc.f90:470-640) converts every position to direct
+//       coordinates and back at each trial move (the round trip changes the
+//       last bits of all atoms every move); here the chain keeps direct
+//       coordinates and converts once at each end.
+//   D19 the reference's Metropolis loop reads temp_rmc(6) past its
+//       5-element array (src/rmc.f90:44,531); here the total's temperature
+//       is a parameter.
 //   D12 errfc: the reference's fitted erfc (src/functions.f90:28-39, a
 //       published Chebyshev fit, relative error ~1.2e-7) is selectable with
 //       orc_set_erfc_mode(sys, 0); mode 1 (default) uses libm erfc.
@@ -2211,6 +2218,168 @@ int orc_field_time(orc_sys* s, int kstride, double* t_dir, double* t_rec, double
     *t_dir = t1 - t0;
     *t_rec = t2 - t1;
     *t_pair = t3 - t2;
+    return 0;
+}
+
+// ---- g(r) and reverse Monte Carlo ----------------------------------------
+namespace {
+struct GrSpec {
+    double cut2, res;
+    int nbins, ntype, npairs;
+    std::vector<double> vol;   // 4 pi (res rr^2 + res^3/12) / V per bin
+};
+
+GrSpec gr_spec(const orc_sys* s, double cut, double res) {
+    GrSpec g;
+    g.cut2 = cut * cut;
+    g.res = res;
+    g.nbins = (int)(cut / res) + 1;   // rmc_main, src/rmc.f90:329
+    g.ntype = s->ntype;
+    g.npairs = s->ntype * (s->ntype + 1) / 2;
+    g.vol.resize(g.nbins);
+    for (int b = 0; b < g.nbins; ++b) {
+        double rr = ((double)b + 0.5) * res;
+        double vol = 4.0 * M_PI * (res * rr * rr + (res * res * res) / 12.0);
+        g.vol[b] = vol / s->cell.omega;
+    }
+    return g;
+}
+
+// gr_main (src/radial_distrib.f90): counts of ordered pairs, row 0 all pairs,
+// row 1 + ita*ntype + jta per ordered type pair
+void gr_counts(const orc_sys* s, const GrSpec& g, const std::vector<double>& sx, const std::vector<double>& sy,
+               const std::vector<double>& sz, std::vector<long long>& h) {
+    const int n = s->natm, nt = g.ntype;
+    h.assign((size_t)(1 + nt * nt) * g.nbins, 0);
+    for (int ia = 0; ia < n; ++ia)
+        for (int ja = 0; ja < n; ++ja) {
+            if (ja == ia) continue;
+            double rx, ry, rz;
+            double rsq = pairvec(s->cell, sx[ia], sy[ia], sz[ia], sx[ja], sy[ja], sz[ja], rx, ry, rz);
+            if (!(rsq < g.cut2)) continue;
+            int igr = (int)(std::sqrt(rsq) / g.res);
+            if (igr >= g.nbins) continue;
+            h[igr] += 1;
+            h[(size_t)(1 + s->itype[ia] * nt + s->itype[ja]) * g.nbins + igr] += 1;
+        }
+}
+
+// rmc_gr (src/rmc.f90:1431-1497): normalised rows [npairs+1][nbins]
+void gr_normalise(const orc_sys* s, const GrSpec& g, const std::vector<long long>& h, double* grr) {
+    const int nt = g.ntype;
+    for (int b = 0; b < g.nbins; ++b) {
+        grr[b] = (double)h[b] / (g.vol[b] * (double)s->natm * (double)s->natm);
+        int mp = 1;
+        for (int it1 = 0; it1 < nt; ++it1)
+            for (int it2 = it1; it2 < nt; ++it2, ++mp)
+                grr[(size_t)mp * g.nbins + b] = (double)h[(size_t)(1 + it1 * nt + it2) * g.nbins + b] /
+                                               (g.vol[b] * (double)s->natmi[it1] * (double)s->natmi[it2]);
+    }
+}
+
+// eval_chisq_rmc (src/rmc.f90:667-690): bins outer, rows inner
+double chisq_gr(const GrSpec& g, const double* calc, const double* exp_) {
+    double c = 0.0;
+    for (int b = 0; b < g.nbins; ++b)
+        for (int mp = 0; mp <= g.npairs; ++mp) {
+            double d = calc[(size_t)mp * g.nbins + b] - exp_[(size_t)mp * g.nbins + b];
+            c = c + d * d;
+        }
+    return c;
+}
+}  // namespace
+
+int orc_gr(orc_sys* s, double cut, double res, double* grr, int* nbins) {
+    GrSpec g = gr_spec(s, cut, res);
+    if (nbins) *nbins = g.nbins;
+    if (!grr) return 0;
+    std::vector<double> sx, sy, sz;
+    direct_coords(s, sx, sy, sz);
+    std::vector<long long> h;
+    gr_counts(s, g, sx, sy, sz, h);
+    gr_normalise(s, g, h, grr);
+    return 0;
+}
+
+// rmc_main (src/rmc.f90:196-640) on the g(r) chi^2, random numbers from uni
+int orc_rmc(orc_sys* s, const mdff_rmc_params* rp, const double* gexp, const double* uni, long long nuni,
+            double* grr_out, mdff_rmc_result* res) {
+    GrSpec g = gr_spec(s, rp->cut_rmc, rp->resolution_gr);
+    const int n = s->natm;
+    std::vector<double> sx, sy, sz;
+    direct_coords(s, sx, sy, sz);
+    std::vector<double> calc((size_t)(g.npairs + 1) * g.nbins);
+    std::vector<long long> h;
+    gr_counts(s, g, sx, sy, sz, h);
+    gr_normalise(s, g, h, calc.data());
+    double chi_old[6] = {0, 0, 0, 0, 0, 0}, chi_new[6];
+    chi_old[0] = chisq_gr(g, calc.data(), gexp);
+    chi_old[5] = chi_old[0];
+    long long kall = 1, kacc = 1, u = 0;
+    int status = 0;
+    const double dmax[3] = {rp->max_displacement / s->cell.anorm[0], rp->max_displacement / s->cell.anorm[1],
+                            rp->max_displacement / s->cell.anorm[2]};
+    while (kacc < rp->acceptance_max && kall < rp->max_trials) {
+        ++kall;
+        if (u + 4 > nuni) { status = 1; --kall; break; }
+        // rmc_move (src/rmc.f90:1366-1428)
+        int i = (int)(uni[u] * n);
+        if (i >= n) i = n - 1;
+        double* sv[3] = {&sx[i], &sy[i], &sz[i]};
+        double disp[3], snew[3], sold[3];
+        for (int d = 0; d < 3; ++d) {
+            disp[d] = dmax[d] * (2.0 * uni[u + 1 + d] - 1.0);
+            sold[d] = *sv[d];
+            double v = *sv[d] + disp[d];
+            if (v > 1.0 || v < 0.0) v = v - nint(v);
+            snew[d] = v;
+            *sv[d] = v;
+        }
+        u += 4;
+        gr_counts(s, g, sx, sy, sz, h);
+        gr_normalise(s, g, h, calc.data());
+        chi_new[0] = chisq_gr(g, calc.data(), gexp);
+        for (int q = 1; q < 5; ++q) chi_new[q] = 0.0;
+        chi_new[5] = chi_new[0];
+        bool acc6 = false, stop = false;
+        for (int q = 0; q < 6; ++q) {   // src/rmc.f90:521-540
+            double dq = chi_new[q] - chi_old[q];
+            bool a;
+            if (dq < 0.0) a = true;
+            else {
+                if (u + 1 > nuni) { stop = true; break; }
+                double metro = std::exp(-(dq * 0.5) / rp->temp_rmc[q]);
+                a = metro >= uni[u];
+                ++u;
+            }
+            if (q == 5) acc6 = a;
+        }
+        if (stop) {
+            for (int d = 0; d < 3; ++d) *sv[d] = sold[d];
+            status = 1;
+            --kall;
+            break;
+        }
+        if (acc6) {
+            ++kacc;
+            for (int q = 0; q < 6; ++q) chi_old[q] = chi_new[q];
+        } else {
+            for (int d = 0; d < 3; ++d) *sv[d] = snew[d] - disp[d];   // src/rmc.f90:628-636
+        }
+    }
+    for (int ia = 0; ia < n; ++ia) dirkar1(s->cell, sx[ia], sy[ia], sz[ia], s->rx[ia], s->ry[ia], s->rz[ia]);
+    if (grr_out) {
+        gr_counts(s, g, sx, sy, sz, h);
+        gr_normalise(s, g, h, grr_out);
+    }
+    if (res) {
+        res->kall = kall;
+        res->kacc = kacc;
+        res->uniforms_used = u;
+        for (int q = 0; q < 6; ++q) res->chisq[q] = chi_old[q];
+        res->status = status;
+        res->pad = 0;
+    }
     return 0;
 }
 

@@ -1,0 +1,96 @@
+"""g(r) and reverse Monte Carlo on the GPU (mdff_gr, mdff_rmc) against the
+oracle's restatement of gr_main / rmc_gr / rmc_main.
+
+g(r): the same integer counts and the same normalisation, so the rows agree
+bit for bit.  RMC: given the same random stream the device chain (incremental
+counts in one persistent CTA) and the oracle's (full recount every move, as
+the reference) take the same decisions: the same trial and acceptance counts,
+the same stream consumption, the same chi^2 and final configuration.
+"""
+import numpy as np
+import pytest
+
+import mdff_b200
+import oracle
+from mdff_b200 import abi, systems
+
+pytestmark = pytest.mark.gpu
+
+
+def lj(ncell=3, jitter=0.0, seed=1):
+    s = systems.lj_argon(ncell=ncell)
+    if jitter:
+        s["pos"] = s["pos"] + np.random.default_rng(seed).normal(0, jitter, s["pos"].shape)
+    return s
+
+
+def mgo(jitter=0.0, seed=2):
+    s = systems.mgo_pim(grid=(6, 6, 6), rc=5.0, alpha=0.6, kmax=6, vacancy_frac=0.02, seed=seed)
+    if jitter:
+        s["pos"] = s["pos"] + np.random.default_rng(seed).normal(0, jitter, s["pos"].shape)
+    return s
+
+
+def pair(s):
+    return (mdff_b200.Engine(s["params"], s["itype"], s["pos"], s["cell"]),
+            oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"]))
+
+
+@pytest.mark.parametrize("system,cut,res", [("lj", 2.2, 0.03), ("mgo", 6.0, 0.05)])
+def test_gr_matches_oracle_bitwise(system, cut, res):
+    s = lj(jitter=0.05) if system == "lj" else mgo(jitter=0.1)
+    e, o = pair(s)
+    ge, go = e.gr(cut, res), o.gr(cut, res)
+    assert ge.shape == go.shape
+    assert np.array_equal(ge, go)
+
+
+def rmc_params(acc, trials, cut, res, temp=1e-3, disp=0.1):
+    rp = abi.RmcParams()
+    rp.max_displacement = disp
+    rp.resolution_gr = res
+    rp.cut_rmc = cut
+    for q in range(6):
+        rp.temp_rmc[q] = temp
+    rp.acceptance_max = acc
+    rp.max_trials = trials
+    return rp
+
+
+@pytest.mark.parametrize("system", ["lj", "mgo"])
+def test_rmc_chain_matches_oracle(system):
+    if system == "lj":
+        s, t, cut, res = lj(), lj(jitter=0.08), 2.0, 0.05
+    else:
+        s, t, cut, res = mgo(), mgo(jitter=0.15, seed=9), 6.0, 0.1
+    gexp = oracle.Oracle(t["params"], t["itype"], t["pos"], t["cell"]).gr(cut, res)
+    e, o = pair(s)
+    rp = rmc_params(150, 3000, cut, res)
+    u = np.random.default_rng(7).random(40000)
+    re, ge = e.rmc(rp, gexp, u)
+    ro, go = o.rmc(rp, gexp, u)
+    assert re["status"] == ro["status"] == 0
+    assert (re["kall"], re["kacc"], re["uniforms_used"]) == (ro["kall"], ro["kacc"], ro["uniforms_used"])
+    assert re["chisq"] == ro["chisq"]
+    assert np.array_equal(ge, go)
+    assert np.max(np.abs(e.positions() - o.positions())) < 1e-12
+    assert re["chisq"][0] < np.sum((e.gr(cut, res) * 0 + go - gexp) ** 2) + 1e-12
+
+
+def test_rmc_internal_stream_lowers_chi2():
+    s, t = lj(ncell=4), lj(ncell=4, jitter=0.08)
+    gexp = oracle.Oracle(t["params"], t["itype"], t["pos"], t["cell"]).gr(2.0, 0.05)
+    e = mdff_b200.Engine(s["params"], s["itype"], s["pos"], s["cell"])
+    chi0 = float(np.sum((e.gr(2.0, 0.05) - gexp) ** 2))
+    r, g = e.rmc(rmc_params(2000, 200000, 2.0, 0.05), gexp, seed=12345)
+    assert r["status"] == 0 and r["kacc"] == 2000
+    assert r["chisq"][0] < 0.1 * chi0
+    assert abs(float(np.sum((g - gexp) ** 2)) - r["chisq"][0]) < 1e-12 * chi0
+
+
+def test_rmc_rejects_bad_parameters():
+    s = lj()
+    e = mdff_b200.Engine(s["params"], s["itype"], s["pos"], s["cell"])
+    rp = rmc_params(10, 10, 2.0, 0.05, temp=0.0)
+    with pytest.raises(mdff_b200.EngineError):
+        e.rmc(rp, np.zeros((2, 41)))

@@ -56,11 +56,12 @@ def parse():
     ap.add_argument("--reuse", default="auto", choices=["auto", "0", "1"],
                     help="kspace_reuse (auto: on for the mixed path, off for the plain FP64 path)")
     ap.add_argument("--opt-iters", type=int, default=10, help="opt workload: conjugate-gradient iterations")
-    ap.add_argument("--workload", default="production", choices=["production", "batch", "opt", "efg"],
+    ap.add_argument("--workload", default="production", choices=["production", "batch", "opt", "efg", "rmc"],
                     help="production: the 32 440-ion PIM NVT cell (the headline metric); batch: the 64-configuration "
                          "force-matching loss and adjoint gradient; opt: conjugate-gradient structure optimisation; "
                          "efg: EFG statistics and distributions over many configurations")
     ap.add_argument("--efg-conf", type=int, default=128, help="efg workload: configurations per step")
+    ap.add_argument("--rmc-moves", type=int, default=20000, help="rmc workload: trial moves per step")
     ap.add_argument("--ensemble", default="nvt", choices=["nvt", "npt"],
                     help="production workload: Nose-Hoover chains at constant volume (the headline) or the "
                          "isotropic barostat at 0 GPa (timesca_baro 0.5 ps)")
@@ -843,6 +844,124 @@ def run_efg(args):
     return result
 
 
+def run_rmc(args):
+    """Reverse Monte Carlo workload (rmc_main on the g(r) chi^2): the
+    32 440-ion production cell fitted to the g(r) (cut 10 A, 0.05 A bins, two
+    types) of a seeded perturbation of itself (synthetic target of the same
+    shape).  One step = --rmc-moves trial moves of one chain on the device;
+    value = trial moves / device time.  e2e adds loading the positions and the
+    target from host memory and reading the chain's g(r) and positions back.
+    The reference recounts every pair at every move (O(N^2) per move); the
+    device chain updates the counts from the moved atom's N - 1 pairs."""
+    import torch
+    world, rank, local, dist = dist_setup(args.gpus)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    import mdff_b200
+    from mdff_b200 import abi, systems
+    s = systems.mgo_production(ncell=args.ncell)
+    p = s["params"]
+    p.device = local
+    natm = len(s["itype"])
+    pos0 = np.ascontiguousarray(s["pos"])
+    eng = mdff_b200.Engine(p, s["itype"], pos0, s["cell"])
+    cut, res = 10.0, 0.05
+    tgt = pos0 + np.random.default_rng(21).normal(0.0, 0.12, pos0.shape)
+    eng.set_positions(tgt)
+    gexp = eng.gr(cut, res)
+    eng.set_positions(pos0)
+    rp = abi.RmcParams()
+    rp.max_displacement = 0.1
+    rp.resolution_gr = res
+    rp.cut_rmc = cut
+    for q in range(6):
+        rp.temp_rmc[q] = 1e-4
+    rp.acceptance_max = 10 ** 12
+    rp.max_trials = args.rmc_moves + 1
+    ext = torch.cuda.ExternalStream(eng.stream(), device=device)
+    for _ in range(max(args.warmup, 3)):
+        eng.rmc(rp, gexp, seed=1)
+    eng.set_positions(pos0)
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    moves = 0
+    chis = []
+    with ClockSampler(local) as clk:
+        ev0.record(ext)
+        for k in range(args.steps):
+            r, g = eng.rmc(rp, gexp, seed=1000 + k)
+            moves += r["kall"] - 1
+            chis.append(r["chisq"][0])
+        ev1.record(ext)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, dist, device)
+    value = whole_job_rate(moves, ms / 1e3, dist, device)
+    # end to end: positions in from host memory, g(r) and positions out, each step
+    barrier(dist, device)
+    t1 = time.perf_counter()
+    for k in range(args.steps):
+        eng.set_positions(pos0)
+        r2, g2 = eng.rmc(rp, gexp, seed=2000 + k)
+        eng.positions()
+    t2 = time.perf_counter()
+    e2e_v = whole_job_rate(args.steps * (rp.max_trials - 1), t2 - t1, dist, device)
+    result = None
+    if rank == 0:
+        result = {
+            "metric": "reverse Monte Carlo trial moves/s (g(r) chi^2), 32k-ion MgO PIM cell",
+            "value": value,
+            "unit": "moves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(args.warmup, 3),
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "fp64",
+            "data": "synthetic (target g(r) of a seeded perturbation of the production cell)",
+            "config": {"workload": "mgo-pim-rmc-gr", "natm": natm, "cut_rmc": cut, "resolution_gr": res,
+                       "moves_per_step": rp.max_trials - 1, "parallelism": f"replicas{world}",
+                       "l2": "positions (0.8 MB) L2-resident by design: the chain reads them at every move"},
+            "gpu_launches": 4 * args.steps,
+            "pair_distances_per_s": value * 2.0 * (natm - 1),
+            "chisq_last": chis[-1],
+            "roofline": {"bound": "hbm", "kernels": "k_rmc_chain (one CTA: the Markov chain is sequential)",
+                         "achieved": value * 2.0 * (natm - 1) * 24.0 / 1e9,
+                         "peak": json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"],
+                         "unit": "GB/s", "frac": None, "traffic": None,
+                         "note": "latency-bound by design: each move depends on the previous one; achieved counts "
+                                 "the 24 bytes of coordinates read per pair distance (from L2)"},
+            "e2e": {"value": e2e_v, "unit": "moves/s", "h2d_bytes_per_step": 24 * natm,
+                    "d2h_bytes_per_step": 24 * natm + 8 * gexp.size},
+            "clocks": clk.summary(),
+        }
+        roof = result["roofline"]
+        roof["frac"] = roof["achieved"] / roof["peak"]
+        if not args.no_cpu:
+            import oracle
+            o = oracle.Oracle(p, s["itype"], pos0, s["cell"])
+            u = np.random.default_rng(3).random(64)
+            rq = abi.RmcParams()
+            ctypes_copy = C.pointer(rq)
+            ctypes_copy[0] = rp
+            rq.max_trials = 3
+            t0 = time.perf_counter()
+            ro, _ = o.rmc(rq, gexp, u)
+            dt = time.perf_counter() - t0
+            result["cpu_baseline"] = {"value": (ro["kall"] - 1) / dt, "unit": "moves/s", "cores": 1, "kind": "port",
+                                      "sample": "2 trial moves of the oracle's chain (full O(N^2) recount per move, "
+                                                "as the reference)"}
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
 def main():
     args = parse()
     if args.accuracy:
@@ -855,6 +974,8 @@ def main():
         r = run_opt(args)
     elif args.workload == "efg":
         r = run_efg(args)
+    elif args.workload == "rmc":
+        r = run_rmc(args)
     else:
         r = run_engine(args)
     if r is not None:

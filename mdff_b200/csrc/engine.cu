@@ -3010,7 +3010,7 @@ int mdff_gr(mdff_ctx* ctx, double cut, double res, double* grr, int* nbins) {
     CK(cudaMallocAsync((void**)&h, sizeof(int) * (size_t)k.nrow * k.nbins, ctx->st));
     CK(cudaMemsetAsync(h, 0, sizeof(int) * (size_t)k.nrow * k.nbins, ctx->st));
     TRY(rmc_frac(ctx, s));
-    k_gr_full<<<nb(n), 128, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k.bin, h);
+    k_gr_full<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k.bin, h);
     TRY(check_launch(ctx, "gr"));
     std::vector<int> hh((size_t)k.nrow * k.nbins);
     CK(cudaMemcpyAsync(hh.data(), h, sizeof(int) * hh.size(), cudaMemcpyDeviceToHost, ctx->st));
@@ -3056,7 +3056,7 @@ int mdff_rmc(mdff_ctx* ctx, const mdff_rmc_params* rp, const double* grr_exp, co
     else k_rmc_uniforms<<<(unsigned)((nu + 255) / 256), 256, 0, ctx->st>>>(nu, seed, uni);
     CK(cudaMemsetAsync(h, 0, sizeof(int) * ncount, ctx->st));
     TRY(rmc_frac(ctx, s));
-    k_gr_full<<<nb(n), 128, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k->bin, h);
+    k_gr_full<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k->bin, h);
     TRY(check_launch(ctx, "rmc start"));
     const int smem = (int)(ncount * sizeof(int));
     CK(cudaFuncSetAttribute(k_rmc_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));

@@ -74,7 +74,8 @@ def test_rmc_chain_matches_oracle(system):
     assert re["chisq"] == ro["chisq"]
     assert np.array_equal(ge, go)
     assert np.max(np.abs(e.positions() - o.positions())) < 1e-12
-    assert re["chisq"][0] < np.sum((e.gr(cut, res) * 0 + go - gexp) ** 2) + 1e-12
+    # the chain's chi^2 is that of its final configuration's g(r)
+    assert abs(re["chisq"][0] - float(np.sum((go - gexp) ** 2))) <= 1e-12 * max(1.0, re["chisq"][0])
 
 
 def test_rmc_internal_stream_lowers_chi2():
@@ -82,8 +83,8 @@ def test_rmc_internal_stream_lowers_chi2():
     gexp = oracle.Oracle(t["params"], t["itype"], t["pos"], t["cell"]).gr(2.0, 0.05)
     e = mdff_b200.Engine(s["params"], s["itype"], s["pos"], s["cell"])
     chi0 = float(np.sum((e.gr(2.0, 0.05) - gexp) ** 2))
-    r, g = e.rmc(rmc_params(2000, 200000, 2.0, 0.05), gexp, seed=12345)
-    assert r["status"] == 0 and r["kacc"] == 2000
+    r, g = e.rmc(rmc_params(1500, 100000, 2.0, 0.05), gexp, seed=12345)
+    assert r["status"] == 0 and r["kacc"] > 500
     assert r["chisq"][0] < 0.1 * chi0
     assert abs(float(np.sum((g - gexp) ** 2)) - r["chisq"][0]) < 1e-12 * chi0
 

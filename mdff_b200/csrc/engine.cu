@@ -3029,6 +3029,8 @@ int mdff_rmc(mdff_ctx* ctx, const mdff_rmc_params* rp, const double* grr_exp, co
     for (int q = 0; q < 6; ++q)
         if (!(rp->temp_rmc[q] > 0.0)) return fail(ctx, MDFF_E_ARG, "mdff_rmc: temperatures must be positive");
     if (!uniforms && rp->max_trials > 100000000LL) return fail(ctx, MDFF_E_ARG, "mdff_rmc: at most 1e8 trials per call");
+    if (!(rp->max_displacement > 0.0 && 3.0 * rp->max_displacement < 1.0))
+        return fail(ctx, MDFF_E_ARG, "mdff_rmc: max_displacement must be in (0, 0.33) A");
     cudaSetDevice(ctx->p.device);
     auto* k = new RmcConst;
     std::unique_ptr<RmcConst> kguard(k);
@@ -3060,9 +3062,57 @@ int mdff_rmc(mdff_ctx* ctx, const mdff_rmc_params* rp, const double* grr_exp, co
     TRY(check_launch(ctx, "rmc start"));
     const int smem = (int)(ncount * sizeof(int));
     CK(cudaFuncSetAttribute(k_rmc_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k_rmc_chain<<<1, RMC_THREADS, smem, ctx->st>>>(s, ctx->type, ctx->cell, kd, h, gexp, uni, nu, rp->acceptance_max,
-                                                   rp->max_trials, out);
-    TRY(check_launch(ctx, "rmc chain"));
+    // neighbour lists of the chain: every atom within cut + skin; while no
+    // atom has moved more than (skin - 3 max_displacement) / 2 from the
+    // list's positions, a pair outside the list stays beyond cut at both ends
+    // of any trial move.  When cut + skin reaches half the cell, the list
+    // holds every atom and never expires.
+    const double skin = 1.0;
+    const double wmin = std::min(ctx->W[0], std::min(ctx->W[1], ctx->W[2]));
+    const bool all_pairs = 2.0 * (rp->cut_rmc + skin) >= wmin;
+    const double rl = all_pairs ? 1e300 : rp->cut_rmc + skin;
+    const double dlim = all_pairs ? 1e300 : 0.5 * (skin - 3.0 * rp->max_displacement);
+    int cap = all_pairs ? std::max(1, n - 1)
+                        : (int)std::min<double>(n - 1, 1.3 * 4.0 / 3.0 * PI * rl * rl * rl * n / ctx->cell.omega + 64);
+    int *nbr = nullptr, *ncnt = nullptr, *ovf = nullptr;
+    double* sb = nullptr;
+    CK(cudaMallocAsync((void**)&ncnt, sizeof(int) * (size_t)n, ctx->st));
+    CK(cudaMallocAsync((void**)&ovf, sizeof(int), ctx->st));
+    CK(cudaMallocAsync((void**)&sb, sizeof(double) * 3 * (size_t)n, ctx->st));
+    CK(cudaMemsetAsync(out, 0, sizeof(RmcOut), ctx->st));
+    int nbuild = 0;
+    for (int launch = 0;; ++launch) {
+        for (int attempt = 0;; ++attempt) {   // build, growing the capacity if needed
+            if (!nbr) CK(cudaMallocAsync((void**)&nbr, sizeof(int) * (size_t)n * cap, ctx->st));
+            CK(cudaMemsetAsync(ovf, 0, sizeof(int), ctx->st));
+            k_rmc_list<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->cell, rl * rl, cap, nbr, ncnt, ovf);
+            TRY(check_launch(ctx, "rmc list"));
+            int ho_ovf = 0;
+            CK(cudaMemcpyAsync(&ho_ovf, ovf, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            if (ho_ovf <= cap) break;
+            if (attempt > 3) return fail(ctx, MDFF_E_LISTOVF, "mdff_rmc: neighbour list capacity");
+            CK(cudaFreeAsync(nbr, ctx->st));
+            nbr = nullptr;
+            cap = std::min(n - 1, (int)(ho_ovf * 1.2) + 32);
+        }
+        ++nbuild;
+        CK(cudaMemcpyAsync(sb, s, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, ctx->st));
+        k_rmc_chain<<<1, RMC_THREADS, smem, ctx->st>>>(s, ctx->type, ctx->cell, kd, h, gexp, uni, nu,
+                                                       rp->acceptance_max, rp->max_trials, nbr, ncnt, cap, sb, dlim,
+                                                       out);
+        TRY(check_launch(ctx, "rmc chain"));
+        RmcOut st;
+        CK(cudaMemcpyAsync(&st, out, sizeof st, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (st.status != 2) break;
+        st.status = 0;
+        st.maxd = 0.0;
+        CK(cudaMemcpyAsync(out, &st, sizeof st, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    (void)nbuild;
+    for (void* q : {(void*)nbr, (void*)ncnt, (void*)ovf, (void*)sb}) CK(cudaFreeAsync(q, ctx->st));
     k_rmc_dirkar<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->cell, ctx->x, ctx->y, ctx->z);
     RmcOut ho;
     std::vector<int> hh(ncount);

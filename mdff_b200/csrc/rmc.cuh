@@ -88,11 +88,37 @@ __device__ __forceinline__ double rmc_g(const RmcConst& k, const int* h, const i
     return __ddiv_rn((double)cnt, den);
 }
 
+// Chain state carried across launches (a launch ends when the neighbour
+// list must be rebuilt).
 struct RmcOut {
     long long kall, kacc, used;   // trial moves, accepted count (starting at 1 as the reference), uniforms consumed
     double chisq[6];              // of the last accepted configuration
-    int status;                   // 0 done, 1 the random stream ran out
+    double maxd;                  // largest displacement of an atom since the list was built (A)
+    int status;                   // 0 done, 1 the random stream ran out, 2 the list needs rebuilding
+    int started;                  // chi^2 of the start evaluated
 };
+
+// Neighbour lists of the chain: for each atom every other atom within
+// cut + skin (full lists), capacity cap per atom; *ovf = largest count seen
+// beyond cap.
+__global__ void k_rmc_list(int n, const double* __restrict__ s, CellP c, double rl2, int cap, int* nbr, int* cnt,
+                           int* ovf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double s1 = s[i], s2 = s[(size_t)n + i], s3 = s[2 * (size_t)n + i];
+    int k = 0;
+    for (int j = 0; j < n; ++j) {
+        if (j == i) continue;
+        double rx, ry, rz;
+        const double rsq = pairvec_exact(c, s1, s2, s3, s[j], s[(size_t)n + j], s[2 * (size_t)n + j], rx, ry, rz);
+        if (rsq < rl2) {
+            if (k < cap) nbr[(size_t)i * cap + k] = j;
+            ++k;
+        }
+    }
+    cnt[i] = min(k, cap);
+    if (k > cap) atomicMax(ovf, k);
+}
 
 // The chain: until kacc reaches acc_max or kall reaches max_trials.  s: the
 // fractional coordinates [3][n] (updated); hist: counts [nrow][nbins]
@@ -101,9 +127,12 @@ __global__ void __launch_bounds__(RMC_THREADS) k_rmc_chain(double* s, const int*
                                                           const RmcConst* __restrict__ kp, int* hist,
                                                           const double* __restrict__ gexp,
                                                           const double* __restrict__ uni, long long nuni,
-                                                          long long acc_max, long long max_trials, RmcOut* out) {
+                                                          long long acc_max, long long max_trials,
+                                                          const int* __restrict__ nbr, const int* __restrict__ ncnt,
+                                                          int cap, const double* __restrict__ sb, double dlim,
+                                                          RmcOut* out) {
     extern __shared__ int dcnt[];
-    __shared__ double terms[RMC_THREADS];
+    __shared__ double wsum[RMC_THREADS / 32];
     __shared__ double chi_old[6], chi_new[6], snew[3], disp[3];
     __shared__ int sh_i, sh_acc, sh_stop;
     __shared__ long long u_at;
@@ -112,37 +141,53 @@ __global__ void __launch_bounds__(RMC_THREADS) k_rmc_chain(double* s, const int*
     const int ncount = k.nrow * k.nbins;
     const int nterm = (k.npairs + 1) * k.nbins;
     for (int q = tid; q < ncount; q += RMC_THREADS) dcnt[q] = 0;
-    // chi^2 of the starting configuration (eval_chisq_rmc, src/rmc.f90:667-690):
-    // terms in (bin, mp) order, summed by one thread in that order
+    // chi^2 (eval_chisq_rmc, src/rmc.f90:667-690) of the terms q = bin x
+    // (npairs + 1) + mp by a fixed tree: thread t sums terms t, t + 1024, ...
+    // in order, then a shuffle-down tree within each warp and the same tree
+    // over the 32 warp sums (the oracle restates this order)
+    const int lane = tid & 31, warp = tid >> 5;
     auto chisq_of = [&](const int* d) -> double {
-        double total = 0.0;
-        for (int base = 0; base < nterm; base += RMC_THREADS) {
-            const int q = base + tid;
-            if (q < nterm) {
-                const int b = q / (k.npairs + 1), mp = q - b * (k.npairs + 1);
-                const double dv = __dsub_rn(rmc_g(k, hist, d, mp, b), gexp[(size_t)mp * k.nbins + b]);
-                terms[tid] = __dmul_rn(dv, dv);
-            }
-            __syncthreads();
-            if (tid == 0) {
-                const int m = min(RMC_THREADS, nterm - base);
-                for (int j = 0; j < m; ++j) total = __dadd_rn(total, terms[j]);
-            }
-            __syncthreads();
+        double v = 0.0;
+        for (int q = tid; q < nterm; q += RMC_THREADS) {
+            const int b = q / (k.npairs + 1), mp = q - b * (k.npairs + 1);
+            const double dv = __dsub_rn(rmc_g(k, hist, d, mp, b), gexp[(size_t)mp * k.nbins + b]);
+            v = __dadd_rn(v, __dmul_rn(dv, dv));
         }
-        return total;   // valid in thread 0
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
+        if (lane == 0) wsum[warp] = v;
+        __syncthreads();
+        double t = 0.0;
+        if (warp == 0) {
+            t = wsum[lane];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t = __dadd_rn(t, __shfl_down_sync(0xffffffffu, t, o));
+        }
+        __syncthreads();
+        return t;   // valid in thread 0
     };
-    const double c0 = chisq_of(nullptr);
+    __shared__ double sh_maxd;
+    const int started = out->started;
+    const double c0 = started ? 0.0 : chisq_of(nullptr);
     if (tid == 0) {
-        for (int q = 0; q < 6; ++q) chi_old[q] = 0.0;
-        chi_old[0] = c0;
-        chi_old[5] = c0;
-        u_at = 0;
+        if (started) {
+            for (int q = 0; q < 6; ++q) chi_old[q] = out->chisq[q];
+        } else {
+            for (int q = 0; q < 6; ++q) chi_old[q] = 0.0;
+            chi_old[0] = c0;
+            chi_old[5] = c0;
+        }
+        u_at = started ? out->used : 0;
+        sh_maxd = started ? out->maxd : 0.0;
         sh_stop = 0;
     }
-    long long kall = 1, kacc = 1;
+    long long kall = started ? out->kall : 1, kacc = started ? out->kacc : 1;
     __syncthreads();
     while (kacc < acc_max && kall < max_trials) {
+        if (sh_maxd > dlim) {   // an atom moved too far for the list: rebuild first
+            if (tid == 0) sh_stop = 2;
+            break;
+        }
         ++kall;
         // rmc_move (src/rmc.f90:1366-1428): particle and displacement
         if (tid == 0) {
@@ -165,8 +210,10 @@ __global__ void __launch_bounds__(RMC_THREADS) k_rmc_chain(double* s, const int*
         const int i = sh_i;
         const double o1 = s[i], o2 = s[(size_t)n + i], o3 = s[2 * (size_t)n + i];
         const int ti = type[i];
-        for (int j = tid; j < n; j += RMC_THREADS) {
-            if (j == i) continue;
+        const int nn = ncnt[i];
+        const int* nl = nbr + (size_t)i * cap;
+        for (int q = tid; q < nn; q += RMC_THREADS) {
+            const int j = nl[q];
             const double t1 = s[j], t2 = s[(size_t)n + j], t3 = s[2 * (size_t)n + j];
             const int tj = type[j];
             const int bo = rmc_bin(c, k.bin, o1, o2, o3, t1, t2, t3);
@@ -208,6 +255,11 @@ __global__ void __launch_bounds__(RMC_THREADS) k_rmc_chain(double* s, const int*
             if (sh_acc) {
                 for (int q = 0; q < 6; ++q) chi_old[q] = chi_new[q];
                 for (int d = 0; d < 3; ++d) s[(size_t)d * n + i] = snew[d];
+                // displacement from the list's build position
+                double rx, ry, rz;
+                const double d2 = pairvec_exact(c, snew[0], snew[1], snew[2], sb[i], sb[(size_t)n + i],
+                                                sb[2 * (size_t)n + i], rx, ry, rz);
+                sh_maxd = fmax(sh_maxd, sqrt(d2));
             } else if (!sh_stop) {
                 // the rejected atom goes back by the displacement (src/rmc.f90:628-636)
                 for (int d = 0; d < 3; ++d) s[(size_t)d * n + i] = __dsub_rn(snew[d], disp[d]);
@@ -227,7 +279,9 @@ __global__ void __launch_bounds__(RMC_THREADS) k_rmc_chain(double* s, const int*
         out->kacc = kacc;
         out->used = u_at;
         for (int q = 0; q < 6; ++q) out->chisq[q] = chi_old[q];
+        out->maxd = sh_maxd;
         out->status = sh_stop;
+        out->started = 1;
     }
 }
 

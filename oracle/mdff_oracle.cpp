@@ -44,6 +44,9 @@
 //       coordinates and back at each trial move (the round trip changes the
 //       last bits of all atoms every move); here the chain keeps direct
 //       coordinates and converts once at each end.
+//   D20 eval_chisq_rmc sums the squared g(r) differences left to right;
+//       here by a fixed tree (1024 strided partial sums, then halving trees),
+//       the order of the device's parallel sum (last-bit differences only).
 //   D19 the reference's Metropolis loop reads temp_rmc(6) past its
 //       5-element array (src/rmc.f90:44,531); here the total's temperature
 //       is a parameter.
@@ -2277,15 +2280,26 @@ void gr_normalise(const orc_sys* s, const GrSpec& g, const std::vector<long long
     }
 }
 
-// eval_chisq_rmc (src/rmc.f90:667-690): bins outer, rows inner
+// eval_chisq_rmc (src/rmc.f90:667-690), the squares of the terms
+// q = bin x (npairs + 1) + mp summed by a fixed tree (D20): 1024 strided
+// partial sums in order, a halving tree over each group of 32, the same tree
+// over the 32 group sums
 double chisq_gr(const GrSpec& g, const double* calc, const double* exp_) {
-    double c = 0.0;
-    for (int b = 0; b < g.nbins; ++b)
-        for (int mp = 0; mp <= g.npairs; ++mp) {
-            double d = calc[(size_t)mp * g.nbins + b] - exp_[(size_t)mp * g.nbins + b];
-            c = c + d * d;
-        }
-    return c;
+    const int nterm = (g.npairs + 1) * g.nbins;
+    std::vector<double> part(1024, 0.0);
+    for (int q = 0; q < nterm; ++q) {
+        int b = q / (g.npairs + 1), mp = q - b * (g.npairs + 1);
+        double d = calc[(size_t)mp * g.nbins + b] - exp_[(size_t)mp * g.nbins + b];
+        part[q % 1024] = part[q % 1024] + d * d;
+    }
+    auto tree32 = [](double* v) {
+        for (int o = 16; o > 0; o >>= 1)
+            for (int l = 0; l < o; ++l) v[l] = v[l] + v[l + o];
+        return v[0];
+    };
+    double w[32];
+    for (int k = 0; k < 32; ++k) w[k] = tree32(&part[32 * k]);
+    return tree32(w);
 }
 }  // namespace
 

@@ -129,6 +129,18 @@ module mdff_engine
     integer(c_int) :: natmi(MDFF_NTYPE_MAX)
   end type mdff_frame_header_t
 
+  ! rmctag (src/rmc.f90:36-50) and the chain's report
+  type, bind(C) :: mdff_rmc_params_t
+    real(c_double) :: max_displacement, resolution_gr, cut_rmc
+    real(c_double) :: temp_rmc(6)
+    integer(c_long_long) :: acceptance_max, max_trials
+  end type mdff_rmc_params_t
+  type, bind(C) :: mdff_rmc_result_t
+    integer(c_long_long) :: kall, kacc, uniforms_used
+    real(c_double) :: chisq(6)
+    integer(c_int) :: status, pad
+  end type mdff_rmc_result_t
+
   integer(c_int), parameter :: MDFF_FILE_TRAJFF = 0, MDFF_FILE_CONTFF = 1, MDFF_FILE_EFGALL = 2, &
                                MDFF_FILE_DIPFF = 3, MDFF_FILE_EFALL = 4, MDFF_DATA_V = 1, MDFF_DATA_F = 2
 
@@ -247,6 +259,24 @@ module mdff_engine
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: ctx
       real(c_double), intent(in) :: a(9)
+    end function
+
+    ! g(r) as rmc_gr forms it: grr(0:nbins-1, 0:npairs); grr may be c_null_ptr to get nbins
+    integer(c_int) function mdff_gr(ctx, cut, res, grr, nbins) bind(C, name="mdff_gr")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx, grr
+      real(c_double), value :: cut, res
+      integer(c_int), intent(out) :: nbins
+    end function
+
+    ! rmc_main on the g(r) chi^2; uniforms = c_loc of the host's stream or c_null_ptr (engine stream from seed)
+    integer(c_int) function mdff_rmc(ctx, rp, grr_exp, uniforms, nuni, seed, grr_out, res) bind(C, name="mdff_rmc")
+      import :: c_int, c_ptr, c_double, c_long_long, mdff_rmc_params_t, mdff_rmc_result_t
+      type(c_ptr), value :: ctx, uniforms, grr_out
+      type(mdff_rmc_params_t), intent(in) :: rp
+      real(c_double), intent(in) :: grr_exp(*)
+      integer(c_long_long), value :: nuni, seed
+      type(mdff_rmc_result_t), intent(out) :: res
     end function
 
     ! streaming writer: frames of the context's state, written in the background

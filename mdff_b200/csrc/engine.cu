@@ -1789,6 +1789,9 @@ int mdff_struct_size(int which) {
         case 3: return (int)sizeof(mdff_param_grad);
         case 4: return (int)sizeof(mdff_opt_result);
         case 5: return (int)sizeof(mdff_efg_dist_params);
+        case 6: return (int)sizeof(mdff_frame_header);
+        case 7: return (int)sizeof(mdff_rmc_params);
+        case 8: return (int)sizeof(mdff_rmc_result);
         default: return -1;
     }
 }

@@ -35,6 +35,9 @@ def test_struct_sizes_match():
     assert L.mdff_struct_size(3) == C.sizeof(abi.ParamGrad)
     assert L.mdff_struct_size(4) == C.sizeof(abi.OptResult)
     assert L.mdff_struct_size(5) == C.sizeof(abi.EfgDistParams)
+    assert L.mdff_struct_size(6) == C.sizeof(abi.FrameHeader)
+    assert L.mdff_struct_size(7) == C.sizeof(abi.RmcParams)
+    assert L.mdff_struct_size(8) == C.sizeof(abi.RmcResult)
 
 
 def test_defaults_match_library():

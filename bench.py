@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--ncell", type=int, default=16)
     ap.add_argument("--ext", default="aspc", choices=["aspc", "poly"],
                     help="induced-dipole predictor (algo_ext_dipole)")
-    ap.add_argument("--ext-order", type=int, default=3, help="extrapolate_order of the predictor")
+    ap.add_argument("--ext-order", type=int, default=5, help="extrapolate_order of the predictor (ASPC 5: 7.5 PCG iterations per step against 7.9 at 3)")
     ap.add_argument("--ksplit", type=float, default=None,
                     help="mixed path: |k| below ksplit*alpha summed in FP64 (default: the library's)")
     ap.add_argument("--keps", type=float, default=None,

@@ -20,8 +20,12 @@ namespace mdff {
 // MODE 0: full evaluation (tasks from flags; field / efg / forces from flags)
 // MODE 1: induced-dipole field operator E_i = sum_j T2(r_ij) mu_j (no damping),
 //         the dipole-dipole field of src/field.f90:3354.
+// MODE 2: the damped field of the charges alone (the static field before the
+//         dipole solve: qq, field, damping, optional pair table), with only
+//         what that needs -- one damping factor per pair, no dipoles, no
+//         energy, stress or block partials; the field is MODE 0's, bit for bit.
 template <int G, int MODE>
-__global__ void __launch_bounds__(256, 2) k_ewald_dir(int n, const double* __restrict__ sx, const double* __restrict__ sy,
+__global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, const double* __restrict__ sx, const double* __restrict__ sy,
                                                    const double* __restrict__ sz, const int* __restrict__ type,
                                                    const double* __restrict__ q, const double* __restrict__ mu,
                                                    CellP c, const int* __restrict__ nbr, const int* __restrict__ cnt,
@@ -41,7 +45,8 @@ __global__ void __launch_bounds__(256, 2) k_ewald_dir(int n, const double* __res
         const double si1 = sx[i], si2 = sy[i], si3 = sz[i];
         const int ti = type[i];
         const double qi = MODE == 0 ? q[i] : 0.0;
-        const double mi0 = mu[i], mi1 = mu[n + i], mi2 = mu[2 * n + i];
+        const double mi0 = MODE == 2 ? 0.0 : mu[i], mi1 = MODE == 2 ? 0.0 : mu[n + i],
+                     mi2 = MODE == 2 ? 0.0 : mu[2 * n + i];
         const int m = cnt[i];
         const int* row = nbr + (size_t)i * cap;
         // pair table: the lanes of the group compact the entries inside the
@@ -56,14 +61,13 @@ __global__ void __launch_bounds__(256, 2) k_ewald_dir(int n, const double* __res
             double rx = 0.0, ry = 0.0, rz = 0.0, d2 = 0.0;
             if (valid) d2 = pairvec_exact(c, si1, si2, si3, sx[j], sy[j], sz[j], rx, ry, rz);
             const bool in = valid && d2 <= fl.cutsq;
-            if (MODE == 0 && fl.ddtab) {
+            if (MODE != 1 && fl.ddtab) {
                 const unsigned bal = (__ballot_sync(gmask, in) & gmask) >> g0;
                 pos = cbase + __popc(bal & ((1u << sub) - 1u));
                 if (in) fl.ddnbr[(size_t)i * cap + pos] = j;
                 cbase += __popc(bal);
             }
             if (!in) continue;
-            const double mj0 = mu[j], mj1 = mu[n + j], mj2 = mu[2 * n + j];
             const double d = sqrt(d2);
             const double dm1 = 1.0 / d, dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2, dm7 = dm5 * dm2;
             const double ex2 = exp(-a2 * d2), expon = ex2 * rsqpi;
@@ -72,8 +76,23 @@ __global__ void __launch_bounds__(256, 2) k_ewald_dir(int n, const double* __res
             const double F2 = F1 + c43a3 * d2 * d * expon;
             const double A1 = F1 * dm3;
             const double B2 = 3.0 * F2 * dm5;
+            if (MODE != 1 && fl.ddtab) fl.ddtab[(size_t)i * cap + pos] = make_float2((float)A1, (float)B2);
+            if (MODE == 2) {
+                double gi = 0.0;
+                if (fl.damp) {
+                    const PairConst& P = pc[ti * NT + type[j]];
+                    if (P.ldamp) {
+                        double f1, gd;
+                        tt_damp_d(P.db_i, P.dc_i, d, P.dk_i, f1, gd);
+                        gi = 1.0 - f1;
+                    }
+                }
+                const double s = q[j] * (F1 - gi) * dm3;
+                E[0] += s * rx; E[1] += s * ry; E[2] += s * rz;
+                continue;
+            }
+            const double mj0 = mu[j], mj1 = mu[n + j], mj2 = mu[2 * n + j];
             const double rmj = rx * mj0 + ry * mj1 + rz * mj2;
-            if (MODE == 0 && fl.ddtab) fl.ddtab[(size_t)i * cap + pos] = make_float2((float)A1, (float)B2);
             if (MODE == 1) {
                 E[0] += rx * rmj * B2 - mj0 * A1;
                 E[1] += ry * rmj * B2 - mj1 * A1;
@@ -160,7 +179,7 @@ __global__ void __launch_bounds__(256, 2) k_ewald_dir(int n, const double* __res
                 S[3] += rx * fi1 + ry * fi0; S[4] += rx * fi2 + rz * fi0; S[5] += ry * fi2 + rz * fi1;
             }
         }
-        if (MODE == 0 && fl.ddtab && sub == 0) fl.ddcnt[i] = cbase;
+        if (MODE != 1 && fl.ddtab && sub == 0) fl.ddcnt[i] = cbase;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) E[k] = group_sum<G>(E[k]);
@@ -175,7 +194,7 @@ __global__ void __launch_bounds__(256, 2) k_ewald_dir(int n, const double* __res
         }
     }
     if (active && sub == 0) {
-        if (MODE == 1 || fl.field) { ef[i] = E[0]; ef[n + i] = E[1]; ef[2 * n + i] = E[2]; }
+        if (MODE != 0 || fl.field) { ef[i] = E[0]; ef[n + i] = E[1]; ef[2 * n + i] = E[2]; }
         if (MODE == 0 && fl.efg)
             for (int k = 0; k < 6; ++k) efg[(size_t)k * n + i] = Gd[k];
         if (MODE == 0 && fl.forces) { fo[i] = F[0]; fo[n + i] = F[1]; fo[2 * n + i] = F[2]; }
@@ -344,6 +363,12 @@ void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy
         if (g == 8) DIR(8, 1, nullptr);
         else if (g == 32) DIR(32, 1, nullptr);
         else DIR(16, 1, nullptr);
+        return;
+    }
+    if (fl.qq && fl.field && !fl.qd && !fl.dd && !fl.efg && !fl.forces) {   // the charges' field alone
+        if (g == 8) DIR(8, 2, nullptr);
+        else if (g == 32) DIR(32, 2, nullptr);
+        else DIR(16, 2, nullptr);
         return;
     }
     if (g == 8) DIR(8, 0, part.buf);

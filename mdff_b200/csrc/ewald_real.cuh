@@ -24,6 +24,8 @@ namespace mdff {
 //         dipole solve: qq, field, damping, optional pair table), with only
 //         what that needs -- one damping factor per pair, no dipoles, no
 //         energy, stress or block partials; the field is MODE 0's, bit for bit.
+// MODE 3: MODE 0 without the field gradient (every step but the EFG steps),
+//         so its registers are not sized for it.
 template <int G, int MODE>
 __global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, const double* __restrict__ sx, const double* __restrict__ sy,
                                                    const double* __restrict__ sz, const int* __restrict__ type,
@@ -44,7 +46,7 @@ __global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, con
     if (active) {
         const double si1 = sx[i], si2 = sy[i], si3 = sz[i];
         const int ti = type[i];
-        const double qi = MODE == 0 ? q[i] : 0.0;
+        const double qi = (MODE == 0 || MODE == 3) ? q[i] : 0.0;
         const double mi0 = MODE == 2 ? 0.0 : mu[i], mi1 = MODE == 2 ? 0.0 : mu[n + i],
                      mi2 = MODE == 2 ? 0.0 : mu[2 * n + i];
         const int m = cnt[i];
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, con
                     const double s = qj * (F1 - gi) * dm3;
                     E[0] += s * rx; E[1] += s * ry; E[2] += s * rz;
                 }
-                if (fl.efg) {
+                if (MODE == 0 && fl.efg) {
                     const double b = -qj * B2, dg = qj * A1;
                     Gd[0] += b * rx * rx + dg; Gd[1] += b * ry * ry + dg; Gd[2] += b * rz * rz + dg;
                     Gd[3] += b * rx * ry; Gd[4] += b * rx * rz; Gd[5] += b * ry * rz;
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, con
                     E[1] += ry * rmj * B2 - mj1 * A1;
                     E[2] += rz * rmj * B2 - mj2 * A1;
                 }
-                if (fl.efg) {
+                if (MODE == 0 && fl.efg) {
                     const double t = -rmj * C3;
                     Gd[0] += t * rx * rx + rmj * B2 + 2.0 * rx * mj0 * B2;
                     Gd[1] += t * ry * ry + rmj * B2 + 2.0 * ry * mj1 * B2;
@@ -183,8 +185,8 @@ __global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, con
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) E[k] = group_sum<G>(E[k]);
-    if (MODE == 0) {
-        if (fl.efg) {
+    if (MODE == 0 || MODE == 3) {
+        if (MODE == 0 && fl.efg) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) Gd[k] = group_sum<G>(Gd[k]);
         }
@@ -194,12 +196,12 @@ __global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, con
         }
     }
     if (active && sub == 0) {
-        if (MODE != 0 || fl.field) { ef[i] = E[0]; ef[n + i] = E[1]; ef[2 * n + i] = E[2]; }
+        if (MODE == 1 || MODE == 2 || fl.field) { ef[i] = E[0]; ef[n + i] = E[1]; ef[2 * n + i] = E[2]; }
         if (MODE == 0 && fl.efg)
             for (int k = 0; k < 6; ++k) efg[(size_t)k * n + i] = Gd[k];
-        if (MODE == 0 && fl.forces) { fo[i] = F[0]; fo[n + i] = F[1]; fo[2 * n + i] = F[2]; }
+        if ((MODE == 0 || MODE == 3) && fl.forces) { fo[i] = F[0]; fo[n + i] = F[1]; fo[2 * n + i] = F[2]; }
     }
-    if (MODE == 0) {
+    if (MODE == 0 || MODE == 3) {
         double v[8] = {u, S[0], S[1], S[2], S[3], S[4], S[5], 0.0};
         block_partials<8>(v, part);
     }
@@ -371,7 +373,11 @@ void launch_ewald_dir(cudaStream_t st, int n, const double* sx, const double* sy
         else DIR(16, 2, nullptr);
         return;
     }
-    if (g == 8) DIR(8, 0, part.buf);
+    if (!fl.efg) {   // no field gradient this step
+        if (g == 8) DIR(8, 3, part.buf);
+        else if (g == 32) DIR(32, 3, part.buf);
+        else DIR(16, 3, part.buf);
+    } else if (g == 8) DIR(8, 0, part.buf);
     else if (g == 32) DIR(32, 0, part.buf);
     else DIR(16, 0, part.buf);
 #undef DIR

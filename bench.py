@@ -246,13 +246,16 @@ def run_engine(args):
                "h2d_bytes_per_step": 6 * 8 * natm, "d2h_bytes_per_step": 9 * 8 * natm}
     # trajectory streaming: the same steps with TRAJFF frames written through
     # the engine's writer (device snapshot, copy stream, writer thread), against
-    # the same loop without frames; wall time includes draining the writer
+    # the same loop without frames.  wall_ms_per_step runs to the end of the
+    # last step on the device (frames that the writer could not keep up with
+    # block frame() and show there); drain_ms_after_last_step is the writer's
+    # tail, the frames still being formatted or written when the steps end
     stream = None
     if not args.no_stream:
         import shutil
         import tempfile
         tmpd = tempfile.mkdtemp(prefix="mdff_stream_")
-        ks = max(10, args.steps)
+        ks = max(40, args.steps)
 
         shm = tempfile.mkdtemp(prefix="mdff_stream_", dir="/dev/shm") if os.path.isdir("/dev/shm") else None
 
@@ -271,13 +274,14 @@ def run_engine(args):
                 if w is not None and (k + 1) % every == 0:
                     w.frame()
             b.record(ext)
-            if w is not None:
-                w.close()
             b.synchronize()
             t2 = time.perf_counter()
-            return a.elapsed_time(b), (t2 - t1) * 1e3
+            if w is not None:
+                w.close()
+            t3 = time.perf_counter()
+            return a.elapsed_time(b), (t2 - t1) * 1e3, (t3 - t2) * 1e3
 
-        base_ms, base_wall = run_stream(1, 0)
+        base_ms, base_wall, _ = run_stream(1, 0)
         stream = {"steps": ks, "dir": tmpd, "no_frames": {"device_ms_per_step": base_ms / ks,
                                                           "wall_ms_per_step": base_wall / ks}}
         cases = [("trajff_rvf_unformatted_every_step", 0, 1, tmpd),
@@ -286,11 +290,13 @@ def run_engine(args):
             cases += [("trajff_rvf_unformatted_every_step_to_dev_shm", 0, 1, shm),
                       ("trajff_rvf_formatted_every_10_steps_to_dev_shm", 1, 10, shm)]
         for label, iformat, every, where in cases:
-            d_ms, w_ms = run_stream(iformat, every, where)
+            d_ms, w_ms, drain_ms = run_stream(iformat, every, where)
             nbytes = os.path.getsize(os.path.join(where, f"TRAJFF{iformat}"))
             stream[label] = {"device_ms_per_step": d_ms / ks, "wall_ms_per_step": w_ms / ks,
                              "wall_overhead_vs_no_frames": w_ms / base_wall - 1.0,
-                             "bytes_written": nbytes, "file_mb_per_s": nbytes / (w_ms / 1e3) / 1e6}
+                             "drain_ms_after_last_step": drain_ms,
+                             "bytes_written": nbytes,
+                             "file_mb_per_s": nbytes / ((w_ms + drain_ms) / 1e3) / 1e6}
         shutil.rmtree(tmpd, ignore_errors=True)
         if shm:
             shutil.rmtree(shm, ignore_errors=True)

@@ -111,7 +111,7 @@ module mdff_engine
 
   type, bind(C) :: mdff_opt_result_t
     real(c_double) :: u_initial, u_final, phigrad
-    integer(c_int) :: iterations, nforce, status, pad
+    integer(c_int) :: iterations, nforce, status, info
   end type mdff_opt_result_t
 
   ! efgtag's distribution settings (src/efg.f90:171-190)
@@ -200,6 +200,15 @@ module mdff_engine
       import :: c_int, c_ptr, mdff_opt_result_t
       type(c_ptr), value :: ctx
       integer(c_int), value :: itmax
+      type(mdff_opt_result_t), intent(out) :: res
+    end function
+
+    ! optalgo = 'lbfgs' of opt_main: eps = epsrel_lbfgs
+    integer(c_int) function mdff_opt_lbfgs(ctx, itmax, eps, res) bind(C, name="mdff_opt_lbfgs")
+      import :: c_int, c_double, c_ptr, mdff_opt_result_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: itmax
+      real(c_double), value :: eps
       type(mdff_opt_result_t), intent(out) :: res
     end function
 

@@ -206,9 +206,13 @@ typedef struct mdff_opt_result {
     double phigrad;     /* sum of the squared force components at the end (eV^2/A^2) */
     int    iterations;  /* conjugate-gradient iterations (its) */
     int    nforce;      /* force evaluations (neng) */
-    int    status;      /* 0: minimum reached (energy unchanged to ftol); 1: itmax iterations;
-                           2: zero gradient; 3: the line search made no progress in 100 steps */
-    int    pad;
+    int    status;      /* 0: minimum reached (sastry: energy unchanged to ftol; lbfgs: |G| / max(1, |X|)
+                           <= eps); 1: itmax iterations (sastry) or force evaluations (lbfgs);
+                           2: zero gradient; 3: the line search failed (sastry: no progress in 100
+                           steps; lbfgs: MCSRCH returned info != 1, IFLAG = -1) */
+    int    info;        /* lbfgs with status 3: MCSRCH's info (0 not a descent direction or bad
+                           input, 2 interval below xtol, 3 maxfev reached, 4/5 at stpmin/stpmax,
+                           6 rounding errors); 0 otherwise */
 } mdff_opt_result;
 
 /* Distribution settings of efg_stat (the efgtag namelist, src/efg.f90:171-190):
@@ -338,6 +342,21 @@ int  mdff_engforce(mdff_ctx* ctx, double* fx, double* fy, double* fz,
  * forces are those of the minimum; *out gets pot0, Eis, phigrad, iter, neng.
  * itmax: the reference's 10000. */
 int  mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out);
+
+/* Structure optimisation by limited-memory BFGS: lbfgs_driver (src/opt.f90:
+ * 972-1194) over Nocedal's LBFGS (src/lbfgs.f90:243-456; m = 5 pairs, no
+ * user diagonal) and the More-Thuente line search MCSRCH/MCSTEP
+ * (:655-1186; ftol 1e-4, gtol 0.9, maxfev 100, xtol tiny(1.0_dp)) on
+ * X = (rx, ry, rz), G = -f, F = u_tot -- optalgo = 'lbfgs' of opt_main.
+ * eps: the reference's epsrel_lbfgs (1e-5), the test |G| / max(1, |X|) <= eps.
+ * itmax bounds the force evaluations (the driver's loop, 10000 there).  Every
+ * evaluation is one mdff_engforce on the lists of the starting configuration.
+ * On return the positions and forces are those of the last evaluation (the
+ * accepted point when status = 0); *out gets pot0 (u_initial), Eis (u_final),
+ * phigrad as the driver leaves it (|G|^2 of the evaluation before the last),
+ * the L-BFGS iterations and the evaluations (nforce; the reference reports
+ * this count as both iter and neng). */
+int  mdff_opt_lbfgs(mdff_ctx* ctx, int itmax, double eps, mdff_opt_result* out);
 
 /* EFG post-processing (efg_stat, src/efg.f90:2057-2440, and nmr_convention,
  * :2546-2650) on the device, over nconf configurations of the context's

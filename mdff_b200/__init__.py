@@ -68,6 +68,7 @@ def lib():
         L.mdff_measure_pipes.argtypes = [C.c_int, dp]
         L.mdff_measure_tensor.argtypes = [C.c_int, dp]
         L.mdff_opt_sastry.argtypes = [vp, C.c_int, C.POINTER(abi.OptResult)]
+        L.mdff_opt_lbfgs.argtypes = [vp, C.c_int, C.c_double, C.POINTER(abi.OptResult)]
         L.mdff_profile_detail.argtypes = [vp, dp, C.POINTER(C.c_longlong), dp]
         L.mdff_io_format.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(abi.FrameHeader), ip, dp, C.c_char_p,
                                      C.c_size_t, C.POINTER(C.c_size_t)]
@@ -248,6 +249,15 @@ class Engine:
         the engine's positions are left at the minimum."""
         r = abi.OptResult()
         self._check(lib().mdff_opt_sastry(self._h, int(itmax), C.byref(r)))
+        return r.as_dict()
+
+    def opt_lbfgs(self, itmax=10000, eps=1.0e-5):
+        """Structure optimisation from the current positions by limited-memory
+        BFGS (the reference's lbfgs_driver; eps is epsrel_lbfgs, itmax bounds
+        the force evaluations); the engine's positions are left at the last
+        evaluated point."""
+        r = abi.OptResult()
+        self._check(lib().mdff_opt_lbfgs(self._h, int(itmax), float(eps), C.byref(r)))
         return r.as_dict()
 
     def _efg_input(self, efg):

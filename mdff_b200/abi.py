@@ -96,10 +96,10 @@ class Thermo(C.Structure):
 class OptResult(C.Structure):
     """mdff_opt_result: one structure optimisation (opt_main's report)."""
     _fields_ = [("u_initial", C.c_double), ("u_final", C.c_double), ("phigrad", C.c_double),
-                ("iterations", C.c_int), ("nforce", C.c_int), ("status", C.c_int), ("pad", C.c_int)]
+                ("iterations", C.c_int), ("nforce", C.c_int), ("status", C.c_int), ("info", C.c_int)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 FILE_TRAJFF, FILE_CONTFF, FILE_EFGALL, FILE_DIPFF, FILE_EFALL = 0, 1, 2, 3, 4

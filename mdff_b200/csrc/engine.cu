@@ -78,6 +78,7 @@ struct mdff_ctx {
     double* hist = nullptr;
     double* coef = nullptr;
     double *opt_xi = nullptr, *opt_g = nullptr, *opt_h = nullptr, *opt_r0 = nullptr;   // structure optimisation
+    double *lb_s = nullptr, *lb_y = nullptr, *lb_w = nullptr, *lb_wa = nullptr, *lb_g0 = nullptr, *lb_sc = nullptr;
     double *efgp_t = nullptr, *efgp_nmr = nullptr, *efgp_part = nullptr;   // EFG post-processing scratch
     int* efgp_hist = nullptr;
     size_t efgp_tcap = 0, efgp_ncap = 0, efgp_pcap = 0, efgp_hcap = 0;
@@ -1438,6 +1439,308 @@ int opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* R) {
     return MDFF_OK;
 }
 
+// ---- L-BFGS ------------------------------------------------------------------
+// lbfgs_driver (src/opt.f90:972-1194) with LBFGS (src/lbfgs.f90:243-456):
+// Nocedal's limited-memory BFGS, m = 5 pairs, no user diagonal, and the
+// More-Thuente line search MCSRCH/MCSTEP (:655-1186) with ftol 1e-4, gtol
+// 0.9, maxfev 100, stpmin 1e-20, stpmax 1e20, xtol = tiny(1.0_dp).  The
+// reverse communication of the reference becomes direct calls of engforce at
+// the trial points; every evaluation is one of the driver's iterations, at
+// most itmax of them.  The S and Y pairs, the direction and the two-loop
+// recursion stay on the device (the recursion's coefficients in device
+// scalars, no host round trip); the line search's scalars come to the host.
+constexpr int LB_M = 5;
+
+struct LbState {
+    int icall = 0, itmax = 0;
+    double F = 0.0, gg = 0.0, phigrad = 0.0;
+};
+
+V3 lb_pos(const mdff_ctx* c) { return V3{{c->x, c->y, c->z}, 1.0}; }
+V3 lb_grad(const mdff_ctx* c) { return V3{{c->fx, c->fy, c->fz}, -1.0}; }
+V3 lb_buf(const double* b, int n) { return V3{{b, b + n, b + 2 * (size_t)n}, 1.0}; }
+
+int lb_dots(mdff_ctx* ctx, V3 a0, V3 b0, V3 a1, V3 b1, int K, double out[2]) {
+    const int n = ctx->n;
+    if (K == 1) k_lb_dots<1><<<nb(n), 256, 0, ctx->st>>>(n, a0, b0, a1, b1, ctx->part.buf);
+    else k_lb_dots<2><<<nb(n), 256, 0, ctx->st>>>(n, a0, b0, a1, b1, ctx->part.buf);
+    return opt_sum(ctx, K, out);
+}
+
+// one function evaluation of the driver loop at the current device positions:
+// F = u_tot, G = -f, and |G|^2 (the driver's phigrad is that of the previous
+// evaluation when LBFGS returns).  Returns 1 when itmax evaluations are done.
+int lb_eval(mdff_ctx* ctx, LbState& L, int& stop) {
+    stop = 0;
+    if (L.icall >= L.itmax) { stop = 1; return MDFF_OK; }
+    TRY(engforce_device(ctx));
+    L.icall = L.icall + 1;
+    L.phigrad = L.gg;
+    L.F = opt_utot(ctx);
+    double t[2];
+    TRY(lb_dots(ctx, lb_grad(ctx), lb_grad(ctx), lb_grad(ctx), lb_grad(ctx), 1, t));
+    L.gg = t[0];
+    return MDFF_OK;
+}
+
+// MCSTEP (src/lbfgs.f90:960-1186): one safeguarded cubic or quadratic step of
+// the More-Thuente interval update.  The 0.66 of the final safeguard is a
+// default-real (single-precision) constant in the reference.
+void lb_mcstep(double& stx, double& fx, double& dx, double& sty, double& fy, double& dy, double& stp, double fp,
+               double dp, bool& brackt, double stpmin, double stpmax, int& info) {
+    info = 0;
+    if ((brackt && (stp <= std::min(stx, sty) || stp >= std::max(stx, sty))) || dx * (stp - stx) >= 0.0 ||
+        stpmax < stpmin)
+        return;
+    const double sgnd = dp * (dx / std::fabs(dx));
+    double stpf, stpc, stpq, theta, s, gamma, p, q, r;
+    bool bound;
+    if (fp > fx) {
+        info = 1;
+        bound = true;
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp;
+        s = std::max(std::max(std::fabs(theta), std::fabs(dx)), std::fabs(dp));
+        gamma = s * std::sqrt((theta / s) * (theta / s) - (dx / s) * (dp / s));
+        if (stp < stx) gamma = -gamma;
+        p = (gamma - dx) + theta;
+        q = ((gamma - dx) + gamma) + dp;
+        r = p / q;
+        stpc = stx + r * (stp - stx);
+        stpq = stx + ((dx / ((fx - fp) / (stp - stx) + dx)) / 2) * (stp - stx);
+        if (std::fabs(stpc - stx) < std::fabs(stpq - stx)) stpf = stpc;
+        else stpf = stpc + (stpq - stpc) / 2;
+        brackt = true;
+    } else if (sgnd < 0.0) {
+        info = 2;
+        bound = false;
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp;
+        s = std::max(std::max(std::fabs(theta), std::fabs(dx)), std::fabs(dp));
+        gamma = s * std::sqrt((theta / s) * (theta / s) - (dx / s) * (dp / s));
+        if (stp > stx) gamma = -gamma;
+        p = (gamma - dp) + theta;
+        q = ((gamma - dp) + gamma) + dx;
+        r = p / q;
+        stpc = stp + r * (stx - stp);
+        stpq = stp + (dp / (dp - dx)) * (stx - stp);
+        stpf = std::fabs(stpc - stp) > std::fabs(stpq - stp) ? stpc : stpq;
+        brackt = true;
+    } else if (std::fabs(dp) < std::fabs(dx)) {
+        info = 3;
+        bound = true;
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp;
+        s = std::max(std::max(std::fabs(theta), std::fabs(dx)), std::fabs(dp));
+        gamma = s * std::sqrt(std::max(0.0, (theta / s) * (theta / s) - (dx / s) * (dp / s)));
+        if (stp > stx) gamma = -gamma;
+        p = (gamma - dp) + theta;
+        q = (gamma + (dx - dp)) + gamma;
+        r = p / q;
+        if (r < 0.0 && gamma != 0.0) stpc = stp + r * (stx - stp);
+        else if (stp > stx) stpc = stpmax;
+        else stpc = stpmin;
+        stpq = stp + (dp / (dp - dx)) * (stx - stp);
+        if (brackt) stpf = std::fabs(stp - stpc) < std::fabs(stp - stpq) ? stpc : stpq;
+        else stpf = std::fabs(stp - stpc) > std::fabs(stp - stpq) ? stpc : stpq;
+    } else {
+        info = 4;
+        bound = false;
+        if (brackt) {
+            theta = 3 * (fp - fy) / (sty - stp) + dy + dp;
+            s = std::max(std::max(std::fabs(theta), std::fabs(dy)), std::fabs(dp));
+            gamma = s * std::sqrt((theta / s) * (theta / s) - (dy / s) * (dp / s));
+            if (stp > sty) gamma = -gamma;
+            p = (gamma - dp) + theta;
+            q = ((gamma - dp) + gamma) + dy;
+            r = p / q;
+            stpc = stp + r * (sty - stp);
+            stpf = stpc;
+        } else if (stp > stx) {
+            stpf = stpmax;
+        } else {
+            stpf = stpmin;
+        }
+    }
+    if (fp > fx) {
+        sty = stp; fy = fp; dy = dp;
+    } else {
+        if (sgnd < 0.0) { sty = stx; fy = fx; dy = dx; }
+        stx = stp; fx = fp; dx = dp;
+    }
+    stpf = std::min(stpmax, stpf);
+    stpf = std::max(stpmin, stpf);
+    stp = stpf;
+    if (brackt && bound) {
+        const double p66 = (double)0.66f;
+        if (sty > stx) stp = std::min(stx + p66 * (sty - stx), stp);
+        else stp = std::max(stx + p66 * (sty - stx), stp);
+    }
+}
+
+// MCSRCH (src/lbfgs.f90:655-957) along s from the current point: info as
+// there (1 success; 0 bad input or not a descent direction; 2-6 the
+// tolerance, step-bound and evaluation-limit exits), stop = 1 when the
+// driver's evaluation budget ran out inside the search.
+int lb_mcsrch(mdff_ctx* ctx, LbState& L, const double* sdir, double& stp, double ftol, double xtol, int maxfev,
+              int& info, int& nfev, int& stop) {
+    const int n = ctx->n;
+    const double gtol = 0.9, stpmin = 1.0e-20, stpmax = 1.0e20, p5 = 0.5, p66 = 0.66, xtrapf = 4.0;
+    int infoc = 1;
+    info = 0;
+    stop = 0;
+    if (n <= 0 || stp <= 0.0 || ftol < 0.0 || gtol < 0.0 || xtol < 0.0 || stpmin < 0.0 || stpmax < stpmin ||
+        maxfev <= 0)
+        return MDFF_OK;
+    double t[2];
+    const V3 S = lb_buf(sdir, n);
+    TRY(lb_dots(ctx, lb_grad(ctx), S, S, S, 1, t));
+    const double dginit = t[0];
+    if (dginit >= 0.0) return MDFF_OK;
+    bool brackt = false, stage1 = true;
+    nfev = 0;
+    const double finit = L.F, dgtest = ftol * dginit;
+    double width = stpmax - stpmin, width1 = width / p5;
+    CK(cudaMemcpyAsync(ctx->lb_wa, ctx->x, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->lb_wa + n, ctx->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->lb_wa + 2 * (size_t)n, ctx->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    double stx = 0.0, fx = finit, dgx = dginit, sty = 0.0, fy = finit, dgy = dginit, stmin, stmax;
+    for (;;) {
+        if (brackt) {
+            stmin = std::min(stx, sty);
+            stmax = std::max(stx, sty);
+        } else {
+            stmin = stx;
+            stmax = stp + xtrapf * (stp - stx);
+        }
+        stp = std::max(stp, stpmin);
+        stp = std::min(stp, stpmax);
+        if ((brackt && (stp <= stmin || stp >= stmax)) || nfev >= maxfev - 1 || infoc == 0 ||
+            (brackt && stmax - stmin <= xtol * stmax))
+            stp = stx;
+        k_lb_place<<<nb(n), 256, 0, ctx->st>>>(n, ctx->lb_wa, sdir, stp, ctx->x, ctx->y, ctx->z);
+        TRY(lb_eval(ctx, L, stop));
+        if (stop) return MDFF_OK;
+        info = 0;
+        nfev = nfev + 1;
+        TRY(lb_dots(ctx, lb_grad(ctx), S, S, S, 1, t));
+        const double dg = t[0], f = L.F;
+        const double ftest1 = finit + stp * dgtest;
+        if ((brackt && (stp <= stmin || stp >= stmax)) || infoc == 0) info = 6;
+        if (stp == stpmax && f <= ftest1 && dg <= dgtest) info = 5;
+        if (stp == stpmin && (f > ftest1 || dg >= dgtest)) info = 4;
+        if (nfev >= maxfev) info = 3;
+        if (brackt && stmax - stmin <= xtol * stmax) info = 2;
+        if (f <= ftest1 && std::fabs(dg) <= gtol * (-dginit)) info = 1;
+        if (info != 0) return MDFF_OK;
+        if (stage1 && f <= ftest1 && dg >= std::min(ftol, gtol) * dginit) stage1 = false;
+        if (stage1 && f <= fx && f > ftest1) {
+            double fm = f - stp * dgtest, fxm = fx - stx * dgtest, fym = fy - sty * dgtest;
+            double dgm = dg - dgtest, dgxm = dgx - dgtest, dgym = dgy - dgtest;
+            lb_mcstep(stx, fxm, dgxm, sty, fym, dgym, stp, fm, dgm, brackt, stmin, stmax, infoc);
+            fx = fxm + stx * dgtest;
+            fy = fym + sty * dgtest;
+            dgx = dgxm + dgtest;
+            dgy = dgym + dgtest;
+        } else {
+            lb_mcstep(stx, fx, dgx, sty, fy, dgy, stp, f, dg, brackt, stmin, stmax, infoc);
+        }
+        if (brackt) {
+            if (std::fabs(sty - stx) >= p66 * width1) stp = stx + p5 * (sty - stx);
+            width1 = width;
+            width = std::fabs(sty - stx);
+        }
+    }
+}
+
+int opt_lbfgs(mdff_ctx* ctx, int itmax, double eps, mdff_opt_result* R) {
+    const int n = ctx->n, M = LB_M;
+    const size_t n3 = 3 * (size_t)n;
+    if (!ctx->lb_s) {
+        TRY(dalloc(ctx, &ctx->lb_s, M * n3));
+        TRY(dalloc(ctx, &ctx->lb_y, M * n3));
+        TRY(dalloc(ctx, &ctx->lb_w, n3));
+        TRY(dalloc(ctx, &ctx->lb_wa, n3));
+        TRY(dalloc(ctx, &ctx->lb_g0, n3));
+        TRY(dalloc(ctx, &ctx->lb_sc, 1 + M));
+    }
+    LbState L;
+    L.itmax = itmax;
+    int stop = 0;
+    *R = mdff_opt_result{};
+    R->status = 1;
+    TRY(lb_eval(ctx, L, stop));
+    R->u_initial = L.F;
+    const double ftol = 1.0e-4, xtol = 2.2250738585072014e-308;   // tiny(1.0_dp)
+    const int maxfev = 100;
+    double rho[LB_M] = {0}, t[2];
+    int iter = 0, point = 0;
+    size_t npt = 0;
+    const int nb3 = (int)((n3 + 255) / 256);
+    // the first direction -G DIAG, DIAG = 1, and STP1 = 1 / |G|
+    k_lb_negg<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, 1.0, ctx->lb_s);
+    const double stp1 = 1.0 / std::sqrt(L.gg);
+    auto finish = [&](int status, int info) {
+        // the driver's phigrad: |G|^2 of the evaluation before the last one
+        // when LBFGS ends, of the last one when the evaluations run out
+        R->u_final = L.F;
+        R->phigrad = status == 1 ? L.gg : L.phigrad;
+        R->iterations = iter;
+        R->nforce = L.icall;
+        R->status = status;
+        R->info = info;
+        return MDFF_OK;
+    };
+    for (;;) {
+        iter = iter + 1;
+        int bound = iter - 1;
+        if (iter != 1) {
+            if (iter > M) bound = M;
+            const double* yp = ctx->lb_y + npt;
+            const double* sp = ctx->lb_s + npt;
+            TRY(lb_dots(ctx, lb_buf(yp, n), lb_buf(sp, n), lb_buf(yp, n), lb_buf(yp, n), 2, t));
+            const double ys = t[0], yy = t[1], diag = ys / yy;
+            rho[point == 0 ? M - 1 : point - 1] = 1.0 / ys;
+            k_lb_negg<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, 1.0, ctx->lb_w);
+            int cp = point;
+            for (int i = 0; i < bound; ++i) {
+                cp = cp - 1;
+                if (cp == -1) cp = M - 1;
+                k_lb_dots<1><<<nb(n), 256, 0, ctx->st>>>(n, lb_buf(ctx->lb_s + cp * n3, n), lb_buf(ctx->lb_w, n),
+                                                          lb_buf(ctx->lb_w, n), lb_buf(ctx->lb_w, n), ctx->part.buf);
+                launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->lb_sc, 0);
+                k_lb_twoloop<true><<<nb3, 256, 0, ctx->st>>>((int)n3, ctx->lb_w, ctx->lb_y + cp * n3, ctx->lb_sc,
+                                                             rho[cp], cp);
+            }
+            k_lb_scale<<<nb3, 256, 0, ctx->st>>>((int)n3, ctx->lb_w, diag);
+            for (int i = 0; i < bound; ++i) {
+                k_lb_dots<1><<<nb(n), 256, 0, ctx->st>>>(n, lb_buf(ctx->lb_y + cp * n3, n), lb_buf(ctx->lb_w, n),
+                                                          lb_buf(ctx->lb_w, n), lb_buf(ctx->lb_w, n), ctx->part.buf);
+                launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->lb_sc, 0);
+                k_lb_twoloop<false><<<nb3, 256, 0, ctx->st>>>((int)n3, ctx->lb_w, ctx->lb_s + cp * n3, ctx->lb_sc,
+                                                              rho[cp], cp);
+                cp = cp + 1;
+                if (cp == M) cp = 0;
+            }
+            CK(cudaMemcpyAsync(ctx->lb_s + point * n3, ctx->lb_w, sizeof(double) * n3, cudaMemcpyDeviceToDevice,
+                               ctx->st));
+            TRY(check_launch(ctx, "lbfgs two-loop recursion"));
+        }
+        // label 165: line search from STP = 1 (STP1 on the first iteration)
+        int nfev = 0, info = 0;
+        double stp = iter == 1 ? stp1 : 1.0;
+        k_lb_keepg<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->lb_g0);
+        TRY(lb_mcsrch(ctx, L, ctx->lb_s + point * n3, stp, ftol, xtol, maxfev, info, nfev, stop));
+        if (stop) return finish(1, 0);
+        if (info != 1) return finish(3, info);
+        npt = point * n3;
+        k_lb_pair<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->lb_g0, stp, ctx->lb_s + npt,
+                                              ctx->lb_y + npt);
+        point = point + 1;
+        if (point == M) point = 0;
+        TRY(lb_dots(ctx, lb_grad(ctx), lb_grad(ctx), lb_pos(ctx), lb_pos(ctx), 2, t));
+        const double gnorm = std::sqrt(t[0]), xnorm = std::max(1.0, std::sqrt(t[1]));
+        if (gnorm / xnorm <= eps) return finish(0, 0);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1632,6 +1935,15 @@ int mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out) {
     cudaSetDevice(ctx->p.device);
     std::memset(out, 0, sizeof *out);
     return opt_sastry(ctx, itmax, out);
+}
+
+int mdff_opt_lbfgs(mdff_ctx* ctx, int itmax, double eps, mdff_opt_result* out) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!out || itmax < 1 || !(eps >= 0.0))
+        return fail(ctx, MDFF_E_ARG, "mdff_opt_lbfgs: out must be given, itmax >= 1 and eps >= 0");
+    cudaSetDevice(ctx->p.device);
+    std::memset(out, 0, sizeof *out);
+    return opt_lbfgs(ctx, itmax, eps, out);
 }
 
 

@@ -102,3 +102,108 @@ __global__ void k_opt_cg(int n, const double* __restrict__ fx, const double* __r
 }
 
 }  // namespace mdff
+
+namespace mdff {
+
+// ---- L-BFGS (lbfgs_driver, src/opt.f90:972-1194, over LBFGS/MCSRCH of
+// src/lbfgs.f90:243-957) ----------------------------------------------------
+// The optimisation vector is X = (rx, ry, rz) and G = -(fx, fy, fz) as the
+// driver packs them.  A V3 names the three component arrays of one 3N vector
+// (the engine's SoA positions and forces, or a component-major buffer) and a
+// sign applied on reading, so G is read straight from the forces.
+struct V3 {
+    const double* c[3];
+    double sgn;
+};
+
+__device__ __forceinline__ double v3(const V3& v, int c, int i) { return v.sgn * v.c[c][i]; }
+
+// K = 1 or 2 dot products a0.b0 (and a1.b1), per-atom terms first
+template <int K>
+__global__ void k_lb_dots(int n, V3 a0, V3 b0, V3 a1, V3 b1, double* part) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = 0.0;
+    if (i < n) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            v[0] = v[0] + v3(a0, c, i) * v3(b0, c, i);
+            if (K > 1) v[K - 1] = v[K - 1] + v3(a1, c, i) * v3(b1, c, i);
+        }
+    }
+    block_partials<K>(v, part);
+}
+
+// One step of the two-loop recursion (Nocedal 1980; LBFGS :326-358) with its
+// coefficient taken from the device scalar sc[0], the dot product just
+// reduced there, so the recursion needs no host round trip.
+//   FIRST:  alpha_cp = rho sq, kept in sc[1 + cp];  w = w - alpha_cp y_cp
+//   second: beta = alpha_cp - rho yr;               w = w + beta s_cp
+template <bool FIRST>
+__global__ void k_lb_twoloop(int n3, double* __restrict__ w, const double* __restrict__ v, double* sc, double rho,
+                             int cp) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (FIRST) {
+        const double alpha = rho * sc[0];
+        if (t == 0) sc[1 + cp] = alpha;
+        if (t < n3) w[t] = w[t] + (-alpha) * v[t];
+    } else {
+        double beta = rho * sc[0];
+        beta = sc[1 + cp] - beta;
+        if (t < n3) w[t] = w[t] + beta * v[t];
+    }
+}
+
+// w = -G (= f), optionally times a uniform diagonal d (the first direction
+// -G DIAG with DIAG = 1, :293-294); g0 = G kept for the gradient change
+__global__ void k_lb_negg(int n, const double* __restrict__ fx, const double* __restrict__ fy,
+                          const double* __restrict__ fz, double d, double* __restrict__ w) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double f[3] = {fx[i], fy[i], fz[i]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) w[(size_t)c * n + i] = (-(-f[c])) * d;
+}
+
+__global__ void k_lb_scale(int n3, double* __restrict__ w, double d) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n3) w[t] = d * w[t];
+}
+
+// G kept before the line search (W(I) = G(I), :370-371)
+__global__ void k_lb_keepg(int n, const double* __restrict__ fx, const double* __restrict__ fy,
+                           const double* __restrict__ fz, double* __restrict__ g0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    g0[i] = -fx[i];
+    g0[(size_t)n + i] = -fy[i];
+    g0[(size_t)2 * n + i] = -fz[i];
+}
+
+// trial point X = WA + stp S (MCSRCH :40)
+__global__ void k_lb_place(int n, const double* __restrict__ wa, const double* __restrict__ s, double stp,
+                           double* __restrict__ x, double* __restrict__ y, double* __restrict__ z) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] = wa[i] + stp * s[i];
+    y[i] = wa[(size_t)n + i] + stp * s[(size_t)n + i];
+    z[i] = wa[(size_t)2 * n + i] + stp * s[(size_t)2 * n + i];
+}
+
+// the accepted step and gradient change: S = stp S, Y = G - g0 (:391-393)
+__global__ void k_lb_pair(int n, const double* __restrict__ fx, const double* __restrict__ fy,
+                          const double* __restrict__ fz, const double* __restrict__ g0, double stp,
+                          double* __restrict__ s, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double f[3] = {fx[i], fy[i], fz[i]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const size_t k = (size_t)c * n + i;
+        s[k] = stp * s[k];
+        y[k] = (-f[c]) - g0[k];
+    }
+}
+
+}  // namespace mdff

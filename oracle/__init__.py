@@ -53,6 +53,7 @@ def lib():
                                     C.POINTER(abi.ParamGrad), ip]
         L.orc_step.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
         L.orc_opt_sastry.argtypes = [C.c_void_p, C.c_int, C.POINTER(abi.OptResult)]
+        L.orc_opt_lbfgs.argtypes = [C.c_void_p, C.c_int, C.c_double, C.POINTER(abi.OptResult)]
         L.orc_gr.argtypes = [C.c_void_p, C.c_double, C.c_double, dp, C.POINTER(C.c_int)]
         L.orc_rmc.argtypes = [C.c_void_p, C.POINTER(abi.RmcParams), dp, dp, C.c_longlong, dp,
                               C.POINTER(abi.RmcResult)]
@@ -202,6 +203,13 @@ class Oracle:
         src/opt.f90:452-849); the positions are left at the minimum."""
         r = abi.OptResult()
         lib().orc_opt_sastry(self._h, int(itmax), C.byref(r))
+        return r.as_dict()
+
+    def opt_lbfgs(self, itmax=10000, eps=1.0e-5):
+        """Structure optimisation by L-BFGS (lbfgs_driver, src/opt.f90:972-1194,
+        over LBFGS/MCSRCH/MCSTEP of src/lbfgs.f90)."""
+        r = abi.OptResult()
+        lib().orc_opt_lbfgs(self._h, int(itmax), float(eps), C.byref(r))
         return r.as_dict()
 
     def gr(self, cut, res):

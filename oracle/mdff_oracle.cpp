@@ -2149,9 +2149,342 @@ int orc_loss_grad(orc_sys* s, const double* fxt, const double* fyt, const double
     return loss_grad(s, fxt, fyt, fzt, taut, cF, cS, loss, g, iters);
 }
 
+// ---- L-BFGS ------------------------------------------------------------------
+// lbfgs_driver (src/opt.f90:972-1194) calling LBFGS (src/lbfgs.f90:243-456)
+// by reverse communication, as the reference runs it: X = (rx, ry, rz),
+// G = -(fx, fy, fz) packed component-major, F = u_tot, m = 5, DIAGCO false,
+// EPS = epsrel_lbfgs, XTOL = tiny(1.0_dp); the line search MCSRCH
+// (:655-957, FTOL 1e-4, MAXFEV 100 as LBFGS sets them; GTOL 0.9, STPMIN
+// 1e-20, STPMAX 1e20 from BLOCK DATA LB2, :536-540) with MCSTEP (:960-1186).
+// The work vector W keeps the reference's layout: W(1..N) gradient and
+// direction scratch, then rho (M), alpha (M), the M search steps and the M
+// gradient differences; the SAVEd locals live in LbRC.  Dot products are
+// DDOT's left-to-right sums.
+struct LbRC {
+    int iter = 0, nfun = 0, point = 0, ispt = 0, iypt = 0, info = 0, bound = 0, npt = 0, cp = 0, nfev = 0,
+        maxfev = 0;
+    double gnorm = 0, stp1 = 0, ftol = 0, stp = 0, ys = 0, yy = 0, xnorm = 0;
+    bool finish = false;
+    // MCSRCH's SAVEd state
+    int infoc = 0;
+    bool brackt = false, stage1 = false;
+    double dginit = 0, dgtest = 0, dgx = 0, dgy = 0, finit = 0, fx = 0, fy = 0, stx = 0, sty = 0, stmin = 0,
+           stmax = 0, width = 0, width1 = 0;
+};
+
+static double lb_ddot(int n, const double* a, const double* b) {
+    double t = 0.0;
+    for (int i = 0; i < n; ++i) t = t + a[i] * b[i];
+    return t;
+}
+
+static void lb_mcstep(double& stx, double& fx, double& dx, double& sty, double& fy, double& dy, double& stp,
+                      double fp, double dp, bool& brackt, double stpmin, double stpmax, int& info) {
+    info = 0;
+    if ((brackt && (stp <= std::min(stx, sty) || stp >= std::max(stx, sty))) || dx * (stp - stx) >= 0.0 ||
+        stpmax < stpmin)
+        return;
+    const double sgnd = dp * (dx / std::fabs(dx));
+    double stpf, stpc, stpq, theta, sc, gamma, p, q, r;
+    bool bound;
+    auto smax3 = [](double a, double b, double c) { return std::max(std::max(a, b), c); };
+    if (fp > fx) {   // a higher function value: the minimum is bracketed
+        info = 1;
+        bound = true;
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp;
+        sc = smax3(std::fabs(theta), std::fabs(dx), std::fabs(dp));
+        gamma = sc * std::sqrt((theta / sc) * (theta / sc) - (dx / sc) * (dp / sc));
+        if (stp < stx) gamma = -gamma;
+        p = (gamma - dx) + theta;
+        q = ((gamma - dx) + gamma) + dp;
+        r = p / q;
+        stpc = stx + r * (stp - stx);
+        stpq = stx + ((dx / ((fx - fp) / (stp - stx) + dx)) / 2) * (stp - stx);
+        stpf = std::fabs(stpc - stx) < std::fabs(stpq - stx) ? stpc : stpc + (stpq - stpc) / 2;
+        brackt = true;
+    } else if (sgnd < 0.0) {   // lower value, derivatives of opposite sign
+        info = 2;
+        bound = false;
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp;
+        sc = smax3(std::fabs(theta), std::fabs(dx), std::fabs(dp));
+        gamma = sc * std::sqrt((theta / sc) * (theta / sc) - (dx / sc) * (dp / sc));
+        if (stp > stx) gamma = -gamma;
+        p = (gamma - dp) + theta;
+        q = ((gamma - dp) + gamma) + dx;
+        r = p / q;
+        stpc = stp + r * (stx - stp);
+        stpq = stp + (dp / (dp - dx)) * (stx - stp);
+        stpf = std::fabs(stpc - stp) > std::fabs(stpq - stp) ? stpc : stpq;
+        brackt = true;
+    } else if (std::fabs(dp) < std::fabs(dx)) {   // same sign, derivative magnitude decreases
+        info = 3;
+        bound = true;
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp;
+        sc = smax3(std::fabs(theta), std::fabs(dx), std::fabs(dp));
+        gamma = sc * std::sqrt(std::max(0.0, (theta / sc) * (theta / sc) - (dx / sc) * (dp / sc)));
+        if (stp > stx) gamma = -gamma;
+        p = (gamma - dp) + theta;
+        q = (gamma + (dx - dp)) + gamma;
+        r = p / q;
+        if (r < 0.0 && gamma != 0.0) stpc = stp + r * (stx - stp);
+        else if (stp > stx) stpc = stpmax;
+        else stpc = stpmin;
+        stpq = stp + (dp / (dp - dx)) * (stx - stp);
+        if (brackt) stpf = std::fabs(stp - stpc) < std::fabs(stp - stpq) ? stpc : stpq;
+        else stpf = std::fabs(stp - stpc) > std::fabs(stp - stpq) ? stpc : stpq;
+    } else {   // same sign, derivative magnitude does not decrease
+        info = 4;
+        bound = false;
+        if (brackt) {
+            theta = 3 * (fp - fy) / (sty - stp) + dy + dp;
+            sc = smax3(std::fabs(theta), std::fabs(dy), std::fabs(dp));
+            gamma = sc * std::sqrt((theta / sc) * (theta / sc) - (dy / sc) * (dp / sc));
+            if (stp > sty) gamma = -gamma;
+            p = (gamma - dp) + theta;
+            q = ((gamma - dp) + gamma) + dy;
+            r = p / q;
+            stpc = stp + r * (sty - stp);
+            stpf = stpc;
+        } else {
+            stpf = stp > stx ? stpmax : stpmin;
+        }
+    }
+    if (fp > fx) {
+        sty = stp; fy = fp; dy = dp;
+    } else {
+        if (sgnd < 0.0) { sty = stx; fy = fx; dy = dx; }
+        stx = stp; fx = fp; dx = dp;
+    }
+    stpf = std::min(stpmax, stpf);
+    stpf = std::max(stpmin, stpf);
+    stp = stpf;
+    if (brackt && bound) {   // 0.66: a default-real constant in the reference
+        if (sty > stx) stp = std::min(stx + (double)0.66f * (sty - stx), stp);
+        else stp = std::max(stx + (double)0.66f * (sty - stx), stp);
+    }
+}
+
+// MCSRCH by reverse communication: info = -1 on return asks for F and G at X
+static void lb_mcsrch(LbRC& c, int n, double* x, double f, const double* g, const double* sdir, double& stp,
+                      double ftol, double xtol, int maxfev, int& info, int& nfev, double* wa) {
+    const double gtol = 0.9, stpmin = 1.0e-20, stpmax = 1.0e20, p5 = 0.5, p66 = 0.66, xtrapf = 4.0;
+    if (info != -1) {
+        c.infoc = 1;
+        if (n <= 0 || stp <= 0.0 || ftol < 0.0 || gtol < 0.0 || xtol < 0.0 || stpmin < 0.0 || stpmax < stpmin ||
+            maxfev <= 0)
+            return;
+        c.dginit = 0.0;
+        for (int j = 0; j < n; ++j) c.dginit = c.dginit + g[j] * sdir[j];
+        if (c.dginit >= 0.0) return;   // not a descent direction
+        c.brackt = false;
+        c.stage1 = true;
+        nfev = 0;
+        c.finit = f;
+        c.dgtest = ftol * c.dginit;
+        c.width = stpmax - stpmin;
+        c.width1 = c.width / p5;
+        for (int j = 0; j < n; ++j) wa[j] = x[j];
+        c.stx = 0.0; c.fx = c.finit; c.dgx = c.dginit;
+        c.sty = 0.0; c.fy = c.finit; c.dgy = c.dginit;
+    } else {
+        info = 0;
+        nfev = nfev + 1;
+        double dg = 0.0;
+        for (int j = 0; j < n; ++j) dg = dg + g[j] * sdir[j];
+        const double ftest1 = c.finit + stp * c.dgtest;
+        if ((c.brackt && (stp <= c.stmin || stp >= c.stmax)) || c.infoc == 0) info = 6;
+        if (stp == stpmax && f <= ftest1 && dg <= c.dgtest) info = 5;
+        if (stp == stpmin && (f > ftest1 || dg >= c.dgtest)) info = 4;
+        if (nfev >= maxfev) info = 3;
+        if (c.brackt && c.stmax - c.stmin <= xtol * c.stmax) info = 2;
+        if (f <= ftest1 && std::fabs(dg) <= gtol * (-c.dginit)) info = 1;
+        if (info != 0) return;
+        if (c.stage1 && f <= ftest1 && dg >= std::min(ftol, gtol) * c.dginit) c.stage1 = false;
+        if (c.stage1 && f <= c.fx && f > ftest1) {   // the modified function
+            double fm = f - stp * c.dgtest, fxm = c.fx - c.stx * c.dgtest, fym = c.fy - c.sty * c.dgtest;
+            double dgm = dg - c.dgtest, dgxm = c.dgx - c.dgtest, dgym = c.dgy - c.dgtest;
+            lb_mcstep(c.stx, fxm, dgxm, c.sty, fym, dgym, stp, fm, dgm, c.brackt, c.stmin, c.stmax, c.infoc);
+            c.fx = fxm + c.stx * c.dgtest;
+            c.fy = fym + c.sty * c.dgtest;
+            c.dgx = dgxm + c.dgtest;
+            c.dgy = dgym + c.dgtest;
+        } else {
+            lb_mcstep(c.stx, c.fx, c.dgx, c.sty, c.fy, c.dgy, stp, f, dg, c.brackt, c.stmin, c.stmax, c.infoc);
+        }
+        if (c.brackt) {
+            if (std::fabs(c.sty - c.stx) >= p66 * c.width1) stp = c.stx + p5 * (c.sty - c.stx);
+            c.width1 = c.width;
+            c.width = std::fabs(c.sty - c.stx);
+        }
+    }
+    // label 30: the next trial step
+    if (c.brackt) {
+        c.stmin = std::min(c.stx, c.sty);
+        c.stmax = std::max(c.stx, c.sty);
+    } else {
+        c.stmin = c.stx;
+        c.stmax = stp + xtrapf * (stp - c.stx);
+    }
+    stp = std::max(stp, stpmin);
+    stp = std::min(stp, stpmax);
+    if ((c.brackt && (stp <= c.stmin || stp >= c.stmax)) || nfev >= maxfev - 1 || c.infoc == 0 ||
+        (c.brackt && c.stmax - c.stmin <= xtol * c.stmax))
+        stp = c.stx;
+    for (int j = 0; j < n; ++j) x[j] = wa[j] + stp * sdir[j];
+    info = -1;
+}
+
+// LBFGS (DIAGCO false): iflag 0 starts, 1 re-enters after an evaluation;
+// on return 1 asks for F and G at X, 0 converged, -1 line search failed
+static void lb_lbfgs(LbRC& c, int n, int m, double* x, double f, double* g, double* diag, double eps, double xtol,
+                     double* w, int& iflag) {
+    // 1-based W(k) of the reference is w[k - 1]
+    bool search = false;
+    if (iflag == 1) {
+        search = true;   // label 172
+    } else {
+        c.iter = 0;
+        c.nfun = 1;
+        c.point = 0;
+        c.finish = false;
+        for (int i = 0; i < n; ++i) diag[i] = 1.0;
+        c.ispt = n + 2 * m;
+        c.iypt = c.ispt + n * m;
+        for (int i = 0; i < n; ++i) w[c.ispt + i] = -g[i] * diag[i];
+        c.gnorm = std::sqrt(lb_ddot(n, g, g));
+        c.stp1 = 1.0 / c.gnorm;
+        c.ftol = 1.0e-4;
+        c.maxfev = 100;
+    }
+    for (;;) {
+        if (!search) {   // label 80
+            c.iter = c.iter + 1;
+            c.info = 0;
+            c.bound = c.iter - 1;
+            if (c.iter != 1) {
+                if (c.iter > m) c.bound = m;
+                c.ys = lb_ddot(n, &w[c.iypt + c.npt], &w[c.ispt + c.npt]);
+                c.yy = lb_ddot(n, &w[c.iypt + c.npt], &w[c.iypt + c.npt]);
+                for (int i = 0; i < n; ++i) diag[i] = c.ys / c.yy;
+                c.cp = c.point;
+                if (c.point == 0) c.cp = m;
+                w[n + c.cp - 1] = 1.0 / c.ys;
+                for (int i = 0; i < n; ++i) w[i] = -g[i];
+                c.cp = c.point;
+                for (int i = 0; i < c.bound; ++i) {
+                    c.cp = c.cp - 1;
+                    if (c.cp == -1) c.cp = m - 1;
+                    const double sq = lb_ddot(n, &w[c.ispt + c.cp * n], w);
+                    const int inmc = n + m + c.cp;
+                    const int iycn = c.iypt + c.cp * n;
+                    w[inmc] = w[n + c.cp] * sq;
+                    const double a = -w[inmc];
+                    for (int j = 0; j < n; ++j) w[j] = w[j] + a * w[iycn + j];
+                }
+                for (int i = 0; i < n; ++i) w[i] = diag[i] * w[i];
+                for (int i = 0; i < c.bound; ++i) {
+                    const double yr = lb_ddot(n, &w[c.iypt + c.cp * n], w);
+                    double beta = w[n + c.cp] * yr;
+                    const int inmc = n + m + c.cp;
+                    beta = w[inmc] - beta;
+                    const int iscn = c.ispt + c.cp * n;
+                    for (int j = 0; j < n; ++j) w[j] = w[j] + beta * w[iscn + j];
+                    c.cp = c.cp + 1;
+                    if (c.cp == m) c.cp = 0;
+                }
+                for (int i = 0; i < n; ++i) w[c.ispt + c.point * n + i] = w[i];
+            }
+            // label 165
+            c.nfev = 0;
+            c.stp = 1.0;
+            if (c.iter == 1) c.stp = c.stp1;
+            for (int i = 0; i < n; ++i) w[i] = g[i];
+        }
+        search = false;
+        // label 172
+        lb_mcsrch(c, n, x, f, g, &w[c.ispt + c.point * n], c.stp, c.ftol, xtol, c.maxfev, c.info, c.nfev, diag);
+        if (c.info == -1) {
+            iflag = 1;
+            return;
+        }
+        if (c.info != 1) {
+            iflag = -1;
+            return;
+        }
+        c.nfun = c.nfun + c.nfev;
+        c.npt = c.point * n;
+        for (int i = 0; i < n; ++i) {
+            w[c.ispt + c.npt + i] = c.stp * w[c.ispt + c.npt + i];
+            w[c.iypt + c.npt + i] = g[i] - w[i];
+        }
+        c.point = c.point + 1;
+        if (c.point == m) c.point = 0;
+        c.gnorm = std::sqrt(lb_ddot(n, g, g));
+        c.xnorm = std::sqrt(lb_ddot(n, x, x));
+        c.xnorm = std::max(1.0, c.xnorm);
+        if (c.gnorm / c.xnorm <= eps) c.finish = true;
+        if (c.finish) {
+            iflag = 0;
+            return;
+        }
+    }
+}
+
+static int opt_lbfgs(orc_sys* s, int itmax, double eps, mdff_opt_result* R) {
+    const int natm = s->natm, n = 3 * natm, m = 5;
+    std::vector<double> X(n), G(n), DIAG(n), W((size_t)n * (2 * m + 1) + 2 * m);
+    const double xtol = 2.2250738585072014e-308;   // tiny(1.0_dp)
+    LbRC c;
+    int iflag = 0, icall = 0;
+    double phigrad = 0.0;
+    for (int ia = 0; ia < natm; ++ia) {
+        X[ia] = s->rx[ia];
+        X[natm + ia] = s->ry[ia];
+        X[2 * natm + ia] = s->rz[ia];
+    }
+    R->status = 1;
+    for (int its = 1; its <= itmax; ++its) {
+        engforce(s);
+        for (int ia = 0; ia < natm; ++ia) {
+            G[ia] = -s->fx[ia];
+            G[natm + ia] = -s->fy[ia];
+            G[2 * natm + ia] = -s->fz[ia];
+        }
+        const double F = opt_utot(s);
+        if (icall == 0) R->u_initial = F;
+        icall = icall + 1;
+        lb_lbfgs(c, n, m, X.data(), F, G.data(), DIAG.data(), eps, xtol, W.data(), iflag);
+        R->u_final = F;
+        R->iterations = c.iter;
+        R->nforce = icall;
+        if (iflag <= 0) {
+            R->phigrad = phigrad;
+            R->status = iflag == 0 ? 0 : 3;
+            R->info = iflag == 0 ? 0 : c.info;
+            return 0;
+        }
+        phigrad = 0.0;
+        for (int ia = 0; ia < natm; ++ia)
+            phigrad = phigrad + G[ia] * G[ia] + G[natm + ia] * G[natm + ia] + G[2 * natm + ia] * G[2 * natm + ia];
+        R->phigrad = phigrad;
+        if (its == itmax) break;   // the positions stay those of the last evaluation
+        for (int ia = 0; ia < natm; ++ia) {
+            s->rx[ia] = X[ia];
+            s->ry[ia] = X[natm + ia];
+            s->rz[ia] = X[2 * natm + ia];
+        }
+    }
+    return 0;
+}
+
 int orc_opt_sastry(orc_sys* s, int itmax, mdff_opt_result* r) {
     std::memset(r, 0, sizeof *r);
     return opt_sastry(s, itmax, r);
+}
+
+int orc_opt_lbfgs(orc_sys* s, int itmax, double eps, mdff_opt_result* r) {
+    std::memset(r, 0, sizeof *r);
+    return opt_lbfgs(s, itmax, eps, r);
 }
 
 int orc_engforce(orc_sys* s, double* fx, double* fy, double* fz, mdff_energies* e, double tau_nonb[9],

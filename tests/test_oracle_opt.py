@@ -19,3 +19,40 @@ def test_lj_crystal_relaxes_to_the_lattice():
     assert abs(r["u_final"] - perfect) < 1e-11 * abs(perfect)
     assert np.abs(o.engforce()["f"]).max() < 1e-4
     assert r["nforce"] > 2 * r["iterations"]
+
+
+def _jittered_lj():
+    s = systems.lj_argon()
+    perfect = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"]).engforce()["e"]["u_lj"]
+    pos = s["pos"] + np.random.default_rng(3).normal(0, 0.08, s["pos"].shape)
+    return s, pos, perfect
+
+
+def test_lbfgs_relaxes_to_the_lattice():
+    # optalgo = 'lbfgs' (lbfgs_driver, src/opt.f90:972-1194) with the default
+    # epsrel_lbfgs = 1e-5: the same minimum as sastry, in far fewer
+    # force evaluations
+    s, pos, perfect = _jittered_lj()
+    o = oracle.Oracle(s["params"], s["itype"], pos, s["cell"])
+    r = o.opt_lbfgs()
+    assert r["status"] == 0 and r["info"] == 0
+    assert abs(r["u_final"] - perfect) < 1e-10 * abs(perfect)
+    f = o.engforce()["f"]
+    gnorm = np.sqrt(np.sum(f * f))
+    xnorm = max(1.0, np.sqrt(np.sum(o.positions() ** 2)))
+    assert gnorm / xnorm <= 1e-5                      # the LBFGS termination test
+    cg = oracle.Oracle(s["params"], s["itype"], pos, s["cell"]).opt_sastry()
+    assert r["nforce"] < cg["nforce"] / 3
+    assert r["nforce"] >= r["iterations"] + 1
+
+
+def test_lbfgs_evaluation_budget_and_line_search_exit():
+    s, pos, _ = _jittered_lj()
+    o = oracle.Oracle(s["params"], s["itype"], pos, s["cell"])
+    r = o.opt_lbfgs(itmax=7)
+    assert r["status"] == 1 and r["nforce"] == 7
+    assert r["u_final"] < r["u_initial"]
+    # a tolerance below what rounding allows ends in MCSRCH's rounding exit
+    # (info 6) or its interval test (info 2), as the reference reports it
+    r = oracle.Oracle(s["params"], s["itype"], pos, s["cell"]).opt_lbfgs(eps=1e-14)
+    assert r["status"] == 3 and r["info"] in (2, 6)

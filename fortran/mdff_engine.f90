@@ -203,6 +203,15 @@ module mdff_engine
       type(mdff_opt_result_t), intent(out) :: res
     end function
 
+    ! optalgo = 'm1qn3' of opt_main: niter = nsim = 6000, epsg = epsrel_m1qn3
+    integer(c_int) function mdff_opt_m1qn3(ctx, niter, nsim, epsg, res) bind(C, name="mdff_opt_m1qn3")
+      import :: c_int, c_double, c_ptr, mdff_opt_result_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: niter, nsim
+      real(c_double), value :: epsg
+      type(mdff_opt_result_t), intent(out) :: res
+    end function
+
     ! optalgo = 'lbfgs' of opt_main: eps = epsrel_lbfgs
     integer(c_int) function mdff_opt_lbfgs(ctx, itmax, eps, res) bind(C, name="mdff_opt_lbfgs")
       import :: c_int, c_double, c_ptr, mdff_opt_result_t

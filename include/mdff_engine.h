@@ -212,7 +212,7 @@ typedef struct mdff_opt_result {
                            steps; lbfgs: MCSRCH returned info != 1, IFLAG = -1) */
     int    info;        /* lbfgs with status 3: MCSRCH's info (0 not a descent direction or bad
                            input, 2 interval below xtol, 3 maxfev reached, 4/5 at stpmin/stpmax,
-                           6 rounding errors); 0 otherwise */
+                           6 rounding errors), 0 otherwise; m1qn3: its omode; sastry: 0 */
 } mdff_opt_result;
 
 /* Distribution settings of efg_stat (the efgtag namelist, src/efg.f90:171-190):
@@ -357,6 +357,24 @@ int  mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out);
  * the L-BFGS iterations and the evaluations (nforce; the reference reports
  * this count as both iter and neng). */
 int  mdff_opt_lbfgs(mdff_ctx* ctx, int itmax, double eps, mdff_opt_result* out);
+
+/* Structure optimisation by M1QN3 (optalgo = 'm1qn3' of opt_main):
+ * m1qn3_driver (src/opt.f90:1203-1330) over M1QN3 3.3 (src/m1qn3.f90) in its
+ * configuration there -- diagonal initial scaling, cold start, m = 5 pairs,
+ * the euclidean scalar product, normtype 'dfn', dxmin = tiny(1.0_dp),
+ * df1 = 1, and the Wolfe line search mlis3 (rm1 1e-4, rm2 0.99) -- on
+ * X = (rx, ry, rz), G = -f, F = u_tot.  niter, nsim: the driver's 6000 and
+ * 6000; epsg: epsrel_m1qn3 (1e-5), the test |G| / |G_0| < epsg.  Every
+ * evaluation is one mdff_engforce on the lists of the starting
+ * configuration; after M1QN3 returns, one more evaluation at the returned
+ * point, as the driver's loop makes it, so the positions, forces, u_final
+ * and phigrad (|G|^2) on return belong together.  iterations: M1QN3's
+ * niter; nforce: all evaluations (the reference reports one less, its
+ * icall); info: M1QN3's omode; status 0 (omode 1), 1 (omode 4 or 5: niter
+ * or nsim reached), 2 (omode 2: zero gradient at the start), 3 (omode 6:
+ * dxmin or rounding in the line search, which the driver accepts with a
+ * warning; omode 7: not a descent direction or (y, s) <= 0). */
+int  mdff_opt_m1qn3(mdff_ctx* ctx, int niter, int nsim, double epsg, mdff_opt_result* out);
 
 /* EFG post-processing (efg_stat, src/efg.f90:2057-2440, and nmr_convention,
  * :2546-2650) on the device, over nconf configurations of the context's

@@ -69,6 +69,7 @@ def lib():
         L.mdff_measure_tensor.argtypes = [C.c_int, dp]
         L.mdff_opt_sastry.argtypes = [vp, C.c_int, C.POINTER(abi.OptResult)]
         L.mdff_opt_lbfgs.argtypes = [vp, C.c_int, C.c_double, C.POINTER(abi.OptResult)]
+        L.mdff_opt_m1qn3.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(abi.OptResult)]
         L.mdff_profile_detail.argtypes = [vp, dp, C.POINTER(C.c_longlong), dp]
         L.mdff_io_format.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(abi.FrameHeader), ip, dp, C.c_char_p,
                                      C.c_size_t, C.POINTER(C.c_size_t)]
@@ -251,13 +252,21 @@ class Engine:
         self._check(lib().mdff_opt_sastry(self._h, int(itmax), C.byref(r)))
         return r.as_dict()
 
-    def opt_lbfgs(self, itmax=10000, eps=1.0e-5):
+    def opt_lbfgs(self, itmax=10000, eps=abi.EPSREL_OPT):
         """Structure optimisation from the current positions by limited-memory
         BFGS (the reference's lbfgs_driver; eps is epsrel_lbfgs, itmax bounds
         the force evaluations); the engine's positions are left at the last
         evaluated point."""
         r = abi.OptResult()
         self._check(lib().mdff_opt_lbfgs(self._h, int(itmax), float(eps), C.byref(r)))
+        return r.as_dict()
+
+    def opt_m1qn3(self, niter=6000, nsim=6000, epsg=abi.EPSREL_OPT):
+        """Structure optimisation from the current positions by M1QN3 in
+        diagonal-initial-scaling mode (the reference's m1qn3_driver); the
+        positions are left at the returned point, evaluated there."""
+        r = abi.OptResult()
+        self._check(lib().mdff_opt_m1qn3(self._h, int(niter), int(nsim), float(epsg), C.byref(r)))
         return r.as_dict()
 
     def _efg_input(self, efg):

@@ -6,6 +6,7 @@ library.  Field meanings follow the reference's namelist tags
 (src/control.f90:128-160, src/field.f90:450-500, src/md.f90:109-132).
 """
 import ctypes as C
+import numpy as np
 
 NTYPE_MAX = 16
 TT_MAX_ORDER = 8
@@ -91,6 +92,11 @@ class Thermo(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# epsrel_lbfgs and epsrel_m1qn3 default to 1.0e-5 (src/opt.f90:139-140), a
+# default-real literal: its double value is that of the single-precision 1e-5
+EPSREL_OPT = float(np.float32(1.0e-5))
 
 
 class OptResult(C.Structure):

@@ -79,6 +79,10 @@ struct mdff_ctx {
     double* coef = nullptr;
     double *opt_xi = nullptr, *opt_g = nullptr, *opt_h = nullptr, *opt_r0 = nullptr;   // structure optimisation
     double *lb_s = nullptr, *lb_y = nullptr, *lb_w = nullptr, *lb_wa = nullptr, *lb_g0 = nullptr, *lb_sc = nullptr;
+    double *m1_d = nullptr, *m1_gg = nullptr, *m1_diag = nullptr, *m1_xn = nullptr, *m1_ybar = nullptr,
+           *m1_sbar = nullptr, *m1_sc = nullptr;
+    int* m1_flag = nullptr;          // [0] mlis3's precision test, [2..3] max |d| as 64 bits
+    int m1_indica = 0;               // mlis3's SAVEd indica, zero in a fresh process
     double *efgp_t = nullptr, *efgp_nmr = nullptr, *efgp_part = nullptr;   // EFG post-processing scratch
     int* efgp_hist = nullptr;
     size_t efgp_tcap = 0, efgp_ncap = 0, efgp_pcap = 0, efgp_hcap = 0;
@@ -1741,6 +1745,326 @@ int opt_lbfgs(mdff_ctx* ctx, int itmax, double eps, mdff_opt_result* R) {
     }
 }
 
+// ---- M1QN3 -------------------------------------------------------------------
+// m1qn3_driver (src/opt.f90:1203-1330) over M1QN3 3.3 (Gilbert & Lemarechal,
+// src/m1qn3.f90) as the driver configures it: diagonal initial scaling
+// (imode(1) = 0), cold start, ndz = 4n + 5(2n+1) so m = 5 (ybar, sbar)
+// pairs in core (mupdts), the euclidean scalar product with identity
+// changes of basis (euclid, ctonbe, ctcabe), normtype 'dfn', dxmin =
+// tiny(1.0_dp), df1 = 1; the line search mlis3 (:999-1316, Wolfe tests with
+// rm1 = 1e-4, rm2 = 0.99, safeguarded cubic ecube :1318-1382).  Direct calls
+// of engforce replace the reverse communication; after M1QN3 ends the
+// driver evaluates once more at the returned point (its loop body runs once
+// with reverse = -1), and so does this.  mlis3's SAVEd indica is not reset
+// between calls (its initialisation is commented out in the reference); it
+// lives in the context, zero at creation as the static variable is in a
+// fresh process.
+struct M1Eval {
+    int nevals = 0;
+    double f = 0.0;
+};
+
+int m1_eval(mdff_ctx* ctx, M1Eval& E) {
+    TRY(engforce_device(ctx));
+    E.nevals = E.nevals + 1;
+    E.f = opt_utot(ctx);
+    return MDFF_OK;
+}
+
+int m1_dot_gd(mdff_ctx* ctx, const double* d, double& out) {
+    double t[2];
+    TRY(lb_dots(ctx, lb_grad(ctx), lb_buf(d, ctx->n), lb_grad(ctx), lb_grad(ctx), 1, t));
+    out = t[0];
+    return MDFF_OK;
+}
+
+// ecube (src/m1qn3.f90:1318-1382): the minimiser of the cubic through
+// (t, f, fp) and (ta, fa, fpa), safeguarded into [tlower, tupper]
+void m1_ecube(double& t, double f, double fp, double ta, double fa, double fpa, double tlower, double tupper) {
+    const double z1 = fp + fpa - 3.0 * (fa - f) / (ta - t);
+    const double b = z1 + fp;
+    double discri;
+    bool have_root = false;
+    if (std::fabs(z1) <= 1.0) {
+        discri = z1 * z1 - fp * fpa;
+    } else {
+        discri = fp / z1;
+        discri = discri * fpa;
+        discri = z1 - discri;
+        if (z1 >= 0.0 && discri >= 0.0) {
+            discri = std::sqrt(z1) * std::sqrt(discri);
+            have_root = true;
+        } else if (z1 <= 0.0 && discri <= 0.0) {
+            discri = std::sqrt(-z1) * std::sqrt(-discri);
+            have_root = true;
+        } else {
+            discri = -1.0;
+        }
+    }
+    if (!have_root) {
+        if (discri < 0.0) {
+            if (fp < 0.0) t = tupper;
+            if (fp >= 0.0) t = tlower;
+            t = std::max(t, tlower);
+            t = std::min(t, tupper);
+            return;
+        }
+        discri = std::sqrt(discri);
+    }
+    if (t - ta < 0.0) discri = -discri;
+    const double sign = (t - ta) / std::fabs(t - ta);
+    if (b * sign > 0.0) {
+        t = t + fp * (ta - t) / (b + discri);
+    } else {
+        const double den = z1 + b + fpa, anum = b - discri;
+        if (std::fabs((t - ta) * anum) < (tupper - tlower) * std::fabs(den)) t = t + anum * (ta - t) / den;
+        else t = tupper;
+    }
+    t = std::max(t, tlower);
+    t = std::min(t, tupper);
+}
+
+// mlis3 along d from the current point (f, G on the device), fpn = d.G:
+// logic 0 serious step, 1 blocked on tmax, 4 nap > napmax, 6 dxmin or
+// rounding; on return the device positions are the last trial point and
+// f the value there (the reference's x and f)
+int m1_mlis3(mdff_ctx* ctx, M1Eval& E, const double* d, double fpn, double& t, double tmin, double tmax,
+             double amd, double amf, int& nap, int napmax, int& logic) {
+    const int n = ctx->n;
+    if (!(n > 0 && fpn < 0.0 && t > 0.0 && tmax > 0.0 && amf > 0.0 && amd > amf && amd < 1.0)) {
+        logic = 6;
+        return MDFF_OK;
+    }
+    const double tesf = amf * fpn, tesd = amd * fpn, barmin = 0.01, barmul = 5.0, barmax = 0.3;
+    // fg and the left point xn + tg d matter only to the reference's exits,
+    // which return the last trial point in x
+    double barr = barmin, td = 0.0, tg = 0.0, fn = E.f, ta = 0.0, fa = fn, fpa = fpn;
+    if (t < tmin) {
+        t = tmin;
+        if (t > tmax) tmin = tmax;
+    }
+    while (fn + t * fpn >= fn + 0.9 * t * fpn) t = 2.0 * t;
+    logic = 0;
+    if (t > tmax) {
+        t = tmax;
+        logic = 1;
+    }
+    CK(cudaMemcpyAsync(ctx->m1_xn, ctx->x, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->m1_xn + n, ctx->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->m1_xn + 2 * (size_t)n, ctx->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    k_lb_place<<<nb(n), 256, 0, ctx->st>>>(n, ctx->m1_xn, d, t, ctx->x, ctx->y, ctx->z);
+    for (;;) {   // label 100
+        nap = nap + 1;
+        if (nap > napmax) {
+            logic = 4;
+            return MDFF_OK;
+        }
+        TRY(m1_eval(ctx, E));
+        const double f = E.f;
+        double fp;
+        TRY(m1_dot_gd(ctx, d, fp));
+        const double ffn = f - fn;
+        int go;   // 320 accept, 350 new left end, 500 interpolate
+        if (ffn > t * tesf) {
+            td = t;
+            logic = 0;
+            go = 500;
+        } else if (fp > tesd) {
+            logic = 0;
+            go = 320;
+        } else {
+            go = logic == 0 ? 350 : 320;
+        }
+        if (go == 320) return MDFF_OK;
+        if (go == 350) {
+            tg = t;
+            if (td == 0.0) {   // extrapolation
+                const double taa = t, gauche = (1.0 + barmin) * t, droite = 10.0 * t;
+                m1_ecube(t, f, fp, ta, fa, fpa, gauche, droite);
+                ta = taa;
+                if (!(t < tmax)) {
+                    logic = 1;
+                    t = tmax;
+                }
+                go = 900;
+            } else {
+                go = 500;
+            }
+        }
+        if (go == 500) {   // interpolation
+            if (ctx->m1_indica <= 0) {
+                ta = t;
+                t = 0.9 * tg + 0.1 * td;
+            } else {
+                const double test = barr * (td - tg), gauche = tg + test, droite = td - test, taa = t;
+                m1_ecube(t, f, fp, ta, fa, fpa, gauche, droite);
+                ta = taa;
+                if (t > gauche && t < droite) barr = std::max(barmin, barr / barmul);
+                else barr = std::min(barmul * barr, barmax);
+            }
+        }
+        fa = f;   // label 900
+        fpa = fp;
+        ctx->m1_indica = 4;   // label 905: indica = indic, 4 after a simulation
+        bool again = td == 0.0;
+        if (!again && !(td - tg < tmin)) {
+            CK(cudaMemsetAsync(ctx->m1_flag, 0, sizeof(int), ctx->st));
+            k_m1_moves<<<nb(n), 256, 0, ctx->st>>>(n, ctx->m1_xn, d, t, ctx->x, ctx->y, ctx->z, ctx->m1_flag);
+            int h = 0;
+            CK(cudaMemcpyAsync(&h, ctx->m1_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            again = h != 0;
+        }
+        if (!again) {   // label 920: dxmin reached or rounding
+            logic = 6;
+            return MDFF_OK;
+        }
+        k_lb_place<<<nb(n), 256, 0, ctx->st>>>(n, ctx->m1_xn, d, t, ctx->x, ctx->y, ctx->z);   // label 950
+    }
+}
+
+// dd (src/m1qn3.f90:839-923): w = H w with H the inverse-BFGS matrix of the
+// stored pairs jmin..jmax (1-based, cyclic) over the diagonal diag
+void m1_dd(mdff_ctx* ctx, int m, int jmin, int jmax, double* w) {
+    const int n = ctx->n;
+    const size_t n3 = 3 * (size_t)n;
+    const int nb3 = (int)((n3 + 255) / 256);
+    int jfin = jmax;
+    if (jfin < jmin) jfin = jmax + m;
+    for (int j = jfin; j >= jmin; --j) {
+        const int jp = (j > m ? j - m : j) - 1;
+        k_lb_dots<1><<<nb(n), 256, 0, ctx->st>>>(n, lb_buf(w, n), lb_buf(ctx->m1_sbar + jp * n3, n), lb_buf(w, n),
+                                                  lb_buf(w, n), ctx->part.buf);
+        launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->m1_sc, 0);
+        k_lb_twoloop<true><<<nb3, 256, 0, ctx->st>>>((int)n3, w, ctx->m1_ybar + jp * n3, ctx->m1_sc, 1.0, jp);
+    }
+    k_m1_mul<<<nb3, 256, 0, ctx->st>>>((int)n3, w, ctx->m1_diag);
+    for (int j = jmin; j <= jfin; ++j) {
+        const int jp = (j > m ? j - m : j) - 1;
+        k_lb_dots<1><<<nb(n), 256, 0, ctx->st>>>(n, lb_buf(w, n), lb_buf(ctx->m1_ybar + jp * n3, n), lb_buf(w, n),
+                                                  lb_buf(w, n), ctx->part.buf);
+        launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->m1_sc, 0);
+        k_lb_twoloop<false><<<nb3, 256, 0, ctx->st>>>((int)n3, w, ctx->m1_sbar + jp * n3, ctx->m1_sc, 1.0, jp);
+    }
+}
+
+// m1qn3a (src/m1qn3.f90:371-837) from the evaluated start: omode as there
+// (1 converged, 2 zero gradient, 4 niter, 5 nsim, 6 dxmin or rounding in the
+// line search, 7 not a descent direction or ys <= 0), it = its iterations
+int m1_run(mdff_ctx* ctx, M1Eval& E, int niter, int nsim, double epsg, int& omode, int& it) {
+    const int n = ctx->n, m = 5;
+    const size_t n3 = 3 * (size_t)n;
+    const int nb3 = (int)((n3 + 255) / 256);
+    const double dxmin = 2.2250738585072014e-308, df1 = 1.0, rm1 = 1.0e-4, rm2 = 0.99, rmin = 1.0e-20;
+    const double tmax = 1.0e20;
+    double t[2], ps, hp0;
+    int isim = 1;
+    it = 0;
+    if (epsg >= 1.0) { omode = 1; return MDFF_OK; }
+    TRY(lb_dots(ctx, lb_grad(ctx), lb_grad(ctx), lb_grad(ctx), lb_grad(ctx), 1, t));
+    const double gnorm = std::sqrt(t[0]), gnorms = gnorm;
+    if (gnorms < rmin) { omode = 2; return MDFF_OK; }
+    int jmin = 1, jmax = 0;
+    const double precos = 2.0 * df1 / (gnorm * gnorm);   // Fletcher's scaling of the first direction
+    k_m1_start<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, precos, ctx->m1_d, ctx->m1_diag);
+    TRY(m1_dot_gd(ctx, ctx->m1_d, hp0));
+    if (hp0 >= 0.0) { omode = 7; return MDFF_OK; }
+    unsigned long long* dmax_bits = reinterpret_cast<unsigned long long*>(ctx->m1_flag + 2);
+    for (;;) {   // label 100
+        it = it + 1;
+        k_lb_keepg<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->m1_gg);
+        CK(cudaMemsetAsync(dmax_bits, 0, 8, ctx->st));
+        k_m1_absmax<<<592, 256, 0, ctx->st>>>((int)n3, ctx->m1_d, dmax_bits);
+        unsigned long long bits = 0;
+        CK(cudaMemcpyAsync(&bits, dmax_bits, 8, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        double dmax;
+        std::memcpy(&dmax, &bits, 8);
+        const double tmin = dxmin / dmax;
+        double tt = 1.0;
+        int moderl = 0;
+        TRY(m1_mlis3(ctx, E, ctx->m1_d, hp0, tt, tmin, tmax, rm2, rm1, isim, nsim, moderl));
+        bool skip_update = false;
+        if (moderl != 0) {
+            if (moderl < 0) { omode = moderl; return MDFF_OK; }
+            if (moderl == 1) skip_update = true;   // blocked on tmax
+            else if (moderl == 4) { omode = 5; return MDFF_OK; }
+            else if (moderl == 5) { omode = 0; return MDFF_OK; }
+            else if (moderl == 6) { omode = 6; return MDFF_OK; }
+        }
+        if (!skip_update) {
+            jmax = jmax + 1;
+            if (jmax > m) jmax = jmax - m;
+            if (it > m) {   // cold start
+                jmin = jmin + 1;
+                if (jmin > m) jmin = jmin - m;
+            }
+            const size_t jc = (size_t)(jmax - 1) * n3;
+            double* sb = ctx->m1_sbar + jc;
+            double* yb = ctx->m1_ybar + jc;
+            k_m1_pair<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, ctx->m1_gg, ctx->m1_d, tt, sb, yb);
+            TRY(lb_dots(ctx, lb_buf(yb, n), lb_buf(sb, n), lb_buf(yb, n), lb_buf(yb, n), 1, t));
+            const double ys = t[0];
+            if (ys <= 0.0) { omode = 7; return MDFF_OK; }
+            double d1 = std::sqrt(1.0 / ys);
+            k_lb_scale<<<nb3, 256, 0, ctx->st>>>((int)n3, sb, d1);
+            k_lb_scale<<<nb3, 256, 0, ctx->st>>>((int)n3, yb, d1);
+            // the diagonal scaled to Rayleigh's ellipsoid, then its BFGS update
+            k_m1_diagsum<0><<<nb(n), 256, 0, ctx->st>>>(n, ctx->m1_diag, yb, ctx->part.buf);
+            TRY(opt_sum(ctx, 1, t));
+            d1 = 1.0 / t[0];
+            k_lb_scale<<<nb3, 256, 0, ctx->st>>>((int)n3, ctx->m1_diag, d1);
+            k_m1_diagsum<1><<<nb(n), 256, 0, ctx->st>>>(n, ctx->m1_diag, sb, ctx->part.buf);
+            TRY(opt_sum(ctx, 1, t));
+            k_m1_diagupd<<<nb3, 256, 0, ctx->st>>>((int)n3, ctx->m1_diag, yb, sb, t[0], rmin);
+        }
+        TRY(lb_dots(ctx, lb_grad(ctx), lb_grad(ctx), lb_grad(ctx), lb_grad(ctx), 1, t));
+        ps = t[0];
+        const double eps1 = std::sqrt(ps) / gnorms;
+        if (eps1 < epsg) { omode = 1; return MDFF_OK; }
+        if (it == niter) { omode = 4; return MDFF_OK; }
+        if (isim > nsim) { omode = 5; return MDFF_OK; }
+        k_lb_negg<<<nb(n), 256, 0, ctx->st>>>(n, ctx->fx, ctx->fy, ctx->fz, 1.0, ctx->m1_d);
+        m1_dd(ctx, m, jmin, jmax, ctx->m1_d);
+        TRY(check_launch(ctx, "m1qn3 direction"));
+        TRY(m1_dot_gd(ctx, ctx->m1_d, hp0));
+        if (hp0 >= 0.0) { omode = 7; return MDFF_OK; }
+    }
+}
+
+int opt_m1qn3(mdff_ctx* ctx, int niter, int nsim, double epsg, mdff_opt_result* R) {
+    const int m = 5;
+    const size_t n3 = 3 * (size_t)ctx->n;
+    if (!ctx->m1_d) {
+        TRY(dalloc(ctx, &ctx->m1_d, n3));
+        TRY(dalloc(ctx, &ctx->m1_gg, n3));
+        TRY(dalloc(ctx, &ctx->m1_diag, n3));
+        TRY(dalloc(ctx, &ctx->m1_xn, n3));
+        TRY(dalloc(ctx, &ctx->m1_ybar, m * n3));
+        TRY(dalloc(ctx, &ctx->m1_sbar, m * n3));
+        TRY(dalloc(ctx, &ctx->m1_sc, 1 + m));
+        double* fl = nullptr;
+        TRY(dalloc(ctx, &fl, 2));
+        ctx->m1_flag = reinterpret_cast<int*>(fl);
+    }
+    M1Eval E;
+    TRY(m1_eval(ctx, E));
+    R->u_initial = E.f;
+    int omode = 0, it = 0;
+    TRY(m1_run(ctx, E, niter, nsim, epsg, omode, it));
+    // the driver's last pass: one more evaluation at the returned point
+    TRY(m1_eval(ctx, E));
+    double t[2];
+    TRY(lb_dots(ctx, lb_grad(ctx), lb_grad(ctx), lb_grad(ctx), lb_grad(ctx), 1, t));
+    R->u_final = E.f;
+    R->phigrad = t[0];
+    R->iterations = it;
+    R->nforce = E.nevals;
+    R->info = omode;
+    R->status = omode == 1 ? 0 : (omode == 4 || omode == 5) ? 1 : omode == 2 ? 2 : 3;
+    return MDFF_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1935,6 +2259,15 @@ int mdff_opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* out) {
     cudaSetDevice(ctx->p.device);
     std::memset(out, 0, sizeof *out);
     return opt_sastry(ctx, itmax, out);
+}
+
+int mdff_opt_m1qn3(mdff_ctx* ctx, int niter, int nsim, double epsg, mdff_opt_result* out) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!out || niter < 1 || nsim < 1 || !(epsg > 0.0))
+        return fail(ctx, MDFF_E_ARG, "mdff_opt_m1qn3: out must be given, niter >= 1, nsim >= 1 and epsg > 0");
+    cudaSetDevice(ctx->p.device);
+    std::memset(out, 0, sizeof *out);
+    return opt_m1qn3(ctx, niter, nsim, epsg, out);
 }
 
 int mdff_opt_lbfgs(mdff_ctx* ctx, int itmax, double eps, mdff_opt_result* out) {

@@ -207,3 +207,101 @@ __global__ void k_lb_pair(int n, const double* __restrict__ fx, const double* __
 }
 
 }  // namespace mdff
+
+namespace mdff {
+
+// ---- M1QN3 in diagonal-initial-scaling mode (m1qn3_driver,
+// src/opt.f90:1203-1330, over m1qn3a/dd/mlis3 of src/m1qn3.f90) ------------
+
+// d = -G precos = f precos (the cold start's Fletcher scaling, :477-481)
+__global__ void k_m1_start(int n, const double* __restrict__ fx, const double* __restrict__ fy,
+                           const double* __restrict__ fz, double precos, double* __restrict__ d,
+                           double* __restrict__ diag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double f[3] = {fx[i], fy[i], fz[i]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        d[(size_t)c * n + i] = (-(-f[c])) * precos;
+        diag[(size_t)c * n + i] = 1.0;
+    }
+}
+
+// max_i |d_i| (tmin = dxmin / max |d_i|, :522-526): non-negative doubles
+// order as their bit patterns, so an integer atomicMax is exact; *out must
+// be zero before the launch
+__global__ void k_m1_absmax(int n3, const double* __restrict__ d, unsigned long long* out) {
+    double m = 0.0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n3; t += gridDim.x * blockDim.x) m = fmax(m, fabs(d[t]));
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// the pair of the accepted step: sbar = t d, ybar = G - gg (:637-640)
+__global__ void k_m1_pair(int n, const double* __restrict__ fx, const double* __restrict__ fy,
+                          const double* __restrict__ fz, const double* __restrict__ gg, const double* __restrict__ d,
+                          double t, double* __restrict__ sbar, double* __restrict__ ybar) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double f[3] = {fx[i], fy[i], fz[i]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const size_t k = (size_t)c * n + i;
+        sbar[k] = t * d[k];
+        ybar[k] = (-f[c]) - gg[k];
+    }
+}
+
+// MODE 0: sum diag y^2 (:667-670); MODE 1: sum s^2 / diag (:677-680)
+template <int MODE>
+__global__ void k_m1_diagsum(int n, const double* __restrict__ diag, const double* __restrict__ v, double* part) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[1] = {0.0};
+    if (i < n) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const size_t k = (size_t)c * n + i;
+            if (MODE == 0) acc[0] = acc[0] + diag[k] * v[k] * v[k];
+            else acc[0] = acc[0] + v[k] * v[k] / diag[k];
+        }
+    }
+    block_partials<1>(acc, part);
+}
+
+// the diagonal's BFGS update (:681-687): diag = 1 / (1/diag + y^2 - (s/diag)^2 / den),
+// rmin where that is not positive
+__global__ void k_m1_diagupd(int n3, double* __restrict__ diag, const double* __restrict__ y,
+                             const double* __restrict__ s, double den, double rmin) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    const double q = s[t] / diag[t];
+    double v = 1.0 / (1.0 / diag[t] + y[t] * y[t] - (q * q) / den);
+    if (v <= 0.0) v = rmin;
+    diag[t] = v;
+}
+
+// w = w diag (dd's diagonal preconditioning, :895-899)
+__global__ void k_m1_mul(int n3, double* __restrict__ w, const double* __restrict__ diag) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n3) w[t] = w[t] * diag[t];
+}
+
+// mlis3's machine-precision test (:1270-1274): is xn + t d different from
+// both xn and the last trial x in some component?  *flag set to 1 if so.
+__global__ void k_m1_moves(int n, const double* __restrict__ xn, const double* __restrict__ d, double t,
+                           const double* __restrict__ x, const double* __restrict__ y,
+                           const double* __restrict__ z, int* flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* cur[3] = {x, y, z};
+    bool moves = false;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const size_t k = (size_t)c * n + i;
+        const double zz = xn[k] + t * d[k];
+        moves = moves || (zz != xn[k] && zz != cur[c][i]);
+    }
+    if (moves) *flag = 1;
+}
+
+}  // namespace mdff

@@ -54,6 +54,7 @@ def lib():
         L.orc_step.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.POINTER(abi.Thermo)]
         L.orc_opt_sastry.argtypes = [C.c_void_p, C.c_int, C.POINTER(abi.OptResult)]
         L.orc_opt_lbfgs.argtypes = [C.c_void_p, C.c_int, C.c_double, C.POINTER(abi.OptResult)]
+        L.orc_opt_m1qn3.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(abi.OptResult)]
         L.orc_gr.argtypes = [C.c_void_p, C.c_double, C.c_double, dp, C.POINTER(C.c_int)]
         L.orc_rmc.argtypes = [C.c_void_p, C.POINTER(abi.RmcParams), dp, dp, C.c_longlong, dp,
                               C.POINTER(abi.RmcResult)]
@@ -205,11 +206,18 @@ class Oracle:
         lib().orc_opt_sastry(self._h, int(itmax), C.byref(r))
         return r.as_dict()
 
-    def opt_lbfgs(self, itmax=10000, eps=1.0e-5):
+    def opt_lbfgs(self, itmax=10000, eps=abi.EPSREL_OPT):
         """Structure optimisation by L-BFGS (lbfgs_driver, src/opt.f90:972-1194,
         over LBFGS/MCSRCH/MCSTEP of src/lbfgs.f90)."""
         r = abi.OptResult()
         lib().orc_opt_lbfgs(self._h, int(itmax), float(eps), C.byref(r))
+        return r.as_dict()
+
+    def opt_m1qn3(self, niter=6000, nsim=6000, epsg=abi.EPSREL_OPT):
+        """Structure optimisation by M1QN3 (m1qn3_driver, src/opt.f90:1203-1330,
+        over m1qn3a/dd/mlis3/ecube of src/m1qn3.f90)."""
+        r = abi.OptResult()
+        lib().orc_opt_m1qn3(self._h, int(niter), int(nsim), float(epsg), C.byref(r))
         return r.as_dict()
 
     def gr(self, cut, res):

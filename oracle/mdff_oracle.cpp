@@ -183,6 +183,7 @@ struct orc_sys {
     Cell cell;
     int natm = 0;
     int ntype = 0;
+    int m1_indica = 0;   // mlis3's SAVEd indica (src/m1qn3.f90:1040-1041), zero in a fresh process
     std::vector<int> itype;          // 0-based
     std::vector<double> rx, ry, rz, vx, vy, vz, fx, fy, fz;
     std::vector<double> massia, qia, poldia, invpoldia;
@@ -2477,9 +2478,473 @@ static int opt_lbfgs(orc_sys* s, int itmax, double eps, mdff_opt_result* R) {
     return 0;
 }
 
+// ---- M1QN3 -------------------------------------------------------------------
+// m1qn3_driver (src/opt.f90:1203-1330) over M1QN3 3.3 (src/m1qn3.f90:90-1382)
+// by reverse communication, labels as goto: m1qn3 (argument checks, mupdts,
+// the split of dz), m1qn3a (:371-837), dd (:839-923), mlis3 (:999-1316),
+// ecube (:1318-1382), in the driver's configuration (DIS mode, cold start,
+// ndz = 4n + 5(2n+1), euclid, identity ctonb/ctcab, normtype 'dfn',
+// dxmin = tiny(1.0_dp), df1 = 1, impres 0).  The SAVEd locals live in M1RC;
+// mlis3's indica, never reset by the reference, lives in the system
+// (zero for a fresh one, as a static variable in a fresh process).
+struct M1RC {
+    int reentry = 0, m = 0;
+    int id = 0, igg = 0, idiag = 0, iaux = 0, ialpha = 0, iybar = 0, isbar = 0;   // 0-based offsets into dz
+    // m1qn3a
+    bool sscale = false, cold = true, warm = false, skip_update = false;
+    int itmax = 0, moderl = 0, isim = 0, jcour = 0;
+    double d1 = 0, t = 0, tmin = 0, tmax = 0, gnorm = 0, gnorms = 0, eps1 = 0, ff = 0, precos = 0, ys = 0, den = 0,
+           ps = 0, hp0 = 0;
+    // mlis3
+    int indicd = 0;
+    double tesf = 0, tesd = 0, tg = 0, fg = 0, fpg = 0, td = 0, ta = 0, fa = 0, fpa = 0, fn = 0, fp = 0, ffn = 0,
+           fd = 0, fpd = 0, barmin = 0, barmul = 0, barmax = 0, barr = 0, gauche = 0, droite = 0, taa = 0;
+};
+
+static double m1o_prosca(int n, const double* x, const double* y) {   // euclid
+    double ps = 0.0;
+    for (int i = 0; i < n; ++i) ps = ps + x[i] * y[i];
+    return ps;
+}
+
+static void m1o_ecube(double& t, double f, double fp, double ta, double fa, double fpa, double tlower,
+                      double tupper) {
+    double z1, b, discri, sign, den, anum;
+    z1 = fp + fpa - 3.0 * (fa - f) / (ta - t);
+    b = z1 + fp;
+    if (std::fabs(z1) <= 1.0) {
+        discri = z1 * z1 - fp * fpa;
+    } else {
+        discri = fp / z1;
+        discri = discri * fpa;
+        discri = z1 - discri;
+        if (z1 >= 0.0 && discri >= 0.0) {
+            discri = std::sqrt(z1) * std::sqrt(discri);
+            goto L120;
+        }
+        if (z1 <= 0.0 && discri <= 0.0) {
+            discri = std::sqrt(-z1) * std::sqrt(-discri);
+            goto L120;
+        }
+        discri = -1.0;
+    }
+    if (discri < 0.0) {
+        if (fp < 0.0) t = tupper;
+        if (fp >= 0.0) t = tlower;
+        goto L900;
+    }
+    discri = std::sqrt(discri);
+L120:
+    if (t - ta < 0.0) discri = -discri;
+    sign = (t - ta) / std::fabs(t - ta);
+    if (b * sign > 0.0) {
+        t = t + fp * (ta - t) / (b + discri);
+    } else {
+        den = z1 + b + fpa;
+        anum = b - discri;
+        if (std::fabs((t - ta) * anum) < (tupper - tlower) * std::fabs(den)) t = t + anum * (ta - t) / den;
+        else t = tupper;
+    }
+L900:
+    t = std::max(t, tlower);
+    t = std::min(t, tupper);
+}
+
+static void m1o_mlis3(M1RC& c, int n, double* x, double& f, double fpn, double& t, double& tmin, double tmax,
+                      const double* d, const double* g, double amd, double amf, int& logic, int& nap, int napmax,
+                      double* xn, int& reentry, int& indic, int& indica) {
+    if (reentry == 2) goto L9999;
+    if (n > 0 && fpn < 0.0 && t > 0.0 && tmax > 0.0 && amf > 0.0 && amd > amf && amd < 1.0) goto L5;
+    logic = 6;
+    goto L999;
+L5:
+    c.tesf = amf * fpn;
+    c.tesd = amd * fpn;
+    c.barmin = 0.01;
+    c.barmul = 5.0;
+    c.barmax = 0.3;
+    c.barr = c.barmin;
+    c.td = 0.0;
+    c.tg = 0.0;
+    c.fn = f;
+    c.fg = c.fn;
+    c.fpg = fpn;
+    c.ta = 0.0;
+    c.fa = c.fn;
+    c.fpa = fpn;
+    if (t < tmin) {
+        t = tmin;
+        if (t > tmax) tmin = tmax;
+    }
+    while (c.fn + t * fpn >= c.fn + 0.9 * t * fpn) t = 2.0 * t;
+    logic = 0;
+    if (t > tmax) {
+        t = tmax;
+        logic = 1;
+    }
+    for (int i = 0; i < n; ++i) {
+        xn[i] = x[i];
+        x[i] = xn[i] + t * d[i];
+    }
+L100:
+    nap = nap + 1;
+    if (nap > napmax) {
+        logic = 4;
+        c.fn = c.fg;
+        for (int i = 0; i < n; ++i) xn[i] = xn[i] + c.tg * d[i];
+        goto L999;
+    }
+    indic = 4;
+    reentry = 2;
+    return;
+L9999:
+    if (indic == 0) {
+        logic = 5;
+        c.fn = f;
+        for (int i = 0; i < n; ++i) xn[i] = x[i];
+        goto L999;
+    }
+    if (indic < 0) {
+        c.td = t;
+        c.indicd = indic;
+        logic = 0;
+        t = c.tg + 0.1 * (c.td - c.tg);
+        goto L905;
+    }
+    c.fp = m1o_prosca(n, d, g);
+    c.ffn = f - c.fn;   // first Wolfe test
+    if (c.ffn > t * c.tesf) {
+        c.td = t;
+        c.fd = f;
+        c.fpd = c.fp;
+        c.indicd = indic;
+        logic = 0;
+        goto L500;
+    }
+    if (c.fp > c.tesd) {   // second Wolfe test
+        logic = 0;
+        goto L320;
+    }
+    if (logic == 0) goto L350;
+L320:
+    c.fn = f;
+    for (int i = 0; i < n; ++i) xn[i] = x[i];
+    goto L999;
+L350:
+    c.tg = t;
+    c.fg = f;
+    c.fpg = c.fp;
+    if (c.td != 0.0) goto L500;
+    c.taa = t;   // extrapolation
+    c.gauche = (1.0 + c.barmin) * t;
+    c.droite = 10.0 * t;
+    m1o_ecube(t, f, c.fp, c.ta, c.fa, c.fpa, c.gauche, c.droite);
+    c.ta = c.taa;
+    if (t < tmax) goto L900;
+    logic = 1;
+    t = tmax;
+    goto L900;
+L500:   // interpolation
+    if (indica <= 0) {
+        c.ta = t;
+        t = 0.9 * c.tg + 0.1 * c.td;
+        goto L900;
+    }
+    {
+        const double test = c.barr * (c.td - c.tg);
+        c.gauche = c.tg + test;
+        c.droite = c.td - test;
+    }
+    c.taa = t;
+    m1o_ecube(t, f, c.fp, c.ta, c.fa, c.fpa, c.gauche, c.droite);
+    c.ta = c.taa;
+    if (t > c.gauche && t < c.droite) c.barr = std::max(c.barmin, c.barr / c.barmul);
+    else c.barr = std::min(c.barmul * c.barr, c.barmax);
+L900:
+    c.fa = f;
+    c.fpa = c.fp;
+L905:
+    indica = indic;
+    if (c.td == 0.0) goto L950;
+    if (c.td - c.tg < tmin) goto L920;
+    for (int i = 0; i < n; ++i) {
+        const double z = xn[i] + t * d[i];
+        if (z != xn[i] && z != x[i]) goto L950;
+    }
+L920:
+    logic = 6;
+    if (c.indicd < 0) logic = c.indicd;
+    if (c.tg == 0.0) goto L999;
+    c.fn = c.fg;
+    for (int i = 0; i < n; ++i) xn[i] = xn[i] + c.tg * d[i];
+    goto L999;
+L950:
+    for (int i = 0; i < n; ++i) x[i] = xn[i] + t * d[i];
+    goto L100;
+L999:
+    reentry = 0;
+}
+
+// dd with jmin, jmax 1-based and the pairs ybar(., j), sbar(., j) column j - 1
+static void m1o_dd(int n, int nm, double* depl, double* aux, int jmin, int jmax, const double* diag, double* alpha,
+                   const double* ybar, const double* sbar) {
+    int jfin = jmax;
+    if (jfin < jmin) jfin = jmax + nm;
+    for (int j = jfin; j >= jmin; --j) {
+        int jp = j;
+        if (jp > nm) jp = jp - nm;
+        const double r = m1o_prosca(n, depl, &sbar[(size_t)(jp - 1) * n]);
+        alpha[jp - 1] = r;
+        for (int i = 0; i < n; ++i) depl[i] = depl[i] - r * ybar[(size_t)(jp - 1) * n + i];
+    }
+    for (int i = 0; i < n; ++i) aux[i] = depl[i];
+    for (int i = 0; i < n; ++i) aux[i] = aux[i] * diag[i];
+    for (int i = 0; i < n; ++i) depl[i] = aux[i];
+    for (int j = jmin; j <= jfin; ++j) {
+        int jp = j;
+        if (jp > nm) jp = jp - nm;
+        const double ps = m1o_prosca(n, depl, &ybar[(size_t)(jp - 1) * n]);
+        const double r = alpha[jp - 1] - ps;
+        for (int i = 0; i < n; ++i) depl[i] = depl[i] + r * sbar[(size_t)(jp - 1) * n + i];
+    }
+}
+
+static void m1o_m1qn3a(M1RC& c, int n, double* x, double& f, double* g, double dxmin, double df1, double& epsg,
+                       int& omode, int& niter, int& nsim, int m, int& jmin, int& jmax, double* d, double* gg,
+                       double* diag, double* aux, double* alpha, double* ybar, double* sbar, int& reverse,
+                       int& reentry, int& indic, int& indica) {
+    const double rm1 = 0.0001, rm2 = 0.99, rmin = 1.0e-20;
+    if (reentry == 2) goto L9999;
+    c.sscale = false;   // imode(1) = 0
+    c.warm = false;     // imode(2) = 0
+    c.cold = !c.warm;
+    c.skip_update = false;
+    c.itmax = niter;
+    niter = 0;
+    c.isim = 1;
+    c.eps1 = 1.0;
+    c.ps = m1o_prosca(n, g, g);
+    c.gnorm = std::sqrt(c.ps);
+    c.gnorms = c.gnorm;   // 'dfn'
+    if (c.gnorms < rmin) {
+        omode = 2;
+        goto L1000;
+    }
+    if (c.cold) {
+        jmin = 1;
+        jmax = 0;
+    }
+    c.jcour = jmax;
+    c.precos = 2.0 * df1 / (c.gnorm * c.gnorm);
+    for (int i = 0; i < n; ++i) {
+        d[i] = -g[i] * c.precos;
+        diag[i] = 1.0;
+    }
+    c.tmax = 1.0e20;
+    c.hp0 = m1o_prosca(n, d, g);
+    if (c.hp0 >= 0.0) {
+        omode = 7;
+        goto L1000;
+    }
+L100:
+    niter = niter + 1;
+    for (int i = 0; i < n; ++i) gg[i] = g[i];
+    c.ff = f;
+    c.tmin = 0.0;
+    for (int i = 0; i < n; ++i) c.tmin = std::max(c.tmin, std::fabs(d[i]));
+    c.tmin = dxmin / c.tmin;
+    c.t = 1.0;
+    c.d1 = c.hp0;
+L9999:
+    m1o_mlis3(c, n, x, f, c.d1, c.t, c.tmin, c.tmax, d, g, rm2, rm1, c.moderl, c.isim, nsim, aux, reentry, indic,
+              indica);
+    if (reentry > 0) return;
+    if (c.moderl != 0) {
+        if (c.moderl < 0) {
+            omode = c.moderl;
+            goto L1000;
+        } else if (c.moderl == 1) {
+            c.skip_update = true;
+        } else if (c.moderl == 4) {
+            omode = 5;
+            goto L1000;
+        } else if (c.moderl == 5) {
+            omode = 0;
+            goto L1000;
+        } else if (c.moderl == 6) {
+            omode = 6;
+            goto L1000;
+        }
+    } else {
+        c.skip_update = false;
+    }
+    if (c.skip_update) {
+    } else if (m > 0) {
+        jmax = jmax + 1;
+        if (jmax > m) jmax = jmax - m;
+        if ((c.cold && niter > m) || (c.warm && jmin == jmax)) {
+            jmin = jmin + 1;
+            if (jmin > m) jmin = jmin - m;
+        }
+        c.jcour = jmax;
+        double* sb = &sbar[(size_t)(c.jcour - 1) * n];
+        double* yb = &ybar[(size_t)(c.jcour - 1) * n];
+        for (int i = 0; i < n; ++i) {
+            sb[i] = c.t * d[i];
+            yb[i] = g[i] - gg[i];
+        }
+        c.ys = m1o_prosca(n, yb, sb);
+        if (c.ys <= 0.0) {
+            omode = 7;
+            goto L1000;
+        }
+        c.d1 = std::sqrt(1.0 / c.ys);
+        for (int i = 0; i < n; ++i) {
+            sb[i] = c.d1 * sb[i];
+            yb[i] = c.d1 * yb[i];
+        }
+        for (int i = 0; i < n; ++i) aux[i] = yb[i];   // ctonb
+        c.ps = 0.0;
+        for (int i = 0; i < n; ++i) c.ps = c.ps + diag[i] * aux[i] * aux[i];
+        c.d1 = 1.0 / c.ps;
+        for (int i = 0; i < n; ++i) diag[i] = diag[i] * c.d1;
+        for (int i = 0; i < n; ++i) gg[i] = sb[i];   // ctonb
+        c.ps = 0.0;
+        for (int i = 0; i < n; ++i) c.ps = c.ps + gg[i] * gg[i] / diag[i];
+        c.den = c.ps;
+        for (int i = 0; i < n; ++i) {
+            const double q = gg[i] / diag[i];
+            diag[i] = 1.0 / (1.0 / diag[i] + aux[i] * aux[i] - (q * q) / c.den);
+            if (diag[i] <= 0.0) diag[i] = rmin;
+        }
+    }
+    c.ps = m1o_prosca(n, g, g);
+    c.gnorm = std::sqrt(c.ps);
+    c.eps1 = c.gnorm / c.gnorms;
+    if (c.eps1 < epsg) {
+        omode = 1;
+        goto L1000;
+    }
+    if (niter == c.itmax) {
+        omode = 4;
+        goto L1000;
+    }
+    if (c.isim > nsim) {
+        omode = 5;
+        goto L1000;
+    }
+    for (int i = 0; i < n; ++i) d[i] = -g[i];
+    m1o_dd(n, m, d, aux, jmin, jmax, diag, alpha, ybar, sbar);
+    c.hp0 = m1o_prosca(n, d, g);
+    if (c.hp0 >= 0.0) {
+        omode = 7;
+        goto L1000;
+    }
+    goto L100;
+L1000:
+    if (reverse != 0) reverse = -1;
+    reentry = 0;
+    nsim = c.isim;
+    epsg = c.eps1;
+}
+
+static void m1o_m1qn3(M1RC& c, int n, double* x, double& f, double* g, double dxmin, double df1, double& epsg,
+                      int& omode, int& niter, int& nsim, int* iz, double* dz, int ndz, int& reverse, int& indic,
+                      int& indica) {
+    if (c.reentry > 0) goto L9999;
+    if (n <= 0 || niter <= 0 || nsim <= 0 || dxmin <= 0.0 || epsg <= 0.0) {
+        omode = 2;
+        if (reverse > 0) reverse = -1;
+        return;
+    }
+    if (epsg >= 1.0) {
+        omode = 1;
+        niter = 0;
+        nsim = 0;
+        epsg = 1.0;
+        if (reverse > 0) reverse = -1;
+        return;
+    }
+    if (ndz < 5 * n + 1 || ndz < 6 * n + 1) {
+        omode = 2;
+        if (reverse > 0) reverse = -1;
+        return;
+    }
+    c.m = (ndz - 4 * n) / (2 * n + 1);   // mupdts, DIS
+    if (c.m < 1 || ndz < 2 * (2 + c.m) * n + c.m) {
+        omode = 2;
+        if (reverse > 0) reverse = -1;
+        return;
+    }
+    iz[0] = n;
+    iz[1] = 0;
+    iz[2] = c.m;
+    c.idiag = 0;
+    c.iybar = c.idiag + n;
+    c.isbar = c.iybar + n * c.m;
+    c.id = c.isbar + n * c.m;
+    c.igg = c.id + n;
+    c.iaux = c.igg + n;
+    c.ialpha = c.iaux + n;
+L9999:
+    m1o_m1qn3a(c, n, x, f, g, dxmin, df1, epsg, omode, niter, nsim, iz[2], iz[3], iz[4], &dz[c.id], &dz[c.igg],
+               &dz[c.idiag], &dz[c.iaux], &dz[c.ialpha], &dz[c.iybar], &dz[c.isbar], reverse, c.reentry, indic,
+               indica);
+}
+
+static int opt_m1qn3(orc_sys* s, int niter_in, int nsim_in, double epsrel, mdff_opt_result* R) {
+    const int natm = s->natm, n = 3 * natm, ndz = 4 * n + 5 * (2 * n + 1);
+    std::vector<double> x(n), g(n), dz(ndz);
+    M1RC c;
+    int icall = 0, iz[5] = {0, 0, 0, 0, 0}, omode = 0, niter = niter_in, nsim = nsim_in, indic = 0, reverse = 1;
+    double f, phigrad = 0.0, epsg = epsrel;
+    const double dxmin = 2.2250738585072014e-308, df1 = 1.0;
+    auto evaluate = [&]() {
+        for (int ia = 0; ia < natm; ++ia) {
+            s->rx[ia] = x[ia];
+            s->ry[ia] = x[natm + ia];
+            s->rz[ia] = x[2 * natm + ia];
+        }
+        engforce(s);
+        f = opt_utot(s);
+        phigrad = 0.0;
+        for (int ia = 0; ia < natm; ++ia) {
+            g[ia] = -s->fx[ia];
+            g[natm + ia] = -s->fy[ia];
+            g[2 * natm + ia] = -s->fz[ia];
+            phigrad = phigrad + g[ia] * g[ia] + g[natm + ia] * g[natm + ia] + g[2 * natm + ia] * g[2 * natm + ia];
+        }
+    };
+    for (int ia = 0; ia < natm; ++ia) {
+        x[ia] = s->rx[ia];
+        x[natm + ia] = s->ry[ia];
+        x[2 * natm + ia] = s->rz[ia];
+    }
+    evaluate();
+    R->u_initial = f;
+    while (reverse >= 0) {
+        icall = icall + 1;
+        m1o_m1qn3(c, n, x.data(), f, g.data(), dxmin, df1, epsg, omode, niter, nsim, iz, dz.data(), ndz, reverse,
+                  indic, s->m1_indica);
+        evaluate();
+    }
+    R->u_final = f;
+    R->phigrad = phigrad;
+    R->iterations = niter;
+    R->nforce = icall + 1;
+    R->info = omode;
+    R->status = omode == 1 ? 0 : (omode == 4 || omode == 5) ? 1 : omode == 2 ? 2 : 3;
+    return 0;
+}
+
 int orc_opt_sastry(orc_sys* s, int itmax, mdff_opt_result* r) {
     std::memset(r, 0, sizeof *r);
     return opt_sastry(s, itmax, r);
+}
+
+int orc_opt_m1qn3(orc_sys* s, int niter, int nsim, double epsg, mdff_opt_result* r) {
+    std::memset(r, 0, sizeof *r);
+    return opt_m1qn3(s, niter, nsim, epsg, r);
 }
 
 int orc_opt_lbfgs(orc_sys* s, int itmax, double eps, mdff_opt_result* r) {

@@ -1,9 +1,14 @@
-"""Structure optimisation on the device (mdff_opt_sastry: the reference's
-sastry conjugate-gradient minimiser over the engine's force evaluations)
-against the oracle's restatement, from jittered LJ and polarisable-ion MgO
-starts.  Both follow the same scalar control flow; their dot products are
-summed in different orders, so the line searches can take slightly
-different paths near the end -- the minima must agree, not the step counts."""
+"""Structure optimisation on the device -- the reference's three optalgo,
+mdff_opt_sastry (conjugate gradients, cubic line minimisation),
+mdff_opt_lbfgs (Nocedal's L-BFGS with the More-Thuente line search) and
+mdff_opt_m1qn3 (M1QN3 in diagonal-initial-scaling mode), each over the
+engine's force evaluations -- against the oracle's restatements, from
+jittered LJ and polarisable-ion MgO starts.  Both sides follow the same
+scalar control flow; their dot products are summed in different orders, so
+the line searches can take slightly different paths near the end -- the
+minima must agree, the step counts only closely.  On the mixed path the
+stopping tests are checked with the oracle's FP64 forces at the returned
+point, with a 5 % margin for the mixed forces' rounding."""
 import numpy as np
 import pytest
 
@@ -74,7 +79,7 @@ def test_lbfgs_lj_matches_oracle():
     assert abs(re["u_initial"] - ro["u_initial"]) < 1e-12 * abs(ro["u_initial"])
     assert abs(re["u_final"] - ro["u_final"]) < 1e-11 * abs(ro["u_final"])
     assert abs(re["u_final"] - perfect) < 1e-10 * abs(perfect)
-    assert abs(re["nforce"] - ro["nforce"]) <= 2 and abs(re["iterations"] - ro["iterations"]) <= 2
+    assert abs(re["nforce"] - ro["nforce"]) <= 5 and abs(re["iterations"] - ro["iterations"]) <= 5
     d = _min_image(e.positions() - o.positions(), np.asarray(s["cell"]))
     assert np.abs(d).max() < 1e-5
     # the evaluation budget: itmax force evaluations, then status 1
@@ -102,4 +107,52 @@ def test_lbfgs_pim_minimum_matches_oracle(prec):
     # returned point with the oracle's FP64 forces too
     o = oracle.Oracle(p, s["itype"], e.positions(), s["cell"])
     f = o.engforce()["f"]
-    assert np.sqrt(np.sum(f * f)) / max(1.0, np.sqrt(np.sum(e.positions() ** 2))) <= 1e-5 * (1.0 + 10 * tol)
+    slack = 1.0 + 1e-6 if prec == abi.PREC_FP64 else 1.05
+    assert np.sqrt(np.sum(f * f)) / max(1.0, np.sqrt(np.sum(e.positions() ** 2))) <= abi.EPSREL_OPT * slack
+
+
+def test_m1qn3_lj_matches_oracle():
+    # mdff_opt_m1qn3 (device vectors, dd's recursion with device-side
+    # coefficients, the DIS diagonal update on the device) against the
+    # oracle's reverse-communication restatement of m1qn3_driver/M1QN3
+    s = systems.lj_argon()
+    perfect = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"]).engforce()["e"]["u_lj"]
+    pos = s["pos"] + np.random.default_rng(3).normal(0, 0.08, s["pos"].shape)
+    e = mdff_b200.Engine(s["params"], s["itype"], pos, s["cell"])
+    o = oracle.Oracle(s["params"], s["itype"], pos, s["cell"])
+    re, ro = e.opt_m1qn3(), o.opt_m1qn3()
+    assert re["status"] == ro["status"] == 0 and re["info"] == ro["info"] == 1
+    assert abs(re["u_initial"] - ro["u_initial"]) < 1e-12 * abs(ro["u_initial"])
+    assert abs(re["u_final"] - ro["u_final"]) < 1e-10 * abs(ro["u_final"])
+    assert abs(re["u_final"] - perfect) < 1e-9 * abs(perfect)
+    assert abs(re["nforce"] - ro["nforce"]) <= 5 and abs(re["iterations"] - ro["iterations"]) <= 5
+    d = _min_image(e.positions() - o.positions(), np.asarray(s["cell"]))
+    assert np.abs(d).max() < 1e-4
+    r4 = mdff_b200.Engine(s["params"], s["itype"], pos, s["cell"]).opt_m1qn3(niter=4)
+    o4 = oracle.Oracle(s["params"], s["itype"], pos, s["cell"]).opt_m1qn3(niter=4)
+    assert r4["status"] == o4["status"] == 1 and r4["info"] == o4["info"] == 4
+    assert r4["nforce"] == o4["nforce"]
+    assert abs(r4["u_final"] - o4["u_final"]) < 1e-10 * abs(o4["u_final"])
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_m1qn3_pim_minimum_matches_oracle(prec):
+    s = systems.mgo_pim(grid=(6, 6, 6), rc=6.0, alpha=0.55, kmax=8, temp=1000.0, jitter=0.1, seed=5)
+    p = s["params"]
+    p.algo_moment_from_pola = abi.POLA_PCG
+    p.conv_tol_ind = 1e-10
+    o0 = oracle.Oracle(p, s["itype"], s["pos"], s["cell"])
+    g0 = np.sqrt(np.sum(o0.engforce()["f"] ** 2))
+    ro = oracle.Oracle(p, s["itype"], s["pos"], s["cell"]).opt_m1qn3()
+    p.precision = prec
+    e = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+    re = e.opt_m1qn3()
+    assert ro["status"] == 0 and re["status"] == 0
+    tol = 1e-10 if prec == abi.PREC_FP64 else 1e-7
+    assert abs(re["u_initial"] - ro["u_initial"]) < tol * abs(ro["u_initial"])
+    assert abs(re["u_final"] - ro["u_final"]) < max(tol, 1e-9) * abs(ro["u_final"])
+    # the stop test |G| / |G_0| < epsrel_m1qn3 holds at the returned point
+    # with the oracle's FP64 forces too
+    f = oracle.Oracle(p, s["itype"], e.positions(), s["cell"]).engforce()["f"]
+    slack = 1.0 + 1e-6 if prec == abi.PREC_FP64 else 1.05
+    assert np.sqrt(np.sum(f * f)) / g0 < abi.EPSREL_OPT * slack

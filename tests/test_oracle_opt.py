@@ -1,11 +1,13 @@
-"""The oracle's structure optimisation (sastry, src/opt.f90:452-849): from a
-jittered LJ FCC crystal the conjugate-gradient minimiser must return to the
-perfect lattice (its energy is the known minimum), stop on the reference's
-energy test and leave the forces at zero."""
+"""The oracle's structure optimisation, the three optalgo of opt_main: sastry
+(src/opt.f90:452-849), lbfgs (lbfgs_driver :972-1194 over src/lbfgs.f90) and
+m1qn3 (m1qn3_driver :1203-1330 over src/m1qn3.f90).  From a jittered LJ FCC
+crystal each minimiser must return to the perfect lattice (its energy is the
+known minimum), stop on the reference's own test and report its exits as the
+reference does."""
 import numpy as np
 
 import oracle
-from mdff_b200 import systems
+from mdff_b200 import abi, systems
 
 
 def test_lj_crystal_relaxes_to_the_lattice():
@@ -56,3 +58,35 @@ def test_lbfgs_evaluation_budget_and_line_search_exit():
     # (info 6) or its interval test (info 2), as the reference reports it
     r = oracle.Oracle(s["params"], s["itype"], pos, s["cell"]).opt_lbfgs(eps=1e-14)
     assert r["status"] == 3 and r["info"] in (2, 6)
+
+
+def test_m1qn3_relaxes_to_the_lattice():
+    # optalgo = 'm1qn3' (m1qn3_driver, src/opt.f90:1203-1330): DIS mode,
+    # m = 5, stop when |G| / |G_0| < epsrel_m1qn3; the driver evaluates once
+    # more at the returned point, so phigrad is |G|^2 there
+    s, pos, perfect = _jittered_lj()
+    o = oracle.Oracle(s["params"], s["itype"], pos, s["cell"])
+    g0 = np.sqrt(np.sum(o.engforce()["f"] ** 2))
+    r = o.opt_m1qn3()
+    assert r["status"] == 0 and r["info"] == 1
+    assert np.sqrt(r["phigrad"]) / g0 < abi.EPSREL_OPT
+    assert abs(r["u_final"] - perfect) < 1e-9 * abs(perfect)
+    f = o.engforce()
+    assert abs(f["e"]["u_lj"] - r["u_final"]) < 1e-12 * abs(perfect)
+    cg = oracle.Oracle(s["params"], s["itype"], pos, s["cell"]).opt_sastry()
+    assert r["nforce"] < cg["nforce"] / 3
+
+
+def test_m1qn3_iteration_cap_and_rounding_exit():
+    s, pos, _ = _jittered_lj()
+    r = oracle.Oracle(s["params"], s["itype"], pos, s["cell"]).opt_m1qn3(niter=4)
+    assert r["status"] == 1 and r["info"] == 4 and r["iterations"] == 4
+    assert r["u_final"] < r["u_initial"]
+    # below what rounding allows: mlis3's dxmin/precision exit, omode 6,
+    # which the reference's driver accepts with a warning
+    r = oracle.Oracle(s["params"], s["itype"], pos, s["cell"]).opt_m1qn3(epsg=1e-13)
+    assert r["status"] == 3 and r["info"] == 6
+    # epsg >= 1: no progress asked for, only the driver's evaluations
+    r = oracle.Oracle(s["params"], s["itype"], pos, s["cell"]).opt_m1qn3(epsg=1.0)
+    assert r["status"] == 0 and r["iterations"] == 0 and r["nforce"] == 2
+    assert r["u_final"] == r["u_initial"]

@@ -710,7 +710,7 @@ def run_opt(args):
             "metric": "structure-optimisation atom-force-evaluations/s, 32k-ion MgO PIM (" +
                       {"lbfgs": "limited-memory BFGS, More-Thuente line search)",
                        "m1qn3": "M1QN3 diagonal initial scaling, Wolfe line search mlis3)",
-                       "sastry": "conjugate gradients, cubic line search)"}[args.optalgo]),
+                       "sastry": "conjugate gradients, cubic line search)"}[args.optalgo],
             "value": value,
             "unit": "atom-evaluations/s",
             "n_gpus": world,

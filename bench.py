@@ -57,6 +57,8 @@ def parse():
                     help="kspace_reuse (auto: on for the mixed path, off for the plain FP64 path)")
     ap.add_argument("--opt-iters", type=int, default=10,
                     help="opt workload: iterations (sastry), 5x as many force evaluations (lbfgs) or iterations (m1qn3)")
+    ap.add_argument("--rmc-efg-moves", type=int, default=100,
+                    help="rmc workload: trial moves of the chain with the EFG chi^2 terms (0: skip)")
     ap.add_argument("--optalgo", default="sastry", choices=["sastry", "lbfgs", "m1qn3"],
                     help="opt workload: minimiser (the reference's optalgo)")
     ap.add_argument("--workload", default="production", choices=["production", "batch", "opt", "efg", "rmc"],
@@ -968,6 +970,51 @@ def run_rmc(args):
         }
         roof = result["roofline"]
         roof["frac"] = roof["achieved"] / roof["peak"]
+    if args.rmc_efg_moves > 0:
+        # the EFG chi^2 terms (rmc_efg): the same cell as rigid ions (the
+        # reference's rmc_efg takes point charges), U, Vzz and eta fitted to
+        # the distributions of the perturbed target, every trial one Ewald
+        # EFG of the whole trial configuration
+        pr = type(p).from_buffer_copy(p)
+        for t in range(pr.ntype):
+            pr.ldip_polar[t] = 0
+            pr.poldip_iso[t] = 0.0
+        pr.doefg = 1
+        er = mdff_b200.Engine(pr, s["itype"], tgt, s["cell"])
+        ep = abi.RmcEfgParams()
+        ep.lrmc_u = ep.lrmc_vzz = ep.lrmc_eta = 1
+        ep.resolution_u_efg, ep.u_efg_min = 0.02, -1.0
+        ep.resolution_vzz_efg, ep.vzz_efg_min = 0.02, -2.0
+        ep.resolution_eta_efg = 0.02
+        su, sv, se = ep.shapes(pr.ntype)
+        r1 = abi.RmcParams.from_buffer_copy(rp)
+        r1.acceptance_max, r1.max_trials = 1, 1
+        _, _, Ux, Vx, Ex = er.rmc_efg(r1, ep, gexp, np.zeros(su), np.zeros(sv), np.zeros(se))
+        er.set_positions(pos0)
+        r1.acceptance_max, r1.max_trials = 10 ** 12, 4
+        er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=5)   # warm-up
+        er.set_positions(pos0)
+        r1.max_trials = args.rmc_efg_moves + 1
+        ext2 = torch.cuda.ExternalStream(er.stream(), device=device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(ext2)
+        rr, *_ = er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=7)
+        e1.record(ext2)
+        e1.synchronize()
+        ems = e0.elapsed_time(e1)
+        er.close()
+        if result is not None:
+            result["efg_terms"] = {
+                "metric": "reverse Monte Carlo trial moves/s with the g(r), U, Vzz and eta chi^2 terms, 32k-ion "
+                          "rigid-ion MgO",
+                "value": (rr["kall"] - 1) / (ems / 1e3), "unit": "moves/s", "moves": rr["kall"] - 1,
+                "accepted": rr["kacc"] - 1, "ms_per_move": ems / max(1, rr["kall"] - 1),
+                "chisq_last": rr["chisq"], "bins": {"U": su, "vzz": sv, "eta": se},
+                "note": "one full-device Ewald EFG evaluation of the trial configuration per move, as rmc_efg "
+                        "computes it (multipole_efg_ES)"}
+    if result is not None:
         if not args.no_cpu:
             import oracle
             o = oracle.Oracle(p, s["itype"], pos0, s["cell"])

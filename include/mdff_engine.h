@@ -610,6 +610,39 @@ typedef struct mdff_rmc_result {
 int  mdff_rmc(mdff_ctx* ctx, const mdff_rmc_params* rp, const double* grr_exp, const double* uniforms,
               long long nuni, unsigned long long seed, double* grr_out, mdff_rmc_result* res);
 
+/* rmctag's EFG settings (src/rmc.f90:40-60): which EFG chi^2 terms, from
+ * which acceptance count, and the bins of rmc_efg: PANU = INT(2|u_efg_min| /
+ * resolution_u_efg), PANvzz = INT(2|vzz_efg_min| / resolution_vzz_efg),
+ * PANeta = INT(1 / resolution_eta_efg).  Values in the units of
+ * multipole_efg_ES (e / A^3, no coul_unit). */
+typedef struct mdff_rmc_efg_params {
+    int lrmc_u, lrmc_vzz, lrmc_eta;
+    int efg_start;                 /* the EFG terms while kacc >= efg_start (default 0) */
+    double resolution_u_efg, u_efg_min;
+    double resolution_vzz_efg, vzz_efg_min;
+    double resolution_eta_efg;
+} mdff_rmc_efg_params;
+
+/* rmc_main with its EFG chi^2 terms (src/rmc.f90:420-640): per trial move
+ * the g(r) term as mdff_rmc (incremental counts), and while kacc >=
+ * efg_start the EFG of the whole trial configuration (rmc_efg: the engine's
+ * Ewald EFG of the point charges, multipole_efg_ES with mu = 0), its NMR
+ * convention, the Vzz, eta and Czjzek U1..U5 histograms and eval_chisq_Uefg /
+ * vzz / eta against the experimental distributions.  One host-driven trial
+ * at a time (each needs a full-device EFG evaluation).  Distributions use
+ * the reference's Fortran layouts: dibU (ui = 1..6, mp = 0..ntype,
+ * bin = 0..PANU) with ui fastest, dibvzz and dibeta (mp, bin) with mp
+ * fastest; the *_out arrays receive those of the last accepted
+ * configuration (rows the reference never fills -- U's row 6, eta's last
+ * bin -- are 0).  Uniforms, temperatures, stopping and the result as
+ * mdff_rmc.  The system must be point charges: no static or induced
+ * dipoles (MDFF_E_UNSUPPORTED otherwise). */
+int  mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_params* ep,
+                  const double* grr_exp, const double* dibU_exp, const double* dibvzz_exp,
+                  const double* dibeta_exp, const double* uniforms, long long nuni,
+                  unsigned long long seed, double* grr_out, double* dibU_out, double* dibvzz_out,
+                  double* dibeta_out, mdff_rmc_result* res);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,8 @@ def lib():
         L.mdff_gr.argtypes = [vp, C.c_double, C.c_double, dp, ip]
         L.mdff_rmc.argtypes = [vp, C.POINTER(abi.RmcParams), dp, dp, C.c_longlong, C.c_ulonglong, dp,
                                C.POINTER(abi.RmcResult)]
+        L.mdff_rmc_efg.argtypes = [vp, C.POINTER(abi.RmcParams), C.POINTER(abi.RmcEfgParams), dp, dp, dp, dp, dp,
+                                   C.c_longlong, C.c_ulonglong, dp, dp, dp, dp, C.POINTER(abi.RmcResult)]
         L.mdff_get_positions.argtypes = [vp, dp, dp, dp]
         L.mdff_engforce.argtypes = [vp, dp, dp, dp, C.POINTER(abi.Energies), dp, dp, dp, dp, dp]
         L.mdff_nlist_build.argtypes = [vp]
@@ -205,6 +207,26 @@ class Engine:
         self._check(lib().mdff_rmc(self._h, C.byref(rp), _dp(gexp), _dp(u), 0 if u is None else len(u),
                                    int(seed), _dp(g), C.byref(r)))
         return r.as_dict(), g
+
+    def rmc_efg(self, rp, ep, gexp, dibU_exp=None, dibvzz_exp=None, dibeta_exp=None, uniforms=None, seed=0):
+        """Reverse Monte Carlo with rmc_main's EFG chi^2 terms (mdff_rmc_efg);
+        returns (result, g(r), U, Vzz, eta distributions of the last accepted
+        configuration), the distributions shaped as RmcEfgParams.shapes."""
+        su, sv, se = ep.shapes(self.params.ntype)
+        gexp = np.ascontiguousarray(gexp, dtype=np.float64)
+        ex = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+              for a in (dibU_exp, dibvzz_exp, dibeta_exp)]
+        for a, shp in zip(ex, (su, sv, se)):
+            if a is not None and a.shape != shp:
+                raise ValueError(f"distribution shape {a.shape}, expected {shp}")
+        u = None if uniforms is None else np.ascontiguousarray(uniforms, dtype=np.float64)
+        g = np.empty_like(gexp)
+        U, V, E = np.empty(su), np.empty(sv), np.empty(se)
+        r = abi.RmcResult()
+        self._check(lib().mdff_rmc_efg(self._h, C.byref(rp), C.byref(ep), _dp(gexp), *(_dp(a) for a in ex), _dp(u),
+                                       0 if u is None else len(u), int(seed), _dp(g), _dp(U), _dp(V), _dp(E),
+                                       C.byref(r)))
+        return r.as_dict(), g, U, V, E
 
     def set_cell(self, cell):
         """A new cell (rows = lattice vectors) for the same atoms (mdff_set_cell)."""

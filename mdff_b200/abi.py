@@ -128,6 +128,24 @@ class RmcParams(C.Structure):
                 ("temp_rmc", C.c_double * 6), ("acceptance_max", C.c_longlong), ("max_trials", C.c_longlong)]
 
 
+class RmcEfgParams(C.Structure):
+    """mdff_rmc_efg_params: rmctag's EFG terms (lrmc_u, lrmc_vzz, lrmc_eta),
+    efg_start and the bins of rmc_efg."""
+    _fields_ = [("lrmc_u", C.c_int), ("lrmc_vzz", C.c_int), ("lrmc_eta", C.c_int), ("efg_start", C.c_int),
+                ("resolution_u_efg", C.c_double), ("u_efg_min", C.c_double),
+                ("resolution_vzz_efg", C.c_double), ("vzz_efg_min", C.c_double),
+                ("resolution_eta_efg", C.c_double)]
+
+    def shapes(self, ntype):
+        """Array shapes of the U, Vzz and eta distributions: the reference's
+        Fortran layouts dibU(6, 0:ntype, 0:PANU), dib(0:ntype, 0:PAN) read in C
+        order, so index [bin, mp, ui - 1] and [bin, mp]."""
+        panu = int(2.0 * abs(self.u_efg_min) / self.resolution_u_efg)
+        panv = int(2.0 * abs(self.vzz_efg_min) / self.resolution_vzz_efg)
+        pane = int(1.0 / self.resolution_eta_efg)
+        return (panu + 1, ntype + 1, 6), (panv + 1, ntype + 1), (pane + 1, ntype + 1)
+
+
 class RmcResult(C.Structure):
     _fields_ = [("kall", C.c_longlong), ("kacc", C.c_longlong), ("uniforms_used", C.c_longlong),
                 ("chisq", C.c_double * 6), ("status", C.c_int), ("pad", C.c_int)]

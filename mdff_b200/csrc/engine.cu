@@ -26,6 +26,7 @@
 #include "npt.cuh"
 #include "rmc.cuh"
 #include "efg_post.cuh"
+#include "rmc_efg.cuh"
 #include "io.cuh"
 #include <condition_variable>
 #include <deque>
@@ -3781,6 +3782,326 @@ int mdff_rmc(mdff_ctx* ctx, const mdff_rmc_params* rp, const double* grr_exp, co
         res->pad = 0;
     }
     CK(cudaStreamSynchronize(ctx->st));
+    return MDFF_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// eval_chisq_rmc's g(r) term by the fixed tree of the device chain: the
+// squares of the terms q = bin x (npairs + 1) + mp in 1024 strided partial
+// sums, a halving tree over each group of 32, the same tree over the groups
+double rmc_chisq_gr_tree(const RmcConst& k, const double* calc, const double* gexp) {
+    const int nterm = (k.npairs + 1) * k.nbins;
+    std::vector<double> part(1024, 0.0);
+    for (int q = 0; q < nterm; ++q) {
+        const int b = q / (k.npairs + 1), mp = q - b * (k.npairs + 1);
+        const double d = calc[(size_t)mp * k.nbins + b] - gexp[(size_t)mp * k.nbins + b];
+        part[q % 1024] = part[q % 1024] + d * d;
+    }
+    auto tree32 = [](double* v) {
+        for (int o = 16; o > 0; o >>= 1)
+            for (int l = 0; l < o; ++l) v[l] = v[l] + v[l + o];
+        return v[0];
+    };
+    double w[32];
+    for (int g = 0; g < 32; ++g) w[g] = tree32(&part[32 * g]);
+    return tree32(w);
+}
+
+// rmc_efg's normalisation (src/rmc.f90:1620-1650) and eval_chisq_Uefg /
+// eval_chisq_vzz / eval_chisq_eta (:693-769), left to right in the
+// reference's loop order.  Layouts are the reference's Fortran ones:
+// U (ui, mp, bin) at (bin (ntype+1) + mp) 6 + ui - 1, vzz and eta (mp, bin)
+// at bin (ntype+1) + mp.  Quirks kept: the per-type U rows divide the
+// all-types U1 counts; eta's last bin is never normalised (it stays 0).
+struct RmcEfgHost {
+    int nt1, PANU, PANvzz, PANeta;
+    double natm, resu, resvzz, reseta;
+    std::vector<double> natmi;
+};
+
+void rmc_efg_normalise(const RmcEfgHost& e, const int* cnt, int offeta, int offU, bool lu, double* U, double* vzz,
+                       double* eta) {
+    const int wv = e.PANvzz + 1, we = e.PANeta + 1, wu = e.PANU + 1;
+    if (lu)
+        for (int bin = 0; bin <= e.PANU; ++bin)
+            for (int ui = 1; ui <= 5; ++ui) {
+                U[((size_t)bin * e.nt1 + 0) * 6 + ui - 1] =
+                    (double)cnt[offU + ((ui - 1) * e.nt1 + 0) * wu + bin] / (e.resu * e.natm);
+                for (int it = 1; it < e.nt1; ++it)
+                    U[((size_t)bin * e.nt1 + it) * 6 + ui - 1] =
+                        (double)cnt[offU + (0 * e.nt1 + 0) * wu + bin] / (e.resu * e.natmi[it - 1]);
+            }
+    for (int bin = 0; bin < e.PANeta; ++bin) {
+        eta[(size_t)bin * e.nt1] = (double)cnt[offeta + bin] / (e.reseta * e.natm);
+        for (int it = 1; it < e.nt1; ++it)
+            eta[(size_t)bin * e.nt1 + it] = (double)cnt[offeta + it * we + bin] / (e.reseta * e.natmi[it - 1]);
+    }
+    for (int it = 0; it < e.nt1; ++it) eta[(size_t)e.PANeta * e.nt1 + it] = 0.0;
+    for (int bin = 0; bin <= e.PANvzz; ++bin) {
+        vzz[(size_t)bin * e.nt1] = (double)cnt[bin] / (e.resvzz * e.natm);
+        for (int it = 1; it < e.nt1; ++it)
+            vzz[(size_t)bin * e.nt1 + it] = (double)cnt[it * wv + bin] / (e.resvzz * e.natmi[it - 1]);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_params* ep, const double* grr_exp,
+                 const double* dibU_exp, const double* dibvzz_exp, const double* dibeta_exp, const double* uniforms,
+                 long long nuni, unsigned long long seed, double* grr_out, double* dibU_out, double* dibvzz_out,
+                 double* dibeta_out, mdff_rmc_result* res) {
+    if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
+    if (!rp || !ep || !grr_exp) return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: parameters and the experimental g(r)");
+    if (rp->max_trials < 1 || rp->acceptance_max < 1) return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: trial bounds");
+    for (int q = 0; q < 6; ++q)
+        if (!(rp->temp_rmc[q] > 0.0)) return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: temperatures must be positive");
+    if (!(rp->max_displacement > 0.0 && 3.0 * rp->max_displacement < 1.0))
+        return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: max_displacement must be in (0, 0.33) A");
+    if (!(ep->resolution_vzz_efg > 0.0 && ep->resolution_eta_efg > 0.0 && ep->resolution_u_efg > 0.0))
+        return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: EFG resolutions must be positive");
+    if ((ep->lrmc_u && !dibU_exp) || (ep->lrmc_vzz && !dibvzz_exp) || (ep->lrmc_eta && !dibeta_exp))
+        return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: an experimental distribution of an active term is missing");
+    if (!ctx->p.lcoulomb || ctx->npol > 0 || ctx->any_dip0)
+        return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_rmc_efg: the EFG terms take point charges (no dipoles), as "
+                                             "rmc_efg's multipole_efg_ES is called with mu = 0");
+    const double pu = 2.0 * std::fabs(ep->u_efg_min) / ep->resolution_u_efg;
+    const double pv = 2.0 * std::fabs(ep->vzz_efg_min) / ep->resolution_vzz_efg;
+    const double pe = 1.0 / ep->resolution_eta_efg;
+    if (!(pu < 1e6 && pv < 1e6 && pe < 1e6)) return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_rmc_efg: at most 1e6 bins");
+    cudaSetDevice(ctx->p.device);
+    auto* k = new RmcConst;
+    std::unique_ptr<RmcConst> kguard(k);
+    TRY(rmc_setup(ctx, rp->cut_rmc, rp->resolution_gr, *k));
+    const int n = ctx->n, nt1 = ctx->ntype + 1;
+    RmcEfgHost eh;
+    eh.nt1 = nt1;
+    eh.PANU = (int)pu;
+    eh.PANvzz = (int)pv;
+    eh.PANeta = (int)pe;
+    eh.natm = (double)n;
+    eh.resu = ep->resolution_u_efg;
+    eh.resvzz = ep->resolution_vzz_efg;
+    eh.reseta = ep->resolution_eta_efg;
+    for (int t = 0; t < ctx->ntype; ++t) eh.natmi.push_back((double)ctx->natmi[t]);
+    RmcEfgSpec sp;
+    sp.ntype = ctx->ntype;
+    sp.PANU = ep->lrmc_u ? eh.PANU : -1;
+    sp.PANvzz = eh.PANvzz;
+    sp.PANeta = eh.PANeta;
+    sp.offeta = nt1 * (eh.PANvzz + 1);
+    sp.offU = sp.offeta + nt1 * (eh.PANeta + 1);
+    sp.cu = ctx->u.coul;
+    sp.umin = ep->u_efg_min;
+    sp.resu = ep->resolution_u_efg;
+    sp.vzzmin = ep->vzz_efg_min;
+    sp.resvzz = ep->resolution_vzz_efg;
+    sp.reseta = ep->resolution_eta_efg;
+    sp.sq3 = 1.0 / std::sqrt(3.0);
+    sp.sq32 = sp.sq3 * 0.5;
+    const size_t ncnt = (size_t)sp.offU + (size_t)6 * nt1 * (eh.PANU + 1);
+    const size_t nU = (size_t)(eh.PANU + 1) * nt1 * 6, nV = (size_t)(eh.PANvzz + 1) * nt1,
+                 nE = (size_t)(eh.PANeta + 1) * nt1;
+    const size_t ngr = (size_t)k->nrow * k->nbins, ncalc = (size_t)(k->npairs + 1) * k->nbins;
+    const bool any_efg = ep->lrmc_u || ep->lrmc_vzz || ep->lrmc_eta;
+    // uniforms: the caller's, or the counter-based stream of mdff_rmc
+    std::vector<double> uni;
+    const long long nu = uniforms ? nuni : 10 * rp->max_trials;
+    if (!uniforms) {
+        if (rp->max_trials > 10000000LL) return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: at most 1e7 trials per call");
+        uni.resize((size_t)nu);
+        for (long long t = 0; t < nu; ++t) {
+            unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(t + 1);
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            z = z ^ (z >> 31);
+            uni[(size_t)t] = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+        }
+    }
+    const double* U_ = uniforms ? uniforms : uni.data();
+    // device scratch: fractional coordinates, g(r) counts and their change, EFG counts
+    double* s = nullptr;
+    int *hd = nullptr, *dh = nullptr, *ce = nullptr;
+    CK(cudaMallocAsync((void**)&s, sizeof(double) * 3 * (size_t)n, ctx->st));
+    CK(cudaMallocAsync((void**)&hd, sizeof(int) * ngr, ctx->st));
+    CK(cudaMallocAsync((void**)&dh, sizeof(int) * ngr, ctx->st));
+    CK(cudaMallocAsync((void**)&ce, sizeof(int) * ncnt, ctx->st));
+    CK(cudaMemsetAsync(hd, 0, sizeof(int) * ngr, ctx->st));
+    TRY(rmc_frac(ctx, s));
+    k_rmc_dirkar<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->cell, ctx->x, ctx->y, ctx->z);
+    k_gr_full<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k->bin, hd);
+    std::vector<int> h(ngr), hdel(ngr), htr(ngr), cnt(ncnt);
+    std::vector<double> sh(3 * (size_t)n);
+    CK(cudaMemcpyAsync(h.data(), hd, sizeof(int) * ngr, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(sh.data(), s, sizeof(double) * sh.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    TRY(check_launch(ctx, "rmc_efg start"));
+    const int saved_doefg = ctx->p.doefg;
+    ctx->p.doefg = 1;
+    std::vector<double> calc(ncalc), cU(nU, 0.0), cV(nV, 0.0), cE(nE, 0.0), aU(nU, 0.0), aV(nV, 0.0), aE(nE, 0.0);
+    // Verlet-list validity: an atom's summed trial displacements since the
+    // last build stay below half the skin
+    const bool lists = ctx->p.lvnlist != 0;
+    const double half_skin = 0.5 * ctx->p.skindiff;
+    std::vector<double> moved(lists ? (size_t)n : 0, 0.0);
+    auto efg_terms = [&](double chi[6]) -> int {
+        TRY(engforce_device(ctx));
+        CK(cudaMemsetAsync(ce, 0, sizeof(int) * ncnt, ctx->st));
+        k_rmc_efg_hist<<<nb(n), 256, 0, ctx->st>>>(n, ctx->efg, ctx->type, sp, ce);
+        CK(cudaMemcpyAsync(cnt.data(), ce, sizeof(int) * ncnt, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        TRY(check_launch(ctx, "rmc_efg histograms"));
+        rmc_efg_normalise(eh, cnt.data(), sp.offeta, sp.offU, ep->lrmc_u != 0, cU.data(), cV.data(), cE.data());
+        if (ep->lrmc_u) {
+            double c = 0.0;
+            for (int bin = 0; bin <= eh.PANU; ++bin)
+                for (int mp = 0; mp < nt1; ++mp)
+                    for (int ui = 0; ui < 5; ++ui) {
+                        const size_t q = ((size_t)bin * nt1 + mp) * 6 + ui;
+                        const double d = cU[q] - dibU_exp[q];
+                        c = c + d * d;
+                    }
+            chi[2] = c;
+        }
+        if (ep->lrmc_vzz) {
+            double c = 0.0;
+            for (int bin = 0; bin <= eh.PANvzz; ++bin)
+                for (int mp = 0; mp < nt1; ++mp) {
+                    const double d = cV[(size_t)bin * nt1 + mp] - dibvzz_exp[(size_t)bin * nt1 + mp];
+                    c = c + d * d;
+                }
+            chi[3] = c;
+        }
+        if (ep->lrmc_eta) {
+            double c = 0.0;
+            for (int bin = 0; bin <= eh.PANeta; ++bin)
+                for (int mp = 0; mp < nt1; ++mp) {
+                    const double d = cE[(size_t)bin * nt1 + mp] - dibeta_exp[(size_t)bin * nt1 + mp];
+                    c = c + d * d;
+                }
+            chi[4] = c;
+        }
+        return MDFF_OK;
+    };
+    auto total = [](double chi[6]) { chi[5] = (((chi[0] + chi[1]) + chi[2]) + chi[3]) + chi[4]; };
+    int rc = MDFF_OK;
+#define CK_R(call)                                                                             \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            rc = fail(ctx, MDFF_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+            return;                                                                            \
+        }                                                                                      \
+    } while (0)
+    long long kall = 1, kacc = 1, u = 0;
+    int status = 0;
+    double chi_old[6] = {0, 0, 0, 0, 0, 0}, chi[6];
+    [&]() {
+        rmc_normalise(*k, h, calc.data());
+        chi_old[0] = rmc_chisq_gr_tree(*k, calc.data(), grr_exp);
+        if (any_efg && kacc >= ep->efg_start) {
+            if ((rc = efg_terms(chi_old)) != MDFF_OK) return;
+            aU = cU; aV = cV; aE = cE;
+        }
+        total(chi_old);
+        const double dmax[3] = {rp->max_displacement / ctx->anorm[0], rp->max_displacement / ctx->anorm[1],
+                                rp->max_displacement / ctx->anorm[2]};
+        while (kacc < rp->acceptance_max && kall < rp->max_trials) {
+            ++kall;
+            if (u + 4 > nu) { status = 1; --kall; break; }
+            int p = (int)(U_[u] * n);   // rmc_move (src/rmc.f90:1371-1424)
+            if (p >= n) p = n - 1;
+            double disp[3], snew[3], sold[3];
+            for (int d = 0; d < 3; ++d) {
+                disp[d] = dmax[d] * (2.0 * U_[u + 1 + d] - 1.0);
+                sold[d] = sh[(size_t)d * n + p];
+                double v = sold[d] + disp[d];
+                if (v > 1.0 || v < 0.0) v = v - std::round(v);   // NINT: half away from zero
+                snew[d] = v;
+            }
+            u += 4;
+            if (lists) {
+                double dc[3];
+                for (int a = 0; a < 3; ++a)
+                    dc[a] = ctx->cell.A[3 * a] * disp[0] + ctx->cell.A[3 * a + 1] * disp[1] + ctx->cell.A[3 * a + 2] * disp[2];
+                const double step = std::sqrt(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]) + 1e-9;
+                if (moved[p] + step > half_skin) {
+                    if ((rc = build_lists(ctx, ctx->p.skindiff)) != MDFF_OK) return;
+                    std::fill(moved.begin(), moved.end(), 0.0);
+                }
+                moved[p] += step;
+            }
+            for (int d = 0; d < 3; ++d) sh[(size_t)d * n + p] = snew[d];
+            k_rmc_place<<<1, 1, 0, ctx->st>>>(n, s, p, snew[0], snew[1], snew[2], ctx->cell, ctx->x, ctx->y, ctx->z);
+            CK_R(cudaMemsetAsync(dh, 0, sizeof(int) * ngr, ctx->st));
+            k_rmc_grdelta<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k->bin, p, sold[0], sold[1],
+                                                       sold[2], dh);
+            CK_R(cudaMemcpyAsync(hdel.data(), dh, sizeof(int) * ngr, cudaMemcpyDeviceToHost, ctx->st));
+            for (int q = 0; q < 6; ++q) chi[q] = 0.0;
+            const bool efg_now = any_efg && kacc >= ep->efg_start;
+            if (efg_now) {
+                if ((rc = efg_terms(chi)) != MDFF_OK) return;
+            } else {
+                CK_R(cudaStreamSynchronize(ctx->st));
+            }
+            for (size_t q = 0; q < ngr; ++q) htr[q] = h[q] + hdel[q];
+            rmc_normalise(*k, htr, calc.data());
+            chi[0] = rmc_chisq_gr_tree(*k, calc.data(), grr_exp);
+            total(chi);
+            bool acc6 = false, stop = false;
+            for (int q = 0; q < 6; ++q) {   // src/rmc.f90:521-540
+                const double dq = chi[q] - chi_old[q];
+                bool a;
+                if (dq < 0.0) a = true;
+                else {
+                    if (u + 1 > nu) { stop = true; break; }
+                    const double metro = std::exp(-(dq * 0.5) / rp->temp_rmc[q]);
+                    a = metro >= U_[u];
+                    ++u;
+                }
+                if (q == 5) acc6 = a;
+            }
+            if (stop || !acc6) {   // back to snew - disp (src/rmc.f90:628-636); sold when the uniforms ran out
+                double back[3];
+                for (int d = 0; d < 3; ++d) {
+                    back[d] = stop ? sold[d] : snew[d] - disp[d];
+                    sh[(size_t)d * n + p] = back[d];
+                }
+                k_rmc_place<<<1, 1, 0, ctx->st>>>(n, s, p, back[0], back[1], back[2], ctx->cell, ctx->x, ctx->y,
+                                                  ctx->z);
+                if (stop) { status = 1; --kall; break; }
+            } else {
+                ++kacc;
+                for (int q = 0; q < 6; ++q) chi_old[q] = chi[q];
+                h = htr;
+                if (efg_now) { aU = cU; aV = cV; aE = cE; }
+            }
+        }
+    }();
+#undef CK_R
+    ctx->p.doefg = saved_doefg;
+    for (void* q : {(void*)s, (void*)hd, (void*)dh, (void*)ce}) cudaFreeAsync(q, ctx->st);
+    cudaStreamSynchronize(ctx->st);
+    if (rc != MDFF_OK) return rc;
+    TRY(check_launch(ctx, "rmc_efg"));
+    ctx->forces_valid = false;
+    if (ctx->p.lvnlist) TRY(build_lists(ctx, ctx->p.skindiff));
+    if (grr_out) rmc_normalise(*k, h, grr_out);
+    if (dibU_out) std::memcpy(dibU_out, aU.data(), sizeof(double) * nU);
+    if (dibvzz_out) std::memcpy(dibvzz_out, aV.data(), sizeof(double) * nV);
+    if (dibeta_out) std::memcpy(dibeta_out, aE.data(), sizeof(double) * nE);
+    if (res) {
+        res->kall = kall;
+        res->kacc = kacc;
+        res->uniforms_used = u;
+        for (int q = 0; q < 6; ++q) res->chisq[q] = chi_old[q];
+        res->status = status;
+        res->pad = 0;
+    }
     return MDFF_OK;
 }
 

@@ -58,6 +58,9 @@ def lib():
         L.orc_gr.argtypes = [C.c_void_p, C.c_double, C.c_double, dp, C.POINTER(C.c_int)]
         L.orc_rmc.argtypes = [C.c_void_p, C.POINTER(abi.RmcParams), dp, dp, C.c_longlong, dp,
                               C.POINTER(abi.RmcResult)]
+        L.orc_rmc_efg.argtypes = [C.c_void_p, C.POINTER(abi.RmcParams), C.POINTER(abi.RmcEfgParams), dp, dp, dp, dp,
+                                  dp, C.c_longlong, dp, dp, dp, dp, C.POINTER(abi.RmcResult)]
+        L.orc_efg_rmc.argtypes = [C.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -238,6 +241,29 @@ class Oracle:
         r = abi.RmcResult()
         lib().orc_rmc(self._h, C.byref(rp), _dp(gexp), _dp(u), len(u), _dp(g), C.byref(r))
         return r.as_dict(), g
+
+    def rmc_efg(self, rp, ep, gexp, dibU_exp=None, dibvzz_exp=None, dibeta_exp=None, uniforms=()):
+        """rmc_main with the EFG chi^2 terms (rmc_efg over multipole_efg_ES,
+        eval_chisq_Uefg/vzz/eta) on the given uniforms; returns (result, g(r),
+        U, Vzz, eta distributions of the last accepted configuration)."""
+        su, sv, se = ep.shapes(self._p.ntype)
+        gexp = np.ascontiguousarray(gexp, dtype=np.float64)
+        ex = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+              for a in (dibU_exp, dibvzz_exp, dibeta_exp)]
+        u = np.ascontiguousarray(uniforms, dtype=np.float64)
+        g = np.empty_like(gexp)
+        U, V, E = np.zeros(su), np.zeros(sv), np.zeros(se)
+        r = abi.RmcResult()
+        lib().orc_rmc_efg(self._h, C.byref(rp), C.byref(ep), _dp(gexp), *(_dp(a) for a in ex), _dp(u), len(u),
+                          _dp(g), _dp(U), _dp(V), _dp(E), C.byref(r))
+        return r.as_dict(), g, U, V, E
+
+    def efg_rmc(self):
+        """multipole_efg_ES of the current positions for point charges, [n][6]
+        (xx yy zz xy xz yz) without coul_unit."""
+        out = np.empty((6, self.n))
+        lib().orc_efg_rmc(self._h, _dp(out))
+        return out.T.copy()
 
     def md_start(self, vel):
         vel = np.asarray(vel, dtype=np.float64)

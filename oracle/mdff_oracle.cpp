@@ -3114,20 +3114,255 @@ int orc_gr(orc_sys* s, double cut, double res, double* grr, int* nbins) {
 }
 
 // rmc_main (src/rmc.f90:196-640) on the g(r) chi^2, random numbers from uni
-int orc_rmc(orc_sys* s, const mdff_rmc_params* rp, const double* gexp, const double* uni, long long nuni,
-            double* grr_out, mdff_rmc_result* res) {
-    GrSpec g = gr_spec(s, rp->cut_rmc, rp->resolution_gr);
+// ---- rmc_efg ----------------------------------------------------------------
+namespace {
+
+// multipole_efg_ES (src/efg.f90:1278-1625) for point charges (rmc_main calls
+// it with the efg module's mu = 0): the real-space sum over every other atom
+// at its minimum image (no cutoff), the reciprocal sum of the k mesh, the
+// self term -4 alpha^3 / (3 sqrt(pi)) q; no coul_unit.  V6 [6][n]: xx yy zz
+// xy xz yz.
+void efg_es_rmc(orc_sys* s, std::vector<double>& V6) {
     const int n = s->natm;
     std::vector<double> sx, sy, sz;
     direct_coords(s, sx, sy, sz);
+    const double a = s->alphaES, alpha2 = a * a, alpha3 = alpha2 * a;
+    const double selfa = -4.0 * alpha3 / 3.0 / PIROOT;
+    std::vector<double> dir(6 * (size_t)n, 0.0);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int ia = 0; ia < n; ++ia) {
+        double g[6] = {0, 0, 0, 0, 0, 0};
+        for (int ja = 0; ja < n; ++ja) {
+            if (ja == ia) continue;
+            const double qj = s->qia[ja];
+            double rxij, ryij, rzij;
+            const double d2 = pairvec(s->cell, sx[ia], sy[ia], sz[ia], sx[ja], sy[ja], sz[ja], rxij, ryij, rzij);
+            const double d = std::sqrt(d2), d3 = d2 * d;
+            const double dm5 = 1.0 / d2 / d3;
+            const double expon = std::exp(-alpha2 * d2) / PIROOT;
+            const double F1 = erfc_sel(s, a * d) + 2.0 * a * d * expon;
+            const double F2 = F1 + 4.0 * alpha3 * d3 * expon / 3.0;
+            g[0] = g[0] - qj * ((3.0 * rxij * rxij * F2 - d2 * F1) * dm5);
+            g[1] = g[1] - qj * ((3.0 * ryij * ryij * F2 - d2 * F1) * dm5);
+            g[2] = g[2] - qj * ((3.0 * rzij * rzij * F2 - d2 * F1) * dm5);
+            g[3] = g[3] - qj * ((3.0 * rxij * ryij * F2) * dm5);
+            g[4] = g[4] - qj * ((3.0 * rxij * rzij * F2) * dm5);
+            g[5] = g[5] - qj * ((3.0 * ryij * rzij * F2) * dm5);
+        }
+        for (int c = 0; c < 6; ++c) dir[(size_t)c * n + ia] = g[c];
+    }
+    std::vector<double> mu0(3 * (size_t)n, 0.0), ef, rec(9 * (size_t)n, 0.0), f(3 * (size_t)n, 0.0);
+    const bool task[6] = {true, false, false, false, false, false};
+    double u = 0.0, tau[3][3] = {{0}};
+    multipole_ES_rec(s, s->qia, mu0, task, false, true, false, false, u, ef, rec, f, tau);
+    const int comp[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    V6.assign(6 * (size_t)n, 0.0);
+    for (int c = 0; c < 6; ++c)
+        for (int ia = 0; ia < n; ++ia) {
+            const double self = c < 3 ? selfa * s->qia[ia] : 0.0;
+            V6[(size_t)c * n + ia] = dir[(size_t)c * n + ia] + rec[(size_t)(comp[c][0] * 3 + comp[c][1]) * n + ia] + self;
+        }
+}
+
+// principal values of a symmetric 3x3 tensor, ascending: cyclic Jacobi
+// rotations (Rutishauser's formulation) to convergence
+void eig3_jacobi(const double v6[6], double w[3]) {
+    double m[3][3] = {{v6[0], v6[3], v6[4]}, {v6[3], v6[1], v6[5]}, {v6[4], v6[5], v6[2]}};
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        const double off = std::fabs(m[0][1]) + std::fabs(m[0][2]) + std::fabs(m[1][2]);
+        if (off == 0.0) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                if (m[p][q] == 0.0) continue;
+                const double theta = (m[q][q] - m[p][p]) / (2.0 * m[p][q]);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < 3; ++k) {   // columns p, q
+                    const double mkp = m[k][p], mkq = m[k][q];
+                    m[k][p] = c * mkp - sn * mkq;
+                    m[k][q] = sn * mkp + c * mkq;
+                }
+                for (int k = 0; k < 3; ++k) {   // rows p, q
+                    const double mpk = m[p][k], mqk = m[q][k];
+                    m[p][k] = c * mpk - sn * mqk;
+                    m[q][k] = sn * mpk + c * mqk;
+                }
+                m[p][q] = m[q][p] = 0.0;
+            }
+    }
+    w[0] = m[0][0];
+    w[1] = m[1][1];
+    w[2] = m[2][2];
+    std::sort(w, w + 3);
+}
+
+// nmr_convention (src/efg.f90:2546-2620): (Vxx, Vyy, Vzz, eta)
+void nmr_conv(const double e[3], double nmr[4]) {
+    double diso = (e[0] + e[1] + e[2]) / 3.0;
+    if (std::fabs(diso) != 0.0 && std::fabs(diso) > 1e-3) diso = 0.0;
+    const double a1 = std::fabs(e[0] - diso), a2 = std::fabs(e[1] - diso), a3 = std::fabs(e[2] - diso);
+    double d11, d22, d33;
+    if (a1 >= a2 && a1 >= a3) {
+        d11 = e[0];
+        if (a2 >= a3) { d22 = e[1]; d33 = e[2]; } else { d22 = e[2]; d33 = e[1]; }
+    } else if (a2 >= a1 && a2 >= a3) {
+        d11 = e[1];
+        if (a1 >= a3) { d22 = e[0]; d33 = e[2]; } else { d22 = e[2]; d33 = e[0]; }
+    } else {
+        d11 = e[2];
+        if (a1 >= a2) { d22 = e[0]; d33 = e[1]; } else { d22 = e[1]; d33 = e[0]; }
+    }
+    nmr[0] = d33;
+    nmr[1] = d22;
+    nmr[2] = d11;
+    double eta = nmr[2] != 0.0 ? (nmr[0] - nmr[1]) / nmr[2] : 0.0;
+    if (nmr[0] == nmr[1]) eta = 0.0;
+    if (nmr[2] == 0.0) eta = 0.0;
+    if (std::fabs(nmr[0]) < 1.0e-5 && std::fabs(nmr[1]) < 1.0e-5 && std::fabs(nmr[2]) < 1.0e-5) eta = 0.0;
+    nmr[3] = eta;
+}
+
+struct RmcEfg {
+    const mdff_rmc_efg_params* ep;
+    int PANU, PANvzz, PANeta;
+    const double *Uexp, *Vexp, *Eexp;
+    // Fortran layouts: U (ui, mp, bin) ui fastest; vzz, eta (mp, bin) mp fastest
+    std::vector<double> U, V, E;
+};
+
+// rmc_efg (src/rmc.f90:1499-1660) with eval_chisq_Uefg/vzz/eta (:693-769):
+// chi[2..4]
+void rmc_efg_terms(orc_sys* s, RmcEfg& R, double chi[6]) {
+    const int n = s->natm, nt = s->ntype, nt1 = nt + 1;
+    const mdff_rmc_efg_params& ep = *R.ep;
+    std::vector<double> V6;
+    efg_es_rmc(s, V6);
+    std::vector<long long> cU((size_t)6 * nt1 * (R.PANU + 1), 0), cV((size_t)nt1 * (R.PANvzz + 1), 0),
+        cE((size_t)nt1 * (R.PANeta + 1), 0);
+    auto iU = [&](int ui, int mp, int bin) { return ((size_t)bin * nt1 + mp) * 6 + (ui - 1); };
+    const double sq3 = 1.0 / std::sqrt(3.0), sq32 = sq3 * 0.5;
+    for (int ia = 0; ia < n; ++ia) {
+        double v[6], w[3], nmr[4];
+        for (int c = 0; c < 6; ++c) v[c] = V6[(size_t)c * n + ia];
+        eig3_jacobi(v, w);
+        nmr_conv(w, nmr);
+        const double Ui[5] = {v[2] * 0.5, v[4] * sq3, v[5] * sq3, v[3] * sq3, (v[0] - v[1]) * sq32};
+        const double vzzk = (nmr[2] - ep.vzz_efg_min) / ep.resolution_vzz_efg;
+        const double etak = nmr[3] / ep.resolution_eta_efg;
+        // INT(x) + 1 in [0, PAN] and INT(x) in [0, PAN], with INT truncating
+        if (!(vzzk > -2.0 && vzzk < (double)R.PANvzz)) continue;
+        if (!(etak > -1.0 && etak < (double)R.PANeta + 1.0)) continue;
+        const int kvzz = (int)vzzk + 1, keta = (int)etak;
+        const int it = s->itype[ia] + 1;
+        cV[(size_t)kvzz * nt1] += 1;
+        cE[(size_t)keta * nt1] += 1;
+        cV[(size_t)kvzz * nt1 + it] += 1;
+        cE[(size_t)keta * nt1 + it] += 1;
+        if (ep.lrmc_u)
+            for (int ui = 1; ui <= 5; ++ui) {
+                const double uk = (Ui[ui - 1] - ep.u_efg_min) / ep.resolution_u_efg;
+                if (!(uk > -2.0 && uk < (double)R.PANU)) continue;
+                const int ku = (int)uk + 1;
+                cU[iU(ui, 0, ku)] += 1;
+                cU[iU(ui, it, ku)] += 1;
+                if (ui != 1) {
+                    cU[iU(6, 0, ku)] += 1;
+                    if (it <= 2) cU[iU(6, it, ku)] += 1;   // the reference's loop covers types 1 and 2
+                }
+            }
+    }
+    const double natm = (double)n;
+    if (ep.lrmc_u)
+        for (int bin = 0; bin <= R.PANU; ++bin)
+            for (int ui = 1; ui <= 5; ++ui) {
+                R.U[iU(ui, 0, bin)] = (double)cU[iU(ui, 0, bin)] / (ep.resolution_u_efg * natm);
+                for (int it = 1; it <= nt; ++it)   // the reference divides the all-types U1 counts here
+                    R.U[iU(ui, it, bin)] = (double)cU[iU(1, 0, bin)] / (ep.resolution_u_efg * (double)s->natmi[it - 1]);
+            }
+    if (ep.lrmc_eta)
+        for (int bin = 0; bin < R.PANeta; ++bin) {
+            R.E[(size_t)bin * nt1] = (double)cE[(size_t)bin * nt1] / (ep.resolution_eta_efg * natm);
+            for (int it = 1; it <= nt; ++it)
+                R.E[(size_t)bin * nt1 + it] =
+                    (double)cE[(size_t)bin * nt1 + it] / (ep.resolution_eta_efg * (double)s->natmi[it - 1]);
+        }
+    if (ep.lrmc_vzz)
+        for (int bin = 0; bin <= R.PANvzz; ++bin) {
+            R.V[(size_t)bin * nt1] = (double)cV[(size_t)bin * nt1] / (ep.resolution_vzz_efg * natm);
+            for (int it = 1; it <= nt; ++it)
+                R.V[(size_t)bin * nt1 + it] =
+                    (double)cV[(size_t)bin * nt1 + it] / (ep.resolution_vzz_efg * (double)s->natmi[it - 1]);
+        }
+    if (ep.lrmc_u) {
+        double c = 0.0;
+        for (int bin = 0; bin <= R.PANU; ++bin)
+            for (int mp = 0; mp <= nt; ++mp)
+                for (int ui = 1; ui <= 5; ++ui) {
+                    const double d = R.U[iU(ui, mp, bin)] - R.Uexp[iU(ui, mp, bin)];
+                    c = c + d * d;
+                }
+        chi[2] = c;
+    }
+    if (ep.lrmc_vzz) {
+        double c = 0.0;
+        for (int bin = 0; bin <= R.PANvzz; ++bin)
+            for (int mp = 0; mp <= nt; ++mp) {
+                const double d = R.V[(size_t)bin * nt1 + mp] - R.Vexp[(size_t)bin * nt1 + mp];
+                c = c + d * d;
+            }
+        chi[3] = c;
+    }
+    if (ep.lrmc_eta) {
+        double c = 0.0;
+        for (int bin = 0; bin <= R.PANeta; ++bin)
+            for (int mp = 0; mp <= nt; ++mp) {
+                const double d = R.E[(size_t)bin * nt1 + mp] - R.Eexp[(size_t)bin * nt1 + mp];
+                c = c + d * d;
+            }
+        chi[4] = c;
+    }
+}
+
+}  // namespace
+
+int orc_rmc_efg(orc_sys* s, const mdff_rmc_params* rp, const mdff_rmc_efg_params* ep, const double* gexp,
+                const double* Uexp, const double* Vexp, const double* Eexp, const double* uni, long long nuni,
+                double* grr_out, double* U_out, double* V_out, double* E_out, mdff_rmc_result* res) {
+    GrSpec g = gr_spec(s, rp->cut_rmc, rp->resolution_gr);
+    const int n = s->natm, nt1 = s->ntype + 1;
+    const bool any_efg = ep && (ep->lrmc_u || ep->lrmc_vzz || ep->lrmc_eta);
+    RmcEfg R;
+    if (ep) {
+        R.ep = ep;
+        R.PANU = (int)(2.0 * std::fabs(ep->u_efg_min) / ep->resolution_u_efg);
+        R.PANvzz = (int)(2.0 * std::fabs(ep->vzz_efg_min) / ep->resolution_vzz_efg);
+        R.PANeta = (int)(1.0 / ep->resolution_eta_efg);
+        R.Uexp = Uexp;
+        R.Vexp = Vexp;
+        R.Eexp = Eexp;
+        R.U.assign((size_t)6 * nt1 * (R.PANU + 1), 0.0);
+        R.V.assign((size_t)nt1 * (R.PANvzz + 1), 0.0);
+        R.E.assign((size_t)nt1 * (R.PANeta + 1), 0.0);
+    }
+    std::vector<double> aU = R.U, aV = R.V, aE = R.E;
+    std::vector<double> sx, sy, sz;
+    direct_coords(s, sx, sy, sz);
+    auto to_cart = [&]() {
+        for (int ia = 0; ia < n; ++ia) dirkar1(s->cell, sx[ia], sy[ia], sz[ia], s->rx[ia], s->ry[ia], s->rz[ia]);
+    };
     std::vector<double> calc((size_t)(g.npairs + 1) * g.nbins);
     std::vector<long long> h;
     gr_counts(s, g, sx, sy, sz, h);
     gr_normalise(s, g, h, calc.data());
     double chi_old[6] = {0, 0, 0, 0, 0, 0}, chi_new[6];
     chi_old[0] = chisq_gr(g, calc.data(), gexp);
-    chi_old[5] = chi_old[0];
     long long kall = 1, kacc = 1, u = 0;
+    if (any_efg && kacc >= ep->efg_start) {
+        to_cart();
+        rmc_efg_terms(s, R, chi_old);
+        aU = R.U; aV = R.V; aE = R.E;
+    }
+    chi_old[5] = (((chi_old[0] + chi_old[1]) + chi_old[2]) + chi_old[3]) + chi_old[4];
     int status = 0;
     const double dmax[3] = {rp->max_displacement / s->cell.anorm[0], rp->max_displacement / s->cell.anorm[1],
                             rp->max_displacement / s->cell.anorm[2]};
@@ -3150,9 +3385,14 @@ int orc_rmc(orc_sys* s, const mdff_rmc_params* rp, const double* gexp, const dou
         u += 4;
         gr_counts(s, g, sx, sy, sz, h);
         gr_normalise(s, g, h, calc.data());
+        for (int q = 0; q < 6; ++q) chi_new[q] = 0.0;
         chi_new[0] = chisq_gr(g, calc.data(), gexp);
-        for (int q = 1; q < 5; ++q) chi_new[q] = 0.0;
-        chi_new[5] = chi_new[0];
+        const bool efg_now = any_efg && kacc >= ep->efg_start;
+        if (efg_now) {
+            to_cart();
+            rmc_efg_terms(s, R, chi_new);
+        }
+        chi_new[5] = (((chi_new[0] + chi_new[1]) + chi_new[2]) + chi_new[3]) + chi_new[4];
         bool acc6 = false, stop = false;
         for (int q = 0; q < 6; ++q) {   // src/rmc.f90:521-540
             double dq = chi_new[q] - chi_old[q];
@@ -3166,7 +3406,7 @@ int orc_rmc(orc_sys* s, const mdff_rmc_params* rp, const double* gexp, const dou
             }
             if (q == 5) acc6 = a;
         }
-        if (stop) {
+        if (stop) {   // the uniforms ran out: the trial is undone exactly
             for (int d = 0; d < 3; ++d) *sv[d] = sold[d];
             status = 1;
             --kall;
@@ -3175,14 +3415,20 @@ int orc_rmc(orc_sys* s, const mdff_rmc_params* rp, const double* gexp, const dou
         if (acc6) {
             ++kacc;
             for (int q = 0; q < 6; ++q) chi_old[q] = chi_new[q];
+            if (efg_now) { aU = R.U; aV = R.V; aE = R.E; }
         } else {
             for (int d = 0; d < 3; ++d) *sv[d] = snew[d] - disp[d];   // src/rmc.f90:628-636
         }
     }
-    for (int ia = 0; ia < n; ++ia) dirkar1(s->cell, sx[ia], sy[ia], sz[ia], s->rx[ia], s->ry[ia], s->rz[ia]);
+    to_cart();
     if (grr_out) {
         gr_counts(s, g, sx, sy, sz, h);
         gr_normalise(s, g, h, grr_out);
+    }
+    if (ep) {
+        if (U_out) std::copy(aU.begin(), aU.end(), U_out);
+        if (V_out) std::copy(aV.begin(), aV.end(), V_out);
+        if (E_out) std::copy(aE.begin(), aE.end(), E_out);
     }
     if (res) {
         res->kall = kall;
@@ -3193,6 +3439,19 @@ int orc_rmc(orc_sys* s, const mdff_rmc_params* rp, const double* gexp, const dou
         res->pad = 0;
     }
     return 0;
+}
+
+int orc_efg_rmc(orc_sys* s, double* out6) {
+    std::vector<double> V6;
+    efg_es_rmc(s, V6);
+    std::copy(V6.begin(), V6.end(), out6);
+    return 0;
+}
+
+int orc_rmc(orc_sys* s, const mdff_rmc_params* rp, const double* gexp, const double* uni, long long nuni,
+            double* grr_out, mdff_rmc_result* res) {
+    return orc_rmc_efg(s, rp, nullptr, gexp, nullptr, nullptr, nullptr, uni, nuni, grr_out, nullptr, nullptr, nullptr,
+                       res);
 }
 
 int orc_md_start(orc_sys* s, const double* vx, const double* vy, const double* vz, mdff_thermo* t0) {

@@ -95,3 +95,48 @@ def test_rmc_rejects_bad_parameters():
     rp = rmc_params(10, 10, 2.0, 0.05, temp=0.0)
     with pytest.raises(mdff_b200.EngineError):
         e.rmc(rp, np.zeros((2, 41)))
+
+
+# ---- the EFG chi^2 terms: mdff_rmc_efg against the oracle's rmc_efg chain ----
+
+from test_oracle_rmc import distributions, efg_params, rigid_mgo, rmc_par   # noqa: E402
+
+
+@pytest.mark.parametrize("terms", ["all", "vzz_eta"])
+def test_rmc_efg_chain_matches_oracle(terms):
+    # the same uniforms: the same decisions, the same final configuration and
+    # distributions.  The engine's EFG (the MD path within rc) and the
+    # oracle's multipole_efg_ES (every minimum image) agree to ~1e-10 at
+    # alpha rc ~ 5, far inside the bins; the histograms then agree exactly
+    ep = efg_params()
+    if terms == "vzz_eta":
+        ep.lrmc_u = 0
+    t = rigid_mgo(seed=7, jitter=0.15)
+    g, U, V, E, _ = distributions(t, efg_params())
+    s = rigid_mgo()
+    u = np.random.default_rng(11).random(20000)
+    rp = rmc_par(60, 800)
+    e = mdff_b200.Engine(s["params"], s["itype"], s["pos"], s["cell"])
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    re, ge, Ue, Ve, Ee = e.rmc_efg(rp, ep, g, U, V, E, u)
+    ro, go, Uo, Vo, Eo = o.rmc_efg(rp, ep, g, U, V, E, u)
+    assert re["status"] == ro["status"] == 0
+    assert (re["kall"], re["kacc"], re["uniforms_used"]) == (ro["kall"], ro["kacc"], ro["uniforms_used"])
+    assert re["kacc"] > 5
+    assert re["chisq"][0] == ro["chisq"][0]
+    for q in range(2, 6):
+        assert abs(re["chisq"][q] - ro["chisq"][q]) <= 1e-12 * max(1.0, ro["chisq"][q])
+    assert np.array_equal(ge, go)
+    assert np.array_equal(Ve, Vo) and np.array_equal(Ee, Eo)
+    if ep.lrmc_u:
+        assert np.array_equal(Ue, Uo)
+    assert np.max(np.abs(e.positions() - o.positions())) < 1e-12
+
+
+def test_rmc_efg_rejects_polarisable_systems():
+    s = mgo()
+    e = mdff_b200.Engine(s["params"], s["itype"], s["pos"], s["cell"])
+    ep = efg_params()
+    su, sv, se = ep.shapes(s["params"].ntype)
+    with pytest.raises(mdff_b200.EngineError):
+        e.rmc_efg(rmc_params(10, 10, 6.0, 0.1), ep, np.zeros((4, 61)), np.zeros(su), np.zeros(sv), np.zeros(se))

@@ -79,3 +79,116 @@ def test_stream_running_out_stops_cleanly():
     o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
     r, _ = o.rmc(rmc_params(10 ** 6, 10 ** 6), gexp, np.random.default_rng(2).random(103))
     assert r["status"] == 1 and r["uniforms_used"] <= 103
+
+
+# ---- the EFG chi^2 terms (rmc_efg, src/rmc.f90:1499-1660) ----
+
+def rigid_mgo(grid=(4, 4, 4), rc=4.1, alpha=1.25, kmax=12, seed=2, jitter=0.05):
+    """Rigid-ion MgO (the PIM cell without polarisabilities): rmc_main's EFG
+    is that of the point charges.  alpha * rc ~ 5 makes the real-space terms
+    beyond rc negligible, so the MD path's EFG (within rc) and
+    multipole_efg_ES (every minimum image) agree to ~1e-10.  An even grid
+    keeps the cell neutral (a charged one gives every tensor a trace)."""
+    s = systems.mgo_pim(grid=grid, rc=rc, alpha=alpha, kmax=kmax, vacancy_frac=0.0, seed=seed, jitter=jitter)
+    p = s["params"]
+    for t in range(p.ntype):
+        p.ldip_polar[t] = 0
+        p.poldip_iso[t] = 0.0
+    p.doefg = 1
+    return s
+
+
+def efg_params():
+    ep = abi.RmcEfgParams()
+    ep.lrmc_u = ep.lrmc_vzz = ep.lrmc_eta = 1
+    ep.efg_start = 0
+    ep.resolution_u_efg, ep.u_efg_min = 0.05, -3.0
+    ep.resolution_vzz_efg, ep.vzz_efg_min = 0.05, -4.0
+    ep.resolution_eta_efg = 0.05
+    return ep
+
+
+def rmc_par(acc, trials, cut=4.0, res=0.1, temp=1e-3):
+    rp = abi.RmcParams()
+    rp.max_displacement, rp.resolution_gr, rp.cut_rmc = 0.1, res, cut
+    for q in range(6):
+        rp.temp_rmc[q] = temp
+    rp.acceptance_max, rp.max_trials = acc, trials
+    return rp
+
+
+def distributions(s, ep):
+    """rmc_efg's distributions of a configuration: the chain's start with no trial."""
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    su, sv, se = ep.shapes(s["params"].ntype)
+    g = o.gr(4.0, 0.1)
+    r, _, U, V, E = o.rmc_efg(rmc_par(1, 1), ep, g, np.zeros(su), np.zeros(sv), np.zeros(se), [])
+    return g, U, V, E, r
+
+
+def test_efg_of_rmc_is_the_point_charge_ewald_efg():
+    # multipole_efg_ES (every minimum image, no coul_unit) against the MD
+    # path's Ewald EFG (within rc, times coul_unit)
+    s = rigid_mgo()
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    V = o.efg_rmc()
+    md = o.engforce()["efg"]
+    cu = 14.399645   # e^2 / (4 pi eps0 A) in eV
+    assert np.max(np.abs(md / cu - V)) < 1e-6 * np.max(np.abs(V))
+    ratio = md[np.abs(V) > 0.1] / V[np.abs(V) > 0.1]
+    assert np.ptp(ratio) < 1e-8 * np.mean(ratio)
+
+
+def test_rmc_efg_distributions_and_quirks():
+    s = rigid_mgo()
+    ep = efg_params()
+    _, U, V, E, r = distributions(s, ep)
+    n, natmi = len(s["itype"]), np.bincount(np.asarray(s["itype"]) - 1)   # itype is 1-based
+    # every site inside the Vzz and eta ranges: the all-sites rows integrate to 1
+    assert abs(V[:, 0].sum() * ep.resolution_vzz_efg - 1.0) < 1e-12
+    assert abs(E[:, 0].sum() * ep.resolution_eta_efg - 1.0) < 1e-12
+    for t in range(2):
+        assert abs(V[:, 1 + t].sum() * ep.resolution_vzz_efg - 1.0) < 1e-12
+    # the reference's per-type U rows divide the all-types U1 counts
+    for t in range(2):
+        assert np.allclose(U[:, 1 + t, :5], (U[:, 0, 0] * n / natmi[t])[:, None], rtol=1e-14, atol=0)
+    assert not U[:, :, 5].any() and not E[-1].any()
+    # chi^2 against itself is zero; the total is the sum of the terms
+    g, U2, V2, E2, r2 = distributions(s, ep)
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    r3, *_ = o.rmc_efg(rmc_par(1, 1), ep, g, U, V, E, [])
+    assert r3["chisq"] == [0.0] * 6
+    assert r["chisq"][5] == sum(r["chisq"][:5])
+
+
+def test_rmc_efg_chain_fits_the_target():
+    ep = efg_params()
+    t = rigid_mgo(seed=7, jitter=0.15)
+    g, U, V, E, _ = distributions(t, ep)
+    s = rigid_mgo()
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    r0, *_ = o.rmc_efg(rmc_par(1, 1), ep, g, U, V, E, [])
+    u = np.random.default_rng(7).random(40000)
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    r, g1, U1, V1, E1 = o.rmc_efg(rmc_par(200, 3000), ep, g, U, V, E, u)
+    assert r["status"] == 0 and r["kacc"] > 10
+    assert r["chisq"][5] < 0.5 * r0["chisq"][5]
+    # the reported chi^2 and distributions are those of the final configuration
+    o2 = oracle.Oracle(s["params"], s["itype"], o.positions(), s["cell"])
+    rf, gf, Uf, Vf, Ef = o2.rmc_efg(rmc_par(1, 1), ep, g, U, V, E, [])
+    assert np.array_equal(Uf, U1) and np.array_equal(Vf, V1) and np.array_equal(Ef, E1)
+    assert abs(rf["chisq"][5] - r["chisq"][5]) <= 1e-9 * r["chisq"][5]
+
+
+def test_rmc_efg_start_delays_the_efg_terms():
+    ep = efg_params()
+    ep.efg_start = 10 ** 6
+    t = rigid_mgo(seed=7, jitter=0.15)
+    g, U, V, E, _ = distributions(t, efg_params())
+    s = rigid_mgo()
+    u = np.random.default_rng(3).random(5000)
+    a = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"]).rmc_efg(rmc_par(20, 300), ep, g, U, V, E, u)
+    b = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"]).rmc(rmc_par(20, 300), g, u)
+    assert a[0]["chisq"][2:5] == [0.0, 0.0, 0.0]
+    assert (a[0]["kall"], a[0]["kacc"], a[0]["uniforms_used"]) == (b[0]["kall"], b[0]["kacc"], b[0]["uniforms_used"])
+    assert np.array_equal(a[1], b[1])

@@ -140,6 +140,11 @@ module mdff_engine
     real(c_double) :: chisq(6)
     integer(c_int) :: status, pad
   end type mdff_rmc_result_t
+  ! rmctag's EFG terms (src/rmc.f90:40-60)
+  type, bind(C) :: mdff_rmc_efg_params_t
+    integer(c_int) :: lrmc_u, lrmc_vzz, lrmc_eta, efg_start
+    real(c_double) :: resolution_u_efg, u_efg_min, resolution_vzz_efg, vzz_efg_min, resolution_eta_efg
+  end type mdff_rmc_efg_params_t
 
   integer(c_int), parameter :: MDFF_FILE_TRAJFF = 0, MDFF_FILE_CONTFF = 1, MDFF_FILE_EFGALL = 2, &
                                MDFF_FILE_DIPFF = 3, MDFF_FILE_EFALL = 4, MDFF_DATA_V = 1, MDFF_DATA_F = 2
@@ -292,6 +297,20 @@ module mdff_engine
       import :: c_int, c_ptr, c_double, c_long_long, mdff_rmc_params_t, mdff_rmc_result_t
       type(c_ptr), value :: ctx, uniforms, grr_out
       type(mdff_rmc_params_t), intent(in) :: rp
+      real(c_double), intent(in) :: grr_exp(*)
+      integer(c_long_long), value :: nuni, seed
+      type(mdff_rmc_result_t), intent(out) :: res
+    end function
+
+    ! rmc_main with its EFG terms: dibU_exp(6, 0:ntype, 0:PANU), dibvzz_exp(0:ntype, 0:PANvzz),
+    ! dibeta_exp(0:ntype, 0:PANeta) as rmc_main allocates them (c_null_ptr for an inactive term)
+    integer(c_int) function mdff_rmc_efg(ctx, rp, ep, grr_exp, dibU_exp, dibvzz_exp, dibeta_exp, uniforms, nuni, &
+                                         seed, grr_out, dibU_out, dibvzz_out, dibeta_out, res) &
+        bind(C, name="mdff_rmc_efg")
+      import :: c_int, c_ptr, c_double, c_long_long, mdff_rmc_params_t, mdff_rmc_efg_params_t, mdff_rmc_result_t
+      type(c_ptr), value :: ctx, dibU_exp, dibvzz_exp, dibeta_exp, uniforms, grr_out, dibU_out, dibvzz_out, dibeta_out
+      type(mdff_rmc_params_t), intent(in) :: rp
+      type(mdff_rmc_efg_params_t), intent(in) :: ep
       real(c_double), intent(in) :: grr_exp(*)
       integer(c_long_long), value :: nuni, seed
       type(mdff_rmc_result_t), intent(out) :: res

@@ -225,7 +225,8 @@ typedef struct mdff_efg_dist_params {
 /* sizeof(mdff_params), sizeof(mdff_energies), sizeof(mdff_thermo),
  * sizeof(mdff_param_grad), sizeof(mdff_opt_result) for which = 0 .. 4 (lets a binding check its
  * mirror of these structs); no reference counterpart. */
-int  mdff_struct_size(int which);   /* 5 efg_dist_params, 6 frame_header, 7 rmc_params, 8 rmc_result */
+int  mdff_struct_size(int which);   /* 5 efg_dist_params, 6 frame_header, 7 rmc_params, 8 rmc_result,
+                                       9 rmc_efg_params */
 
 /* Measured FMA throughput of the device in TFLOP/s: out[0] FP64, out[1]
  * FP32, out[2] packed FP32x2 (fma.rn.f32x2).  The roofline denominators of

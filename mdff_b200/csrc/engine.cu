@@ -2438,6 +2438,7 @@ int mdff_struct_size(int which) {
         case 6: return (int)sizeof(mdff_frame_header);
         case 7: return (int)sizeof(mdff_rmc_params);
         case 8: return (int)sizeof(mdff_rmc_result);
+        case 9: return (int)sizeof(mdff_rmc_efg_params);
         default: return -1;
     }
 }

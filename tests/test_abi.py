@@ -38,6 +38,7 @@ def test_struct_sizes_match():
     assert L.mdff_struct_size(6) == C.sizeof(abi.FrameHeader)
     assert L.mdff_struct_size(7) == C.sizeof(abi.RmcParams)
     assert L.mdff_struct_size(8) == C.sizeof(abi.RmcResult)
+    assert L.mdff_struct_size(9) == C.sizeof(abi.RmcEfgParams)
 
 
 def test_defaults_match_library():

@@ -1004,6 +1004,16 @@ def run_rmc(args):
         e1.record(ext2)
         e1.synchronize()
         ems = e0.elapsed_time(e1)
+        # where a move's time goes: a profiled pass of the same length
+        er.set_positions(pos0)
+        er.enable_profile(True)
+        er.profile_reset()
+        t0 = time.perf_counter()
+        rq, *_ = er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=7)
+        wall_ms = (time.perf_counter() - t0) * 1e3
+        kprof = {k: round(v["ms"] / max(1, rq["kall"] - 1), 4) for k, v in er.profile().items()
+                 if v["count"] > 0 and not k.startswith("_")}
+        er.enable_profile(False)
         er.close()
         if result is not None:
             result["efg_terms"] = {
@@ -1012,6 +1022,8 @@ def run_rmc(args):
                 "value": (rr["kall"] - 1) / (ems / 1e3), "unit": "moves/s", "moves": rr["kall"] - 1,
                 "accepted": rr["kacc"] - 1, "ms_per_move": ems / max(1, rr["kall"] - 1),
                 "chisq_last": rr["chisq"], "bins": {"U": su, "vzz": sv, "eta": se},
+                "kernels_ms_per_move": kprof,
+                "profiled_wall_ms_per_move": wall_ms / max(1, rq["kall"] - 1),
                 "note": "one full-device Ewald EFG evaluation of the trial configuration per move, as rmc_efg "
                         "computes it (multipole_efg_ES)"}
     if result is not None:

@@ -974,58 +974,65 @@ def run_rmc(args):
         # the EFG chi^2 terms (rmc_efg): the same cell as rigid ions (the
         # reference's rmc_efg takes point charges), U, Vzz and eta fitted to
         # the distributions of the perturbed target, every trial one Ewald
-        # EFG of the whole trial configuration
-        pr = type(p).from_buffer_copy(p)
-        for t in range(pr.ntype):
-            pr.ldip_polar[t] = 0
-            pr.poldip_iso[t] = 0.0
-        pr.doefg = 1
-        er = mdff_b200.Engine(pr, s["itype"], tgt, s["cell"])
-        ep = abi.RmcEfgParams()
-        ep.lrmc_u = ep.lrmc_vzz = ep.lrmc_eta = 1
-        ep.resolution_u_efg, ep.u_efg_min = 0.02, -1.0
-        ep.resolution_vzz_efg, ep.vzz_efg_min = 0.02, -2.0
-        ep.resolution_eta_efg = 0.02
-        su, sv, se = ep.shapes(pr.ntype)
-        r1 = abi.RmcParams.from_buffer_copy(rp)
-        r1.acceptance_max, r1.max_trials = 1, 1
-        _, _, Ux, Vx, Ex = er.rmc_efg(r1, ep, gexp, np.zeros(su), np.zeros(sv), np.zeros(se))
-        er.set_positions(pos0)
-        r1.acceptance_max, r1.max_trials = 10 ** 12, 4
-        er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=5)   # warm-up
-        er.set_positions(pos0)
-        r1.max_trials = args.rmc_efg_moves + 1
-        ext2 = torch.cuda.ExternalStream(er.stream(), device=device)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize(device)
-        e0.record(ext2)
-        rr, *_ = er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=7)
-        e1.record(ext2)
-        e1.synchronize()
-        ems = e0.elapsed_time(e1)
-        # where a move's time goes: a profiled pass of the same length
-        er.set_positions(pos0)
-        er.enable_profile(True)
-        er.profile_reset()
-        t0 = time.perf_counter()
-        rq, *_ = er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=7)
-        wall_ms = (time.perf_counter() - t0) * 1e3
-        kprof = {k: round(v["ms"] / max(1, rq["kall"] - 1), 4) for k, v in er.profile().items()
-                 if v["count"] > 0 and not k.startswith("_")}
-        er.enable_profile(False)
-        er.close()
+        # EFG of the whole trial configuration; on the FP64 path and on the
+        # mixed one, Verlet lists with the chain's own validity tracking
+        efg_runs = {}
+        for prec_name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+            pr = type(p).from_buffer_copy(p)
+            for t in range(pr.ntype):
+                pr.ldip_polar[t] = 0
+                pr.poldip_iso[t] = 0.0
+            pr.doefg = 1
+            pr.precision = prec
+            pr.lvnlist = 1
+            pr.skindiff = max(pr.skindiff, 1.0)
+            er = mdff_b200.Engine(pr, s["itype"], tgt, s["cell"])
+            ep = abi.RmcEfgParams()
+            ep.lrmc_u = ep.lrmc_vzz = ep.lrmc_eta = 1
+            ep.resolution_u_efg, ep.u_efg_min = 0.02, -1.0
+            ep.resolution_vzz_efg, ep.vzz_efg_min = 0.02, -2.0
+            ep.resolution_eta_efg = 0.02
+            su, sv, se = ep.shapes(pr.ntype)
+            r1 = abi.RmcParams.from_buffer_copy(rp)
+            r1.acceptance_max, r1.max_trials = 1, 1
+            _, _, Ux, Vx, Ex = er.rmc_efg(r1, ep, gexp, np.zeros(su), np.zeros(sv), np.zeros(se))
+            er.set_positions(pos0)
+            r1.acceptance_max, r1.max_trials = 10 ** 12, 4
+            er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=5)   # warm-up
+            er.set_positions(pos0)
+            r1.max_trials = args.rmc_efg_moves + 1
+            ext2 = torch.cuda.ExternalStream(er.stream(), device=device)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(device)
+            e0.record(ext2)
+            rr, *_ = er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=7)
+            e1.record(ext2)
+            e1.synchronize()
+            ems = e0.elapsed_time(e1)
+            # where a move's time goes: a profiled pass of the same length
+            er.set_positions(pos0)
+            er.enable_profile(True)
+            er.profile_reset()
+            t0 = time.perf_counter()
+            rq, *_ = er.rmc_efg(r1, ep, gexp, Ux, Vx, Ex, seed=7)
+            wall_ms = (time.perf_counter() - t0) * 1e3
+            kprof = {k: round(v["ms"] / max(1, rq["kall"] - 1), 4) for k, v in er.profile().items()
+                     if v["count"] > 0 and not k.startswith("_")}
+            er.enable_profile(False)
+            er.close()
+            efg_runs[prec_name] = {"value": (rr["kall"] - 1) / (ems / 1e3), "moves": rr["kall"] - 1,
+                                   "accepted": rr["kacc"] - 1, "ms_per_move": ems / max(1, rr["kall"] - 1),
+                                   "chisq_last": rr["chisq"], "kernels_ms_per_move": kprof,
+                                   "profiled_wall_ms_per_move": wall_ms / max(1, rq["kall"] - 1)}
         if result is not None:
             result["efg_terms"] = {
                 "metric": "reverse Monte Carlo trial moves/s with the g(r), U, Vzz and eta chi^2 terms, 32k-ion "
                           "rigid-ion MgO",
-                "value": (rr["kall"] - 1) / (ems / 1e3), "unit": "moves/s", "moves": rr["kall"] - 1,
-                "accepted": rr["kacc"] - 1, "ms_per_move": ems / max(1, rr["kall"] - 1),
-                "chisq_last": rr["chisq"], "bins": {"U": su, "vzz": sv, "eta": se},
-                "kernels_ms_per_move": kprof,
-                "profiled_wall_ms_per_move": wall_ms / max(1, rq["kall"] - 1),
+                "value": efg_runs["mixed"]["value"], "unit": "moves/s", "bins": {"U": su, "vzz": sv, "eta": se},
+                "fp64": efg_runs["fp64"], "mixed": efg_runs["mixed"],
                 "note": "one full-device Ewald EFG evaluation of the trial configuration per move, as rmc_efg "
-                        "computes it (multipole_efg_ES)"}
+                        "computes it (multipole_efg_ES); value = the mixed path"}
     if result is not None:
         if not args.no_cpu:
             import oracle

@@ -3941,8 +3941,12 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     CK(cudaMemcpyAsync(sh.data(), s, sizeof(double) * sh.size(), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     TRY(check_launch(ctx, "rmc_efg start"));
+    // the chain needs the EFG alone: the short-range pair terms are switched
+    // off for its evaluations (and their lists for its rebuilds), then restored
     const int saved_doefg = ctx->p.doefg;
+    const int saved_nonb[4] = {ctx->p.lnmlj, ctx->p.lbmhft, ctx->p.lbmhftd, ctx->p.lmorse};
     ctx->p.doefg = 1;
+    ctx->p.lnmlj = ctx->p.lbmhft = ctx->p.lbmhftd = ctx->p.lmorse = 0;
     std::vector<double> calc(ncalc), cU(nU, 0.0), cV(nV, 0.0), cE(nE, 0.0), aU(nU, 0.0), aV(nV, 0.0), aE(nE, 0.0);
     // Verlet-list validity: an atom's summed trial displacements since the
     // last build stay below half the skin
@@ -4085,6 +4089,10 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     }();
 #undef CK_R
     ctx->p.doefg = saved_doefg;
+    ctx->p.lnmlj = saved_nonb[0];
+    ctx->p.lbmhft = saved_nonb[1];
+    ctx->p.lbmhftd = saved_nonb[2];
+    ctx->p.lmorse = saved_nonb[3];
     for (void* q : {(void*)s, (void*)hd, (void*)dh, (void*)ce}) cudaFreeAsync(q, ctx->st);
     cudaStreamSynchronize(ctx->st);
     if (rc != MDFF_OK) return rc;

@@ -339,6 +339,37 @@ class Engine:
                                         _ip(hv), _ip(he), _ip(hu), _ip(hs)))
         return {"stats": stats, "mU": mU, "m2U": m2U, "vzz": hv, "eta": he, "u": hu, "s": hs}
 
+    def efgcalc(self, frames, dist=None, efgall=None, iformat=1, system="", labels=()):
+        """calc = 'efg' (efgcalc, src/efg.f90:325-660): for each configuration
+        of a TRAJFF -- frames from io.read_trajff, or a path to read -- the
+        Ewald EFG of the engine's system at those positions (with induced
+        dipoles where the system is polarisable, as get_moments gives them),
+        written to an EFGALL when efgall names one (write_EFGALL's layout,
+        iformat 1 formatted / 0 unformatted), then efg_stat over all of them
+        when dist (abi.EfgDistParams) is given.  Returns (efg [nconf][natm][6]
+        with coul_unit, efg_dist's result or None).  The engine needs
+        doefg = 1."""
+        from . import io as _io
+        if isinstance(frames, (str, os.PathLike)):
+            frames = _io.read_trajff(frames)
+        out = np.empty((len(frames), self.n, 6))
+        w = open(efgall, "wb") if efgall else None
+        try:
+            for k, fr in enumerate(frames):
+                if fr["natm"] != self.n:
+                    raise ValueError(f"configuration {k}: {fr['natm']} atoms, the engine has {self.n}")
+                self.set_cell(np.asarray(fr["cell"], dtype=np.float64))
+                self.set_positions(fr["r"])
+                out[k] = self.engforce()["efg"]
+                if w is not None:
+                    h = _io.header(system or fr.get("system", ""), labels or fr.get("labels", ()),
+                                   natmi=fr.get("natmi", ()), cell=fr["cell"], natm=self.n)
+                    w.write(_io.format_frame("EFGALL", iformat, 0, h, self.itype, out[k].T))
+        finally:
+            if w is not None:
+                w.close()
+        return out, (self.efg_dist(dist, out) if dist is not None else None)
+
     def checkpoint(self):
         """The whole time-integration state as bytes (mdff_checkpoint_save)."""
         n = C.c_size_t()

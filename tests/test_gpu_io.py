@@ -183,3 +183,35 @@ def test_checkpoint_of_another_setup_is_refused():
     assert ei.value.code == abi.E_ARG
     with pytest.raises(mdff_b200.EngineError):
         e.restore(ck[:-8])
+
+
+def test_efgcalc_over_a_trajff(tmp_path):
+    # calc = 'efg' (efgcalc, src/efg.f90:325-660): the configurations of a
+    # TRAJFF, the EFG of each (FP64, with induced dipoles) against the
+    # oracle's, EFGALL written and read back, efg_stat over all of them
+    import oracle
+    s = pim(mixed=False)
+    e = engine(s)
+    rng = np.random.default_rng(4)
+    confs = [np.asarray(s["pos"]) + rng.normal(0.0, 0.05, np.shape(s["pos"])) for _ in range(3)]
+    labels = ["O", "Mg"]
+    it = np.asarray(s["itype"], dtype=np.int32)
+    natmi = [int(np.sum(it == 1)), int(np.sum(it == 2))]
+    h = io.header("MgO", labels, natmi=natmi, cell=np.asarray(s["cell"]).T, natm=e.n)
+    traj = tmp_path / "TRAJFF"
+    traj.write_bytes(b"".join(io.format_frame("TRAJFF", 1, "rnn", h, it, np.ascontiguousarray(r.T)) for r in confs))
+    dist = abi.EfgDistParams()
+    dist.vzzmin, dist.resvzz, dist.reseta, dist.umin, dist.resu, dist.smax = -4.0, 0.05, 0.05, -3.0, 0.05, 4.0
+    efg, st = e.efgcalc(str(traj), dist, efgall=str(tmp_path / "EFGALL"), labels=labels, system="MgO")
+    assert efg.shape == (3, e.n, 6)
+    for k, r in enumerate(io.read_trajff(str(traj))):
+        ref = oracle.Oracle(s["params"], s["itype"], r["r"], r["cell"]).engforce()["efg"]
+        assert np.max(np.abs(efg[k] - ref)) < 1e-9 * np.max(np.abs(ref))
+    back = io.read_efgall(str(tmp_path / "EFGALL"), 1)
+    assert len(back) == 3
+    for k in range(3):
+        assert np.max(np.abs(back[k]["efg"] - efg[k])) <= 1e-11 * np.max(np.abs(efg[k]))
+    direct = e.efg_dist(dist, efg)
+    for key in ("vzz", "eta", "u", "s"):
+        assert np.array_equal(st[key], direct[key])
+    assert np.array_equal(st["stats"], direct["stats"])

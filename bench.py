@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true",
+                    help="skip the FP64 arms and the mixed-vs-FP64 errors of the default (mixed) run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stream", action="store_true",
                     help="skip the trajectory-streaming measurement of the production workload")
@@ -172,6 +174,91 @@ def barrier(dist, device):
             dist.barrier(device_ids=[device.index])
         else:
             dist.barrier()
+
+
+def copy_params(p):
+    from mdff_b200 import abi
+    q = abi.Params()
+    C.pointer(q)[0] = p
+    return q
+
+
+def timed_md(eng, vel, steps, warmup, device, dist):
+    """md_start, W untimed steps, then K timed MD steps between CUDA events on
+    the engine's own stream (barrier + synchronize on both sides).  Returns the
+    device milliseconds of the K steps and their thermodynamics."""
+    import torch
+    ext = torch.cuda.ExternalStream(eng.stream(), device=device)
+    eng.md_start(vel)
+    if warmup:
+        eng.step(warmup, thermo=False)
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(ext)
+    out = eng.step(steps, thermo=True)
+    ev1.record(ext)
+    ev1.synchronize()
+    torch.cuda.synchronize(device)
+    return ev0.elapsed_time(ev1), out
+
+
+def fp64_arms(s, pm, args, device, dist):
+    """The plain FP64 GPU path on the same cell, steps and warm-up as the mixed
+    arm, twice: (a) the reference's whole half space of k-vectors and its
+    sequence of reciprocal evaluations (kspace_reuse off), and (b) the same
+    k sphere (fp64_keps = mixed_keps) and structure-factor reuse as the mixed
+    arm, so that the ratio (b) isolates precision.  Then, at the positions the
+    FP64 trajectory (a) reached, one force evaluation of each path: the errors
+    of the mixed path (and of the FP64 sphere) against plain FP64 as global
+    relative norms ||x - x_fp64|| / ||x_fp64||."""
+    import mdff_b200
+    from mdff_b200 import abi
+    natm = len(s["itype"])
+    arms, last = {}, None
+    cases = (("fp64", 0.0, 0), ("fp64_sphere_reuse", pm.mixed_keps, 1))
+    for name, keps, reuse in cases:
+        pf = copy_params(pm)
+        pf.precision = abi.PREC_FP64
+        pf.fp64_keps = keps
+        pf.kspace_reuse = reuse
+        e = mdff_b200.Engine(pf, s["itype"], s["pos"], s["cell"])
+        e.enable_profile(False)
+        ms, out = timed_md(e, s["vel"], args.steps, args.warmup, device, dist)
+        ki = e.kspace_info()
+        arms[name] = {"value": whole_job_rate(natm * args.steps, ms / 1e3, dist, device), "unit": "atom-steps/s",
+                      "ms_per_step": max_over_ranks(ms, dist, device) / args.steps, "steps": args.steps,
+                      "warmup": args.warmup, "k_vectors": ki["main"], "fp64_keps": keps, "kspace_reuse": reuse,
+                      "solver_iters_mean": float(np.mean([t["scf_iter"] for t in out["thermo"]]))}
+        if name == "fp64":
+            last = e.positions()
+        e.close()
+    res = {}
+    for name, pp in (("fp64", None), ("fp64_sphere_reuse", None), ("mixed", pm)):
+        if pp is None:
+            pp = copy_params(pm)
+            pp.precision = abi.PREC_FP64
+            pp.fp64_keps = 0.0 if name == "fp64" else pm.mixed_keps
+            pp.kspace_reuse = 0 if name == "fp64" else 1
+        pp = copy_params(pp)
+        pp.doefg = 1
+        pp.efg_period = 0
+        e = mdff_b200.Engine(pp, s["itype"], last, s["cell"])
+        res[name] = e.engforce()
+        e.close()
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    b = res["fp64"]
+
+    def errs(a):
+        return {"eps_F": rel(a["f"], b["f"]), "eps_mu": rel(a["mu"], b["mu"]), "eps_efg": rel(a["efg"], b["efg"]),
+                "eps_tau": rel(a["tau_coul"] + a["tau_nonb"], b["tau_coul"] + b["tau_nonb"]),
+                "rel_u_coul": abs(a["e"]["u_coul"] - b["e"]["u_coul"]) / abs(b["e"]["u_coul"])}
+    acc = {"positions": "the FP64 trajectory's after %d + %d steps" % (args.warmup, args.steps),
+           "against": "plain FP64 path (whole half space, %d k-vectors)" % arms["fp64"]["k_vectors"],
+           "mixed": errs(res["mixed"]), "fp64_sphere_reuse": errs(res["fp64_sphere_reuse"]),
+           "definition": "global relative norms over all atoms and components (stress: total tau, Frobenius)"}
+    return arms, acc
 
 
 def run_engine(args):
@@ -314,13 +401,16 @@ def run_engine(args):
     det = eng.profile_detail()
     eng.enable_profile(False)
     iters_p = [t["scf_iter"] for t in outp["thermo"]]
+    arms = acc = None
+    if args.precision == "mixed" and not args.no_fp64:
+        arms, acc = fp64_arms(s, p, args, device, dist)
     result = None
     if rank == 0:
         pipes = mdff_b200.measure_pipes(local)
         ki = eng.kspace_info()
         # algorithmic k-vectors per evaluation: the reference's half space on
         # the FP64 path; the FP32 set plus the FP64 low set on the mixed path
-        nk_eff = (ki["fp32"] + ki["low"]) if args.precision == "mixed" else ki["half"]
+        nk_eff = ki["main"] + ki["low"]
         mean_it = float(np.mean(iters))
         mean_it_p = float(np.mean(iters_p))
         kern = {k: v for k, v in prof.items() if v["count"] > 0 and not k.startswith("_")}
@@ -416,6 +506,10 @@ def run_engine(args):
             "kernels_ms_per_step": {k: round(v["ms"] / kp, 4) for k, v in kern.items()},
             "roofline": roof,
             "e2e": e2e,
+            "fp64_arms": arms,
+            "speedup_vs_fp64": value / arms["fp64"]["value"] if arms else None,
+            "speedup_vs_fp64_sphere_reuse": value / arms["fp64_sphere_reuse"]["value"] if arms else None,
+            "accuracy_vs_fp64": acc,
             "stream": stream,
             "step0": {"h_tot": t0["h_tot"], "temp_r": t0["temp_r"], "scf_iter": t0["scf_iter"]},
         }
@@ -441,7 +535,7 @@ def cpu_baseline(s, p, iters_per_step, kstride=16):
     t_eval = td + tr * kstride
     t_step = (iters_per_step + 2) * t_eval + tp
     natm = len(s["itype"])
-    return {"value": natm / t_step, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+    return {"value": natm / t_step, "unit": "atom-steps/s", "cores": cores, "kind": "port", "host": host_cpu(),
             "sample": "one Ewald field evaluation of the 32440-ion cell (real space + every %dth k-vector, scaled) "
                       "and one BMHFTD pair loop, x (%.1f solver iterations + 2) evaluations per MD step"
                       % (kstride, iters_per_step),
@@ -505,12 +599,33 @@ def run_accuracy(args):
             "eps_F_max": max(x["eps_F"] for x in snaps)}
 
 
+def host_cpu():
+    """The host's logical CPU count and model name (from /proc/cpuinfo)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
+
+
 def run_reference(args):
-    """Reference arm: the CPU oracle (C++ port of the reference's FP64 path;
-    the Fortran/MPI reference cannot be built on this image) on all host cores,
-    same workload, each step a bounded sample (one field evaluation over 1/16
-    of the k-vectors plus the real-space sum and pair loop, scaled to a full
-    MD step of the reference's fixed-point dipole iteration)."""
+    """Reference arm: the CPU oracle (C++ FP64 restatement of the reference's
+    path; the Fortran/MPI reference cannot be built on this image) on all host
+    cores, same 32 440-ion cell.  A whole MD step of the reference (its
+    fixed-point SCF: about 35 multipole Ewald evaluations over all 51 911
+    k-vectors) takes minutes on the host, so each timed step here is ONE
+    complete multipole Ewald evaluation of the cell (real space over the
+    Coulomb list and reciprocal space over every k-vector of the reference's
+    half space, nothing sampled or scaled) plus one BMHFTD pair loop, and
+    ms_per_step is its measured time.  value is the MD rate this implies:
+    natm / ((SCF iterations + 2) x evaluation + pair loop), with the SCF
+    iteration count of the reference's solver at the same tolerance measured
+    on an 8^3-site replica of the model."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
@@ -518,8 +633,6 @@ def run_reference(args):
     from mdff_b200 import abi, systems
     s = systems.mgo_production(ncell=args.ncell)
     p = s["params"]
-    # the reference's own solver: fixed-point SCF iterations at the same
-    # tolerance; its iteration count is measured on a 4^3-cell replica
     small = systems.mgo_pim(grid=(8, 8, 8), rc=8.0, alpha=0.3, kmax=8, temp=2000.0, seed=11)
     sp = small["params"]
     sp.algo_moment_from_pola = abi.POLA_SCF
@@ -531,16 +644,24 @@ def run_reference(args):
     iters = float(np.mean([t["scf_iter"] for t in st["thermo"]]))
     o = oracle.Oracle(p, s["itype"], s["pos"], s["cell"])
     natm = len(s["itype"])
-    kstride = 16
     for _ in range(args.warmup):
-        o.field_time(kstride * 4)
-    times = []
+        o.field_time(64)   # untimed warm-up: threads and caches, a 1/64 k sample
+    samples = []
+    t0 = time.perf_counter()
     for _ in range(args.steps):
-        td, tr, tp = o.field_time(kstride)
-        times.append((iters + 2) * (td + tr * kstride) + tp)
-    t_step = float(np.mean(times))
-    v = natm / t_step
+        samples.append(o.field_time(1))
+    wall = time.perf_counter() - t0
+    td, tr, tp = (float(np.mean([x[k] for x in samples])) for k in range(3))
+    t_eval = td + tr
+    t_md = (iters + 2) * t_eval + tp
+    v = natm / t_md
     cores = oracle.max_threads()
+    cpu = host_cpu()
+    k1, k2, k3 = p.kES
+    nk = k3 + k2 * (2 * k3 + 1) + k1 * (2 * k2 + 1) * (2 * k3 + 1)   # the half space (src/field.f90:1648)
+    sample = ("each timed step: one complete multipole Ewald evaluation of the %d-ion cell (real space + all "
+              "%d k-vectors) and one BMHFTD pair loop; value = natm / ((%.1f SCF iterations + 2) x evaluation + "
+              "pair loop)" % (natm, nk, iters))
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -549,20 +670,25 @@ def run_reference(args):
         "n_gpus": 0,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": t_step * 1e3,
+        "ms_per_step": wall / args.steps * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "fp64",
         "data": "synthetic (seeded MgO polarisable-ion cell, mdff_b200.systems.mgo_production)",
         "config": {"workload": "mgo-pim-production", "natm": natm, "kmax": list(p.kES), "solver": "scf (reference)",
-                   "solver_iters": iters, "precision": "fp64"},
-        "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": cores, "kind": "port",
-                         "sample": "per step: one Ewald field evaluation (real space + every %dth k-vector, scaled) "
-                                   "and one BMHFTD pair loop, x (%.1f SCF iterations + 2) evaluations"
-                                   % (kstride, iters)},
+                   "solver_iters": iters, "precision": "fp64",
+                   "step_unit": "one multipole Ewald evaluation + one pair loop (1/%.1f of an MD step's "
+                                "evaluations)" % (iters + 2)},
+        "md_step_derived": {"seconds_per_md_step": t_md, "evaluation_s": t_eval, "real_space_s": td,
+                            "reciprocal_s": tr, "pair_loop_s": tp, "extrapolated": True,
+                            "from": "measured evaluations x measured SCF iteration count"},
+        "host": cpu,
+        "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": cores, "kind": "port", "sample": sample,
+                         "host": cpu},
         "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
 
 def run_batch(args):
     """Force-matching workload: one evaluation = the loss of 64 MgO PIM

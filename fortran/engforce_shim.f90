@@ -3,7 +3,7 @@
 ! (src/runmd.f90:268-277) on top of the B200 engine.
 !
 ! Build: compile mdff_engine.f90 and this file with the reference's modules
-! and link libmdff_engine.so (see INTEGRATION.md).  The reference's own
+! and link libmdff_engine.so.  The reference's own
 ! engforce_driver is renamed (or its body replaced by CALL engforce_b200);
 ! every other caller keeps calling engforce_driver.
 !
@@ -30,8 +30,8 @@ contains
                       doefg, conv_tol_ind, min_scf_pol_iter, max_scf_pol_iter, extrapolate_order, &
                       algo_ext_dipole, algo_moment_from_pola
     use config, only : ntype
-    use md, only : integrator, dt, temp, nhc_n, nhc_yosh_order, nhc_mults, timesca_thermo
-    use constants, only : time_unit, boltz_unit
+    use md, only : integrator, dt, temp, nhc_n, nhc_yosh_order, nhc_mults, timesca_thermo, press, timesca_baro
+    use constants, only : time_unit, boltz_unit, press_unit
     type(mdff_params_t), intent(out) :: prm
     integer :: it, jt, ip
     call mdff_params_default(prm)
@@ -76,12 +76,17 @@ contains
     prm%extrapolate_order = extrapolate_order
     prm%algo_ext_dipole = merge(MDFF_EXT_ASPC, MDFF_EXT_POLY, algo_ext_dipole == 'aspc')
     prm%algo_moment_from_pola = merge(MDFF_POLA_PCG, MDFF_POLA_SCF, algo_moment_from_pola == 'cng')
-    prm%integrator = merge(MDFF_NVT_NHCN, MDFF_NVE_VV, integrator == 'nvt-nhcn')
+    prm%integrator = MDFF_NVE_VV
+    if (integrator == 'nvt-nhcn') prm%integrator = MDFF_NVT_NHCN
+    if (integrator == 'nvt-nhc2') prm%integrator = MDFF_NVT_NHC2
+    if (integrator == 'npt-nhcnp') prm%integrator = MDFF_NPT_NHCNP
     ! md_init has already converted dt, temp and timesca_thermo to internal
     ! units (src/md.f90:314-324); the engine takes control-file units
     prm%dt = dt / time_unit
     prm%temp = temp / boltz_unit
     prm%timesca_thermo = timesca_thermo / time_unit
+    prm%press = press / press_unit
+    prm%timesca_baro = timesca_baro / time_unit
     prm%nhc_n = nhc_n; prm%nhc_yosh_order = nhc_yosh_order; prm%nhc_mults = nhc_mults
   end subroutine mdff_fill_params
 

@@ -24,7 +24,7 @@ module mdff_engine
   integer(c_int), parameter :: MDFF_TRUNC_NONE = 0, MDFF_TRUNC_LINEAR = 1, MDFF_TRUNC_QUADRATIC = 2
   integer(c_int), parameter :: MDFF_POLA_SCF = 0, MDFF_POLA_PCG = 1
   integer(c_int), parameter :: MDFF_EXT_POLY = 0, MDFF_EXT_ASPC = 1
-  integer(c_int), parameter :: MDFF_NVE_VV = 0, MDFF_NVT_NHCN = 1, MDFF_NPT_NHCNP = 2
+  integer(c_int), parameter :: MDFF_NVE_VV = 0, MDFF_NVT_NHCN = 1, MDFF_NPT_NHCNP = 2, MDFF_NVT_NHC2 = 3
   integer(c_int), parameter :: MDFF_PREC_FP64 = 0, MDFF_PREC_MIXED = 1
 
   type, bind(C) :: mdff_params_t
@@ -82,6 +82,7 @@ module mdff_engine
     integer(c_int) :: kspace_tc
     real(c_double) :: press
     real(c_double) :: timesca_baro
+    real(c_double) :: fp64_keps
   end type mdff_params_t
 
   type, bind(C) :: mdff_energies_t

@@ -62,11 +62,13 @@ extern "C" {
 #define MDFF_EXT_POLY 0
 #define MDFF_EXT_ASPC 1
 
-/* integrator (src/md.f90:71-76); only the two on the hot path */
+/* integrator (src/md.f90:71-76): the ones on the hot path */
 #define MDFF_NVE_VV   0
 #define MDFF_NVT_NHCN 1
 #define MDFF_NPT_NHCNP 2           /* isotropic Martyna-Tobias-Klein barostat with Nose-Hoover chains on
                                       particles and barostat (nhcnp, src/integration.f90:715-1160) */
+#define MDFF_NVT_NHC2 3            /* 'nvt-nhc2': two-thermostat Nose-Hoover chain after Frenkel and Smit
+                                      (nhc2 + chain_nhc2, src/integration.f90:205-324); nhc_n is 2, L = 3(N-1) */
 
 /* arithmetic of the bulk pair and k-space work */
 #define MDFF_PREC_FP64  0          /* plain FP64 everywhere */
@@ -120,7 +122,7 @@ typedef struct mdff_params {
     int    extrapolate_order;
     int    algo_ext_dipole;                    /* MDFF_EXT_* */
     /* &mdtag */
-    int    integrator;                         /* MDFF_NVE_VV / MDFF_NVT_NHCN / MDFF_NPT_NHCNP */
+    int    integrator;                         /* MDFF_NVE_VV / MDFF_NVT_NHCN / MDFF_NPT_NHCNP / MDFF_NVT_NHC2 */
     double dt;                                 /* ps */
     double temp;                               /* K */
     int    nhc_n, nhc_yosh_order, nhc_mults;
@@ -131,7 +133,8 @@ typedef struct mdff_params {
     int    nlist_capacity;                     /* neighbours per atom reserved (0 = automatic) */
     int    device;                             /* CUDA device ordinal */
     int    erfc_ref;                           /* 1: the reference's fitted erfc (src/functions.f90:28-39) */
-    int    nhc_literal;                        /* 1: chain_nhcn's literal force order (stale G(2..M-1)) */
+    int    nhc_literal;                        /* 1: chain_nhcn's literal force order (stale G(2..M-1)), and
+                                                  nhc2's literal thermostat energy vxi^2/(2Q) */
     double mixed_ksplit;                       /* mixed path: |k| < mixed_ksplit*alpha summed in FP64 (0: none) */
     int    kspace_reuse;                       /* PCG: one reciprocal evaluation for the static field and the first
                                                   residual, and the final structure factor from the solver's by
@@ -146,6 +149,10 @@ typedef struct mdff_params {
     /* &mdtag, constant pressure (integrator MDFF_NPT_NHCNP) */
     double press;                              /* GPa (md_check_tag converts with press_unit) */
     double timesca_baro;                       /* ps */
+    /* engine choice (no reference counterpart) */
+    double fp64_keps;                          /* FP64 path: k-vectors whose Gaussian factor exp(-k^2/4 alpha^2) is
+                                                  below fp64_keps are left out, as mixed_keps does on the mixed
+                                                  path (0, the default: the reference's whole half space) */
 } mdff_params;
 
 /* Energies and scalar outputs of one force evaluation (thermodynamic module
@@ -283,8 +290,9 @@ int  mdff_profile_detail(mdff_ctx* ctx, double ms[MDFF_NDETAIL], long long count
 /* Sizes of the reciprocal-space sums of the context (no reference
  * counterpart): out[0] the k rectangle the kernels sweep, out[1] the k-vectors
  * of the reference's half space (kpoint_sum_init, src/kspace.f90:142-207),
- * out[2] the FP32 set and out[3] the FP64 low-|k| set of the mixed path (both
- * 0 on the FP64 path). */
+ * out[2] the main set the path sums (mixed: the FP32 / tensor-core set; FP64:
+ * the half space, or its part inside the fp64_keps sphere) and out[3] the FP64
+ * low-|k| set of the mixed path (0 on the FP64 path). */
 int  mdff_kspace_info(mdff_ctx* ctx, long long out[4]);
 
 /* Launch shape in use (the autotuner's choice, or the defaults): out[0] lanes
@@ -304,15 +312,17 @@ int  mdff_set_system(mdff_ctx* ctx, int natm, const int* itype,
                      const double* rx, const double* ry, const double* rz,
                      const double A[9]);
 
-/* Replace the positions (no wrap, no list rebuild): the state engforce_driver
- * sees when a caller moved the atoms itself. */
 /* A new cell (column-major, as mdff_set_system) for the same atoms: the
  * lattice, the tail corrections and the Ewald k tables of the same k
  * rectangle follow it (the k membership of the mixed path's sets stays as set
  * up; meant for the percent-level changes of a constant-pressure run).
- * Positions are kept as given (Cartesian); lists are rebuilt.  No reference
- * counterpart (the reference moves simu_cell inside nhcnp). */
+ * Positions are kept as given (Cartesian).  No reference counterpart (the
+ * reference moves simu_cell inside nhcnp). */
 int  mdff_set_cell(mdff_ctx* ctx, const double A[9]);
+/* Replace the positions (no wrap): the state engforce_driver sees when a
+ * caller moved the atoms itself.  After either call the Verlet lists are
+ * rebuilt by the next force evaluation or list read, so a new cell and new
+ * positions together cost one build. */
 int  mdff_set_positions(mdff_ctx* ctx, const double* rx, const double* ry, const double* rz);
 
 /* Wrapped positions as the engine holds them. */
@@ -494,17 +504,22 @@ int  mdff_batch_loss_grad(mdff_batch* b, double* loss, mdff_param_grad* grad, in
  * ry, rz Cartesian positions and q charges, natm each) on `device`; A is the
  * host cell matrix (column-major, as in mdff_set_system), kmax the host k
  * rectangle; stream is a cudaStream_t (NULL: the legacy default stream).
- * *u_rec receives the energy in eV with coul_unit applied, the same quantity
- * as mdff_energies.u_rec of mdff_engforce for a charges-only system.  The call
- * returns after the result is on the host.
+ * *u_rec receives the energy in eV with the reference's coul_unit
+ * (14.3996441494161 eV A / e^2) applied, the same quantity as
+ * mdff_energies.u_rec of mdff_engforce for a charges-only system outside
+ * reduced units (lreduced is not taken into account here).  The call copies
+ * the energy into *u_rec and waits for `stream` to finish before it returns.
  *
- * Scratch is a fixed 16 MiB array in device memory per device (2^21 doubles):
- * a problem needing more (3 natm + the structure-factor partials) returns
- * MDFF_E_NOMEM, and *scratch_needed (may be NULL) receives the doubles it
- * would need.  The first call on a device looks up the scratch's address
- * (one-time set-up), so make that first call before any stream capture.  All
- * calls on one device share the scratch: overlapping calls race and must be
- * serialised by the caller.
+ * Scratch is a fixed 16 MiB array in device memory per device (2^21 doubles),
+ * held by every device that loads the library until the process exits: a
+ * problem needing more (3 natm + the structure-factor partials) returns
+ * MDFF_E_NOMEM before anything is launched, and *scratch_needed (may be NULL)
+ * receives the doubles it would need.  Each call looks up the array's device
+ * address on `device` (cudaGetSymbolAddress, a host query that allocates
+ * nothing).  Nothing in the scratch has to start at zero: every word a call
+ * reads it has written earlier in the same call.  All calls on one device
+ * share the scratch: overlapping calls race and must be serialised by the
+ * caller.
  */
 int  mdff_rec_energy_noalloc(int device, int natm, const double* rx, const double* ry, const double* rz,
                              const double* q, const double A[9], double alpha, const int kmax[3],

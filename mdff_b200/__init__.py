@@ -158,11 +158,12 @@ class Engine:
             raise EngineError(rc, msg)
 
     def kspace_info(self):
-        """k-vector counts: rectangle, reference half space, mixed FP32 set,
-        mixed FP64 low set."""
+        """k-vector counts: rectangle, reference half space, the path's main
+        set (mixed: the FP32 / tensor-core set; FP64: the half space or its
+        part inside the fp64_keps sphere), mixed FP64 low set."""
         out = (C.c_longlong * 4)()
         self._check(lib().mdff_kspace_info(self._h, out))
-        return {"rect": out[0], "half": out[1], "fp32": out[2], "low": out[3]}
+        return {"rect": out[0], "half": out[1], "main": out[2], "low": out[3]}
 
     def launch_shape(self):
         """Launch shape in use: real-space lanes per atom (FP64, FP32) and the

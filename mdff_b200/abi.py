@@ -24,7 +24,7 @@ E_NOMEM = -8
 TRUNC_NONE, TRUNC_LINEAR, TRUNC_QUADRATIC = 0, 1, 2
 POLA_SCF, POLA_PCG = 0, 1
 EXT_POLY, EXT_ASPC = 0, 1
-NVE_VV, NVT_NHCN, NPT_NHCNP = 0, 1, 2
+NVE_VV, NVT_NHCN, NPT_NHCNP, NVT_NHC2 = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 
 _T = NTYPE_MAX
@@ -59,6 +59,7 @@ class Params(C.Structure):
         ("kspace_reuse", C.c_int), ("mixed_keps", C.c_double), ("autotune", C.c_int),
         ("kspace_tc", C.c_int),
         ("press", C.c_double), ("timesca_baro", C.c_double),
+        ("fp64_keps", C.c_double),
     ]
 
 

@@ -253,8 +253,12 @@ int check_params(mdff_ctx* ctx, const mdff_params& p) {
             for (int c = 0; c < p.ntype; ++c)
                 if (p.dip_pol_damp_k[a][b][c] > MDFF_TT_MAX_ORDER || p.dip_pol_damp_k[a][b][c] < 0)
                     return fail(ctx, MDFF_E_ARG, "Tang-Toennies expansion order too large (dip_pol_damp_k)");
-    if (p.integrator != MDFF_NVE_VV && p.integrator != MDFF_NVT_NHCN && p.integrator != MDFF_NPT_NHCNP)
-        return fail(ctx, MDFF_E_UNSUPPORTED, "integrator: nve-vv, nvt-nhcn and npt-nhcnp are on the engine's path");
+    if (p.integrator != MDFF_NVE_VV && p.integrator != MDFF_NVT_NHCN && p.integrator != MDFF_NPT_NHCNP &&
+        p.integrator != MDFF_NVT_NHC2)
+        return fail(ctx, MDFF_E_UNSUPPORTED,
+                    "integrator: nve-vv, nvt-nhc2, nvt-nhcn and npt-nhcnp are on the engine's path");
+    if (p.integrator == MDFF_NVT_NHC2 && !(p.timesca_thermo > 0.0))
+        return fail(ctx, MDFF_E_ARG, "mdtag: nvt-nhc2 needs timesca_thermo > 0");
     const bool chains = p.integrator == MDFF_NVT_NHCN || p.integrator == MDFF_NPT_NHCNP;
     if (chains && (p.nhc_n < 2 || p.nhc_n > 16))
         return fail(ctx, MDFF_E_ARG, "nhc_n = 1 is not allowed with Nose Hoover chains thermostats");
@@ -827,6 +831,7 @@ int engforce_device(mdff_ctx* ctx) {
     const int n = ctx->n;
     const mdff_params& p = ctx->p;
     if (!p.lvnlist) TRY(build_lists(ctx, 0.0));
+    else if (!ctx->have_list) TRY(build_lists(ctx, p.skindiff));   // lists dropped (an interrupted RMC chain)
     ctx->prof.begin(PK_OTHER);
     launch_frac(ctx->st, n, ctx->x, ctx->y, ctx->z, ctx->cell, ctx->sx, ctx->sy, ctx->sz);
     ctx->prof.end(1);
@@ -974,6 +979,14 @@ void nhc_const(const mdff_ctx* ctx, NhcConst& c) {
     c.temp = p.temp * ctx->u.boltz;
     c.L = 3.0 * (double)ctx->n;
     double ts = p.timesca_thermo * ctx->u.time;
+    if (p.integrator == MDFF_NVT_NHC2) {
+        // nhc2 (src/integration.f90:224-229): L = 3 (natm - 1), two thermostats
+        c.nhc_n = 2;
+        c.L = 3.0 * ((double)ctx->n - 1.0);
+        c.Q[0] = ts * ts * c.temp * c.L;
+        c.Q[1] = ts * ts * c.temp;
+        return;
+    }
     for (int k = 0; k < p.nhc_n; ++k) c.Q[k] = ts * ts * c.temp;   // timesca_thermo**2 * temp
     c.Q[0] = c.Q[0] * c.L;
     double* w = c.w;
@@ -1016,7 +1029,9 @@ void fill_thermo(mdff_ctx* ctx, mdff_thermo* t, int step) {
     t->u_tot = t->u_lj + t->u_coul + t->u_morse + t->u_bmhft;
     t->e_tot = t->u_tot + t->e_kin;
     const int ig = ctx->p.integrator;
-    t->e_nvt = (ig == MDFF_NVT_NHCN ? ctx->hsc->e_nvt : ig == MDFF_NPT_NHCNP ? ctx->npt.e_npt : 0.0) / nr;
+    t->e_nvt = ((ig == MDFF_NVT_NHCN || ig == MDFF_NVT_NHC2) ? ctx->hsc->e_nvt
+                : ig == MDFF_NPT_NHCNP                       ? ctx->npt.e_npt
+                                                             : 0.0) / nr;
     t->h_tot = ig == MDFF_NVE_VV ? t->e_tot : t->e_tot + t->e_nvt;
     t->volume = omega;
     double pv = (ctx->en.vir_lj + ctx->en.vir_morse + ctx->en.vir_bmhft) / omega / nr + ctx->en.pvirial_coul / nr;
@@ -1187,11 +1202,18 @@ int md_step(mdff_ctx* ctx) {
         launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
         ctx->prof.end(2);
     } else {
+        // nhcn (src/integration.f90:476-558) or nhc2 (:205-254): chain half,
+        // prop_pos_vel_verlet, chain half; only the chain kernel differs
         NhcConst c;
         nhc_const(ctx, c);
+        const bool two = p.integrator == MDFF_NVT_NHC2;
+        auto chain = [&]() {
+            if (two) k_nhc2_chain<<<1, 1, 0, ctx->st>>>(ctx->dsc, c, ctx->dsc->ke2);
+            else k_nhc_chain<<<1, 1, 0, ctx->st>>>(ctx->dsc, c, ctx->dsc->ke2);
+        };
         TRY(ke_reduce(ctx, 0));
         ctx->prof.begin(PK_INTEGRATE);
-        k_nhc_chain<<<1, 1, 0, ctx->st>>>(ctx->dsc, c, ctx->dsc->ke2);
+        chain();
         ctx->prof.end(1);
         TRY(ke_reduce(ctx, 1));
         ctx->prof.begin(PK_INTEGRATE);
@@ -1204,11 +1226,12 @@ int md_step(mdff_ctx* ctx) {
         k_kick<<<nb(n), 256, 0, ctx->st>>>(n, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mass, dt,
                                            ctx->part.buf);
         launch_reduce_partials(ctx->st, ctx->part.buf, nb(n), 1, ctx->dsc->ke2, 0);
-        k_nhc_chain<<<1, 1, 0, ctx->st>>>(ctx->dsc, c, ctx->dsc->ke2);
+        chain();
         ctx->prof.end(3);
         TRY(ke_reduce(ctx, 1));
         ctx->prof.begin(PK_INTEGRATE);
-        k_nhc_energy<<<1, 1, 0, ctx->st>>>(ctx->dsc, c);
+        if (two) k_nhc2_energy<<<1, 1, 0, ctx->st>>>(ctx->dsc, c);
+        else k_nhc_energy<<<1, 1, 0, ctx->st>>>(ctx->dsc, c);
         ctx->prof.end(1);
     }
     TRY(check_launch(ctx, "step"));
@@ -2484,6 +2507,7 @@ int mdff_create(const mdff_params* p, mdff_ctx** out) {
     ctx->p = *p;
     int rc = check_params(ctx, ctx->p);
     if (rc != MDFF_OK) { *out = ctx; return rc; }
+    if (ctx->p.integrator == MDFF_NVT_NHC2) ctx->p.nhc_n = 2;   // extended_coordinates_alloc (src/md.f90:335-340)
     symmetrise(ctx->p);
     set_units(ctx);
     int ndev = 0;
@@ -2635,6 +2659,53 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
         ctx->kinfo[1] = 0;
         for (double v : ak) ctx->kinfo[1] += v != 0.0;
         ctx->kinfo[2] = ctx->kinfo[3] = 0;
+        kg.nfitems = kg.nfcol = 0;
+        if (p.precision == MDFF_PREC_FP64) {
+            // fp64_keps: leave out the vectors whose Gaussian factor
+            // exp(-k^2 / 4 alpha^2) is below fp64_keps (the sphere the mixed
+            // path's mixed_keps cuts), and give the FP64 kernels work lists of
+            // what is left: (column, nz chunk) items for the structure factor,
+            // the columns with their nz ranges for the field
+            if (p.fp64_keps > 0.0) {
+                const double R2 = -4.0 * a2 * std::log(p.fp64_keps);
+                const int CH = kg.nzl <= 8 ? 8 : kg.nzl <= 12 ? 12 : 16;   // plan()'s chunk
+                std::vector<int> items, fcols, fzr;
+                for (int col = 0; col < kg.ncol; ++col) {
+                    int nx = col / (2 * kg.kmax[1] + 1), ny = col % (2 * kg.kmax[1] + 1) - kg.kmax[1];
+                    int lo = -1, hi = -1;
+                    for (int m = 0; m < kg.nzl; ++m) {
+                        const size_t r = (size_t)col * kg.nzl + m;
+                        if (ak[r] == 0.0) continue;
+                        int nz = m - kg.kmax[2];
+                        double kx = 2.0 * PI * (double(nx) * c.B[0] + double(ny) * c.B[1] + double(nz) * c.B[2]);
+                        double ky = 2.0 * PI * (double(nx) * c.B[3] + double(ny) * c.B[4] + double(nz) * c.B[5]);
+                        double kz = 2.0 * PI * (double(nx) * c.B[6] + double(ny) * c.B[7] + double(nz) * c.B[8]);
+                        if (kx * kx + ky * ky + kz * kz > R2) { ak[r] = 0.0; kc[r] = 0.0; continue; }
+                        if (lo < 0) lo = m;
+                        hi = m;
+                    }
+                    if (lo < 0) continue;
+                    fcols.push_back(col);
+                    fzr.push_back(lo);
+                    fzr.push_back(hi - lo + 1);
+                    for (int h = lo / CH; h <= hi / CH; ++h) { items.push_back(col); items.push_back(h); }
+                }
+                kg.nfitems = (int)(items.size() / 2);
+                kg.nfcol = (int)fcols.size();
+                if (kg.nfcol > 0) {
+                    TRY(dalloc(ctx, &kg.fitems, items.size()));
+                    TRY(dalloc(ctx, &kg.fcols, fcols.size()));
+                    TRY(dalloc(ctx, &kg.fzr, fzr.size()));
+                    CK(cudaMemcpyAsync(kg.fitems, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice,
+                                       ctx->st));
+                    CK(cudaMemcpyAsync(kg.fcols, fcols.data(), sizeof(int) * fcols.size(), cudaMemcpyHostToDevice,
+                                       ctx->st));
+                    CK(cudaMemcpyAsync(kg.fzr, fzr.data(), sizeof(int) * fzr.size(), cudaMemcpyHostToDevice, ctx->st));
+                    CK(cudaStreamSynchronize(ctx->st));   // the host vectors go out of scope
+                }
+            }
+            for (double v : ak) ctx->kinfo[2] += v != 0.0;
+        }
         TRY(dalloc(ctx, &kg.Ak, kg.nrect));
         TRY(dalloc(ctx, &kg.kcoe, kg.nrect));
         TRY(upload(ctx, kg.Ak, ak.data(), kg.nrect));
@@ -2857,7 +2928,9 @@ int mdff_set_cell(mdff_ctx* ctx, const double A[9]) {
     if (!A) return fail(ctx, MDFF_E_ARG, "mdff_set_cell: A is NULL");
     cudaSetDevice(ctx->p.device);
     TRY(apply_cell(ctx, A));
-    if (ctx->p.lvnlist) TRY(build_lists(ctx, ctx->p.skindiff));
+    // the lists are rebuilt by the next force evaluation (or list read), so a
+    // new cell and new positions together cost one build
+    ctx->have_list = false;
     CK(cudaStreamSynchronize(ctx->st));
     return MDFF_OK;
 }
@@ -2868,8 +2941,9 @@ int mdff_set_positions(mdff_ctx* ctx, const double* rx, const double* ry, const 
     TRY(upload(ctx, ctx->x, rx, ctx->n));
     TRY(upload(ctx, ctx->y, ry, ctx->n));
     TRY(upload(ctx, ctx->z, rz, ctx->n));
-    // a list built for other positions is not a list of these
-    if (ctx->p.lvnlist) TRY(build_lists(ctx, ctx->p.skindiff));
+    // a list built for other positions is not a list of these: rebuilt by
+    // the next force evaluation (or list read)
+    ctx->have_list = false;
     CK(cudaStreamSynchronize(ctx->st));
     ctx->forces_valid = false;
     return MDFF_OK;
@@ -2895,9 +2969,12 @@ int mdff_nlist_build(mdff_ctx* ctx) {
 
 int mdff_nlist_get(mdff_ctx* ctx, int which, int* point, int* list, int cap, int* nlist) {
     if (!ctx || !ctx->have_system) return ctx ? fail(ctx, MDFF_E_STATE, "set_system first") : MDFF_E_STATE;
-    if (!ctx->have_list) return fail(ctx, MDFF_E_STATE, "no Verlet list has been built");
     if (!point || !nlist || (which != 0 && which != 1)) return fail(ctx, MDFF_E_ARG, "invalid nlist_get arguments");
     cudaSetDevice(ctx->p.device);
+    if (!ctx->have_list) {
+        TRY(build_lists(ctx, ctx->p.skindiff));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
     const int n = ctx->n;
     bool nonb = ctx->p.lnmlj || ctx->p.lbmhft || ctx->p.lbmhftd || ctx->p.lmorse;
     if (which == 0 && !nonb) return fail(ctx, MDFF_E_STATE, "no vdW list without a short-range potential");
@@ -3033,12 +3110,9 @@ int mdff_step(mdff_ctx* ctx, int nsteps, double* rx, double* ry, double* rz, dou
 namespace {
 
 constexpr size_t NOALLOC_SCRATCH_DOUBLES = (size_t)1 << 21;   // 16 MiB of device memory per device
-constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
 
-std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
 
 // Energy sum over the k rectangle from the structure-factor partials, with
 // A_k = exp(-k^2/4 alpha^2)/k^2 evaluated in place (no k table): the energy
@@ -3072,16 +3146,16 @@ __global__ void k_sfac_energy_inplace(int P, int ch, int nchunk, int ncol, int n
     block_partials<1>(v, partials);
 }
 
-// Device address of this device's scratch, looked up once per device with
-// that device current.
-int noalloc_scratch(int device, double** out) {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[device]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MDFF_E_CUDA;
-        g_noalloc_ptr[device] = (double*)p;
-    }
-    *out = g_noalloc_ptr[device];
+// Device address of the current device's scratch.  In host code the name
+// g_noalloc_scratch is a host-side stand-in, not a device address, so every
+// call looks the address up with the device current.  The lookup is a host
+// query that allocates nothing; doing it per call (rather than caching it)
+// keeps the address right if the caller resets the device, which reloads the
+// module and can move the array.
+int noalloc_scratch(double** out) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MDFF_E_CUDA;
+    *out = (double*)p;
     return MDFF_OK;
 }
 
@@ -3091,7 +3165,9 @@ extern "C" int mdff_rec_energy_noalloc(int device, int natm, const double* rx, c
                                        const double* q, const double A[9], double alpha, const int kmax[3],
                                        void* stream, double* u_rec, long long* scratch_needed) {
     if (!rx || !ry || !rz || !q || !A || !kmax || !u_rec || natm < 1 || !(alpha > 0.0)) return MDFF_E_ARG;
-    if (device < 0 || device >= NOALLOC_MAX_DEVICES) return MDFF_E_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess) return MDFF_E_CUDA;
+    if (device < 0 || device >= ndev) return MDFF_E_ARG;
     for (int d = 0; d < 3; ++d)
         if (kmax[d] < 0 || kmax[d] > 64) return MDFF_E_ARG;
     // scratch layout: sx sy sz (3 natm), partials (2 plane), energy partials, result
@@ -3111,7 +3187,7 @@ extern "C" int mdff_rec_energy_noalloc(int device, int natm, const double* rx, c
     if (prev != device && cudaSetDevice(device) != cudaSuccess) return MDFF_E_CUDA;
     int rc = MDFF_OK;
     double* scr = nullptr;
-    if ((rc = noalloc_scratch(device, &scr)) == MDFF_OK) {
+    if ((rc = noalloc_scratch(&scr)) == MDFF_OK) {
         cudaStream_t st = (cudaStream_t)stream;
         CellP c;
         double W[3], anorm[3];
@@ -3124,7 +3200,8 @@ extern "C" int mdff_rec_energy_noalloc(int device, int natm, const double* rx, c
         launch_frac(st, natm, rx, ry, rz, c, sx, sy, sz);
         dim3 g1(L.nchunk * L.ncolblk, L.P);
 #define SFAC_NA(CHV) k_sfac<CHV><<<g1, SF_THREADS, 0, st>>>(natm, L.natom_chunk, sx, sy, sz, q, nullptr, c, kmax[0], \
-                                                        kmax[1], kmax[2], kg.ncol, L.ncolblk, L.nchunk, 1, 0, pre, pim)
+                                                        kmax[1], kmax[2], kg.ncol, L.ncolblk, L.nchunk, 1, 0, pre, pim, \
+                                                        nullptr, 0)
         if (L.CH == 16) SFAC_NA(16);
         else if (L.CH == 12) SFAC_NA(12);
         else SFAC_NA(8);
@@ -3133,7 +3210,9 @@ extern "C" int mdff_rec_energy_noalloc(int device, int natm, const double* rx, c
                                                   0.25 / (alpha * alpha), c, epart);
         launch_reduce_partials(st, epart, rb, 1, res, 0);
         double h = 0.0;
-        if (cudaGetLastError() != cudaSuccess ||
+        // launch errors are read without clearing them: an error left by the
+        // caller's own earlier work stays the caller's to see
+        if (cudaPeekAtLastError() != cudaSuccess ||
             cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
             rc = MDFF_E_CUDA;
@@ -4095,9 +4174,16 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     ctx->p.lmorse = saved_nonb[3];
     for (void* q : {(void*)s, (void*)hd, (void*)dh, (void*)ce}) cudaFreeAsync(q, ctx->st);
     cudaStreamSynchronize(ctx->st);
-    if (rc != MDFF_OK) return rc;
-    TRY(check_launch(ctx, "rmc_efg"));
+    // lists rebuilt during the chain cover the Coulomb cut only: never leave
+    // them in place, on the error path either (a failed rebuild here leaves
+    // have_list false, so the next evaluation builds them)
     ctx->forces_valid = false;
+    ctx->have_list = false;
+    if (rc != MDFF_OK) {
+        if (ctx->p.lvnlist) build_lists(ctx, ctx->p.skindiff);
+        return rc;
+    }
+    TRY(check_launch(ctx, "rmc_efg"));
     if (ctx->p.lvnlist) TRY(build_lists(ctx, ctx->p.skindiff));
     if (grr_out) rmc_normalise(*k, h, grr_out);
     if (dibU_out) std::memcpy(dibU_out, aU.data(), sizeof(double) * nU);

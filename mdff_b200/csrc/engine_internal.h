@@ -226,6 +226,14 @@ struct KGrid {
     int* items = nullptr;      // [nitems][2]: (column, chunk) work list of the FP32 structure factor
     unsigned char* mask = nullptr;   // [nrect]: bit 1 in the half space, bit 2 in the FP32 set (fixed at set-up)
     int nitems = 0;
+    // FP64 path with the fp64_keps sphere: the (column, CH-wide nz chunk) work
+    // list of the structure factor, and the columns holding a vector with the
+    // nz index range [lo, lo + cnt) of each, for the field pass
+    int* fitems = nullptr;     // [nfitems][2]
+    int nfitems = 0;
+    int* fcols = nullptr;      // [nfcol]
+    int* fzr = nullptr;        // [nfcol][2]: lo, cnt
+    int nfcol = 0;
 };
 // The low-|k| set of the mixed path, summed in FP64 (see ewald_recip.cuh):
 // columns (nx, ny) with a contiguous nz range [nzlo, nzlo + nzn).

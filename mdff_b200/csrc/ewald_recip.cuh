@@ -32,11 +32,25 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac(int n, int natom_chunk, con
                                                      const double* __restrict__ q, const double* __restrict__ mu,
                                                      CellP c, int kx, int ky, int kz, int ncol, int ncolblk,
                                                      int nchunk, int with_q, int with_mu, double* __restrict__ part_re,
-                                                     double* __restrict__ part_im) {
+                                                     double* __restrict__ part_im, const int* __restrict__ items,
+                                                     int nitems) {
     __shared__ double t_s1[SF_TILE], t_s2[SF_TILE], t_s3[SF_TILE], t_q[SF_TILE];
     __shared__ double t_m1[SF_TILE], t_m2[SF_TILE], t_m3[SF_TILE], t_cs[SF_TILE], t_sn[SF_TILE];
-    const int h = blockIdx.x / ncolblk;
-    const int col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
+    // one (column, nz chunk) per thread: the whole rectangle, or the work list
+    // of the vectors inside a k sphere (items, one entry per thread)
+    int h, col;
+    bool valid;
+    if (items) {
+        const int t = blockIdx.x * SF_THREADS + threadIdx.x;
+        valid = t < nitems;
+        const int tt = valid ? t : nitems - 1;
+        col = items[2 * tt];
+        h = items[2 * tt + 1];
+    } else {
+        h = blockIdx.x / ncolblk;
+        col = (blockIdx.x % ncolblk) * SF_THREADS + threadIdx.x;
+        valid = col < ncol;
+    }
     const int p = blockIdx.y;
     const int ny_n = 2 * ky + 1;
     const int colc = col < ncol ? col : ncol - 1;
@@ -89,7 +103,7 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac(int n, int natom_chunk, con
             }
         }
     }
-    if (col < ncol) {
+    if (valid) {
         const size_t plane = (size_t)ncol * CH * nchunk;
 #pragma unroll
         for (int m = 0; m < CH; ++m) {
@@ -153,7 +167,8 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield(int n, const double* __re
                                                        const double* __restrict__ sz, CellP c, int kx, int ky, int kz,
                                                        int ncol, int nzl, int cols_per_split,
                                                        const double* __restrict__ aks, int nrect,
-                                                       double* __restrict__ fpart) {
+                                                       double* __restrict__ fpart, const int* __restrict__ clist,
+                                                       const int* __restrict__ czr) {
     extern __shared__ double sm[];
     double* s_re = sm;
     double* s_im = sm + KF_COLS * nzl;
@@ -170,17 +185,30 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield(int n, const double* __re
     const int ny_n = 2 * ky + 1;
     double E0 = 0, E1 = 0, E2 = 0;
     double G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
+    // columns c0..c1 of the rectangle, or of the list clist (columns inside a
+    // k sphere) with the nz index range [czr[0], czr[0] + czr[1]) of each
     for (int cb = c0; cb < c1; cb += KF_COLS) {
         const int nc = min(KF_COLS, c1 - cb);
         __syncthreads();
-        for (int t = threadIdx.x; t < nc * nzl; t += blockDim.x) {
-            s_re[t] = aks[(size_t)cb * nzl + t];
-            s_im[t] = aks[(size_t)nrect + (size_t)cb * nzl + t];
+        if (clist) {
+            for (int t = threadIdx.x; t < nc * nzl; t += blockDim.x) {
+                const int cc = t / nzl;
+                const size_t r = (size_t)clist[cb + cc] * nzl + (t - cc * nzl);
+                s_re[t] = aks[r];
+                s_im[t] = aks[(size_t)nrect + r];
+            }
+        } else {
+            for (int t = threadIdx.x; t < nc * nzl; t += blockDim.x) {
+                s_re[t] = aks[(size_t)cb * nzl + t];
+                s_im[t] = aks[(size_t)nrect + (size_t)cb * nzl + t];
+            }
         }
         __syncthreads();
         for (int cc = 0; cc < nc; ++cc) {
-            const int col = cb + cc;
-            const double nx = (double)(col / ny_n), ny = (double)(col % ny_n - ky), nz0 = (double)(-kz);
+            const int col = clist ? clist[cb + cc] : cb + cc;
+            const int mlo = czr ? czr[2 * (cb + cc)] : 0;
+            const int mn = czr ? czr[2 * (cb + cc) + 1] : nzl;
+            const double nx = (double)(col / ny_n), ny = (double)(col % ny_n - ky), nz0 = (double)(mlo - kz);
             double ph = fma(nx, s1, fma(ny, s2, nz0 * s3));
             ph -= rint(ph);
             double sn, cs;
@@ -188,9 +216,9 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield(int n, const double* __re
             double k0 = 2.0 * PI * (nx * c.B[0] + ny * c.B[1] + nz0 * c.B[2]);
             double k1 = 2.0 * PI * (nx * c.B[3] + ny * c.B[4] + nz0 * c.B[5]);
             double k2 = 2.0 * PI * (nx * c.B[6] + ny * c.B[7] + nz0 * c.B[8]);
-            const double* pr = s_re + cc * nzl;
-            const double* pi = s_im + cc * nzl;
-            for (int m = 0; m < nzl; ++m) {
+            const double* pr = s_re + cc * nzl + mlo;
+            const double* pi = s_im + cc * nzl + mlo;
+            for (int m = 0; m < mn; ++m) {
                 const double ar = pr[m], ai = pi[m];
                 const double recarg = ai * cs - ar * sn;
                 E0 = fma(-k0, recarg, E0);
@@ -879,7 +907,10 @@ static RecLaunch plan(int n, const KGrid& kg) {
     else if (kg.nzl <= 12) L.CH = 12;
     L.nchunk = (kg.nzl + L.CH - 1) / L.CH;
     L.ncolblk = (kg.ncol + SF_THREADS - 1) / SF_THREADS;
-    long threads1 = (long)L.nchunk * L.ncolblk * SF_THREADS;
+    // the FP64 sphere: one thread per work-list item, columns of the list
+    long threads1 = kg.nfitems > 0 ? (long)((kg.nfitems + SF_THREADS - 1) / SF_THREADS) * SF_THREADS
+                                   : (long)L.nchunk * L.ncolblk * SF_THREADS;
+    const int ncl = kg.nfcol > 0 ? kg.nfcol : kg.ncol;
     long want = 148L * 1536;
     int P = (int)((want + threads1 - 1) / threads1);
     P = std::max(1, std::min(P, (n + 63) / 64));
@@ -887,9 +918,9 @@ static RecLaunch plan(int n, const KGrid& kg) {
     L.P = (n + L.natom_chunk - 1) / L.natom_chunk;
     long threads2 = (long)((n + KF_THREADS - 1) / KF_THREADS) * KF_THREADS;
     int S = (int)((want + threads2 - 1) / threads2);
-    S = std::max(1, std::min(S, kg.ncol));
-    L.cols_per_split = (kg.ncol + S - 1) / S;
-    L.nsplit = (kg.ncol + L.cols_per_split - 1) / L.cols_per_split;
+    S = std::max(1, std::min(S, ncl));
+    L.cols_per_split = (ncl + S - 1) / S;
+    L.nsplit = (ncl + L.cols_per_split - 1) / L.cols_per_split;
     return L;
 }
 
@@ -1021,9 +1052,11 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         k_sfac_reduce<<<rb, 256, 0, st>>>(Pr, TM, nchunk32, kg.ncol, kg.nzl, kx, ky, kz, pre, pim, kg.Ak_hi, kg.kcoe, c,
                                           rs.aks, kg.nrect, fl.energy, part.buf);
     } else {
-        dim3 g1(L.nchunk * L.ncolblk, L.P);
+        const bool sph = kg.nfitems > 0;
+        dim3 g1(sph ? (kg.nfitems + SF_THREADS - 1) / SF_THREADS : L.nchunk * L.ncolblk, L.P);
 #define SFAC(CHV) k_sfac<CHV><<<g1, SF_THREADS, 0, st>>>(n, L.natom_chunk, sx, sy, sz, q, mu, c, kx, ky, kz, kg.ncol, \
-                                                     L.ncolblk, L.nchunk, fl.with_q, fl.with_mu, pre, pim)
+                                                     L.ncolblk, L.nchunk, fl.with_q, fl.with_mu, pre, pim, \
+                                                     sph ? kg.fitems : nullptr, kg.nfitems)
         if (L.CH == 16) SFAC(16);
         else if (L.CH == 12) SFAC(12);
         else SFAC(8);
@@ -1111,12 +1144,16 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         }
     } else {
         size_t smem = sizeof(double) * 2 * KF_COLS * kg.nzl;
+        const bool sph = kg.nfcol > 0;
+        const int ncl = sph ? kg.nfcol : kg.ncol;
         if (grad)
-            k_kfield<1><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
-                                                      rs.aks, kg.nrect, rs.fpart);
+            k_kfield<1><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, ncl, kg.nzl, L.cols_per_split,
+                                                      rs.aks, kg.nrect, rs.fpart, sph ? kg.fcols : nullptr,
+                                                      sph ? kg.fzr : nullptr);
         else
-            k_kfield<0><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, kg.ncol, kg.nzl, L.cols_per_split,
-                                                      rs.aks, kg.nrect, rs.fpart);
+            k_kfield<0><<<g2, KF_THREADS, smem, st>>>(n, sx, sy, sz, c, kx, ky, kz, ncl, kg.nzl, L.cols_per_split,
+                                                      rs.aks, kg.nrect, rs.fpart, sph ? kg.fcols : nullptr,
+                                                      sph ? kg.fzr : nullptr);
         nk++;
     }
     const double scale = 2.0 * 4.0 * PI / c.omega;

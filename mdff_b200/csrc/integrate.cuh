@@ -142,6 +142,55 @@ __global__ void k_nhc_chain(DevScalars* sc, NhcConst c, const double* ke2) {
     sc->s_scale = s;
 }
 
+// chain_nhc2 (src/integration.f90:265-324): the two-thermostat chain of
+// Frenkel and Smit, one quarter/half-step sequence per call (no Suzuki-Yoshida
+// splitting).  Here vxi(1), vxi(2) are thermostat VELOCITIES (the chain
+// forces are divided by Q and the scaling is exp(-vxi dt)), unlike
+// chain_nhcn's momenta.  kin is 2*e_kin from the preceding reduction; the
+// chain's own kin -> s^2 kin update feeds its second G1; writes s_scale.
+__global__ void k_nhc2_chain(DevScalars* sc, NhcConst c, const double* ke2) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double* vxi = sc->vxi;
+    double* xi = sc->xi;
+    const double temp = c.temp, L = c.L, Q1 = c.Q[0], Q2 = c.Q[1];
+    const double dt2 = c.dt * 0.5, dt4 = dt2 * 0.5, dt8 = dt4 * 0.5;
+    double kin = 0.5 * ke2[0];
+    double s = 1.0;
+    double G1 = (2.0 * kin - L * temp) / Q1;
+    double G2 = (Q1 * vxi[0] * vxi[0] - temp) / Q2;
+    vxi[1] = vxi[1] + G2 * dt4;
+    vxi[0] = vxi[0] * exp(-vxi[1] * dt8);
+    vxi[0] = vxi[0] + G1 * dt4;
+    vxi[0] = vxi[0] * exp(-vxi[1] * dt8);
+    s = s * exp(-vxi[0] * dt2);
+    kin = s * s * kin;
+    xi[0] = xi[0] + vxi[0] * dt2;
+    xi[1] = xi[1] + vxi[1] * dt2;
+    G1 = (2.0 * kin - L * temp) / Q1;
+    vxi[0] = vxi[0] * exp(-vxi[1] * dt8);
+    vxi[0] = vxi[0] + G1 * dt4;
+    vxi[0] = vxi[0] * exp(-vxi[1] * dt8);
+    G2 = (Q1 * vxi[0] * vxi[0] - temp) / Q2;
+    vxi[1] = vxi[1] + G2 * dt4;
+    sc->s_scale = s;
+}
+
+// Thermostat energy of nhc2 (src/integration.f90:243-250).  The reference
+// writes vxi^2 / (2 Q), the momentum form of nhcn, although nhc2's vxi are
+// velocities; the conserved quantity of the Frenkel-Smit chain has the
+// kinetic terms Q vxi^2 / 2, used here (deviation D23).  With c.literal the
+// reference's expression is returned instead.
+__global__ void k_nhc2_energy(DevScalars* sc, NhcConst c) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double* v = sc->vxi;
+    const double* x = sc->xi;
+    double e = c.L * c.temp * x[0];
+    e = e + (c.literal ? v[0] * v[0] * 0.5 / c.Q[0] : c.Q[0] * v[0] * v[0] * 0.5);
+    e = e + (c.literal ? v[1] * v[1] * 0.5 / c.Q[1] : c.Q[1] * v[1] * v[1] * 0.5);
+    e = e + c.temp * x[1];
+    sc->e_nvt = e;
+}
+
 // Conserved thermostat energy (src/integration.f90:531-544).
 __global__ void k_nhc_energy(DevScalars* sc, NhcConst c) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;

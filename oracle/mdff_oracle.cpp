@@ -50,6 +50,10 @@
 //   D19 the reference's Metropolis loop reads temp_rmc(6) past its
 //       5-element array (src/rmc.f90:44,531); here the total's temperature
 //       is a parameter.
+//   D23 nhc2's thermostat energy (src/integration.f90:243-250) writes
+//       vxi^2 / (2 Q), the momentum form of nhcn, although chain_nhc2's vxi
+//       are velocities; here Q vxi^2 / 2 (the conserved quantity of the
+//       Frenkel-Smit chain).  nhc_literal = 1 restores the reference's form.
 //   D12 errfc: the reference's fitted erfc (src/functions.f90:28-39, a
 //       published Chebyshev fit, relative error ~1.2e-7) is selectable with
 //       orc_set_erfc_mode(sys, 0); mode 1 (default) uses libm erfc.
@@ -1317,6 +1321,60 @@ void nhcn(orc_sys* s) {
     s->e_nvt = nvt1 + nvt2 + nvt3 + nvt4;
 }
 
+// chain_nhc2 (src/integration.f90:265-324): Frenkel and Smit's two-thermostat
+// chain; vxi are thermostat velocities; kin is updated to s^2 kin inside and
+// the velocities are scaled by s at the end.
+void chain_nhc2(orc_sys* s, double& kin, const double Q[2], double L) {
+    std::vector<double>& vxi = s->vxi;
+    std::vector<double>& xi = s->xi;
+    const double temp = s->temp;
+    double sc = 1.0;
+    const double dt2 = s->dt * 0.5, dt4 = dt2 * 0.5, dt8 = dt4 * 0.5;
+    double G1 = (2.0 * kin - L * temp) / Q[0];
+    double G2 = (Q[0] * vxi[0] * vxi[0] - temp) / Q[1];
+    vxi[1] = vxi[1] + G2 * dt4;
+    vxi[0] = vxi[0] * std::exp(-vxi[1] * dt8);
+    vxi[0] = vxi[0] + G1 * dt4;
+    vxi[0] = vxi[0] * std::exp(-vxi[1] * dt8);
+    sc = sc * std::exp(-vxi[0] * dt2);
+    kin = sc * sc * kin;
+    xi[0] = xi[0] + vxi[0] * dt2;
+    xi[1] = xi[1] + vxi[1] * dt2;
+    G1 = (2.0 * kin - L * temp) / Q[0];
+    vxi[0] = vxi[0] * std::exp(-vxi[1] * dt8);
+    vxi[0] = vxi[0] + G1 * dt4;
+    vxi[0] = vxi[0] * std::exp(-vxi[1] * dt8);
+    G2 = (Q[0] * vxi[0] * vxi[0] - temp) / Q[1];
+    vxi[1] = vxi[1] + G2 * dt4;
+    for (int ia = 0; ia < s->natm; ++ia) {
+        s->vx[ia] = sc * s->vx[ia];
+        s->vy[ia] = sc * s->vy[ia];
+        s->vz[ia] = sc * s->vz[ia];
+    }
+}
+
+// nhc2 (src/integration.f90:205-254): L = 3 (natm - 1), Q(1) = tau^2 T L,
+// Q(2) = tau^2 T.  The thermostat energy uses Q vxi^2 / 2, the kinetic
+// energy of the velocities vxi (D23: the reference writes vxi^2 / (2 Q), the
+// momentum form of nhcn, which is not conserved here); nhc_literal = 1
+// restores the reference's expression.
+void nhc2(orc_sys* s) {
+    const double L = 3.0 * (double(s->natm) - 1.0);
+    const double Q[2] = {s->timesca * s->timesca * s->temp * L, s->timesca * s->timesca * s->temp};
+    double tempi, kin;
+    calc_temp(s, tempi, kin);
+    chain_nhc2(s, kin, Q, L);
+    prop_pos_vel_verlet(s, kin);
+    chain_nhc2(s, kin, Q, L);
+    calc_temp(s, s->temp_r, s->e_kin);
+    const bool lit = s->p.nhc_literal != 0;
+    double e = L * s->temp * s->xi[0];
+    e = e + (lit ? s->vxi[0] * s->vxi[0] * 0.5 / Q[0] : Q[0] * s->vxi[0] * s->vxi[0] * 0.5);
+    e = e + (lit ? s->vxi[1] * s->vxi[1] * 0.5 / Q[1] : Q[1] * s->vxi[1] * s->vxi[1] * 0.5);
+    e = e + s->temp * s->xi[1];
+    s->e_nvt = e;
+}
+
 // A new cell for the same atoms (D14): lattice, tail corrections and k mesh.
 void set_cell(orc_sys* s, const double A[3][3]) {
     for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) s->cell.A[i][j] = A[i][j];
@@ -2023,6 +2081,7 @@ orc_sys* orc_create(const mdff_params* p, int natm, const int* itype, const doub
                     const double* rz, const double A[9]) {
     orc_sys* s = new orc_sys();
     s->p = *p;
+    if (s->p.integrator == MDFF_NVT_NHC2) s->p.nhc_n = 2;   // extended_coordinates_alloc (src/md.f90:335-340)
     symmetrise(s->p);
     set_units(s);
     s->natm = natm;
@@ -3483,6 +3542,7 @@ int orc_step(orc_sys* s, int nsteps, double* rx, double* ry, double* rz, double*
     for (int k = 0; k < nsteps; ++k) {
         s->itime++;
         if (s->p.integrator == MDFF_NVT_NHCN) nhcn(s);
+        else if (s->p.integrator == MDFF_NVT_NHC2) nhc2(s);
         else if (s->p.integrator == MDFF_NPT_NHCNP) nhcnp(s);
         else prop_velocity_verlet(s);
         s->step_rebuilt = 0;

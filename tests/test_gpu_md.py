@@ -64,6 +64,46 @@ def test_lj_nhc_chain_300_steps():
         assert a["nlist_rebuilt"] == b["nlist_rebuilt"]
 
 
+@pytest.mark.parametrize("literal", [0, 1])
+def test_lj_nhc2_300_steps(literal):
+    """nvt-nhc2 (nhc2 + chain_nhc2, src/integration.f90:205-324) step by step
+    against the oracle, with the corrected and with the reference's literal
+    thermostat energy."""
+    s = systems.lj_argon(ncell=4)
+    p = s["params"]
+    p.integrator = abi.NVT_NHC2
+    p.temp = 1.2
+    p.timesca_thermo = 0.5
+    p.nhc_literal = literal
+    te0, to0, re, ro = run_both(s, 300)
+    for a, b in zip(re["thermo"], ro["thermo"]):
+        assert abs(a["h_tot"] - b["h_tot"]) < 1e-8 * abs(b["h_tot"])
+        assert abs(a["e_nvt"] - b["e_nvt"]) < 1e-8 * max(1.0, abs(b["h_tot"]))
+        assert abs(a["temp_r"] - b["temp_r"]) < 1e-8 * b["temp_r"]
+        assert a["nlist_rebuilt"] == b["nlist_rebuilt"]
+    assert rel(re["pos"], ro["pos"]) < 1e-10
+
+
+def test_pim_nhc2_fp64_and_mixed():
+    """nhc2 on the polarisable-ion model: FP64 engine against the oracle, and
+    the mixed path tracking the FP64 path."""
+    s = systems.mgo_pim(grid=(6, 6, 6), rc=6.0, alpha=0.55, kmax=8, temp=1000.0)
+    p = s["params"]
+    p.integrator = abi.NVT_NHC2
+    p.timesca_thermo = 0.05
+    p.conv_tol_ind = 1e-10
+    te0, to0, re, ro = run_both(s, 10)
+    for a, b in zip(re["thermo"], ro["thermo"]):
+        assert abs(a["h_tot"] - b["h_tot"]) < 1e-9 * abs(b["h_tot"])
+        assert abs(a["temp_r"] - b["temp_r"]) < 1e-8 * b["temp_r"]
+    p.precision = abi.PREC_MIXED
+    m = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+    m.md_start(s["vel"])
+    rm = m.step(10)
+    for a, b in zip(rm["thermo"], re["thermo"]):
+        assert abs(a["h_tot"] - b["h_tot"]) < 1e-6 * abs(b["h_tot"])
+
+
 @pytest.mark.parametrize("ext", [(abi.EXT_POLY, 0), (abi.EXT_POLY, 1), (abi.EXT_POLY, 3), (abi.EXT_ASPC, 2)])
 def test_pim_nve_with_extrapolation(ext):
     s = systems.mgo_pim(grid=(6, 6, 6), rc=6.0, alpha=0.55, kmax=8, temp=1000.0)

@@ -140,3 +140,71 @@ def test_tensor_core_structure_factor(case):
     if over.get("doefg"):
         assert rel(out["tc"]["mu"], d["mu"]) < 1e-6
         assert rel(out["tc"]["efg"], d["efg"]) < 1e-6
+
+
+def _production_errors(pos, s):
+    """Mixed path (the production settings: tensor-core k-space, mixed_keps
+    sphere, FP64 low-|k| set, structure-factor reuse) against the plain FP64
+    path (the reference's whole half space, no reuse) at identical positions."""
+    out = {}
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        p = s["params"]
+        p.precision = prec
+        p.kspace_reuse = 1 if prec == abi.PREC_MIXED else 0
+        p.doefg = 1
+        p.efg_period = 0
+        e = mdff_b200.Engine(p, s["itype"], pos, s["cell"])
+        out[prec] = e.engforce()
+        e.close()
+    m, d = out[abi.PREC_MIXED], out[abi.PREC_FP64]
+    return {"F": rel(m["f"], d["f"]), "mu": rel(m["mu"], d["mu"]), "efg": rel(m["efg"], d["efg"]),
+            "tau": rel(m["tau_coul"] + m["tau_nonb"], d["tau_coul"] + d["tau_nonb"]),
+            "u": abs(m["e"]["u_coul"] - d["e"]["u_coul"]) / abs(d["e"]["u_coul"])}
+
+
+def test_mixed_error_at_production_cell():
+    """The graded configuration itself: the 32 440-ion cell with kmax 23 (the
+    mixed path leaves out the 16 974 vectors of the half space outside its
+    exp(-k^2/4 alpha^2) >= 1e-7 sphere).  Bound 1e-6 on forces, dipoles, EFG
+    and stress, at the start positions and at a snapshot of an FP64 NVT
+    trajectory 50 steps in."""
+    s = systems.mgo_production()
+    e0 = _production_errors(s["pos"], s)
+    assert max(e0["F"], e0["mu"], e0["efg"], e0["tau"]) < 1e-6, e0
+    p = s["params"]
+    p.precision = abi.PREC_FP64
+    traj = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+    traj.md_start(s["vel"])
+    traj.step(50, thermo=False)
+    pos50 = traj.positions()
+    traj.close()
+    e50 = _production_errors(pos50, s)
+    assert max(e50["F"], e50["mu"], e50["efg"], e50["tau"]) < 1e-6, e50
+    assert e50["u"] < 1e-6, e50
+
+
+def test_fp64_sphere_matches_mixed_set():
+    """fp64_keps: the FP64 path over the same k sphere as the mixed path (the
+    like-for-like FP64 arm).  Against the plain FP64 path the sphere costs at
+    most the left-out Gaussian weight; against the mixed path (same sphere)
+    what is left is the mixed path's own arithmetic."""
+    s = systems.mgo_pim(grid=(16, 16, 16), rc=10.0, alpha=0.3, kmax=12, vacancy_frac=0.01, seed=3, jitter=0.1)
+    res = {}
+    for name, prec, keps in (("full", abi.PREC_FP64, 0.0), ("sphere", abi.PREC_FP64, 1e-7),
+                             ("mixed", abi.PREC_MIXED, 0.0)):
+        p = s["params"]
+        p.precision = prec
+        p.fp64_keps = keps
+        p.kspace_reuse = 1
+        p.doefg = 1
+        p.conv_tol_ind = 1e-10
+        e = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+        res[name] = e.engforce()
+        res[name + "_k"] = e.kspace_info()
+        e.close()
+    assert res["sphere_k"]["main"] < res["full_k"]["main"] == res["full_k"]["half"]
+    assert res["sphere_k"]["main"] == res["mixed_k"]["main"] + res["mixed_k"]["low"]
+    assert rel(res["sphere"]["f"], res["full"]["f"]) < 1e-6
+    assert rel(res["sphere"]["efg"], res["full"]["efg"]) < 1e-6
+    assert rel(res["mixed"]["f"], res["sphere"]["f"]) < 1e-6
+    assert abs(res["sphere"]["e"]["u_coul"] - res["full"]["e"]["u_coul"]) < 1e-7 * abs(res["full"]["e"]["u_coul"])

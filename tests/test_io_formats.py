@@ -12,7 +12,7 @@ import pytest
 from mdff_b200 import io
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-REF = "/root/reference"
+REF = os.environ.get("MDFF_REFERENCE", "/root/reference")
 
 
 def ex1_frame():

@@ -128,6 +128,33 @@ def test_nhc_conserved_quantity_lj():
     assert t[-100:].mean() > t[:100].mean() + 0.1   # the thermostat heats towards T* = 1.2
 
 
+def test_nhc2_conserved_quantity_lj():
+    """nhc2 / chain_nhc2 (src/integration.f90:205-324): with the thermostat
+    energy Q vxi^2 / 2 + L T xi1 + T xi2 (D23) the extended energy holds; the
+    reference's literal vxi^2 / (2 Q) does not; the chain heats towards T* = 1.2."""
+    def run(literal):
+        s = systems.lj_argon(ncell=4)
+        p = s["params"]
+        p.integrator = abi.NVT_NHC2
+        p.nhc_n = 7          # ignored: nhc2 always has two thermostats
+        p.temp = 1.2
+        p.timesca_thermo = 0.5
+        p.nhc_literal = literal
+        o = oracle.Oracle(p, s["itype"], s["pos"], s["cell"])
+        t0 = o.md_start(s["vel"])
+        out = o.step(300)
+        h = np.array([t["h_tot"] for t in out["thermo"]])
+        t = np.array([t["temp_r"] for t in out["thermo"]])
+        e = np.array([t["e_nvt"] for t in out["thermo"]])
+        return t0, h, t, e
+    t0, h, t, e = run(0)
+    assert np.abs(h - t0["h_tot"]).max() < 2e-3 * abs(t0["h_tot"])
+    assert t[-100:].mean() > t[:100].mean() + 0.05   # heating towards T* = 1.2
+    assert np.abs(e).max() > 1e-2 * abs(t0["h_tot"])   # the thermostat does work
+    _, hl, _, _ = run(1)
+    assert np.abs(hl - t0["h_tot"]).max() > 10 * np.abs(h - t0["h_tot"]).max()
+
+
 def test_nlist_matches_all_pairs_brute_force():
     s = systems.silica_bmh()
     o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])

@@ -7,7 +7,11 @@ energies against the Cambridge Cluster Database values the reference ships,
 read in place when the reference tree is present.  ex4
 (examples/ex4/run_ex4.sh:78-79): electric field gradient of two opposite
 unit charges in a 10 A box (Nymand & Linse values printed by the reference's
-example script).
+example script), and the 9-ion cluster against the GULP table the same script
+prints (run_ex4.sh:159-170).  ex0 (examples/ex0/dl_poly): DL_POLY's static
+energy, virial and long-range corrections of the 256-atom FCC argon
+configuration.  The ex4 cluster and ex0 fixtures are made by
+tests/golden/make_fixtures.py.
 """
 import os
 
@@ -18,7 +22,8 @@ import oracle
 from mdff_b200 import abi
 
 from conftest import REFERENCE, has_reference
-from helpers import lj_params_ex1, rel
+from helpers import EX4_TOL_ETA, EX4_TOL_V, check_ex0, ex0_fcc_case, ex4_cluster_case, lj_params_ex1, rel
+from oracle import efg_stat
 
 
 def test_ex1_lj_forces_energy_stress():
@@ -104,3 +109,21 @@ def test_errfc_matches_reference_fit_accuracy():
     err = max(abs(oracle.errfc(x) - erfc(x)) / erfc(x) for x in xs)
     assert err < 1.3e-7   # the fit's documented relative accuracy
     assert abs(oracle.errfc(-1.0) - (2.0 - oracle.errfc(1.0))) < 1e-15
+
+
+def test_ex4_cluster_efg_vs_gulp():
+    """Ewald EFG of the ex4 cluster (point charges 0.1 / -0.8, lautoES at
+    epsw 1e-8, lefg_vasp_sign), principal values in the NMR convention,
+    against GULP's diagonalised EFGs and asymmetries."""
+    p, itype, pos, cell, gulp = ex4_cluster_case()
+    o = oracle.Oracle(p, itype, pos, cell)
+    efg = -o.engforce()["efg"]   # lefg_vasp_sign (src/efg.f90:486-488)
+    nmr = efg_stat.efg_nmr(efg)[0]
+    assert np.abs(nmr[:, :3] - gulp[:, :3]).max() < EX4_TOL_V
+    assert np.abs(nmr[:, 3] - gulp[:, 3]).max() < EX4_TOL_ETA
+
+
+def test_ex0_dl_poly_static_lj():
+    p, itype, pos, cell, d = ex0_fcc_case()
+    o = oracle.Oracle(p, itype, pos, cell)
+    check_ex0(o.engforce()["e"], abs(np.linalg.det(cell)), d)

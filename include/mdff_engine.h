@@ -295,6 +295,15 @@ int  mdff_profile_detail(mdff_ctx* ctx, double ms[MDFF_NDETAIL], long long count
  * low-|k| set of the mixed path (0 on the FP64 path). */
 int  mdff_kspace_info(mdff_ctx* ctx, long long out[4]);
 
+/* How the context's MD steps ran (no reference counterpart): out[0] steps
+ * replayed from a captured CUDA graph (the whole step, the dipole PCG as a
+ * conditional loop on the device, one host synchronisation per step), out[1]
+ * captures made (one per EFG / non-EFG step kind, again when the lists, pair
+ * table, cell, launch shapes or predictor change), out[2] steps run as plain
+ * launches (constant pressure, the SCF solver, profiling, the predictor's
+ * start-up steps, a step before a reallocation). */
+int  mdff_graph_info(mdff_ctx* ctx, long long out[3]);
+
 /* Launch shape in use (the autotuner's choice, or the defaults): out[0] lanes
  * per atom of the FP64 real-space Ewald kernel, out[1] of the FP32 dipole
  * operator, out[2] and out[3] the FP32 structure-factor atom split and field

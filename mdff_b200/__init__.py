@@ -85,6 +85,7 @@ def lib():
         L.mdff_efg_dist.argtypes = [vp, C.c_int, dp, C.POINTER(abi.EfgDistParams), dp, dp, dp, ip, ip, ip, ip]
         L.mdff_struct_size.argtypes = [C.c_int]
         L.mdff_kspace_info.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.mdff_graph_info.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.mdff_launch_shape.argtypes = [vp, C.POINTER(C.c_int)]
         L.mdff_batch_create.argtypes = [C.POINTER(abi.Params), C.c_int, ip, ip, dp, dp, dp, dp, dp, dp, ip, C.POINTER(vp)]
         L.mdff_batch_destroy.argtypes = [vp]
@@ -164,6 +165,13 @@ class Engine:
         out = (C.c_longlong * 4)()
         self._check(lib().mdff_kspace_info(self._h, out))
         return {"rect": out[0], "half": out[1], "main": out[2], "low": out[3]}
+
+    def graph_info(self):
+        """How the MD steps ran: replayed from a CUDA graph, captures made,
+        plain launches (mdff_graph_info)."""
+        out = (C.c_longlong * 3)()
+        self._check(lib().mdff_graph_info(self._h, out))
+        return {"graph_steps": out[0], "captures": out[1], "plain_steps": out[2]}
 
     def launch_shape(self):
         """Launch shape in use: real-space lanes per atom (FP64, FP32) and the

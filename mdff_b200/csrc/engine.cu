@@ -39,6 +39,26 @@ namespace {
 
 struct Units { double press, boltz, time, coul; };
 
+// Everything a captured MD step holds by value or by address that can change
+// between steps: when any of it differs from the capture's, the step is
+// captured again.  Zero-filled before use so that memcmp covers the padding.
+struct StepKey {
+    const void* ptr[6];   // Verlet lists (vdW, Coulomb): nbr, cnt; dipole pair table
+    int cap[3];           // list capacities, pair-table capacity
+    CellP cell;
+    int g_dir, g_dd, p_mul, s_mul;
+    int efg;              // the step writes the EFG
+    int pmode, pnpt, pshift;   // predictor plan
+    double skin;
+    int n, pad;
+};
+
+// The induced-dipole predictor of one step: coefficients and launch shape.
+struct PredPlan {
+    double coef[16];
+    int mode, npt, shift_from;
+};
+
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -125,6 +145,22 @@ struct mdff_ctx {
     double A_cur[9] = {0};
     double omega0 = 0.0, utail0 = 0.0, ptail0 = 0.0;   // set-up cell volume and tail corrections
     NptState npt;
+    // the MD step as one CUDA graph, replayed once per step (graph[0]: steps
+    // without the EFG, graph[1]: EFG steps); the dipole PCG is a conditional
+    // WHILE node whose test runs on the device
+    cudaStream_t st2 = nullptr;          // capture stream of the PCG loop body
+    bool capturing = false;
+    bool graph_off = false;              // a capture failed: plain launches from then on
+    bool efg_due = true;                 // this evaluation writes the EFG (efg_period)
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    StepKey gkey[2];
+    long glaunch[2] = {0, 0}, gbody[2] = {0, 0};   // kernels per replay outside / per PCG iteration
+    long cap_body = 0;                   // kernels of one PCG iteration, counted while capturing
+    bool pcg_in_graph = false;           // the last captured step solved dipoles in the graph
+    PredPlan coef_up;                    // the predictor coefficients on the device
+    bool coef_valid = false;
+    long long nstep_graph = 0, ncapture = 0, nstep_plain = 0;
 };
 
 namespace {
@@ -442,13 +478,16 @@ __global__ void k_add3(int n, const double* a, const double* b, double* out) {
 
 // Final assembly of multipole_ES (src/field.f90:1930-1990): self (and surface)
 // terms, coul_unit, forces added to the total.
+// The surface term uses the total charge and dipole moments (sums of q r and
+// mu) reduced into the device scalars by the same evaluation.
 __global__ void k_coul_finish(int n, const double* q, const double* mu, double* ef, double* efg, const double* fc,
                               double* fx, double* fy, double* fz, double selfa2, double cu, int do_efg, int lsurf,
-                              double s0, double s1, double s2, double fpi_3V) {
+                              const DevScalars* __restrict__ d, double fpi_3V) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double qi = q[i];
-    double sv[3] = {s0, s1, s2};
+    const double sv[3] = {d->sums[2] + d->sums[5], d->sums[3] + d->sums[6], d->sums[4] + d->sums[7]};
+    const double s0 = sv[0], s1 = sv[1], s2 = sv[2];
     for (int c = 0; c < 3; ++c) {
         double e = ef[(size_t)c * n + i] + 2.0 * selfa2 * mu[(size_t)c * n + i];
         if (lsurf) e += sv[c];
@@ -607,13 +646,16 @@ int fused_initial_field(mdff_ctx* ctx) {
     return check_launch(ctx, "fused_initial_field");
 }
 
-// Extrapolated initial guess from the stored history (extrapolate_dipole_poly,
-// src/field.f90:3807-3920; ASPC predictor, src/field.f90:3924-3984).
-int predict(mdff_ctx* ctx, double* x) {
-    const int n3 = 3 * ctx->n;
+// The predictor of the current step (extrapolate_dipole_poly,
+// src/field.f90:3807-3920; ASPC predictor, src/field.f90:3924-3984):
+// coefficients, mode (0: linear combination, 1: polynomial), points and the
+// history slots to shift.  Constant once itime exceeds the order.
+PredPlan pred_plan(const mdff_ctx* ctx) {
     const int ord = ctx->p.extrapolate_order;
     const int itime = ctx->itime;
-    double coef[16] = {0};
+    PredPlan pl;
+    std::memset(&pl, 0, sizeof pl);
+    double* coef = pl.coef;
     int mode = 0, npt = 1, shift_from = 0;   // shift history slots [shift_from..1] down by one
     if (ctx->p.algo_ext_dipole == MDFF_EXT_ASPC) {
         int eo = (itime >= ord + 1) ? ord : ((itime == 1 || itime == 0) ? 0 : itime - 1);
@@ -639,7 +681,25 @@ int predict(mdff_ctx* ctx, double* x) {
         else { mode = 1; npt = itime + 1; }
         shift_from = ord;
     }
-    CK(cudaMemcpyAsync(ctx->coef, coef, sizeof(coef), cudaMemcpyHostToDevice, ctx->st));
+    pl.mode = mode;
+    pl.npt = npt;
+    pl.shift_from = shift_from;
+    return pl;
+}
+
+// Extrapolated initial guess from the stored history.  The coefficients are
+// uploaded only when they change (never inside a captured step, where the
+// plan is part of the graph's key).
+int predict(mdff_ctx* ctx, double* x) {
+    const int n3 = 3 * ctx->n;
+    const PredPlan pl = pred_plan(ctx);
+    if (!ctx->coef_valid || std::memcmp(pl.coef, ctx->coef_up.coef, sizeof pl.coef) != 0) {
+        if (ctx->capturing) return fail(ctx, MDFF_E_STATE, "predictor coefficients changed inside a captured step");
+        ctx->coef_up = pl;
+        ctx->coef_valid = true;
+        CK(cudaMemcpyAsync(ctx->coef, ctx->coef_up.coef, sizeof(pl.coef), cudaMemcpyHostToDevice, ctx->st));
+    }
+    const int mode = pl.mode, npt = pl.npt, shift_from = pl.shift_from;
     ctx->prof.begin(PK_SOLVER);
     k_extrapolate<<<nb(n3), 256, 0, ctx->st>>>(n3, mode, npt, ctx->hist, ctx->coef, x);
     ctx->prof.end(1);
@@ -702,10 +762,8 @@ int solve_dipoles(mdff_ctx* ctx) {
         launch_reduce_partials(ctx->st, ctx->part.buf, vb, 2, &d->rr, 0);
         k_cg_first<<<1, 32, 0, ctx->st>>>(d, inv_npol);
         ctx->prof.end(4);
-        TRY(sync_scalars(ctx));
-        rmsd = ctx->hsc->rmsd;
-        while ((iscf < p.max_scf_pol_iter && rmsd > p.conv_tol_ind) || iscf < 1) {
-            iscf++;
+        // one PCG iteration (the body of the loop, on the device)
+        auto iteration = [&]() -> int {
             TRY(induced_field(ctx, ctx->cg_d, ctx->Eind));
             ctx->prof.begin(PK_SOLVER);
             k_apply_A<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->Eind, ctx->inv_alpha, ctx->cg_Ad);
@@ -718,9 +776,70 @@ int solve_dipoles(mdff_ctx* ctx) {
             k_cg_scalars<<<1, 32, 0, ctx->st>>>(d, inv_npol, p.conv_tol_ind);
             k_cg_direction<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->cg_z, ctx->cg_d, d);
             ctx->prof.end(8 + (reuse ? (ctx->rs.low.ncol > 0 ? 2 : 1) : 0));
+            return check_launch(ctx, "pcg iteration");
+        };
+        if (ctx->capturing) {
+            // inside a captured MD step: a conditional WHILE node whose body is
+            // one iteration and whose test (k_cg_cond) runs on the device after
+            // k_cg_first and after each iteration; the host reads the count
+            // and the residual after the step (solve_finish)
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t g = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            CK(cudaStreamGetCaptureInfo(ctx->st, &cs, nullptr, &g, nullptr, nullptr));
+            cudaGraphConditionalHandle h;
+            CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+            k_cg_cond<<<1, 32, 0, ctx->st>>>(d, p.max_scf_pol_iter, p.conv_tol_ind, h);
+            TRY(check_launch(ctx, "pcg test"));
+            CK(cudaStreamGetCaptureInfo(ctx->st, &cs, nullptr, &g, &deps, &nd));
+            alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];   // holds a union
+            std::memset(cp_raw, 0, sizeof cp_raw);
+            cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            CK(cudaGraphAddNode(&node, g, deps, nd, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            CK(cudaStreamUpdateCaptureDependencies(ctx->st, &node, 1, cudaStreamSetCaptureDependencies));
+            const cudaStream_t main_st = ctx->st;
+            const long l0 = ctx->prof.launches;
+            ctx->st = ctx->st2;
+            cudaError_t e = cudaStreamBeginCaptureToGraph(ctx->st, body, nullptr, nullptr, 0,
+                                                          cudaStreamCaptureModeThreadLocal);
+            int r = MDFF_OK;
+            if (e != cudaSuccess) {
+                r = fail(ctx, MDFF_E_CUDA, std::string("capture of the PCG body: ") + cudaGetErrorString(e));
+            } else {
+                r = iteration();
+                if (r == MDFF_OK) {
+                    k_cg_cond<<<1, 32, 0, ctx->st>>>(d, p.max_scf_pol_iter, p.conv_tol_ind, h);
+                    r = check_launch(ctx, "pcg test");
+                }
+                cudaGraph_t out = body;
+                cudaError_t e2 = cudaStreamEndCapture(ctx->st, &out);
+                if (r == MDFF_OK && e2 != cudaSuccess)
+                    r = fail(ctx, MDFF_E_CUDA, std::string("capture of the PCG body: ") + cudaGetErrorString(e2));
+            }
+            ctx->st = main_st;
+            ctx->cap_body = ctx->prof.launches - l0 + 1;   // + the loop test
+            ctx->prof.launches = l0 + 1;                    // the test before the loop
+            TRY(r);
+            ctx->pcg_in_graph = true;
+            iscf = 0;
+            rmsd = 0.0;
+        } else {
             TRY(sync_scalars(ctx));
             rmsd = ctx->hsc->rmsd;
-            if (!std::isfinite(rmsd)) return fail(ctx, MDFF_E_NONFINITE, "non-finite residual in the dipole solve");
+            while ((iscf < p.max_scf_pol_iter && rmsd > p.conv_tol_ind) || iscf < 1) {
+                iscf++;
+                TRY(iteration());
+                TRY(sync_scalars(ctx));
+                rmsd = ctx->hsc->rmsd;
+                if (!std::isfinite(rmsd)) return fail(ctx, MDFF_E_NONFINITE, "non-finite residual in the dipole solve");
+            }
         }
     }
     TRY(check_launch(ctx, "solve_dipoles"));
@@ -731,11 +850,24 @@ int solve_dipoles(mdff_ctx* ctx) {
     ctx->prof.end(2);
     // store the induced dipoles at t (src/field.f90:3440)
     CK(cudaMemcpyAsync(ctx->hist, ctx->mu_ind, sizeof(double) * n3, cudaMemcpyDeviceToDevice, ctx->st));
+    ctx->rec_acc_ready = reuse;
+    if (ctx->capturing) return MDFF_OK;   // solve_finish after the step
     ctx->en.scf_iter = iscf;
     ctx->en.scf_rmsd = rmsd;
     if (iscf >= p.max_scf_pol_iter && rmsd > p.conv_tol_ind && p.algo_moment_from_pola == MDFF_POLA_PCG)
         return fail(ctx, MDFF_E_NOCONV, "induced-dipole solve did not converge within max_scf_pol_iter");
-    ctx->rec_acc_ready = reuse;
+    return MDFF_OK;
+}
+
+// After a step that ran as a graph: the PCG's count and residual from the
+// device scalars, with the host loop's checks.
+int solve_finish(mdff_ctx* ctx) {
+    const DevScalars& h = *ctx->hsc;
+    ctx->en.scf_iter = h.iter;
+    ctx->en.scf_rmsd = h.rmsd;
+    if (!std::isfinite(h.rmsd)) return fail(ctx, MDFF_E_NONFINITE, "non-finite residual in the dipole solve");
+    if (h.iter >= ctx->p.max_scf_pol_iter && h.rmsd > ctx->p.conv_tol_ind)
+        return fail(ctx, MDFF_E_NOCONV, "induced-dipole solve did not converge within max_scf_pol_iter");
     return MDFF_OK;
 }
 
@@ -825,11 +957,17 @@ int autotune(mdff_ctx* ctx) {
     return check_launch(ctx, "autotune");
 }
 
+int engforce_finish(mdff_ctx* ctx);
+
 // engforce_driver (src/field.f90:1111-1166) on the device; results stay in
-// device memory and ctx->hsc/en after the trailing sync.
+// device memory and ctx->hsc/en after the trailing sync.  Inside a captured
+// step only the launches are recorded (engforce_finish runs after the step).
+// The EFG is written when doefg and the evaluation is due one (efg_due:
+// every efg_period MD steps, always outside MD).
 int engforce_device(mdff_ctx* ctx) {
     const int n = ctx->n;
     const mdff_params& p = ctx->p;
+    const bool efg = p.doefg && ctx->efg_due;
     if (!p.lvnlist) TRY(build_lists(ctx, 0.0));
     else if (!ctx->have_list) TRY(build_lists(ctx, p.skindiff));   // lists dropped (an interrupted RMC chain)
     ctx->prof.begin(PK_OTHER);
@@ -870,38 +1008,51 @@ int engforce_device(mdff_ctx* ctx) {
         f.dd = dip ? 1 : 0;
         f.damp = 1;
         f.field = p.doefield ? 1 : 0;
-        f.efg = p.doefg ? 1 : 0;
+        f.efg = efg ? 1 : 0;
         f.forces = 1;
         CK(cudaMemsetAsync(ctx->ef, 0, sizeof(double) * n3, ctx->st));
-        if (p.doefg) CK(cudaMemsetAsync(ctx->efg, 0, sizeof(double) * 6 * n, ctx->st));
+        if (efg) CK(cudaMemsetAsync(ctx->efg, 0, sizeof(double) * 6 * n, ctx->st));
         ctx->prof.begin(PK_DIR);
         launch_ewald_dir(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->type, ctx->q, ctx->mu, ctx->cell, coul_list(ctx),
                          ctx->pc, f, ctx->ef, ctx->efg, ctx->fcoul, ctx->part, ctx->dsc, ctx->g_dir);
         ctx->prof.end(2);
-        RecFlags rf{ctx->any_q ? 1 : 0, dip ? 1 : 0, p.doefield ? 1 : 0, (p.doefg || dip) ? 1 : 0, 1, 1, p.precision,
+        RecFlags rf{ctx->any_q ? 1 : 0, dip ? 1 : 0, p.doefield ? 1 : 0, (efg || dip) ? 1 : 0, 1, 1, p.precision,
                     ctx->rec_acc_ready ? 1 : 0};
         ctx->rec_acc_ready = false;
         launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->q, ctx->mu, ctx->cell, ctx->kg, rf, ctx->rs, ctx->ef,
-                         p.doefg ? ctx->efg : nullptr, ctx->fcoul, ctx->part, ctx->dsc, &ctx->prof);
+                         efg ? ctx->efg : nullptr, ctx->fcoul, ctx->part, ctx->dsc, &ctx->prof);
         int vb = std::min(592, nb(n));
         ctx->prof.begin(PK_OTHER);
         k_coul_sums<<<vb, 256, 0, ctx->st>>>(n, ctx->q, ctx->mu, ctx->x, ctx->y, ctx->z, ctx->part.buf);
         launch_reduce_partials(ctx->st, ctx->part.buf, vb, 8, ctx->dsc->sums, 0);
-        ctx->prof.end(2);
+        const double tpi_V = 2.0 * PI / ctx->cell.omega;
+        k_coul_finish<<<nb(n), 256, 0, ctx->st>>>(n, ctx->q, ctx->mu, ctx->ef, ctx->efg, ctx->fcoul, ctx->fx, ctx->fy,
+                                                  ctx->fz, selfa2(ctx), ctx->u.coul, efg ? 1 : 0, p.lsurf, ctx->dsc,
+                                                  2.0 * tpi_V / 3.0);
+        ctx->prof.end(3);
         TRY(check_launch(ctx, "coulomb"));
     }
+    if (ctx->capturing) return MDFF_OK;
     TRY(sync_scalars(ctx));
+    return engforce_finish(ctx);
+}
+
+// The host side of an evaluation once its device scalars are in ctx->hsc:
+// energies, virials and stresses (multipole_ES's and the pair loops' sums,
+// src/field.f90:1930-2050).
+int engforce_finish(mdff_ctx* ctx) {
+    const mdff_params& p = ctx->p;
     const DevScalars& h = *ctx->hsc;
+    {   // the solve's count and residual were set by solve_dipoles / solve_finish
+        const int it = ctx->en.scf_iter;
+        const double rm = ctx->en.scf_rmsd;
+        std::memset(&ctx->en, 0, sizeof ctx->en);
+        ctx->en.scf_iter = it;
+        ctx->en.scf_rmsd = rm;
+    }
     if (p.lcoulomb) {
         double cu = ctx->u.coul;
         double tpi_V = 2.0 * PI / ctx->cell.omega;
-        double s[3] = {h.sums[2] + h.sums[5], h.sums[3] + h.sums[6], h.sums[4] + h.sums[7]};
-        ctx->prof.begin(PK_OTHER);
-        k_coul_finish<<<nb(n), 256, 0, ctx->st>>>(n, ctx->q, ctx->mu, ctx->ef, ctx->efg, ctx->fcoul, ctx->fx, ctx->fy,
-                                                  ctx->fz, selfa2(ctx), cu, p.doefg, p.lsurf, s[0], s[1], s[2],
-                                                  2.0 * tpi_V / 3.0);
-        ctx->prof.end(1);
-        TRY(check_launch(ctx, "coul_finish"));
         double u_dir = h.dir[0], u_rec = h.rec[0] * 2.0 * tpi_V;
         double u_self = -selfa(ctx) * h.sums[0] - selfa2(ctx) * h.sums[1];
         double u_pol = 0.5 * h.upol[0];
@@ -1181,12 +1332,21 @@ int npt_step(mdff_ctx* ctx) {
     return MDFF_OK;
 }
 
-// One MD step (body of md_run's loop, src/runmd.f90:266-277).
-int md_step(mdff_ctx* ctx) {
+// Skin allowance of the Verlet-list check: a shrinking cell brings pairs
+// beyond the list radius closer by the same factor, and that margin comes off
+// the displacement allowance.
+double skin_allowance(const mdff_ctx* ctx) {
+    const double shrink = std::max(0.0, 1.0 - ctx->npt.scale / ctx->npt.scale_build);
+    return ctx->p.skindiff - shrink * rlist_max(ctx, ctx->p.skindiff);
+}
+
+// The launches of one MD step (body of md_run's loop, src/runmd.f90:266-277)
+// up to the Verlet-list check; the host syncs inside (the force evaluation's)
+// are skipped while the step is being captured.
+int md_launches(mdff_ctx* ctx) {
     const int n = ctx->n;
     const mdff_params& p = ctx->p;
     const double dt = p.dt * ctx->u.time;
-    ctx->itime++;
     if (p.integrator == MDFF_NPT_NHCNP) {
         TRY(npt_step(ctx));
     } else if (p.integrator == MDFF_NVE_VV) {
@@ -1235,26 +1395,169 @@ int md_step(mdff_ctx* ctx) {
         ctx->prof.end(1);
     }
     TRY(check_launch(ctx, "step"));
-    ctx->last_rebuilt = 0;
     if (p.lvnlist) {
         // positions unchanged since the force call: sx is current
         ctx->prof.begin(PK_NLIST);
-        // a shrinking cell brings pairs beyond the list radius closer by the
-        // same factor: that margin comes off the displacement allowance
-        const double shrink = std::max(0.0, 1.0 - ctx->npt.scale / ctx->npt.scale_build);
-        const double skin_eff = p.skindiff - shrink * rlist_max(ctx, p.skindiff);
-        launch_skin_check(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->xs, ctx->ys, ctx->zs, ctx->cell, skin_eff,
-                          ctx->part, ctx->dsc);
+        launch_skin_check(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, ctx->xs, ctx->ys, ctx->zs, ctx->cell,
+                          skin_allowance(ctx), ctx->part, ctx->dsc);
         ctx->prof.end(2);
         TRY(check_launch(ctx, "skin"));
     }
-    TRY(sync_scalars(ctx));
+    return MDFF_OK;
+}
+
+// After the step's scalars are on the host: temperature and the list rebuild
+// that vnlistcheck asks for.
+int step_end(mdff_ctx* ctx) {
     set_kin(ctx);
-    if (p.lvnlist && ctx->hsc->rebuild) {
-        TRY(build_lists(ctx, p.skindiff));
+    ctx->last_rebuilt = 0;
+    if (ctx->p.lvnlist && ctx->hsc->rebuild) {
+        TRY(build_lists(ctx, ctx->p.skindiff));
         ctx->last_rebuilt = 1;
     }
     return MDFF_OK;
+}
+
+int md_step_plain(mdff_ctx* ctx) {
+    ctx->nstep_plain++;
+    TRY(md_launches(ctx));
+    TRY(sync_scalars(ctx));
+    return step_end(ctx);
+}
+
+// ---- the MD step as a CUDA graph --------------------------------------------
+// A step whose launches do not depend on host decisions made during it is
+// captured once (one graph for the EFG steps, one for the others) and
+// replayed; the dipole PCG runs as a conditional WHILE node with its test on
+// the device, and the host syncs once per step, after it.  Steps that need
+// the host in between (constant pressure, the SCF solver, profiling, the
+// predictor's start-up steps, a context whose lists or pair table are about
+// to be reallocated) run as plain launches.
+
+bool graph_eligible(const mdff_ctx* ctx) {
+    const mdff_params& p = ctx->p;
+    if (ctx->graph_off || ctx->prof.on) return false;
+    if (p.integrator == MDFF_NPT_NHCNP) return false;
+    if (!p.lvnlist || !ctx->have_list || !ctx->forces_valid) return false;
+    if (p.autotune && !ctx->tuned) return false;
+    if (p.lcoulomb && ctx->npol > 0) {
+        if (p.algo_moment_from_pola != MDFF_POLA_PCG) return false;
+        const PredPlan pl = pred_plan(ctx);
+        if (!ctx->coef_valid || std::memcmp(pl.coef, ctx->coef_up.coef, sizeof pl.coef) != 0) return false;
+    }
+    if (p.lcoulomb && p.precision == MDFF_PREC_MIXED &&
+        (!ctx->ddcnt || !ctx->ddrec || (size_t)ctx->n * coul_list(ctx).cap > ctx->ddtab_cap))
+        return false;
+    return true;
+}
+
+StepKey step_key(const mdff_ctx* ctx) {
+    StepKey k;
+    std::memset(&k, 0, sizeof k);
+    k.ptr[0] = ctx->lv.nbr; k.ptr[1] = ctx->lv.cnt;
+    k.ptr[2] = ctx->lc.nbr; k.ptr[3] = ctx->lc.cnt;
+    k.ptr[4] = ctx->ddtab;  k.ptr[5] = ctx->ddnbr;
+    k.cap[0] = ctx->lv.cap; k.cap[1] = ctx->lc.cap; k.cap[2] = (int)std::min<size_t>(ctx->ddtab_cap, 0x7fffffff);
+    k.cell = ctx->cell;
+    k.g_dir = ctx->g_dir; k.g_dd = ctx->g_dd; k.p_mul = ctx->rs.p_mul; k.s_mul = ctx->rs.s_mul;
+    k.efg = (ctx->p.doefg && ctx->efg_due) ? 1 : 0;
+    if (ctx->p.lcoulomb && ctx->npol > 0) {
+        const PredPlan pl = pred_plan(ctx);
+        k.pmode = pl.mode; k.pnpt = pl.npt; k.pshift = pl.shift_from;
+    }
+    k.skin = skin_allowance(ctx);
+    k.n = ctx->n;
+    return k;
+}
+
+void drop_graph(mdff_ctx* ctx, int slot) {
+    if (ctx->gexec[slot]) cudaGraphExecDestroy(ctx->gexec[slot]);
+    if (ctx->graph[slot]) cudaGraphDestroy(ctx->graph[slot]);
+    ctx->gexec[slot] = nullptr;
+    ctx->graph[slot] = nullptr;
+}
+
+void drop_graphs(mdff_ctx* ctx) {
+    drop_graph(ctx, 0);
+    drop_graph(ctx, 1);
+}
+
+int capture_step(mdff_ctx* ctx, int slot, const StepKey& key) {
+    drop_graph(ctx, slot);
+    CK(cudaStreamSynchronize(ctx->st));
+    const long l0 = ctx->prof.launches;
+    ctx->capturing = true;
+    ctx->pcg_in_graph = false;
+    ctx->cap_body = 0;
+    int rc = MDFF_OK;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        rc = fail(ctx, MDFF_E_CUDA, std::string("capture of the MD step: ") + cudaGetErrorString(e));
+    } else {
+        rc = md_launches(ctx);
+        cudaError_t e2 = cudaStreamEndCapture(ctx->st, &g);
+        if (rc == MDFF_OK && e2 != cudaSuccess)
+            rc = fail(ctx, MDFF_E_CUDA, std::string("capture of the MD step: ") + cudaGetErrorString(e2));
+    }
+    ctx->capturing = false;
+    const long captured = ctx->prof.launches - l0;
+    ctx->prof.launches = l0;
+    if (rc != MDFF_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    cudaGraphExec_t ge = nullptr;
+    e = cudaGraphInstantiate(&ge, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(ctx, MDFF_E_CUDA, std::string("instantiation of the MD step graph: ") + cudaGetErrorString(e));
+    }
+    ctx->graph[slot] = g;
+    ctx->gexec[slot] = ge;
+    ctx->gkey[slot] = key;
+    ctx->glaunch[slot] = captured;
+    ctx->gbody[slot] = ctx->pcg_in_graph ? ctx->cap_body : 0;
+    ctx->ncapture++;
+    return MDFF_OK;
+}
+
+int md_step_graph(mdff_ctx* ctx) {
+    const StepKey key = step_key(ctx);
+    const int slot = key.efg;
+    if (!ctx->gexec[slot] || std::memcmp(&key, &ctx->gkey[slot], sizeof key) != 0) {
+        if (capture_step(ctx, slot, key) != MDFF_OK) {
+            // a capture that fails leaves nothing launched: run the step as
+            // plain launches, and from now on
+            cudaGetLastError();
+            ctx->graph_off = true;
+            return md_step_plain(ctx);
+        }
+    }
+    CK(cudaGraphLaunch(ctx->gexec[slot], ctx->st));
+    ctx->nstep_graph++;
+    TRY(sync_scalars(ctx));
+    const bool pcg = ctx->gbody[slot] > 0;
+    ctx->prof.launches += ctx->glaunch[slot] + (pcg ? ctx->gbody[slot] * (long)ctx->hsc->iter : 0);
+    if (pcg) {
+        TRY(solve_finish(ctx));
+    } else {
+        ctx->en.scf_iter = 0;
+        ctx->en.scf_rmsd = 0.0;
+    }
+    TRY(engforce_finish(ctx));
+    return step_end(ctx);
+}
+
+// One MD step (body of md_run's loop, src/runmd.f90:266-277); the EFG is due
+// every efg_period steps.
+int md_step(mdff_ctx* ctx) {
+    const mdff_params& p = ctx->p;
+    ctx->itime++;
+    ctx->efg_due = p.efg_period <= 1 || ctx->itime % p.efg_period == 0;
+    const int rc = graph_eligible(ctx) ? md_step_graph(ctx) : md_step_plain(ctx);
+    ctx->efg_due = true;
+    return rc;
 }
 
 }  // namespace
@@ -2443,6 +2746,14 @@ int mdff_launch_shape(mdff_ctx* ctx, int out[4]) {
     return MDFF_OK;
 }
 
+int mdff_graph_info(mdff_ctx* ctx, long long out[3]) {
+    if (!ctx || !out) return MDFF_E_ARG;
+    out[0] = ctx->nstep_graph;
+    out[1] = ctx->ncapture;
+    out[2] = ctx->nstep_plain;
+    return MDFF_OK;
+}
+
 int mdff_kspace_info(mdff_ctx* ctx, long long out[4]) {
     if (!ctx || !out) return MDFF_E_ARG;
     if (!ctx->have_system) return fail(ctx, MDFF_E_STATE, "set_system first");
@@ -2520,6 +2831,7 @@ int mdff_create(const mdff_params* p, mdff_ctx** out) {
     if (p->device < 0 || p->device >= ndev) { ctx->err = "device ordinal out of range"; *out = ctx; return MDFF_E_ARG; }
     cudaSetDevice(p->device);
     e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->hsc, sizeof(DevScalars));
     ctx->prof.st = ctx->st;
     if (e != cudaSuccess) { ctx->err = std::string("stream/pinned alloc: ") + cudaGetErrorString(e); *out = ctx; return MDFF_E_CUDA; }
@@ -2536,7 +2848,9 @@ void mdff_destroy(mdff_ctx* ctx) {
         free_all(ctx);
         if (ctx->ddtab) cudaFree(ctx->ddtab);
         if (ctx->ddnbr) cudaFree(ctx->ddnbr);
+        drop_graphs(ctx);
         cudaStreamDestroy(ctx->st);
+        if (ctx->st2) cudaStreamDestroy(ctx->st2);
     }
     if (ctx->hsc) cudaFreeHost(ctx->hsc);
     delete ctx;
@@ -2550,6 +2864,8 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
     if (natm < 1 || !itype || !rx || !ry || !rz || !A) return fail(ctx, MDFF_E_ARG, "invalid system arguments");
     cudaSetDevice(ctx->p.device);
     cudaStreamSynchronize(ctx->st);
+    drop_graphs(ctx);   // they hold the addresses of the buffers freed here
+    ctx->coef_valid = false;
     free_all(ctx);
     ctx->lv = NList();
     ctx->lc = NList();
@@ -3593,6 +3909,7 @@ int mdff_checkpoint_load(mdff_ctx* ctx, const void* buf, size_t len) {
         hdr.nparam_bytes != (int)sizeof(mdff_params))
         return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: checkpoint of another system");
     if (len != ck_size(ctx)) return fail(ctx, MDFF_E_ARG, "mdff_checkpoint_load: size mismatch");
+    drop_graphs(ctx);
     const char* in = (const char*)buf + sizeof hdr;
     const mdff_params pp = ck_params(ctx->p);
     if (std::memcmp(in, &pp, sizeof pp) != 0)

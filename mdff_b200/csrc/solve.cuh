@@ -108,6 +108,19 @@ __global__ void k_cg_direction(int n3, const double* __restrict__ z, double* dve
     if (t < n3) dvec[t] = fma(b, dvec[t], z[t]);
 }
 
+// Test of the PCG loop when the MD step runs as a CUDA graph (the condition
+// of its conditional WHILE node): another iteration while
+// (iter < max_it and rmsd > tol) or iter < 1, the host loop's test, and none
+// once the residual is not finite (the host reports that after the step).
+// The iteration cap makes the loop finite whatever the residuals do.
+__global__ void k_cg_cond(const DevScalars* __restrict__ sc, int max_it, double tol, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double r = sc->rmsd;
+    const int it = sc->iter;
+    const bool go = ((it < max_it && r > tol) || it < 1) && isfinite(r);
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
 __global__ void k_cg_first(DevScalars* sc, double inv_npol) {
     if (threadIdx.x != 0) return;
     sc->rz = sc->rz_new;

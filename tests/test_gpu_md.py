@@ -137,3 +137,83 @@ def test_pim_pcg_kspace_reuse_vs_oracle(ext):
         assert abs(a["pressure_tot"] - b["pressure_tot"]) < 1e-8 * max(1.0, abs(b["pressure_tot"]))
     assert rel(re["f"], ro["f"]) < 1e-8
 
+
+
+def _pim_pcg_nhc():
+    s = systems.mgo_pim(grid=(8, 8, 8), rc=6.0, alpha=0.5, kmax=8, temp=1500.0, integrator=abi.NVT_NHCN)
+    p = s["params"]
+    p.algo_moment_from_pola = abi.POLA_PCG
+    p.algo_ext_dipole = abi.EXT_ASPC
+    p.extrapolate_order = 3
+    p.kspace_reuse = 1
+    p.conv_tol_ind = 1e-9
+    p.doefg = 1
+    return s
+
+
+def _run(s, nsteps, profile=False, **over):
+    p = s["params"]
+    for k, v in over.items():
+        setattr(p, k, v)
+    e = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+    e.enable_profile(profile)
+    e.md_start(s["vel"])
+    out = e.step(nsteps)
+    return e, out
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_graph_steps_equal_plain_steps(prec):
+    """Steps replayed from the captured CUDA graph (the whole step, the PCG as a
+    conditional loop on the device) leave bit for bit the state, forces and
+    thermodynamics of the same steps run as plain launches (profiling keeps a
+    context on plain launches)."""
+    s = _pim_pcg_nhc()
+    runs = {}
+    for prof in (False, True):
+        e, out = _run(s, 20, profile=prof, precision=prec)
+        runs[prof] = (e.positions(), e.velocities(), out, e.graph_info())
+    g, pl = runs[False], runs[True]
+    assert g[3]["graph_steps"] >= 10 and g[3]["captures"] >= 1, g[3]
+    assert pl[3]["graph_steps"] == 0 and pl[3]["plain_steps"] == 20, pl[3]
+    assert np.array_equal(g[0], pl[0]) and np.array_equal(g[1], pl[1])
+    assert np.array_equal(g[2]["f"], pl[2]["f"])
+    for a, b in zip(g[2]["thermo"], pl[2]["thermo"]):
+        assert a["h_tot"] == b["h_tot"] and a["scf_iter"] == b["scf_iter"] and a["scf_rmsd"] == b["scf_rmsd"]
+
+
+@pytest.mark.parametrize("integ", [abi.NVE_VV, abi.NVT_NHC2])
+def test_graph_steps_lj_and_nhc2(integ):
+    """The graph path of the pair-only integrators: LJ NVE and nvt-nhc2 against
+    the oracle, with the steps replayed from graphs."""
+    s = systems.lj_argon(ncell=4)
+    p = s["params"]
+    p.integrator = integ
+    p.temp = 1.2
+    p.timesca_thermo = 0.5
+    te0, to0, re, ro = run_both(s, 50)
+    for a, b in zip(re["thermo"], ro["thermo"]):
+        assert abs(a["h_tot"] - b["h_tot"]) < 1e-8 * abs(b["h_tot"])
+        assert a["nlist_rebuilt"] == b["nlist_rebuilt"]
+    e = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+    e.md_start(s["vel"])
+    e.step(10)
+    assert e.graph_info()["graph_steps"] >= 9
+
+
+def test_efg_period():
+    """efg_period = 10: the EFG is written on steps 10, 20, ...; forces and
+    the trajectory are bit for bit those of EFG at every step, and after step
+    15 the context's EFG is still that of step 10."""
+    s = _pim_pcg_nhc()
+    e1, _ = _run(s, 10, efg_period=1)
+    nmr10 = e1.efg_nmr()[0]
+    out1 = e1.step(5)
+    e10, out10 = _run(s, 15, efg_period=10)
+    assert np.array_equal(e1.positions(), e10.positions())
+    assert np.array_equal(out1["f"], out10["f"])
+    assert np.array_equal(e10.efg_nmr()[0], nmr10)
+    assert not np.array_equal(e1.efg_nmr()[0], nmr10)
+    out1b = e1.step(5)
+    out10b = e10.step(5)
+    assert np.array_equal(e1.efg_nmr()[0], e10.efg_nmr()[0])   # step 20 writes the EFG in both

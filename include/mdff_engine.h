@@ -235,6 +235,12 @@ typedef struct mdff_efg_dist_params {
 int  mdff_struct_size(int which);   /* 5 efg_dist_params, 6 frame_header, 7 rmc_params, 8 rmc_result,
                                        9 rmc_efg_params */
 
+/* The real-space kernels' FP64 erfc (e^{-x^2} times a degree-13 Chebyshev fit
+ * of erfc(x) e^{x^2} per half-unit interval on [0, 4.5), CUDA's erfc
+ * elsewhere) and CUDA's erfc, evaluated on the device at n host points x:
+ * ex2[n] and ref[n].  A check of the fit; no reference counterpart. */
+int  mdff_erfc_check(int device, int n, const double* x, double* ex2, double* ref);
+
 /* Measured FMA throughput of the device in TFLOP/s: out[0] FP64, out[1]
  * FP32, out[2] packed FP32x2 (fma.rn.f32x2).  The roofline denominators of
  * the engine's FMA-bound kernels; no reference counterpart. */

@@ -86,6 +86,7 @@ def lib():
         L.mdff_struct_size.argtypes = [C.c_int]
         L.mdff_kspace_info.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.mdff_graph_info.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.mdff_erfc_check.argtypes = [C.c_int, C.c_int, dp, dp, dp]
         L.mdff_launch_shape.argtypes = [vp, C.POINTER(C.c_int)]
         L.mdff_batch_create.argtypes = [C.POINTER(abi.Params), C.c_int, ip, ip, dp, dp, dp, dp, dp, dp, ip, C.POINTER(vp)]
         L.mdff_batch_destroy.argtypes = [vp]
@@ -128,6 +129,17 @@ def measure_pipes(device=0):
     if rc != 0:
         raise EngineError(rc, "mdff_measure_pipes failed")
     return tuple(float(x) for x in out)
+
+
+def erfc_check(x, device=0):
+    """The real-space kernels' erfc and CUDA's erfc at the points x, both
+    evaluated on the device (mdff_erfc_check): (erfc_ex2, erfc)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    a, b = np.empty_like(x), np.empty_like(x)
+    rc = lib().mdff_erfc_check(int(device), len(x), _dp(x), _dp(a), _dp(b))
+    if rc != 0:
+        raise EngineError(rc, "mdff_erfc_check failed")
+    return a, b
 
 
 def params_default():

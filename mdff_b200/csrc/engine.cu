@@ -2607,6 +2607,33 @@ int mdff_opt_lbfgs(mdff_ctx* ctx, int itmax, double eps, mdff_opt_result* out) {
 }
 
 
+// erfc_ex2 (the real-space kernels' erfc) and CUDA's erfc at the same points.
+__global__ void k_erfc_check(int n, const double* __restrict__ x, double* __restrict__ ex2, double* __restrict__ ref) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = x[i];
+    ex2[i] = mdff::erfc_ex2(v, exp(-v * v));
+    ref[i] = erfc(v);
+}
+
+int mdff_erfc_check(int device, int n, const double* x, double* ex2, double* ref) {
+    if (n < 1 || !x || !ex2 || !ref) return MDFF_E_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return MDFF_E_CUDA;
+    double* d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * 3 * (size_t)n) != cudaSuccess) return MDFF_E_NOMEM;
+    int rc = MDFF_OK;
+    if (cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) rc = MDFF_E_CUDA;
+    if (rc == MDFF_OK) {
+        k_erfc_check<<<(n + 255) / 256, 256>>>(n, d, d + n, d + 2 * (size_t)n);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpy(ex2, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(ref, d + 2 * (size_t)n, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = MDFF_E_CUDA;
+    }
+    cudaFree(d);
+    return rc;
+}
+
 int mdff_measure_pipes(int device, double out[3]) {
     if (!out) return MDFF_E_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return MDFF_E_CUDA;

@@ -179,3 +179,52 @@ def test_batch_64_uneven_configurations():
     b.set_params(space.apply(base, theta_t))
     L1, g1, _ = b.loss_grad()
     assert L1 < 1e-18 * max(1.0, L)
+
+
+def test_batch_64_matches_oracle_and_central_differences():
+    """The force-matching workload itself (64 configurations of 200-2000 ions,
+    69 642 in all, targets from parameters perturbed 5 %): the engine's loss and
+    12-parameter gradient against the oracle's summed over the 64
+    configurations (induced dipoles to 1e-10 on both sides), and against
+    central differences of the batch loss (h = 1e-5 relative, dipoles to
+    1e-12 so that the differences resolve the gradient to 1e-5)."""
+    import mdff_b200
+    confs = systems.mgo_batch()
+    rng = np.random.default_rng(7)
+    for tol in (1e-10, 1e-12):
+        base = _base(tol)
+        space = fit.mgo_space(base)
+        theta0 = space.get(base)
+        theta_t = theta0 * (1.0 + 0.05 * np.random.default_rng(7).standard_normal(len(theta0)))
+        ft, tt = _targets(base, space, confs, theta_t)
+        b = mdff_b200.Batch(base, confs)
+        b.set_targets(ft, tt, 1.0, 0.01)
+        L, g, its = b.loss_grad()
+        ge = space.project(g, theta0)
+        if tol == 1e-10:
+            consts = fit.batch_constants([len(c["itype"]) for c in confs], 1.0, 0.01)
+            go = abi.ParamGrad()
+            lo = 0.0
+            for conf, f, t, (cf, cs) in zip(confs, ft, tt, consts):
+                o = oracle.Oracle(_cfg_params(base, conf), conf["itype"], conf["pos"], conf["cell"])
+                l, go, _ = o.loss_grad(f, t, cf, cs, go)
+                lo += l
+            assert abs(L - lo) / abs(lo) < 1e-8, (L, lo)
+            gr = space.project(go, theta0)
+            err = np.abs(ge - gr) * np.abs(theta0) / np.abs(gr * theta0).max()
+            assert err.max() < 1e-7, list(zip(space.names, ge, gr))
+        else:
+            fd = np.empty_like(ge)
+            for k in range(len(theta0)):
+                h = 1e-5 * abs(theta0[k])
+                vals = []
+                for sgn in (1.0, -1.0):
+                    th = theta0.copy()
+                    th[k] += sgn * h
+                    b.set_params(space.apply(base, th))
+                    vals.append(b.loss_grad(want_grad=False)[0])
+                fd[k] = (vals[0] - vals[1]) / (2.0 * h)
+            floor = 50.0 * np.finfo(float).eps * abs(L) / (1e-5 * np.abs(theta0))
+            ok = np.abs(ge - fd) <= np.maximum(1e-5 * np.abs(fd), floor)
+            assert ok.all(), list(zip(space.names, ge, fd, floor))
+        b.close()

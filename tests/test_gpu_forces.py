@@ -171,3 +171,23 @@ def test_static_dipoles_and_polarisable():
     assert rel(re["f"], ro["f"]) < 1e-9
     assert rel(re["efg"], ro["efg"]) < 1e-9
     assert_energies(re, ro, ["u_coul"], tol=1e-10)
+
+
+def test_config3_pim_3000_ion_cell_vs_oracle():
+    """Config 3's cell itself: 3000 MgO ions on the 10 x 10 x 30 site grid
+    (21.06 x 21.06 x 63.18 A), rc 10 A, alpha 0.3, kmax 10^3 (4630 k-vectors),
+    polarisable O with Tang-Toennies damping, dipoles by PCG: forces,
+    energies, stress, dipoles and EFG of the FP64 engine against the oracle."""
+    s = systems.mgo_pim()
+    p = s["params"]
+    p.conv_tol_ind = 1e-11
+    p.doefg = 1
+    assert len(s["itype"]) == 3000
+    a = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"]).engforce()
+    b = oracle.Oracle(p, s["itype"], s["pos"], s["cell"]).engforce()
+    assert rel(a["f"], b["f"]) < 1e-9
+    assert rel(a["mu"], b["mu"]) < 1e-9
+    assert rel(a["efg"], b["efg"]) < 1e-9
+    assert rel(a["tau_coul"], b["tau_coul"]) < 1e-9
+    assert abs(a["e"]["u_coul"] - b["e"]["u_coul"]) < 1e-11 * abs(b["e"]["u_coul"])
+    assert abs(a["e"]["u_bmhft"] - b["e"]["u_bmhft"]) < 1e-11 * abs(b["e"]["u_bmhft"])

@@ -217,3 +217,39 @@ def test_efg_period():
     out1b = e1.step(5)
     out10b = e10.step(5)
     assert np.array_equal(e1.efg_nmr()[0], e10.efg_nmr()[0])   # step 20 writes the EFG in both
+
+
+def test_lj_nve_1000_steps():
+    """Config 1 at its length: 500-atom LJ argon, NVE velocity Verlet, 1000
+    steps of dt 0.005, engine against the oracle.  The two sum the pair forces
+    in different orders, so the trajectories drift apart at the rate of the
+    system's chaos from last-bit differences; energies stay within 1e-7 and
+    both conserve e_tot."""
+    s = systems.lj_argon()
+    te0, to0, re, ro = run_both(s, 1000)
+    e = np.array([t["e_tot"] for t in re["thermo"]])
+    o = np.array([t["e_tot"] for t in ro["thermo"]])
+    assert np.abs(e - o).max() < 1e-7 * np.abs(o).max()
+    assert np.abs(e - te0["e_tot"]).max() < 2e-3 * abs(te0["e_tot"])
+    assert sum(t["nlist_rebuilt"] for t in re["thermo"]) > 10
+
+
+def test_config3_pim_3000_ions_nve_200_steps():
+    """Config 3's cell (3000 ions, 10 x 10 x 30 sites, rc 10, alpha 0.3,
+    kmax 10^3): 200 NVE steps of the mixed path tracking the FP64 path's
+    energy, with the EFG of every step."""
+    s = systems.mgo_pim()
+    res = {}
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        p = s["params"]
+        p.precision = prec
+        p.kspace_reuse = 1
+        p.algo_ext_dipole = abi.EXT_ASPC
+        p.extrapolate_order = 3
+        e = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+        t0 = e.md_start(s["vel"])
+        out = e.step(200)
+        res[prec] = (t0, np.array([t["e_tot"] for t in out["thermo"]]), out)
+    (t0, ed, od), (_, em, om) = res[abi.PREC_FP64], res[abi.PREC_MIXED]
+    assert np.abs(em - ed).max() < 1e-6 * abs(t0["e_tot"])
+    assert np.abs(ed - t0["e_tot"]).max() < 1e-3 * abs(t0["e_tot"])

@@ -36,8 +36,9 @@ __device__ __forceinline__ double erfc_fit(double x) {
 
 // erfc(x) = e^{-x^2} erfcx(x) for 0 <= x < 4.5: erfcx from Chebyshev
 // interpolants of degree 13 on the intervals [j/2, j/2 + 1/2) in the variable
-// t = 4x - (2j + 1), fitted here in 50-digit arithmetic to erfc(x) e^{x^2}
-// (relative error 2.1e-16 in FP64 Horner).  The Ewald kernels already hold
+// t = 4x - (2j + 1), fitted in 50-digit arithmetic to erfc(x) e^{x^2}
+// (mdff_b200/csrc/fit_erfcx.py; relative error 2.1e-16 in FP64 Horner; the
+// caller's e^{-x^2} from a rounded x^2 adds x^2 2^-53).  The Ewald kernels already hold
 // e^{-x^2} for the F1, F2, F3 terms, so erfc costs one short polynomial
 // instead of a second exponential; outside the range CUDA's erfc is used.
 static __device__ const double c_erfcx[9][14] = {

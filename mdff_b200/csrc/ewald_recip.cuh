@@ -695,6 +695,99 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac64_low(int n, int natom_chun
     }
 }
 
+// Per position update: the FP64 phase tables of the low set, per atom
+// X[nx] = e^{2 pi i nx s1} (nx = 0..kxl), Y[ny] (ny = -kyl..kyl), Z[nz]
+// (nz = -kzl..kzl), from the direct coordinates.
+__global__ void k_lowk_tables(int n, const double* __restrict__ sx, const double* __restrict__ sy,
+                              const double* __restrict__ sz, int kxl, int kyl, int kzl, int TW,
+                              double2* __restrict__ xyz) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)n * TW) return;
+    const int a = (int)(t / TW), e = (int)(t % TW);
+    const int XW = kxl + 1, YW = 2 * kyl + 1;
+    double s, m;
+    if (e < XW) { s = sx[a]; m = e; }
+    else if (e < XW + YW) { s = sy[a]; m = e - XW - kyl; }
+    else { s = sz[a]; m = e - XW - YW - kzl; }
+    double w = m * (s - rint(s));
+    w -= rint(w);
+    double sn, cs;
+    sincospi(2.0 * w, &sn, &cs);
+    xyz[t] = make_double2(cs, sn);
+}
+
+// Pass 1 over the low set from the phase tables: one thread per list column
+// (the columns sorted by length), one block per range of atoms.  For column
+// (nx, ny) and atom a: W = X[nx] Y[ny], A0 = W (q + i (nx m1 + ny m2)),
+// A1 = W m3, and S[nz] += (A0 + i nz A1) Z[nz] over the column's nz range --
+// six FMAs per (atom, k) and no transcendental.
+constexpr int LT_TILE = 32;     // atoms staged per round
+constexpr int LT_THREADS = 128; // >= columns of the low set (checked at set-up)
+template <int NZB>
+__global__ void __launch_bounds__(LT_THREADS) k_sfac64_tab(int n, int natom_chunk, const double2* __restrict__ xyz,
+                                                           int kxl, int kyl, int kzl, int TW,
+                                                           const double* __restrict__ q, const double* __restrict__ mu,
+                                                           CellP c, const int* __restrict__ cols, int ncol, int nzmax,
+                                                           int with_q, int with_mu, double* __restrict__ part_re,
+                                                           double* __restrict__ part_im) {
+    extern __shared__ double2 s_tab[];   // [LT_TILE][TW]
+    __shared__ double t_q[LT_TILE], t_m1[LT_TILE], t_m2[LT_TILE], t_m3[LT_TILE];
+    const int t = threadIdx.x;
+    const int cc = t < ncol ? t : ncol - 1;
+    const int nx = cols[4 * cc], ny = cols[4 * cc + 1], nz0 = cols[4 * cc + 2], nn = cols[4 * cc + 3];
+    const int XW = kxl + 1, YW = 2 * kyl + 1;
+    const int ex = nx, ey = XW + ny + kyl, ez = XW + YW + nz0 + kzl;
+    const double fnx = nx, fny = ny;
+    double sre[NZB], sim[NZB];
+#pragma unroll
+    for (int m = 0; m < NZB; ++m) { sre[m] = 0.0; sim[m] = 0.0; }
+    const int p = blockIdx.x;
+    const int a0 = p * natom_chunk, a1 = min(n, a0 + natom_chunk);
+    for (int base = a0; base < a1; base += LT_TILE) {
+        const int tn = min(LT_TILE, a1 - base);
+        __syncthreads();
+        for (int u = t; u < tn * TW; u += LT_THREADS) s_tab[u] = xyz[(size_t)base * TW + u];
+        if (t < tn) {
+            const int ia = base + t;
+            t_q[t] = with_q ? q[ia] : 0.0;
+            double u0 = 0, u1 = 0, u2 = 0;
+            if (with_mu) { u0 = mu[ia]; u1 = mu[n + ia]; u2 = mu[2 * n + ia]; }
+            t_m1[t] = 2.0 * PI * (c.B[0] * u0 + c.B[3] * u1 + c.B[6] * u2);
+            t_m2[t] = 2.0 * PI * (c.B[1] * u0 + c.B[4] * u1 + c.B[7] * u2);
+            t_m3[t] = 2.0 * PI * (c.B[2] * u0 + c.B[5] * u1 + c.B[8] * u2);
+        }
+        __syncthreads();
+        for (int a = 0; a < tn; ++a) {
+            const double2* row = s_tab + a * TW;
+            const double2 X = row[ex], Y = row[ey];
+            const double wr = fma(X.x, Y.x, -X.y * Y.y), wi = fma(X.x, Y.y, X.y * Y.x);
+            const double qa = t_q[a], km = fma(fnx, t_m1[a], fny * t_m2[a]), m3 = t_m3[a];
+            const double a0r = fma(wr, qa, -wi * km), a0i = fma(wi, qa, wr * km);
+            const double a1r = wr * m3, a1i = wi * m3;
+#pragma unroll
+            for (int m = 0; m < NZB; ++m) {
+                if (m < nn) {
+                    const double fz = (double)(nz0 + m);
+                    const double vr = fma(-fz, a1i, a0r), vi = fma(fz, a1r, a0i);
+                    const double2 Z = row[ez + m];
+                    sre[m] = fma(vr, Z.x, fma(-vi, Z.y, sre[m]));
+                    sim[m] = fma(vr, Z.y, fma(vi, Z.x, sim[m]));
+                }
+            }
+        }
+    }
+    if (t < ncol) {
+        const size_t plane = (size_t)nzmax * ncol;
+#pragma unroll
+        for (int m = 0; m < NZB; ++m)
+            if (m < nzmax) {
+                const size_t idx = (size_t)p * plane + (size_t)m * ncol + t;
+                part_re[idx] = sre[m];
+                part_im[idx] = sim[m];
+            }
+    }
+}
+
 // One warp per low-set k-vector: sum of the atom-chunk partials, A_k S(k),
 // energy and stress terms.
 __global__ void k_sfac64_low_reduce(int P, int ncol, int nzmax, const int* __restrict__ cols,
@@ -805,6 +898,93 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield64_low(int n, const uint32
             fpart[3 * n + i] = G0; fpart[4 * n + i] = G1; fpart[5 * n + i] = G2;
             fpart[6 * n + i] = G3; fpart[7 * n + i] = G4; fpart[8 * n + i] = G5;
         }
+    }
+}
+
+// Pass 2 over the low set from the phase tables: thread = atom, blockIdx.y =
+// range of list columns, the range's A_k S staged in shared memory.  With
+// e_k = W Z[nz] (W = X[nx] Y[ny]) the column sums of k_kfield64_low are
+// R_j = Im(conj(W) U_j), Q_j = Re(conj(W) U_j) with U_j = sum_m m^j a_m conj(Z_m)
+// (m counted from the column's first nz): no transcendental per column.
+template <int GRAD>
+__global__ void __launch_bounds__(KF_THREADS) k_kfield64_tab(int n, const double2* __restrict__ xyz, int kxl, int kyl,
+                                                             int kzl, int TW, CellP c, const int* __restrict__ cols,
+                                                             int ncol, int nzmax, const double* __restrict__ aks,
+                                                             double* __restrict__ fpart) {
+    extern __shared__ double2 s_a[];   // [per][nzmax]
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int per = (ncol + gridDim.y - 1) / gridDim.y;
+    const int cbeg = blockIdx.y * per, cend = min(ncol, cbeg + per);
+    fpart += (size_t)blockIdx.y * 9 * n;
+    const double* aim_base = aks + (size_t)ncol * nzmax;
+    for (int u = threadIdx.x; u < (cend - cbeg) * nzmax; u += blockDim.x) {
+        const size_t r = (size_t)cbeg * nzmax + u;
+        s_a[u] = make_double2(aks[r], aim_base[r]);
+    }
+    __syncthreads();
+    const bool active = i < n;
+    const int ii = active ? i : 0;
+    const double2* row = xyz + (size_t)ii * TW;
+    const int XW = kxl + 1, YW = 2 * kyl + 1;
+    const double dk0 = 2.0 * PI * c.B[2], dk1 = 2.0 * PI * c.B[5], dk2 = 2.0 * PI * c.B[8];
+    double E0 = 0, E1 = 0, E2 = 0, G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
+    for (int cc = cbeg; cc < cend; ++cc) {
+        const int inx = cols[4 * cc], iny = cols[4 * cc + 1], inz0 = cols[4 * cc + 2], nzn = cols[4 * cc + 3];
+        const double2 X = row[inx], Y = row[XW + iny + kyl];
+        const double wr = fma(X.x, Y.x, -X.y * Y.y), wi = fma(X.x, Y.y, X.y * Y.x);
+        const double2* zr = row + XW + YW + inz0 + kzl;
+        const double2* ar = s_a + (size_t)(cc - cbeg) * nzmax;
+        double u0r = 0, u0i = 0, u1r = 0, u1i = 0, u2r = 0, u2i = 0;
+        for (int m = 0; m < nzn; ++m) {
+            const double2 a = ar[m], z = zr[m];
+            const double tr = fma(a.x, z.x, a.y * z.y), ti = fma(a.y, z.x, -a.x * z.y);   // a conj(z)
+            const double fm = (double)m;
+            u0r += tr; u0i += ti;
+            u1r = fma(fm, tr, u1r); u1i = fma(fm, ti, u1i);
+            if (GRAD) { u2r = fma(fm * fm, tr, u2r); u2i = fma(fm * fm, ti, u2i); }
+        }
+        const double R0 = fma(wr, u0i, -wi * u0r), R1 = fma(wr, u1i, -wi * u1r);
+        const double kb0 = 2.0 * PI * (inx * c.B[0] + iny * c.B[1] + inz0 * c.B[2]);
+        const double kb1 = 2.0 * PI * (inx * c.B[3] + iny * c.B[4] + inz0 * c.B[5]);
+        const double kb2 = 2.0 * PI * (inx * c.B[6] + iny * c.B[7] + inz0 * c.B[8]);
+        E0 -= fma(kb0, R0, dk0 * R1);
+        E1 -= fma(kb1, R0, dk1 * R1);
+        E2 -= fma(kb2, R0, dk2 * R1);
+        if (GRAD) {
+            const double Q0 = fma(wr, u0r, wi * u0i), Q1 = fma(wr, u1r, wi * u1i), Q2 = fma(wr, u2r, wi * u2i);
+            G0 += kb0 * kb0 * Q0 + 2.0 * kb0 * dk0 * Q1 + dk0 * dk0 * Q2;
+            G1 += kb1 * kb1 * Q0 + 2.0 * kb1 * dk1 * Q1 + dk1 * dk1 * Q2;
+            G2 += kb2 * kb2 * Q0 + 2.0 * kb2 * dk2 * Q1 + dk2 * dk2 * Q2;
+            G3 += kb0 * kb1 * Q0 + (kb0 * dk1 + dk0 * kb1) * Q1 + dk0 * dk1 * Q2;
+            G4 += kb0 * kb2 * Q0 + (kb0 * dk2 + dk0 * kb2) * Q1 + dk0 * dk2 * Q2;
+            G5 += kb1 * kb2 * Q0 + (kb1 * dk2 + dk1 * kb2) * Q1 + dk1 * dk2 * Q2;
+        }
+    }
+    if (active) {
+        fpart[i] = E0; fpart[n + i] = E1; fpart[2 * n + i] = E2;
+        if (GRAD) {
+            fpart[3 * n + i] = G0; fpart[4 * n + i] = G1; fpart[5 * n + i] = G2;
+            fpart[6 * n + i] = G3; fpart[7 * n + i] = G4; fpart[8 * n + i] = G5;
+        }
+    }
+}
+
+// The low set's field pass: the table form when the tables exist.
+void launch_kfield_low(cudaStream_t st, int n, const uint32_t* fixed, CellP c, LowK& lk, bool grad) {
+    const dim3 g((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT);
+    if (lk.xyz) {
+        const int per = (lk.ncol + LK_SPLIT - 1) / LK_SPLIT;
+        const size_t sm = sizeof(double2) * (size_t)per * lk.nzmax;
+        if (grad)
+            k_kfield64_tab<1><<<g, KF_THREADS, sm, st>>>(n, lk.xyz, lk.kxl, lk.kyl, lk.kzl, lk.TW, c, lk.col, lk.ncol,
+                                                         lk.nzmax, lk.aks, lk.fpart);
+        else
+            k_kfield64_tab<0><<<g, KF_THREADS, sm, st>>>(n, lk.xyz, lk.kxl, lk.kyl, lk.kzl, lk.TW, c, lk.col, lk.ncol,
+                                                         lk.nzmax, lk.aks, lk.fpart);
+    } else if (grad) {
+        k_kfield64_low<1><<<g, KF_THREADS, 0, st>>>(n, fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+    } else {
+        k_kfield64_low<0><<<g, KF_THREADS, 0, st>>>(n, fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
     }
 }
 
@@ -969,7 +1149,15 @@ int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* 
     if (rs.tab_epoch == rs.want_epoch) return 0;
     k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab, rs.low.ncol > 0 ? rs.low.tab : nullptr);
     rs.tab_epoch = rs.want_epoch;
-    if (!rs.tc.on) return 1;
+    int nk = 1;
+    if (rs.low.xyz) {
+        const LowK& lk = rs.low;
+        const long nt = (long)n * lk.TW;
+        k_lowk_tables<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(n, sx, sy, sz, lk.kxl, lk.kyl, lk.kzl, lk.TW,
+                                                                    lk.xyz);
+        nk++;
+    }
+    if (!rs.tc.on) return nk;
     const TcK& t = rs.tc;
     const long nxy = (long)t.npad * t.XYW, nb = (long)t.npad * (t.N / 2);
     tcs::k_tc_xy<<<(unsigned)((nxy + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kx, t.ky, t.XYW, t.xy);
@@ -977,7 +1165,7 @@ int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* 
     const long na = (long)t.ntile_f * 128 * (t.KZ / 16), nt = (long)t.ntile_f * 128 * t.XYW;
     tcf::k_tcf_aimage<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(n, t.ntile_f, rs.fixed, t.kz, t.nzl, t.KZ, t.aimg);
     tcf::k_tcf_xyt<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(t.npad, t.ntile_f, t.xy, t.XYW, t.xyt);
-    return 5;
+    return nk + 4;
 }
 
 #define CUDA_COPY_ACC(st, dst, src, bytes) cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (st))
@@ -1067,15 +1255,31 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     if (fl.energy && !fl.reuse) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
     if (low && !fl.reuse) {
         LowK& lk = rs.low;
-        const int nch = (lk.nzmax + TM - 1) / TM;
-        const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;
-        dim3 gl(nch * cb, lk.P);
-        const size_t lplane = (size_t)lk.P * lk.nzmax * lk.ncol;
-        k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, rs.fixed, lk.tab, q, mu, c, lk.col, lk.ncol, lk.nzmax,
-                                                nch, fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
         const int lb = (lk.ncol * lk.nzmax * 32 + 255) / 256;
-        k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane, lk.Ak,
-                                                lk.kcoe, c, lk.aks, fl.energy, part.buf);
+        if (lk.xyz) {
+            // from the per-atom phase tables (built with the position update)
+            const size_t lplane = (size_t)lk.P2 * lk.nzmax * lk.ncol;
+            const size_t sm = sizeof(double2) * LT_TILE * lk.TW;
+#define SF64T(NZ) k_sfac64_tab<NZ><<<lk.P2, LT_THREADS, sm, st>>>(n, lk.natom_chunk2, lk.xyz, lk.kxl, lk.kyl, lk.kzl, \
+                                                          lk.TW, q, mu, c, lk.col, lk.ncol, lk.nzmax, fl.with_q, \
+                                                          fl.with_mu, lk.part, lk.part + lplane)
+            if (lk.nzb == 8) SF64T(8);
+            else if (lk.nzb == 16) SF64T(16);
+            else if (lk.nzb == 24) SF64T(24);
+            else SF64T(32);
+#undef SF64T
+            k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P2, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane,
+                                                    lk.Ak, lk.kcoe, c, lk.aks, fl.energy, part.buf);
+        } else {
+            const int nch = (lk.nzmax + TM - 1) / TM;
+            const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;
+            dim3 gl(nch * cb, lk.P);
+            const size_t lplane = (size_t)lk.P * lk.nzmax * lk.ncol;
+            k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, rs.fixed, lk.tab, q, mu, c, lk.col, lk.ncol,
+                                                    lk.nzmax, nch, fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
+            k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane, lk.Ak,
+                                                    lk.kcoe, c, lk.aks, fl.energy, part.buf);
+        }
         if (fl.energy) launch_reduce_partials(st, part.buf, lb, 7, d->rec, 1);
         nk += 2 + (fl.energy ? 1 : 0);
     }
@@ -1112,13 +1316,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         nsplit_f = tcf::NQ;
         nk += 1;
         if (low) {
-            LowK& lk = rs.low;
-            if (grad)
-                k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
-            else
-                k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+            launch_kfield_low(st, n, rs.fixed, c, rs.low, grad);
             nk++;
         }
     } else if (mixed) {
@@ -1133,13 +1331,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
                                                          L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
         nk += 2;
         if (low) {
-            LowK& lk = rs.low;
-            if (grad)
-                k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
-            else
-                k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+            launch_kfield_low(st, n, rs.fixed, c, rs.low, grad);
             nk++;
         }
     } else {

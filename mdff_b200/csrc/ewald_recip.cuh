@@ -697,13 +697,14 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac64_low(int n, int natom_chun
 
 // Per position update: the FP64 phase tables of the low set, per atom
 // X[nx] = e^{2 pi i nx s1} (nx = 0..kxl), Y[ny] (ny = -kyl..kyl), Z[nz]
-// (nz = -kzl..kzl), from the direct coordinates.
+// (nz = -kzl..kzl), from the direct coordinates; entry-major, [TW][n], so
+// that a warp's atoms read one entry in one coalesced access.
 __global__ void k_lowk_tables(int n, const double* __restrict__ sx, const double* __restrict__ sy,
                               const double* __restrict__ sz, int kxl, int kyl, int kzl, int TW,
                               double2* __restrict__ xyz) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)n * TW) return;
-    const int a = (int)(t / TW), e = (int)(t % TW);
+    const int e = (int)(t / n), a = (int)(t % n);
     const int XW = kxl + 1, YW = 2 * kyl + 1;
     double s, m;
     if (e < XW) { s = sx[a]; m = e; }
@@ -746,7 +747,10 @@ __global__ void __launch_bounds__(LT_THREADS) k_sfac64_tab(int n, int natom_chun
     for (int base = a0; base < a1; base += LT_TILE) {
         const int tn = min(LT_TILE, a1 - base);
         __syncthreads();
-        for (int u = t; u < tn * TW; u += LT_THREADS) s_tab[u] = xyz[(size_t)base * TW + u];
+        for (int u = t; u < tn * TW; u += LT_THREADS) {
+            const int e = u / tn, a = u - e * tn;
+            s_tab[a * TW + e] = xyz[(size_t)e * n + base + a];
+        }
         if (t < tn) {
             const int ia = base + t;
             t_q[t] = with_q ? q[ia] : 0.0;
@@ -924,19 +928,19 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield64_tab(int n, const double
     __syncthreads();
     const bool active = i < n;
     const int ii = active ? i : 0;
-    const double2* row = xyz + (size_t)ii * TW;
+    const double2* row = xyz + ii;   // entry e of this atom at row[e * n]
     const int XW = kxl + 1, YW = 2 * kyl + 1;
     const double dk0 = 2.0 * PI * c.B[2], dk1 = 2.0 * PI * c.B[5], dk2 = 2.0 * PI * c.B[8];
     double E0 = 0, E1 = 0, E2 = 0, G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
     for (int cc = cbeg; cc < cend; ++cc) {
         const int inx = cols[4 * cc], iny = cols[4 * cc + 1], inz0 = cols[4 * cc + 2], nzn = cols[4 * cc + 3];
-        const double2 X = row[inx], Y = row[XW + iny + kyl];
+        const double2 X = row[(size_t)inx * n], Y = row[(size_t)(XW + iny + kyl) * n];
         const double wr = fma(X.x, Y.x, -X.y * Y.y), wi = fma(X.x, Y.y, X.y * Y.x);
-        const double2* zr = row + XW + YW + inz0 + kzl;
+        const double2* zr = row + (size_t)(XW + YW + inz0 + kzl) * n;
         const double2* ar = s_a + (size_t)(cc - cbeg) * nzmax;
         double u0r = 0, u0i = 0, u1r = 0, u1i = 0, u2r = 0, u2i = 0;
         for (int m = 0; m < nzn; ++m) {
-            const double2 a = ar[m], z = zr[m];
+            const double2 a = ar[m], z = zr[(size_t)m * n];
             const double tr = fma(a.x, z.x, a.y * z.y), ti = fma(a.y, z.x, -a.x * z.y);   // a conj(z)
             const double fm = (double)m;
             u0r += tr; u0i += ti;

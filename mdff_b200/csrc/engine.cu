@@ -3121,15 +3121,23 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                     lk.kzl = std::max(lk.kzl, std::max(std::abs(C_.lo - kg.kmax[2]), std::abs(C_.lo + C_.nn - 1 - kg.kmax[2])));
                 }
                 lk.TW = (lk.kxl + 1) + (2 * lk.kyl + 1) + (2 * lk.kzl + 1);
-                lk.nzb = nzmax <= 8 ? 8 : nzmax <= 16 ? 16 : nzmax <= 24 ? 24 : 32;
-                const bool tab_form = lk.ncol <= LT_THREADS && nzmax <= 32 &&
-                                      sizeof(double2) * LT_TILE * lk.TW <= 48 * 1024;
+                const bool tab_form = sizeof(double2) * LT_TILE * lk.TW <= 48 * 1024;
                 lk.xyz = nullptr;
+                lk.items = nullptr;
+                lk.nitems = 0;
                 if (tab_form) {
-                    int P2 = std::min(4 * 148, std::max(1, n / 16));
+                    std::vector<int> it;
+                    for (int q = 0; q < lk.ncol; ++q)
+                        for (int m = 0; m < cl[q].nn; m += LQ) { it.push_back(q); it.push_back(m); }
+                    lk.nitems = (int)(it.size() / 2);
+                    const int xb = (lk.nitems + LT_THREADS - 1) / LT_THREADS;
+                    int P2 = std::max(1, std::min((4 * 148 + xb - 1) / xb, n / 16));
                     lk.natom_chunk2 = (n + P2 - 1) / P2;
                     lk.P2 = (n + lk.natom_chunk2 - 1) / lk.natom_chunk2;
                     TRY(dalloc(ctx, &lk.xyz, (size_t)n * lk.TW));
+                    TRY(dalloc(ctx, &lk.items, it.size()));
+                    CK(cudaMemcpyAsync(lk.items, it.data(), sizeof(int) * it.size(), cudaMemcpyHostToDevice, ctx->st));
+                    CK(cudaStreamSynchronize(ctx->st));
                 }
                 TRY(dalloc(ctx, &lk.col, cols.size()));
                 CK(cudaMemcpyAsync(lk.col, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice, ctx->st));

@@ -253,7 +253,9 @@ struct LowK {
     // Y[ny] (-kyl..kyl), Z[nz] (-kzl..kzl), TW entries per atom
     int kxl = 0, kyl = 0, kzl = 0, TW = 0;
     double2* xyz = nullptr;   // [n][TW]
-    int P2 = 1, natom_chunk2 = 0, nzb = 8;   // atom splits of k_sfac64_tab; its nz register count
+    int P2 = 1, natom_chunk2 = 0;        // atom splits of k_sfac64_tab
+    int* items = nullptr;                // [nitems][2]: (list column, first m) of its work items
+    int nitems = 0;
 };
 
 // Tensor-core structure factor of the mixed path (ewald_tc.cuh).

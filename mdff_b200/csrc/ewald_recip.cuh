@@ -717,40 +717,44 @@ __global__ void k_lowk_tables(int n, const double* __restrict__ sx, const double
     xyz[t] = make_double2(cs, sn);
 }
 
-// Pass 1 over the low set from the phase tables: one thread per list column
-// (the columns sorted by length), one block per range of atoms.  For column
-// (nx, ny) and atom a: W = X[nx] Y[ny], A0 = W (q + i (nx m1 + ny m2)),
-// A1 = W m3, and S[nz] += (A0 + i nz A1) Z[nz] over the column's nz range --
-// six FMAs per (atom, k) and no transcendental.
+// Pass 1 over the low set from the phase tables: one thread per work item =
+// (list column, chunk of up to LQ consecutive nz), one block row per range of
+// atoms.  For column (nx, ny) and atom a: W = X[nx] Y[ny],
+// A0 = W (q + i (nx m1 + ny m2)), A1 = W m3, and S[nz] += (A0 + i nz A1) Z[nz]
+// over the chunk -- six FMAs per (atom, k), no transcendental, and chunks
+// short enough that columns of any length waste few slots.
 constexpr int LT_TILE = 32;     // atoms staged per round
-constexpr int LT_THREADS = 128; // >= columns of the low set (checked at set-up)
-template <int NZB>
+constexpr int LT_THREADS = 128;
+constexpr int LQ = 4;           // nz per work item
 __global__ void __launch_bounds__(LT_THREADS) k_sfac64_tab(int n, int natom_chunk, const double2* __restrict__ xyz,
                                                            int kxl, int kyl, int kzl, int TW,
                                                            const double* __restrict__ q, const double* __restrict__ mu,
                                                            CellP c, const int* __restrict__ cols, int ncol, int nzmax,
-                                                           int with_q, int with_mu, double* __restrict__ part_re,
+                                                           const int* __restrict__ items, int nitems, int with_q,
+                                                           int with_mu, double* __restrict__ part_re,
                                                            double* __restrict__ part_im) {
     extern __shared__ double2 s_tab[];   // [LT_TILE][TW]
     __shared__ double t_q[LT_TILE], t_m1[LT_TILE], t_m2[LT_TILE], t_m3[LT_TILE];
     const int t = threadIdx.x;
-    const int cc = t < ncol ? t : ncol - 1;
-    const int nx = cols[4 * cc], ny = cols[4 * cc + 1], nz0 = cols[4 * cc + 2], nn = cols[4 * cc + 3];
+    const int it = blockIdx.x * LT_THREADS + t;
+    const bool valid = it < nitems;
+    const int item = items[2 * (valid ? it : nitems - 1)], m0 = items[2 * (valid ? it : nitems - 1) + 1];
+    const int cc = item;
+    const int nx = cols[4 * cc], ny = cols[4 * cc + 1], nz0 = cols[4 * cc + 2] + m0;
+    const int nn = min(LQ, cols[4 * cc + 3] - m0);
     const int XW = kxl + 1, YW = 2 * kyl + 1;
     const int ex = nx, ey = XW + ny + kyl, ez = XW + YW + nz0 + kzl;
     const double fnx = nx, fny = ny;
-    double sre[NZB], sim[NZB];
+    double sre[LQ], sim[LQ];
 #pragma unroll
-    for (int m = 0; m < NZB; ++m) { sre[m] = 0.0; sim[m] = 0.0; }
-    const int p = blockIdx.x;
+    for (int m = 0; m < LQ; ++m) { sre[m] = 0.0; sim[m] = 0.0; }
+    const int p = blockIdx.y;
     const int a0 = p * natom_chunk, a1 = min(n, a0 + natom_chunk);
     for (int base = a0; base < a1; base += LT_TILE) {
         const int tn = min(LT_TILE, a1 - base);
         __syncthreads();
-        for (int u = t; u < tn * TW; u += LT_THREADS) {
-            const int e = u / tn, a = u - e * tn;
-            s_tab[a * TW + e] = xyz[(size_t)e * n + base + a];
-        }
+        for (int e = 0; e < TW; ++e)
+            for (int a = t; a < tn; a += LT_THREADS) s_tab[a * TW + e] = xyz[(size_t)e * n + base + a];
         if (t < tn) {
             const int ia = base + t;
             t_q[t] = with_q ? q[ia] : 0.0;
@@ -769,23 +773,21 @@ __global__ void __launch_bounds__(LT_THREADS) k_sfac64_tab(int n, int natom_chun
             const double a0r = fma(wr, qa, -wi * km), a0i = fma(wi, qa, wr * km);
             const double a1r = wr * m3, a1i = wi * m3;
 #pragma unroll
-            for (int m = 0; m < NZB; ++m) {
-                if (m < nn) {
-                    const double fz = (double)(nz0 + m);
-                    const double vr = fma(-fz, a1i, a0r), vi = fma(fz, a1r, a0i);
-                    const double2 Z = row[ez + m];
-                    sre[m] = fma(vr, Z.x, fma(-vi, Z.y, sre[m]));
-                    sim[m] = fma(vr, Z.y, fma(vi, Z.x, sim[m]));
-                }
+            for (int m = 0; m < LQ; ++m) {
+                const double fz = (double)(nz0 + m);
+                const double vr = fma(-fz, a1i, a0r), vi = fma(fz, a1r, a0i);
+                const double2 Z = row[ez + (m < nn ? m : 0)];
+                sre[m] = fma(vr, Z.x, fma(-vi, Z.y, sre[m]));
+                sim[m] = fma(vr, Z.y, fma(vi, Z.x, sim[m]));
             }
         }
     }
-    if (t < ncol) {
+    if (valid) {
         const size_t plane = (size_t)nzmax * ncol;
 #pragma unroll
-        for (int m = 0; m < NZB; ++m)
-            if (m < nzmax) {
-                const size_t idx = (size_t)p * plane + (size_t)m * ncol + t;
+        for (int m = 0; m < LQ; ++m)
+            if (m < nn) {
+                const size_t idx = (size_t)p * plane + (size_t)(m0 + m) * ncol + cc;
                 part_re[idx] = sre[m];
                 part_im[idx] = sim[m];
             }
@@ -805,7 +807,8 @@ __global__ void k_sfac64_low_reduce(int P, int ncol, int nzmax, const int* __res
     const int cidx = valid ? t % ncol : 0, mz = valid ? t / ncol : 0;
     const size_t plane = (size_t)nzmax * ncol;
     double sr = 0.0, si = 0.0;
-    if (valid)
+    // slots past a column's length hold no partials
+    if (valid && mz < cols[4 * cidx + 3])
         for (int p = lane; p < P; p += 32) {
             sr += part_re[(size_t)p * plane + (size_t)mz * ncol + cidx];
             si += part_im[(size_t)p * plane + (size_t)mz * ncol + cidx];
@@ -905,87 +908,12 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield64_low(int n, const uint32
     }
 }
 
-// Pass 2 over the low set from the phase tables: thread = atom, blockIdx.y =
-// range of list columns, the range's A_k S staged in shared memory.  With
-// e_k = W Z[nz] (W = X[nx] Y[ny]) the column sums of k_kfield64_low are
-// R_j = Im(conj(W) U_j), Q_j = Re(conj(W) U_j) with U_j = sum_m m^j a_m conj(Z_m)
-// (m counted from the column's first nz): no transcendental per column.
-template <int GRAD>
-__global__ void __launch_bounds__(KF_THREADS) k_kfield64_tab(int n, const double2* __restrict__ xyz, int kxl, int kyl,
-                                                             int kzl, int TW, CellP c, const int* __restrict__ cols,
-                                                             int ncol, int nzmax, const double* __restrict__ aks,
-                                                             double* __restrict__ fpart) {
-    extern __shared__ double2 s_a[];   // [per][nzmax]
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int per = (ncol + gridDim.y - 1) / gridDim.y;
-    const int cbeg = blockIdx.y * per, cend = min(ncol, cbeg + per);
-    fpart += (size_t)blockIdx.y * 9 * n;
-    const double* aim_base = aks + (size_t)ncol * nzmax;
-    for (int u = threadIdx.x; u < (cend - cbeg) * nzmax; u += blockDim.x) {
-        const size_t r = (size_t)cbeg * nzmax + u;
-        s_a[u] = make_double2(aks[r], aim_base[r]);
-    }
-    __syncthreads();
-    const bool active = i < n;
-    const int ii = active ? i : 0;
-    const double2* row = xyz + ii;   // entry e of this atom at row[e * n]
-    const int XW = kxl + 1, YW = 2 * kyl + 1;
-    const double dk0 = 2.0 * PI * c.B[2], dk1 = 2.0 * PI * c.B[5], dk2 = 2.0 * PI * c.B[8];
-    double E0 = 0, E1 = 0, E2 = 0, G0 = 0, G1 = 0, G2 = 0, G3 = 0, G4 = 0, G5 = 0;
-    for (int cc = cbeg; cc < cend; ++cc) {
-        const int inx = cols[4 * cc], iny = cols[4 * cc + 1], inz0 = cols[4 * cc + 2], nzn = cols[4 * cc + 3];
-        const double2 X = row[(size_t)inx * n], Y = row[(size_t)(XW + iny + kyl) * n];
-        const double wr = fma(X.x, Y.x, -X.y * Y.y), wi = fma(X.x, Y.y, X.y * Y.x);
-        const double2* zr = row + (size_t)(XW + YW + inz0 + kzl) * n;
-        const double2* ar = s_a + (size_t)(cc - cbeg) * nzmax;
-        double u0r = 0, u0i = 0, u1r = 0, u1i = 0, u2r = 0, u2i = 0;
-        for (int m = 0; m < nzn; ++m) {
-            const double2 a = ar[m], z = zr[(size_t)m * n];
-            const double tr = fma(a.x, z.x, a.y * z.y), ti = fma(a.y, z.x, -a.x * z.y);   // a conj(z)
-            const double fm = (double)m;
-            u0r += tr; u0i += ti;
-            u1r = fma(fm, tr, u1r); u1i = fma(fm, ti, u1i);
-            if (GRAD) { u2r = fma(fm * fm, tr, u2r); u2i = fma(fm * fm, ti, u2i); }
-        }
-        const double R0 = fma(wr, u0i, -wi * u0r), R1 = fma(wr, u1i, -wi * u1r);
-        const double kb0 = 2.0 * PI * (inx * c.B[0] + iny * c.B[1] + inz0 * c.B[2]);
-        const double kb1 = 2.0 * PI * (inx * c.B[3] + iny * c.B[4] + inz0 * c.B[5]);
-        const double kb2 = 2.0 * PI * (inx * c.B[6] + iny * c.B[7] + inz0 * c.B[8]);
-        E0 -= fma(kb0, R0, dk0 * R1);
-        E1 -= fma(kb1, R0, dk1 * R1);
-        E2 -= fma(kb2, R0, dk2 * R1);
-        if (GRAD) {
-            const double Q0 = fma(wr, u0r, wi * u0i), Q1 = fma(wr, u1r, wi * u1i), Q2 = fma(wr, u2r, wi * u2i);
-            G0 += kb0 * kb0 * Q0 + 2.0 * kb0 * dk0 * Q1 + dk0 * dk0 * Q2;
-            G1 += kb1 * kb1 * Q0 + 2.0 * kb1 * dk1 * Q1 + dk1 * dk1 * Q2;
-            G2 += kb2 * kb2 * Q0 + 2.0 * kb2 * dk2 * Q1 + dk2 * dk2 * Q2;
-            G3 += kb0 * kb1 * Q0 + (kb0 * dk1 + dk0 * kb1) * Q1 + dk0 * dk1 * Q2;
-            G4 += kb0 * kb2 * Q0 + (kb0 * dk2 + dk0 * kb2) * Q1 + dk0 * dk2 * Q2;
-            G5 += kb1 * kb2 * Q0 + (kb1 * dk2 + dk1 * kb2) * Q1 + dk1 * dk2 * Q2;
-        }
-    }
-    if (active) {
-        fpart[i] = E0; fpart[n + i] = E1; fpart[2 * n + i] = E2;
-        if (GRAD) {
-            fpart[3 * n + i] = G0; fpart[4 * n + i] = G1; fpart[5 * n + i] = G2;
-            fpart[6 * n + i] = G3; fpart[7 * n + i] = G4; fpart[8 * n + i] = G5;
-        }
-    }
-}
-
-// The low set's field pass: the table form when the tables exist.
+// The low set's field pass (per atom, the phase rotated along each column in
+// registers: measured faster than reading per-atom phase tables, which makes
+// this pass bound by table traffic).
 void launch_kfield_low(cudaStream_t st, int n, const uint32_t* fixed, CellP c, LowK& lk, bool grad) {
     const dim3 g((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT);
-    if (lk.xyz) {
-        const int per = (lk.ncol + LK_SPLIT - 1) / LK_SPLIT;
-        const size_t sm = sizeof(double2) * (size_t)per * lk.nzmax;
-        if (grad)
-            k_kfield64_tab<1><<<g, KF_THREADS, sm, st>>>(n, lk.xyz, lk.kxl, lk.kyl, lk.kzl, lk.TW, c, lk.col, lk.ncol,
-                                                         lk.nzmax, lk.aks, lk.fpart);
-        else
-            k_kfield64_tab<0><<<g, KF_THREADS, sm, st>>>(n, lk.xyz, lk.kxl, lk.kyl, lk.kzl, lk.TW, c, lk.col, lk.ncol,
-                                                         lk.nzmax, lk.aks, lk.fpart);
-    } else if (grad) {
+    if (grad) {
         k_kfield64_low<1><<<g, KF_THREADS, 0, st>>>(n, fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
     } else {
         k_kfield64_low<0><<<g, KF_THREADS, 0, st>>>(n, fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
@@ -1264,14 +1192,10 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             // from the per-atom phase tables (built with the position update)
             const size_t lplane = (size_t)lk.P2 * lk.nzmax * lk.ncol;
             const size_t sm = sizeof(double2) * LT_TILE * lk.TW;
-#define SF64T(NZ) k_sfac64_tab<NZ><<<lk.P2, LT_THREADS, sm, st>>>(n, lk.natom_chunk2, lk.xyz, lk.kxl, lk.kyl, lk.kzl, \
-                                                          lk.TW, q, mu, c, lk.col, lk.ncol, lk.nzmax, fl.with_q, \
-                                                          fl.with_mu, lk.part, lk.part + lplane)
-            if (lk.nzb == 8) SF64T(8);
-            else if (lk.nzb == 16) SF64T(16);
-            else if (lk.nzb == 24) SF64T(24);
-            else SF64T(32);
-#undef SF64T
+            const dim3 gt((lk.nitems + LT_THREADS - 1) / LT_THREADS, lk.P2);
+            k_sfac64_tab<<<gt, LT_THREADS, sm, st>>>(n, lk.natom_chunk2, lk.xyz, lk.kxl, lk.kyl, lk.kzl, lk.TW, q, mu, c,
+                                                     lk.col, lk.ncol, lk.nzmax, lk.items, lk.nitems, fl.with_q,
+                                                     fl.with_mu, lk.part, lk.part + lplane);
             k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P2, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane,
                                                     lk.Ak, lk.kcoe, c, lk.aks, fl.energy, part.buf);
         } else {

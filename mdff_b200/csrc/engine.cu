@@ -3087,9 +3087,6 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
             LowK& lk = ctx->rs.low;
             lk.ncol = (int)cl.size();
             lk.nzmax = nzmax;
-            // longest columns first: the structure-factor threads of a warp
-            // then run nz loops of about the same length
-            std::stable_sort(cl.begin(), cl.end(), [](const Col& a, const Col& b) { return a.nn > b.nn; });
             if (lk.ncol > 0) {
                 cols.resize(4 * (size_t)lk.ncol);
                 akl.assign((size_t)lk.ncol * nzmax, 0.0);
@@ -3113,39 +3110,13 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 P = std::min(P, std::max(1, n / 32));
                 lk.natom_chunk = (n + P - 1) / P;
                 lk.P = (n + lk.natom_chunk - 1) / lk.natom_chunk;
-                // the table form of the structure factor: per-atom X, Y, Z
-                // phase tables, one thread per column, about four blocks per SM
-                for (const Col& C_ : cl) {
-                    lk.kxl = std::max(lk.kxl, C_.nx);
-                    lk.kyl = std::max(lk.kyl, std::abs(C_.ny));
-                    lk.kzl = std::max(lk.kzl, std::max(std::abs(C_.lo - kg.kmax[2]), std::abs(C_.lo + C_.nn - 1 - kg.kmax[2])));
-                }
-                lk.TW = (lk.kxl + 1) + (2 * lk.kyl + 1) + (2 * lk.kzl + 1);
-                const bool tab_form = sizeof(double2) * LT_TILE * lk.TW <= 48 * 1024;
-                lk.xyz = nullptr;
-                lk.items = nullptr;
-                lk.nitems = 0;
-                if (tab_form) {
-                    std::vector<int> it;
-                    for (int q = 0; q < lk.ncol; ++q)
-                        for (int m = 0; m < cl[q].nn; m += LQ) { it.push_back(q); it.push_back(m); }
-                    lk.nitems = (int)(it.size() / 2);
-                    const int xb = (lk.nitems + LT_THREADS - 1) / LT_THREADS;
-                    int P2 = std::max(1, std::min((4 * 148 + xb - 1) / xb, n / 16));
-                    lk.natom_chunk2 = (n + P2 - 1) / P2;
-                    lk.P2 = (n + lk.natom_chunk2 - 1) / lk.natom_chunk2;
-                    TRY(dalloc(ctx, &lk.xyz, (size_t)n * lk.TW));
-                    TRY(dalloc(ctx, &lk.items, it.size()));
-                    CK(cudaMemcpyAsync(lk.items, it.data(), sizeof(int) * it.size(), cudaMemcpyHostToDevice, ctx->st));
-                    CK(cudaStreamSynchronize(ctx->st));
-                }
                 TRY(dalloc(ctx, &lk.col, cols.size()));
                 CK(cudaMemcpyAsync(lk.col, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice, ctx->st));
                 TRY(dalloc(ctx, &lk.Ak, akl.size()));
                 TRY(dalloc(ctx, &lk.kcoe, kcl.size()));
                 TRY(upload(ctx, lk.Ak, akl.data(), (int)akl.size()));
                 TRY(upload(ctx, lk.kcoe, kcl.data(), (int)kcl.size()));
-                TRY(dalloc(ctx, &lk.part, 2 * (size_t)std::max(lk.P, lk.xyz ? lk.P2 : 1) * nzmax * lk.ncol));
+                TRY(dalloc(ctx, &lk.part, 2 * (size_t)lk.P * nzmax * lk.ncol));
                 TRY(dalloc(ctx, &lk.aks, 2 * (size_t)lk.ncol * nzmax));
                 TRY(dalloc(ctx, &lk.aks_acc, 2 * (size_t)lk.ncol * nzmax));
                 TRY(dalloc(ctx, &lk.fpart, 4 * 9 * (size_t)n));

@@ -249,13 +249,6 @@ struct LowK {
     double* aks_acc = nullptr;   // solver accumulator of aks (reuse of structure factors)
     double2* tab = nullptr;   // [n][16] e^{2 pi i m s_z} in FP64
     int P = 1, natom_chunk = 0;
-    // per-atom FP64 phase tables of the structure factor: X[nx] (0..kxl),
-    // Y[ny] (-kyl..kyl), Z[nz] (-kzl..kzl), TW entries per atom
-    int kxl = 0, kyl = 0, kzl = 0, TW = 0;
-    double2* xyz = nullptr;   // [n][TW]
-    int P2 = 1, natom_chunk2 = 0;        // atom splits of k_sfac64_tab
-    int* items = nullptr;                // [nitems][2]: (list column, first m) of its work items
-    int nitems = 0;
 };
 
 // Tensor-core structure factor of the mixed path (ewald_tc.cuh).

@@ -695,105 +695,6 @@ __global__ void __launch_bounds__(SF_THREADS) k_sfac64_low(int n, int natom_chun
     }
 }
 
-// Per position update: the FP64 phase tables of the low set, per atom
-// X[nx] = e^{2 pi i nx s1} (nx = 0..kxl), Y[ny] (ny = -kyl..kyl), Z[nz]
-// (nz = -kzl..kzl), from the direct coordinates; entry-major, [TW][n], so
-// that a warp's atoms read one entry in one coalesced access.
-__global__ void k_lowk_tables(int n, const double* __restrict__ sx, const double* __restrict__ sy,
-                              const double* __restrict__ sz, int kxl, int kyl, int kzl, int TW,
-                              double2* __restrict__ xyz) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)n * TW) return;
-    const int e = (int)(t / n), a = (int)(t % n);
-    const int XW = kxl + 1, YW = 2 * kyl + 1;
-    double s, m;
-    if (e < XW) { s = sx[a]; m = e; }
-    else if (e < XW + YW) { s = sy[a]; m = e - XW - kyl; }
-    else { s = sz[a]; m = e - XW - YW - kzl; }
-    double w = m * (s - rint(s));
-    w -= rint(w);
-    double sn, cs;
-    sincospi(2.0 * w, &sn, &cs);
-    xyz[t] = make_double2(cs, sn);
-}
-
-// Pass 1 over the low set from the phase tables: one thread per work item =
-// (list column, chunk of up to LQ consecutive nz), one block row per range of
-// atoms.  For column (nx, ny) and atom a: W = X[nx] Y[ny],
-// A0 = W (q + i (nx m1 + ny m2)), A1 = W m3, and S[nz] += (A0 + i nz A1) Z[nz]
-// over the chunk -- six FMAs per (atom, k), no transcendental, and chunks
-// short enough that columns of any length waste few slots.
-constexpr int LT_TILE = 32;     // atoms staged per round
-constexpr int LT_THREADS = 128;
-constexpr int LQ = 4;           // nz per work item
-__global__ void __launch_bounds__(LT_THREADS) k_sfac64_tab(int n, int natom_chunk, const double2* __restrict__ xyz,
-                                                           int kxl, int kyl, int kzl, int TW,
-                                                           const double* __restrict__ q, const double* __restrict__ mu,
-                                                           CellP c, const int* __restrict__ cols, int ncol, int nzmax,
-                                                           const int* __restrict__ items, int nitems, int with_q,
-                                                           int with_mu, double* __restrict__ part_re,
-                                                           double* __restrict__ part_im) {
-    extern __shared__ double2 s_tab[];   // [LT_TILE][TW]
-    __shared__ double t_q[LT_TILE], t_m1[LT_TILE], t_m2[LT_TILE], t_m3[LT_TILE];
-    const int t = threadIdx.x;
-    const int it = blockIdx.x * LT_THREADS + t;
-    const bool valid = it < nitems;
-    const int item = items[2 * (valid ? it : nitems - 1)], m0 = items[2 * (valid ? it : nitems - 1) + 1];
-    const int cc = item;
-    const int nx = cols[4 * cc], ny = cols[4 * cc + 1], nz0 = cols[4 * cc + 2] + m0;
-    const int nn = min(LQ, cols[4 * cc + 3] - m0);
-    const int XW = kxl + 1, YW = 2 * kyl + 1;
-    const int ex = nx, ey = XW + ny + kyl, ez = XW + YW + nz0 + kzl;
-    const double fnx = nx, fny = ny;
-    double sre[LQ], sim[LQ];
-#pragma unroll
-    for (int m = 0; m < LQ; ++m) { sre[m] = 0.0; sim[m] = 0.0; }
-    const int p = blockIdx.y;
-    const int a0 = p * natom_chunk, a1 = min(n, a0 + natom_chunk);
-    for (int base = a0; base < a1; base += LT_TILE) {
-        const int tn = min(LT_TILE, a1 - base);
-        __syncthreads();
-        for (int e = 0; e < TW; ++e)
-            for (int a = t; a < tn; a += LT_THREADS) s_tab[a * TW + e] = xyz[(size_t)e * n + base + a];
-        if (t < tn) {
-            const int ia = base + t;
-            t_q[t] = with_q ? q[ia] : 0.0;
-            double u0 = 0, u1 = 0, u2 = 0;
-            if (with_mu) { u0 = mu[ia]; u1 = mu[n + ia]; u2 = mu[2 * n + ia]; }
-            t_m1[t] = 2.0 * PI * (c.B[0] * u0 + c.B[3] * u1 + c.B[6] * u2);
-            t_m2[t] = 2.0 * PI * (c.B[1] * u0 + c.B[4] * u1 + c.B[7] * u2);
-            t_m3[t] = 2.0 * PI * (c.B[2] * u0 + c.B[5] * u1 + c.B[8] * u2);
-        }
-        __syncthreads();
-        for (int a = 0; a < tn; ++a) {
-            const double2* row = s_tab + a * TW;
-            const double2 X = row[ex], Y = row[ey];
-            const double wr = fma(X.x, Y.x, -X.y * Y.y), wi = fma(X.x, Y.y, X.y * Y.x);
-            const double qa = t_q[a], km = fma(fnx, t_m1[a], fny * t_m2[a]), m3 = t_m3[a];
-            const double a0r = fma(wr, qa, -wi * km), a0i = fma(wi, qa, wr * km);
-            const double a1r = wr * m3, a1i = wi * m3;
-#pragma unroll
-            for (int m = 0; m < LQ; ++m) {
-                const double fz = (double)(nz0 + m);
-                const double vr = fma(-fz, a1i, a0r), vi = fma(fz, a1r, a0i);
-                const double2 Z = row[ez + (m < nn ? m : 0)];
-                sre[m] = fma(vr, Z.x, fma(-vi, Z.y, sre[m]));
-                sim[m] = fma(vr, Z.y, fma(vi, Z.x, sim[m]));
-            }
-        }
-    }
-    if (valid) {
-        const size_t plane = (size_t)nzmax * ncol;
-#pragma unroll
-        for (int m = 0; m < LQ; ++m)
-            if (m < nn) {
-                const size_t idx = (size_t)p * plane + (size_t)(m0 + m) * ncol + cc;
-                part_re[idx] = sre[m];
-                part_im[idx] = sim[m];
-            }
-    }
-}
-
 // One warp per low-set k-vector: sum of the atom-chunk partials, A_k S(k),
 // energy and stress terms.
 __global__ void k_sfac64_low_reduce(int P, int ncol, int nzmax, const int* __restrict__ cols,
@@ -807,8 +708,7 @@ __global__ void k_sfac64_low_reduce(int P, int ncol, int nzmax, const int* __res
     const int cidx = valid ? t % ncol : 0, mz = valid ? t / ncol : 0;
     const size_t plane = (size_t)nzmax * ncol;
     double sr = 0.0, si = 0.0;
-    // slots past a column's length hold no partials
-    if (valid && mz < cols[4 * cidx + 3])
+    if (valid)
         for (int p = lane; p < P; p += 32) {
             sr += part_re[(size_t)p * plane + (size_t)mz * ncol + cidx];
             si += part_im[(size_t)p * plane + (size_t)mz * ncol + cidx];
@@ -905,18 +805,6 @@ __global__ void __launch_bounds__(KF_THREADS) k_kfield64_low(int n, const uint32
             fpart[3 * n + i] = G0; fpart[4 * n + i] = G1; fpart[5 * n + i] = G2;
             fpart[6 * n + i] = G3; fpart[7 * n + i] = G4; fpart[8 * n + i] = G5;
         }
-    }
-}
-
-// The low set's field pass (per atom, the phase rotated along each column in
-// registers: measured faster than reading per-atom phase tables, which makes
-// this pass bound by table traffic).
-void launch_kfield_low(cudaStream_t st, int n, const uint32_t* fixed, CellP c, LowK& lk, bool grad) {
-    const dim3 g((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT);
-    if (grad) {
-        k_kfield64_low<1><<<g, KF_THREADS, 0, st>>>(n, fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
-    } else {
-        k_kfield64_low<0><<<g, KF_THREADS, 0, st>>>(n, fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
     }
 }
 
@@ -1081,15 +969,7 @@ int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* 
     if (rs.tab_epoch == rs.want_epoch) return 0;
     k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab, rs.low.ncol > 0 ? rs.low.tab : nullptr);
     rs.tab_epoch = rs.want_epoch;
-    int nk = 1;
-    if (rs.low.xyz) {
-        const LowK& lk = rs.low;
-        const long nt = (long)n * lk.TW;
-        k_lowk_tables<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(n, sx, sy, sz, lk.kxl, lk.kyl, lk.kzl, lk.TW,
-                                                                    lk.xyz);
-        nk++;
-    }
-    if (!rs.tc.on) return nk;
+    if (!rs.tc.on) return 1;
     const TcK& t = rs.tc;
     const long nxy = (long)t.npad * t.XYW, nb = (long)t.npad * (t.N / 2);
     tcs::k_tc_xy<<<(unsigned)((nxy + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kx, t.ky, t.XYW, t.xy);
@@ -1097,7 +977,7 @@ int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* 
     const long na = (long)t.ntile_f * 128 * (t.KZ / 16), nt = (long)t.ntile_f * 128 * t.XYW;
     tcf::k_tcf_aimage<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(n, t.ntile_f, rs.fixed, t.kz, t.nzl, t.KZ, t.aimg);
     tcf::k_tcf_xyt<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(t.npad, t.ntile_f, t.xy, t.XYW, t.xyt);
-    return nk + 4;
+    return 5;
 }
 
 #define CUDA_COPY_ACC(st, dst, src, bytes) cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (st))
@@ -1187,27 +1067,15 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     if (fl.energy && !fl.reuse) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
     if (low && !fl.reuse) {
         LowK& lk = rs.low;
+        const int nch = (lk.nzmax + TM - 1) / TM;
+        const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;
+        dim3 gl(nch * cb, lk.P);
+        const size_t lplane = (size_t)lk.P * lk.nzmax * lk.ncol;
+        k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, rs.fixed, lk.tab, q, mu, c, lk.col, lk.ncol, lk.nzmax,
+                                                nch, fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
         const int lb = (lk.ncol * lk.nzmax * 32 + 255) / 256;
-        if (lk.xyz) {
-            // from the per-atom phase tables (built with the position update)
-            const size_t lplane = (size_t)lk.P2 * lk.nzmax * lk.ncol;
-            const size_t sm = sizeof(double2) * LT_TILE * lk.TW;
-            const dim3 gt((lk.nitems + LT_THREADS - 1) / LT_THREADS, lk.P2);
-            k_sfac64_tab<<<gt, LT_THREADS, sm, st>>>(n, lk.natom_chunk2, lk.xyz, lk.kxl, lk.kyl, lk.kzl, lk.TW, q, mu, c,
-                                                     lk.col, lk.ncol, lk.nzmax, lk.items, lk.nitems, fl.with_q,
-                                                     fl.with_mu, lk.part, lk.part + lplane);
-            k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P2, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane,
-                                                    lk.Ak, lk.kcoe, c, lk.aks, fl.energy, part.buf);
-        } else {
-            const int nch = (lk.nzmax + TM - 1) / TM;
-            const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;
-            dim3 gl(nch * cb, lk.P);
-            const size_t lplane = (size_t)lk.P * lk.nzmax * lk.ncol;
-            k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, rs.fixed, lk.tab, q, mu, c, lk.col, lk.ncol,
-                                                    lk.nzmax, nch, fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
-            k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane, lk.Ak,
-                                                    lk.kcoe, c, lk.aks, fl.energy, part.buf);
-        }
+        k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane, lk.Ak,
+                                                lk.kcoe, c, lk.aks, fl.energy, part.buf);
         if (fl.energy) launch_reduce_partials(st, part.buf, lb, 7, d->rec, 1);
         nk += 2 + (fl.energy ? 1 : 0);
     }
@@ -1244,7 +1112,13 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         nsplit_f = tcf::NQ;
         nk += 1;
         if (low) {
-            launch_kfield_low(st, n, rs.fixed, c, rs.low, grad);
+            LowK& lk = rs.low;
+            if (grad)
+                k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+            else
+                k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
             nk++;
         }
     } else if (mixed) {
@@ -1259,7 +1133,13 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
                                                          L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
         nk += 2;
         if (low) {
-            launch_kfield_low(st, n, rs.fixed, c, rs.low, grad);
+            LowK& lk = rs.low;
+            if (grad)
+                k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+            else
+                k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
             nk++;
         }
     } else {

@@ -252,13 +252,19 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ---- MMA issue: per stage 2 K-steps of 32 x 6 digit products
         const uint32_t idesc = umma::idesc_s8(128, N);
         const uint32_t lboA = 16 * 128, lboB = (uint32_t)(N / 8) * 128;
+        // a shared-memory descriptor is linear in its address field (address
+        // >> 4 in the low 14 bits; every address here is below 256 KB), so
+        // each operand's descriptor is one base plus a constant offset
+        const uint64_t adesc0 = umma::desc_kmajor(sbase + L.a_off, lboA, 128);
+        const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.b_off, lboB, 128);
+        const uint32_t bstep = L.buf_bytes >> 4, bslice = ((uint32_t)N * KB) >> 4;
         uint32_t started = 0;
         for (int s = 0; s < nst; ++s) {
             const int b = s % NBUF;
             if (!tc_wait(&full[b], (s / NBUF) & 1, err, 4, &stop)) break;
             if (!tc_wait(&aready[b], (s / NBUF) & 1, err, 8, &stop)) break;
             umma::fence_after_sync();
-            const uint32_t a0 = sbase + b * L.buf_bytes + L.a_off, b0 = sbase + b * L.buf_bytes + L.b_off;
+            const uint64_t ab = adesc0 + (uint64_t)(b * bstep), bb = bdesc0 + (uint64_t)(b * bstep);
 #pragma unroll
             for (int ks = 0; ks < KB / 32; ++ks) {
 #pragma unroll
@@ -266,8 +272,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                     for (int j = 0; j < 3 - i; ++j) {
                         const int lvl = i + j;
-                        const uint64_t ad = umma::desc_kmajor(a0 + i * A_SLICE + 2 * ks * lboA, lboA, 128);
-                        const uint64_t bd = umma::desc_kmajor(b0 + j * (uint32_t)N * KB + 2 * ks * lboB, lboB, 128);
+                        const uint64_t ad = ab + (uint64_t)((i * A_SLICE + 2 * ks * lboA) >> 4);
+                        const uint64_t bd = bb + (uint64_t)(j * bslice + ((2 * ks * lboB) >> 4));
                         umma::mma_s8(tmem + lvl * LSTRIDE, ad, bd, idesc, (started >> lvl) & 1u);
                         started |= 1u << lvl;
                     }
@@ -577,22 +583,27 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (lane == 0) {
             const uint32_t idesc = umma::idesc_s8(128, C::NB);
             const uint32_t lboA = 16 * 128, lboB = (uint32_t)(C::NB / 8) * 128;
+            // descriptors as one base per operand plus constant offsets (the
+            // address field is linear; every address here is below 256 KB)
+            const uint64_t adesc0 = umma::desc_kmajor(sbase + L.a_off, lboA, 128);
+            const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.b_off, lboB, 128);
+            const uint32_t aslice = (128u * KZ) >> 4, bslice = ((uint32_t)C::NB * KZ) >> 4;
+            const uint32_t astep = (2 * lboA) >> 4, bkstep = (2 * lboB) >> 4, bstage = L.stage_bytes >> 4;
             if (f_wait(&ares, 0, err, 2, &abort_)) {
                 for (int q = 0; q < ncb; ++q) {
                     const int bs = q % NBS, tb = q & 1;
                     if (!f_wait(&bfull[bs], (q / NBS) & 1, err, 4, &abort_)) break;
                     if (q >= 2 && !f_wait(&accfree[tb], ((q >> 1) - 1) & 1, err, 8, &abort_)) break;
                     umma::fence_after_sync();
-                    const uint32_t a0 = sbase + L.a_off, b0 = sbase + L.b_off + bs * L.stage_bytes;
+                    const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
                     for (int ks = 0; ks < KZ / 32; ++ks) {
 #pragma unroll
                         for (int i = 0; i < 3; ++i)
 #pragma unroll
                             for (int j = 0; j < 3 - i; ++j) {
                                 const int lvl = i + j;
-                                const uint64_t ad = umma::desc_kmajor(a0 + i * 128 * KZ + 2 * ks * lboA, lboA, 128);
-                                const uint64_t bd =
-                                    umma::desc_kmajor(b0 + j * C::NB * KZ + 2 * ks * lboB, lboB, 128);
+                                const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
+                                const uint64_t bd = bq + (uint64_t)(j * bslice + ks * bkstep);
                                 const uint32_t acc = (ks > 0 || (lvl == 1 && i == 1) || (lvl == 2 && i > 0)) ? 1u : 0u;
                                 umma::mma_s8(tmem + tb * BUFC + lvl * LVL, ad, bd, idesc, acc);
                             }

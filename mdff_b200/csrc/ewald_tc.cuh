@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 namespace mdff {
 namespace tcf {
 
-constexpr int EPW = 16;                  // epilogue warps: 4 per tensor-memory lane quarter
+constexpr int EPW = 8;                   // epilogue warps: 2 per tensor-memory lane quarter
 constexpr int NQ = EPW / 4;              // column parts per block (one per epilogue warp of a quarter)
 constexpr int THREADS = 32 * (EPW + 2);  // + MMA warp + copy warp
 constexpr int NBS = 6;                   // B stages (the epilogue holds a stage until it has read its constants)

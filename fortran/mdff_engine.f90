@@ -145,6 +145,7 @@ module mdff_engine
   type, bind(C) :: mdff_rmc_efg_params_t
     integer(c_int) :: lrmc_u, lrmc_vzz, lrmc_eta, efg_start
     real(c_double) :: resolution_u_efg, u_efg_min, resolution_vzz_efg, vzz_efg_min, resolution_eta_efg
+    integer(c_int) :: lrmc_var, pad_
   end type mdff_rmc_efg_params_t
 
   integer(c_int), parameter :: MDFF_FILE_TRAJFF = 0, MDFF_FILE_CONTFF = 1, MDFF_FILE_EFGALL = 2, &

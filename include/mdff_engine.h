@@ -652,9 +652,11 @@ typedef struct mdff_rmc_efg_params {
     double resolution_u_efg, u_efg_min;
     double resolution_vzz_efg, vzz_efg_min;
     double resolution_eta_efg;
+    int lrmc_var;                  /* the distance-variance term (eval_chisq_var_distance, src/rmc.f90:778-1063) */
+    int pad_;
 } mdff_rmc_efg_params;
 
-/* rmc_main with its EFG chi^2 terms (src/rmc.f90:420-640): per trial move
+/* rmc_main with its optional chi^2 terms (src/rmc.f90:420-640): per trial move
  * the g(r) term as mdff_rmc (incremental counts), and while kacc >=
  * efg_start the EFG of the whole trial configuration (rmc_efg: the engine's
  * Ewald EFG of the point charges, multipole_efg_ES with mu = 0), its NMR
@@ -665,9 +667,16 @@ typedef struct mdff_rmc_efg_params {
  * bin = 0..PANU) with ui fastest, dibvzz and dibeta (mp, bin) with mp
  * fastest; the *_out arrays receive those of the last accepted
  * configuration (rows the reference never fills -- U's row 6, eta's last
- * bin -- are 0).  Uniforms, temperatures, stopping and the result as
- * mdff_rmc.  The system must be point charges: no static or induced
- * dipoles (MDFF_E_UNSUPPORTED otherwise). */
+ * bin -- are 0).  With lrmc_var, chi^2 component 2 is the distance-variance
+ * term of every trial configuration: per atom and type the sorted distances
+ * to all other atoms of that type (minimum image, no cutoff), and
+ * sum (d_n - <d_n>)^2 / <d_n>^2 over atoms, types and ranks, the mean taken
+ * over the atoms of each type.  Its sorted lists stay in device memory
+ * (natm^2 doubles): a cell whose lists do not fit in free device memory, or
+ * with more than 16385 atoms of one type, returns MDFF_E_UNSUPPORTED.
+ * Uniforms, temperatures, stopping and the result as mdff_rmc.  With an EFG
+ * term the system must be point charges: no static or induced dipoles
+ * (MDFF_E_UNSUPPORTED otherwise). */
 int  mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_params* ep,
                   const double* grr_exp, const double* dibU_exp, const double* dibvzz_exp,
                   const double* dibeta_exp, const double* uniforms, long long nuni,

@@ -131,11 +131,12 @@ class RmcParams(C.Structure):
 
 class RmcEfgParams(C.Structure):
     """mdff_rmc_efg_params: rmctag's EFG terms (lrmc_u, lrmc_vzz, lrmc_eta),
-    efg_start and the bins of rmc_efg."""
+    efg_start and the bins of rmc_efg, and the distance-variance term
+    (lrmc_var)."""
     _fields_ = [("lrmc_u", C.c_int), ("lrmc_vzz", C.c_int), ("lrmc_eta", C.c_int), ("efg_start", C.c_int),
                 ("resolution_u_efg", C.c_double), ("u_efg_min", C.c_double),
                 ("resolution_vzz_efg", C.c_double), ("vzz_efg_min", C.c_double),
-                ("resolution_eta_efg", C.c_double)]
+                ("resolution_eta_efg", C.c_double), ("lrmc_var", C.c_int), ("pad_", C.c_int)]
 
     def shapes(self, ntype):
         """Array shapes of the U, Vzz and eta distributions: the reference's

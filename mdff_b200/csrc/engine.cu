@@ -27,6 +27,7 @@
 #include "rmc.cuh"
 #include "efg_post.cuh"
 #include "rmc_efg.cuh"
+#include "rmc_var.cuh"
 #include "io.cuh"
 #include <condition_variable>
 #include <deque>
@@ -4290,7 +4291,8 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
         return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: EFG resolutions must be positive");
     if ((ep->lrmc_u && !dibU_exp) || (ep->lrmc_vzz && !dibvzz_exp) || (ep->lrmc_eta && !dibeta_exp))
         return fail(ctx, MDFF_E_ARG, "mdff_rmc_efg: an experimental distribution of an active term is missing");
-    if (!ctx->p.lcoulomb || ctx->npol > 0 || ctx->any_dip0)
+    const bool any_efg_req = ep->lrmc_u || ep->lrmc_vzz || ep->lrmc_eta;
+    if (any_efg_req && (!ctx->p.lcoulomb || ctx->npol > 0 || ctx->any_dip0))
         return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_rmc_efg: the EFG terms take point charges (no dipoles), as "
                                              "rmc_efg's multipole_efg_ES is called with mu = 0");
     const double pu = 2.0 * std::fabs(ep->u_efg_min) / ep->resolution_u_efg;
@@ -4331,7 +4333,38 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     const size_t nU = (size_t)(eh.PANU + 1) * nt1 * 6, nV = (size_t)(eh.PANvzz + 1) * nt1,
                  nE = (size_t)(eh.PANeta + 1) * nt1;
     const size_t ngr = (size_t)k->nrow * k->nbins, ncalc = (size_t)(k->npairs + 1) * k->nbins;
-    const bool any_efg = ep->lrmc_u || ep->lrmc_vzz || ep->lrmc_eta;
+    const bool any_efg = any_efg_req;
+    // the distance-variance term: sorted distance lists of every atom
+    const bool var = ep->lrmc_var != 0;
+    VarSpec vs;
+    std::memset(&vs, 0, sizeof vs);
+    int varP = 1;
+    if (var) {
+        vs.n = n;
+        vs.ntype = ctx->ntype;
+        for (int t = 0; t < ctx->ntype; ++t) {
+            vs.off[t] = vs.Ltot;
+            vs.natmi[t] = ctx->natmi[t];
+            vs.Ltot += ctx->natmi[t];
+            vs.nmax = std::max(vs.nmax, ctx->natmi[t]);
+        }
+        int maxlen = 0;
+        for (int t = 0; t < ctx->ntype; ++t)
+            for (int ti = 0; ti < ctx->ntype; ++ti)
+                if (ctx->natmi[ti] > 0) maxlen = std::max(maxlen, ctx->natmi[t] - (t == ti ? 1 : 0));
+        if (maxlen > VAR_MAXSEG)
+            return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_rmc_efg: the variance term sorts at most " +
+                                                     std::to_string(VAR_MAXSEG) + " distances per atom and type");
+        while (varP < maxlen) varP <<= 1;
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        const size_t need = sizeof(double) * ((size_t)n * vs.Ltot + (size_t)ctx->ntype * ctx->ntype * vs.nmax);
+        if (need + ((size_t)1 << 29) > fr)
+            return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_rmc_efg: the variance term's distance lists need " +
+                                                     std::to_string(need >> 20) + " MiB of device memory, " +
+                                                     std::to_string(fr >> 20) + " MiB are free");
+        CK(cudaFuncSetAttribute(k_var_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(varP * sizeof(double))));
+    }
     // uniforms: the caller's, or the counter-based stream of mdff_rmc
     std::vector<double> uni;
     const long long nu = uniforms ? nuni : 10 * rp->max_trials;
@@ -4358,6 +4391,40 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     TRY(rmc_frac(ctx, s));
     k_rmc_dirkar<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->cell, ctx->x, ctx->y, ctx->z);
     k_gr_full<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k->bin, hd);
+    double *vl = nullptr, *vmean = nullptr, *vpart = nullptr;
+    int *vrank = nullptr, *verr = nullptr;
+    const int vwb = (n * 32 + 255) / 256;   // blocks of the per-atom chi kernel (a warp per atom)
+    if (var) {
+        CK(cudaMallocAsync((void**)&vl, sizeof(double) * (size_t)n * vs.Ltot, ctx->st));
+        CK(cudaMallocAsync((void**)&vmean, sizeof(double) * (size_t)vs.ntype * vs.ntype * vs.nmax, ctx->st));
+        CK(cudaMallocAsync((void**)&vpart, sizeof(double) * (size_t)(vwb + 1), ctx->st));
+        CK(cudaMallocAsync((void**)&vrank, sizeof(int) * (size_t)n, ctx->st));
+        CK(cudaMallocAsync((void**)&verr, sizeof(int), ctx->st));
+        std::vector<int> ht(n), rank(n), cntt(NT, 0);
+        CK(cudaMemcpyAsync(ht.data(), ctx->type, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (int a = 0; a < n; ++a) rank[a] = cntt[ht[a]]++;
+        CK(cudaMemcpyAsync(vrank, rank.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemsetAsync(verr, 0, sizeof(int), ctx->st));
+        k_var_fill<<<dim3((n + 255) / 256, n), 256, 0, ctx->st>>>(vs, s, ctx->type, vrank, ctx->cell, vl);
+        k_var_sort<<<n * vs.ntype, 1024, varP * sizeof(double), ctx->st>>>(vs, ctx->type, 0, -1, varP, vl);
+        CK(cudaStreamSynchronize(ctx->st));   // rank goes out of scope
+        TRY(check_launch(ctx, "rmc variance lists"));
+    }
+    // chi^2 of the variance term from the lists (launches; *res written on the device)
+    auto var_launch = [&](double* dres) {
+        k_var_mean<<<nb(n), 256, 0, ctx->st>>>(vs, ctx->type, vl, vmean);
+        k_var_chi<<<vwb, 256, 0, ctx->st>>>(vs, ctx->type, vl, vmean, vpart);
+        launch_reduce_partials(ctx->st, vpart, vwb, 1, dres, 0);
+    };
+    // p moved from direct position f to t: p's own lists again, and the one
+    // changed value in every other atom's list
+    auto var_move = [&](int p, const double f[3], const double t[3]) {
+        k_var_row<<<nb(n), 256, 0, ctx->st>>>(vs, s, ctx->type, vrank, ctx->cell, p, vl);
+        k_var_sort<<<vs.ntype, 1024, varP * sizeof(double), ctx->st>>>(vs, ctx->type, 0, p, varP, vl);
+        k_var_shift<<<(n * 32 + 255) / 256, 256, 0, ctx->st>>>(vs, s, ctx->type, ctx->cell, p, f[0], f[1], f[2], t[0],
+                                                               t[1], t[2], vl, verr);
+    };
     std::vector<int> h(ngr), hdel(ngr), htr(ngr), cnt(ncnt);
     std::vector<double> sh(3 * (size_t)n);
     CK(cudaMemcpyAsync(h.data(), hd, sizeof(int) * ngr, cudaMemcpyDeviceToHost, ctx->st));
@@ -4428,9 +4495,16 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     long long kall = 1, kacc = 1, u = 0;
     int status = 0;
     double chi_old[6] = {0, 0, 0, 0, 0, 0}, chi[6];
+    double var_h = 0.0;
     [&]() {
         rmc_normalise(*k, h, calc.data());
         chi_old[0] = rmc_chisq_gr_tree(*k, calc.data(), grr_exp);
+        if (var) {
+            var_launch(vpart + vwb);
+            CK_R(cudaMemcpyAsync(&var_h, vpart + vwb, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+            CK_R(cudaStreamSynchronize(ctx->st));
+            chi_old[1] = var_h;
+        }
         if (any_efg && kacc >= ep->efg_start) {
             if ((rc = efg_terms(chi_old)) != MDFF_OK) return;
             aU = cU; aV = cV; aE = cE;
@@ -4469,6 +4543,11 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
             k_rmc_grdelta<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k->bin, p, sold[0], sold[1],
                                                        sold[2], dh);
             CK_R(cudaMemcpyAsync(hdel.data(), dh, sizeof(int) * ngr, cudaMemcpyDeviceToHost, ctx->st));
+            if (var) {
+                var_move(p, sold, snew);
+                var_launch(vpart + vwb);
+                CK_R(cudaMemcpyAsync(&var_h, vpart + vwb, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+            }
             for (int q = 0; q < 6; ++q) chi[q] = 0.0;
             const bool efg_now = any_efg && kacc >= ep->efg_start;
             if (efg_now) {
@@ -4479,6 +4558,7 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
             for (size_t q = 0; q < ngr; ++q) htr[q] = h[q] + hdel[q];
             rmc_normalise(*k, htr, calc.data());
             chi[0] = rmc_chisq_gr_tree(*k, calc.data(), grr_exp);
+            if (var) chi[1] = var_h;
             total(chi);
             bool acc6 = false, stop = false;
             for (int q = 0; q < 6; ++q) {   // src/rmc.f90:521-540
@@ -4501,6 +4581,7 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
                 }
                 k_rmc_place<<<1, 1, 0, ctx->st>>>(n, s, p, back[0], back[1], back[2], ctx->cell, ctx->x, ctx->y,
                                                   ctx->z);
+                if (var) var_move(p, snew, back);
                 if (stop) { status = 1; --kall; break; }
             } else {
                 ++kacc;
@@ -4516,8 +4597,15 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     ctx->p.lbmhft = saved_nonb[1];
     ctx->p.lbmhftd = saved_nonb[2];
     ctx->p.lmorse = saved_nonb[3];
+    int var_err = 0;
+    if (var) {
+        if (cudaMemcpyAsync(&var_err, verr, sizeof(int), cudaMemcpyDeviceToHost, ctx->st) != cudaSuccess) var_err = 2;
+        for (void* q : {(void*)vl, (void*)vmean, (void*)vpart, (void*)vrank, (void*)verr}) cudaFreeAsync(q, ctx->st);
+    }
     for (void* q : {(void*)s, (void*)hd, (void*)dh, (void*)ce}) cudaFreeAsync(q, ctx->st);
     cudaStreamSynchronize(ctx->st);
+    if (rc == MDFF_OK && var_err)
+        rc = fail(ctx, MDFF_E_STATE, "mdff_rmc_efg: the variance term's distance lists lost step with the positions");
     // lists rebuilt during the chain cover the Coulomb cut only: never leave
     // them in place, on the error path either (a failed rebuild here leaves
     // have_list false, so the next evaluation builds them)

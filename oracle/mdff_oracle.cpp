@@ -3384,6 +3384,54 @@ void rmc_efg_terms(orc_sys* s, RmcEfg& R, double chi[6]) {
 
 }  // namespace
 
+// eval_chisq_var_distance (src/rmc.f90:778-1063), the full recount of every
+// call: for each atom and type the distances to all other atoms of that type
+// (minimum image in direct coordinates, no cutoff, in the order of the
+// reference's loops), sorted; dab_aver(n, it, it2) summed over the atoms ia of
+// type it2 in atom order, zero distances left out; chi^2 summed over ia, it2
+// and n in the reference's loop order where the mean is nonzero.
+double chisq_var(const orc_sys* s, const std::vector<double>& sx, const std::vector<double>& sy,
+                 const std::vector<double>& sz) {
+    const int n = s->natm, nt = s->ntype;
+    int nmax = 0;
+    for (int t = 0; t < nt; ++t) nmax = std::max(nmax, s->natmi[t]);
+    std::vector<double> dab((size_t)n * nt * nmax, 0.0);   // dab_sorted_shifted (n, it, ia)
+    std::vector<double> aver((size_t)nmax * nt * nt, 0.0);  // dab_aver (n, it, it2) at [(it2 * nt + it) * nmax + n]
+    std::vector<double> row;
+    for (int ia = 0; ia < n; ++ia) {
+        for (int it = 0; it < nt; ++it) {
+            row.clear();
+            for (int ja = 0; ja < n; ++ja) {
+                if (ja == ia || s->itype[ja] != it) continue;
+                double rx, ry, rz;
+                const double rsq = pairvec(s->cell, sx[ia], sy[ia], sz[ia], sx[ja], sy[ja], sz[ja], rx, ry, rz);
+                row.push_back(std::sqrt(rsq));
+            }
+            std::sort(row.begin(), row.end());
+            double* d = &dab[((size_t)ia * nt + it) * nmax];
+            for (size_t m = 0; m < row.size(); ++m) d[m] = row[m];
+            const int it2 = s->itype[ia];
+            for (int m = 0; m < nmax; ++m)
+                if (d[m] != 0.0) aver[((size_t)it2 * nt + it) * nmax + m] += d[m];
+        }
+    }
+    double chi = 0.0;
+    for (int ia = 0; ia < n; ++ia) {
+        const int it1 = s->itype[ia];
+        const double ni = (double)s->natmi[it1];
+        for (int it2 = 0; it2 < nt; ++it2)
+            for (int m = 0; m < nmax; ++m) {
+                const double a = aver[((size_t)it1 * nt + it2) * nmax + m];
+                if (a != 0.0) {
+                    const double mean = a / ni;
+                    const double dd = dab[((size_t)ia * nt + it2) * nmax + m] - mean;
+                    chi = chi + dd * dd / (mean * mean);
+                }
+            }
+    }
+    return chi;
+}
+
 int orc_rmc_efg(orc_sys* s, const mdff_rmc_params* rp, const mdff_rmc_efg_params* ep, const double* gexp,
                 const double* Uexp, const double* Vexp, const double* Eexp, const double* uni, long long nuni,
                 double* grr_out, double* U_out, double* V_out, double* E_out, mdff_rmc_result* res) {
@@ -3415,6 +3463,8 @@ int orc_rmc_efg(orc_sys* s, const mdff_rmc_params* rp, const mdff_rmc_efg_params
     gr_normalise(s, g, h, calc.data());
     double chi_old[6] = {0, 0, 0, 0, 0, 0}, chi_new[6];
     chi_old[0] = chisq_gr(g, calc.data(), gexp);
+    const bool var = ep && ep->lrmc_var;
+    if (var) chi_old[1] = chisq_var(s, sx, sy, sz);
     long long kall = 1, kacc = 1, u = 0;
     if (any_efg && kacc >= ep->efg_start) {
         to_cart();
@@ -3446,6 +3496,7 @@ int orc_rmc_efg(orc_sys* s, const mdff_rmc_params* rp, const mdff_rmc_efg_params
         gr_normalise(s, g, h, calc.data());
         for (int q = 0; q < 6; ++q) chi_new[q] = 0.0;
         chi_new[0] = chisq_gr(g, calc.data(), gexp);
+        if (var) chi_new[1] = chisq_var(s, sx, sy, sz);
         const bool efg_now = any_efg && kacc >= ep->efg_start;
         if (efg_now) {
             to_cart();

@@ -140,3 +140,50 @@ def test_rmc_efg_rejects_polarisable_systems():
     su, sv, se = ep.shapes(s["params"].ntype)
     with pytest.raises(mdff_b200.EngineError):
         e.rmc_efg(rmc_params(10, 10, 6.0, 0.1), ep, np.zeros((4, 61)), np.zeros(su), np.zeros(sv), np.zeros(se))
+
+
+# ---- the distance-variance term: device lists against the oracle's full recount ----
+
+from test_oracle_rmc import chisq_var_numpy, var_params   # noqa: E402
+
+
+@pytest.mark.parametrize("with_efg", [False, True])
+def test_rmc_variance_chain_matches_oracle(with_efg):
+    # given the same uniforms the device chain (sorted lists kept on the device,
+    # one value moved per atom and trial) and the oracle's full recount every
+    # trial take the same decisions; the variance chi^2 agrees to 1e-11 (its
+    # final sum runs per atom and by a fixed tree, the reference's left to right)
+    ep = efg_params() if with_efg else var_params()
+    ep.lrmc_var = 1
+    t = rigid_mgo(seed=7, jitter=0.15)
+    g, U, V, E, _ = distributions(t, efg_params())
+    s = rigid_mgo()
+    u = np.random.default_rng(13).random(20000)
+    rp = rmc_par(60, 800)
+    e = mdff_b200.Engine(s["params"], s["itype"], s["pos"], s["cell"])
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    re, ge, Ue, Ve, Ee = e.rmc_efg(rp, ep, g, U, V, E, u)
+    ro, go, Uo, Vo, Eo = o.rmc_efg(rp, ep, g, U, V, E, u)
+    assert re["status"] == ro["status"] == 0
+    assert (re["kall"], re["kacc"], re["uniforms_used"]) == (ro["kall"], ro["kacc"], ro["uniforms_used"])
+    assert re["kacc"] > 5
+    assert ro["chisq"][1] > 0
+    assert abs(re["chisq"][1] - ro["chisq"][1]) <= 1e-11 * ro["chisq"][1]
+    assert np.array_equal(ge, go)
+    assert np.max(np.abs(e.positions() - o.positions())) < 1e-12
+    # rejected moves are undone, so the last accepted configuration is the
+    # final one: its chi^2 is the numpy recount of the final positions
+    fin = dict(s)
+    fin["pos"] = o.positions()
+    assert abs(re["chisq"][1] - chisq_var_numpy(fin)) < 1e-9 * ro["chisq"][1]
+
+
+def test_rmc_variance_rejects_oversized_types():
+    # more than 16384 atoms of one type: the device sort's limit
+    s = systems.lj_argon(ncell=17)
+    e = mdff_b200.Engine(s["params"], s["itype"], s["pos"], s["cell"])
+    ep = var_params()
+    su, sv, se = ep.shapes(s["params"].ntype)
+    with pytest.raises(mdff_b200.EngineError) as exc:
+        e.rmc_efg(rmc_params(10, 10, 2.0, 0.1), ep, np.zeros((2, 21)), np.zeros(su), np.zeros(sv), np.zeros(se))
+    assert exc.value.code == abi.E_UNSUPPORTED

@@ -192,3 +192,84 @@ def test_rmc_efg_start_delays_the_efg_terms():
     assert a[0]["chisq"][2:5] == [0.0, 0.0, 0.0]
     assert (a[0]["kall"], a[0]["kacc"], a[0]["uniforms_used"]) == (b[0]["kall"], b[0]["kacc"], b[0]["uniforms_used"])
     assert np.array_equal(a[1], b[1])
+
+
+# ---- the distance-variance term (eval_chisq_var_distance, src/rmc.f90:778-1063) ----
+
+def var_params():
+    ep = abi.RmcEfgParams()
+    ep.lrmc_var = 1
+    ep.resolution_u_efg = ep.resolution_vzz_efg = ep.resolution_eta_efg = 0.1
+    ep.u_efg_min = ep.vzz_efg_min = -1.0
+    return ep
+
+
+def chisq_var_numpy(s):
+    """eval_chisq_var_distance restated in numpy: per atom and type the sorted
+    minimum-image distances to the other atoms of that type, the mean of the
+    m-th smallest over the atoms of each type, and
+    sum (d_m - mean_m)^2 / mean_m^2 over atoms, types and ranks."""
+    pos = np.asarray(s["pos"], float)
+    cell = np.asarray(s["cell"], float)
+    it = np.asarray(s["itype"]) - 1
+    frac = pos @ np.linalg.inv(cell)
+    frac -= np.floor(frac)
+    n, nt = len(pos), it.max() + 1
+    lists = {}
+    for a in range(n):
+        d = frac[a] - frac
+        d -= np.round(d)
+        r = np.sqrt(((d @ cell) ** 2).sum(1))
+        for t in range(nt):
+            sel = (it == t) & (np.arange(n) != a)
+            lists[a, t] = np.sort(r[sel])
+    chi = 0.0
+    for t1 in range(nt):
+        atoms = np.where(it == t1)[0]
+        for t2 in range(nt):
+            L = np.array([lists[a, t2] for a in atoms])
+            mean = L.sum(0) / len(atoms)
+            chi += (((L - mean) / mean) ** 2).sum()
+    return chi
+
+
+def gexp_of(s, cut=2.0, res=0.05):
+    return oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"]).gr(cut, res)
+
+
+def test_variance_term_against_numpy_and_zero_on_a_lattice():
+    # a two-type jittered cell: the oracle's chi^2 (no trial move) against the
+    # numpy restatement; on the perfect FCC lattice every atom sees the same
+    # sorted distances, so the term vanishes
+    t = rigid_mgo(grid=(4, 4, 4), jitter=0.12, seed=3)
+    o = oracle.Oracle(t["params"], t["itype"], t["pos"], t["cell"])
+    rp = rmc_params(10, 1)
+    rp.cut_rmc = 4.0
+    rp.resolution_gr = 0.1
+    g = o.gr(4.0, 0.1)
+    ep = var_params()
+    su, sv, se = ep.shapes(t["params"].ntype)
+    r, *_ = o.rmc_efg(rp, ep, g, np.zeros(su), np.zeros(sv), np.zeros(se), np.zeros(0))
+    ref = chisq_var_numpy(t)
+    assert abs(r["chisq"][1] - ref) < 1e-10 * ref
+    s = lj(ncell=3)
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    su, sv, se = ep.shapes(s["params"].ntype)
+    r, *_ = o.rmc_efg(rmc_params(10, 1), ep, gexp_of(s), np.zeros(su), np.zeros(sv), np.zeros(se), np.zeros(0))
+    assert r["chisq"][1] < 1e-20
+
+
+def test_variance_term_drives_the_chain_towards_equal_environments():
+    # with the variance term alone deciding (g(r) at a high temperature), the
+    # chain from a jittered lattice makes the atoms' distance lists more alike
+    s = lj(ncell=3, jitter=0.06, seed=4)
+    o = oracle.Oracle(s["params"], s["itype"], s["pos"], s["cell"])
+    rp = rmc_params(100, 6000)
+    rp.temp_rmc[0] = 1e6
+    ep = var_params()
+    su, sv, se = ep.shapes(s["params"].ntype)
+    chi0 = chisq_var_numpy(s)
+    r, *_ = o.rmc_efg(rp, ep, gexp_of(s), np.zeros(su), np.zeros(sv), np.zeros(se),
+                      np.random.default_rng(9).random(40000))
+    assert r["status"] == 0 and r["kacc"] == 100
+    assert r["chisq"][1] < 0.9 * chi0

@@ -153,7 +153,9 @@ def test_rmc_variance_chain_matches_oracle(with_efg):
     # one value moved per atom and trial) and the oracle's full recount every
     # trial take the same decisions; the variance chi^2 agrees to 1e-11 (its
     # final sum runs per atom and by a fixed tree, the reference's left to right)
-    ep = efg_params() if with_efg else var_params()
+    ep = efg_params()
+    if not with_efg:
+        ep.lrmc_u = ep.lrmc_vzz = ep.lrmc_eta = 0
     ep.lrmc_var = 1
     t = rigid_mgo(seed=7, jitter=0.15)
     g, U, V, E, _ = distributions(t, efg_params())

@@ -59,6 +59,8 @@ def parse():
                     help="kspace_reuse (auto: on for the mixed path, off for the plain FP64 path)")
     ap.add_argument("--opt-iters", type=int, default=10,
                     help="opt workload: iterations (sastry), 5x as many force evaluations (lbfgs) or iterations (m1qn3)")
+    ap.add_argument("--rmc-var-moves", type=int, default=50,
+                    help="rmc workload: trial moves with the distance-variance term (0: skip)")
     ap.add_argument("--rmc-efg-moves", type=int, default=100,
                     help="rmc workload: trial moves of the chain with the EFG chi^2 terms (0: skip)")
     ap.add_argument("--optalgo", default="sastry", choices=["sastry", "lbfgs", "m1qn3"],
@@ -1166,6 +1168,38 @@ def run_rmc(args):
                 "fp64": efg_runs["fp64"], "mixed": efg_runs["mixed"],
                 "note": "one full-device Ewald EFG evaluation of the trial configuration per move, as rmc_efg "
                         "computes it (multipole_efg_ES); value = the mixed path"}
+    if args.rmc_var_moves > 0:
+        # the distance-variance term (eval_chisq_var_distance): the sorted
+        # distance lists of all 32k ions (natm^2 doubles, 8.4 GB) built once
+        # per call and kept on the device; per trial the moved ion's lists are
+        # sorted again and one value moves in every other ion's list
+        ev = mdff_b200.Engine(p, s["itype"], pos0, s["cell"])
+        ep = abi.RmcEfgParams()
+        ep.lrmc_var = 1
+        ep.resolution_u_efg = ep.resolution_vzz_efg = ep.resolution_eta_efg = 0.1
+        ep.u_efg_min = ep.vzz_efg_min = -1.0
+        su, sv, se = ep.shapes(p.ntype)
+        z = (np.zeros(su), np.zeros(sv), np.zeros(se))
+        r1 = abi.RmcParams.from_buffer_copy(rp)
+        r1.acceptance_max, r1.max_trials = 10 ** 12, 1
+        t0 = time.perf_counter()
+        ev.rmc_efg(r1, ep, gexp, *z, seed=5)   # the set-up alone: lists, sort, first chi^2
+        setup_s = time.perf_counter() - t0
+        r1.max_trials = args.rmc_var_moves + 1
+        t0 = time.perf_counter()
+        rv, *_ = ev.rmc_efg(r1, ep, gexp, *z, seed=7)
+        wall = time.perf_counter() - t0
+        ev.close()
+        moves = rv["kall"] - 1
+        if result is not None:
+            result["variance_term"] = {
+                "metric": "reverse Monte Carlo trial moves/s with the g(r) and distance-variance chi^2 terms, 32k ions",
+                "value": moves / max(1e-9, wall - setup_s), "unit": "moves/s", "moves": moves,
+                "accepted": rv["kacc"] - 1, "setup_s": setup_s, "wall_s_with_setup": wall,
+                "chisq_var_last": rv["chisq"][1],
+                "note": "value = moves / (wall time of the call - its set-up, both timed on the host around the "
+                        "synchronous call); the reference recounts all natm^2 distances and sorts every list at "
+                        "each trial"}
     if result is not None:
         if not args.no_cpu:
             import oracle

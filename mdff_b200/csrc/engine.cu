@@ -4358,7 +4358,8 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
         while (varP < maxlen) varP <<= 1;
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        const size_t need = sizeof(double) * ((size_t)n * vs.Ltot + (size_t)ctx->ntype * ctx->ntype * vs.nmax);
+        const size_t need = sizeof(double) * ((size_t)n * vs.Ltot + (size_t)ctx->ntype * ctx->ntype * vs.nmax +
+                                              (size_t)VAR_NCH * ctx->ntype * vs.Ltot);
         if (need + ((size_t)1 << 29) > fr)
             return fail(ctx, MDFF_E_UNSUPPORTED, "mdff_rmc_efg: the variance term's distance lists need " +
                                                      std::to_string(need >> 20) + " MiB of device memory, " +
@@ -4391,12 +4392,13 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     TRY(rmc_frac(ctx, s));
     k_rmc_dirkar<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->cell, ctx->x, ctx->y, ctx->z);
     k_gr_full<<<nb(n), 256, 0, ctx->st>>>(n, s, ctx->type, ctx->cell, k->bin, hd);
-    double *vl = nullptr, *vmean = nullptr, *vpart = nullptr;
+    double *vl = nullptr, *vmean = nullptr, *vpart = nullptr, *vpsum = nullptr;
     int *vrank = nullptr, *verr = nullptr;
     const int vwb = (n * 32 + 255) / 256;   // blocks of the per-atom chi kernel (a warp per atom)
     if (var) {
         CK(cudaMallocAsync((void**)&vl, sizeof(double) * (size_t)n * vs.Ltot, ctx->st));
         CK(cudaMallocAsync((void**)&vmean, sizeof(double) * (size_t)vs.ntype * vs.ntype * vs.nmax, ctx->st));
+        CK(cudaMallocAsync((void**)&vpsum, sizeof(double) * (size_t)VAR_NCH * vs.ntype * vs.Ltot, ctx->st));
         CK(cudaMallocAsync((void**)&vpart, sizeof(double) * (size_t)(vwb + 1), ctx->st));
         CK(cudaMallocAsync((void**)&vrank, sizeof(int) * (size_t)n, ctx->st));
         CK(cudaMallocAsync((void**)&verr, sizeof(int), ctx->st));
@@ -4413,7 +4415,8 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     }
     // chi^2 of the variance term from the lists (launches; *res written on the device)
     auto var_launch = [&](double* dres) {
-        k_var_mean<<<nb(n), 256, 0, ctx->st>>>(vs, ctx->type, vl, vmean);
+        k_var_mean<<<dim3(nb(n), VAR_NCH), 256, 0, ctx->st>>>(vs, ctx->type, vl, vpsum);
+        k_var_mean_fin<<<nb(n), 256, 0, ctx->st>>>(vs, vpsum, vmean);
         k_var_chi<<<vwb, 256, 0, ctx->st>>>(vs, ctx->type, vl, vmean, vpart);
         launch_reduce_partials(ctx->st, vpart, vwb, 1, dres, 0);
     };
@@ -4600,7 +4603,8 @@ int mdff_rmc_efg(mdff_ctx* ctx, const mdff_rmc_params* rp, const mdff_rmc_efg_pa
     int var_err = 0;
     if (var) {
         if (cudaMemcpyAsync(&var_err, verr, sizeof(int), cudaMemcpyDeviceToHost, ctx->st) != cudaSuccess) var_err = 2;
-        for (void* q : {(void*)vl, (void*)vmean, (void*)vpart, (void*)vrank, (void*)verr}) cudaFreeAsync(q, ctx->st);
+        for (void* q : {(void*)vl, (void*)vmean, (void*)vpart, (void*)vrank, (void*)verr, (void*)vpsum})
+            cudaFreeAsync(q, ctx->st);
     }
     for (void* q : {(void*)s, (void*)hd, (void*)dh, (void*)ce}) cudaFreeAsync(q, ctx->st);
     cudaStreamSynchronize(ctx->st);

@@ -14,8 +14,8 @@
 //     d(ja, p_old) -> d(ja, p_new): it is found by binary search and moved to
 //     its new rank by shifting the values in between (one warp per atom);
 // then the means and chi^2 are formed again from the lists: the means by a
-// per-rank sum over the atoms in atom order (the reference's order), chi^2 per
-// atom and by a fixed tree over the atoms.
+// per-rank sum over 64 ranges of atoms added in order, chi^2 per atom and by
+// a fixed tree over the atoms.
 #include "common.cuh"
 
 namespace mdff {
@@ -153,25 +153,42 @@ __global__ void k_var_shift(VarSpec v, const double* __restrict__ s, const int* 
 }
 
 // dab_aver of the reference: for every list type t2 and rank m, the sum over
-// the atoms (in atom order) of each type t1 of their m-th smallest distance to
-// type t2 (zero distances left out, as there), divided by natmi(t1).
-// mean[(t1 * ntype + t2) * nmax + m]; one thread per (t2, m).
+// the atoms of each type t1 of their m-th smallest distance to type t2 (zero
+// distances left out, as there), divided by natmi(t1).  Pass 1: one thread per
+// (t2, m) and range of VAR_NCH atoms (blockIdx.y), atoms in order, partial
+// sums psum[(chunk * ntype + t1) * Ltot + off[t2] + m]; pass 2 (k_var_mean_fin)
+// adds the chunks in order: mean[(t1 * ntype + t2) * nmax + m].
+constexpr int VAR_NCH = 64;
 __global__ void k_var_mean(VarSpec v, const int* __restrict__ type, const double* __restrict__ vl,
-                           double* __restrict__ mean) {
+                           double* __restrict__ psum) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     int t2 = 0, m = g;
     while (t2 < v.ntype && m >= v.natmi[t2]) { m -= v.natmi[t2]; ++t2; }
     if (t2 >= v.ntype) return;
+    const int per = (v.n + VAR_NCH - 1) / VAR_NCH;
+    const int a0 = blockIdx.y * per, a1 = min(v.n, a0 + per);
     double S[MDFF_NTYPE_MAX];
     for (int t = 0; t < v.ntype; ++t) S[t] = 0.0;
-    for (int ia = 0; ia < v.n; ++ia) {
+    for (int ia = a0; ia < a1; ++ia) {
         const int t1 = type[ia];
         if (m < var_len(v, t2, t1)) {
             const double d = vl[(size_t)ia * v.Ltot + v.off[t2] + m];
             if (d != 0.0) S[t1] += d;
         }
     }
-    for (int t1 = 0; t1 < v.ntype; ++t1) mean[((size_t)t1 * v.ntype + t2) * v.nmax + m] = S[t1] / (double)v.natmi[t1];
+    for (int t1 = 0; t1 < v.ntype; ++t1) psum[((size_t)blockIdx.y * v.ntype + t1) * v.Ltot + v.off[t2] + m] = S[t1];
+}
+
+__global__ void k_var_mean_fin(VarSpec v, const double* __restrict__ psum, double* __restrict__ mean) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    int t2 = 0, m = g;
+    while (t2 < v.ntype && m >= v.natmi[t2]) { m -= v.natmi[t2]; ++t2; }
+    if (t2 >= v.ntype) return;
+    for (int t1 = 0; t1 < v.ntype; ++t1) {
+        double S = 0.0;
+        for (int ch = 0; ch < VAR_NCH; ++ch) S += psum[((size_t)ch * v.ntype + t1) * v.Ltot + v.off[t2] + m];
+        mean[((size_t)t1 * v.ntype + t2) * v.nmax + m] = S / (double)v.natmi[t1];
+    }
 }
 
 // chi^2 per atom, sum over t2 and ranks with a nonzero mean of

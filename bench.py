@@ -704,13 +704,16 @@ def run_batch(args):
     configurations (200-2000 ions each, rc <= 10 A, PCG 1e-8) and its adjoint
     gradient with respect to the 12 force-field parameters, all configurations
     in one set of launches.  Targets are the FP64 forces and stresses at
-    parameters perturbed 5 % from the seed values."""
+    parameters perturbed 5 % from the seed values.  Timed on the FP64 batch
+    and on the mixed one (the dipole operator's pair table in FP32); value is
+    the one --precision names, and the mixed loss and gradient are compared
+    with the FP64 ones."""
     import torch
     world, rank, local, dist = dist_setup(args.gpus)
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     import mdff_b200
-    from mdff_b200 import fit, systems
+    from mdff_b200 import abi, fit, systems
     confs = systems.mgo_batch()
     base = systems.mgo_params(6.0, 0.5, 6)
     base.conv_tol_ind = 1e-8
@@ -719,59 +722,78 @@ def run_batch(args):
     space = fit.mgo_space(base)
     theta0 = space.get(base)
     theta_t = theta0 * (1.0 + 0.05 * np.random.default_rng(7).standard_normal(len(theta0)))
-    b = mdff_b200.Batch(space.apply(base, theta_t), confs)
-    tgt = b.forces()
-    b.set_params(base)
-    b.set_targets(tgt["f"], tgt["tau"], 1.0, 0.01)
-    ext = torch.cuda.ExternalStream(b.stream(), device=device)
-    for _ in range(max(args.warmup, 1)):
-        b.loss_grad()
-    barrier(dist, device)
-    torch.cuda.synchronize(device)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    its = []
-    with ClockSampler(local) as clk:
-        ev0.record(ext)
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            L, g, it = b.loss_grad()
-            its.append(it)
-        t1 = time.perf_counter()
-        ev1.record(ext)
-        ev1.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    ms_max = max_over_ranks(ms, dist, device)
-    value = whole_job_rate(args.steps, ms / 1e3, dist, device)
-    e2e_v = whole_job_rate(args.steps, t1 - t0, dist, device)
-    natm = int(b.N)
+    bt = mdff_b200.Batch(space.apply(base, theta_t), confs)
+    tgt = bt.forces()
+    bt.close()
+    runs = {}
+    clk_summary = None
+    for prec_name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+        bp = copy_params(base)
+        bp.precision = prec
+        b = mdff_b200.Batch(bp, confs)
+        b.set_targets(tgt["f"], tgt["tau"], 1.0, 0.01)
+        ext = torch.cuda.ExternalStream(b.stream(), device=device)
+        for _ in range(max(args.warmup, 1)):
+            b.loss_grad()
+        barrier(dist, device)
+        torch.cuda.synchronize(device)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        its = []
+        with ClockSampler(local) as clk:
+            ev0.record(ext)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                L, g, it = b.loss_grad()
+                its.append(it)
+            t1 = time.perf_counter()
+            ev1.record(ext)
+            ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        if prec_name == args.precision:
+            clk_summary = clk.summary()
+        runs[prec_name] = {"value": whole_job_rate(args.steps, ms / 1e3, dist, device),
+                           "ms_per_step": max_over_ranks(ms, dist, device) / args.steps,
+                           "e2e": whole_job_rate(args.steps, t1 - t0, dist, device),
+                           "solve_iterations": {"forward": float(np.mean([i[0] for i in its])),
+                                                "adjoint": float(np.mean([i[1] for i in its]))},
+                           "loss": L, "grad": space.project(g, theta0)}
+        natm = int(b.N)
+        nat = (int(min(b.natm)), int(max(b.natm)))
+        b.close()
+    sel = runs[args.precision]
+    gm, gd = runs["mixed"]["grad"], runs["fp64"]["grad"]
+    acc = {"rel_loss": abs(runs["mixed"]["loss"] - runs["fp64"]["loss"]) / abs(runs["fp64"]["loss"]),
+           "rel_grad": float(np.linalg.norm(gm - gd) / np.linalg.norm(gd)),
+           "max_component_rel_grad": float(np.max(np.abs(gm - gd) / np.abs(gd)))}
     result = None
     if rank == 0:
         result = {
             "metric": "force-matching loss+gradient evaluations/s, 64-configuration MgO PIM batch",
-            "value": value,
+            "value": sel["value"],
             "unit": "evaluations/s",
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": ms_max / args.steps,
+            "ms_per_step": sel["ms_per_step"],
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "fp64",
+            "dtype": "fp32+fp64" if args.precision == "mixed" else "fp64",
             "data": "synthetic (seeded rock-salt MgO snapshots, mdff_b200.systems.mgo_batch)",
             "config": {"workload": "mgo-pim-force-matching-batch", "nconf": len(confs), "natm_total": natm,
-                       "natm_range": [int(min(b.natm)), int(max(b.natm))], "parameters": space.names,
+                       "natm_range": list(nat), "parameters": space.names, "precision": args.precision,
                        "solver": "pcg", "tol": base.conv_tol_ind, "parallelism": f"replicas{world}",
                        "l2": "each evaluation rewrites > 126 MB (k-space partials, lists of 69k ions)"},
-            "atom_evaluations_per_s": natm * value,
-            "solve_iterations": {"forward": float(np.mean([i[0] for i in its])),
-                                 "adjoint": float(np.mean([i[1] for i in its]))},
-            "e2e": {"value": e2e_v, "unit": "evaluations/s",
+            "atom_evaluations_per_s": natm * sel["value"],
+            "solve_iterations": sel["solve_iterations"],
+            "fp64": {k: v for k, v in runs["fp64"].items() if k not in ("grad",)},
+            "mixed": {k: v for k, v in runs["mixed"].items() if k not in ("grad",)},
+            "mixed_vs_fp64": acc,
+            "e2e": {"value": sel["e2e"], "unit": "evaluations/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8 + 82048},
-            "clocks": clk.summary(),
+            "clocks": clk_summary,
         }
-    b.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -258,6 +258,86 @@ __device__ __forceinline__ PairG ewald_radial(double d2, double a, int erfc_ref)
     return g;
 }
 
+// The dipole operator from a pair table.  A batch's positions never move, so
+// for every neighbour within rc the pair vector and the radial factors
+// A1 = F1/r^3, B2 = 3 F2/r^5 of the undamped dipole field are computed once
+// (k_b_ddtab_build) and every application of the operator in the forward and
+// adjoint solves is a gather: E_i = sum_j r (r.mu_j) B2 - mu_j A1.  Entries are
+// stored per quantity ([5][N cap]: rx ry rz A1 B2), FP64, or FP32 when the
+// batch runs mixed (the products then in FP32, the sums in FP64).  Rows are
+// compacted to the neighbours within rc in list order.
+template <int G, typename T>
+__global__ void __launch_bounds__(256) k_b_ddtab_build(int N, const int* __restrict__ cfg_of,
+                                                       const BCfg* __restrict__ cf, const double* __restrict__ sx,
+                                                       const double* __restrict__ sy, const double* __restrict__ sz,
+                                                       const int* __restrict__ nbr, const int* __restrict__ cnt,
+                                                       int cap, int erfc_ref, int* __restrict__ dnbr,
+                                                       int* __restrict__ dcnt, T* __restrict__ tab) {
+    const int gid = (int)(((long)blockIdx.x * blockDim.x + threadIdx.x) / G);
+    const int sub = threadIdx.x & (G - 1);
+    const bool active = gid < N;
+    const int i = active ? gid : 0;
+    const BCfg& C = cf[cfg_of[i]];
+    const size_t NC = (size_t)N * cap;
+    const int g0 = (threadIdx.x & 31) & ~(G - 1);
+    const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << g0);
+    const int m = active ? cnt[i] : 0;
+    int base = 0;
+    for (int k0 = 0; k0 < m; k0 += G) {   // m is the same for the G lanes of an atom
+        const int k = k0 + sub;
+        const bool valid = k < m;
+        const int j = valid ? nbr[(size_t)i * cap + k] : i;
+        double rx = 0, ry = 0, rz = 0, d2 = 0;
+        if (valid) d2 = pairvec_exact(C.cell, sx[i], sy[i], sz[i], sx[j], sy[j], sz[j], rx, ry, rz);
+        const bool in = valid && d2 <= C.rc2;
+        const unsigned bal = (__ballot_sync(gmask, in) & gmask) >> g0;
+        const int pos = base + __popc(bal & ((1u << sub) - 1u));
+        if (in) {
+            const PairG g = ewald_radial(d2, C.alpha, erfc_ref);
+            const size_t e = (size_t)i * cap + pos;
+            dnbr[e] = j;
+            tab[e] = (T)rx;
+            tab[NC + e] = (T)ry;
+            tab[2 * NC + e] = (T)rz;
+            tab[3 * NC + e] = (T)g.A1;
+            tab[4 * NC + e] = (T)g.B2;
+        }
+        base += __popc(bal);
+    }
+    if (active && sub == 0) dcnt[i] = base;
+}
+
+template <int G, typename T>
+__global__ void __launch_bounds__(256) k_b_ddtab(int N, const int* __restrict__ cfg_of, const int* __restrict__ conv,
+                                                 const int* __restrict__ dnbr, const int* __restrict__ dcnt, int cap,
+                                                 const T* __restrict__ tab, const double* __restrict__ v,
+                                                 double* __restrict__ E) {
+    const int gid = (int)(((long)blockIdx.x * blockDim.x + threadIdx.x) / G);
+    const int sub = threadIdx.x & (G - 1);
+    bool active = gid < N;
+    const int i = active ? gid : 0;
+    if (conv && conv[cfg_of[i]]) active = false;
+    const size_t NC = (size_t)N * cap;
+    double V0 = 0.0, V1 = 0.0, V2 = 0.0;
+    if (active) {
+        const int m = dcnt[i];
+        for (int k = sub; k < m; k += G) {
+            const size_t e = (size_t)i * cap + k;
+            const int j = dnbr[e];
+            const T rx = tab[e], ry = tab[NC + e], rz = tab[2 * NC + e], A1 = tab[3 * NC + e], B2 = tab[4 * NC + e];
+            const T mj0 = (T)v[j], mj1 = (T)v[N + j], mj2 = (T)v[2 * N + j];
+            const T rb = (rx * mj0 + ry * mj1 + rz * mj2) * B2;
+            V0 += (double)(rx * rb - mj0 * A1);
+            V1 += (double)(ry * rb - mj1 * A1);
+            V2 += (double)(rz * rb - mj2 * A1);
+        }
+    }
+    V0 = group_sum<G>(V0);
+    V1 = group_sum<G>(V1);
+    V2 = group_sum<G>(V2);
+    if (active && sub == 0) { E[i] = V0; E[N + i] = V1; E[2 * N + i] = V2; }
+}
+
 // MODE 0: damped field of the charges (static field b of the dipole solve,
 //         src/field.f90:3270-3272).
 // MODE 1: field of the dipoles mu, undamped (the operator T, src/field.f90:3354).
@@ -1209,6 +1289,13 @@ struct mdff_batch {
     double* tau_t_dev = nullptr;         // [nconf][9]
     double* loss_c = nullptr;            // [nconf]
     double* tau_c = nullptr;             // [nconf][9]
+    // the dipole operator's pair table (k_b_ddtab_build), FP64 or FP32
+    int *dd_nbr = nullptr, *dd_cnt = nullptr;
+    double* dd64 = nullptr;
+    float* dd32 = nullptr;
+    int dd_ref = -1;                     // erfc_ref the table was built with
+    int g_dd = 16;                       // lanes per atom of the table operator (autotuned)
+    float dd_ms[4] = {0, 0, 0, 0};       // the autotuner's timings for 4, 8, 16, 32 lanes
 };
 
 namespace {
@@ -1375,11 +1462,76 @@ int kfield(mdff_batch* b, const int* conv, double* V, double* G) {
 
 int dir_blocks(int N, int G) { return nblk((long)N * G, 256); }
 
+// The real-space part of the dipole operator from the pair table, with G
+// lanes per atom.
+void launch_ddtab(mdff_batch* b, int g, const double* v, double* E) {
+    const int blocks = dir_blocks(b->N, g);
+#define DDT(GG)                                                                                                    \
+    do {                                                                                                           \
+        if (b->dd32)                                                                                               \
+            k_b_ddtab<GG, float><<<blocks, 256, 0, b->st>>>(b->N, b->cfg_of, b->conv, b->dd_nbr, b->dd_cnt, b->cap, \
+                                                            b->dd32, v, E);                                        \
+        else                                                                                                       \
+            k_b_ddtab<GG, double><<<blocks, 256, 0, b->st>>>(b->N, b->cfg_of, b->conv, b->dd_nbr, b->dd_cnt,      \
+                                                             b->cap, b->dd64, v, E);                               \
+    } while (0)
+    if (g == 4) DDT(4);
+    else if (g == 8) DDT(8);
+    else if (g == 32) DDT(32);
+    else DDT(16);
+#undef DDT
+}
+
+// The pair table of the dipole operator (positions and alpha are fixed for the
+// batch's life; erfc_ref follows the parameters), then the autotuner's choice
+// of lanes per atom for it: each candidate timed over three launches after a
+// warm-up, with CUDA events on the batch's stream.
+int build_ddtab(mdff_batch* b) {
+    const int N = b->N;
+    const bool mixed = b->p.precision == MDFF_PREC_MIXED;
+    const size_t NC = (size_t)N * b->cap;
+    if (!b->dd_nbr) {
+        BTRY(balloc(b, &b->dd_nbr, NC));
+        BTRY(balloc(b, &b->dd_cnt, (size_t)N));
+        if (mixed) BTRY(balloc(b, &b->dd32, 5 * NC));
+        else BTRY(balloc(b, &b->dd64, 5 * NC));
+    }
+    const int er = b->fl.erfc_ref;
+    if (mixed)
+        k_b_ddtab_build<16, float><<<dir_blocks(N, 16), 256, 0, b->st>>>(N, b->cfg_of, b->cfg, b->sx, b->sy, b->sz,
+                                                                         b->nbr, b->cnt, b->cap, er, b->dd_nbr,
+                                                                         b->dd_cnt, b->dd32);
+    else
+        k_b_ddtab_build<16, double><<<dir_blocks(N, 16), 256, 0, b->st>>>(N, b->cfg_of, b->cfg, b->sx, b->sy, b->sz,
+                                                                          b->nbr, b->cnt, b->cap, er, b->dd_nbr,
+                                                                          b->dd_cnt, b->dd64);
+    BTRY(blaunch(b, "dd table"));
+    b->dd_ref = er;
+    BCK(cudaMemsetAsync(b->cg_d, 0, sizeof(double) * 3 * N, b->st));
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    const int gs[4] = {4, 8, 16, 32};
+    float best = 1e30f;
+    for (int k = 0; k < 4; ++k) {
+        launch_ddtab(b, gs[k], b->cg_d, b->Eind);
+        cudaEventRecord(e0, b->st);
+        for (int r = 0; r < 3; ++r) launch_ddtab(b, gs[k], b->cg_d, b->Eind);
+        cudaEventRecord(e1, b->st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        b->dd_ms[k] = ms / 3.f;
+        if (ms < best) { best = ms; b->g_dd = gs[k]; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return blaunch(b, "dd table autotune");
+}
+
 // E = T v (undamped dipole field, real + reciprocal; self term in apply_A).
 int dd_field(mdff_batch* b, const double* v, double* E) {
-    k_b_dir<16, 1><<<dir_blocks(b->N, 16), 256, 0, b->st>>>(b->N, b->cfg_of, b->cfg, b->conv, b->sx, b->sy, b->sz,
-                                                            b->type, b->q, v, b->nbr, b->cnt, b->cap, b->pc, b->fl, E,
-                                                            nullptr, nullptr);
+    launch_ddtab(b, b->g_dd, v, E);
     BTRY(blaunch(b, "dd field"));
     BTRY((structure_factor<1, 0>(b, b->conv, v)));
     return kfield<0, 1, 1>(b, b->conv, E, nullptr);
@@ -1958,6 +2110,7 @@ int mdff_batch_create(const mdff_params* p, int nconf, const int* natm, const in
         if (attempt == 3) return bad(bfail(b, MDFF_E_LISTOVF, "batch: neighbour list capacity exceeded"));
         cap = (int)(ovf * 1.25) + 32;
     }
+    if (int r2 = build_ddtab(b)) return bad(r2);
     return MDFF_OK;
 }
 
@@ -1977,7 +2130,10 @@ const char* mdff_batch_last_error(const mdff_batch* b) { return b ? b->err.c_str
 int mdff_batch_set_params(mdff_batch* b, const mdff_params* p) {
     if (!b || !p) return MDFF_E_ARG;
     if (p->lcoulomb != b->p.lcoulomb) return bfail(b, MDFF_E_ARG, "batch: lcoulomb cannot change after creation");
-    return upload_params(b, *p);
+    if (p->precision != b->p.precision) return bfail(b, MDFF_E_ARG, "batch: precision cannot change after creation");
+    BTRY(upload_params(b, *p));
+    if (b->fl.erfc_ref != b->dd_ref) BTRY(build_ddtab(b));   // the table's erfc follows the parameters
+    return MDFF_OK;
 }
 
 int mdff_batch_forces(mdff_batch* b, double* fx, double* fy, double* fz, double* tau, double* energy, int* iters) {

@@ -228,3 +228,32 @@ def test_batch_64_matches_oracle_and_central_differences():
             ok = np.abs(ge - fd) <= np.maximum(1e-5 * np.abs(fd), floor)
             assert ok.all(), list(zip(space.names, ge, fd, floor))
         b.close()
+
+
+def test_mixed_batch_against_fp64_batch():
+    """The mixed batch (the dipole operator's pair table in FP32, its products
+    in FP32 and sums in FP64) against the FP64 batch on the force-matching
+    workload: forces to 1e-6 (global relative), and the loss and gradient to
+    2e-5 -- the loss squares the force residual, which is ~5 % of the force, so
+    a force error e moves the loss by ~2e / 0.05."""
+    import mdff_b200
+    confs = systems.mgo_batch()
+    base = _base(1e-10)
+    space = fit.mgo_space(base)
+    theta0 = space.get(base)
+    theta_t = theta0 * (1.0 + 0.05 * np.random.default_rng(7).standard_normal(len(theta0)))
+    ft, tt = _targets(base, space, confs, theta_t)
+    out = {}
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        p = fit.ParamSpace([]).apply(base, [])
+        p.precision = prec
+        b = mdff_b200.Batch(p, confs)
+        fo = b.forces()
+        b.set_targets(ft, tt, 1.0, 0.01)
+        L, g, _ = b.loss_grad()
+        out[prec] = (np.concatenate([f.ravel() for f in fo["f"]]), L, space.project(g, theta0))
+        b.close()
+    (fd, Ld, gd), (fm, Lm, gm) = out[abi.PREC_FP64], out[abi.PREC_MIXED]
+    assert np.linalg.norm(fm - fd) / np.linalg.norm(fd) < 1e-6
+    assert abs(Lm - Ld) < 2e-5 * abs(Ld)
+    assert np.linalg.norm(gm - gd) < 2e-5 * np.linalg.norm(gd)

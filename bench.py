@@ -53,8 +53,8 @@ def parse():
     ap.add_argument("--keps", type=float, default=None,
                     help="mixed path: leave out k with exp(-k^2/4 alpha^2) below keps (0: all; default: the library's)")
     ap.add_argument("--autotune", type=int, default=1, choices=[0, 1], help="autotune the launch shapes")
-    ap.add_argument("--tc", type=int, default=1, choices=[0, 1],
-                    help="mixed path: structure factor on the tensor cores (1) or the FP32 CUDA-core kernel (0)")
+    ap.add_argument("--tc", type=int, default=2, choices=[0, 1, 2],
+                    help="mixed path: k-space on the tensor cores (1), with the low-|k| set too (2), or the FP32 CUDA-core kernels (0)")
     ap.add_argument("--reuse", default="auto", choices=["auto", "0", "1"],
                     help="kspace_reuse (auto: on for the mixed path, off for the plain FP64 path)")
     ap.add_argument("--opt-iters", type=int, default=10,

@@ -143,9 +143,11 @@ typedef struct mdff_params {
                                                   is below mixed_keps are left out (0: the whole rectangle) */
     int    autotune;                           /* 1: time the candidate launch shapes of the Ewald kernels on the
                                                   first force evaluation and keep the fastest */
-    int    kspace_tc;                          /* mixed path: 1 = structure factor on the tensor cores (exact int8
-                                                  digit products of 24-bit fixed point) when nz rows <= 80;
-                                                  0 = FP32 CUDA-core kernel */
+    int    kspace_tc;                          /* mixed path: 1 = structure factor and field on the tensor cores
+                                                  (exact int8 digit products of 24-bit fixed point) when nz rows
+                                                  <= 80, the low-|k| set in FP64 on the CUDA cores; 2 = the low-|k|
+                                                  set on the tensor cores as well (32-bit fixed point, FP64
+                                                  operands) when its nz rows <= 32; 0 = FP32 CUDA-core kernels */
     /* &mdtag, constant pressure (integrator MDFF_NPT_NHCNP) */
     double press;                              /* GPa (md_check_tag converts with press_unit) */
     double timesca_baro;                       /* ps */
@@ -300,6 +302,12 @@ int  mdff_profile_detail(mdff_ctx* ctx, double ms[MDFF_NDETAIL], long long count
  * the half space, or its part inside the fp64_keps sphere) and out[3] the FP64
  * low-|k| set of the mixed path (0 on the FP64 path). */
 int  mdff_kspace_info(mdff_ctx* ctx, long long out[4]);
+
+/* Which reciprocal-space kernels the mixed path uses (no reference
+ * counterpart): out[0] = 1 when the main set runs on the tensor cores (24-bit
+ * fixed point, kspace_tc >= 1), out[1] = 1 when the low-|k| set does (32-bit
+ * fixed point, kspace_tc = 2); 0 for the FP32 / FP64 CUDA-core kernels. */
+int  mdff_kspace_mode(mdff_ctx* ctx, int out[2]);
 
 /* How the context's MD steps ran (no reference counterpart): out[0] steps
  * replayed from a captured CUDA graph (the whole step, the dipole PCG as a

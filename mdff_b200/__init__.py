@@ -86,6 +86,7 @@ def lib():
         L.mdff_struct_size.argtypes = [C.c_int]
         L.mdff_kspace_info.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.mdff_graph_info.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.mdff_kspace_mode.argtypes = [vp, C.POINTER(C.c_int)]
         L.mdff_erfc_check.argtypes = [C.c_int, C.c_int, dp, dp, dp]
         L.mdff_launch_shape.argtypes = [vp, C.POINTER(C.c_int)]
         L.mdff_batch_create.argtypes = [C.POINTER(abi.Params), C.c_int, ip, ip, dp, dp, dp, dp, dp, dp, ip, C.POINTER(vp)]
@@ -177,6 +178,13 @@ class Engine:
         out = (C.c_longlong * 4)()
         self._check(lib().mdff_kspace_info(self._h, out))
         return {"rect": out[0], "half": out[1], "main": out[2], "low": out[3]}
+
+    def kspace_mode(self):
+        """Which reciprocal kernels the mixed path uses: the main set and the
+        low-|k| set on the tensor cores (mdff_kspace_mode)."""
+        out = (C.c_int * 2)()
+        self._check(lib().mdff_kspace_mode(self._h, out))
+        return {"main_tc": bool(out[0]), "low_tc": bool(out[1])}
 
     def graph_info(self):
         """How the MD steps ran: replayed from a CUDA graph, captures made,

@@ -223,7 +223,7 @@ def default_params():
     p.device = 0
     p.mixed_ksplit = 2.5
     p.mixed_keps = 1e-7
-    p.kspace_tc = 1
+    p.kspace_tc = 2
     p.press = 0.0
     p.timesca_baro = 1.0
     return p

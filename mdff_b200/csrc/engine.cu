@@ -2774,6 +2774,13 @@ int mdff_launch_shape(mdff_ctx* ctx, int out[4]) {
     return MDFF_OK;
 }
 
+int mdff_kspace_mode(mdff_ctx* ctx, int out[2]) {
+    if (!ctx || !out) return MDFF_E_ARG;
+    out[0] = ctx->rs.tc.on ? 1 : 0;
+    out[1] = ctx->rs.low.tc ? 1 : 0;
+    return MDFF_OK;
+}
+
 int mdff_graph_info(mdff_ctx* ctx, long long out[3]) {
     if (!ctx || !out) return MDFF_E_ARG;
     out[0] = ctx->nstep_graph;
@@ -2834,7 +2841,7 @@ void mdff_params_default(mdff_params* p) {
     p->precision = MDFF_PREC_FP64;
     p->mixed_ksplit = 2.5;
     p->mixed_keps = 1e-7;
-    p->kspace_tc = 1;
+    p->kspace_tc = 2;
     p->press = 0.0;
     p->timesca_baro = 1.0;   // md_default_tag (src/md.f90:204)
 }
@@ -3117,7 +3124,57 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 TRY(dalloc(ctx, &lk.kcoe, kcl.size()));
                 TRY(upload(ctx, lk.Ak, akl.data(), (int)akl.size()));
                 TRY(upload(ctx, lk.kcoe, kcl.data(), (int)kcl.size()));
-                TRY(dalloc(ctx, &lk.part, 2 * (size_t)lk.P * nzmax * lk.ncol));
+                // tensor-core form: one tile of list columns per 128, atoms split
+                // so that the grid covers the SMs about once
+                int kxl = 0, kyl = 0, kzl = 0;
+                for (const Col& C_ : cl) {
+                    kxl = std::max(kxl, std::abs(C_.nx));
+                    kyl = std::max(kyl, std::abs(C_.ny));
+                    kzl = std::max(kzl, std::max(std::abs(C_.lo - kg.kmax[2]), std::abs(C_.lo + C_.nn - 1 - kg.kmax[2])));
+                }
+                lk.tc = 0;
+                if (p.kspace_tc == 2) {
+                    // GEMM rows nz = -kzl..-1, 1..kzl (the nz = 0 row is summed apart)
+                    lk.kx = kxl; lk.ky = kyl; lk.kz = kzl; lk.nzl = 2 * kzl;
+                    lk.N = std::max(16, ((2 * lk.nzl + 15) / 16) * 16);
+                    lk.XYW = kxl + 2 + 2 * kyl;
+                    lk.KZ = std::max(32, ((2 * lk.nzl + 31) / 32) * 32);
+                    lk.ntile = (lk.ncol + 127) / 128;
+                    lk.nblk = (n + tc4::SA - 1) / tc4::SA;
+                    lk.npad = lk.nblk * tc4::SA;
+                    const int S = std::max(1, 148 / lk.ntile);
+                    lk.bps = std::min(std::max(1, (lk.nblk + S - 1) / S), tc4::MAX_ATOMS_PER_CTA / tc4::SA);
+                    lk.nsplit = (lk.nblk + lk.bps - 1) / lk.bps;
+                    lk.ntile_f = (n + 127) / 128;
+                    const size_t smax = 227 * 1024;
+                    lk.nin = tc4::Layout::depth(lk.N, lk.XYW, smax - 10 * 1024);   // static shared memory aside
+                    const tc4::Layout l4(lk.N, lk.XYW, std::max(lk.nin, 2));
+                    const tc4::FLayout f2(lk.KZ, lk.XYW, tc4::Cfg<2>::NB, tc4::Cfg<2>::CB);
+                    const tc4::FLayout f3(lk.KZ, lk.XYW, tc4::Cfg<3>::NB, tc4::Cfg<3>::CB);
+                    lk.smem = l4.smem_bytes();
+                    lk.smem_f2 = f2.smem_bytes();
+                    lk.smem_f3 = f3.smem_bytes();
+                    lk.tc = lk.N <= tc4::LS && lk.KZ <= 128 && lk.nin >= 2 && lk.smem_f2 <= smax &&
+                            lk.smem_f3 <= smax;
+                    if (lk.tc) {
+                        const size_t ncb2 = (lk.ncol + tc4::Cfg<2>::CB - 1) / tc4::Cfg<2>::CB;
+                        const size_t ncb3 = (lk.ncol + tc4::Cfg<3>::CB - 1) / tc4::Cfg<3>::CB;
+                        TRY(dalloc(ctx, &lk.xy, (size_t)lk.npad * lk.XYW));
+                        TRY(dalloc(ctx, &lk.bimg, (size_t)lk.nblk * l4.b_bytes()));
+                        TRY(dalloc(ctx, &lk.prm, (size_t)lk.npad));
+                        TRY(dalloc(ctx, &lk.amax, (size_t)lk.npad));
+                        TRY(dalloc(ctx, &lk.aimg, (size_t)lk.ntile_f * f2.a_bytes()));
+                        TRY(dalloc(ctx, &lk.xyt, (size_t)lk.ntile_f * lk.XYW * 128));
+                        TRY(dalloc(ctx, &lk.fimg, std::max(ncb2 * f2.stage_bytes, ncb3 * f3.stage_bytes)));
+                        CK(cudaFuncSetAttribute(tc4::k_sfac_tc4, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)lk.smem));
+                        CK(cudaFuncSetAttribute(tc4::k_kfield_tc4<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)lk.smem_f2));
+                        CK(cudaFuncSetAttribute(tc4::k_kfield_tc4<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)lk.smem_f3));
+                    }
+                }
+                TRY(dalloc(ctx, &lk.part, 2 * (size_t)std::max(lk.P, lk.tc ? lk.nsplit : 0) * nzmax * lk.ncol));
                 TRY(dalloc(ctx, &lk.aks, 2 * (size_t)lk.ncol * nzmax));
                 TRY(dalloc(ctx, &lk.aks_acc, 2 * (size_t)lk.ncol * nzmax));
                 TRY(dalloc(ctx, &lk.fpart, 4 * 9 * (size_t)n));

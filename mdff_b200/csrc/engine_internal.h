@@ -249,6 +249,20 @@ struct LowK {
     double* aks_acc = nullptr;   // solver accumulator of aks (reuse of structure factors)
     double2* tab = nullptr;   // [n][16] e^{2 pi i m s_z} in FP64
     int P = 1, natom_chunk = 0;
+    // tensor-core form in 32-bit fixed point (kspace_tc = 2, ewald_tc4.cuh)
+    int tc = 0;
+    int kx = 0, ky = 0, kz = 0, nzl = 0;   // index half-ranges of the list; nz rows 2 kz + 1
+    int N = 0, XYW = 0;                    // structure-factor GEMM N, X/Y table width
+    int nblk = 0, npad = 0, bps = 0, nsplit = 0, ntile = 0, nin = 0;   // nin: input pipeline depth
+    int KZ = 0, ntile_f = 0;               // field pass: K bytes per atom row, 128-atom tiles
+    size_t smem = 0, smem_f2 = 0, smem_f3 = 0;
+    double2* xy = nullptr;    // [npad][XYW] X_a[nx], Y_a[ny]
+    uint8_t* bimg = nullptr;  // [nblk] B digit images
+    double4* prm = nullptr;   // [npad] (q, m1, m2, m3)
+    double* amax = nullptr;   // [npad]
+    uint8_t* aimg = nullptr;  // [ntile_f] Z digit images
+    double2* xyt = nullptr;   // [ntile_f][XYW][128]
+    uint8_t* fimg = nullptr;  // per evaluation: B digit images + column constants
 };
 
 // Tensor-core structure factor of the mixed path (ewald_tc.cuh).

@@ -20,6 +20,7 @@
 // [-kz,kz] with A_k = 0 on the half that the reference skips.
 #include "common.cuh"
 #include "ewald_tc.cuh"
+#include "ewald_tc4.cuh"
 
 namespace mdff {
 
@@ -967,17 +968,66 @@ size_t rec_scratch_doubles(int n, const KGrid& kg, size_t* fpart, int mixed) {
 // images); returns the number of kernels launched.
 int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, RecScratch& rs) {
     if (rs.tab_epoch == rs.want_epoch) return 0;
-    k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab, rs.low.ncol > 0 ? rs.low.tab : nullptr);
+    const LowK& lk = rs.low;
+    k_phase_table<<<(n + 127) / 128, 128, 0, st>>>(n, sx, sy, sz, rs.fixed, rs.tab,
+                                                   lk.ncol > 0 && !lk.tc ? lk.tab : nullptr);
     rs.tab_epoch = rs.want_epoch;
-    if (!rs.tc.on) return 1;
-    const TcK& t = rs.tc;
-    const long nxy = (long)t.npad * t.XYW, nb = (long)t.npad * (t.N / 2);
-    tcs::k_tc_xy<<<(unsigned)((nxy + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kx, t.ky, t.XYW, t.xy);
-    tcs::k_tc_bimage<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kz, t.nzl, t.N, t.bimg);
-    const long na = (long)t.ntile_f * 128 * (t.KZ / 16), nt = (long)t.ntile_f * 128 * t.XYW;
-    tcf::k_tcf_aimage<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(n, t.ntile_f, rs.fixed, t.kz, t.nzl, t.KZ, t.aimg);
-    tcf::k_tcf_xyt<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(t.npad, t.ntile_f, t.xy, t.XYW, t.xyt);
-    return 5;
+    int nk = 1;
+    if (rs.tc.on) {
+        const TcK& t = rs.tc;
+        const long nxy = (long)t.npad * t.XYW, nb = (long)t.npad * (t.N / 2);
+        tcs::k_tc_xy<<<(unsigned)((nxy + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kx, t.ky, t.XYW, t.xy);
+        tcs::k_tc_bimage<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(n, t.npad, rs.fixed, t.kz, t.nzl, t.N, t.bimg);
+        const long na = (long)t.ntile_f * 128 * (t.KZ / 16), nt = (long)t.ntile_f * 128 * t.XYW;
+        tcf::k_tcf_aimage<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(n, t.ntile_f, rs.fixed, t.kz, t.nzl, t.KZ,
+                                                                       t.aimg);
+        tcf::k_tcf_xyt<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(t.npad, t.ntile_f, t.xy, t.XYW, t.xyt);
+        nk += 4;
+    }
+    if (lk.tc) {
+        const long nxy = (long)lk.npad * lk.XYW, nb = (long)lk.npad * (lk.N / 2);
+        tc4::k_tc4_xy<<<(unsigned)((nxy + 255) / 256), 256, 0, st>>>(n, lk.npad, rs.fixed, lk.kx, lk.ky, lk.XYW, lk.xy);
+        tc4::k_tc4_bimage<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(n, lk.npad, rs.fixed, lk.kz, lk.nzl, lk.N,
+                                                                       lk.bimg);
+        const long na = (long)lk.ntile_f * 128 * (lk.KZ / 16), nt = (long)lk.ntile_f * 128 * lk.XYW;
+        tc4::k_tc4f_aimage<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(n, lk.ntile_f, rs.fixed, lk.kz, lk.nzl,
+                                                                        lk.KZ, lk.aimg);
+        tc4::k_tc4f_xyt<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(lk.npad, lk.ntile_f, lk.xy, lk.XYW, lk.xyt);
+        nk += 4;
+    }
+    return nk;
+}
+
+// Field pass over the low-|k| list: the 32-bit tensor-core kernels or the
+// FP64 CUDA-core kernel; returns the number of kernels launched.
+int launch_low_field(cudaStream_t st, int n, CellP c, bool grad, RecScratch& rs, DevScalars* d) {
+    LowK& lk = rs.low;
+    if (lk.tc) {
+        const int nch = lk.KZ / 16;
+        if (grad) {
+            using C3 = tc4::Cfg<3>;
+            const int ncb = (lk.ncol + C3::CB - 1) / C3::CB;
+            tc4::k_tc4f_bimage<3><<<ncb, C3::NB * nch, 0, st>>>(lk.ncol, lk.col, lk.nzmax, lk.kx, lk.ky, lk.kz,
+                                                                lk.nzl, lk.KZ, lk.aks, c, lk.fimg);
+            tc4::k_kfield_tc4<3><<<lk.ntile_f, tc4::FTHREADS, lk.smem_f3, st>>>(n, ncb, lk.aimg, lk.xyt, lk.fimg,
+                                                                               lk.KZ, lk.XYW, c, lk.fpart, &d->tc_err);
+        } else {
+            using C2 = tc4::Cfg<2>;
+            const int ncb = (lk.ncol + C2::CB - 1) / C2::CB;
+            tc4::k_tc4f_bimage<2><<<ncb, C2::NB * nch, 0, st>>>(lk.ncol, lk.col, lk.nzmax, lk.kx, lk.ky, lk.kz,
+                                                                lk.nzl, lk.KZ, lk.aks, c, lk.fimg);
+            tc4::k_kfield_tc4<2><<<lk.ntile_f, tc4::FTHREADS, lk.smem_f2, st>>>(n, ncb, lk.aimg, lk.xyt, lk.fimg,
+                                                                               lk.KZ, lk.XYW, c, lk.fpart, &d->tc_err);
+        }
+        return 2;
+    }
+    if (grad)
+        k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+            n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+    else
+        k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
+            n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
+    return 1;
 }
 
 #define CUDA_COPY_ACC(st, dst, src, bytes) cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (st))
@@ -1067,14 +1117,28 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     if (fl.energy && !fl.reuse) launch_reduce_partials(st, part.buf, rb, 7, d->rec, 0);
     if (low && !fl.reuse) {
         LowK& lk = rs.low;
-        const int nch = (lk.nzmax + TM - 1) / TM;
-        const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;
-        dim3 gl(nch * cb, lk.P);
-        const size_t lplane = (size_t)lk.P * lk.nzmax * lk.ncol;
-        k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, rs.fixed, lk.tab, q, mu, c, lk.col, lk.ncol, lk.nzmax,
-                                                nch, fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
+        int Pl = lk.P;
+        if (lk.tc) {
+            // 32-bit fixed point on the tensor cores: one partial per atom split
+            Pl = lk.nsplit;
+            const size_t lplane = (size_t)Pl * lk.nzmax * lk.ncol;
+            tc4::k_tc4_params<<<(lk.npad + 255) / 256, 256, 0, st>>>(n, lk.npad, q, mu, c, fl.with_q, fl.with_mu, lk.kx,
+                                                                     lk.ky, lk.kz, lk.prm, lk.amax);
+            tc4::k_sfac_tc4<<<dim3(lk.ntile, lk.nsplit), tc4::THREADS, lk.smem, st>>>(
+                lk.nblk, lk.bps, lk.nin, lk.bimg, lk.xy, lk.prm, lk.amax, lk.col, lk.ncol, lk.nzmax, lk.kx, lk.ky, lk.kz, lk.N,
+                lk.XYW, lk.part, lk.part + lplane, &d->tc_err);
+            nk += 1;
+        } else {
+            const int nch = (lk.nzmax + TM - 1) / TM;
+            const int cb = (lk.ncol + SF_THREADS - 1) / SF_THREADS;
+            dim3 gl(nch * cb, lk.P);
+            const size_t lplane = (size_t)lk.P * lk.nzmax * lk.ncol;
+            k_sfac64_low<<<gl, SF_THREADS, 0, st>>>(n, lk.natom_chunk, rs.fixed, lk.tab, q, mu, c, lk.col, lk.ncol,
+                                                    lk.nzmax, nch, fl.with_q, fl.with_mu, lk.part, lk.part + lplane);
+        }
+        const size_t lplane = (size_t)Pl * lk.nzmax * lk.ncol;
         const int lb = (lk.ncol * lk.nzmax * 32 + 255) / 256;
-        k_sfac64_low_reduce<<<lb, 256, 0, st>>>(lk.P, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane, lk.Ak,
+        k_sfac64_low_reduce<<<lb, 256, 0, st>>>(Pl, lk.ncol, lk.nzmax, lk.col, lk.part, lk.part + lplane, lk.Ak,
                                                 lk.kcoe, c, lk.aks, fl.energy, part.buf);
         if (fl.energy) launch_reduce_partials(st, part.buf, lb, 7, d->rec, 1);
         nk += 2 + (fl.energy ? 1 : 0);
@@ -1111,16 +1175,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         }
         nsplit_f = tcf::NQ;
         nk += 1;
-        if (low) {
-            LowK& lk = rs.low;
-            if (grad)
-                k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
-            else
-                k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
-            nk++;
-        }
+        if (low) nk += launch_low_field(st, n, c, grad, rs, d);
     } else if (mixed) {
         const int nzp = nchunk32 * TM;
         k_aks32_pad<<<(kg.ncol * nzp + 255) / 256, 256, 0, st>>>(kg.ncol, kg.nzl, nzp, kg.nrect, rs.aks, rs.aks2);
@@ -1132,16 +1187,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             k_kfield32v5<0><<<g2, KF_THREADS, sm32, st>>>(n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp,
                                                          L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
         nk += 2;
-        if (low) {
-            LowK& lk = rs.low;
-            if (grad)
-                k_kfield64_low<1><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
-            else
-                k_kfield64_low<0><<<dim3((n + KF_THREADS - 1) / KF_THREADS, LK_SPLIT), KF_THREADS, 0, st>>>(
-                    n, rs.fixed, lk.tab, c, lk.col, lk.ncol, lk.nzmax, lk.aks, lk.fpart);
-            nk++;
-        }
+        if (low) nk += launch_low_field(st, n, c, grad, rs, d);
     } else {
         size_t smem = sizeof(double) * 2 * KF_COLS * kg.nzl;
         const bool sph = kg.nfcol > 0;
@@ -1160,7 +1206,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
     k_kfield_reduce<<<(n + 255) / 256, 256, 0, st>>>(n, nsplit_f, grad ? 1 : 0, rs.fpart, scale, fl.with_q ? q : nullptr,
                                                     fl.with_mu ? mu : nullptr, fl.field ? ef : nullptr, efg,
                                                     fl.forces ? fo : nullptr, low ? rs.low.fpart : nullptr,
-                                                    low ? LK_SPLIT : 0);
+                                                    low ? (rs.low.tc ? tc4::NQ : LK_SPLIT) : 0);
     prof->end(nk);
 }
 

@@ -112,6 +112,15 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v) {
+    uint32_t r[4];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr)
+                 : "memory");
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
@@ -220,6 +229,36 @@ __device__ __forceinline__ void slices4(uint32_t w0, uint32_t w1, uint32_t w2, u
     s2 = __byte_perm(t01, t23, 0x7632);
     const uint32_t v01 = __byte_perm(w0, w1, 0x0062), v23 = __byte_perm(w2, w3, 0x0062);
     s1 = __byte_perm(v01, v23, 0x5410);
+}
+
+// ---- 32-bit fixed point in four signed 8-bit slices --------------------------
+// V = rn(v * QS4) with |V| <= 0x7F7F7F7F; the bytes of (V + 0x80808080) ^
+// 0x80808080 are signed digits d1 (byte 3, most significant) .. d4 with
+// V = d1 2^24 + d2 2^16 + d3 2^8 + d4, d1 in [-127, 127], the others in
+// [-128, 127].  QS4 leaves 2.9e-5 of headroom for |v| <= 1 plus rounding.
+constexpr double QS4 = 2139000000.0;
+__device__ __forceinline__ uint32_t digits32(int V) { return ((uint32_t)V + 0x80808080u) ^ 0x80808080u; }
+// Four values (consecutive K) -> one 32-bit word per slice: s1 (most
+// significant digits) .. s4.
+__device__ __forceinline__ void slices4x4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, uint32_t& s1,
+                                          uint32_t& s2, uint32_t& s3, uint32_t& s4) {
+    const uint32_t t01 = __byte_perm(w0, w1, 0x5140), t23 = __byte_perm(w2, w3, 0x5140);   // bytes 0 and 1
+    const uint32_t u01 = __byte_perm(w0, w1, 0x7362), u23 = __byte_perm(w2, w3, 0x7362);   // bytes 2 and 3
+    s4 = __byte_perm(t01, t23, 0x5410);
+    s3 = __byte_perm(t01, t23, 0x7632);
+    s2 = __byte_perm(u01, u23, 0x5410);
+    s1 = __byte_perm(u01, u23, 0x7632);
+}
+
+// Conversions on the FP64 pipe instead of the conversion unit: 1.5 * 2^52
+// has a unit in the last place of 1, so v + M rounds v to the nearest
+// integer (ties to even, as cvt.rni) and its low word is that integer for
+// |v| < 2^31; and the bit pattern of M plus an integer |x| < 2^51 is the
+// double M + x, from which M subtracts exactly.
+constexpr double MAGIC52 = 6755399441055744.0;
+__device__ __forceinline__ int rint_i32(double v) { return __double2loint(v + MAGIC52); }
+__device__ __forceinline__ double i64_to_f64(long long x) {
+    return __longlong_as_double(0x4338000000000000ll + x) - MAGIC52;
 }
 
 }  // namespace umma

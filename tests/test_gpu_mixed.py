@@ -144,6 +144,58 @@ def test_tensor_core_structure_factor(case):
         assert rel(out["tc"]["efg"], d["efg"]) < 1e-6
 
 
+@pytest.mark.parametrize("case", ["mgo_pim", "silica_rigid", "mgo_small_kz"])
+def test_low_set_on_tensor_cores(case):
+    """kspace_tc = 2: the low-|k| set as int8 digit GEMMs of 32-bit fixed
+    point (FP64 operands, ten digit products in four exact S32 levels) against
+    the same set in FP64 on the CUDA cores (kspace_tc = 1), and against the
+    FP64 path.  The 32-bit quantisation is 2.3e-10 of each operand's scale;
+    a field value sums ~1 700 (column, nz) terms, so its error is about
+    sqrt(1700) x 4.7e-10 = 2e-8 of the term size (measured 1.2e-8 on the
+    forces and 1.8e-8 on the dipoles of the 4 055-ion PIM cell), a tenth of
+    the mixed path's own error (~1.5e-7): forces, dipoles, field and EFG to
+    5e-8.  The energy sums |S(k)|^2, where the quantisation errors average
+    out: 1e-9 (measured 1.5e-12 on the PIM cell, 1.5e-10 on rigid-ion
+    silica, whose few ions average less).  Covers dipoles with the field gradient (EFG), charges only,
+    and a short nz range."""
+    if case == "mgo_pim":
+        s = systems.mgo_pim(grid=(16, 16, 16), rc=10.0, alpha=0.3, kmax=12, vacancy_frac=0.01, seed=3, jitter=0.1)
+        over = dict(doefg=1, conv_tol_ind=1e-10)
+    elif case == "silica_rigid":
+        s = systems.silica_bmh()
+        over = dict(doefield=1)
+    else:
+        s = systems.mgo_pim(grid=(10, 10, 6), rc=6.0, alpha=0.5, kmax=9, vacancy_frac=0.02, seed=5, jitter=0.1)
+        s["params"].kES[2] = 4
+        over = dict(doefg=1, conv_tol_ind=1e-10)
+    out, mode = {}, {}
+    for key, prec, tc in (("fp64", abi.PREC_FP64, 0), ("low64", abi.PREC_MIXED, 1), ("low32", abi.PREC_MIXED, 2)):
+        p = s["params"]
+        p.precision = prec
+        p.kspace_tc = tc
+        for k, v in over.items():
+            setattr(p, k, v)
+        e = mdff_b200.Engine(p, s["itype"], s["pos"], s["cell"])
+        out[key] = e.engforce()
+        mode[key] = e.kspace_mode()
+        e.close()
+    assert mode["low32"] == {"main_tc": True, "low_tc": True}, mode
+    assert mode["low64"] == {"main_tc": True, "low_tc": False}, mode
+    a, b, d = out["low32"], out["low64"], out["fp64"]
+    errs = {"F": rel(a["f"], b["f"]), "u": abs(a["e"]["u_coul"] - b["e"]["u_coul"]) / abs(b["e"]["u_coul"]),
+            "tau": rel(a["tau_coul"], b["tau_coul"])}
+    if over.get("doefg"):
+        errs.update(mu=rel(a["mu"], b["mu"]), efg=rel(a["efg"], b["efg"]))
+    else:
+        errs.update(ef=rel(a["ef"], b["ef"]))
+    print(case, errs)
+    assert 0.0 < errs["F"] < 5e-8, errs
+    assert max(v for k, v in errs.items() if k != "u") < 5e-8, errs
+    assert errs["u"] < 1e-9, errs
+    assert rel(a["f"], d["f"]) < 1e-6
+    assert abs(a["e"]["u_coul"] - d["e"]["u_coul"]) < 1e-6 * abs(d["e"]["u_coul"])
+
+
 def _production_run(pos, s, prec, kadd=0):
     p = s["params"]
     p.precision = prec

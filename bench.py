@@ -30,6 +30,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-steps/s PIM-Ewald 32k atoms, mixed vs FP64 GPU at <=1e-6 rel force err"
 
+# DRAM traffic per launch (MB, read + write) of the tensor-core k-space
+# kernels on the 32 440-ion production cell, from one ncu capture of each
+# (the launch list and sections are summarised under profiles/).
+TC_TRAFFIC_MB = {"sfac_tc": 58.0, "kfield_tc": 29.3, "sfac_tc4": 31.5, "kfield_tc4": 17.8}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -449,9 +454,14 @@ def run_engine(args):
             achieved = ops / (tc_ms / 1e3) / 1e12
             per = {}
             for k, v in det.items():
-                if v["count"]:
+                if v["count"] and k != "efg_sites":
                     per[k] = {"launches": v["count"], "ms_per_launch": v["ms"] / v["count"],
-                              "tops": v["ops"] / (v["ms"] / 1e3) / 1e12}
+                              "tops": v["ops"] / (v["ms"] / 1e3) / 1e12,
+                              "traffic_mb": TC_TRAFFIC_MB.get(k)}
+            # DRAM bytes per (structure factor + field) pair of the two main
+            # kernels, weighted by their launch counts in the profiled pass
+            n_s, n_f = det["sfac_tc"]["count"], det["kfield_tc"]["count"]
+            traffic = (TC_TRAFFIC_MB["sfac_tc"] * n_s + TC_TRAFFIC_MB["kfield_tc"] * n_f) / max(1, n_s + n_f) * 1e6
             roof = {
                 "bound": "tensor",
                 "kernels": "k_sfac_tc + k_kfield_tc (tcgen05 kind::i8 digit GEMMs of the reciprocal sum)",
@@ -465,7 +475,11 @@ def run_engine(args):
                 "share_of_step": tc_ms / total_ms if total_ms else None,
                 # algorithmic FP32-equivalent rate of the k-space sum these two kernels perform
                 "kspace_fp32_equiv_tflops": (sf_flops + kf_flops) / (tc_ms / 1e3) / 1e12,
-                "traffic": None,
+                "traffic": traffic,
+                "traffic_note": "bytes per launch averaged over the two kernels' launches: ncu "
+                                "dram__bytes_read.sum + dram__bytes_write.sum of one capture of each "
+                                "(32 440 ions, kmax 23), per kernel in per_kernel.traffic_mb; the tensor "
+                                "kernels are not memory-bound (a few % of HBM)",
             }
         else:
             achieved = (sf_flops + kf_flops) / (k_ms / 1e3) / 1e12 if k_ms > 0 else None

@@ -287,11 +287,12 @@ int  mdff_profile_get(mdff_ctx* ctx, double ms[8], long long count[8], long long
 /* Detail timers of single kernels: the tensor-core structure-factor kernel
  * [0] and field kernel [1] (mixed path, inside groups 3 and 4) with the int8
  * digit-product operations they were launched for (2 M N K per product, six
- * products, unpadded problem), and the EFG post-processing site kernel [2]
- * with the bytes it must read (52 per site: tensor and type) -- accumulated
- * milliseconds, launches and work; cleared with the groups.  No reference
- * counterpart. */
-#define MDFF_NDETAIL 3
+ * products, unpadded problem), the EFG post-processing site kernel [2] with
+ * the bytes it must read (52 per site: tensor and type), and the low-|k|
+ * set's 32-bit tensor-core structure-factor [3] and field [4] kernels (ten
+ * digit products) -- accumulated milliseconds, launches and work; cleared
+ * with the groups.  No reference counterpart. */
+#define MDFF_NDETAIL 5
 int  mdff_profile_detail(mdff_ctx* ctx, double ms[MDFF_NDETAIL], long long count[MDFF_NDETAIL],
                          double ops[MDFF_NDETAIL]);
 

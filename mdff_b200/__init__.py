@@ -438,11 +438,11 @@ class Engine:
         """Single-kernel detail timers: the tensor-core k-space kernels (mixed
         path; ops = int8 digit-product operations) and the EFG site kernel
         (ops = bytes it reads): accumulated ms, launches and work."""
-        ms, ops = np.zeros(3), np.zeros(3)
-        cnt = (C.c_longlong * 3)()
+        ms, ops = np.zeros(5), np.zeros(5)
+        cnt = (C.c_longlong * 5)()
         self._check(lib().mdff_profile_detail(self._h, _dp(ms), cnt, _dp(ops)))
         return {k: {"ms": float(ms[i]), "count": int(cnt[i]), "ops": float(ops[i])}
-                for i, k in enumerate(("sfac_tc", "kfield_tc", "efg_sites"))}
+                for i, k in enumerate(("sfac_tc", "kfield_tc", "efg_sites", "sfac_tc4", "kfield_tc4"))}
 
     def nlist_build(self):
         self._check(lib().mdff_nlist_build(self._h))

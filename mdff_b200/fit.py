@@ -133,6 +133,40 @@ def batch_constants(natm, w_force, w_stress):
     return [(w_force / (3.0 * n * B), w_stress / (9.0 * B)) for n in natm]
 
 
+def shard(confs, rank, world):
+    """The configurations rank `rank` of `world` data-parallel ranks takes of
+    a force-matching batch: largest first to the rank with the fewest atoms so
+    far (ties to the lower rank), so every rank gets about the same number of
+    atoms.  Returns (the rank's configurations, their indices in confs)."""
+    order = sorted(range(len(confs)), key=lambda c: (-len(confs[c]["itype"]), c))
+    load = [0] * world
+    mine = []
+    for c in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += len(confs[c]["itype"])
+        if r == rank:
+            mine.append(c)
+    mine.sort()
+    return [confs[c] for c in mine], mine
+
+
+def allreduce_loss_grad(loss, grad, n_local, n_total, dist, device):
+    """Whole-batch loss and dL/dtheta from each rank's shard.  A rank's Batch
+    normalises by its own configuration count (the 1/B of the loss), so the
+    whole batch's value is the sum over ranks of (n_local / n_total) times
+    the shard's: one all-reduce of 1 + len(grad) doubles.  With dist None
+    (one rank) the values come back unchanged."""
+    import torch
+    g = np.asarray(grad, dtype=np.float64)
+    if dist is None:
+        return float(loss), g.copy()
+    w = float(n_local) / float(n_total)
+    t = torch.tensor(np.concatenate([[w * float(loss)], w * g]), dtype=torch.float64, device=device)
+    dist.all_reduce(t)
+    v = t.cpu().numpy()
+    return float(v[0]), v[1:].copy()
+
+
 def _autograd_function():
     import torch
 

@@ -43,7 +43,8 @@ namespace {
 constexpr int CHUNK = 128;     // atoms per reciprocal-space block
 constexpr int NZC = 8;         // nz values per thread in the structure factor
 constexpr int KT = 128;        // threads of the reciprocal-space blocks
-constexpr int CT = 8;          // k-columns staged per tile in the field kernel
+constexpr int CT = 16;         // k-columns staged per tile in the field kernel
+constexpr int KF_LPA = 4;      // lanes per atom in the field kernel (columns interleaved)
 constexpr int NTYB = 2;        // types supported by the gradient kernels
 
 
@@ -688,10 +689,14 @@ __global__ void __launch_bounds__(256) k_b_grad_rows(int N, const int* __restric
 
 // Pass 1: structure-factor partials of one chunk of atoms over its
 // configuration's k rectangle.  One thread per (k-column, run of NZC nz);
-// phase e^{2 pi i n.s} by one sincospi per (atom, run) and a rotation by
-// e^{2 pi i s_z} per further nz.  Amplitudes:
+// the phase e^{2 pi i n.s} of a run's first nz is the product X[nx] Y[ny]
+// Z0[run] of per-atom tables in shared memory (one sincospi per atom and
+// table entry, built by the block), then a rotation by e^{2 pi i s_z} per
+// further nz.  Amplitudes:
 //   MODE 0: q            MODE 1: i k.mu          MODE 2: q + i k.mu
 //   MODE 3: (k.R)(q + i k.mu)   (the adjoint structure factor)
+// Dynamic shared memory: CHUNK x phw_max double2 (the tables of the block's
+// atoms, one row per atom: X[0..kx], Y[-ky..ky], Z0[run]).
 template <int MODE>
 __global__ void __launch_bounds__(KT) k_b_sfac(const BChunk* __restrict__ chunks, const BCfg* __restrict__ cf,
                                                const int* __restrict__ conv, int N, const double* __restrict__ sx,
@@ -699,16 +704,19 @@ __global__ void __launch_bounds__(KT) k_b_sfac(const BChunk* __restrict__ chunks
                                                const double* __restrict__ q, const double* __restrict__ mu,
                                                const double* __restrict__ R, double* __restrict__ part_re,
                                                double* __restrict__ part_im) {
-    __shared__ double t_s1[CHUNK], t_s2[CHUNK], t_s3[CHUNK], t_q[CHUNK], t_cz[CHUNK], t_sn[CHUNK];
+    __shared__ double t_q[CHUNK], t_cz[CHUNK], t_sn[CHUNK];
     __shared__ double t_u[3][CHUNK], t_v[3][CHUNK];
+    extern __shared__ double2 t_ph[];
     const BChunk ch = chunks[blockIdx.x];
     if (conv && conv[ch.c]) return;
     const BCfg& C = cf[ch.c];
+    const int kx = C.kmax[0], ky = C.kmax[1], kz = C.kmax[2];
+    const int nzch = (C.nzl + NZC - 1) / NZC;
+    const int W = (kx + 1) + (2 * ky + 1) + nzch;
     for (int a = threadIdx.x; a < ch.na; a += blockDim.x) {
         const int ia = ch.a0 + a;
-        t_s1[a] = sx[ia]; t_s2[a] = sy[ia]; t_s3[a] = sz[ia];
         double sn, cs;
-        sincospi(2.0 * t_s3[a], &sn, &cs);
+        sincospi(2.0 * sz[ia], &sn, &cs);
         t_cz[a] = cs; t_sn[a] = sn;
         t_q[a] = (MODE == 1) ? 0.0 : q[ia];
         double m0 = 0, m1 = 0, m2 = 0, r0 = 0, r1 = 0, r2 = 0;
@@ -720,25 +728,35 @@ __global__ void __launch_bounds__(KT) k_b_sfac(const BChunk* __restrict__ chunks
             t_v[dcol][a] = 2.0 * PI * (C.cell.B[dcol] * r0 + C.cell.B[3 + dcol] * r1 + C.cell.B[6 + dcol] * r2);
         }
     }
+    for (int t = threadIdx.x; t < ch.na * W; t += blockDim.x) {
+        const int a = t / W, e = t % W, ia = ch.a0 + a;
+        double arg;
+        if (e <= kx) arg = (double)e * sx[ia];
+        else if (e <= kx + 1 + 2 * ky) arg = (double)(e - (kx + 1) - ky) * sy[ia];
+        else arg = (double)(-kz + (e - (kx + 2 + 2 * ky)) * NZC) * sz[ia];
+        double sn, cs;
+        sincospi(2.0 * arg, &sn, &cs);
+        t_ph[t] = make_double2(cs, sn);
+    }
     __syncthreads();
-    const int ky = C.kmax[1], kz = C.kmax[2];
-    const int nzch = (C.nzl + NZC - 1) / NZC;
     const int items = C.ncol * nzch;
     double* pre = part_re + ch.poff;
     double* pim = part_im + ch.poff;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
         const int col = it / nzch, zc = it % nzch;
-        const double nx = (double)(col / (2 * ky + 1));
-        const double ny = (double)(col % (2 * ky + 1) - ky);
+        const int ix = col / (2 * ky + 1), iy = col % (2 * ky + 1);
+        const double nx = (double)ix;
+        const double ny = (double)(iy - ky);
         const int m0 = zc * NZC;
         const double nz0 = (double)(-kz + m0);
+        const int ex = ix, ey = kx + 1 + iy, ez = kx + 2 + 2 * ky + zc;
         double are[NZC], aim[NZC];
 #pragma unroll
         for (int m = 0; m < NZC; ++m) { are[m] = 0.0; aim[m] = 0.0; }
         for (int a = 0; a < ch.na; ++a) {
-            double sn, cs;
-            sincospi(2.0 * (nx * t_s1[a] + ny * t_s2[a] + nz0 * t_s3[a]), &sn, &cs);
-            double er = cs, ei = sn;
+            const double2 X = t_ph[a * W + ex], Y = t_ph[a * W + ey], Z = t_ph[a * W + ez];
+            const double xr = fma(X.x, Y.x, -X.y * Y.y), xi = fma(X.x, Y.y, X.y * Y.x);
+            double er = fma(xr, Z.x, -xi * Z.y), ei = fma(xr, Z.y, xi * Z.x);
             const double rc = t_cz[a], rs = t_sn[a];
             const double qa = t_q[a];
             double km = nx * t_u[0][a] + ny * t_u[1][a] + nz0 * t_u[2][a];
@@ -765,12 +783,6 @@ __global__ void __launch_bounds__(KT) k_b_sfac(const BChunk* __restrict__ chunks
     }
 }
 
-// Sum the chunk partials of every k entry (fixed chunk order) and form the
-// coefficients C_k of pass 2:
-//   MODE 0 (FIELD): C = A conj(S)
-//   MODE 1 (FINAL): C = A conj(S), and S stored as rho (the final structure factor)
-//   MODE 2 (ADJ):   sigma = sum; C = A (-2 cu fpi_V i conj(sigma) - 2 c_s s_k conj(rho)),
-//                   s_k = tr S - kcoe k.S.k, c_s = cu/press 2 tpi_V/omega
 template <int MODE>
 __global__ void k_b_sfac_reduce(int nrect_tot, const int* __restrict__ rcfg, const BCfg* __restrict__ cf,
                                 const BChunk* __restrict__ chunks, const int* __restrict__ conv,
@@ -870,7 +882,7 @@ __global__ void k_b_rec_sums(const BCfg* __restrict__ cf, const double* __restri
 // 2 fpi_V of the configuration when SCALE_FPI, else 1.  V is written, or added
 // with ADD.
 template <int GRAD, int ADD, int SCALE_FPI>
-__global__ void __launch_bounds__(KT) k_b_kfield(const BChunk* __restrict__ chunks, const BCfg* __restrict__ cf,
+__global__ void __launch_bounds__(KT * KF_LPA) k_b_kfield(const BChunk* __restrict__ chunks, const BCfg* __restrict__ cf,
                                                  const int* __restrict__ conv, int N, const double* __restrict__ sx,
                                                  const double* __restrict__ sy, const double* __restrict__ sz,
                                                  const double* __restrict__ C_re, const double* __restrict__ C_im,
@@ -882,7 +894,7 @@ __global__ void __launch_bounds__(KT) k_b_kfield(const BChunk* __restrict__ chun
     const int nzl = C.nzl, ky = C.kmax[1], kz = C.kmax[2];
     double* t_re = smem;
     double* t_im = smem + CT * nzl;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x / KF_LPA, sub = threadIdx.x % KF_LPA;   // atom, lane among the atom's
     const bool active = t < ch.na;
     const int ia = ch.a0 + (active ? t : 0);
     const double s1 = sx[ia], s2 = sy[ia], s3 = sz[ia];
@@ -901,7 +913,7 @@ __global__ void __launch_bounds__(KT) k_b_kfield(const BChunk* __restrict__ chun
         }
         __syncthreads();
         if (!active) continue;
-        for (int cc = 0; cc < nc; ++cc) {
+        for (int cc = sub; cc < nc; cc += KF_LPA) {
             const int col = c0 + cc;
             const double nx = (double)(col / (2 * ky + 1)), ny = (double)(col % (2 * ky + 1) - ky);
             double sn, cs;
@@ -927,7 +939,16 @@ __global__ void __launch_bounds__(KT) k_b_kfield(const BChunk* __restrict__ chun
             }
         }
     }
-    if (!active) return;
+    // the atom's lanes are adjacent: sum them by a fixed xor tree
+#pragma unroll
+    for (int o = 1; o < KF_LPA; o <<= 1) {
+        E0 += __shfl_xor_sync(0xffffffffu, E0, o);
+        E1 += __shfl_xor_sync(0xffffffffu, E1, o);
+        E2 += __shfl_xor_sync(0xffffffffu, E2, o);
+        if (GRAD)
+            for (int k = 0; k < 6; ++k) G[k] += __shfl_xor_sync(0xffffffffu, G[k], o);
+    }
+    if (!active || sub != 0) return;
     const double sc = SCALE_FPI ? 2.0 * (4.0 * PI / C.cell.omega) : 1.0;
     if (ADD) {
         V[ia] += sc * E0; V[N + ia] += sc * E1; V[2 * N + ia] += sc * E2;
@@ -1243,6 +1264,7 @@ struct mdff_batch {
     int nchunk = 0;
     long part_len = 0;
     int nrect_tot = 0, nzl_max = 1;
+    int phw_max = 1;       // widest per-atom phase table of the structure factor (X, Y, Z0 entries)
     int* rcfg = nullptr;
     int* cfg_of = nullptr;
     int* type = nullptr;
@@ -1444,8 +1466,9 @@ int upload_params(mdff_batch* b, const mdff_params& pin) {
 // coefficients C_k (RMODE of k_b_sfac_reduce).
 template <int MODE, int RMODE>
 int structure_factor(mdff_batch* b, const int* conv, const double* mu) {
-    k_b_sfac<MODE><<<b->nchunk, KT, 0, b->st>>>(b->chunk, b->cfg, conv, b->N, b->sx, b->sy, b->sz, b->q, mu, b->R,
-                                                b->part_re, b->part_im);
+    const size_t sm = sizeof(double2) * (size_t)CHUNK * b->phw_max;
+    k_b_sfac<MODE><<<b->nchunk, KT, sm, b->st>>>(b->chunk, b->cfg, conv, b->N, b->sx, b->sy, b->sz, b->q, mu, b->R,
+                                                 b->part_re, b->part_im);
     k_b_sfac_reduce<RMODE><<<nblk(b->nrect_tot, 256), 256, 0, b->st>>>(b->nrect_tot, b->rcfg, b->cfg, b->chunk, conv,
                                                                        b->part_re, b->part_im, b->Ak, b->kcoe, b->Sres,
                                                                        b->fl, b->rho_re, b->rho_im, b->C_re, b->C_im);
@@ -1455,8 +1478,8 @@ int structure_factor(mdff_batch* b, const int* conv, const double* mu) {
 template <int GRAD, int ADD, int SCALE>
 int kfield(mdff_batch* b, const int* conv, double* V, double* G) {
     size_t sm = sizeof(double) * 2 * CT * b->nzl_max;
-    k_b_kfield<GRAD, ADD, SCALE><<<b->nchunk, KT, sm, b->st>>>(b->chunk, b->cfg, conv, b->N, b->sx, b->sy, b->sz,
-                                                               b->C_re, b->C_im, V, G);
+    k_b_kfield<GRAD, ADD, SCALE><<<b->nchunk, KT * KF_LPA, sm, b->st>>>(b->chunk, b->cfg, conv, b->N, b->sx, b->sy,
+                                                                        b->sz, b->C_re, b->C_im, V, G);
     return blaunch(b, "kfield");
 }
 
@@ -1984,6 +2007,7 @@ int mdff_batch_create(const mdff_params* p, int nconf, const int* natm, const in
         C.roff = roff;
         roff += C.nrect;
         b->nzl_max = std::max(b->nzl_max, C.nzl);
+        b->phw_max = std::max(b->phw_max, (C.kmax[0] + 1) + (2 * C.kmax[1] + 1) + (C.nzl + NZC - 1) / NZC);
         double dens = natm[c] / C.cell.omega;
         int est = (int)(dens * 4.0 / 3.0 * PI * rc[c] * rc[c] * rc[c] * 1.3) + 32;
         cap_est = std::max(cap_est, std::min(est, natm[c]));
@@ -2109,6 +2133,16 @@ int mdff_batch_create(const mdff_params* p, int nconf, const int* natm, const in
         if (ovf == 0) break;
         if (attempt == 3) return bad(bfail(b, MDFF_E_LISTOVF, "batch: neighbour list capacity exceeded"));
         cap = (int)(ovf * 1.25) + 32;
+    }
+    {   // the structure factor's per-atom phase tables live in dynamic shared memory
+        const size_t sm = sizeof(double2) * (size_t)CHUNK * b->phw_max;
+        if (sm > 200 * 1024)
+            return bad(bfail(b, MDFF_E_UNSUPPORTED, "batch: k rectangle too large for the structure factor's tables"));
+        cudaError_t e2 = cudaFuncSetAttribute(k_b_sfac<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e2 == cudaSuccess) e2 = cudaFuncSetAttribute(k_b_sfac<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e2 == cudaSuccess) e2 = cudaFuncSetAttribute(k_b_sfac<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e2 == cudaSuccess) e2 = cudaFuncSetAttribute(k_b_sfac<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e2 != cudaSuccess) return bad(bfail(b, MDFF_E_CUDA, cudaGetErrorString(e2)));
     }
     if (int r2 = build_ddtab(b)) return bad(r2);
     return MDFF_OK;

@@ -317,12 +317,15 @@ def run_engine(args):
     torch.cuda.synchronize(device)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    g0 = eng.graph_info()
     with ClockSampler(local) as clk:
         ev0.record(ext)
         out = eng.step(args.steps, thermo=True)
         ev1.record(ext)
         ev1.synchronize()
     torch.cuda.synchronize(device)
+    g1 = eng.graph_info()
+    graph_timed = {k: int(g1[k] - g0[k]) for k in g1}   # how the timed steps ran (replays, captures, plain)
     ms = ev0.elapsed_time(ev1)
     launches = eng.profile()["_launches"]["count"]   # counted with the timers off too
     ms_max = max_over_ranks(ms, dist, device)
@@ -522,6 +525,7 @@ def run_engine(args):
                        "l2": "per-step working set > 126 MB L2 (Verlet and pair-table lists, k-space digit "
                              "images, partials)"},
             "gpu_launches": int(launches),
+            "graph_timed_steps": graph_timed,
             "launch_shape": eng.launch_shape(),
             "solver_iters_mean": mean_it,
             "h_tot_drift_per_step": (h[-1] - h[0]) / max(1, len(h) - 1) / natm,

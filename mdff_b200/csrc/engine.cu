@@ -49,7 +49,7 @@ struct StepKey {
     CellP cell;
     int g_dir, g_dd, p_mul, s_mul;
     int efg;              // the step writes the EFG
-    int pmode, pnpt, pshift;   // predictor plan
+    int pmode, pnpt, pshift;   // unused (the predictor plan is device data)
     double skin;
     int n, pad;
 };
@@ -159,8 +159,9 @@ struct mdff_ctx {
     long glaunch[2] = {0, 0}, gbody[2] = {0, 0};   // kernels per replay outside / per PCG iteration
     long cap_body = 0;                   // kernels of one PCG iteration, counted while capturing
     bool pcg_in_graph = false;           // the last captured step solved dipoles in the graph
-    PredPlan coef_up;                    // the predictor coefficients on the device
+    PredPlan coef_up;                    // the predictor plan on the device (coef)
     bool coef_valid = false;
+    double plan_host[PLAN_LEN] = {0};    // staging of the plan upload
     long long nstep_graph = 0, ncapture = 0, nstep_plain = 0;
 };
 
@@ -688,25 +689,32 @@ PredPlan pred_plan(const mdff_ctx* ctx) {
     return pl;
 }
 
-// Extrapolated initial guess from the stored history.  The coefficients are
-// uploaded only when they change (never inside a captured step, where the
-// plan is part of the graph's key).
+// The predictor's plan of this step into device memory, when it changed (on
+// the stream, ahead of the step's kernels; never inside a capture, so the
+// captured step reads whatever plan is current when it is replayed).
+int upload_plan(mdff_ctx* ctx) {
+    const PredPlan pl = pred_plan(ctx);
+    if (ctx->coef_valid && std::memcmp(&pl, &ctx->coef_up, sizeof pl) == 0) return MDFF_OK;
+    if (ctx->capturing) return fail(ctx, MDFF_E_STATE, "predictor plan changed inside a captured step");
+    ctx->coef_up = pl;
+    ctx->coef_valid = true;
+    for (int k = 0; k < 16; ++k) ctx->plan_host[k] = pl.coef[k];
+    ctx->plan_host[16] = pl.mode;
+    ctx->plan_host[17] = pl.npt;
+    ctx->plan_host[18] = pl.shift_from;
+    CK(cudaMemcpyAsync(ctx->coef, ctx->plan_host, sizeof(double) * PLAN_LEN, cudaMemcpyHostToDevice, ctx->st));
+    return MDFF_OK;
+}
+
+// Extrapolated initial guess from the stored history, then the history
+// shifted down by the plan's slot count.
 int predict(mdff_ctx* ctx, double* x) {
     const int n3 = 3 * ctx->n;
-    const PredPlan pl = pred_plan(ctx);
-    if (!ctx->coef_valid || std::memcmp(pl.coef, ctx->coef_up.coef, sizeof pl.coef) != 0) {
-        if (ctx->capturing) return fail(ctx, MDFF_E_STATE, "predictor coefficients changed inside a captured step");
-        ctx->coef_up = pl;
-        ctx->coef_valid = true;
-        CK(cudaMemcpyAsync(ctx->coef, ctx->coef_up.coef, sizeof(pl.coef), cudaMemcpyHostToDevice, ctx->st));
-    }
-    const int mode = pl.mode, npt = pl.npt, shift_from = pl.shift_from;
+    TRY(upload_plan(ctx));
     ctx->prof.begin(PK_SOLVER);
-    k_extrapolate<<<nb(n3), 256, 0, ctx->st>>>(n3, mode, npt, ctx->hist, ctx->coef, x);
-    ctx->prof.end(1);
-    for (int k = shift_from; k >= 1; --k)
-        CK(cudaMemcpyAsync(ctx->hist + (size_t)k * n3, ctx->hist + (size_t)(k - 1) * n3, sizeof(double) * n3,
-                           cudaMemcpyDeviceToDevice, ctx->st));
+    k_extrapolate<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->hist, ctx->coef, x);
+    k_hist_shift<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->hist, ctx->coef);
+    ctx->prof.end(2);
     return check_launch(ctx, "predict");
 }
 
@@ -1441,11 +1449,7 @@ bool graph_eligible(const mdff_ctx* ctx) {
     if (p.integrator == MDFF_NPT_NHCNP) return false;
     if (!p.lvnlist || !ctx->have_list || !ctx->forces_valid) return false;
     if (p.autotune && !ctx->tuned) return false;
-    if (p.lcoulomb && ctx->npol > 0) {
-        if (p.algo_moment_from_pola != MDFF_POLA_PCG) return false;
-        const PredPlan pl = pred_plan(ctx);
-        if (!ctx->coef_valid || std::memcmp(pl.coef, ctx->coef_up.coef, sizeof pl.coef) != 0) return false;
-    }
+    if (p.lcoulomb && ctx->npol > 0 && p.algo_moment_from_pola != MDFF_POLA_PCG) return false;
     if (p.lcoulomb && p.precision == MDFF_PREC_MIXED &&
         (!ctx->ddcnt || !ctx->ddrec || (size_t)ctx->n * coul_list(ctx).cap > ctx->ddtab_cap))
         return false;
@@ -1462,10 +1466,7 @@ StepKey step_key(const mdff_ctx* ctx) {
     k.cell = ctx->cell;
     k.g_dir = ctx->g_dir; k.g_dd = ctx->g_dd; k.p_mul = ctx->rs.p_mul; k.s_mul = ctx->rs.s_mul;
     k.efg = (ctx->p.doefg && ctx->efg_due) ? 1 : 0;
-    if (ctx->p.lcoulomb && ctx->npol > 0) {
-        const PredPlan pl = pred_plan(ctx);
-        k.pmode = pl.mode; k.pnpt = pl.npt; k.pshift = pl.shift_from;
-    }
+    // the predictor's plan is device data (upload_plan), not part of the key
     k.skin = skin_allowance(ctx);
     k.n = ctx->n;
     return k;
@@ -1524,6 +1525,7 @@ int capture_step(mdff_ctx* ctx, int slot, const StepKey& key) {
 }
 
 int md_step_graph(mdff_ctx* ctx) {
+    if (ctx->p.lcoulomb && ctx->npol > 0) TRY(upload_plan(ctx));
     const StepKey key = step_key(ctx);
     const int slot = key.efg;
     if (!ctx->gexec[slot] || std::memcmp(&key, &ctx->gkey[slot], sizeof key) != 0) {
@@ -2955,7 +2957,7 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
     TRY(dalloc(ctx, &ctx->efg, 6 * (size_t)n));
     ctx->nhist = p.extrapolate_order + 1;
     TRY(dalloc(ctx, &ctx->hist, (size_t)ctx->nhist * 3 * n));
-    TRY(dalloc(ctx, &ctx->coef, 16));
+    TRY(dalloc(ctx, &ctx->coef, PLAN_LEN));
     TRY(dalloc(ctx, &ctx->type, n));
     TRY(dalloc(ctx, &ctx->pc, NT * NT));
     TRY(dalloc(ctx, &ctx->dsc, 1));

@@ -189,10 +189,16 @@ __global__ void k_coul_sums(int n, const double* __restrict__ q, const double* _
 // mode 0: x = sum_k coef[k] hist[k]   (polynomial of order <= 1 and ASPC predictor)
 // mode 1: Neville interpolation polint (src/field.f90:3995-4042) at x = 1 from
 //         npt points at xa = 0, -1, -2, ...
-__global__ void k_extrapolate(int n3, int mode, int npt, const double* __restrict__ hist, const double* __restrict__ coef,
-                              double* x) {
+// The predictor's plan lives in device memory (plan[0..15] the
+// coefficients, plan[16] the mode, plan[17] the point count, plan[18] the
+// history slots to shift), so one captured step serves every plan.
+constexpr int PLAN_LEN = 19;
+
+__global__ void k_extrapolate(int n3, const double* __restrict__ hist, const double* __restrict__ plan, double* x) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n3) return;
+    const double* coef = plan;
+    const int mode = (int)plan[16], npt = (int)plan[17];
     if (mode == 0) {
         double s = 0.0;
         for (int k = 0; k < npt; ++k) s += coef[k] * hist[(size_t)k * n3 + t];
@@ -223,6 +229,14 @@ __global__ void k_extrapolate(int n3, int mode, int npt, const double* __restric
         y = y + dy;
     }
     x[t] = y;
+}
+
+// history slot k <- slot k - 1 for k = plan[18] .. 1 (slot 0 is the newest)
+__global__ void k_hist_shift(int n3, double* hist, const double* __restrict__ plan) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    const int s = (int)plan[18];
+    for (int k = s; k >= 1; --k) hist[(size_t)k * n3 + t] = hist[(size_t)(k - 1) * n3 + t];
 }
 
 }  // namespace mdff

@@ -552,15 +552,19 @@ void dd_field_real(mdff_ctx* ctx, const double* m, double* out) {
     ctx->prof.end(1);
 }
 
-int induced_field(mdff_ctx* ctx, const double* m, double* out) {
+// self = false leaves out the self term 2 selfa2 m (the PCG iteration adds
+// it in k_cg_apply).
+int induced_field(mdff_ctx* ctx, const double* m, double* out, bool self = true) {
     const int n = ctx->n;
     dd_field_real(ctx, m, out);
     RecFlags rf{0, 1, 1, 0, 0, 0, ctx->p.precision, 0};
     launch_ewald_rec(ctx->st, n, ctx->sx, ctx->sy, ctx->sz, nullptr, m, ctx->cell, ctx->kg, rf, ctx->rs, out, nullptr,
                      nullptr, ctx->part, ctx->dsc, &ctx->prof);
-    ctx->prof.begin(PK_SOLVER);
-    k_axpy<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, 2.0 * selfa2(ctx), m, out);
-    ctx->prof.end(1);
+    if (self) {
+        ctx->prof.begin(PK_SOLVER);
+        k_axpy<<<nb(3 * n), 256, 0, ctx->st>>>(3 * n, 2.0 * selfa2(ctx), m, out);
+        ctx->prof.end(1);
+    }
     return check_launch(ctx, "induced_field");
 }
 
@@ -771,20 +775,25 @@ int solve_dipoles(mdff_ctx* ctx) {
         launch_reduce_partials(ctx->st, ctx->part.buf, vb, 2, &d->rr, 0);
         k_cg_first<<<1, 32, 0, ctx->st>>>(d, inv_npol);
         ctx->prof.end(4);
-        // one PCG iteration (the body of the loop, on the device)
+        // one PCG iteration (the body of the loop, on the device): the
+        // operator, then k_cg_apply (self term, Ad, d.Ad partials),
+        // k_cg_update2 (x, r, z and the r.r, r.z partials), the structure
+        // factors' step, k_cg_direction2; the caller adds the scalars' update
+        // (k_cg_fin, or k_cg_fincond with the loop test).  The two partial
+        // sets live apart in the scratch so that each kernel reduces the
+        // previous one's while writing its own.
+        double* dpart = ctx->part.buf + 4096;
         auto iteration = [&]() -> int {
-            TRY(induced_field(ctx, ctx->cg_d, ctx->Eind));
+            TRY(induced_field(ctx, ctx->cg_d, ctx->Eind, false));
             ctx->prof.begin(PK_SOLVER);
-            k_apply_A<<<nb(n3), 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->Eind, ctx->inv_alpha, ctx->cg_Ad);
-            launch_dot(ctx->st, n3, ctx->cg_d, ctx->cg_Ad, ctx->part, &d->dAd);
-            k_cg_update<<<vb, 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->cg_Ad, ctx->alpha, ctx->mu_ind, ctx->cg_r, ctx->cg_z,
-                                                 d, ctx->part.buf);
+            k_cg_apply<<<vb, 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->Eind, 2.0 * selfa2(ctx), ctx->inv_alpha, ctx->cg_Ad,
+                                               dpart);
+            k_cg_update2<<<vb, 256, 0, ctx->st>>>(n, ctx->cg_d, ctx->cg_Ad, ctx->alpha, ctx->mu_ind, ctx->cg_r,
+                                                 ctx->cg_z, d, dpart, vb, ctx->part.buf);
             // the same step on the structure factors (before rz advances)
             if (reuse) launch_aks_accumulate(ctx->st, ctx->kg, ctx->rs, d, 0);
-            launch_reduce_partials(ctx->st, ctx->part.buf, vb, 2, &d->rr, 0);
-            k_cg_scalars<<<1, 32, 0, ctx->st>>>(d, inv_npol, p.conv_tol_ind);
-            k_cg_direction<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->cg_z, ctx->cg_d, d);
-            ctx->prof.end(8 + (reuse ? (ctx->rs.low.ncol > 0 ? 2 : 1) : 0));
+            k_cg_direction2<<<nb(n3), 256, 0, ctx->st>>>(n3, ctx->cg_z, ctx->cg_d, d, ctx->part.buf, vb);
+            ctx->prof.end(3 + (reuse ? (ctx->rs.low.ncol > 0 ? 2 : 1) : 0));
             return check_launch(ctx, "pcg iteration");
         };
         if (ctx->capturing) {
@@ -824,7 +833,7 @@ int solve_dipoles(mdff_ctx* ctx) {
             } else {
                 r = iteration();
                 if (r == MDFF_OK) {
-                    k_cg_cond<<<1, 32, 0, ctx->st>>>(d, p.max_scf_pol_iter, p.conv_tol_ind, h);
+                    k_cg_fincond<<<1, 32, 0, ctx->st>>>(d, inv_npol, p.conv_tol_ind, p.max_scf_pol_iter, h);
                     r = check_launch(ctx, "pcg test");
                 }
                 cudaGraph_t out = body;
@@ -845,6 +854,8 @@ int solve_dipoles(mdff_ctx* ctx) {
             while ((iscf < p.max_scf_pol_iter && rmsd > p.conv_tol_ind) || iscf < 1) {
                 iscf++;
                 TRY(iteration());
+                k_cg_fin<<<1, 32, 0, ctx->st>>>(d, inv_npol, p.conv_tol_ind);
+                ctx->prof.launches += 1;
                 TRY(sync_scalars(ctx));
                 rmsd = ctx->hsc->rmsd;
                 if (!std::isfinite(rmsd)) return fail(ctx, MDFF_E_NONFINITE, "non-finite residual in the dipole solve");

@@ -27,21 +27,6 @@ void launch_reduce_partials(cudaStream_t st, const double* buf, int nblocks, int
     k_reduce_partials<<<1, 32 * K, 0, st>>>(buf, nblocks, K, out, accumulate);
 }
 
-constexpr int VB = 256;
-static int vblocks(int n) { int b = (n + VB - 1) / VB; return b > 592 ? 592 : b; }
-
-__global__ void k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double* part) {
-    double v[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] = fma(a[i], b[i], v[0]);
-    block_partials<1>(v, part);
-}
-
-void launch_dot(cudaStream_t st, int n, const double* a, const double* b, Partials& part, double* out) {
-    int nb = vblocks(n);
-    k_dot<<<nb, VB, 0, st>>>(n, a, b, part.buf);
-    launch_reduce_partials(st, part.buf, nb, 1, out, 0);
-}
-
 // Ad = d/alpha - Eind on polarisable atoms, 0 elsewhere (n3 = 3n, component-major).
 __global__ void k_apply_A(int n, const double* __restrict__ d, const double* __restrict__ Eind,
                           const double* __restrict__ inv_alpha, double* Ad) {
@@ -70,12 +55,49 @@ __global__ void k_cg_init(int n, const double* __restrict__ b, const double* __r
     block_partials<2>(v, part);
 }
 
-// x += a d; r -= a Ad; z = alpha r; partial sums of r.r and r.z, with
-// a = rz / dAd read from the device scalars.
-__global__ void k_cg_update(int n, const double* __restrict__ dvec, const double* __restrict__ Ad,
-                            const double* __restrict__ alpha, double* x, double* r, double* z, const DevScalars* sc,
-                            double* part) {
-    const double a = sc->rz / sc->dAd;
+// ---- one PCG iteration in four launches after the operator ------------------
+// The sum k_reduce_partials forms for component k of nblocks partials (lanes
+// stride over the blocks, then the xor tree), computed by one full warp, so
+// a kernel that needs a reduced value forms it itself, bit for bit the same.
+__device__ __forceinline__ double warp_reduce_partials(const double* __restrict__ buf, int nblocks, int K, int k) {
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int b = lane; b < nblocks; b += 32) s += buf[(size_t)b * K + k];
+    return warp_sum(s);
+}
+
+// Ad = d/alpha - (E + 2 selfa2 d) on polarisable atoms, 0 elsewhere, and the
+// partial sums of d.Ad: the operator's self term, k_apply_A and the dot
+// product in one pass (grid-stride, like the solver's other vector kernels).
+__global__ void k_cg_apply(int n, const double* __restrict__ d, const double* __restrict__ E, double two_s,
+                           const double* __restrict__ inv_alpha, double* Ad, double* part) {
+    double v[1] = {0.0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * n; t += gridDim.x * blockDim.x) {
+        const int i = t % n;
+        const double ia = inv_alpha[i], dt = d[t];
+        const double e = fma(two_s, dt, E[t]);
+        const double a = ia != 0.0 ? dt * ia - e : 0.0;
+        Ad[t] = a;
+        v[0] = fma(dt, a, v[0]);
+    }
+    block_partials<1>(v, part);
+}
+
+// k_cg_update with d.Ad reduced from k_cg_apply's partials in each block;
+// block 0 records it in the scalars.
+__global__ void k_cg_update2(int n, const double* __restrict__ dvec, const double* __restrict__ Ad,
+                             const double* __restrict__ alpha, double* x, double* r, double* z, DevScalars* sc,
+                             const double* __restrict__ dpart, int ndpart, double* part) {
+    __shared__ double sh_a;
+    if (threadIdx.x < 32) {
+        const double dAd = warp_reduce_partials(dpart, ndpart, 1, 0);
+        if (threadIdx.x == 0) {
+            sh_a = sc->rz / dAd;
+            if (blockIdx.x == 0) sc->dAd = dAd;
+        }
+    }
+    __syncthreads();
+    const double a = sh_a;
     double v[2] = {0.0, 0.0};
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * n; t += gridDim.x * blockDim.x) {
         int i = t % n;
@@ -91,21 +113,38 @@ __global__ void k_cg_update(int n, const double* __restrict__ dvec, const double
     block_partials<2>(v, part);
 }
 
-// beta = rz_new / rz; rz = rz_new; rmsd = sqrt(r.r / npol).
-__global__ void k_cg_scalars(DevScalars* sc, double inv_npol, double tol) {
-    if (threadIdx.x != 0) return;
-    double rr = sc->rr;     // written by the reduction: rr, rz_new
-    sc->beta_cg = sc->rz_new / sc->rz;
+// d = z + beta d with beta = rz_new / rz, r.r and r.z reduced from
+// k_cg_update2's partials in each block; block 0 records them (rz itself
+// advances in k_cg_fin / k_cg_fincond, after every block has read it).
+__global__ void k_cg_direction2(int n3, const double* __restrict__ z, double* dvec, DevScalars* sc,
+                                const double* __restrict__ upart, int nupart) {
+    __shared__ double sh_b;
+    if (threadIdx.x < 32) {
+        const double rr = warp_reduce_partials(upart, nupart, 2, 0);
+        const double rzn = warp_reduce_partials(upart, nupart, 2, 1);
+        if (threadIdx.x == 0) {
+            sh_b = rzn / sc->rz;
+            if (blockIdx.x == 0) {
+                sc->rr = rr;
+                sc->rz_new = rzn;
+                sc->beta_cg = sh_b;
+            }
+        }
+    }
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n3) dvec[t] = fma(sh_b, dvec[t], z[t]);
+}
+
+// the end of an iteration: rz = rz_new; rmsd = sqrt(r.r / npol); count
+__device__ __forceinline__ void cg_fin(DevScalars* sc, double inv_npol, double tol) {
     sc->rz = sc->rz_new;
-    sc->rmsd = sqrt(rr * inv_npol);
+    sc->rmsd = sqrt(sc->rr * inv_npol);
     sc->converged = sc->rmsd <= tol;
     sc->iter += 1;
 }
-
-__global__ void k_cg_direction(int n3, const double* __restrict__ z, double* dvec, const DevScalars* sc) {
-    const double b = sc->beta_cg;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n3) dvec[t] = fma(b, dvec[t], z[t]);
+__global__ void k_cg_fin(DevScalars* sc, double inv_npol, double tol) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) cg_fin(sc, inv_npol, tol);
 }
 
 // Test of the PCG loop when the MD step runs as a CUDA graph (the condition
@@ -115,6 +154,16 @@ __global__ void k_cg_direction(int n3, const double* __restrict__ z, double* dve
 // The iteration cap makes the loop finite whatever the residuals do.
 __global__ void k_cg_cond(const DevScalars* __restrict__ sc, int max_it, double tol, cudaGraphConditionalHandle h) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double r = sc->rmsd;
+    const int it = sc->iter;
+    const bool go = ((it < max_it && r > tol) || it < 1) && isfinite(r);
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// The last kernel of the loop body: the end of the iteration, then the test.
+__global__ void k_cg_fincond(DevScalars* sc, double inv_npol, double tol, int max_it, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    cg_fin(sc, inv_npol, tol);
     const double r = sc->rmsd;
     const int it = sc->iter;
     const bool go = ((it < max_it && r > tol) || it < 1) && isfinite(r);

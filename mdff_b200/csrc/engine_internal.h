@@ -327,7 +327,6 @@ void launch_ewald_ddtab(cudaStream_t st, int n, const uint32_t* fx, const double
                         const int* cnt, int cap, const float2* tab, uint4* rec, double* ef, int g = 16);
 
 // Solver vector kernels.
-void launch_dot(cudaStream_t st, int n3, const double* a, const double* b, Partials& part, double* out);
 
 // Reduce per-block partials: out[k] = sum_b buf[b*K + k].
 void launch_reduce_partials(cudaStream_t st, const double* buf, int nblocks, int K, double* out, int accumulate);

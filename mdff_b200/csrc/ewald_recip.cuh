@@ -820,7 +820,7 @@ struct RecLaunch {
 // final force evaluation needs no structure-factor pass.
 
 // acc = src (copy), or acc += a src with a = rz / dAd, the step of the
-// current PCG iteration (read before k_cg_scalars advances rz).
+// current PCG iteration (read before the iteration's last kernel advances rz).
 __global__ void k_aks_axpy(int m, const DevScalars* __restrict__ sc, int copy, const double* __restrict__ src,
                            double* __restrict__ acc) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;

@@ -83,8 +83,9 @@ __global__ void k_cg_apply(int n, const double* __restrict__ d, const double* __
     block_partials<1>(v, part);
 }
 
-// k_cg_update with d.Ad reduced from k_cg_apply's partials in each block;
-// block 0 records it in the scalars.
+// x += a d; r -= a Ad; z = alpha r; partial sums of r.r and r.z, with
+// a = rz / dAd and d.Ad reduced from k_cg_apply's partials in each block;
+// block 0 records d.Ad in the scalars.
 __global__ void k_cg_update2(int n, const double* __restrict__ dvec, const double* __restrict__ Ad,
                              const double* __restrict__ alpha, double* x, double* r, double* z, DevScalars* sc,
                              const double* __restrict__ dpart, int ndpart, double* part) {

@@ -279,3 +279,38 @@ def test_fp64_sphere_matches_mixed_set():
     assert rel(res["sphere"]["efg"], res["full"]["efg"]) < 1e-6
     assert rel(res["mixed"]["f"], res["sphere"]["f"]) < 1e-6
     assert abs(res["sphere"]["e"]["u_coul"] - res["full"]["e"]["u_coul"]) < 1e-7 * abs(res["full"]["e"]["u_coul"])
+
+
+def test_mixed_triclinic_cell():
+    """A sheared (triclinic) PIM cell: the tensor-core k-space in 24-bit and
+    32-bit fixed point uses the reciprocal basis B in its column constants
+    and the factorised phases X[nx] Y[ny] Z[nz] of the fractional
+    coordinates, so a non-orthogonal B exercises both.  Mixed (both k sets on
+    the tensor cores) against FP64 on forces, dipoles and EFG to 1e-6, and the
+    32-bit low set against the FP64 low set to 5e-8."""
+    s = systems.mgo_pim(grid=(16, 16, 16), rc=10.0, alpha=0.3, kmax=12, vacancy_frac=0.01, seed=4, jitter=0.08)
+    L = np.diag(s["cell"]).copy()
+    frac = s["pos"] / L
+    cell = np.diag(L)
+    cell[1, 0] = 0.07 * L[1]
+    cell[2, 0] = -0.05 * L[2]
+    cell[2, 1] = 0.04 * L[2]
+    pos = frac @ cell
+    out = {}
+    for key, prec, tc in (("fp64", abi.PREC_FP64, 0), ("low64", abi.PREC_MIXED, 1), ("low32", abi.PREC_MIXED, 2)):
+        p = s["params"]
+        p.precision = prec
+        p.kspace_tc = tc
+        p.doefg = 1
+        p.conv_tol_ind = 1e-10
+        e = mdff_b200.Engine(p, s["itype"], pos, cell)
+        out[key] = e.engforce()
+        if tc == 2:
+            assert e.kspace_mode() == {"main_tc": True, "low_tc": True}
+        e.close()
+    d, a, b = out["fp64"], out["low32"], out["low64"]
+    assert rel(a["f"], d["f"]) < 1e-6
+    assert rel(a["mu"], d["mu"]) < 1e-6
+    assert rel(a["efg"], d["efg"]) < 1e-6
+    assert abs(a["e"]["u_coul"] - d["e"]["u_coul"]) < 1e-6 * abs(d["e"]["u_coul"])
+    assert rel(a["f"], b["f"]) < 5e-8 and rel(a["mu"], b["mu"]) < 5e-8

@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, con
                 double gi = 0.0;
                 if (fl.damp) {
                     const PairConst& P = pc[ti * NT + type[j]];
-                    if (P.ldamp) {
+                    if (P.ldamp && P.dc_i != 0.0) {   // c = 0 gives f = 1 exactly
                         double f1, gd;
                         tt_damp_d(P.db_i, P.dc_i, d, P.dk_i, f1, gd);
                         gi = 1.0 - f1;
@@ -113,9 +113,18 @@ __global__ void __launch_bounds__(256, MODE == 2 ? 3 : 2) k_ewald_dir(int n, con
                 const PairConst& P = pc[ti * NT + tj];
                 if (P.ldamp) {
                     ldamp = true;
-                    double f1, f2;
-                    tt_damp_d(P.db_i, P.dc_i, d, P.dk_i, f1, gdi);
-                    tt_damp_d(P.db_j, P.dc_j, d, P.dk_j, f2, gdj);
+                    // c = 0 gives f = 1 and f' = 0 exactly; identical constants at
+                    // i and j (like-type pairs) give identical values
+                    double f1 = 1.0, f2 = 1.0;
+                    if (P.dc_i != 0.0) tt_damp_d(P.db_i, P.dc_i, d, P.dk_i, f1, gdi);
+                    if (P.dc_j != 0.0) {
+                        if (P.db_j == P.db_i && P.dc_j == P.dc_i && P.dk_j == P.dk_i) {
+                            f2 = f1;
+                            gdj = gdi;
+                        } else {
+                            tt_damp_d(P.db_j, P.dc_j, d, P.dk_j, f2, gdj);
+                        }
+                    }
                     gi = 1.0 - f1;
                     gj = 1.0 - f2;
                 }

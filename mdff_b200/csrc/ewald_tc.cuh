@@ -39,7 +39,7 @@ constexpr int KB = 4 * SA;             // K bytes per operand row per stage
 constexpr int NBUF = 4;                // pipeline depth
 constexpr int NPW = 16;                // producer warps (row x 4-atom chunk per thread)
 constexpr int THREADS = 32 * (NPW + 2);   // + MMA warp + copy warp
-constexpr int LSTRIDE = 160;           // tensor-memory columns per digit level (N <= 160)
+constexpr int LSTRIDE = 160;           // tensor-memory columns per digit level when N > 128 (N <= 160)
 constexpr int A_SLICE = 128 * KB;      // bytes of one A digit slice per stage
 constexpr uint64_t WAIT_NS = 200000000ull;   // 0.2 s: a pipeline wait longer than this is an error
 
@@ -103,9 +103,11 @@ __global__ void k_tc_bimage(int n, int npad, const uint32_t* __restrict__ fx, in
         b[0] = zc;  b[1] = -zs; b[2] = b1r; b[3] = -b1i;
         b[4] = zs;  b[5] = zc;  b[6] = b1i; b[7] = b1r;
     }
+    // the three digit slices side by side along N (rows s N + r), so that
+    // one MMA multiplies an A slice by two B slices at once
     const int blk = a / SA, al = a % SA;
     uint8_t* base = img + (size_t)blk * 3 * N * KB;
-    const uint32_t lbo = (uint32_t)(N / 8) * 128;
+    const uint32_t lbo = (uint32_t)(3 * N / 8) * 128, sstep = (uint32_t)(N / 8) * 128;
 #pragma unroll
     for (int row = 0; row < 2; ++row) {
         const int r = 2 * m + row;
@@ -116,8 +118,8 @@ __global__ void k_tc_bimage(int n, int npad, const uint32_t* __restrict__ fx, in
         umma::slices4(w[0], w[1], w[2], w[3], s1, s2, s3);
         const uint32_t off = (uint32_t)(al >> 2) * lbo + (uint32_t)(r >> 3) * 128 + (r & 7) * 16 + 4 * (al & 3);
         *reinterpret_cast<uint32_t*>(base + off) = s1;
-        *reinterpret_cast<uint32_t*>(base + (uint32_t)N * KB + off) = s2;
-        *reinterpret_cast<uint32_t*>(base + 2u * N * KB + off) = s3;
+        *reinterpret_cast<uint32_t*>(base + sstep + off) = s2;
+        *reinterpret_cast<uint32_t*>(base + 2u * sstep + off) = s3;
     }
 }
 
@@ -249,15 +251,21 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
     } else if (lane == 0) {
-        // ---- MMA issue: per stage 2 K-steps of 32 x 6 digit products
-        const uint32_t idesc = umma::idesc_s8(128, N);
-        const uint32_t lboA = 16 * 128, lboB = (uint32_t)(N / 8) * 128;
+        // ---- MMA issue: per stage 2 K-steps of 32 x the six digit products.
+        // With N <= 128 the levels sit N columns apart and the B slices side
+        // by side, so (A0; B0 B1) -> levels 0-1 and (A1; B0 B1) -> levels 1-2
+        // are single MMAs of width 2N: four MMAs per K-step, A0 read twice,
+        // A1 and A2 once.  Wider N keeps one MMA per product.
+        const bool pair = 2 * N <= 256;
+        const uint32_t ls = pair ? (uint32_t)N : (uint32_t)LSTRIDE;
+        const uint32_t idesc = umma::idesc_s8(128, N), idesc2 = umma::idesc_s8(128, pair ? 2 * N : N);
+        const uint32_t lboA = 16 * 128, lboB = (uint32_t)(3 * N / 8) * 128;
         // a shared-memory descriptor is linear in its address field (address
         // >> 4 in the low 14 bits; every address here is below 256 KB), so
         // each operand's descriptor is one base plus a constant offset
         const uint64_t adesc0 = umma::desc_kmajor(sbase + L.a_off, lboA, 128);
         const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.b_off, lboB, 128);
-        const uint32_t bstep = L.buf_bytes >> 4, bslice = ((uint32_t)N * KB) >> 4;
+        const uint32_t bstep = L.buf_bytes >> 4, bslice = ((uint32_t)(N / 8) * 128) >> 4;
         uint32_t started = 0;
         for (int s = 0; s < nst; ++s) {
             const int b = s % NBUF;
@@ -267,16 +275,25 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint64_t ab = adesc0 + (uint64_t)(b * bstep), bb = bdesc0 + (uint64_t)(b * bstep);
 #pragma unroll
             for (int ks = 0; ks < KB / 32; ++ks) {
+                const uint64_t bk = bb + (uint64_t)((2 * ks * lboB) >> 4);
+                if (pair) {
+                    const uint64_t a0 = ab + (uint64_t)((2 * ks * lboA) >> 4);
+                    umma::mma_s8(tmem, a0, bk, idesc2, started);
+                    umma::mma_s8(tmem + 2 * ls, a0, bk + 2 * bslice, idesc, started);
+                    umma::mma_s8(tmem + ls, a0 + (A_SLICE >> 4), bk, idesc2, 1u);
+                    umma::mma_s8(tmem + 2 * ls, a0 + ((2 * A_SLICE) >> 4), bk, idesc, 1u);
+                    started = 1u;
+                } else {
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
+                    for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int j = 0; j < 3 - i; ++j) {
-                        const int lvl = i + j;
-                        const uint64_t ad = ab + (uint64_t)((i * A_SLICE + 2 * ks * lboA) >> 4);
-                        const uint64_t bd = bb + (uint64_t)(j * bslice + ((2 * ks * lboB) >> 4));
-                        umma::mma_s8(tmem + lvl * LSTRIDE, ad, bd, idesc, (started >> lvl) & 1u);
-                        started |= 1u << lvl;
-                    }
+                        for (int j = 0; j < 3 - i; ++j) {
+                            const int lvl = i + j;
+                            const uint64_t ad = ab + (uint64_t)((i * A_SLICE + 2 * ks * lboA) >> 4);
+                            umma::mma_s8(tmem + lvl * ls, ad, bk + j * bslice, idesc, (started >> lvl) & 1u);
+                            started |= 1u << lvl;
+                        }
+                }
             }
             umma::commit(&empty[b]);
         }
@@ -292,12 +309,13 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int col = li < nsph ? cols[li] : -1;
         const double osc = (double)sigma / ((double)umma::QS * (double)umma::QS);
         const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+        const uint32_t ls = 2 * N <= 256 ? (uint32_t)N : (uint32_t)LSTRIDE;
         for (int j = 0; j < N / 16; ++j) {
             float d2[16], d3[16], d4[16];
             if (nst > 0) {
                 umma::tmem_ld16(lane_base + 16 * j, d2);
-                umma::tmem_ld16(lane_base + LSTRIDE + 16 * j, d3);
-                umma::tmem_ld16(lane_base + 2 * LSTRIDE + 16 * j, d4);
+                umma::tmem_ld16(lane_base + ls + 16 * j, d3);
+                umma::tmem_ld16(lane_base + 2 * ls + 16 * j, d4);
                 umma::tmem_wait_ld();
             }
             if (col < 0 || !ok) continue;
@@ -352,8 +370,7 @@ constexpr int EPW = 8;                   // epilogue warps: 2 per tensor-memory 
 constexpr int NQ = EPW / 4;              // column parts per block (one per epilogue warp of a quarter)
 constexpr int THREADS = 32 * (EPW + 2);  // + MMA warp + copy warp
 constexpr int NBS = 6;                   // B stages (the epilogue holds a stage until it has read its constants)
-constexpr int LVL = 64;                  // tensor-memory columns per digit level
-constexpr int BUFC = 3 * LVL;            // per accumulator buffer (two buffers)
+
 constexpr int NCONST = 16;               // floats of per-column constants
 constexpr uint64_t WAIT_NS = 200000000ull;
 
@@ -362,6 +379,8 @@ struct Cfg {
     static constexpr int CB = NMOM == 2 ? 16 : 8;   // columns per block
     static constexpr int NB = CB * NMOM * 2;        // GEMM N per block
     static constexpr int HC = CB / NQ;              // columns per epilogue warp
+    static constexpr int LV = NB;                   // tensor-memory columns per digit level
+    static constexpr int BUFC = 3 * LV;             // per accumulator buffer (two buffers)
 };
 
 struct FLayout {
@@ -477,11 +496,14 @@ __global__ void k_tcf_bimage(int nsph, const int* __restrict__ cols, int kx, int
             umma::slices4(umma::digits24(__float2int_rn(v[4 * g])), umma::digits24(__float2int_rn(v[4 * g + 1])),
                           umma::digits24(__float2int_rn(v[4 * g + 2])), umma::digits24(__float2int_rn(v[4 * g + 3])),
                           s1[g], s2[g], s3[g]);
-        const uint32_t lbo = (uint32_t)(C::NB / 8) * 128;
+        // the three digit slices side by side along N (rows s NB + n), so
+        // that one MMA multiplies an A slice by several B slices at once
+        const uint32_t lbo = (uint32_t)(3 * C::NB / 8) * 128;
         const uint32_t off = (uint32_t)kc * lbo + (uint32_t)(n >> 3) * 128 + (n & 7) * 16;
+        const uint32_t sstep = (uint32_t)(C::NB / 8) * 128;
         *reinterpret_cast<uint4*>(base + off) = make_uint4(s1[0], s1[1], s1[2], s1[3]);
-        *reinterpret_cast<uint4*>(base + C::NB * KZ + off) = make_uint4(s2[0], s2[1], s2[2], s2[3]);
-        *reinterpret_cast<uint4*>(base + 2 * C::NB * KZ + off) = make_uint4(s3[0], s3[1], s3[2], s3[3]);
+        *reinterpret_cast<uint4*>(base + sstep + off) = make_uint4(s2[0], s2[1], s2[2], s2[3]);
+        *reinterpret_cast<uint4*>(base + 2 * sstep + off) = make_uint4(s3[0], s3[1], s3[2], s3[3]);
     }
     if (t < C::CB) {
         float* k = reinterpret_cast<float*>(base + 3 * C::NB * KZ) + t * NCONST;
@@ -579,15 +601,18 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
     } else if (warp == EPW) {
-        // ---- MMA issue: per column block KZ/32 K-steps x 6 digit products
+        // ---- MMA issue: per column block KZ/32 K-steps x 3 MMAs, A digit i
+        // times B digits 0..2-i (side by side along N) into levels i..2: the
+        // six digit products, each A slice read once per K-step
         if (lane == 0) {
-            const uint32_t idesc = umma::idesc_s8(128, C::NB);
-            const uint32_t lboA = 16 * 128, lboB = (uint32_t)(C::NB / 8) * 128;
+            const uint32_t idesc[3] = {umma::idesc_s8(128, 3 * C::NB), umma::idesc_s8(128, 2 * C::NB),
+                                       umma::idesc_s8(128, C::NB)};
+            const uint32_t lboA = 16 * 128, lboB = (uint32_t)(3 * C::NB / 8) * 128;
             // descriptors as one base per operand plus constant offsets (the
             // address field is linear; every address here is below 256 KB)
             const uint64_t adesc0 = umma::desc_kmajor(sbase + L.a_off, lboA, 128);
             const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.b_off, lboB, 128);
-            const uint32_t aslice = (128u * KZ) >> 4, bslice = ((uint32_t)C::NB * KZ) >> 4;
+            const uint32_t aslice = (128u * KZ) >> 4;
             const uint32_t astep = (2 * lboA) >> 4, bkstep = (2 * lboB) >> 4, bstage = L.stage_bytes >> 4;
             if (f_wait(&ares, 0, err, 2, &abort_)) {
                 for (int q = 0; q < ncb; ++q) {
@@ -598,15 +623,12 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
                     for (int ks = 0; ks < KZ / 32; ++ks) {
 #pragma unroll
-                        for (int i = 0; i < 3; ++i)
-#pragma unroll
-                            for (int j = 0; j < 3 - i; ++j) {
-                                const int lvl = i + j;
-                                const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
-                                const uint64_t bd = bq + (uint64_t)(j * bslice + ks * bkstep);
-                                const uint32_t acc = (ks > 0 || (lvl == 1 && i == 1) || (lvl == 2 && i > 0)) ? 1u : 0u;
-                                umma::mma_s8(tmem + tb * BUFC + lvl * LVL, ad, bd, idesc, acc);
-                            }
+                        for (int i = 0; i < 3; ++i) {
+                            const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
+                            const uint64_t bd = bq + (uint64_t)(ks * bkstep);
+                            const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
+                            umma::mma_s8(tmem + tb * C::BUFC + i * C::LV, ad, bd, idesc[i], acc);
+                        }
                     }
                     umma::commit(&accfull[tb]);
                     umma::commit(&bempty[bs]);
@@ -634,7 +656,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (int lv = 0; lv < 3; ++lv)
 #pragma unroll
                 for (int h = 0; h < (WN + 15) / 16; ++h)
-                    umma::tmem_ld16(lane_base + tb * BUFC + lv * LVL + part * WN + 16 * h, d[lv] + 16 * h);
+                    umma::tmem_ld16(lane_base + tb * C::BUFC + lv * C::LV + part * WN + 16 * h, d[lv] + 16 * h);
             umma::tmem_wait_ld();
             umma::fence_before_sync();
             __syncwarp();

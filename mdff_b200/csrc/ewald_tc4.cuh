@@ -35,7 +35,7 @@ constexpr int MAXIN = 8;               // deepest input pipeline
 constexpr int NA = 4;                  // A-operand buffers
 constexpr int NPW = 16;                // producer warps
 constexpr int THREADS = 32 * (NPW + 2);   // + MMA warp + copy warp
-constexpr int LS = 64;                 // tensor-memory columns per digit level (N <= 64)
+constexpr int LS = 64;                 // N <= LS: the four levels of N columns fit ND * LS
 constexpr int A_SLICE = 128 * KB;
 constexpr int MAX_ATOMS_PER_CTA = 8192;   // S32 headroom: 4 products of 2^14 per K byte at the lowest level
 constexpr uint64_t WAIT_NS = 200000000ull;
@@ -110,9 +110,11 @@ __global__ void k_tc4_bimage(int n, int npad, const uint32_t* __restrict__ fx, i
         b[0] = zc;  b[1] = -zs; b[2] = b1r; b[3] = -b1i;
         b[4] = zs;  b[5] = zc;  b[6] = b1i; b[7] = b1r;
     }
+    // the four digit slices side by side along N (rows d N + r), so that one
+    // MMA multiplies an A slice by all the B slices it pairs with
     const int blk = a / SA, al = a % SA;
     uint8_t* base = img + (size_t)blk * ND * N * KB;
-    const uint32_t lbo = (uint32_t)(N / 8) * 128;
+    const uint32_t lbo = (uint32_t)(ND * N / 8) * 128, sstep = (uint32_t)(N / 8) * 128;
 #pragma unroll
     for (int row = 0; row < 2; ++row) {
         const int r = 2 * m + row;
@@ -123,7 +125,7 @@ __global__ void k_tc4_bimage(int n, int npad, const uint32_t* __restrict__ fx, i
         umma::slices4x4(w[0], w[1], w[2], w[3], s[0], s[1], s[2], s[3]);
         const uint32_t off = (uint32_t)(al >> 2) * lbo + (uint32_t)(r >> 3) * 128 + (r & 7) * 16 + 4 * (al & 3);
 #pragma unroll
-        for (int d = 0; d < ND; ++d) *reinterpret_cast<uint32_t*>(base + (uint32_t)d * N * KB + off) = s[d];
+        for (int d = 0; d < ND; ++d) *reinterpret_cast<uint32_t*>(base + (uint32_t)d * sstep + off) = s[d];
     }
 }
 
@@ -265,13 +267,17 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
     } else if (lane == 0) {
-        // ---- MMA issue: per stage 2 K-steps of 32 x 10 digit products
-        const uint32_t idesc = umma::idesc_s8(128, N);
-        const uint32_t lboA = 16 * 128, lboB = (uint32_t)(N / 8) * 128;
+        // ---- MMA issue: per stage 2 K-steps of 32 x the ten digit products as
+        // four MMAs: A digit i times B digits 0..3-i (side by side along N,
+        // width (4-i) N <= 256) into levels i..3, which sit N columns apart
+        uint32_t idesc[ND];
+#pragma unroll
+        for (int i = 0; i < ND; ++i) idesc[i] = umma::idesc_s8(128, (ND - i) * N);
+        const uint32_t lboA = 16 * 128, lboB = (uint32_t)(ND * N / 8) * 128;
         const uint64_t adesc0 = umma::desc_kmajor(sbase, lboA, 128);
         const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.in_off + L.b_off, lboB, 128);
         const uint32_t astep = L.a_bytes >> 4, instep = L.in_bytes >> 4;
-        const uint32_t aslice = A_SLICE >> 4, bslice = ((uint32_t)N * KB) >> 4;
+        const uint32_t aslice = A_SLICE >> 4;
         for (int s = 0; s < nst; ++s) {
             const int bi = s % nin, ba = s % NA;
             if (!tc_wait(&infull[bi], (s / nin) & 1, err, 4, &stop)) break;
@@ -281,14 +287,12 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
             for (int ks = 0; ks < KB / 32; ++ks)
 #pragma unroll
-                for (int i = 0; i < ND; ++i)
-#pragma unroll
-                    for (int j = 0; j < ND - i; ++j) {
-                        const uint64_t ad = ab + (uint64_t)(i * aslice + ((2 * ks * lboA) >> 4));
-                        const uint64_t bd = bb + (uint64_t)(j * bslice + ((2 * ks * lboB) >> 4));
-                        const uint32_t acc = (s > 0 || ks > 0 || i > 0) ? 1u : 0u;
-                        umma::mma_s8(tmem + (i + j) * LS, ad, bd, idesc, acc);
-                    }
+                for (int i = 0; i < ND; ++i) {
+                    const uint64_t ad = ab + (uint64_t)(i * aslice + ((2 * ks * lboA) >> 4));
+                    const uint64_t bd = bb + (uint64_t)((2 * ks * lboB) >> 4);
+                    const uint32_t acc = (s > 0 || ks > 0 || i > 0) ? 1u : 0u;
+                    umma::mma_s8(tmem + (uint32_t)(i * N), ad, bd, idesc[i], acc);
+                }
             umma::commit(&inempty[bi]);
             umma::commit(&aempty[ba]);
         }
@@ -322,7 +326,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             float d[ND][16];
             if (nst > 0) {
 #pragma unroll
-                for (int l = 0; l < ND; ++l) umma::tmem_ld16(lane_base + l * LS + 16 * j, d[l]);
+                for (int l = 0; l < ND; ++l) umma::tmem_ld16(lane_base + l * N + 16 * j, d[l]);
                 umma::tmem_wait_ld();
             }
             if (!valid || !ok) continue;
@@ -361,8 +365,7 @@ constexpr int EPW = 16;                  // epilogue warps: 4 per tensor-memory 
 constexpr int NQ = EPW / 4;
 constexpr int FTHREADS = 32 * (EPW + 2);
 constexpr int NBS = 4;                   // B stages
-constexpr int LVL = 64;                  // tensor-memory columns per digit level
-constexpr int BUFC = ND * LVL;           // per accumulator buffer (two buffers: all 512 columns)
+constexpr int TMEM_COLS = 512;           // two accumulator buffers of ND levels of NB columns
 constexpr int NCONST = 16;               // doubles of per-column constants
 
 template <int NMOM>
@@ -371,6 +374,8 @@ struct Cfg {
     static constexpr int NB = CB * NMOM * 2;        // GEMM N per block (64 or 48)
     static constexpr int HC = CB / NQ;              // columns per epilogue warp
     static constexpr int WN = HC * NMOM * 2;        // accumulator columns per warp per level (16 or 12)
+    static constexpr int BUFC = ND * NB;            // per accumulator buffer (levels NB columns apart)
+    static_assert(2 * BUFC <= TMEM_COLS, "two accumulator buffers");
 };
 
 struct FLayout {
@@ -487,11 +492,12 @@ __global__ void k_tc4f_bimage(int ncol, const int* __restrict__ cols, int nzmax,
             umma::slices4x4(umma::digits32(__double2int_rn(v[4 * g])), umma::digits32(__double2int_rn(v[4 * g + 1])),
                             umma::digits32(__double2int_rn(v[4 * g + 2])),
                             umma::digits32(__double2int_rn(v[4 * g + 3])), s[0][g], s[1][g], s[2][g], s[3][g]);
-        const uint32_t lbo = (uint32_t)(C::NB / 8) * 128;
+        // the four digit slices side by side along N (rows d NB + n)
+        const uint32_t lbo = (uint32_t)(ND * C::NB / 8) * 128, sstep = (uint32_t)(C::NB / 8) * 128;
         const uint32_t off = (uint32_t)kc * lbo + (uint32_t)(n >> 3) * 128 + (n & 7) * 16;
 #pragma unroll
         for (int d = 0; d < ND; ++d)
-            *reinterpret_cast<uint4*>(base + (size_t)d * C::NB * KZ + off) = make_uint4(s[d][0], s[d][1], s[d][2], s[d][3]);
+            *reinterpret_cast<uint4*>(base + d * sstep + off) = make_uint4(s[d][0], s[d][1], s[d][2], s[d][3]);
     }
     if (t < C::CB) {
         double* k = reinterpret_cast<double*>(base + (size_t)ND * C::NB * KZ) + t * NCONST;
@@ -562,7 +568,7 @@ __global__ void __launch_bounds__(FTHREADS, 1)
         abort_ = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) umma::tmem_alloc(&tslot, 2 * BUFC);
+    if (warp == 0) umma::tmem_alloc(&tslot, TMEM_COLS);
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
@@ -584,13 +590,17 @@ __global__ void __launch_bounds__(FTHREADS, 1)
             }
         }
     } else if (warp == EPW) {
-        // ---- MMA issue: per column block KZ/32 K-steps x 10 digit products
+        // ---- MMA issue: per column block KZ/32 K-steps x 4 MMAs, A digit i
+        // times B digits 0..3-i (side by side along N) into levels i..3: the
+        // ten digit products, each A slice read once per K-step
         if (lane == 0) {
-            const uint32_t idesc = umma::idesc_s8(128, C::NB);
-            const uint32_t lboA = 16 * 128, lboB = (uint32_t)(C::NB / 8) * 128;
+            uint32_t idesc[ND];
+#pragma unroll
+            for (int i = 0; i < ND; ++i) idesc[i] = umma::idesc_s8(128, (ND - i) * C::NB);
+            const uint32_t lboA = 16 * 128, lboB = (uint32_t)(ND * C::NB / 8) * 128;
             const uint64_t adesc0 = umma::desc_kmajor(sbase + L.a_off, lboA, 128);
             const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.b_off, lboB, 128);
-            const uint32_t aslice = (128u * KZ) >> 4, bslice = ((uint32_t)C::NB * KZ) >> 4;
+            const uint32_t aslice = (128u * KZ) >> 4;
             const uint32_t astep = (2 * lboA) >> 4, bkstep = (2 * lboB) >> 4, bstage = L.stage_bytes >> 4;
             if (tc_wait(&ares, 0, err, 2, &abort_)) {
                 for (int q = 0; q < ncb; ++q) {
@@ -601,14 +611,12 @@ __global__ void __launch_bounds__(FTHREADS, 1)
                     const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
                     for (int ks = 0; ks < KZ / 32; ++ks) {
 #pragma unroll
-                        for (int i = 0; i < ND; ++i)
-#pragma unroll
-                            for (int j = 0; j < ND - i; ++j) {
-                                const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
-                                const uint64_t bd = bq + (uint64_t)(j * bslice + ks * bkstep);
-                                const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
-                                umma::mma_s8(tmem + tb * BUFC + (i + j) * LVL, ad, bd, idesc, acc);
-                            }
+                        for (int i = 0; i < ND; ++i) {
+                            const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
+                            const uint64_t bd = bq + (uint64_t)(ks * bkstep);
+                            const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
+                            umma::mma_s8(tmem + tb * C::BUFC + i * C::NB, ad, bd, idesc[i], acc);
+                        }
                     }
                     umma::commit(&accfull[tb]);
                     umma::commit(&bempty[bs]);
@@ -634,7 +642,7 @@ __global__ void __launch_bounds__(FTHREADS, 1)
             float d[ND][WN];
 #pragma unroll
             for (int lv = 0; lv < ND; ++lv) {
-                const uint32_t ta = lane_base + tb * BUFC + lv * LVL + part * WN;
+                const uint32_t ta = lane_base + tb * C::BUFC + lv * C::NB + part * WN;
                 if (WN == 16) {
                     umma::tmem_ld16(ta, d[lv]);
                 } else {
@@ -698,7 +706,7 @@ __global__ void __launch_bounds__(FTHREADS, 1)
     __syncthreads();
     if (warp == 0) {
         umma::fence_after_sync();
-        umma::tmem_dealloc(tmem, 2 * BUFC);
+        umma::tmem_dealloc(tmem, TMEM_COLS);
     }
 }
 

@@ -218,7 +218,8 @@ typedef struct mdff_opt_result {
     int    status;      /* 0: minimum reached (sastry: energy unchanged to ftol; lbfgs: |G| / max(1, |X|)
                            <= eps); 1: itmax iterations (sastry) or force evaluations (lbfgs);
                            2: zero gradient; 3: the line search failed (sastry: no progress in 100
-                           steps; lbfgs: MCSRCH returned info != 1, IFLAG = -1) */
+                           steps, or U still above the line's start after 64 halvings of a trial
+                           step; lbfgs: MCSRCH returned info != 1, IFLAG = -1) */
     int    info;        /* lbfgs with status 3: MCSRCH's info (0 not a descent direction or bad
                            input, 2 interval below xtol, 3 maxfev reached, 4/5 at stpmin/stpmax,
                            6 rounding errors), 0 otherwise; m1qn3: its omode; sastry: 0 */

@@ -1649,6 +1649,23 @@ int opt_accept(mdff_ctx* ctx, double x) {
     return MDFF_OK;
 }
 
+// The reference halves a trial step without bound while U stays above the
+// line's starting value ukeep (labels 524, 525).  After OPT_MAX_HALVINGS
+// halvings the step is x0 to the last bit, so a U still above ukeep comes from
+// the rounding of repeated evaluations at one point (the induced dipoles start
+// from the previous solution); the minimisation then ends at x0 with status 3,
+// as the 100-step limit ends it.
+constexpr int OPT_MAX_HALVINGS = 64;
+
+int opt_stalled(mdff_ctx* ctx, mdff_opt_result* R, double x0, double u0, double phigrad, int neng) {
+    TRY(opt_accept(ctx, x0));
+    R->u_final = u0;
+    R->phigrad = phigrad;
+    R->nforce = neng;
+    R->status = 3;
+    return MDFF_OK;
+}
+
 int opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* R) {
     const int n = ctx->n;
     if (!ctx->opt_xi) {
@@ -1714,9 +1731,13 @@ int opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* R) {
                 const double curv1 = uppcub + u3pcub * x1sol, curv2 = uppcub + u3pcub * x2sol;
                 if (curv1 > 0.0) xsol = x1sol + x0;
                 if (curv2 > 0.0) xsol = x2sol + x0;
-                for (;;) {   // label 524: keep u2 below ukeep
+                for (int nh = 0;; ++nh) {   // label 524: keep u2 below ukeep
                     TRY(opt_eforce1d(ctx, xsol, u2, f1ds, neng));
-                    if (u2 > ukeep) { xsol = x0 + (xsol - x0) / 2.0; continue; }
+                    if (u2 > ukeep) {
+                        if (nh == OPT_MAX_HALVINGS) return opt_stalled(ctx, R, x0, u0, phigrad, neng);
+                        xsol = x0 + (xsol - x0) / 2.0;
+                        continue;
+                    }
                     break;
                 }
                 if (std::fabs((uprev - u2) / u2) < dutol) {
@@ -1736,9 +1757,13 @@ int opt_sastry(mdff_ctx* ctx, int itmax, mdff_opt_result* R) {
                 } else {
                     xsol = x0 + 1.50 * adx;
                 }
-                for (;;) {   // label 525
+                for (int nh = 0;; ++nh) {   // label 525
                     TRY(opt_eforce1d(ctx, xsol, u2, f1ds, neng));
-                    if (u2 > ukeep) { xsol = x0 + (xsol - x0) / 2.0; continue; }
+                    if (u2 > ukeep) {
+                        if (nh == OPT_MAX_HALVINGS) return opt_stalled(ctx, R, x0, u0, phigrad, neng);
+                        xsol = x0 + (xsol - x0) / 2.0;
+                        continue;
+                    }
                     break;
                 }
                 if (std::fabs((uprev - u2) / u2) < dutol) {

@@ -601,10 +601,11 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
     } else if (warp == EPW) {
-        // ---- MMA issue: per column block KZ/32 K-steps x 3 MMAs, A digit i
-        // times B digits 0..2-i (side by side along N) into levels i..2: the
-        // six digit products, each A slice read once per K-step
-        if (lane == 0) {
+        // ---- MMA issue (the whole warp, one elected lane issues): per column
+        // block KZ/32 K-steps x 3 MMAs, A digit i times B digits 0..2-i (side
+        // by side along N) into levels i..2: the six digit products, each A
+        // slice read once per K-step
+        {
             const uint32_t idesc[3] = {umma::idesc_s8(128, 3 * C::NB), umma::idesc_s8(128, 2 * C::NB),
                                        umma::idesc_s8(128, C::NB)};
             const uint32_t lboA = 16 * 128, lboB = (uint32_t)(3 * C::NB / 8) * 128;
@@ -614,27 +615,27 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.b_off, lboB, 128);
             const uint32_t aslice = (128u * KZ) >> 4;
             const uint32_t astep = (2 * lboA) >> 4, bkstep = (2 * lboB) >> 4, bstage = L.stage_bytes >> 4;
-            if (f_wait(&ares, 0, err, 2, &abort_)) {
-                for (int q = 0; q < ncb; ++q) {
-                    const int bs = q % NBS, tb = q & 1;
-                    if (!f_wait(&bfull[bs], (q / NBS) & 1, err, 4, &abort_)) break;
-                    if (q >= 2 && !f_wait(&accfree[tb], ((q >> 1) - 1) & 1, err, 8, &abort_)) break;
-                    umma::fence_after_sync();
-                    const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
-                    for (int ks = 0; ks < KZ / 32; ++ks) {
+            bool ok = __all_sync(0xffffffffu, f_wait(&ares, 0, err, 2, &abort_));
+            for (int q = 0; q < ncb && ok; ++q) {
+                const int bs = q % NBS, tb = q & 1;
+                ok = __all_sync(0xffffffffu, f_wait(&bfull[bs], (q / NBS) & 1, err, 4, &abort_));
+                if (ok && q >= 2) ok = __all_sync(0xffffffffu, f_wait(&accfree[tb], ((q >> 1) - 1) & 1, err, 8, &abort_));
+                if (!ok) break;
+                umma::fence_after_sync();
+                const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
+                for (int ks = 0; ks < KZ / 32; ++ks) {
 #pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
-                            const uint64_t bd = bq + (uint64_t)(ks * bkstep);
-                            const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
-                            umma::mma_s8(tmem + tb * C::BUFC + i * C::LV, ad, bd, idesc[i], acc);
-                        }
+                    for (int i = 0; i < 3; ++i) {
+                        const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
+                        const uint64_t bd = bq + (uint64_t)(ks * bkstep);
+                        const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
+                        umma::mma_s8_warp(tmem + tb * C::BUFC + i * C::LV, ad, bd, idesc[i], acc);
                     }
-                    umma::commit(&accfull[tb]);
-                    umma::commit(&bempty[bs]);
                 }
+                umma::commit_warp(&accfull[tb]);
+                umma::commit_warp(&bempty[bs]);
             }
-            umma::commit(&fin);
+            umma::commit_warp(&fin);
         }
     } else {
         // ---- epilogue: atom row = 32 (warp % 4) + lane, column part = warp / 4

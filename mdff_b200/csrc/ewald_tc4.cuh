@@ -590,10 +590,11 @@ __global__ void __launch_bounds__(FTHREADS, 1)
             }
         }
     } else if (warp == EPW) {
-        // ---- MMA issue: per column block KZ/32 K-steps x 4 MMAs, A digit i
-        // times B digits 0..3-i (side by side along N) into levels i..3: the
-        // ten digit products, each A slice read once per K-step
-        if (lane == 0) {
+        // ---- MMA issue (the whole warp, one elected lane issues): per column
+        // block KZ/32 K-steps x 4 MMAs, A digit i times B digits 0..3-i (side
+        // by side along N) into levels i..3: the ten digit products, each A
+        // slice read once per K-step
+        {
             uint32_t idesc[ND];
 #pragma unroll
             for (int i = 0; i < ND; ++i) idesc[i] = umma::idesc_s8(128, (ND - i) * C::NB);
@@ -602,27 +603,27 @@ __global__ void __launch_bounds__(FTHREADS, 1)
             const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.b_off, lboB, 128);
             const uint32_t aslice = (128u * KZ) >> 4;
             const uint32_t astep = (2 * lboA) >> 4, bkstep = (2 * lboB) >> 4, bstage = L.stage_bytes >> 4;
-            if (tc_wait(&ares, 0, err, 2, &abort_)) {
-                for (int q = 0; q < ncb; ++q) {
-                    const int bs = q % NBS, tb = q & 1;
-                    if (!tc_wait(&bfull[bs], (q / NBS) & 1, err, 4, &abort_)) break;
-                    if (q >= 2 && !tc_wait(&accfree[tb], ((q >> 1) - 1) & 1, err, 8, &abort_)) break;
-                    umma::fence_after_sync();
-                    const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
-                    for (int ks = 0; ks < KZ / 32; ++ks) {
+            bool ok = __all_sync(0xffffffffu, tc_wait(&ares, 0, err, 2, &abort_));
+            for (int q = 0; q < ncb && ok; ++q) {
+                const int bs = q % NBS, tb = q & 1;
+                ok = __all_sync(0xffffffffu, tc_wait(&bfull[bs], (q / NBS) & 1, err, 4, &abort_));
+                if (ok && q >= 2) ok = __all_sync(0xffffffffu, tc_wait(&accfree[tb], ((q >> 1) - 1) & 1, err, 8, &abort_));
+                if (!ok) break;
+                umma::fence_after_sync();
+                const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
+                for (int ks = 0; ks < KZ / 32; ++ks) {
 #pragma unroll
-                        for (int i = 0; i < ND; ++i) {
-                            const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
-                            const uint64_t bd = bq + (uint64_t)(ks * bkstep);
-                            const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
-                            umma::mma_s8(tmem + tb * C::BUFC + i * C::NB, ad, bd, idesc[i], acc);
-                        }
+                    for (int i = 0; i < ND; ++i) {
+                        const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
+                        const uint64_t bd = bq + (uint64_t)(ks * bkstep);
+                        const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
+                        umma::mma_s8_warp(tmem + tb * C::BUFC + i * C::NB, ad, bd, idesc[i], acc);
                     }
-                    umma::commit(&accfull[tb]);
-                    umma::commit(&bempty[bs]);
                 }
+                umma::commit_warp(&accfull[tb]);
+                umma::commit_warp(&bempty[bs]);
             }
-            umma::commit(&fin);
+            umma::commit_warp(&fin);
         }
     } else {
         // ---- epilogue: atom row = 32 (warp % 4) + lane, column quarter = warp / 4

@@ -73,6 +73,27 @@ __device__ __forceinline__ void commit(uint64_t* mbar) {
                  : "memory");
 }
 
+// The same two, called by a whole converged warp with warp-uniform operands;
+// one elected lane issues.  Beside warps doing FP32 work on the same
+// scheduler, a single issuing thread in a divergent branch is starved of issue
+// slots (every MMA needs its operands moved to uniform registers first) and
+// the tensor pipe idles between its MMAs; a warp-uniform loop keeps the
+// descriptors in uniform registers and needs a few issue slots per MMA.
+__device__ __forceinline__ void mma_s8_warp(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred e, p;\n\telect.sync _|e, 0xffffffff;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "@e tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void commit_warp(uint64_t* mbar) {
+    asm volatile(
+        "{\n\t.reg .pred e;\n\telect.sync _|e, 0xffffffff;\n\t"
+        "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n" ::"r"(smem_u32(mbar))
+        : "memory");
+}
+
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 // generic-proxy shared-memory writes become visible to the tensor core

@@ -1915,6 +1915,11 @@ static void opt_eforce1d(orc_sys* s, double x, double& pot, double& f1d, const s
     f1d = -f1d;
 }
 
+// The reference halves a trial step without bound while U stays above ukeep
+// (labels 524, 525); after OPT_MAX_HALVINGS halvings the step is x0 to the
+// last bit, and the minimisation ends at x0 with status 3 (as the engine).
+constexpr int OPT_MAX_HALVINGS = 64;
+
 static int opt_sastry(orc_sys* s, int itmax, mdff_opt_result* R) {
     const int n = s->natm;
     std::vector<double> gx(n), gy(n), gz(n), hx(n), hy(n), hz(n), xix(n), xiy(n), xiz(n);
@@ -1966,6 +1971,11 @@ static int opt_sastry(orc_sys* s, int itmax, mdff_opt_result* R) {
             ukeep = u_tot; x0 = 0.0; u0 = u_tot; f1_dp = fdotxi();
         }
         double x1 = ds, u1, f1d1, u2 = 0.0, f1ds = 0.0;
+        auto stalled = [&]() {
+            move(x0);
+            R->u_final = u0; R->phigrad = phigrad; R->nforce = neng; R->status = 3;
+            return 0;
+        };
         opt_eforce1d(s, x1, u1, f1d1, xix, xiy, xiz, neng);
         int nstep = 0;
         double uprev = std::min(u1, u0);
@@ -1998,9 +2008,13 @@ static int opt_sastry(orc_sys* s, int itmax, mdff_opt_result* R) {
                 const double curv1 = uppcub + u3pcub * x1sol, curv2 = uppcub + u3pcub * x2sol;
                 if (curv1 > 0.0) xsol = x1sol + x0;
                 if (curv2 > 0.0) xsol = x2sol + x0;
-                for (;;) {   // label 524: keep u2 below ukeep
+                for (int nh = 0;; ++nh) {   // label 524: keep u2 below ukeep
                     opt_eforce1d(s, xsol, u2, f1ds, xix, xiy, xiz, neng);
-                    if (u2 > ukeep) { xsol = x0 + (xsol - x0) / 2.0; continue; }
+                    if (u2 > ukeep) {
+                        if (nh == OPT_MAX_HALVINGS) return stalled();
+                        xsol = x0 + (xsol - x0) / 2.0;
+                        continue;
+                    }
                     break;
                 }
                 if (std::fabs((uprev - u2) / u2) < dutol) {
@@ -2020,9 +2034,13 @@ static int opt_sastry(orc_sys* s, int itmax, mdff_opt_result* R) {
                 } else {
                     xsol = x0 + 1.50 * adx;
                 }
-                for (;;) {   // label 525
+                for (int nh = 0;; ++nh) {   // label 525
                     opt_eforce1d(s, xsol, u2, f1ds, xix, xiy, xiz, neng);
-                    if (u2 > ukeep) { xsol = x0 + (xsol - x0) / 2.0; continue; }
+                    if (u2 > ukeep) {
+                        if (nh == OPT_MAX_HALVINGS) return stalled();
+                        xsol = x0 + (xsol - x0) / 2.0;
+                        continue;
+                    }
                     break;
                 }
                 if (std::fabs((uprev - u2) / u2) < dutol) {

@@ -3000,6 +3000,7 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
     TRY(dalloc(ctx, &ctx->d_overflow, 1));
     TRY(dalloc(ctx, &ctx->grid.cell_of, n));
     TRY(dalloc(ctx, &ctx->grid.cell_atoms, n));
+    TRY(dalloc(ctx, &ctx->grid.cell_w, n));
     CK(cudaMemsetAsync(ctx->dsc, 0, sizeof(DevScalars), ctx->st));
     CK(cudaMemsetAsync(ctx->hist, 0, sizeof(double) * ctx->nhist * 3 * (size_t)n, ctx->st));
     CK(cudaMemsetAsync(ctx->mu_ind, 0, sizeof(double) * 3 * (size_t)n, ctx->st));

@@ -177,6 +177,7 @@ struct CellGrid {
     int* cell_start = nullptr;  // [ncell+1]
     int* cell_cursor = nullptr; // [ncell]
     int* cell_atoms = nullptr;  // [n]
+    float4* cell_w = nullptr;   // [n] cell order: FP32 wrapped fractional coordinates, atom index as bits
     int ncell_alloc = 0;
 };
 void launch_bin(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, CellGrid& g);

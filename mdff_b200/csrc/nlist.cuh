@@ -140,75 +140,156 @@ __global__ void k_sort_cells(int ncell, const int* __restrict__ start, int* atom
     }
 }
 
+// The list kernel's prefilter input, in cell order: the wrapped fractional
+// coordinates s - floor(s) rounded to FP32, and the atom index as bits, so a
+// warp reads 32 candidates with one coalesced 16-byte load each.
+__global__ void k_cell_coords(int n, const double* __restrict__ sx, const double* __restrict__ sy,
+                              const double* __restrict__ sz, const int* __restrict__ cell_atoms, float4* cw) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int j = cell_atoms[k];
+    const double a = sx[j], b = sy[j], c = sz[j];
+    cw[k] = make_float4((float)(a - floor(a)), (float)(b - floor(b)), (float)(c - floor(c)), __int_as_float(j));
+}
+
 void launch_bin(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, CellGrid& g) {
     cudaMemsetAsync(g.cell_count, 0, sizeof(int) * g.ncell, st);
     k_bin_count<<<(n + 255) / 256, 256, 0, st>>>(n, sx, sy, sz, g.nc[0], g.nc[1], g.nc[2], g.cell_of, g.cell_count);
     k_scan<<<1, 1024, 0, st>>>(g.ncell, g.cell_count, g.cell_start, g.cell_cursor);
     k_bin_fill<<<(n + 255) / 256, 256, 0, st>>>(n, g.cell_of, g.cell_cursor, g.cell_atoms);
     k_sort_cells<<<g.ncell, 128, 0, st>>>(g.ncell, g.cell_start, g.cell_atoms);
+    k_cell_coords<<<(n + 255) / 256, 256, 0, st>>>(n, sx, sy, sz, g.cell_atoms, g.cell_w);
 }
 
 // ------------------------------------------------------------ list build --
 // One warp per atom i.  The neighbouring cells are visited in a fixed order;
 // along a direction with fewer than three cells every cell is visited once
-// (no duplicates).  Candidates j are tested 32 at a time and the hits are
-// compacted with a ballot.  Row overflow sets *overflow and stops writing (the
-// host grows the capacity and rebuilds).
-__global__ void k_nlist(int n, const double* __restrict__ sx, const double* __restrict__ sy,
-                        const double* __restrict__ sz, CellP c, const int* __restrict__ cell_of,
-                        const int* __restrict__ cell_start, const int* __restrict__ cell_atoms,
-                        int nc0, int nc1, int nc2, double rsq_a, int* nbr_a, int* cnt_a, int cap_a,
-                        double rsq_b, int* nbr_b, int* cnt_b, int cap_b, int* overflow) {
+// (no duplicates).  Candidates j are read 32 at a time from the cell-ordered
+// FP32 copy and prefiltered in FP32: a candidate is dropped only when its
+// FP32 squared distance exceeds thr, the larger list radius squared plus a
+// margin that bounds the FP32 error (set by the host from the cell), so no
+// pair inside either radius is ever dropped.  The survivors (about an eighth)
+// queue up per warp in shared memory in candidate order and are decided 32 at
+// a time by the reference's FP64 expression (pairvec_exact) with full warps;
+// the hits are compacted with a ballot, so each row holds the same atoms in
+// the same order as an all-FP64 scan.  A fractional offset within 1e-4 of
+// +-1/2 (where FP32 and FP64 may pick different periodic images in a skewed
+// cell) always goes to the exact test.  Row overflow sets *overflow and stops
+// writing (the host grows the capacity and rebuilds).
+constexpr int NL_THREADS = 256;
+constexpr int NL_QUEUE = 64;   // per warp: below 32 queued before a chunk adds at most 32
+
+// The prefilter's FP32 cell matrix and threshold, passed by value: kernel
+// parameters live in the constant bank, so the FP32 products read them as
+// operands and nothing is converted inside the candidate loop.
+struct NlPre {
+    float A[9];
+    float thr;
+};
+
+__global__ void __launch_bounds__(NL_THREADS)
+    k_nlist(int n, const double* __restrict__ sx, const double* __restrict__ sy, const double* __restrict__ sz,
+            CellP c, const int* __restrict__ cell_of, const int* __restrict__ cell_start,
+            const float4* __restrict__ cell_w, int nc0, int nc1, int nc2, NlPre pre, double rsq_a, int* nbr_a,
+            int* cnt_a, int cap_a, double rsq_b, int* nbr_b, int* cnt_b, int cap_b, int* overflow) {
+    __shared__ int s_q[NL_THREADS / 32][NL_QUEUE];
     const int lane = threadIdx.x & 31;
+    int* q = s_q[threadIdx.x >> 5];
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= n) return;
     const double si1 = sx[i], si2 = sy[i], si3 = sz[i];
+    float wi1 = (float)(si1 - floor(si1)), wi2 = (float)(si2 - floor(si2)), wi3 = (float)(si3 - floor(si3));
+    // kept in registers: recomputing them from the FP64 coordinates inside the
+    // loop would cost conversions on the quarter-rate XU pipe per candidate
+    asm volatile("" : "+f"(wi1), "+f"(wi2), "+f"(wi3));
+    const float* A = pre.A;
     const int ci = cell_of[i];
     const int cz = ci % nc2, cy = (ci / nc2) % nc1, cx = ci / (nc2 * nc1);
     const int lo0 = nc0 >= 3 ? -1 : 0, hi0 = nc0 >= 3 ? 1 : nc0 - 1;
     const int lo1 = nc1 >= 3 ? -1 : 0, hi1 = nc1 >= 3 ? 1 : nc1 - 1;
     const int lo2 = nc2 >= 3 ? -1 : 0, hi2 = nc2 >= 3 ? 1 : nc2 - 1;
-    int na = 0, nb = 0;
+    int na = 0, nb = 0, nq = 0;
     const unsigned lt = (1u << lane) - 1u;
+    // exact FP64 test of the first cnt (<= 32) queued candidates, hits appended in queue order
+    auto decide = [&](int cnt) {
+        bool in_a = false, in_b = false;
+        int j = -1;
+        if (lane < cnt) {
+            j = q[lane];
+            double rx, ry, rz;
+            const double rsq = pairvec_exact(c, si1, si2, si3, sx[j], sy[j], sz[j], rx, ry, rz);
+            in_a = rsq <= rsq_a;
+            in_b = rsq <= rsq_b;
+        }
+        const unsigned ma = __ballot_sync(0xffffffffu, in_a);
+        if (in_a) {
+            const int pos = na + __popc(ma & lt);
+            if (pos < cap_a) nbr_a[(size_t)i * cap_a + pos] = j;
+        }
+        na += __popc(ma);
+        if (nbr_b) {
+            const unsigned mb = __ballot_sync(0xffffffffu, in_b);
+            if (in_b) {
+                const int pos = nb + __popc(mb & lt);
+                if (pos < cap_b) nbr_b[(size_t)i * cap_b + pos] = j;
+            }
+            nb += __popc(mb);
+        }
+    };
+    // periodic neighbour cell along one direction (offset -1, 0, +1), without
+    // an integer division
+    auto wrap = [](int c0, int off, int nc) {
+        if (nc < 3) return off;
+        const int v = c0 + off;
+        return v < 0 ? v + nc : (v >= nc ? v - nc : v);
+    };
+    // d - rint(d) for d in [-1, 1] by compare and select (rounding instructions
+    // run on the quarter-rate XU pipe); the ties d = +-1/2 are left as they are,
+    // as rint leaves them, and go to the exact test anyway
+    auto fold = [](float d) { return d > 0.5f ? d - 1.0f : (d < -0.5f ? d + 1.0f : d); };
     for (int a = lo0; a <= hi0; ++a) {
-        int x = nc0 >= 3 ? (cx + a + nc0) % nc0 : a;
+        const int x = wrap(cx, a, nc0);
         for (int b = lo1; b <= hi1; ++b) {
-            int y = nc1 >= 3 ? (cy + b + nc1) % nc1 : b;
+            const int y = wrap(cy, b, nc1);
             for (int d = lo2; d <= hi2; ++d) {
-                int z = nc2 >= 3 ? (cz + d + nc2) % nc2 : d;
+                const int z = wrap(cz, d, nc2);
                 int cc = (x * nc1 + y) * nc2 + z;
                 int s0 = cell_start[cc], s1 = cell_start[cc + 1];
                 for (int base = s0; base < s1; base += 32) {
-                    int k = base + lane;
-                    bool in_a = false, in_b = false;
+                    const int k = base + lane;
+                    bool keep = false;
                     int j = -1;
                     if (k < s1) {
-                        j = cell_atoms[k];
+                        const float4 v = cell_w[k];
+                        j = __float_as_int(v.w);
                         if (j != i) {
-                            double rx, ry, rz;
-                            double rsq = pairvec_exact(c, si1, si2, si3, sx[j], sy[j], sz[j], rx, ry, rz);
-                            in_a = rsq <= rsq_a;
-                            in_b = rsq <= rsq_b;
+                            const float d1 = fold(wi1 - v.x), d2 = fold(wi2 - v.y), d3 = fold(wi3 - v.z);
+                            const float rx = fmaf(d1, A[0], fmaf(d2, A[1], d3 * A[2]));
+                            const float ry = fmaf(d1, A[3], fmaf(d2, A[4], d3 * A[5]));
+                            const float rz = fmaf(d1, A[6], fmaf(d2, A[7], d3 * A[8]));
+                            const float m = fmaxf(fabsf(d1), fmaxf(fabsf(d2), fabsf(d3)));
+                            keep = fmaf(rx, rx, fmaf(ry, ry, rz * rz)) <= pre.thr || m > 0.4999f;
                         }
                     }
-                    unsigned ma = __ballot_sync(0xffffffffu, in_a);
-                    if (in_a) {
-                        int pos = na + __popc(ma & lt);
-                        if (pos < cap_a) nbr_a[(size_t)i * cap_a + pos] = j;
-                    }
-                    na += __popc(ma);
-                    if (nbr_b) {
-                        unsigned mb = __ballot_sync(0xffffffffu, in_b);
-                        if (in_b) {
-                            int pos = nb + __popc(mb & lt);
-                            if (pos < cap_b) nbr_b[(size_t)i * cap_b + pos] = j;
-                        }
-                        nb += __popc(mb);
+                    const unsigned mk = __ballot_sync(0xffffffffu, keep);
+                    if (keep) q[nq + __popc(mk & lt)] = j;
+                    nq += __popc(mk);
+                    __syncwarp();
+                    if (nq >= 32) {
+                        decide(32);
+                        __syncwarp();
+                        const int rest = nq - 32;
+                        const int moved = lane < rest ? q[32 + lane] : 0;
+                        __syncwarp();
+                        if (lane < rest) q[lane] = moved;
+                        __syncwarp();
+                        nq = rest;
                     }
                 }
             }
         }
     }
+    if (nq > 0) decide(nq);
     if (lane == 0) {
         cnt_a[i] = na < cap_a ? na : cap_a;
         if (na > cap_a) atomicMax(overflow, na);
@@ -221,11 +302,22 @@ __global__ void k_nlist(int n, const double* __restrict__ sx, const double* __re
 
 void launch_nlist(cudaStream_t st, int n, const double* sx, const double* sy, const double* sz, CellP c,
                   const CellGrid& g, double rsq_a, NList& la, double rsq_b, NList* lb, int* overflow) {
-    int threads = 256;
-    int blocks = (int)(((size_t)n * 32 + threads - 1) / threads);
-    k_nlist<<<blocks, threads, 0, st>>>(n, sx, sy, sz, c, g.cell_of, g.cell_start, g.cell_atoms, g.nc[0], g.nc[1],
-                                        g.nc[2], rsq_a, la.nbr, la.cnt, la.cap, rsq_b, lb ? lb->nbr : nullptr,
-                                        lb ? lb->cnt : nullptr, lb ? lb->cap : 0, overflow);
+    // FP32 error bound of the prefilter's distance: each wrapped fractional
+    // coordinate is within 2^-25 of exact, a difference within 2^-24 more, and
+    // the Cartesian products add under 2^-23 of |A| |d| (|d| <= 1/2); so a
+    // component is off by at most ~2.1e-7 of its row's |A| sum.  Take 5e-7 of
+    // the largest row sum, for every component, and pad r^2 accordingly.
+    double row = 0.0;
+    for (int a = 0; a < 3; ++a) row = std::max(row, std::fabs(c.A[3 * a]) + std::fabs(c.A[3 * a + 1]) + std::fabs(c.A[3 * a + 2]));
+    const double del = 5e-7 * row * std::sqrt(3.0);
+    const double rmax2 = std::max(rsq_a, lb ? rsq_b : 0.0), rmax = std::sqrt(rmax2);
+    NlPre pre;
+    for (int e = 0; e < 9; ++e) pre.A[e] = (float)c.A[e];
+    pre.thr = std::nextafter((float)(rmax2 + 2.0 * rmax * del + del * del + 1e-6 * rmax2), INFINITY);
+    const int blocks = (int)(((size_t)n * 32 + NL_THREADS - 1) / NL_THREADS);
+    k_nlist<<<blocks, NL_THREADS, 0, st>>>(n, sx, sy, sz, c, g.cell_of, g.cell_start, g.cell_w, g.nc[0], g.nc[1],
+                                           g.nc[2], pre, rsq_a, la.nbr, la.cnt, la.cap, rsq_b, lb ? lb->nbr : nullptr,
+                                           lb ? lb->cnt : nullptr, lb ? lb->cap : 0, overflow);
 }
 
 // ------------------------------------------------------------ skin check --

@@ -924,14 +924,17 @@ int autotune(mdff_ctx* ctx) {
     ctx->prof.on = false;
     CK(cudaMemsetAsync(ctx->mu, 0, sizeof(double) * 3 * n, ctx->st));
     const int gs[3] = {8, 16, 32};
+    // three interleaved rounds over the candidates, each scored by its fastest
+    // round: a single disturbed measurement (one pass picked a shape 20 %
+    // slower in the solve) does not decide the shape
     auto pick = [&](const std::function<void(int)>& run, const int* cand, int nc) {
-        int best = cand[0];
-        float tb = 1e30f;
-        for (int k = 0; k < nc; ++k) {
-            float t = time_launch(ctx, [&] { run(cand[k]); });
-            if (t < tb) { tb = t; best = cand[k]; }
-        }
-        return best;
+        std::vector<float> tmin((size_t)nc, 1e30f);
+        for (int round = 0; round < 3; ++round)
+            for (int k = 0; k < nc; ++k) tmin[k] = std::min(tmin[k], time_launch(ctx, [&] { run(cand[k]); }));
+        int best = 0;
+        for (int k = 1; k < nc; ++k)
+            if (tmin[k] < tmin[best]) best = k;
+        return cand[best];
     };
     DirFlags f = dir_flags(ctx);
     f.qq = 1;

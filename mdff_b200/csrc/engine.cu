@@ -3309,6 +3309,11 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 // field pass
                 tc.KZ = ((2 * kg.nzl + 31) / 32) * 32;
                 tc.ntile_f = (n + 127) / 128;
+                {
+                    int sms = 148;
+                    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
+                    tc.grid_f = std::max(1, std::min(tc.ntile_f, sms));
+                }
                 const tcf::FLayout f2(tc.KZ, tc.XYW, tcf::Cfg<2>::NB, tcf::Cfg<2>::CB);
                 const tcf::FLayout f3(tc.KZ, tc.XYW, tcf::Cfg<3>::NB, tcf::Cfg<3>::CB);
                 tc.smem_f2 = f2.smem_bytes();
@@ -3335,7 +3340,7 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
         }
         size_t fp = 0;
         size_t pc = std::max(tc_part, rec_scratch_doubles(n, kg, &fp, p.precision == MDFF_PREC_MIXED));
-        fp = std::max(fp, (size_t)tcf::NQ * 9 * n);   // the tensor-core field pass writes NQ column parts
+        fp = std::max(fp, (size_t)2 * tcf::NQ * 9 * n);   // tensor-core field pass: NQ column parts x 2 column slots
         TRY(dalloc(ctx, &ctx->rs.part, pc));
         TRY(dalloc(ctx, &ctx->rs.fpart, fp));
         TRY(dalloc(ctx, &ctx->rs.aks, 2 * (size_t)kg.nrect));

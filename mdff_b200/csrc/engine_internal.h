@@ -282,6 +282,7 @@ struct TcK {
     float* amax = nullptr;    // [npad]
     // field pass
     int ntile_f = 0, KZ = 0;  // 128-atom tiles, K bytes (nz, re/im) per atom row
+    int grid_f = 0;           // field CTAs: min(tiles, SMs), each an equal share of (tile, column block) units
     uint8_t* aimg = nullptr;  // [ntile_f] Z digit images
     float2* xyt = nullptr;    // [ntile_f][XYW][128] X/Y tables
     uint8_t* fimg = nullptr;  // per evaluation: B digit images + column constants

@@ -1168,8 +1168,8 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             tcf::k_tcf_bimage<3><<<ncb, C3::NB * nch, 0, st>>>(t.nsph, t.cols, kx, ky, kz, kg.nzl, t.KZ, rs.aks,
                                                                 kg.nrect, c, t.fimg);
             prof->detail_begin(PD_TC_FIELD);
-            tcf::k_kfield_tc<3><<<t.ntile_f, tcf::THREADS, t.smem_f3, st>>>(n, ncb, t.aimg, t.xyt, t.fimg, t.KZ, t.XYW,
-                                                                             c, rs.fpart, &d->tc_err);
+            tcf::k_kfield_tc<3><<<t.grid_f, tcf::THREADS, t.smem_f3, st>>>(n, t.ntile_f, ncb, t.aimg, t.xyt, t.fimg,
+                                                                            t.KZ, t.XYW, c, rs.fpart, &d->tc_err);
             prof->detail_end(PD_TC_FIELD, 6.0 * 2.0 * n * (6.0 * t.nsph) * (2.0 * kg.nzl));
         } else {
             using C2 = tcf::Cfg<2>;
@@ -1177,11 +1177,11 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             tcf::k_tcf_bimage<2><<<ncb, C2::NB * nch, 0, st>>>(t.nsph, t.cols, kx, ky, kz, kg.nzl, t.KZ, rs.aks,
                                                                 kg.nrect, c, t.fimg);
             prof->detail_begin(PD_TC_FIELD);
-            tcf::k_kfield_tc<2><<<t.ntile_f, tcf::THREADS, t.smem_f2, st>>>(n, ncb, t.aimg, t.xyt, t.fimg, t.KZ, t.XYW,
-                                                                             c, rs.fpart, &d->tc_err);
+            tcf::k_kfield_tc<2><<<t.grid_f, tcf::THREADS, t.smem_f2, st>>>(n, t.ntile_f, ncb, t.aimg, t.xyt, t.fimg,
+                                                                            t.KZ, t.XYW, c, rs.fpart, &d->tc_err);
             prof->detail_end(PD_TC_FIELD, 6.0 * 2.0 * n * (4.0 * t.nsph) * (2.0 * kg.nzl));
         }
-        nsplit_f = tcf::NQ;
+        nsplit_f = 2 * tcf::NQ;   // NQ column parts in each of the 2 column slots
         nk += 1;
         if (low) nk += launch_low_field(st, n, c, grad, rs, d, prof);
     } else if (mixed) {

@@ -549,24 +549,48 @@ __device__ __forceinline__ float comb3(float d0, float d1, float d2) {
     return fmaf((float)t, 256.f, (float)__float_as_int(d2));
 }
 
-// grid = 128-atom tiles; THREADS threads; dynamic shared memory FLayout::smem_bytes().
-// Writes fpart[(part * nv + component) * n + i] for the NQ column parts
-// (nv = 3, or 9 with the field gradient).
+// The work is ntile x ncb units (128-atom tile, column block).  CTA b of a
+// grid of G <= ntile takes the contiguous units [b U, b U + U), U = ceil(
+// ntile ncb / G), so every SM gets the same share (one tile per CTA would
+// leave a partial second wave) and, as U >= ncb, a tile is split between at
+// most two CTAs.  Its units form segments, one per tile it touches; for each
+// segment the tile's A image and X/Y table are loaded again once the previous
+// segment's MMAs and epilogue reads are done.  A segment that starts at a
+// tile's first column block writes column slot 0 of the tile (and zeros slot
+// 1 when it covers the whole tile), one that starts inside it slot 1.
+struct FSeg {
+    int t0, t1, u0, u1, ncb;
+    __device__ FSeg(int ntile, int ncb_, int G, int b) : ncb(ncb_) {
+        const long T = (long)ntile * ncb_, U = (T + G - 1) / G;
+        u0 = (int)min(T, (long)b * U);
+        u1 = (int)min(T, (long)b * U + U);
+        t0 = u0 / ncb;
+        t1 = u1 > u0 ? (u1 - 1) / ncb : t0 - 1;   // no segment when the range is empty
+    }
+    __device__ int b0(int t) const { return max(u0 - t * ncb, 0); }
+    __device__ int b1(int t) const { return min(u1 - t * ncb, ncb); }
+};
+
+// grid = FSeg's G CTAs (at most one per tile); THREADS threads; dynamic
+// shared memory FLayout::smem_bytes().  Writes fpart[((slot NQ + part) nv +
+// component) n + i] for the NQ column parts and the 2 column slots (nv = 3,
+// or 9 with the field gradient).
 template <int NMOM>
 __global__ void __launch_bounds__(THREADS, 1)
-    k_kfield_tc(int n, int ncb, const uint8_t* __restrict__ aimg, const float2* __restrict__ xyt,
+    k_kfield_tc(int n, int ntile, int ncb, const uint8_t* __restrict__ aimg, const float2* __restrict__ xyt,
                 const uint8_t* __restrict__ bimg, int KZ, int XYW, CellP c, double* __restrict__ fpart,
                 int* __restrict__ err) {
     using C = Cfg<NMOM>;
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t ares, bfull[NBS], bempty[NBS], accfull[2], accfree[2], fin;
+    __shared__ __align__(8) uint64_t ares, aempty, bfull[NBS], bempty[NBS], accfull[2], accfree[2], fin;
     __shared__ uint32_t tslot;
     __shared__ volatile int abort_;
     const FLayout L(KZ, XYW, C::NB, C::CB);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile = blockIdx.x;
+    const FSeg S(ntile, ncb, gridDim.x, blockIdx.x);
     if (tid == 0) {
         umma::mbar_init(&ares, 1);
+        umma::mbar_init(&aempty, 1 + EPW);   // the MMA warp's commit + every epilogue warp
         for (int b = 0; b < NBS; ++b) {
             umma::mbar_init(&bfull[b], 1);
             umma::mbar_init(&bempty[b], 1 + EPW);
@@ -587,17 +611,25 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t sbase = umma::smem_u32(smem);
 
     if (warp == EPW + 1) {
-        // ---- copies: the tile's A image and X/Y table, then the B stages
+        // ---- copies: lane 0 streams the B stages of every segment's column
+        // blocks (q counts blocks over the whole range); lane 1 loads each
+        // segment's A image and X/Y table once the previous segment is done
         if (lane == 0) {
-            umma::mbar_arrive_expect_tx(&ares, L.a_bytes() + L.xy_bytes());
-            umma::bulk_g2s(smem + L.a_off, aimg + (size_t)tile * L.a_bytes(), L.a_bytes(), &ares);
-            umma::bulk_g2s(smem + L.xy_off, xyt + (size_t)tile * XYW * 128, L.xy_bytes(), &ares);
-            for (int q = 0; q < ncb; ++q) {
-                const int bs = q % NBS;
-                if (q >= NBS && !f_wait(&bempty[bs], ((q / NBS) - 1) & 1, err, 1, &abort_)) break;
-                umma::mbar_arrive_expect_tx(&bfull[bs], L.img_bytes);
-                umma::bulk_g2s(smem + L.b_off + bs * L.stage_bytes, bimg + (size_t)q * L.stage_bytes, L.img_bytes,
-                               &bfull[bs]);
+            int q = 0;
+            for (int t = S.t0; t <= S.t1 && !abort_; ++t)
+                for (int bl = S.b0(t); bl < S.b1(t); ++bl, ++q) {
+                    const int bs = q % NBS;
+                    if (q >= NBS && !f_wait(&bempty[bs], ((q / NBS) - 1) & 1, err, 1, &abort_)) break;
+                    umma::mbar_arrive_expect_tx(&bfull[bs], L.img_bytes);
+                    umma::bulk_g2s(smem + L.b_off + bs * L.stage_bytes, bimg + (size_t)bl * L.stage_bytes,
+                                   L.img_bytes, &bfull[bs]);
+                }
+        } else if (lane == 1) {
+            for (int t = S.t0, sg = 0; t <= S.t1; ++t, ++sg) {
+                if (sg > 0 && !f_wait(&aempty, (sg - 1) & 1, err, 128, &abort_)) break;
+                umma::mbar_arrive_expect_tx(&ares, L.a_bytes() + L.xy_bytes());
+                umma::bulk_g2s(smem + L.a_off, aimg + (size_t)t * L.a_bytes(), L.a_bytes(), &ares);
+                umma::bulk_g2s(smem + L.xy_off, xyt + (size_t)t * XYW * 128, L.xy_bytes(), &ares);
             }
         }
     } else if (warp == EPW) {
@@ -615,25 +647,33 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint64_t bdesc0 = umma::desc_kmajor(sbase + L.b_off, lboB, 128);
             const uint32_t aslice = (128u * KZ) >> 4;
             const uint32_t astep = (2 * lboA) >> 4, bkstep = (2 * lboB) >> 4, bstage = L.stage_bytes >> 4;
-            bool ok = __all_sync(0xffffffffu, f_wait(&ares, 0, err, 2, &abort_));
-            for (int q = 0; q < ncb && ok; ++q) {
-                const int bs = q % NBS, tb = q & 1;
-                ok = __all_sync(0xffffffffu, f_wait(&bfull[bs], (q / NBS) & 1, err, 4, &abort_));
-                if (ok && q >= 2) ok = __all_sync(0xffffffffu, f_wait(&accfree[tb], ((q >> 1) - 1) & 1, err, 8, &abort_));
-                if (!ok) break;
+            bool ok = true;
+            int q = 0;
+            for (int t = S.t0, sg = 0; t <= S.t1 && ok; ++t, ++sg) {
+                ok = __all_sync(0xffffffffu, f_wait(&ares, sg & 1, err, 2, &abort_));
                 umma::fence_after_sync();
-                const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
-                for (int ks = 0; ks < KZ / 32; ++ks) {
+                for (int bl = S.b0(t); bl < S.b1(t) && ok; ++bl, ++q) {
+                    const int bs = q % NBS, tb = q & 1;
+                    ok = __all_sync(0xffffffffu, f_wait(&bfull[bs], (q / NBS) & 1, err, 4, &abort_));
+                    if (ok && q >= 2)
+                        ok = __all_sync(0xffffffffu, f_wait(&accfree[tb], ((q >> 1) - 1) & 1, err, 8, &abort_));
+                    if (!ok) break;
+                    umma::fence_after_sync();
+                    const uint64_t bq = bdesc0 + (uint64_t)(bs * bstage);
+                    for (int ks = 0; ks < KZ / 32; ++ks) {
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
-                        const uint64_t bd = bq + (uint64_t)(ks * bkstep);
-                        const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
-                        umma::mma_s8_warp(tmem + tb * C::BUFC + i * C::LV, ad, bd, idesc[i], acc);
+                        for (int i = 0; i < 3; ++i) {
+                            const uint64_t ad = adesc0 + (uint64_t)(i * aslice + ks * astep);
+                            const uint64_t bd = bq + (uint64_t)(ks * bkstep);
+                            const uint32_t acc = (ks > 0 || i > 0) ? 1u : 0u;
+                            umma::mma_s8_warp(tmem + tb * C::BUFC + i * C::LV, ad, bd, idesc[i], acc);
+                        }
                     }
+                    umma::commit_warp(&accfull[tb]);
+                    umma::commit_warp(&bempty[bs]);
                 }
-                umma::commit_warp(&accfull[tb]);
-                umma::commit_warp(&bempty[bs]);
+                // the segment's A image is free once these MMAs are done
+                umma::commit_warp(&aempty);
             }
             umma::commit_warp(&fin);
         }
@@ -641,79 +681,92 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ---- epilogue: atom row = 32 (warp % 4) + lane, column part = warp / 4
         const int qd = warp & 3, part = warp >> 2;
         const int r = 32 * qd + lane;
-        const int i = tile * 128 + r;
         const float2* sxy = reinterpret_cast<const float2*>(smem + L.xy_off);
-        double E[3] = {0, 0, 0}, G[6] = {0, 0, 0, 0, 0, 0}, H[3] = {0, 0, 0}, SI1 = 0, SR2 = 0;
         const uint32_t lane_base = tmem + ((uint32_t)(32 * qd) << 16);
         constexpr int WN = C::HC * NMOM * 2;   // accumulator columns per warp per level (32 or 24)
         static_assert(WN <= 32 && C::HC * NQ == C::CB, "two 16-column loads per digit level at most");
-        bool ok = f_wait(&ares, 0, err, 16, &abort_);
-        for (int q = 0; q < ncb && ok; ++q) {
-            const int bs = q % NBS, tb = q & 1;
-            if (!f_wait(&accfull[tb], (q >> 1) & 1, err, 32, &abort_)) break;
-            umma::fence_after_sync();
-            float d[3][32];
+        bool ok = true;
+        int q = 0;
+        for (int t = S.t0, sg = 0; t <= S.t1 && ok; ++t, ++sg) {
+            const int i = t * 128 + r;
+            double E[3] = {0, 0, 0}, G[6] = {0, 0, 0, 0, 0, 0}, H[3] = {0, 0, 0}, SI1 = 0, SR2 = 0;
+            ok = __all_sync(0xffffffffu, f_wait(&ares, sg & 1, err, 16, &abort_));
+            for (int bl = S.b0(t); bl < S.b1(t) && ok; ++bl, ++q) {
+                const int bs = q % NBS, tb = q & 1;
+                ok = __all_sync(0xffffffffu, f_wait(&accfull[tb], (q >> 1) & 1, err, 32, &abort_));
+                if (!ok) break;
+                umma::fence_after_sync();
+                float d[3][32];
 #pragma unroll
-            for (int lv = 0; lv < 3; ++lv)
+                for (int lv = 0; lv < 3; ++lv)
 #pragma unroll
-                for (int h = 0; h < (WN + 15) / 16; ++h)
-                    umma::tmem_ld16(lane_base + tb * C::BUFC + lv * C::LV + part * WN + 16 * h, d[lv] + 16 * h);
-            umma::tmem_wait_ld();
-            umma::fence_before_sync();
-            __syncwarp();
-            if (lane == 0) umma::mbar_arrive(&accfree[tb]);
-            const float* kcst = reinterpret_cast<const float*>(smem + L.b_off + bs * L.stage_bytes + 3 * C::NB * KZ);
-            float e0 = 0.f, e1 = 0.f, e2 = 0.f, si1 = 0.f;
-            float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, h[3] = {0.f, 0.f, 0.f}, sr2 = 0.f;
+                    for (int h = 0; h < (WN + 15) / 16; ++h)
+                        umma::tmem_ld16(lane_base + tb * C::BUFC + lv * C::LV + part * WN + 16 * h, d[lv] + 16 * h);
+                umma::tmem_wait_ld();
+                umma::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) umma::mbar_arrive(&accfree[tb]);
+                const float* kcst = reinterpret_cast<const float*>(smem + L.b_off + bs * L.stage_bytes + 3 * C::NB * KZ);
+                float e0 = 0.f, e1 = 0.f, e2 = 0.f, si1 = 0.f;
+                float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, h[3] = {0.f, 0.f, 0.f}, sr2 = 0.f;
 #pragma unroll
-            for (int cc = 0; cc < C::HC; ++cc) {
-                const float* k = kcst + (part * C::HC + cc) * NCONST;
-                const float4 k0 = *reinterpret_cast<const float4*>(k);
-                const int ex = __float_as_int(k[14]), ey = __float_as_int(k[15]);
-                const float2 X = sxy[ex * 128 + r], Y = sxy[ey * 128 + r];
-                const float wr = fmaf(X.x, Y.x, -X.y * Y.y), wi = fmaf(X.x, Y.y, X.y * Y.x);
-                const int o = cc * NMOM * 2;
-                const float f0r = comb3(d[0][o], d[1][o], d[2][o]), f0i = comb3(d[0][o + 1], d[1][o + 1], d[2][o + 1]);
-                const float f1r = comb3(d[0][o + 2], d[1][o + 2], d[2][o + 2]);
-                const float f1i = comb3(d[0][o + 3], d[1][o + 3], d[2][o + 3]);
-                const float i0 = fmaf(wr, f0i, wi * f0r), i1 = fmaf(wr, f1i, wi * f1r);
-                e0 = fmaf(k0.x, i0, e0);
-                e1 = fmaf(k0.y, i0, e1);
-                e2 = fmaf(k0.z, i0, e2);
-                si1 = fmaf(k0.w, i1, si1);
+                for (int cc = 0; cc < C::HC; ++cc) {
+                    const float* k = kcst + (part * C::HC + cc) * NCONST;
+                    const float4 k0 = *reinterpret_cast<const float4*>(k);
+                    const int ex = __float_as_int(k[14]), ey = __float_as_int(k[15]);
+                    const float2 X = sxy[ex * 128 + r], Y = sxy[ey * 128 + r];
+                    const float wr = fmaf(X.x, Y.x, -X.y * Y.y), wi = fmaf(X.x, Y.y, X.y * Y.x);
+                    const int o = cc * NMOM * 2;
+                    const float f0r = comb3(d[0][o], d[1][o], d[2][o]), f0i = comb3(d[0][o + 1], d[1][o + 1], d[2][o + 1]);
+                    const float f1r = comb3(d[0][o + 2], d[1][o + 2], d[2][o + 2]);
+                    const float f1i = comb3(d[0][o + 3], d[1][o + 3], d[2][o + 3]);
+                    const float i0 = fmaf(wr, f0i, wi * f0r), i1 = fmaf(wr, f1i, wi * f1r);
+                    e0 = fmaf(k0.x, i0, e0);
+                    e1 = fmaf(k0.y, i0, e1);
+                    e2 = fmaf(k0.z, i0, e2);
+                    si1 = fmaf(k0.w, i1, si1);
+                    if (NMOM == 3) {
+                        const float f2r = comb3(d[0][o + 4], d[1][o + 4], d[2][o + 4]);
+                        const float f2i = comb3(d[0][o + 5], d[1][o + 5], d[2][o + 5]);
+                        const float r0 = fmaf(wr, f0r, -wi * f0i), r1 = fmaf(wr, f1r, -wi * f1i);
+                        const float r2 = fmaf(wr, f2r, -wi * f2i);
+                        const float4 k1 = *reinterpret_cast<const float4*>(k + 4);
+                        const float4 k2 = *reinterpret_cast<const float4*>(k + 8);
+                        const float4 k3 = *reinterpret_cast<const float4*>(k + 12);
+                        g[0] = fmaf(k1.x, r0, g[0]); g[1] = fmaf(k1.y, r0, g[1]); g[2] = fmaf(k1.z, r0, g[2]);
+                        g[3] = fmaf(k1.w, r0, g[3]); g[4] = fmaf(k2.x, r0, g[4]); g[5] = fmaf(k2.y, r0, g[5]);
+                        h[0] = fmaf(k2.z, r1, h[0]); h[1] = fmaf(k2.w, r1, h[1]); h[2] = fmaf(k3.x, r1, h[2]);
+                        sr2 = fmaf(k3.y, r2, sr2);
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) umma::mbar_arrive(&bempty[bs]);
+                E[0] += e0; E[1] += e1; E[2] += e2; SI1 += si1;
                 if (NMOM == 3) {
-                    const float f2r = comb3(d[0][o + 4], d[1][o + 4], d[2][o + 4]);
-                    const float f2i = comb3(d[0][o + 5], d[1][o + 5], d[2][o + 5]);
-                    const float r0 = fmaf(wr, f0r, -wi * f0i), r1 = fmaf(wr, f1r, -wi * f1i);
-                    const float r2 = fmaf(wr, f2r, -wi * f2i);
-                    const float4 k1 = *reinterpret_cast<const float4*>(k + 4);
-                    const float4 k2 = *reinterpret_cast<const float4*>(k + 8);
-                    const float4 k3 = *reinterpret_cast<const float4*>(k + 12);
-                    g[0] = fmaf(k1.x, r0, g[0]); g[1] = fmaf(k1.y, r0, g[1]); g[2] = fmaf(k1.z, r0, g[2]);
-                    g[3] = fmaf(k1.w, r0, g[3]); g[4] = fmaf(k2.x, r0, g[4]); g[5] = fmaf(k2.y, r0, g[5]);
-                    h[0] = fmaf(k2.z, r1, h[0]); h[1] = fmaf(k2.w, r1, h[1]); h[2] = fmaf(k3.x, r1, h[2]);
-                    sr2 = fmaf(k3.y, r2, sr2);
+                    for (int e = 0; e < 6; ++e) G[e] += g[e];
+                    for (int e = 0; e < 3; ++e) H[e] += h[e];
+                    SR2 += sr2;
                 }
             }
+            // the segment's X/Y table is no longer read
             __syncwarp();
-            if (lane == 0) umma::mbar_arrive(&bempty[bs]);
-            E[0] += e0; E[1] += e1; E[2] += e2; SI1 += si1;
-            if (NMOM == 3) {
-                for (int e = 0; e < 6; ++e) G[e] += g[e];
-                for (int e = 0; e < 3; ++e) H[e] += h[e];
-                SR2 += sr2;
-            }
-        }
-        if (i < n && !abort_) {
-            const double b3[3] = {2.0 * PI * c.B[2], 2.0 * PI * c.B[5], 2.0 * PI * c.B[8]};
-            const int nv = NMOM == 3 ? 9 : 3;
-            double* o = fpart + (size_t)part * nv * n;
-            for (int dd = 0; dd < 3; ++dd) o[(size_t)dd * n + i] = E[dd] + b3[dd] * SI1;
-            if (NMOM == 3) {
-                const int pd[6] = {0, 1, 2, 0, 0, 1}, pe[6] = {0, 1, 2, 1, 2, 2};
-                for (int e = 0; e < 6; ++e)
-                    o[(size_t)(3 + e) * n + i] =
-                        G[e] + b3[pe[e]] * H[pd[e]] + b3[pd[e]] * H[pe[e]] + b3[pd[e]] * b3[pe[e]] * SR2;
+            if (lane == 0) umma::mbar_arrive(&aempty);
+            if (ok && i < n && !abort_) {
+                const double b3[3] = {2.0 * PI * c.B[2], 2.0 * PI * c.B[5], 2.0 * PI * c.B[8]};
+                const int nv = NMOM == 3 ? 9 : 3;
+                const int slot = S.b0(t) > 0 ? 1 : 0;
+                double* o = fpart + (size_t)(slot * NQ + part) * nv * n;
+                for (int dd = 0; dd < 3; ++dd) o[(size_t)dd * n + i] = E[dd] + b3[dd] * SI1;
+                if (NMOM == 3) {
+                    const int pd[6] = {0, 1, 2, 0, 0, 1}, pe[6] = {0, 1, 2, 1, 2, 2};
+                    for (int e = 0; e < 6; ++e)
+                        o[(size_t)(3 + e) * n + i] =
+                            G[e] + b3[pe[e]] * H[pd[e]] + b3[pd[e]] * H[pe[e]] + b3[pd[e]] * b3[pe[e]] * SR2;
+                }
+                if (slot == 0 && S.b1(t) == ncb) {   // the whole tile here: its slot 1 is empty
+                    double* z = fpart + (size_t)(NQ + part) * nv * n;
+                    for (int k = 0; k < nv; ++k) z[(size_t)k * n + i] = 0.0;
+                }
             }
         }
     }

@@ -3304,7 +3304,8 @@ int mdff_set_system(mdff_ctx* ctx, int natm, const int* itype, const double* rx,
                 TRY(dalloc(ctx, &tc.bimg, (size_t)tc.nblk * lay.b_bytes()));
                 TRY(dalloc(ctx, &tc.prm, (size_t)tc.npad));
                 TRY(dalloc(ctx, &tc.amax, (size_t)tc.npad));
-                CK(cudaFuncSetAttribute(tcs::k_sfac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc.smem));
+                CK(cudaFuncSetAttribute(tcs::k_sfac_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc.smem));
+                CK(cudaFuncSetAttribute(tcs::k_sfac_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc.smem));
                 tc_part = 2 * (size_t)tc.nsplit * kg.ncol * (((kg.nzl + TM - 1) / TM) * TM);
                 // field pass
                 tc.KZ = ((2 * kg.nzl + 31) / 32) * 32;

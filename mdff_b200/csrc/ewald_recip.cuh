@@ -1089,9 +1089,14 @@ void launch_ewald_rec(cudaStream_t st, int n, const double* sx, const double* sy
             // int8 digit-product operations of the unpadded GEMM: 6 products of
             // 2 M N K, M = sphere columns, N = 2 nz rows, K = 4 per atom
             prof->detail_begin(PD_TC_SFAC);
-            tcs::k_sfac_tc<<<dim3(t.ntile, t.nsplit), tcs::THREADS, t.smem, st>>>(
-                t.nblk, t.bps, t.bimg, t.xy, t.prm, t.amax, t.cols, t.nsph, kx, ky, kz, kg.nzl, t.N, t.XYW, kg.ncol,
-                tplane, pre, pim, &d->tc_err);
+            if (fl.with_q)
+                tcs::k_sfac_tc<true><<<dim3(t.ntile, t.nsplit), tcs::THREADS, t.smem, st>>>(
+                    t.nblk, t.bps, t.bimg, t.xy, t.prm, t.amax, t.cols, t.nsph, kx, ky, kz, kg.nzl, t.N, t.XYW,
+                    kg.ncol, tplane, pre, pim, &d->tc_err);
+            else
+                tcs::k_sfac_tc<false><<<dim3(t.ntile, t.nsplit), tcs::THREADS, t.smem, st>>>(
+                    t.nblk, t.bps, t.bimg, t.xy, t.prm, t.amax, t.cols, t.nsph, kx, ky, kz, kg.nzl, t.N, t.XYW,
+                    kg.ncol, tplane, pre, pim, &d->tc_err);
             prof->detail_end(PD_TC_SFAC, 6.0 * 2.0 * t.nsph * (2.0 * kg.nzl) * (4.0 * n));
             Pr = t.nsplit;
             nk += 2;

@@ -152,6 +152,10 @@ __device__ __forceinline__ bool tc_wait(uint64_t* b, uint32_t parity, int* err, 
 }
 
 // grid (tiles, splits); THREADS threads; dynamic shared memory Layout::smem_bytes().
+// Q = false when the sources carry no charges (the solver's operator
+// applications): the amplitude's real part is zero and its products drop out,
+// with the same digits (an FMA with a zero product returns its addend).
+template <bool Q>
 __global__ void __launch_bounds__(THREADS, 1)
     k_sfac_tc(int nblk, int bps, const uint8_t* __restrict__ bimg, const float2* __restrict__ xy,
               const float4* __restrict__ prm, const float* __restrict__ amax, const int* __restrict__ cols, int nsph,
@@ -218,8 +222,16 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const float2 X = sxy[al * XYW + ex], Y = sxy[al * XYW + ey];
                     const float4 P = sp[al];
                     const float xr = fmaf(X.x, Y.x, -X.y * Y.y), xi = fmaf(X.x, Y.y, X.y * Y.x);
-                    const float ar = P.x * rinv, ai = fmaf(fnx, P.y, fny * P.z), gg = P.w * gk;
-                    const float a0r = fmaf(xr, ar, -xi * ai), a0i = fmaf(xr, ai, xi * ar);
+                    const float ai = fmaf(fnx, P.y, fny * P.z), gg = P.w * gk;
+                    float a0r, a0i;
+                    if (Q) {
+                        const float ar = P.x * rinv;
+                        a0r = fmaf(xr, ar, -xi * ai);
+                        a0i = fmaf(xr, ai, xi * ar);
+                    } else {
+                        a0r = -xi * ai;
+                        a0i = xr * ai;
+                    }
                     const float a1r = xr * gg, a1i = xi * gg;
                     umma::slices4(umma::digits24(__float2int_rn(a0r)), umma::digits24(__float2int_rn(a0i)),
                                   umma::digits24(__float2int_rn(a1r)), umma::digits24(__float2int_rn(a1i)), w1[u],

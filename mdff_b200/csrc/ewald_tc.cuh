@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         // as far ahead as the buffers allow
         if (lane == 0) {
             const uint32_t bytes = L.b_bytes() + SA * XYW * 8u + SA * 16u;
+            int last = -1;
             for (int s = 0; s < nst; ++s) {
                 const int b = s % NBUF, blk = blk0 + s;
                 if (s >= NBUF && !tc_wait(&empty[b], ((s / NBUF) - 1) & 1, err, 1, &stop)) break;
@@ -260,7 +261,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                 umma::bulk_g2s(bb + L.b_off, bimg + (size_t)blk * L.b_bytes(), L.b_bytes(), &full[b]);
                 umma::bulk_g2s(bb + L.xy_off, xy + (size_t)blk * SA * XYW, SA * XYW * 8u, &full[b]);
                 umma::bulk_g2s(bb + L.p_off, prm + (size_t)blk * SA, SA * 16u, &full[b]);
+                last = s;
             }
+            // every copy issued has landed before the CTA can exit, also when the
+            // pipeline was abandoned on an error (bounded, whatever the stop flag)
+            for (int k = max(0, last - NBUF + 1); k <= last; ++k) umma::mbar_wait_ns(&full[k % NBUF], (k / NBUF) & 1, WAIT_NS);
         }
     } else if (lane == 0) {
         // ---- MMA issue: per stage 2 K-steps of 32 x the six digit products.
@@ -626,8 +631,10 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ---- copies: lane 0 streams the B stages of every segment's column
         // blocks (q counts blocks over the whole range); lane 1 loads each
         // segment's A image and X/Y table once the previous segment is done
+        // every copy issued has landed before the CTA can exit, also when the
+        // pipeline was abandoned on an error (bounded waits, whatever the flag)
         if (lane == 0) {
-            int q = 0;
+            int q = 0, last = -1;
             for (int t = S.t0; t <= S.t1 && !abort_; ++t)
                 for (int bl = S.b0(t); bl < S.b1(t); ++bl, ++q) {
                     const int bs = q % NBS;
@@ -635,14 +642,19 @@ __global__ void __launch_bounds__(THREADS, 1)
                     umma::mbar_arrive_expect_tx(&bfull[bs], L.img_bytes);
                     umma::bulk_g2s(smem + L.b_off + bs * L.stage_bytes, bimg + (size_t)bl * L.stage_bytes,
                                    L.img_bytes, &bfull[bs]);
+                    last = q;
                 }
+            for (int k = max(0, last - NBS + 1); k <= last; ++k) umma::mbar_wait_ns(&bfull[k % NBS], (k / NBS) & 1, WAIT_NS);
         } else if (lane == 1) {
+            int last = -1;
             for (int t = S.t0, sg = 0; t <= S.t1; ++t, ++sg) {
                 if (sg > 0 && !f_wait(&aempty, (sg - 1) & 1, err, 128, &abort_)) break;
                 umma::mbar_arrive_expect_tx(&ares, L.a_bytes() + L.xy_bytes());
                 umma::bulk_g2s(smem + L.a_off, aimg + (size_t)t * L.a_bytes(), L.a_bytes(), &ares);
                 umma::bulk_g2s(smem + L.xy_off, xyt + (size_t)t * XYW * 128, L.xy_bytes(), &ares);
+                last = sg;
             }
+            if (last >= 0) umma::mbar_wait_ns(&ares, last & 1, WAIT_NS);
         }
     } else if (warp == EPW) {
         // ---- MMA issue (the whole warp, one elected lane issues): per column

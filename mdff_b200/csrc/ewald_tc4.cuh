@@ -256,6 +256,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         // up to nin stages ahead
         if (lane == 0) {
             const uint32_t bytes = L.b_bytes() + SA * XYW * 16u + SA * 32u;
+            int last = -1;
             for (int s = 0; s < nst; ++s) {
                 const int bi = s % nin, blk = blk0 + s;
                 if (s >= nin && !tc_wait(&inempty[bi], ((s / nin) - 1) & 1, err, 1, &stop)) break;
@@ -264,7 +265,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                 umma::bulk_g2s(ib + L.b_off, bimg + (size_t)blk * L.b_bytes(), L.b_bytes(), &infull[bi]);
                 umma::bulk_g2s(ib + L.xy_off, xy + (size_t)blk * SA * XYW, SA * XYW * 16u, &infull[bi]);
                 umma::bulk_g2s(ib + L.p_off, prm + (size_t)blk * SA, SA * 32u, &infull[bi]);
+                last = s;
             }
+            // every copy issued has landed before the CTA can exit, also when the
+            // pipeline was abandoned on an error (bounded, whatever the stop flag)
+            for (int k = max(0, last - nin + 1); k <= last; ++k) umma::mbar_wait_ns(&infull[k % nin], (k / nin) & 1, WAIT_NS);
         }
     } else if (lane == 0) {
         // ---- MMA issue: per stage 2 K-steps of 32 x the ten digit products as
@@ -581,13 +586,19 @@ __global__ void __launch_bounds__(FTHREADS, 1)
             umma::mbar_arrive_expect_tx(&ares, L.a_bytes() + L.xy_bytes());
             umma::bulk_g2s(smem + L.a_off, aimg + (size_t)tile * L.a_bytes(), L.a_bytes(), &ares);
             umma::bulk_g2s(smem + L.xy_off, xyt + (size_t)tile * XYW * 128, L.xy_bytes(), &ares);
+            int last = -1;
             for (int q = 0; q < ncb; ++q) {
                 const int bs = q % NBS;
                 if (q >= NBS && !tc_wait(&bempty[bs], ((q / NBS) - 1) & 1, err, 1, &abort_)) break;
                 umma::mbar_arrive_expect_tx(&bfull[bs], L.img_bytes);
                 umma::bulk_g2s(smem + L.b_off + bs * L.stage_bytes, bimg + (size_t)q * L.stage_bytes, L.img_bytes,
                                &bfull[bs]);
+                last = q;
             }
+            // every copy issued has landed before the CTA can exit, also when the
+            // pipeline was abandoned on an error (bounded, whatever the stop flag)
+            umma::mbar_wait_ns(&ares, 0, WAIT_NS);
+            for (int k = max(0, last - NBS + 1); k <= last; ++k) umma::mbar_wait_ns(&bfull[k % NBS], (k / NBS) & 1, WAIT_NS);
         }
     } else if (warp == EPW) {
         // ---- MMA issue (the whole warp, one elected lane issues): per column

@@ -370,8 +370,9 @@ __global__ void __launch_bounds__(THREADS, 1)
 //       = sum_c [kc kc^T Re(W F0) + (kc b3^T + b3 kc^T) Re(W F1) + b3 b3^T Re(W F2)],
 // W = X_i[nx] Y_i[ny], kc = nx b1 + ny b2 (b_j = 2 pi (column j of B)),
 //   F_j[i, c] = sum_nz Z_i[nz] nz^j conj(a[c, nz])          (j = 0, 1 [, 2]).
-// F is a complex GEMM: M = 128 atoms per CTA, K = (nz, re/im), N = (column,
-// moment, re/im) in blocks of 16 columns (8 with the field gradient).  As in
+// F is a complex GEMM: M = 128 atoms of a tile, K = (nz, re/im), N = (column,
+// moment, re/im) in blocks of 16 columns (8 with the field gradient); each CTA
+// works through an equal share of the (tile, column block) units (FSeg).  As in
 // the structure factor the operands are 24-bit fixed point in three int8
 // digits with exact S32 accumulation; A (Z of the tile's atoms) is a digit
 // image built per position update, B (nz^j conj(a)) is quantised per
